@@ -1,0 +1,324 @@
+"""Benchmark: coset LDE + Keccak Merkle commit of a 2^20 x 256 Goldilocks trace
+(blowup 4 -> 2^22 rows, Keccak-256 tree over 2^22 per-row leaves, each leaf
+the 256 canonical u64 of one bit-reversed LDE row in little-endian).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One process per GPU (torchrun for N > 1); every rank commits its own trace
+(independent tables, no collective on the data path: weak scaling). A step is
+one LDE + leaves + tree + root readback over one trace. Rank 0 prints one
+JSON line. Inputs are seeded uniform field elements (synthetic).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+P = 0xFFFFFFFF00000001
+LOG_N, M, BLOWUP = 20, 256, 4
+ROWS_PER_LEAF, LITTLE_ENDIAN = 1, True
+METRIC = "proved cycles/s (trace rows committed per second: coset LDE + Keccak Merkle commit)"
+UNIT = "rows/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--log-n", type=int, default=LOG_N)
+    ap.add_argument("--cols", type=int, default=M)
+    ap.add_argument("--blowup", type=int, default=BLOWUP)
+    ap.add_argument("--leaf-layout", default="row-le", choices=["row-le", "pair-be"],
+                    help="row-le: one row per leaf, LE bytes (this workload); pair-be: the prover's row-pair BE leaf")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-log-n", type=int, default=17)
+    return ap.parse_args()
+
+
+def workload(a):
+    rpl, le = (1, True) if a.leaf_layout == "row-le" else (2, False)
+    return {"workload": f"coset LDE {1 << a.log_n}x{a.cols} blowup {a.blowup} + Keccak-256 Merkle commit",
+            "log_n": a.log_n, "cols": a.cols, "blowup": a.blowup, "lde_rows": (1 << a.log_n) * a.blowup,
+            "rows_per_leaf": rpl, "leaf_bytes": "le" if le else "be", "coset_offset": 3,
+            "field": "goldilocks", "l2": "inputs (2 GiB trace, 8 GiB LDE) exceed the 126 MB L2; no flush needed",
+            "parallelism": f"replicas x{a.gpus}"}, rpl, le
+
+
+def synth_trace(n, m, seed):
+    rng = np.random.default_rng(seed)
+    x = rng.integers(0, 2**64, size=(n, m), dtype=np.uint64)
+    # rejection-free uniform in [0, p): the 2^-32 tail above p is folded down
+    return np.where(x >= np.uint64(P), x - np.uint64(P), x)
+
+
+def coset_weights(n, g=3):
+    """g^i / n (crypto/stark/src/prover.rs:458-467), computed with Python ints."""
+    ninv = pow(n, P - 2, P)
+    w = np.empty(n, np.uint64)
+    cur = ninv
+    # blocked power table to keep this fast for n = 2^20
+    step = 4096
+    gs = [pow(g, i, P) for i in range(step)]
+    gstep = pow(g, step, P)
+    base = ninv
+    for b in range(0, n, step):
+        for i in range(min(step, n - b)):
+            w[b + i] = base * gs[i] % P
+        base = base * gstep % P
+    return w
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(a, rpl, le, steps=1):
+    """The oracle (C restatement of the reference CPU path, OpenMP on all host
+    cores) on a bounded sample: 2^cpu_sample_log_n rows x all columns."""
+    import oracle as O
+    n = 1 << a.cpu_sample_log_n
+    t = synth_trace(n, a.cols, 7)
+    w = coset_weights(n)
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        lde = O.coset_lde_row_major(t, a.blowup, w)
+        lv = O.leaves_row_major(lde, rpl, le)
+        O.merkle_root(lv)
+        times.append(time.perf_counter() - t0)
+    dt = statistics.median(times)
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
+    return {"value": n / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"oracle (C restatement, OpenMP) on {n}x{a.cols} rows, blowup {a.blowup}, same leaf layout; "
+                      f"{dt:.2f} s per sample (log n {a.cpu_sample_log_n} vs {a.log_n}: NTT depth slightly favours the CPU)"}
+
+
+def run_reference(a, rank, world):
+    if rank != 0:
+        return
+    cfg, rpl, le = workload(a)
+    cb = cpu_baseline(a, rpl, le, steps=max(1, min(a.steps, 3)))
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": (1 << a.cpu_sample_log_n) / cb["value"] * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64 (Goldilocks)",
+            "data": "synthetic", "config": cfg, "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference is Rust (cargo absent here); its CPU path is timed as the C restatement"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        run_reference(a, rank, world)
+        return
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    from lambda_vm_b200 import native
+    from lambda_vm_b200.device import backend, PinnedBuffer
+    import ctypes as C
+    L = native.lib()
+    be = backend(local)
+    cfg, rpl, le = workload(a)
+    n, m, B = 1 << a.log_n, a.cols, a.blowup
+    N = n * B
+    nl = N // rpl
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+    lay = native.LeafLayout(rpl, 1 if le else 0, 0, 0)
+
+    trace = synth_trace(n, m, 1234 + rank)
+    w = coset_weights(n)
+    d_trace = torch.empty(n * m, dtype=torch.int64, device="cuda")
+    d_w = torch.empty(n, dtype=torch.int64, device="cuda")
+    d_out = torch.empty(N * m, dtype=torch.int64, device="cuda")
+    d_nodes = torch.empty((2 * nl - 1) * 4, dtype=torch.int64, device="cuda")
+    d_trace.copy_(torch.from_numpy(trace.view(np.int64).reshape(-1)))
+    d_w.copy_(torch.from_numpy(w.view(np.int64)))
+    torch.cuda.synchronize()
+    root = (C.c_uint8 * 32)()
+    leaves_ptr = d_nodes.data_ptr() + (nl - 1) * 32
+
+    ev = {k: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for k in ("lde", "leaves", "tree")}
+    kt = {"lde": [], "leaves": [], "tree": []}
+
+    def step(record):
+        with torch.cuda.stream(stream):
+            if record:
+                ev["lde"][0].record(stream)
+            native.check(L.sg_coset_lde(be.h, sh, d_trace.data_ptr(), n, m, B, d_w.data_ptr(), d_out.data_ptr()))
+            if record:
+                ev["lde"][1].record(stream)
+                ev["leaves"][0].record(stream)
+            native.check(L.sg_keccak_leaves(be.h, sh, d_out.data_ptr(), N, m, C.byref(lay), leaves_ptr))
+            if record:
+                ev["leaves"][1].record(stream)
+                ev["tree"][0].record(stream)
+            native.check(L.sg_merkle_build(be.h, sh, leaves_ptr, nl, d_nodes.data_ptr(), root))
+            if record:
+                ev["tree"][1].record(stream)
+        if record:
+            for k in kt:
+                kt[k].append(ev[k][0].elapsed_time(ev[k][1]))
+
+    for _ in range(a.warmup):
+        step(False)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = be.launches()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(a.steps):
+        step(False)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    total_ms = t0.elapsed_time(t1)
+    launches = be.launches() - launches0
+    # per-kernel event breakdown over separate instrumented steps
+    for _ in range(max(2, min(a.steps, 5))):
+        step(True)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if dist:
+        tt = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+        dist.barrier()
+    ms = total_ms / a.steps
+
+    # e2e through the public C-ABI entry point with host buffers (pinned):
+    # H2D of trace + weights, LDE + commit, root D2H, every step.
+    pin = PinnedBuffer(n * m * 8)
+    pin.view(np.uint64)[:] = trace.reshape(-1)
+    wpin = PinnedBuffer(n * 8)
+    wpin.view(np.uint64)[:] = w
+    e2e_steps = max(2, min(a.steps, 5))
+    h = C.c_void_p()
+    for i in range(1 + e2e_steps):
+        if i == 1:
+            torch.cuda.synchronize()
+            et0 = time.perf_counter()
+        native.check(L.sg_lde_commit(be.h, sh, pin.ptr, 0, n, m, B, wpin.ptr, C.byref(lay), None, C.byref(h), root))
+        L.sg_lde_free(be.h, h)
+    e2e_s = (time.perf_counter() - et0) / e2e_steps
+    pin.close()
+    wpin.close()
+
+    if dist:
+        tt = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    med = {k: statistics.median(v) for k, v in kt.items()}
+    # Algorithmic bytes (one launch set): LDE reads n*m*8 and writes B*n*m*8;
+    # leaves read B*n*m*8 and write 32 B per leaf.
+    alg = {"lde": (n * m + N * m) * 8, "leaves": N * m * 8 + nl * 32, "tree": (nl - 1) * 96}
+    dom = max(med, key=med.get)
+    achieved = alg[dom] / (med[dom] * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": {"lde": "k_dft_pass (coset LDE, 4 launches)", "leaves": "k_leaves",
+                                          "tree": "k_merkle_levels"}[dom],
+                "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                "peak_source": peak_src, "traffic": None,
+                "per_kernel_ms": {k: round(v, 3) for k, v in med.items()},
+                "per_kernel_gbs": {k: round(alg[k] / (med[k] * 1e-3) / 1e9, 1) for k in med},
+                "note": "Goldilocks butterflies and Keccak run on the INT pipes; see profiles/ for issue utilisation"}
+    value = world * n / (ms * 1e-3)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u64 (Goldilocks mod-p integer)", "data": "synthetic (seeded uniform field elements)",
+            "config": cfg, "gpu_launches": launches, "clocks": clk, "roofline": roofline,
+            "e2e": {"value": world * n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": n * m * 8 + n * 8,
+                    "d2h_bytes_per_step": 32, "ms_per_step": e2e_s * 1e3,
+                    "path": "sg_lde_commit(host pinned trace) -> root"}}
+    if not a.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline(a, rpl, le)
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

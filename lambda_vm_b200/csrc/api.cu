@@ -1,0 +1,341 @@
+// C-ABI entry points: context, memory, NTT/LDE, leaves, tree, LDE + commit.
+// The per-function reference correspondences are listed in include/starkgpu.h.
+#include <string.h>
+
+#include <string>
+
+#include "common.cuh"
+
+namespace sg {
+
+static thread_local std::string g_err;
+void set_error(const std::string& msg) { g_err = msg; }
+const char* last_error() { return g_err.c_str(); }
+
+int dev_alloc(Ctx* ctx, cudaStream_t st, uint64_t bytes, void** out) {
+    *out = nullptr;
+    if (bytes == 0) return SG_OK;
+    int64_t f = ctx->fail_alloc_after.load();
+    if (f > 0) {
+        if (ctx->fail_alloc_after.fetch_sub(1) == 1) {
+            set_error("injected allocation failure");
+            return SG_ERR_OOM;
+        }
+    }
+    uint64_t cur = ctx->in_use.fetch_add(bytes) + bytes;
+    if (cur > ctx->budget) {
+        ctx->in_use.fetch_sub(bytes);
+        set_error("HBM budget exceeded: need " + std::to_string(bytes) + " bytes, budget " +
+                  std::to_string(ctx->budget) + ", in use " + std::to_string(cur - bytes));
+        return SG_ERR_BUDGET;
+    }
+    uint64_t pk = ctx->peak.load();
+    while (cur > pk && !ctx->peak.compare_exchange_weak(pk, cur)) {
+    }
+    cudaError_t e = cudaMallocAsync(out, bytes, st);
+    if (e != cudaSuccess) {
+        ctx->in_use.fetch_sub(bytes);
+        *out = nullptr;
+        set_error(std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
+        return e == cudaErrorMemoryAllocation ? SG_ERR_OOM : SG_ERR_CUDA;
+    }
+    return SG_OK;
+}
+
+int dev_free(Ctx* ctx, cudaStream_t st, void* p, uint64_t bytes) {
+    if (!p) return SG_OK;
+    cudaError_t e = cudaFreeAsync(p, st);
+    ctx->in_use.fetch_sub(bytes);
+    if (e != cudaSuccess) {
+        set_error(std::string("cudaFreeAsync: ") + cudaGetErrorString(e));
+        return SG_ERR_CUDA;
+    }
+    return SG_OK;
+}
+
+}  // namespace sg
+
+using namespace sg;
+
+struct sg_lde {
+    uint64_t* d_lde = nullptr;
+    uint64_t lde_rows = 0, row_u64 = 0;
+    uint8_t* d_nodes = nullptr;
+    uint64_t leaves_len = 0;
+    uint8_t root[32] = {0};
+};
+
+static Ctx* C(sg_ctx* c) { return reinterpret_cast<Ctx*>(c); }
+
+extern "C" {
+
+const char* sg_last_error(void) { return last_error(); }
+
+int sg_ctx_create(int device, uint64_t budget, sg_ctx** out) {
+    SG_CHECK_ARG(out, "null output");
+    *out = nullptr;
+    int count = 0;
+    SG_CUDA(cudaGetDeviceCount(&count));
+    SG_CHECK_ARG(device >= 0 && device < count, "device index out of range");
+    SG_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    SG_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10) {
+        set_error("this library is built for sm_100a (B200); found sm_" + std::to_string(prop.major) +
+                  std::to_string(prop.minor));
+        return SG_ERR_UNSUPPORTED;
+    }
+    Ctx* ctx = new Ctx();
+    ctx->device = device;
+    size_t free_b = 0, total_b = 0;
+    SG_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    ctx->budget = budget ? budget : (uint64_t)(0.9 * (double)free_b);
+    // Keep freed blocks in the stream-ordered pool instead of returning them to
+    // the driver each time: repeated commits then allocate without syscalls.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t thr = ctx->budget;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    *out = reinterpret_cast<sg_ctx*>(ctx);
+    return SG_OK;
+}
+
+void sg_ctx_destroy(sg_ctx* c) {
+    Ctx* ctx = C(c);
+    if (!ctx) return;
+    cudaDeviceSynchronize();
+    for (auto& kv : ctx->roots) cudaFree(kv.second);
+    delete ctx;
+}
+
+int sg_ctx_memory(sg_ctx* c, uint64_t* in_use, uint64_t* peak) {
+    SG_CHECK_ARG(c, "null context");
+    if (in_use) *in_use = C(c)->in_use.load();
+    if (peak) *peak = C(c)->peak.load();
+    return SG_OK;
+}
+
+uint64_t sg_ctx_launches(sg_ctx* c) { return c ? C(c)->launches.load() : 0; }
+
+int sg_ctx_fail_alloc_after(sg_ctx* c, int64_t n) {
+    SG_CHECK_ARG(c && n >= 0, "bad argument");
+    C(c)->fail_alloc_after.store(n == 0 ? -1 : n);
+    return SG_OK;
+}
+
+int sg_dev_alloc(sg_ctx* c, void* stream, uint64_t bytes, void** d_out) {
+    SG_CHECK_ARG(c && d_out, "null argument");
+    return dev_alloc(C(c), (cudaStream_t)stream, bytes, d_out);
+}
+
+int sg_dev_free(sg_ctx* c, void* stream, void* p, uint64_t bytes) {
+    SG_CHECK_ARG(c, "null context");
+    return dev_free(C(c), (cudaStream_t)stream, p, bytes);
+}
+
+int sg_memcpy_h2d(sg_ctx* c, void* stream, void* dst, const void* src, uint64_t bytes) {
+    SG_CHECK_ARG(c, "null context");
+    if (!bytes) return SG_OK;
+    SG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, (cudaStream_t)stream));
+    return SG_OK;
+}
+
+int sg_memcpy_d2h(sg_ctx* c, void* stream, void* dst, const void* src, uint64_t bytes) {
+    SG_CHECK_ARG(c, "null context");
+    if (!bytes) return SG_OK;
+    SG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    return SG_OK;
+}
+
+int sg_stream_sync(sg_ctx* c, void* stream) {
+    SG_CHECK_ARG(c, "null context");
+    SG_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    return SG_OK;
+}
+
+int sg_host_alloc(uint64_t bytes, void** out) {
+    SG_CHECK_ARG(out, "null output");
+    SG_CUDA(cudaMallocHost(out, bytes ? bytes : 1));
+    return SG_OK;
+}
+
+int sg_host_free(void* p) {
+    if (p) SG_CUDA(cudaFreeHost(p));
+    return SG_OK;
+}
+
+int sg_ntt_forward(sg_ctx* c, void* stream, uint64_t* d, uint64_t n, uint64_t m) {
+    SG_CHECK_ARG(c, "null context");
+    return ntt_rows(C(c), (cudaStream_t)stream, d, n, m, 0, 0);
+}
+
+int sg_ntt_inverse(sg_ctx* c, void* stream, uint64_t* d, uint64_t n, uint64_t m) {
+    SG_CHECK_ARG(c, "null context");
+    return ntt_rows(C(c), (cudaStream_t)stream, d, n, m, 1, 1);
+}
+
+int sg_coset_lde(sg_ctx* c, void* stream, const uint64_t* d_trace, uint64_t n, uint64_t m, uint32_t blowup,
+                 const uint64_t* d_weights, uint64_t* d_out) {
+    SG_CHECK_ARG(c, "null context");
+    SG_CHECK_ARG(blowup >= 1, "blowup must be >= 1");
+    if (n == 0 || m == 0) return SG_OK;
+    SG_CHECK_ARG(d_trace && d_weights && d_out, "null buffer");
+    return coset_lde(C(c), (cudaStream_t)stream, d_trace, n, m, blowup, d_weights, d_out);
+}
+
+static int resolve_layout(const sg_leaf_layout* lay, uint64_t row_u64, uint32_t* R, int* le, uint64_t* c0,
+                          uint64_t* c1) {
+    sg_leaf_layout d = {2, 0, 0, 0};
+    if (!lay) lay = &d;
+    *R = lay->rows_per_leaf;
+    *le = lay->little_endian ? 1 : 0;
+    *c0 = lay->col_start;
+    *c1 = lay->col_end ? lay->col_end : row_u64;
+    SG_CHECK_ARG(*R >= 1, "rows_per_leaf must be >= 1");
+    SG_CHECK_ARG(*c0 < *c1 && *c1 <= row_u64, "leaf column range");
+    return SG_OK;
+}
+
+int sg_keccak_leaves(sg_ctx* c, void* stream, const uint64_t* d_data, uint64_t num_rows, uint64_t row_u64,
+                     const sg_leaf_layout* layout, uint8_t* d_out) {
+    SG_CHECK_ARG(c, "null context");
+    if (num_rows == 0) return SG_OK;
+    uint32_t R;
+    int le;
+    uint64_t c0, c1;
+    SG_TRY(resolve_layout(layout, row_u64, &R, &le, &c0, &c1));
+    return leaves_row_major(C(c), (cudaStream_t)stream, d_data, num_rows, row_u64, c0, c1, R, le, d_out);
+}
+
+uint64_t sg_merkle_leaves_len(uint64_t num_leaves) {
+    uint64_t L = 1;
+    while (L < num_leaves) L <<= 1;
+    return num_leaves ? L : 0;
+}
+
+int sg_merkle_build(sg_ctx* c, void* stream, const uint8_t* d_leaves, uint64_t num_leaves, uint8_t* d_nodes,
+                    uint8_t root_out[32]) {
+    SG_CHECK_ARG(c, "null context");
+    SG_CHECK_ARG(num_leaves > 0, "empty leaf set");
+    cudaStream_t st = (cudaStream_t)stream;
+    const uint64_t L = sg_merkle_leaves_len(num_leaves);
+    uint8_t* leaf_dst = d_nodes + (L - 1) * 32;
+    if (leaf_dst != d_leaves) SG_CUDA(cudaMemcpyAsync(leaf_dst, d_leaves, num_leaves * 32, cudaMemcpyDeviceToDevice, st));
+    SG_TRY(pad_leaves(C(c), st, leaf_dst, num_leaves, L));
+    SG_TRY(merkle_inner(C(c), st, d_nodes, L));
+    if (root_out) {
+        SG_CUDA(cudaMemcpyAsync(root_out, d_nodes, 32, cudaMemcpyDeviceToHost, st));
+        SG_CUDA(cudaStreamSynchronize(st));
+    }
+    return SG_OK;
+}
+
+int sg_lde_commit(sg_ctx* c, void* stream, const uint64_t* trace, int trace_on_device, uint64_t n, uint64_t row_u64,
+                  uint32_t blowup, const uint64_t* weights, const sg_leaf_layout* layout, uint64_t* host_lde_out,
+                  sg_lde** out, uint8_t root_out[32]) {
+    SG_CHECK_ARG(c && out && trace && weights, "null argument");
+    *out = nullptr;
+    Ctx* ctx = C(c);
+    cudaStream_t st = (cudaStream_t)stream;
+    SG_CHECK_ARG(n >= 2 && log2_exact(n) >= 0, "n must be a power of two >= 2");
+    SG_CHECK_ARG(blowup >= 1 && log2_exact(blowup) >= 0, "blowup must be a power of two");
+    SG_CHECK_ARG(row_u64 >= 1, "row width must be >= 1");
+    uint32_t R;
+    int le;
+    uint64_t c0, c1;
+    SG_TRY(resolve_layout(layout, row_u64, &R, &le, &c0, &c1));
+    const uint64_t lde_rows = n * blowup;
+    SG_CHECK_ARG(lde_rows % R == 0, "rows_per_leaf must divide the LDE size");
+    const uint64_t num_leaves = lde_rows / R;
+    const uint64_t L = num_leaves;  // power of two
+    sg_lde* h = new sg_lde();
+    h->lde_rows = lde_rows;
+    h->row_u64 = row_u64;
+    h->leaves_len = L;
+    uint64_t* d_trace = nullptr;
+    uint64_t* d_w = nullptr;
+    const uint64_t trace_bytes = n * row_u64 * 8;
+    int rc = SG_OK;
+    do {
+        rc = dev_alloc(ctx, st, lde_rows * row_u64 * 8, (void**)&h->d_lde);
+        if (rc) break;
+        rc = dev_alloc(ctx, st, (2 * L - 1) * 32, (void**)&h->d_nodes);
+        if (rc) break;
+        rc = dev_alloc(ctx, st, n * 8, (void**)&d_w);
+        if (rc) break;
+        if (cudaMemcpyAsync(d_w, weights, n * 8, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+            set_error("weights upload failed");
+            rc = SG_ERR_CUDA;
+            break;
+        }
+        const uint64_t* src = trace;
+        if (!trace_on_device) {
+            rc = dev_alloc(ctx, st, trace_bytes, (void**)&d_trace);
+            if (rc) break;
+            if (cudaMemcpyAsync(d_trace, trace, trace_bytes, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+                set_error("trace upload failed");
+                rc = SG_ERR_CUDA;
+                break;
+            }
+            src = d_trace;
+        }
+        rc = coset_lde(ctx, st, src, n, row_u64, blowup, d_w, h->d_lde);
+        if (rc) break;
+        rc = leaves_row_major(ctx, st, h->d_lde, lde_rows, row_u64, c0, c1, R, le, h->d_nodes + (L - 1) * 32);
+        if (rc) break;
+        rc = merkle_inner(ctx, st, h->d_nodes, L);
+        if (rc) break;
+        if (cudaMemcpyAsync(h->root, h->d_nodes, 32, cudaMemcpyDeviceToHost, st) != cudaSuccess) {
+            set_error("root download failed");
+            rc = SG_ERR_CUDA;
+            break;
+        }
+        if (host_lde_out &&
+            cudaMemcpyAsync(host_lde_out, h->d_lde, lde_rows * row_u64 * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess) {
+            set_error("LDE download failed");
+            rc = SG_ERR_CUDA;
+            break;
+        }
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            set_error(std::string("lde commit: ") + cudaGetErrorString(e));
+            rc = SG_ERR_CUDA;
+            break;
+        }
+    } while (0);
+    if (d_trace) dev_free(ctx, st, d_trace, trace_bytes);
+    if (d_w) dev_free(ctx, st, d_w, n * 8);
+    if (rc != SG_OK) {
+        if (h->d_lde) dev_free(ctx, st, h->d_lde, lde_rows * row_u64 * 8);
+        if (h->d_nodes) dev_free(ctx, st, h->d_nodes, (2 * L - 1) * 32);
+        delete h;
+        return rc;
+    }
+    if (root_out) memcpy(root_out, h->root, 32);
+    *out = h;
+    return SG_OK;
+}
+
+int sg_lde_get_info(const sg_lde* h, sg_lde_info* info) {
+    SG_CHECK_ARG(h && info, "null argument");
+    info->d_lde = h->d_lde;
+    info->lde_rows = h->lde_rows;
+    info->row_u64 = h->row_u64;
+    info->d_nodes = h->d_nodes;
+    info->leaves_len = h->leaves_len;
+    memcpy(info->root, h->root, 32);
+    return SG_OK;
+}
+
+void sg_lde_free(sg_ctx* c, sg_lde* h) {
+    if (!c || !h) return;
+    Ctx* ctx = C(c);
+    // Freed on the legacy stream: ordered after all prior work that used the handle.
+    cudaDeviceSynchronize();
+    dev_free(ctx, nullptr, h->d_lde, h->lde_rows * h->row_u64 * 8);
+    dev_free(ctx, nullptr, h->d_nodes, (2 * h->leaves_len - 1) * 32);
+    delete h;
+}
+
+}  // extern "C"

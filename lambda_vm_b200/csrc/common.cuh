@@ -1,0 +1,94 @@
+// Internal runtime shared by the C-ABI entry points: error reporting, the
+// per-GPU context (stream-ordered allocator under an HBM budget, cached
+// twiddle tables) and launch helpers. Nothing here is exported.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <atomic>
+#include <map>
+#include <mutex>
+#include <string>
+
+#include "../../include/starkgpu.h"
+
+namespace sg {
+
+void set_error(const std::string& msg);
+const char* last_error();
+
+#define SG_CHECK_ARG(cond, msg)                               \
+    do {                                                      \
+        if (!(cond)) {                                        \
+            ::sg::set_error(std::string("invalid argument: ") + (msg)); \
+            return SG_ERR_INVALID;                            \
+        }                                                     \
+    } while (0)
+
+#define SG_CUDA(call)                                                                   \
+    do {                                                                                \
+        cudaError_t _e = (call);                                                        \
+        if (_e != cudaSuccess) {                                                        \
+            ::sg::set_error(std::string(#call) + ": " + cudaGetErrorString(_e));         \
+            return _e == cudaErrorMemoryAllocation ? SG_ERR_OOM : SG_ERR_CUDA;          \
+        }                                                                               \
+    } while (0)
+
+#define SG_TRY(call)               \
+    do {                           \
+        int _rc = (call);          \
+        if (_rc != SG_OK) return _rc; \
+    } while (0)
+
+struct Ctx {
+    int device = 0;
+    uint64_t budget = 0;              // bytes this context may hold on the device
+    std::atomic<uint64_t> in_use{0};  // bytes currently allocated through this context
+    std::atomic<uint64_t> peak{0};
+    std::atomic<uint64_t> launches{0};  // kernels launched through this context
+    std::mutex mu;
+    // W_N[e] = omega_N^e for N = 2^log, keyed by log. Device-resident, built once.
+    std::map<uint32_t, uint64_t*> roots;
+    // Fault injection for host-side failure tests: when > 0, the next
+    // allocation that would bring the count to zero fails with SG_ERR_OOM.
+    std::atomic<int64_t> fail_alloc_after{-1};
+};
+
+// Stream-ordered allocation charged against the context budget.
+int dev_alloc(Ctx* ctx, cudaStream_t st, uint64_t bytes, void** out);
+int dev_free(Ctx* ctx, cudaStream_t st, void* p, uint64_t bytes);
+
+// Table of omega_{2^log}^e, e in [0, 2^log), cached per context.
+int roots_table(Ctx* ctx, cudaStream_t st, uint32_t log, const uint64_t** out);
+
+inline int log2_exact(uint64_t n) {
+    if (n == 0 || (n & (n - 1))) return -1;
+    int l = 0;
+    while ((1ULL << l) < n) ++l;
+    return l;
+}
+
+inline int check_launch(Ctx* ctx, const char* what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error(std::string(what) + ": " + cudaGetErrorString(e));
+        return SG_ERR_CUDA;
+    }
+    ctx->launches.fetch_add(1, std::memory_order_relaxed);
+    return SG_OK;
+}
+
+// ---- internal kernel drivers (ntt.cu, merkle.cu) ----
+enum Dir { FWD = 0, INV = 1 };
+// Batched natural-order DFT over the rows of a row-major n x m matrix.
+int ntt_rows(Ctx* ctx, cudaStream_t st, uint64_t* d, uint64_t n, uint64_t m, int inverse, int scale_inverse);
+// Coset LDE: out ((B*n) x m, row-major, canonical) from trace (n x m) and coset weights.
+int coset_lde(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t n, uint64_t m, uint64_t blowup,
+              const uint64_t* weights, uint64_t* out);
+int leaves_row_major(Ctx* ctx, cudaStream_t st, const uint64_t* data, uint64_t num_rows, uint64_t row_u64,
+                     uint64_t col_start, uint64_t col_end, uint32_t rows_per_leaf, int little_endian,
+                     uint8_t* out);
+int merkle_inner(Ctx* ctx, cudaStream_t st, uint8_t* nodes, uint64_t num_leaves_pow2);
+int pad_leaves(Ctx* ctx, cudaStream_t st, uint8_t* leaves, uint64_t n, uint64_t L);
+
+}  // namespace sg

@@ -1,0 +1,230 @@
+// Goldilocks (p = 2^64 - 2^32 + 1) and its cubic extension Fp3 = Fp[w]/(w^3 - 2)
+// for sm_100a. Same field semantics as crypto/math/src/field/goldilocks.rs:72-216
+// and extensions_goldilocks.rs:280-420: values live in [0, 2^64), reduced mod p
+// but not necessarily canonical; gl_canon() maps to [0, p) at the boundaries
+// (hashing, host output). All arithmetic is exact 64-bit modular integer math
+// written as explicit 32-bit carry chains so the INT pipes see the minimum.
+#pragma once
+#include <stdint.h>
+
+#define GL_P 0xFFFFFFFF00000001ULL
+#define GL_EPS 0xFFFFFFFFULL
+
+namespace gl {
+
+__device__ __forceinline__ uint32_t lo32(uint64_t x) { return (uint32_t)x; }
+__device__ __forceinline__ uint32_t hi32(uint64_t x) { return (uint32_t)(x >> 32); }
+__device__ __forceinline__ uint64_t pack(uint32_t lo, uint32_t hi) {
+    return ((uint64_t)hi << 32) | lo;
+}
+
+__device__ __forceinline__ uint64_t canon(uint64_t a) { return a >= GL_P ? a - GL_P : a; }
+
+// a + b mod p. One conditional EPS fold per carry; the second carry can only
+// occur when both inputs are >= p.
+__device__ __forceinline__ uint64_t add(uint64_t a, uint64_t b) {
+    uint32_t r0, r1, c;
+    asm("add.cc.u32 %0, %3, %5;\n\t"
+        "addc.cc.u32 %1, %4, %6;\n\t"
+        "addc.u32 %2, 0, 0;"
+        : "=r"(r0), "=r"(r1), "=r"(c)
+        : "r"(lo32(a)), "r"(hi32(a)), "r"(lo32(b)), "r"(hi32(b)));
+    uint32_t fix = 0u - c;  // 0 or 0xFFFFFFFF == EPS
+    uint32_t c2;
+    asm("add.cc.u32 %0, %0, %3;\n\t"
+        "addc.cc.u32 %1, %1, 0;\n\t"
+        "addc.u32 %2, 0, 0;"
+        : "+r"(r0), "+r"(r1), "=r"(c2)
+        : "r"(fix));
+    uint64_t r = pack(r0, r1);
+    if (c2) r += GL_EPS;  // r < EPS after a second wrap, so this cannot carry
+    return r;
+}
+
+// a - b mod p.
+__device__ __forceinline__ uint64_t sub(uint64_t a, uint64_t b) {
+    uint32_t r0, r1, br;
+    asm("sub.cc.u32 %0, %3, %5;\n\t"
+        "subc.cc.u32 %1, %4, %6;\n\t"
+        "subc.u32 %2, 0, 0;"
+        : "=r"(r0), "=r"(r1), "=r"(br)
+        : "r"(lo32(a)), "r"(hi32(a)), "r"(lo32(b)), "r"(hi32(b)));
+    uint32_t br2;
+    asm("sub.cc.u32 %0, %0, %3;\n\t"
+        "subc.cc.u32 %1, %1, 0;\n\t"
+        "subc.u32 %2, 0, 0;"
+        : "+r"(r0), "+r"(r1), "=r"(br2)
+        : "r"(br));  // br is 0 or 0xFFFFFFFF == EPS
+    uint64_t r = pack(r0, r1);
+    if (br2) r -= GL_EPS;  // r >= 2^64 - EPS after a second wrap, so this cannot borrow
+    return r;
+}
+
+// Reduce the 128-bit value (x3:x2:x1:x0) mod p using 2^64 = EPS, 2^96 = -1.
+__device__ __forceinline__ uint64_t reduce128(uint32_t x0, uint32_t x1, uint32_t x2, uint32_t x3) {
+    // t0 = lo - hi_hi, folding a borrow as -EPS (cannot borrow twice).
+    uint32_t t0, t1, b;
+    asm("sub.cc.u32 %0, %3, %5;\n\t"
+        "subc.cc.u32 %1, %4, 0;\n\t"
+        "subc.u32 %2, 0, 0;"
+        : "=r"(t0), "=r"(t1), "=r"(b)
+        : "r"(x0), "r"(x1), "r"(x3));
+    asm("sub.cc.u32 %0, %0, %2;\n\t"
+        "subc.u32 %1, %1, 0;"
+        : "+r"(t0), "+r"(t1)
+        : "r"(b));
+    // u = hi_lo * EPS = (x2 << 32) - x2
+    uint32_t u0, u1;
+    asm("sub.cc.u32 %0, 0, %2;\n\t"
+        "subc.u32 %1, %2, 0;"
+        : "=r"(u0), "=r"(u1)
+        : "r"(x2));
+    // r = t + u, carry folds +EPS (cannot carry twice).
+    uint32_t c;
+    asm("add.cc.u32 %0, %0, %3;\n\t"
+        "addc.cc.u32 %1, %1, %4;\n\t"
+        "addc.u32 %2, 0, 0;"
+        : "+r"(t0), "+r"(t1), "=r"(c)
+        : "r"(u0), "r"(u1));
+    asm("add.cc.u32 %0, %0, %2;\n\t"
+        "addc.u32 %1, %1, 0;"
+        : "+r"(t0), "+r"(t1)
+        : "r"(0u - c));
+    return pack(t0, t1);
+}
+
+// Full 64x64 -> 128 product as four 32-bit limbs.
+__device__ __forceinline__ void mul128(uint64_t a, uint64_t b, uint32_t& r0, uint32_t& r1, uint32_t& r2,
+                                       uint32_t& r3) {
+    uint32_t a0 = lo32(a), a1 = hi32(a), b0 = lo32(b), b1 = hi32(b);
+    asm("mul.lo.u32 %0, %4, %6;\n\t"
+        "mul.hi.u32 %1, %4, %6;\n\t"
+        "mad.lo.cc.u32 %1, %4, %7, %1;\n\t"
+        "madc.hi.u32 %2, %4, %7, 0;\n\t"
+        "mad.lo.cc.u32 %1, %5, %6, %1;\n\t"
+        "madc.hi.cc.u32 %2, %5, %6, %2;\n\t"
+        "madc.hi.u32 %3, %5, %7, 0;\n\t"
+        "mad.lo.cc.u32 %2, %5, %7, %2;\n\t"
+        "addc.u32 %3, %3, 0;"
+        : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+        : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ uint64_t mul(uint64_t a, uint64_t b) {
+    uint32_t r0, r1, r2, r3;
+    mul128(a, b, r0, r1, r2, r3);
+    return reduce128(r0, r1, r2, r3);
+}
+
+__device__ __forceinline__ uint64_t sqr(uint64_t a) { return mul(a, a); }
+
+__device__ __forceinline__ uint64_t neg(uint64_t a) {
+    uint64_t c = canon(a);
+    return c == 0 ? 0 : GL_P - c;
+}
+
+__device__ __forceinline__ uint64_t pow(uint64_t a, uint64_t e) {
+    uint64_t r = 1;
+    while (e) {
+        if (e & 1) r = mul(r, a);
+        a = mul(a, a);
+        e >>= 1;
+    }
+    return r;
+}
+
+__device__ __forceinline__ uint64_t inv(uint64_t a) { return pow(a, GL_P - 2); }
+
+// ---------------------------------------------------------------- Fp3
+struct fe3 {
+    uint64_t c0, c1, c2;
+};
+
+__device__ __forceinline__ fe3 f3(uint64_t a, uint64_t b, uint64_t c) { return fe3{a, b, c}; }
+__device__ __forceinline__ fe3 add3(fe3 a, fe3 b) { return fe3{add(a.c0, b.c0), add(a.c1, b.c1), add(a.c2, b.c2)}; }
+__device__ __forceinline__ fe3 sub3(fe3 a, fe3 b) { return fe3{sub(a.c0, b.c0), sub(a.c1, b.c1), sub(a.c2, b.c2)}; }
+__device__ __forceinline__ fe3 mulb3(fe3 a, uint64_t s) { return fe3{mul(a.c0, s), mul(a.c1, s), mul(a.c2, s)}; }
+
+// Accumulate three 128-bit products and reduce once: sum overflow past 2^128
+// folds 2^128 = EPS^2 mod p (same identity as goldilocks.rs dot_product_3).
+__device__ __forceinline__ uint64_t dot3(uint64_t a0, uint64_t b0, uint64_t a1, uint64_t b1, uint64_t a2,
+                                         uint64_t b2) {
+    uint32_t s0, s1, s2, s3, t0, t1, t2, t3, ov;
+    mul128(a0, b0, s0, s1, s2, s3);
+    mul128(a1, b1, t0, t1, t2, t3);
+    asm("add.cc.u32 %0, %0, %5;\n\t"
+        "addc.cc.u32 %1, %1, %6;\n\t"
+        "addc.cc.u32 %2, %2, %7;\n\t"
+        "addc.cc.u32 %3, %3, %8;\n\t"
+        "addc.u32 %4, 0, 0;"
+        : "+r"(s0), "+r"(s1), "+r"(s2), "+r"(s3), "=r"(ov)
+        : "r"(t0), "r"(t1), "r"(t2), "r"(t3));
+    mul128(a2, b2, t0, t1, t2, t3);
+    asm("add.cc.u32 %0, %0, %5;\n\t"
+        "addc.cc.u32 %1, %1, %6;\n\t"
+        "addc.cc.u32 %2, %2, %7;\n\t"
+        "addc.cc.u32 %3, %3, %8;\n\t"
+        "addc.u32 %4, %4, 0;"
+        : "+r"(s0), "+r"(s1), "+r"(s2), "+r"(s3), "+r"(ov)
+        : "r"(t0), "r"(t1), "r"(t2), "r"(t3));
+    uint64_t r = reduce128(s0, s1, s2, s3);
+    // EPS^2 = 2^64 - 2^33 + 1 < p; add it `ov` (0..2) times.
+    const uint64_t EPS2 = 0xFFFFFFFE00000001ULL;
+    if (ov) {
+        r = add(r, EPS2);
+        if (ov > 1) r = add(r, EPS2);
+    }
+    return r;
+}
+
+__device__ __forceinline__ fe3 mul3(fe3 a, fe3 b) {
+    uint64_t b1_2 = add(b.c1, b.c1), b2_2 = add(b.c2, b.c2);
+    return fe3{dot3(a.c0, b.c0, a.c1, b2_2, a.c2, b1_2), dot3(a.c0, b.c1, a.c1, b.c0, a.c2, b2_2),
+               dot3(a.c0, b.c2, a.c1, b.c1, a.c2, b.c0)};
+}
+
+// Norm-based inverse (extensions_goldilocks.rs:359-390). Returns 0 for 0.
+__device__ __forceinline__ fe3 inv3(fe3 a) {
+    uint64_t a0s = sqr(a.c0), a1s = sqr(a.c1), a2s = sqr(a.c2);
+    uint64_t a0c = mul(a0s, a.c0), a1c = mul(a1s, a.c1), a2c = mul(a2s, a.c2);
+    uint64_t a012 = mul(mul(a.c0, a.c1), a.c2);
+    uint64_t a1c2 = add(a1c, a1c);
+    uint64_t a2c4 = add(a2c, a2c);
+    a2c4 = add(a2c4, a2c4);
+    uint64_t six = add(add(a012, a012), a012);
+    six = add(six, six);
+    uint64_t norm = sub(add(add(a0c, a1c2), a2c4), six);
+    uint64_t ni = inv(canon(norm));
+    uint64_t a1a2 = mul(a.c1, a.c2), a0a1 = mul(a.c0, a.c1), a0a2 = mul(a.c0, a.c2);
+    return fe3{mul(sub(a0s, add(a1a2, a1a2)), ni), mul(sub(add(a2s, a2s), a0a1), ni), mul(sub(a1s, a0a2), ni)};
+}
+
+__device__ __forceinline__ fe3 canon3(fe3 a) { return fe3{canon(a.c0), canon(a.c1), canon(a.c2)}; }
+
+}  // namespace gl
+
+// ---------------------------------------------------------------- host-side constexpr field math
+// Used to bake roots of unity into kernels as compile-time constants.
+namespace glc {
+constexpr uint64_t P = GL_P;
+constexpr uint64_t mul(uint64_t a, uint64_t b) {
+    return (uint64_t)(((unsigned __int128)a * b) % P);
+}
+constexpr uint64_t pow(uint64_t a, uint64_t e) {
+    uint64_t r = 1;
+    while (e) {
+        if (e & 1) r = mul(r, a);
+        a = mul(a, a);
+        e >>= 1;
+    }
+    return r;
+}
+// Primitive 2^k-th root of unity, derived from the two-adic generator
+// 1753635133440165772 exactly as traits.rs:83-95 does (repeated squaring).
+constexpr uint64_t root(uint32_t log_n) {
+    uint64_t r = 1753635133440165772ULL;
+    for (uint32_t i = 0; i < 32 - log_n; i++) r = mul(r, r);
+    return log_n == 0 ? 1 : r;
+}
+constexpr uint64_t inv(uint64_t a) { return pow(a, P - 2); }
+}  // namespace glc
