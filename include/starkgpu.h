@@ -100,6 +100,22 @@ SG_API int sg_ntt_inverse(sg_ctx* ctx, void* stream, uint64_t* d_data, uint64_t 
 SG_API int sg_coset_lde(sg_ctx* ctx, void* stream, const uint64_t* d_trace, uint64_t n, uint64_t m, uint32_t blowup,
                  const uint64_t* d_weights, uint64_t* d_out);
 
+/* ---- allocation-free coset LDE. No counterpart in the reference: an extra
+ *      entry point for callers that cannot allocate device memory at call time
+ *      (a serving process that reserves all of its HBM at start-up and must not
+ *      grow it mid-request, or an FFI host that wants no hidden allocation and
+ *      no context object). Same arguments and result as sg_coset_lde, but no
+ *      context and no allocation: its scratch is a static device array of
+ *      SG_STATIC_SCRATCH_BYTES per GPU, held until the process exits. Requires
+ *      (blowup*n + 2*n*m) * 8 <= SG_STATIC_SCRATCH_BYTES, else SG_ERR_INVALID.
+ *      The first call on a device (with that device current) looks up the
+ *      array's device address; make it before any stream capture. Calls share
+ *      the array, so calls that overlap on the GPU race and must be serialized
+ *      by the caller. ---- */
+#define SG_STATIC_SCRATCH_BYTES (32ull << 20)
+SG_API int sg_coset_lde_static(void* stream, const uint64_t* d_trace, uint64_t n, uint64_t m, uint32_t blowup,
+                               const uint64_t* d_weights, uint64_t* d_out);
+
 /* ---- leaves: replaces merkle::keccak_leaves_base / keccak_leaves_ext3
  *      (crypto/math-cuda/src/merkle.rs:33,83) over a row-major matrix
  *      (num_rows x row_u64). d_leaves_out: num_rows/rows_per_leaf x 32 bytes,

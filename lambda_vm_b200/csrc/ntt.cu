@@ -447,3 +447,136 @@ int roots_table(Ctx* ctx, cudaStream_t st, uint32_t log, const uint64_t** out) {
 }
 
 }  // namespace sg
+
+// ---------------------------------------------------------------- allocation-free coset LDE
+//
+// sg_coset_lde_static computes exactly what sg_coset_lde computes, for callers
+// that cannot allocate device memory at call time: a serving process that
+// reserves its whole HBM allowance when it starts and treats any later
+// cudaMalloc as a failure (under co-tenant memory pressure such a call can
+// fail, and cudaMalloc/cudaFree can synchronize the device and stall the other
+// proofs in flight), or a foreign-language host that wants one call with no
+// hidden allocation and no context object to manage.
+//
+// Its scratch (the omega table, the coefficient matrix and the four-step
+// intermediate) lives in one file-scope device array of SG_STATIC_SCRATCH_BYTES
+// that every GPU which loads this library holds until the process exits. The
+// array's host-side name is only a stand-in for the symbol, so the first call
+// on each device, with that device current, looks up its device address with
+// cudaGetSymbolAddress and caches it; make that first call before any stream
+// capture. All calls share the array: two calls that overlap on the GPU (on
+// different streams, or from different threads) race on it and must be
+// serialized by the caller. Nothing needs clearing between calls, because each
+// call writes every scratch word before it reads it.
+namespace sg {
+
+static __device__ __align__(256) uint64_t g_lde_scratch[SG_STATIC_SCRATCH_BYTES / sizeof(uint64_t)];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mu;
+uint64_t* g_static_scratch[kMaxDevices] = {};
+Ctx g_static_ctx;  // launch accounting only; it never allocates
+
+int static_scratch(uint64_t** out) {
+    int dev = 0;
+    SG_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) {
+        set_error("device index out of range for the static scratch table");
+        return SG_ERR_UNSUPPORTED;
+    }
+    std::lock_guard<std::mutex> g(g_static_mu);
+    if (!g_static_scratch[dev]) {
+        void* p = nullptr;
+        SG_CUDA(cudaGetSymbolAddress(&p, g_lde_scratch));
+        g_static_scratch[dev] = (uint64_t*)p;
+    }
+    *out = g_static_scratch[dev];
+    return SG_OK;
+}
+}  // namespace
+
+}  // namespace sg
+
+extern "C" int sg_coset_lde_static(void* stream, const uint64_t* d_trace, uint64_t n, uint64_t m, uint32_t blowup,
+                                   const uint64_t* d_weights, uint64_t* d_out) {
+    using namespace sg;
+    if (n == 0 || m == 0) return SG_OK;
+    SG_CHECK_ARG(d_trace && d_weights && d_out, "null buffer");
+    const int logn = log2_exact(n), logB = log2_exact(blowup);
+    SG_CHECK_ARG(logn >= 0, "n must be a power of two");
+    SG_CHECK_ARG(logB >= 0, "blowup must be a power of two");
+    const int logN = logn + logB;
+    SG_CHECK_ARG(logN <= 32 && logn <= 24, "LDE size out of range");
+    const uint64_t N = 1ULL << logN;
+    const uint64_t need = N + 2 * n * m;  // u64 words: omega table + coefficients + four-step intermediate
+    if (need > SG_STATIC_SCRATCH_BYTES / sizeof(uint64_t)) {
+        set_error("sg_coset_lde_static: needs " + std::to_string(need * 8) +
+                  " bytes of scratch ((blowup*n + 2*n*m) * 8) but the static scratch holds " +
+                  std::to_string((unsigned long long)SG_STATIC_SCRATCH_BYTES) + "; use sg_coset_lde");
+        return SG_ERR_INVALID;
+    }
+    uint64_t* scratch = nullptr;
+    SG_TRY(static_scratch(&scratch));
+    cudaStream_t st = (cudaStream_t)stream;
+    Ctx* ctx = &g_static_ctx;
+    uint64_t* W = scratch;
+    uint64_t* coef = scratch + N;
+    uint64_t* tmp = coef + n * m;
+    k_roots<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(W, N, glc::root((uint32_t)logN));
+    SG_TRY(check_launch(ctx, "k_roots"));
+    if (logn <= 12) {
+        PassArgs I = base_args(d_trace, coef, m, logn, true, W, logN);
+        I.in_ps = 1;
+        I.out_ps = 1;
+        I.post_kind = 2;
+        I.weights = d_weights;
+        SG_TRY(run_pass(ctx, st, I, 1));
+        PassArgs F = base_args(coef, d_out, m, logn, false, W, logN);
+        F.in_ps = 1;
+        F.reps = blowup;
+        F.pre_kind = 1;
+        F.pre_log = logN;
+        F.out_ps = blowup;
+        F.out_rs = 1;
+        F.canon_out = 1;
+        return run_pass(ctx, st, F, 1);
+    }
+    const uint32_t l1 = logn / 2, l2 = logn - l1;
+    const uint64_t N1 = 1ULL << l1, N2 = 1ULL << l2;
+    PassArgs I1 = base_args(d_trace, tmp, m, l1, true, W, logN);
+    I1.in_ts = 1;
+    I1.in_ps = N2;
+    I1.out_ts = 1;
+    I1.out_ps = N2;
+    I1.post_kind = 1;
+    I1.post_log = logn;
+    SG_TRY(run_pass(ctx, st, I1, N2));
+    PassArgs I2 = base_args(tmp, coef, m, l2, true, W, logN);
+    I2.in_ts = N2;
+    I2.in_ps = 1;
+    I2.out_ts = 1;
+    I2.out_ps = N1;
+    I2.post_kind = 2;
+    I2.weights = d_weights;
+    SG_TRY(run_pass(ctx, st, I2, N1));
+    PassArgs F1 = base_args(coef, d_out, m, l1, false, W, logN);
+    F1.in_ts = 1;
+    F1.in_ps = N2;
+    F1.reps = blowup;
+    F1.pre_kind = 1;
+    F1.pre_log = logN;
+    F1.post_kind = 1;
+    F1.post_log = logn;
+    F1.out_ts = (uint64_t)blowup * N1;
+    F1.out_ps = blowup;
+    F1.out_rs = 1;
+    SG_TRY(run_pass(ctx, st, F1, N2));
+    PassArgs F2 = base_args(d_out, d_out, m, l2, false, W, logN);
+    F2.in_ts = 1;
+    F2.in_ps = (uint64_t)blowup * N1;
+    F2.out_ts = 1;
+    F2.out_ps = (uint64_t)blowup * N1;
+    F2.canon_out = 1;
+    return run_pass(ctx, st, F2, N1 * blowup);
+}

@@ -54,7 +54,9 @@ PROTOTYPES = {
     "sg_lde_get_info": (i32, [vp, C.POINTER(LdeInfo)]),
     "sg_lde_free": (None, [vp, vp]),
     "sg_grind": (i32, [vp, vp, vp, C.c_uint8, C.POINTER(u64)]),
+    "sg_coset_lde_static": (i32, [vp, vp, u64, u64, u32, vp, vp]),
 }
+SG_STATIC_SCRATCH_BYTES = 32 << 20
 
 _lib = None
 
