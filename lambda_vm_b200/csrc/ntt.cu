@@ -5,14 +5,20 @@
 // natural-order output) and crypto/math-cuda/src/ntt.rs:57-66 (natural-order
 // forward / inverse NTT, the inverse scaled by 1/n).
 //
-// Design. Every pass is one kernel, `k_dft_pass`: a CTA owns a tile of L points
-// (rows) x C columns, stages it in shared memory in bit-reversed point order
-// (coalesced C*8-byte row segments from HBM), runs an in-place radix-2^q DIT
-// whose 2^q-point butterfly networks live in registers (q <= 5, so at most
-// two shared-memory round trips for L = 1024), and writes the tile back.
-// Per-point factors (coset weights, four-step twiddles, coset shifts) depend
-// only on the row, so each is fetched once per tile into shared memory and
-// reused by all C columns.
+// Design. Every pass is one launch of `k_dft<LOGL>`, a persistent kernel whose
+// CTAs walk tiles of L = 2^LOGL points (rows) x C columns. The DFT of a tile is
+// an in-place radix-2^q decimation-in-time whose 2^q-point butterfly networks
+// live in registers (q <= 5); the stage plan is fixed at compile time per L:
+//   stage 1 gathers its 2^q1 inputs straight from HBM (bit-reversed point
+//           order is just an address permutation), with coalesced C*8-byte
+//           row segments, and leaves its outputs in shared memory;
+//   middle stages (L > 1024 only) run in place in shared memory;
+//   the last stage reads shared memory and writes its outputs straight to HBM.
+// So an L = 1024 tile costs one shared-memory round trip. Per-point factors
+// (coset weights, four-step twiddles, coset shifts) depend only on the row, so
+// each is computed once per tile and shared by its C columns; all roots of
+// unity come from two small tables (omega_N^e = lo[e mod 2^h] * hi[e >> h])
+// that stay in L1, instead of an N-entry table read with a large stride.
 //
 // Sizes above 4096 use the four-step split n = N1 * N2:
 //   step 1: for each j2, DFT_N1 over rows i*N2 + j2, times w_n^{j2 k1}, written in place;
@@ -64,10 +70,31 @@ __device__ __forceinline__ void dit_reg(uint64_t* v) {
 
 template <int Q>
 __device__ __forceinline__ uint32_t brev_q(uint32_t r) {
-    return __brev(r) >> (32 - Q);
+    if constexpr (Q == 0)
+        return 0;
+    else
+        return __brev(r) >> (32 - Q);
 }
 
-__device__ __forceinline__ uint32_t spad(uint32_t i) { return i + (i >> 5); }
+// omega_N^e = lo[e & (2^h - 1)] * hi[e >> h], N = 2^logN.
+struct Tw {
+    const uint64_t* lo;
+    const uint64_t* hi;
+    uint32_t h;
+    uint32_t logN;
+};
+
+__device__ __forceinline__ uint64_t tw_pow(const Tw& t, uint64_t e) {
+    return gl::mul(__ldg(t.lo + (e & ((1ULL << t.h) - 1))), __ldg(t.hi + (e >> t.h)));
+}
+
+// omega_{2^logM}^{+-x}
+__device__ __forceinline__ uint64_t tw_root(const Tw& t, uint32_t logM, uint64_t x, bool inv) {
+    const uint64_t mask = (1ULL << t.logN) - 1;
+    uint64_t e = (x << (t.logN - logM)) & mask;
+    if (inv) e = (mask + 1 - e) & mask;
+    return tw_pow(t, e);
+}
 
 struct PassArgs {
     const uint64_t* in;
@@ -79,8 +106,7 @@ struct PassArgs {
     uint64_t in_ts, in_ps;
     uint64_t out_ts, out_ps, out_rs;
     uint32_t reps;
-    const uint64_t* W;  // W[e] = omega_{2^logW}^e
-    uint32_t logW;
+    Tw tw;
     uint32_t pre_kind;   // 0: none, 1: omega_{2^pre_log}^{in_row * rep}
     uint32_t pre_log;
     uint32_t post_kind;  // 0: none, 1: omega_{2^post_log}^{+-(tile*k)}, 2: weights[out_row], 3: scalar
@@ -90,166 +116,249 @@ struct PassArgs {
     uint32_t canon_out;
 };
 
-// One in-place radix-2^Q DIT stage over all C columns of the tile.
-template <int Q>
-__device__ __forceinline__ void dit_stage(uint64_t* S, const uint64_t* WL, uint32_t logL, int C, uint32_t cs,
-                                          uint32_t logNs, bool inv) {
-    constexpr uint32_t R = 1u << Q;
-    const uint32_t L = 1u << logL;
-    const uint32_t per_col = L >> Q;
-    const uint32_t items = (uint32_t)C * per_col;
-    const uint32_t Ns = 1u << logNs;
-    for (uint32_t w = threadIdx.x; w < items; w += blockDim.x) {
-        const uint32_t c = w >> (logL - Q);
-        const uint32_t j = w & (per_col - 1);
+// Compile-time stage plan per tile length: radix exponents, columns per tile,
+// threads per CTA.
+template <int LOGL>
+struct Plan {
+    static constexpr int NST = LOGL == 0 ? 0 : (LOGL <= 5 ? 1 : (LOGL <= 10 ? 2 : 3));
+    static constexpr int Q1 = NST == 1 ? LOGL : (NST == 2 ? (LOGL + 1) / 2 : 4);
+    static constexpr int Q2 = NST == 2 ? LOGL / 2 : (NST == 3 ? 4 : 0);
+    static constexpr int Q3 = NST == 3 ? LOGL - 8 : 0;
+    static constexpr int C = LOGL <= 7 ? 32 : (LOGL <= 9 ? 16 : (LOGL <= 11 ? 8 : 4));
+    static constexpr int T = LOGL >= 11 ? 512 : 256;
+    static constexpr uint32_t L = 1u << LOGL;
+    static constexpr uint32_t CS0 = L + (NST > 1 ? (L >> Q1) : 0);
+    static constexpr uint32_t CP = C < 16 ? C : 16;
+    static constexpr uint32_t CSMOD = 16 / CP;  // column stride = CSMOD (mod 16): no bank conflicts
+    static constexpr uint32_t CS = CS0 + ((CSMOD + 16 - CS0 % 16) % 16);
+    static constexpr uint32_t S_WORDS = NST > 1 ? C * CS : 0;
+    static constexpr uint32_t WL_WORDS = NST > 1 ? L : 0;
+    static constexpr uint32_t F_WORDS = NST > 1 ? L : 2 * L;  // one buffer reused for pre and post
+    static constexpr size_t SMEM = (size_t)(S_WORDS + WL_WORDS + F_WORDS) * 8;
+};
+
+template <int LOGL>
+__device__ __forceinline__ uint32_t tpad(uint32_t p) {
+    using PL = Plan<LOGL>;
+    if constexpr (PL::NST > 1)
+        return p + (p >> PL::Q1);
+    else
+        return p;
+}
+
+__device__ __forceinline__ uint64_t finish(const PassArgs& a, uint64_t v, uint64_t f) {
+    if (a.post_kind == 1 || a.post_kind == 2)
+        v = gl::mul(v, f);
+    else if (a.post_kind == 3)
+        v = gl::mul(v, a.scalar);
+    return a.canon_out ? gl::canon(v) : v;
+}
+
+// Middle stage: in place in shared memory.
+template <int LOGL, int Q, int LOGNS, bool INV>
+__device__ __forceinline__ void mid_stage(uint64_t* S, const uint64_t* WL) {
+    using PL = Plan<LOGL>;
+    constexpr uint32_t R = 1u << Q, Ns = 1u << LOGNS, per_col = PL::L >> Q;
+    constexpr uint32_t items = PL::C * per_col;
+    for (uint32_t w = threadIdx.x; w < items; w += PL::T) {
+        const uint32_t c = w % PL::C, j = w / PL::C;
         const uint32_t k = j & (Ns - 1);
-        const uint32_t base = ((j >> logNs) << (logNs + Q)) + k;
-        uint64_t* col = S + (size_t)c * cs;
+        const uint32_t base = ((j >> LOGNS) << (LOGNS + Q)) + k;
+        uint64_t* col = S + c * PL::CS;
         uint64_t v[R];
 #pragma unroll
-        for (uint32_t r = 0; r < R; ++r) v[r] = col[spad(base + r * Ns)];
-        if (logNs > 0) {
-            // twiddle omega_{Ns R}^{k * brev(r)} = omega_L^{k * brev(r) * L / (Ns R)}
-            const uint32_t sh = logL - logNs - Q;
+        for (uint32_t r = 0; r < R; ++r) v[r] = col[tpad<LOGL>(base + r * Ns)];
+        constexpr uint32_t sh = LOGL - LOGNS - Q;
 #pragma unroll
-            for (uint32_t r = 1; r < R; ++r) v[r] = gl::mul(v[r], WL[(k * brev_q<Q>(r)) << sh]);
-        }
-        if (inv)
-            dit_reg<Q, true>(v);
-        else
-            dit_reg<Q, false>(v);
+        for (uint32_t r = 1; r < R; ++r) v[r] = gl::mul(v[r], WL[(k * brev_q<Q>(r)) << sh]);
+        dit_reg<Q, INV>(v);
 #pragma unroll
-        for (uint32_t r = 0; r < R; ++r) col[spad(base + r * Ns)] = v[r];
+        for (uint32_t r = 0; r < R; ++r) col[tpad<LOGL>(base + r * Ns)] = v[r];
     }
 }
 
-__device__ void tile_dft(uint64_t* S, const uint64_t* WL, uint32_t logL, int C, uint32_t cs, bool inv) {
-    const int nst = (int)(logL + 4) / 5;
-    uint32_t rem = logL, logNs = 0;
-    for (int s = 0; s < nst; ++s) {
-        const uint32_t q = (rem + (nst - s) - 1) / (nst - s);
-        switch (q) {
-            case 1: dit_stage<1>(S, WL, logL, C, cs, logNs, inv); break;
-            case 2: dit_stage<2>(S, WL, logL, C, cs, logNs, inv); break;
-            case 3: dit_stage<3>(S, WL, logL, C, cs, logNs, inv); break;
-            case 4: dit_stage<4>(S, WL, logL, C, cs, logNs, inv); break;
-            default: dit_stage<5>(S, WL, logL, C, cs, logNs, inv); break;
+template <int LOGL, bool INV>
+__device__ __forceinline__ void tile_body(const PassArgs& a, uint64_t* S, const uint64_t* WL, uint64_t* F,
+                                          uint64_t pt, uint64_t col0, uint32_t ncols, uint32_t rep) {
+    using PL = Plan<LOGL>;
+    constexpr uint32_t L = PL::L, C = PL::C, T = PL::T;
+    uint64_t* Fpre = F;
+    uint64_t* Fpost = PL::NST > 1 ? F : F + L;
+    // ---- pre factors
+    if (a.pre_kind == 1) {
+        const uint64_t pmask = (1ULL << a.pre_log) - 1;
+        for (uint32_t i = threadIdx.x; i < L; i += T) {
+            const uint64_t row = pt * a.in_ts + (uint64_t)i * a.in_ps;
+            Fpre[i] = tw_root(a.tw, a.pre_log, (row * rep) & pmask, false);
         }
-        rem -= q;
-        logNs += q;
-        __syncthreads();
     }
-}
-
-__device__ __forceinline__ uint64_t wlookup(const uint64_t* W, uint32_t logW, uint32_t logM, uint64_t e, bool inv) {
-    // omega_{2^logM}^{+-e}
-    const uint64_t mask = (1ULL << logW) - 1;
-    uint64_t idx = (e << (logW - logM)) & mask;
-    if (inv) idx = (mask + 1 - idx) & mask;
-    return W[idx];
-}
-
-template <int C>
-__global__ void __launch_bounds__(256) k_dft_pass(PassArgs a) {
-    extern __shared__ uint64_t sm[];
-    const uint32_t L = 1u << a.logL;
-    const uint32_t cs = L + (L >> 5) + 1;  // padded smem column stride (u64)
-    uint64_t* S = sm;
-    uint64_t* WL = S + (size_t)C * cs;
-    uint64_t* F = WL + L;
-    const uint64_t tile = blockIdx.x;
-    const uint64_t col0 = (uint64_t)blockIdx.y * C;
-    const uint32_t ncols = (uint32_t)min((uint64_t)C, a.m - col0);
-    const bool inv = a.inverse != 0;
-    const uint32_t T = blockDim.x;
-
-    for (uint32_t e = threadIdx.x; e < L; e += T) WL[e] = wlookup(a.W, a.logW, a.logL, e, inv);
-
-    for (uint32_t rep = 0; rep < a.reps; ++rep) {
-        if (a.pre_kind == 1) {
-            const uint64_t pmask = (1ULL << a.pre_log) - 1;
-            for (uint32_t i = threadIdx.x; i < L; i += T) {
-                const uint64_t row = tile * a.in_ts + (uint64_t)i * a.in_ps;
-                F[i] = wlookup(a.W, a.logW, a.pre_log, (row * rep) & pmask, false);
-            }
-        }
-        __syncthreads();
-        // load (coalesced along columns), bit-reverse the point index into smem
-        const uint32_t tot = L * C;
-        for (uint32_t e = threadIdx.x; e < tot; e += T) {
-            const uint32_t i = e / C, c = e % C;
-            uint64_t v = 0;
-            if (c < ncols) {
-                const uint64_t row = tile * a.in_ts + (uint64_t)i * a.in_ps;
-                v = a.in[row * a.m + col0 + c];
-                if (a.pre_kind == 1) v = gl::mul(v, F[i]);
-            }
-            const uint32_t p = a.logL ? (__brev(i) >> (32 - a.logL)) : 0;
-            S[(size_t)c * cs + spad(p)] = v;
-        }
-        __syncthreads();
-        tile_dft(S, WL, a.logL, C, cs, inv);
+    if constexpr (PL::NST <= 1) {
         if (a.post_kind == 1) {
             const uint64_t pmask = (1ULL << a.post_log) - 1;
             for (uint32_t k = threadIdx.x; k < L; k += T)
-                F[k] = wlookup(a.W, a.logW, a.post_log, (tile * k) & pmask, inv);
+                Fpost[k] = tw_root(a.tw, a.post_log, (pt * k) & pmask, INV);
         } else if (a.post_kind == 2) {
             for (uint32_t k = threadIdx.x; k < L; k += T)
-                F[k] = a.weights[tile * a.out_ts + (uint64_t)k * a.out_ps + (uint64_t)rep * a.out_rs];
+                Fpost[k] = a.weights[pt * a.out_ts + (uint64_t)k * a.out_ps + (uint64_t)rep * a.out_rs];
         }
-        __syncthreads();
-        for (uint32_t e = threadIdx.x; e < tot; e += T) {
-            const uint32_t k = e / C, c = e % C;
+    }
+    __syncthreads();
+    const uint64_t* in = a.in + (pt * a.in_ts) * a.m + col0;
+    uint64_t* out = a.out + (pt * a.out_ts + (uint64_t)rep * a.out_rs) * a.m + col0;
+    const uint64_t ip = a.in_ps * a.m, op = a.out_ps * a.m;
+    if constexpr (PL::NST == 0) {
+        for (uint32_t c = threadIdx.x; c < C; c += T) {
             if (c < ncols) {
-                uint64_t v = S[(size_t)c * cs + spad(k)];
-                if (a.post_kind == 1 || a.post_kind == 2)
-                    v = gl::mul(v, F[k]);
-                else if (a.post_kind == 3)
-                    v = gl::mul(v, a.scalar);
-                if (a.canon_out) v = gl::canon(v);
-                const uint64_t row = tile * a.out_ts + (uint64_t)k * a.out_ps + (uint64_t)rep * a.out_rs;
-                a.out[row * a.m + col0 + c] = v;
+                uint64_t v = in[c];
+                if (a.pre_kind == 1) v = gl::mul(v, Fpre[0]);
+                out[c] = finish(a, v, Fpost[0]);
             }
         }
+        return;
+    } else {
+        // ---- stage 1: HBM -> registers -> (smem | HBM)
+        constexpr int Q = PL::Q1;
+        constexpr uint32_t R = 1u << Q, per_col = L >> Q, items = C * per_col;
+        for (uint32_t w = threadIdx.x; w < items; w += T) {
+            const uint32_t c = w % C, j = w / C;
+            const uint32_t jb = brev_q<LOGL - Q>(j);
+            uint64_t v[R];
+            if (c < ncols) {
+                const uint64_t* src = in + (uint64_t)jb * ip + c;
+#pragma unroll
+                for (uint32_t r = 0; r < R; ++r) v[r] = __ldg(src + (uint64_t)(brev_q<Q>(r) * per_col) * ip);
+                if (a.pre_kind == 1) {
+#pragma unroll
+                    for (uint32_t r = 0; r < R; ++r) v[r] = gl::mul(v[r], Fpre[jb + brev_q<Q>(r) * per_col]);
+                }
+            } else {
+#pragma unroll
+                for (uint32_t r = 0; r < R; ++r) v[r] = 0;
+            }
+            dit_reg<Q, INV>(v);
+            if constexpr (PL::NST == 1) {
+                if (c < ncols) {
+#pragma unroll
+                    for (uint32_t q = 0; q < R; ++q) out[(uint64_t)q * op + c] = finish(a, v[q], Fpost[q]);
+                }
+            } else {
+                uint64_t* col = S + c * PL::CS;
+#pragma unroll
+                for (uint32_t q = 0; q < R; ++q) col[tpad<LOGL>(j * R + q)] = v[q];
+            }
+        }
+    }
+    if constexpr (PL::NST > 1) {
         __syncthreads();
+        // post factors reuse the pre-factor buffer (stage 1 has finished reading it)
+        if (a.post_kind == 1) {
+            const uint64_t pmask = (1ULL << a.post_log) - 1;
+            for (uint32_t k = threadIdx.x; k < L; k += T)
+                Fpost[k] = tw_root(a.tw, a.post_log, (pt * k) & pmask, INV);
+        } else if (a.post_kind == 2) {
+            for (uint32_t k = threadIdx.x; k < L; k += T)
+                Fpost[k] = a.weights[pt * a.out_ts + (uint64_t)k * a.out_ps + (uint64_t)rep * a.out_rs];
+        }
+        if constexpr (PL::NST == 3) {
+            mid_stage<LOGL, PL::Q2, PL::Q1, INV>(S, WL);
+        }
+        __syncthreads();
+        // ---- last stage: smem -> registers -> HBM
+        constexpr int Q = PL::NST == 2 ? PL::Q2 : PL::Q3;
+        constexpr int LOGNS = LOGL - Q;
+        constexpr uint32_t R = 1u << Q, Ns = 1u << LOGNS, items = C * Ns;
+        for (uint32_t w = threadIdx.x; w < items; w += T) {
+            const uint32_t c = w % C, k = w / C;
+            const uint64_t* col = S + c * PL::CS;
+            uint64_t v[R];
+#pragma unroll
+            for (uint32_t r = 0; r < R; ++r) v[r] = col[tpad<LOGL>(k + r * Ns)];
+#pragma unroll
+            for (uint32_t r = 1; r < R; ++r) v[r] = gl::mul(v[r], WL[k * brev_q<Q>(r)]);
+            dit_reg<Q, INV>(v);
+            if (c < ncols) {
+#pragma unroll
+                for (uint32_t q = 0; q < R; ++q)
+                    out[(uint64_t)(k + q * Ns) * op + c] = finish(a, v[q], Fpost[k + q * Ns]);
+            }
+        }
     }
 }
 
-static int cols_for(uint32_t logL) { return logL <= 9 ? 16 : (logL <= 11 ? 8 : 4); }
-
-template <int C>
-static int launch_pass(Ctx* ctx, cudaStream_t st, const PassArgs& a, uint64_t ntiles) {
-    const uint32_t L = 1u << a.logL;
-    const size_t smem = ((size_t)C * (L + (L >> 5) + 1) + 2 * (size_t)L) * sizeof(uint64_t);
-    static bool configured = false;
-    if (!configured) {
-        SG_CUDA(cudaFuncSetAttribute(k_dft_pass<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-        configured = true;
+// One instantiation per (tile length, direction): each launch carries only the
+// butterfly code it runs, which keeps the unrolled networks in the I-cache.
+template <int LOGL, bool INV>
+__global__ void __launch_bounds__(Plan<LOGL>::T, Plan<LOGL>::T == 256 ? 2 : 1)
+    k_dft(PassArgs a, uint64_t ntiles, uint32_t ctiles) {
+    using PL = Plan<LOGL>;
+    extern __shared__ uint64_t sm[];
+    uint64_t* S = sm;
+    uint64_t* WL = S + PL::S_WORDS;
+    uint64_t* F = WL + PL::WL_WORDS;
+    if constexpr (PL::NST > 1) {
+        for (uint32_t e = threadIdx.x; e < PL::L; e += PL::T) WL[e] = tw_root(a.tw, LOGL, e, INV);
     }
-    const uint64_t ctiles = (a.m + C - 1) / C;
-    if (ntiles > 0x7fffffffULL || ctiles > 65535) {
-        set_error("dft pass grid too large");
+    const uint64_t total = ntiles * ctiles;
+    for (uint64_t t = blockIdx.x; t < total; t += gridDim.x) {
+        const uint64_t pt = t / ctiles;
+        const uint64_t col0 = (t % ctiles) * PL::C;
+        const uint32_t ncols = (uint32_t)min((uint64_t)PL::C, a.m - col0);
+        for (uint32_t rep = 0; rep < a.reps; ++rep) {
+            __syncthreads();  // the previous tile is done with S and F
+            tile_body<LOGL, INV>(a, S, WL, F, pt, col0, ncols, rep);
+        }
+    }
+}
+
+template <int LOGL, bool INV>
+static int launch_dft_dir(Ctx* ctx, cudaStream_t st, const PassArgs& a, uint64_t ntiles) {
+    using PL = Plan<LOGL>;
+    static int blocks_per_sm = 0;
+    static int num_sms = 0;
+    if (!blocks_per_sm) {
+        SG_CUDA(cudaFuncSetAttribute(k_dft<LOGL, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PL::SMEM));
+        int dev = 0;
+        SG_CUDA(cudaGetDevice(&dev));
+        SG_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
+        SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_dft<LOGL, INV>, PL::T, PL::SMEM));
+        if (blocks_per_sm < 1) blocks_per_sm = 1;
+    }
+    const uint64_t ctiles = (a.m + PL::C - 1) / PL::C;
+    if (ctiles > 0xffffffffULL) {
+        set_error("too many columns");
         return SG_ERR_UNSUPPORTED;
     }
-    dim3 grid((unsigned)ntiles, (unsigned)ctiles);
-    k_dft_pass<C><<<grid, 256, smem, st>>>(a);
-    return check_launch(ctx, "k_dft_pass");
+    const uint64_t total = ntiles * ctiles;
+    const uint64_t grid = total < (uint64_t)num_sms * blocks_per_sm ? total : (uint64_t)num_sms * blocks_per_sm;
+    k_dft<LOGL, INV><<<(unsigned)grid, PL::T, PL::SMEM, st>>>(a, ntiles, (uint32_t)ctiles);
+    return check_launch(ctx, "k_dft");
+}
+
+template <int LOGL>
+static int launch_dft(Ctx* ctx, cudaStream_t st, const PassArgs& a, uint64_t ntiles) {
+    return a.inverse ? launch_dft_dir<LOGL, true>(ctx, st, a, ntiles) : launch_dft_dir<LOGL, false>(ctx, st, a, ntiles);
 }
 
 static int run_pass(Ctx* ctx, cudaStream_t st, const PassArgs& a, uint64_t ntiles) {
-    if (a.logL > 12) {
-        set_error("dft pass longer than 4096 points");
-        return SG_ERR_UNSUPPORTED;
-    }
-    switch (cols_for(a.logL)) {
-        case 16: return launch_pass<16>(ctx, st, a, ntiles);
-        case 8: return launch_pass<8>(ctx, st, a, ntiles);
-        default: return launch_pass<4>(ctx, st, a, ntiles);
+    switch (a.logL) {
+        case 0: return launch_dft<0>(ctx, st, a, ntiles);
+        case 1: return launch_dft<1>(ctx, st, a, ntiles);
+        case 2: return launch_dft<2>(ctx, st, a, ntiles);
+        case 3: return launch_dft<3>(ctx, st, a, ntiles);
+        case 4: return launch_dft<4>(ctx, st, a, ntiles);
+        case 5: return launch_dft<5>(ctx, st, a, ntiles);
+        case 6: return launch_dft<6>(ctx, st, a, ntiles);
+        case 7: return launch_dft<7>(ctx, st, a, ntiles);
+        case 8: return launch_dft<8>(ctx, st, a, ntiles);
+        case 9: return launch_dft<9>(ctx, st, a, ntiles);
+        case 10: return launch_dft<10>(ctx, st, a, ntiles);
+        case 11: return launch_dft<11>(ctx, st, a, ntiles);
+        case 12: return launch_dft<12>(ctx, st, a, ntiles);
+        default: set_error("dft pass longer than 4096 points"); return SG_ERR_UNSUPPORTED;
     }
 }
 
-static PassArgs base_args(const uint64_t* in, uint64_t* out, uint64_t m, uint32_t logL, bool inv, const uint64_t* W,
-                          uint32_t logW) {
+static PassArgs base_args(const uint64_t* in, uint64_t* out, uint64_t m, uint32_t logL, bool inv, const Tw& tw) {
     PassArgs a{};
     a.in = in;
     a.out = out;
@@ -257,9 +366,67 @@ static PassArgs base_args(const uint64_t* in, uint64_t* out, uint64_t m, uint32_
     a.logL = logL;
     a.inverse = inv ? 1 : 0;
     a.reps = 1;
-    a.W = W;
-    a.logW = logW;
+    a.tw = tw;
     return a;
+}
+
+// Two-level root tables for N = 2^logN: lo = omega^[0, 2^h), hi = omega^(2^h * [0, 2^(logN-h))).
+static inline uint32_t tw_h(uint32_t logN) { return (logN + 1) / 2; }
+static inline uint64_t tw_words(uint32_t logN) { return (1ULL << tw_h(logN)) + (1ULL << (logN - tw_h(logN))); }
+
+__global__ void k_tw_tables(uint64_t* lo, uint64_t nlo, uint64_t* hi, uint64_t nhi, uint64_t omega, uint32_t h) {
+    const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < nlo) lo[e] = gl::canon(gl::pow(omega, e));
+    if (e < nhi) hi[e] = gl::canon(gl::pow(omega, e << h));
+}
+
+static int build_tw(Ctx* ctx, cudaStream_t st, uint32_t logN, uint64_t* mem, Tw* out) {
+    const uint32_t h = tw_h(logN);
+    const uint64_t nlo = 1ULL << h, nhi = 1ULL << (logN - h);
+    const uint64_t mx = nlo > nhi ? nlo : nhi;
+    k_tw_tables<<<(unsigned)((mx + 255) / 256), 256, 0, st>>>(mem, nlo, mem + nlo, nhi, glc::root(logN), h);
+    SG_TRY(check_launch(ctx, "k_tw_tables"));
+    out->lo = mem;
+    out->hi = mem + nlo;
+    out->h = h;
+    out->logN = logN;
+    return SG_OK;
+}
+
+int roots_table(Ctx* ctx, cudaStream_t st, uint32_t log, const uint64_t** out) {
+    std::lock_guard<std::mutex> g(ctx->mu);
+    auto it = ctx->roots.find(log);
+    if (it != ctx->roots.end()) {
+        *out = it->second;
+        return SG_OK;
+    }
+    const uint64_t words = tw_words(log);
+    uint64_t* mem = nullptr;
+    // Tables persist for the context lifetime: plain cudaMalloc, charged to the budget.
+    if (ctx->in_use.load() + words * 8 > ctx->budget) {
+        set_error("HBM budget exceeded by twiddle table");
+        return SG_ERR_BUDGET;
+    }
+    SG_CUDA(cudaMalloc((void**)&mem, words * 8));
+    ctx->in_use.fetch_add(words * 8);
+    Tw tw;
+    int rc = build_tw(ctx, st, log, mem, &tw);
+    if (rc != SG_OK) return rc;
+    // Other streams may read the table next: finish building it before publishing.
+    SG_CUDA(cudaStreamSynchronize(st));
+    ctx->roots[log] = mem;
+    *out = mem;
+    return SG_OK;
+}
+
+static int ctx_tw(Ctx* ctx, cudaStream_t st, uint32_t logN, Tw* tw) {
+    const uint64_t* mem = nullptr;
+    SG_TRY(roots_table(ctx, st, logN, &mem));
+    tw->h = tw_h(logN);
+    tw->logN = logN;
+    tw->lo = mem;
+    tw->hi = mem + (1ULL << tw->h);
+    return SG_OK;
 }
 
 int ntt_rows(Ctx* ctx, cudaStream_t st, uint64_t* d, uint64_t n, uint64_t m, int inverse, int scale_inverse) {
@@ -270,15 +437,15 @@ int ntt_rows(Ctx* ctx, cudaStream_t st, uint64_t* d, uint64_t n, uint64_t m, int
         set_error("NTT longer than 2^24 rows is not supported by the two-pass kernel");
         return SG_ERR_UNSUPPORTED;
     }
-    const uint64_t* W = nullptr;
-    SG_TRY(roots_table(ctx, st, (uint32_t)logn, &W));
+    Tw tw;
+    SG_TRY(ctx_tw(ctx, st, (uint32_t)logn, &tw));
     uint64_t ninv = 0;
     if (inverse && scale_inverse) {
         // 1/n = p - (p-1)/n for n | p-1
         ninv = GL_P - (GL_P - 1) / n;
     }
     if (logn <= 12) {
-        PassArgs a = base_args(d, d, m, logn, inverse, W, logn);
+        PassArgs a = base_args(d, d, m, logn, inverse, tw);
         a.in_ps = 1;
         a.out_ps = 1;
         if (ninv) {
@@ -291,7 +458,7 @@ int ntt_rows(Ctx* ctx, cudaStream_t st, uint64_t* d, uint64_t n, uint64_t m, int
     const uint32_t l1 = logn / 2, l2 = logn - l1;
     const uint64_t N1 = 1ULL << l1, N2 = 1ULL << l2;
     // step 1 in place
-    PassArgs s1 = base_args(d, d, m, l1, inverse, W, logn);
+    PassArgs s1 = base_args(d, d, m, l1, inverse, tw);
     s1.in_ts = 1;
     s1.in_ps = N2;
     s1.out_ts = 1;
@@ -301,7 +468,7 @@ int ntt_rows(Ctx* ctx, cudaStream_t st, uint64_t* d, uint64_t n, uint64_t m, int
     SG_TRY(run_pass(ctx, st, s1, N2));
     uint64_t* tmp = nullptr;
     SG_TRY(dev_alloc(ctx, st, n * m * 8, (void**)&tmp));
-    PassArgs s2 = base_args(d, tmp, m, l2, inverse, W, logn);
+    PassArgs s2 = base_args(d, tmp, m, l2, inverse, tw);
     s2.in_ts = N2;
     s2.in_ps = 1;
     s2.out_ts = 1;
@@ -323,6 +490,67 @@ int ntt_rows(Ctx* ctx, cudaStream_t st, uint64_t* d, uint64_t n, uint64_t m, int
     return rc != SG_OK ? rc : rc2;
 }
 
+// The LDE pass sequence over caller-provided scratch: coef (n x m) always,
+// tmp (n x m) when n > 4096.
+static int lde_passes(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t n, uint64_t m, uint64_t blowup,
+                      const uint64_t* weights, uint64_t* out, const Tw& tw, uint64_t* coef, uint64_t* tmp) {
+    const int logn = log2_exact(n), logN = (int)tw.logN;
+    if (logn <= 12) {
+        PassArgs I = base_args(trace, coef, m, logn, true, tw);
+        I.in_ps = 1;
+        I.out_ps = 1;
+        I.post_kind = 2;
+        I.weights = weights;
+        SG_TRY(run_pass(ctx, st, I, 1));
+        PassArgs F = base_args(coef, out, m, logn, false, tw);
+        F.in_ps = 1;
+        F.reps = (uint32_t)blowup;
+        F.pre_kind = 1;
+        F.pre_log = logN;
+        F.out_ps = blowup;
+        F.out_rs = 1;
+        F.canon_out = 1;
+        return run_pass(ctx, st, F, 1);
+    }
+    const uint32_t l1 = logn / 2, l2 = logn - l1;
+    const uint64_t N1 = 1ULL << l1, N2 = 1ULL << l2;
+    PassArgs I1 = base_args(trace, tmp, m, l1, true, tw);
+    I1.in_ts = 1;
+    I1.in_ps = N2;
+    I1.out_ts = 1;
+    I1.out_ps = N2;
+    I1.post_kind = 1;
+    I1.post_log = logn;
+    SG_TRY(run_pass(ctx, st, I1, N2));
+    PassArgs I2 = base_args(tmp, coef, m, l2, true, tw);
+    I2.in_ts = N2;
+    I2.in_ps = 1;
+    I2.out_ts = 1;
+    I2.out_ps = N1;
+    I2.post_kind = 2;
+    I2.weights = weights;
+    SG_TRY(run_pass(ctx, st, I2, N1));
+    PassArgs F1 = base_args(coef, out, m, l1, false, tw);
+    F1.in_ts = 1;
+    F1.in_ps = N2;
+    F1.reps = (uint32_t)blowup;
+    F1.pre_kind = 1;
+    F1.pre_log = logN;
+    F1.post_kind = 1;
+    F1.post_log = logn;
+    F1.out_ts = blowup * N1;
+    F1.out_ps = blowup;
+    F1.out_rs = 1;
+    SG_TRY(run_pass(ctx, st, F1, N2));
+    PassArgs F2 = base_args(out, out, m, l2, false, tw);
+    F2.in_ts = 1;
+    F2.in_ps = blowup * N1;
+    F2.out_ts = 1;
+    F2.out_ps = blowup * N1;
+    F2.canon_out = 1;
+    return run_pass(ctx, st, F2, N1 * blowup);
+}
+
 int coset_lde(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t n, uint64_t m, uint64_t blowup,
               const uint64_t* weights, uint64_t* out) {
     if (n == 0 || m == 0) return SG_OK;
@@ -335,115 +563,18 @@ int coset_lde(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t n, uint
         set_error("traces longer than 2^24 rows are not supported by the two-pass kernel");
         return SG_ERR_UNSUPPORTED;
     }
-    const uint64_t* W = nullptr;
-    SG_TRY(roots_table(ctx, st, (uint32_t)logN, &W));
+    Tw tw;
+    SG_TRY(ctx_tw(ctx, st, (uint32_t)logN, &tw));
     uint64_t* coef = nullptr;
+    uint64_t* tmp = nullptr;
     SG_TRY(dev_alloc(ctx, st, n * m * 8, (void**)&coef));
     int rc = SG_OK;
-    if (logn <= 12) {
-        PassArgs I = base_args(trace, coef, m, logn, true, W, logN);
-        I.in_ps = 1;
-        I.out_ps = 1;
-        I.post_kind = 2;
-        I.weights = weights;
-        rc = run_pass(ctx, st, I, 1);
-        if (rc == SG_OK) {
-            PassArgs F = base_args(coef, out, m, logn, false, W, logN);
-            F.in_ps = 1;
-            F.reps = (uint32_t)blowup;
-            F.pre_kind = 1;
-            F.pre_log = logN;
-            F.out_ps = blowup;
-            F.out_rs = 1;
-            F.canon_out = 1;
-            rc = run_pass(ctx, st, F, 1);
-        }
-    } else {
-        const uint32_t l1 = logn / 2, l2 = logn - l1;
-        const uint64_t N1 = 1ULL << l1, N2 = 1ULL << l2;
-        uint64_t* tmp = nullptr;
-        rc = dev_alloc(ctx, st, n * m * 8, (void**)&tmp);
-        if (rc == SG_OK) {
-            PassArgs I1 = base_args(trace, tmp, m, l1, true, W, logN);
-            I1.in_ts = 1;
-            I1.in_ps = N2;
-            I1.out_ts = 1;
-            I1.out_ps = N2;
-            I1.post_kind = 1;
-            I1.post_log = logn;
-            rc = run_pass(ctx, st, I1, N2);
-            if (rc == SG_OK) {
-                PassArgs I2 = base_args(tmp, coef, m, l2, true, W, logN);
-                I2.in_ts = N2;
-                I2.in_ps = 1;
-                I2.out_ts = 1;
-                I2.out_ps = N1;
-                I2.post_kind = 2;
-                I2.weights = weights;
-                rc = run_pass(ctx, st, I2, N1);
-            }
-            int rf = dev_free(ctx, st, tmp, n * m * 8);
-            if (rc == SG_OK) rc = rf;
-        }
-        if (rc == SG_OK) {
-            PassArgs F1 = base_args(coef, out, m, l1, false, W, logN);
-            F1.in_ts = 1;
-            F1.in_ps = N2;
-            F1.reps = (uint32_t)blowup;
-            F1.pre_kind = 1;
-            F1.pre_log = logN;
-            F1.post_kind = 1;
-            F1.post_log = logn;
-            F1.out_ts = blowup * N1;
-            F1.out_ps = blowup;
-            F1.out_rs = 1;
-            rc = run_pass(ctx, st, F1, N2);
-        }
-        if (rc == SG_OK) {
-            PassArgs F2 = base_args(out, out, m, l2, false, W, logN);
-            F2.in_ts = 1;
-            F2.in_ps = blowup * N1;
-            F2.out_ts = 1;
-            F2.out_ps = blowup * N1;
-            F2.canon_out = 1;
-            rc = run_pass(ctx, st, F2, N1 * blowup);
-        }
-    }
-    int rf = dev_free(ctx, st, coef, n * m * 8);
-    return rc != SG_OK ? rc : rf;
-}
-
-// W[e] = omega^e for e in [0, N): each thread raises omega to its own exponent.
-__global__ void k_roots(uint64_t* W, uint64_t N, uint64_t omega) {
-    const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e < N) W[e] = gl::canon(gl::pow(omega, e));
-}
-
-int roots_table(Ctx* ctx, cudaStream_t st, uint32_t log, const uint64_t** out) {
-    std::lock_guard<std::mutex> g(ctx->mu);
-    auto it = ctx->roots.find(log);
-    if (it != ctx->roots.end()) {
-        *out = it->second;
-        return SG_OK;
-    }
-    const uint64_t N = 1ULL << log;
-    uint64_t* W = nullptr;
-    // Tables persist for the context lifetime: plain cudaMalloc, charged to the budget.
-    if (ctx->in_use.load() + N * 8 > ctx->budget) {
-        set_error("HBM budget exceeded by twiddle table");
-        return SG_ERR_BUDGET;
-    }
-    SG_CUDA(cudaMalloc((void**)&W, N * 8));
-    ctx->in_use.fetch_add(N * 8);
-    const uint64_t omega = glc::root(log);
-    k_roots<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(W, N, omega);
-    int rc = check_launch(ctx, "k_roots");
+    if (logn > 12) rc = dev_alloc(ctx, st, n * m * 8, (void**)&tmp);
+    if (rc == SG_OK) rc = lde_passes(ctx, st, trace, n, m, blowup, weights, out, tw, coef, tmp);
+    int rf = dev_free(ctx, st, tmp, n * m * 8);
+    int rf2 = dev_free(ctx, st, coef, n * m * 8);
     if (rc != SG_OK) return rc;
-    // Other streams may read the table next: finish building it before publishing.
-    SG_CUDA(cudaStreamSynchronize(st));
-    ctx->roots[log] = W;
-    *out = W;
-    return SG_OK;
+    return rf != SG_OK ? rf : rf2;
 }
 
 }  // namespace sg
@@ -520,63 +651,15 @@ extern "C" int sg_coset_lde_static(void* stream, const uint64_t* d_trace, uint64
     SG_TRY(static_scratch(&scratch));
     cudaStream_t st = (cudaStream_t)stream;
     Ctx* ctx = &g_static_ctx;
-    uint64_t* W = scratch;
-    uint64_t* coef = scratch + N;
-    uint64_t* tmp = coef + n * m;
-    k_roots<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(W, N, glc::root((uint32_t)logN));
-    SG_TRY(check_launch(ctx, "k_roots"));
-    if (logn <= 12) {
-        PassArgs I = base_args(d_trace, coef, m, logn, true, W, logN);
-        I.in_ps = 1;
-        I.out_ps = 1;
-        I.post_kind = 2;
-        I.weights = d_weights;
-        SG_TRY(run_pass(ctx, st, I, 1));
-        PassArgs F = base_args(coef, d_out, m, logn, false, W, logN);
-        F.in_ps = 1;
-        F.reps = blowup;
-        F.pre_kind = 1;
-        F.pre_log = logN;
-        F.out_ps = blowup;
-        F.out_rs = 1;
-        F.canon_out = 1;
-        return run_pass(ctx, st, F, 1);
+    // Scratch layout: [root tables | coefficients (n x m) | four-step intermediate (n x m)].
+    const uint64_t tw_region = tw_words((uint32_t)logN) > N ? tw_words((uint32_t)logN) : N;
+    if (tw_region + 2 * n * m > SG_STATIC_SCRATCH_BYTES / sizeof(uint64_t)) {
+        set_error("sg_coset_lde_static: request does not fit the static scratch; use sg_coset_lde");
+        return SG_ERR_INVALID;
     }
-    const uint32_t l1 = logn / 2, l2 = logn - l1;
-    const uint64_t N1 = 1ULL << l1, N2 = 1ULL << l2;
-    PassArgs I1 = base_args(d_trace, tmp, m, l1, true, W, logN);
-    I1.in_ts = 1;
-    I1.in_ps = N2;
-    I1.out_ts = 1;
-    I1.out_ps = N2;
-    I1.post_kind = 1;
-    I1.post_log = logn;
-    SG_TRY(run_pass(ctx, st, I1, N2));
-    PassArgs I2 = base_args(tmp, coef, m, l2, true, W, logN);
-    I2.in_ts = N2;
-    I2.in_ps = 1;
-    I2.out_ts = 1;
-    I2.out_ps = N1;
-    I2.post_kind = 2;
-    I2.weights = d_weights;
-    SG_TRY(run_pass(ctx, st, I2, N1));
-    PassArgs F1 = base_args(coef, d_out, m, l1, false, W, logN);
-    F1.in_ts = 1;
-    F1.in_ps = N2;
-    F1.reps = blowup;
-    F1.pre_kind = 1;
-    F1.pre_log = logN;
-    F1.post_kind = 1;
-    F1.post_log = logn;
-    F1.out_ts = (uint64_t)blowup * N1;
-    F1.out_ps = blowup;
-    F1.out_rs = 1;
-    SG_TRY(run_pass(ctx, st, F1, N2));
-    PassArgs F2 = base_args(d_out, d_out, m, l2, false, W, logN);
-    F2.in_ts = 1;
-    F2.in_ps = (uint64_t)blowup * N1;
-    F2.out_ts = 1;
-    F2.out_ps = (uint64_t)blowup * N1;
-    F2.canon_out = 1;
-    return run_pass(ctx, st, F2, N1 * blowup);
+    Tw tw;
+    SG_TRY(build_tw(ctx, st, (uint32_t)logN, scratch, &tw));
+    uint64_t* coef = scratch + tw_region;
+    uint64_t* tmp = coef + n * m;
+    return lde_passes(ctx, st, d_trace, n, m, blowup, d_weights, d_out, tw, coef, tmp);
 }
