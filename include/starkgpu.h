@@ -157,6 +157,148 @@ SG_API void sg_lde_free(sg_ctx* ctx, sg_lde* lde);
  *      (stark::grinding::inner_hash_lanes). Returns the smallest valid nonce. ---- */
 SG_API int sg_grind(sg_ctx* ctx, void* stream, const uint64_t inner_lanes[4], uint8_t grinding_factor, uint64_t* nonce_out);
 
+
+/* ---- Fiat-Shamir transcript: replaces DefaultTranscript
+ *      (crypto/crypto/src/fiat_shamir/default_transcript.rs:31-146) and
+ *      IsStarkTranscript::sample_z_ood_with_domain_params (is_transcript.rs:44-75).
+ *      Host-side; field elements are absorbed as canonical big-endian bytes. ---- */
+typedef struct sg_transcript sg_transcript;
+SG_API sg_transcript* sg_transcript_new(const uint8_t* data, uint64_t len);
+SG_API sg_transcript* sg_transcript_clone(const sg_transcript* t);
+SG_API void sg_transcript_free(sg_transcript* t);
+SG_API void sg_transcript_append(sg_transcript* t, const uint8_t* data, uint64_t len);
+SG_API void sg_transcript_append_base(sg_transcript* t, uint64_t v);
+SG_API void sg_transcript_append_ext3(sg_transcript* t, const uint64_t v[3]);
+SG_API void sg_transcript_sample(sg_transcript* t, uint8_t out[32]);
+SG_API void sg_transcript_state(const sg_transcript* t, uint8_t out[32]);
+SG_API uint64_t sg_transcript_sample_base(sg_transcript* t);
+SG_API void sg_transcript_sample_ext3(sg_transcript* t, uint64_t out[3]);
+SG_API uint64_t sg_transcript_sample_u64(sg_transcript* t, uint64_t upper_bound);
+SG_API void sg_transcript_sample_z_ood(sg_transcript* t, uint64_t trace_len, uint64_t lde_len, uint64_t coset_offset,
+                                       uint64_t out[3]);
+/* Keccak-256 (original padding) of a host buffer. */
+SG_API void sg_keccak256(const uint8_t* data, uint64_t len, uint8_t out[32]);
+
+/* ---- batch inversion: replaces inverse::batch_inverse_ext3 / _dev
+ *      (crypto/math-cuda/src/inverse.rs:53,157). n ext3 elements in, their
+ *      inverses out (may alias). zero_found (host, may be NULL) reports a zero
+ *      input, for which the outputs are undefined (the reference errors). ---- */
+SG_API int sg_batch_inverse_ext3(sg_ctx* ctx, void* stream, const uint64_t* d_in, uint64_t n, uint64_t* d_out,
+                                 int* zero_found);
+/* ---- inverse denominators: replaces inverse::compute_and_invert_denoms_ext3_dev
+ *      (inverse.rs:241). d_out[k*n + i] = 1/(z_k - x_i) (x_minus_z = 0, R3 OOD)
+ *      or 1/(x_i - z_k) (x_minus_z = 1, R4 DEEP); z_host: k ext3 scalars. ---- */
+SG_API int sg_inv_denoms_ext3(sg_ctx* ctx, void* stream, const uint64_t* d_x, uint64_t n, const uint64_t* z_host,
+                              uint32_t k, int x_minus_z, uint64_t* d_out, int* zero_found);
+/* ---- barycentric OOD sums: replaces barycentric::barycentric_{base,ext3}_multi_on_device
+ *      (crypto/math-cuda/src/barycentric.rs:379,449). For each of k <= 8 points
+ *      and each column c < cols: d_out[k*cols + c] (ext3) =
+ *      sum_{i<n} points[i] * col_c(row i*row_stride) * inv_denoms[k*n + i].
+ *      d_data is row-major (row_u64 u64 per row); ext3 != 0 reads 3-u64 elements. ---- */
+SG_API int sg_barycentric_sums(sg_ctx* ctx, void* stream, const uint64_t* d_data, uint64_t row_u64,
+                               uint64_t row_stride, int ext3, uint64_t cols, const uint64_t* d_points,
+                               const uint64_t* d_inv_denoms, uint64_t n, uint32_t k, uint64_t* d_out);
+/* ---- DEEP composition: replaces deep::deep_composition_ext3_fully_resident_keep
+ *      (crypto/math-cuda/src/deep.rs:316). Per LDE row i:
+ *        sum_j gh_j (H_j(x_i) - h_ood_j) inv_h[i] + sum_{j,k} gt_{jk} (t_j(x_i) - t_ood_{jk}) inv_t[k*rows+i]
+ *      main rows x m (base), aux rows x a (ext3), parts rows x p (ext3), all row-major;
+ *      h_ood/gammas_h: p ext3 (host); trace_ood/gammas_tr: (m+a)*k ext3 (host, index j*k+kk).
+ *      bitrev_out != 0 writes row i at bit-reversed position (FRI order). ---- */
+SG_API int sg_deep_composition(sg_ctx* ctx, void* stream, const uint64_t* d_main, uint64_t m, const uint64_t* d_aux,
+                               uint64_t a, const uint64_t* d_parts, uint64_t p, uint64_t rows, const uint64_t* h_ood,
+                               const uint64_t* trace_ood, const uint64_t* gammas_h, const uint64_t* gammas_tr,
+                               uint32_t k, const uint64_t* d_inv_h, const uint64_t* d_inv_t, int bitrev_out,
+                               uint64_t* d_out);
+/* ---- FRI fold: replaces the fold of FriCommitState::fold_and_commit_layer
+ *      (crypto/math-cuda/src/fri.rs:110; fri_functions.rs:15-61). d_in: 2h ext3 in
+ *      bit-reversed order; d_out[j] = (lo+hi) + inv_tw[j]*zeta*(lo-hi). Optionally
+ *      writes the next layer's twiddles tw[2j]^2 (h/2) and the folded layer's
+ *      Merkle leaves Keccak(out[2j] || out[2j+1]) (h/2 x 32 bytes). ---- */
+SG_API int sg_fri_fold_layer(sg_ctx* ctx, void* stream, const uint64_t* d_in, uint64_t h, const uint64_t* d_inv_tw,
+                             const uint64_t zeta[3], uint64_t* d_out, uint64_t* d_inv_tw_next, uint8_t* d_leaves);
+/* FRI layer leaves over n ext3 evaluations (keccak_fri_leaves_ext3, keccak.cu:384). */
+SG_API int sg_fri_leaves(sg_ctx* ctx, void* stream, const uint64_t* d_evals, uint64_t n, uint8_t* d_leaves);
+/* ---- row gathers for query openings: replaces barycentric::gather_rows_{base,ext3}_on_device
+ *      (barycentric.rs:522,561) and fri::gather_ext3_at (fri.rs:260): d_out[q*width + c] =
+ *      d_data[rows[q]*row_u64 + col0 + c]. ---- */
+SG_API int sg_gather_rows(sg_ctx* ctx, void* stream, const uint64_t* d_data, uint64_t row_u64, uint64_t nrows,
+                          uint64_t col0, uint64_t width, const uint32_t* d_rows, uint32_t nq, uint64_t* d_out);
+
+/* LogUp CSR descriptor (crypto/math-cuda/src/logup.rs:26-44), host arrays. */
+typedef struct {
+    uint32_t num_interactions;
+    const uint64_t* bus_ids;              /* [K] */
+    const uint32_t* elem_offsets;         /* [K+1] */
+    const uint32_t* elem_alpha_idx;       /* [elems] */
+    const uint64_t* elem_consts;          /* [elems] */
+    const uint32_t* term_offsets;         /* [elems+1] */
+    const uint64_t* term_coefs;           /* [terms] */
+    const uint32_t* term_cols;            /* [terms] */
+    uint32_t num_out_cols;                /* committed + virtual term columns */
+    const uint32_t* out_col_offsets;      /* [num_out_cols+1] */
+    const uint32_t* out_col_interactions; /* [...] */
+    const uint64_t* mult_consts;          /* [K] */
+    const uint32_t* mult_term_offsets;    /* [K+1] */
+    const uint64_t* mult_term_coefs;      /* [...] */
+    const uint32_t* mult_term_cols;       /* [...] */
+    uint32_t num_committed;               /* the first num_committed out columns are committed */
+} sg_logup_desc;
+/* ---- LogUp aux build: replaces logup::logup_aux_resident (crypto/math-cuda/src/logup.rs:311;
+ *      CPU lookup.rs:1660-1842). d_main: n x m row-major. d_aux: n x (num_committed+1)
+ *      ext3 row-major: committed term columns then the accumulated column.
+ *      alpha_powers: num_alpha ext3 (host). Writes the table contribution L. ---- */
+SG_API int sg_logup_aux(sg_ctx* ctx, void* stream, const uint64_t* d_main, uint64_t n, uint64_t m,
+                        const sg_logup_desc* desc, const uint64_t* alpha_powers, uint32_t num_alpha,
+                        const uint64_t z[3], uint64_t* d_aux, uint64_t table_contribution[3]);
+
+
+/* Lowered constraint program (DeviceProgram, crypto/stark/src/constraint_ir/device.rs):
+ * nodes are {op, a, b, res} u32 quadruples with the reference's OP_* tags,
+ * operand encoding (kind << 29 | payload) and RES_EXT_BIT slot packing. */
+typedef struct {
+    const uint32_t* nodes;
+    uint32_t num_nodes;
+    const uint64_t* base_consts;
+    uint32_t num_base_consts;
+    const uint64_t* ext_consts; /* 3 u64 per constant */
+    uint32_t num_ext_consts;
+    const uint32_t* roots;      /* slot | RES_EXT_BIT, one per constraint */
+    uint32_t num_roots;
+    uint32_t num_base_slots;
+    uint32_t num_ext_slots;
+} sg_device_program;
+
+/* Composition accumulation (CompositionAccum, crypto/math-cuda/src/constraint_interp.rs:157). */
+typedef struct {
+    const uint64_t* beta_trans; /* host: num_roots ext3 */
+    const uint64_t* d_z_inv;    /* device: z_len base values, used cyclically (row % z_len) */
+    uint64_t z_len;
+    uint32_t num_boundary;
+    const uint64_t* b_col;      /* host: num_boundary */
+    const uint64_t* b_is_aux;   /* host: num_boundary (0 = main, 1 = aux) */
+    const uint64_t* b_value;    /* host: num_boundary ext3 */
+    const uint64_t* b_beta;     /* host: num_boundary ext3 */
+    const uint64_t* d_b_z_inv;  /* device: num_boundary x rows base values */
+} sg_composition;
+
+/* ---- constraint evaluation: replaces constraint_interp::eval_composition_on_device
+ *      (crypto/math-cuda/src/constraint_interp.rs:353; kernel semantics of
+ *      constraint_interp.cu:379-468) when comp != NULL: d_out = H, rows ext3;
+ *      and constraint_interp::eval_constraints_on_device (constraint_interp.rs:53)
+ *      when comp == NULL: d_out = per-constraint evals [c*rows + row] ext3.
+ *      Trace frames read row (row + offset*next_step) mod rows of the row-major
+ *      main (rows x m) and aux (rows x a ext3) LDEs. rap/alpha: host ext3 tables. ---- */
+SG_API int sg_eval_constraints(sg_ctx* ctx, void* stream, const sg_device_program* prog, const uint64_t* rap,
+                               uint32_t n_rap, const uint64_t* alpha, uint32_t n_alpha,
+                               const uint64_t table_offset[3], const uint64_t* d_main, uint64_t m,
+                               const uint64_t* d_aux, uint64_t a, uint64_t rows, uint64_t next_step,
+                               const sg_composition* comp, uint64_t* d_out);
+/* ---- degree-2 composition split: replaces decompose_d2_ext3 (constraint_interp.cu:477;
+ *      prover.rs:1557-1662). d_h: lde_rows ext3; d_inv_2x: lde_rows/2 values 1/(2x_i);
+ *      d_out: lde_rows/2 rows of [H0, H1] (6 u64 per row). ---- */
+SG_API int sg_decompose_d2(sg_ctx* ctx, void* stream, const uint64_t* d_h, uint64_t lde_rows, const uint64_t* d_inv_2x,
+                           uint64_t* d_out);
+
 #ifdef __cplusplus
 }
 #endif

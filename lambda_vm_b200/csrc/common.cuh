@@ -12,6 +12,21 @@
 
 #include "../../include/starkgpu.h"
 
+// Host-side field helpers (transcript.cu); internal to the library.
+extern "C" {
+uint64_t sg_host_gl_canon(uint64_t a);
+uint64_t sg_host_gl_add(uint64_t a, uint64_t b);
+uint64_t sg_host_gl_sub(uint64_t a, uint64_t b);
+uint64_t sg_host_gl_mul(uint64_t a, uint64_t b);
+uint64_t sg_host_gl_pow(uint64_t a, uint64_t e);
+uint64_t sg_host_gl_inv(uint64_t a);
+void sg_host_fp3_add(const uint64_t* a, const uint64_t* b, uint64_t* c);
+void sg_host_fp3_sub(const uint64_t* a, const uint64_t* b, uint64_t* c);
+void sg_host_fp3_mul(const uint64_t* a, const uint64_t* b, uint64_t* c);
+void sg_host_fp3_pow(const uint64_t* a, uint64_t e, uint64_t* out);
+int sg_host_fp3_inv(const uint64_t* a, uint64_t* out);
+}
+
 namespace sg {
 
 void set_error(const std::string& msg);

@@ -1,0 +1,421 @@
+// Constraint evaluation (round 2) and the composition split for sm_100a.
+//
+// Reference behaviour:
+//  * program format: crypto/stark/src/constraint_ir/device.rs (DeviceNode
+//    {op, a, b, res}, OP_* tags, operand kind << 29 | payload, RES_EXT_BIT),
+//    so a DeviceProgram lowered by the reference runs here unchanged;
+//  * per-row semantics: eval_device_program (device.rs) / constraint_interp.cu
+//    eval_program_row, with frame rows r = (row + offset * next_step) mod rows;
+//  * composition: evaluator.rs accumulation,
+//      H(row) = z_inv[row % z_len] * sum_c beta_c C_c(row)
+//             + sum_b z_b_inv[b][row] * beta_b * (trace_b(row) - value_b);
+//  * degree-2 split: prover.rs:1557-1662 decompose, H0 = (h(x)+h(-x))/2,
+//    H1 = (h(x)-h(-x)) / (2x).
+//
+// Design: one thread per LDE row walks the program; its value slots (the
+// lowering's max-live-set, base and ext classes) live in SHARED memory,
+// laid out slot-major so a warp's accesses to one slot are consecutive.
+// The reference keeps these slots in global memory, where their traffic
+// dominates the walk. Trace reads come from the row-major resident LDEs.
+#include <vector>
+
+#include "common.cuh"
+#include "gl.cuh"
+
+namespace sg {
+
+using gl::fe3;
+
+#define OP_CONST_BASE 0u
+#define OP_CONST_EXT 1u
+#define OP_VAR 2u
+#define OP_RAP_CHALLENGE 3u
+#define OP_ALPHA_POW 4u
+#define OP_TABLE_OFFSET 5u
+#define OP_ADD 6u
+#define OP_SUB 7u
+#define OP_MUL 8u
+#define OP_NEG 9u
+#define OP_EMBED 10u
+#define OPK_SHIFT 29u
+#define OPK_PAYLOAD_MASK 0x1FFFFFFFu
+#define OPK_BASE_SLOT 0u
+#define OPK_EXT_SLOT 1u
+#define OPK_BASE_CONST 2u
+#define OPK_EXT_CONST 3u
+#define OPK_RAP 4u
+#define OPK_ALPHA 5u
+#define OPK_OFFSET 6u
+#define RES_EXT_BIT 0x80000000u
+#define RES_SLOT_MASK 0x7FFFFFFFu
+
+struct Uni {
+    const uint64_t* base_consts;
+    const uint64_t* ext_consts;  // 3 per entry
+    const uint64_t* rap;
+    const uint64_t* alpha;
+    fe3 offset;
+};
+
+struct SlotFile {
+    uint64_t* vb;  // base slot s at vb[s * st]
+    uint64_t* ve;  // ext slot s component k at ve[(3s + k) * st]
+    uint64_t st;
+    __device__ __forceinline__ uint64_t gb(uint32_t s) const { return vb[(uint64_t)s * st]; }
+    __device__ __forceinline__ void pb(uint32_t s, uint64_t v) const { vb[(uint64_t)s * st] = v; }
+    __device__ __forceinline__ fe3 ge(uint32_t s) const {
+        const uint64_t* p = ve + (uint64_t)s * 3 * st;
+        return fe3{p[0], p[st], p[2 * st]};
+    }
+    __device__ __forceinline__ void pe(uint32_t s, fe3 v) const {
+        uint64_t* p = ve + (uint64_t)s * 3 * st;
+        p[0] = v.c0;
+        p[st] = v.c1;
+        p[2 * st] = v.c2;
+    }
+};
+
+__device__ __forceinline__ bool is_base_kind(uint32_t enc) {
+    const uint32_t k = enc >> OPK_SHIFT;
+    return k == OPK_BASE_SLOT || k == OPK_BASE_CONST;
+}
+__device__ __forceinline__ uint64_t base_op(uint32_t enc, const SlotFile& f, const Uni& u) {
+    const uint32_t p = enc & OPK_PAYLOAD_MASK;
+    return (enc >> OPK_SHIFT) == OPK_BASE_SLOT ? f.gb(p) : __ldg(u.base_consts + p);
+}
+__device__ __forceinline__ fe3 ext_op(uint32_t enc, const SlotFile& f, const Uni& u) {
+    const uint32_t p = enc & OPK_PAYLOAD_MASK;
+    switch (enc >> OPK_SHIFT) {
+        case OPK_BASE_SLOT: return fe3{f.gb(p), 0, 0};
+        case OPK_EXT_SLOT: return f.ge(p);
+        case OPK_BASE_CONST: return fe3{__ldg(u.base_consts + p), 0, 0};
+        case OPK_EXT_CONST: return fe3{__ldg(u.ext_consts + 3 * p), __ldg(u.ext_consts + 3 * p + 1), __ldg(u.ext_consts + 3 * p + 2)};
+        case OPK_RAP: return fe3{__ldg(u.rap + 3 * p), __ldg(u.rap + 3 * p + 1), __ldg(u.rap + 3 * p + 2)};
+        case OPK_ALPHA: return fe3{__ldg(u.alpha + 3 * p), __ldg(u.alpha + 3 * p + 1), __ldg(u.alpha + 3 * p + 2)};
+        default: return u.offset;
+    }
+}
+
+struct Trace {
+    const uint64_t* main;
+    uint64_t m;
+    const uint64_t* aux;  // rows x A ext3
+    uint64_t A;
+    uint64_t rows;
+    uint64_t next_step;
+};
+
+__device__ __forceinline__ void walk(const uint4* nodes, uint32_t num_nodes, const Uni& u, const SlotFile& f,
+                                     const Trace& t, uint64_t row) {
+    for (uint32_t i = 0; i < num_nodes; ++i) {
+        const uint4 nd = __ldg(nodes + i);
+        const uint32_t slot = nd.w & RES_SLOT_MASK;
+        const bool rx = (nd.w & RES_EXT_BIT) != 0;
+        switch (nd.x) {
+            case OP_VAR: {
+                const uint32_t off = (nd.z >> 8) & 0xFFu;
+                uint64_t r = row + (uint64_t)off * t.next_step;
+                if (r >= t.rows) r -= t.rows;
+                const uint32_t col = nd.y & 0xFFFFu;
+                if ((nd.z >> 16) & 1u)
+                    f.pb(slot, t.main[r * t.m + col]);
+                else {
+                    const uint64_t* p = t.aux + (r * t.A + col) * 3;
+                    f.pe(slot, fe3{p[0], p[1], p[2]});
+                }
+                break;
+            }
+            case OP_ADD:
+                if (!rx)
+                    f.pb(slot, gl::add(base_op(nd.y, f, u), base_op(nd.z, f, u)));
+                else if (is_base_kind(nd.y)) {
+                    const uint64_t x = base_op(nd.y, f, u);
+                    const fe3 y = ext_op(nd.z, f, u);
+                    f.pe(slot, fe3{gl::add(x, y.c0), y.c1, y.c2});
+                } else if (is_base_kind(nd.z)) {
+                    const fe3 x = ext_op(nd.y, f, u);
+                    f.pe(slot, fe3{gl::add(x.c0, base_op(nd.z, f, u)), x.c1, x.c2});
+                } else
+                    f.pe(slot, gl::add3(ext_op(nd.y, f, u), ext_op(nd.z, f, u)));
+                break;
+            case OP_SUB:
+                if (!rx)
+                    f.pb(slot, gl::sub(base_op(nd.y, f, u), base_op(nd.z, f, u)));
+                else if (is_base_kind(nd.y)) {
+                    const uint64_t x = base_op(nd.y, f, u);
+                    const fe3 y = ext_op(nd.z, f, u);
+                    f.pe(slot, fe3{gl::sub(x, y.c0), gl::sub(0, y.c1), gl::sub(0, y.c2)});
+                } else if (is_base_kind(nd.z)) {
+                    const fe3 x = ext_op(nd.y, f, u);
+                    f.pe(slot, fe3{gl::sub(x.c0, base_op(nd.z, f, u)), x.c1, x.c2});
+                } else
+                    f.pe(slot, gl::sub3(ext_op(nd.y, f, u), ext_op(nd.z, f, u)));
+                break;
+            case OP_MUL:
+                if (!rx)
+                    f.pb(slot, gl::mul(base_op(nd.y, f, u), base_op(nd.z, f, u)));
+                else if (is_base_kind(nd.y))
+                    f.pe(slot, gl::mulb3(ext_op(nd.z, f, u), base_op(nd.y, f, u)));
+                else if (is_base_kind(nd.z))
+                    f.pe(slot, gl::mulb3(ext_op(nd.y, f, u), base_op(nd.z, f, u)));
+                else
+                    f.pe(slot, gl::mul3(ext_op(nd.y, f, u), ext_op(nd.z, f, u)));
+                break;
+            case OP_NEG:
+                if (!rx)
+                    f.pb(slot, gl::neg(base_op(nd.y, f, u)));
+                else {
+                    const fe3 x = ext_op(nd.y, f, u);
+                    f.pe(slot, fe3{gl::neg(x.c0), gl::neg(x.c1), gl::neg(x.c2)});
+                }
+                break;
+            case OP_EMBED: f.pe(slot, ext_op(nd.y, f, u)); break;
+            case OP_CONST_BASE: f.pb(slot, __ldg(u.base_consts + nd.y)); break;
+            case OP_CONST_EXT: f.pe(slot, ext_op((OPK_EXT_CONST << OPK_SHIFT) | nd.y, f, u)); break;
+            case OP_RAP_CHALLENGE: f.pe(slot, ext_op((OPK_RAP << OPK_SHIFT) | nd.y, f, u)); break;
+            case OP_ALPHA_POW: f.pe(slot, ext_op((OPK_ALPHA << OPK_SHIFT) | nd.y, f, u)); break;
+            case OP_TABLE_OFFSET: f.pe(slot, u.offset); break;
+            default: break;
+        }
+    }
+}
+
+__device__ __forceinline__ fe3 root_val(uint32_t enc, const SlotFile& f) {
+    const uint32_t s = enc & RES_SLOT_MASK;
+    return (enc & RES_EXT_BIT) ? f.ge(s) : fe3{f.gb(s), 0, 0};
+}
+
+struct Comp {
+    const uint64_t* beta;     // num_roots ext3
+    const uint64_t* z_inv;    // z_len base
+    uint64_t z_len;
+    uint32_t nb;              // boundary constraints
+    const uint64_t* b_col;    // nb
+    const uint64_t* b_aux;    // nb (0/1)
+    const uint64_t* b_value;  // nb ext3
+    const uint64_t* b_beta;   // nb ext3
+    const uint64_t* b_zinv;   // nb x rows
+};
+
+// mode 0: composition H(row); mode 1: per-constraint matrix evals[c*rows + row].
+__global__ void k_constraints(const uint4* nodes, uint32_t num_nodes, const uint32_t* roots, uint32_t num_roots,
+                              uint32_t nbs, uint32_t nes, Uni u, Trace t, Comp cp, int mode, uint64_t* out,
+                              uint64_t* gscratch) {
+    extern __shared__ uint64_t shs[];
+    const uint64_t T = blockDim.x;
+    SlotFile f;
+    if (gscratch) {
+        const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+        const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        f.vb = gscratch + g;
+        f.ve = gscratch + (uint64_t)nbs * nthreads + g;
+        f.st = nthreads;
+    } else {
+        f.vb = shs + threadIdx.x;
+        f.ve = shs + (uint64_t)nbs * T + threadIdx.x;
+        f.st = T;
+    }
+    for (uint64_t row = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; row < t.rows;
+         row += (uint64_t)gridDim.x * blockDim.x) {
+        walk(nodes, num_nodes, u, f, t, row);
+        if (mode == 1) {
+            for (uint32_t c = 0; c < num_roots; ++c) {
+                const fe3 v = gl::canon3(root_val(roots[c], f));
+                uint64_t* o = out + 3 * ((uint64_t)c * t.rows + row);
+                o[0] = v.c0;
+                o[1] = v.c1;
+                o[2] = v.c2;
+            }
+            continue;
+        }
+        fe3 sum{0, 0, 0};
+        for (uint32_t c = 0; c < num_roots; ++c) {
+            const uint32_t enc = roots[c];
+            const fe3 b{__ldg(cp.beta + 3 * c), __ldg(cp.beta + 3 * c + 1), __ldg(cp.beta + 3 * c + 2)};
+            if (enc & RES_EXT_BIT)
+                sum = gl::add3(sum, gl::mul3(b, f.ge(enc & RES_SLOT_MASK)));
+            else
+                sum = gl::add3(sum, gl::mulb3(b, f.gb(enc & RES_SLOT_MASK)));
+        }
+        fe3 h = gl::mulb3(sum, __ldg(cp.z_inv + row % cp.z_len));
+        for (uint32_t b = 0; b < cp.nb; ++b) {
+            const uint64_t col = cp.b_col[b];
+            fe3 cell;
+            if (cp.b_aux[b]) {
+                const uint64_t* p = t.aux + (row * t.A + col) * 3;
+                cell = fe3{p[0], p[1], p[2]};
+            } else {
+                cell = fe3{t.main[row * t.m + col], 0, 0};
+            }
+            const fe3 val{cp.b_value[3 * b], cp.b_value[3 * b + 1], cp.b_value[3 * b + 2]};
+            const fe3 bb{cp.b_beta[3 * b], cp.b_beta[3 * b + 1], cp.b_beta[3 * b + 2]};
+            const fe3 zb = gl::mulb3(bb, cp.b_zinv[(uint64_t)b * t.rows + row]);
+            h = gl::add3(h, gl::mul3(zb, gl::sub3(cell, val)));
+        }
+        h = gl::canon3(h);
+        out[3 * row] = h.c0;
+        out[3 * row + 1] = h.c1;
+        out[3 * row + 2] = h.c2;
+    }
+}
+
+// H0[i] = (h[i] + h[i+n]) / 2, H1[i] = inv_2x[i] (h[i] - h[i+n]); out rows: [H0 | H1] ext3.
+__global__ void k_decompose_d2(const uint64_t* h, const uint64_t* inv_2x, uint64_t two_inv, uint64_t n,
+                               uint64_t* out) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const fe3 x{h[3 * i], h[3 * i + 1], h[3 * i + 2]};
+    const fe3 y{h[3 * (i + n)], h[3 * (i + n) + 1], h[3 * (i + n) + 2]};
+    const fe3 a = gl::canon3(gl::mulb3(gl::add3(x, y), two_inv));
+    const fe3 b = gl::canon3(gl::mulb3(gl::sub3(x, y), inv_2x[i]));
+    uint64_t* o = out + 6 * i;
+    o[0] = a.c0;
+    o[1] = a.c1;
+    o[2] = a.c2;
+    o[3] = b.c0;
+    o[4] = b.c1;
+    o[5] = b.c2;
+}
+
+}  // namespace sg
+
+using namespace sg;
+
+extern "C" {
+
+int sg_eval_constraints(sg_ctx* c, void* stream, const sg_device_program* prog, const uint64_t* rap, uint32_t n_rap,
+                        const uint64_t* alpha, uint32_t n_alpha, const uint64_t table_offset[3],
+                        const uint64_t* d_main, uint64_t m, const uint64_t* d_aux, uint64_t a, uint64_t rows,
+                        uint64_t next_step, const sg_composition* comp, uint64_t* d_out) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(c);
+    SG_CHECK_ARG(ctx && prog && table_offset, "null argument");
+    SG_CHECK_ARG(rows >= 1 && next_step < rows, "bad row count / frame step");
+    cudaStream_t st = (cudaStream_t)stream;
+    const uint32_t nn = prog->num_nodes, nr = prog->num_roots;
+    const uint32_t nbs = prog->num_base_slots, nes = prog->num_ext_slots;
+    // Validate the blob on the host: every slot, table index, column and frame
+    // offset must be in range, so the walk never reads out of bounds.
+    for (uint32_t i = 0; i < nn; ++i) {
+        const uint32_t* nd = prog->nodes + 4 * i;
+        const uint32_t op = nd[0], slot = nd[3] & RES_SLOT_MASK;
+        const bool rx = (nd[3] & RES_EXT_BIT) != 0;
+        SG_CHECK_ARG(op <= OP_EMBED, "unknown op tag");
+        SG_CHECK_ARG(rx ? slot < nes : slot < nbs, "result slot out of range");
+        auto ok_operand = [&](uint32_t enc) {
+            const uint32_t k = enc >> OPK_SHIFT, p = enc & OPK_PAYLOAD_MASK;
+            switch (k) {
+                case OPK_BASE_SLOT: return p < nbs;
+                case OPK_EXT_SLOT: return p < nes;
+                case OPK_BASE_CONST: return p < prog->num_base_consts;
+                case OPK_EXT_CONST: return p < prog->num_ext_consts;
+                case OPK_RAP: return p < n_rap;
+                case OPK_ALPHA: return p < n_alpha;
+                case OPK_OFFSET: return true;
+                default: return false;
+            }
+        };
+        if (op >= OP_ADD && op <= OP_MUL) SG_CHECK_ARG(ok_operand(nd[1]) && ok_operand(nd[2]), "operand out of range");
+        if (op == OP_NEG || op == OP_EMBED) SG_CHECK_ARG(ok_operand(nd[1]), "operand out of range");
+        if (op == OP_VAR) {
+            const uint32_t col = nd[1] & 0xFFFFu, off = (nd[2] >> 8) & 0xFFu;
+            const bool main = ((nd[2] >> 16) & 1u) != 0;
+            SG_CHECK_ARG(main ? col < m : col < a, "trace column out of range");
+            SG_CHECK_ARG((uint64_t)off * next_step < rows, "frame offset wraps more than once");
+        }
+        if (op == OP_CONST_BASE) SG_CHECK_ARG(nd[1] < prog->num_base_consts, "constant index");
+        if (op == OP_CONST_EXT) SG_CHECK_ARG(nd[1] < prog->num_ext_consts, "constant index");
+        if (op == OP_RAP_CHALLENGE) SG_CHECK_ARG(nd[1] < n_rap, "challenge index");
+        if (op == OP_ALPHA_POW) SG_CHECK_ARG(nd[1] < n_alpha, "alpha index");
+    }
+    for (uint32_t r = 0; r < nr; ++r) {
+        const uint32_t e = prog->roots[r];
+        SG_CHECK_ARG((e & RES_EXT_BIT) ? (e & RES_SLOT_MASK) < nes : (e & RES_SLOT_MASK) < nbs, "root slot");
+    }
+    if (comp) {
+        SG_CHECK_ARG(comp->z_len >= 1 && comp->d_z_inv && comp->beta_trans, "composition inputs");
+        for (uint32_t b = 0; b < comp->num_boundary; ++b)
+            SG_CHECK_ARG(comp->b_is_aux[b] ? comp->b_col[b] < a : comp->b_col[b] < m, "boundary column");
+    }
+    // One device blob: nodes | roots | base consts | ext consts | rap | alpha | comp arrays.
+    std::vector<uint64_t> blob;
+    auto put = [&](const void* p, size_t bytes) {
+        const size_t off = blob.size();
+        blob.resize(off + (bytes + 7) / 8 + 1, 0);
+        if (bytes) memcpy(blob.data() + off, p, bytes);
+        return off;
+    };
+    const size_t o_nodes = put(prog->nodes, 16ull * nn);
+    const size_t o_roots = put(prog->roots, 4ull * nr);
+    const size_t o_bc = put(prog->base_consts, 8ull * prog->num_base_consts);
+    const size_t o_ec = put(prog->ext_consts, 24ull * prog->num_ext_consts);
+    const size_t o_rap = put(rap, 24ull * n_rap);
+    const size_t o_al = put(alpha, 24ull * n_alpha);
+    size_t o_beta = 0, o_bcol = 0, o_baux = 0, o_bval = 0, o_bbeta = 0;
+    const uint32_t nb = comp ? comp->num_boundary : 0;
+    if (comp) {
+        o_beta = put(comp->beta_trans, 24ull * nr);
+        o_bcol = put(comp->b_col, 8ull * nb);
+        o_baux = put(comp->b_is_aux, 8ull * nb);
+        o_bval = put(comp->b_value, 24ull * nb);
+        o_bbeta = put(comp->b_beta, 24ull * nb);
+    }
+    // Shared-memory slot file when it fits (>= 32 threads per CTA), else global.
+    const uint64_t per_thread = (uint64_t)nbs + 3ull * nes;
+    int T = 128;
+    while (T > 32 && per_thread * T * 8 > 160 * 1024) T -= 32;
+    const bool use_smem = per_thread * T * 8 <= 160 * 1024;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    uint64_t blocks = (rows + T - 1) / T;
+    const uint64_t max_blocks = (uint64_t)sms * 16;
+    if (blocks > max_blocks) blocks = max_blocks;
+    uint64_t* d_blob = nullptr;
+    uint64_t* d_scr = nullptr;
+    const uint64_t bb = 8 * blob.size();
+    const uint64_t sb = use_smem ? 0 : per_thread * blocks * T * 8;
+    SG_TRY(dev_alloc(ctx, st, bb, (void**)&d_blob));
+    int rc = SG_OK;
+    if (!use_smem) rc = dev_alloc(ctx, st, sb, (void**)&d_scr);
+    if (rc == SG_OK && cudaMemcpyAsync(d_blob, blob.data(), bb, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+        set_error("constraints: program upload failed");
+        rc = SG_ERR_CUDA;
+    }
+    if (rc == SG_OK) {
+        Uni u{d_blob + o_bc, d_blob + o_ec, d_blob + o_rap, d_blob + o_al,
+              fe3{table_offset[0], table_offset[1], table_offset[2]}};
+        Trace t{d_main, m, d_aux, a, rows, next_step};
+        Comp cp{};
+        if (comp) {
+            cp = Comp{d_blob + o_beta, comp->d_z_inv, comp->z_len, nb, d_blob + o_bcol, d_blob + o_baux,
+                      d_blob + o_bval, d_blob + o_bbeta, comp->d_b_z_inv};
+        }
+        const size_t smem = use_smem ? per_thread * T * 8 : 0;
+        if (smem > 48 * 1024) cudaFuncSetAttribute(k_constraints, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_constraints<<<(unsigned)blocks, T, smem, st>>>((const uint4*)(d_blob + o_nodes), nn,
+                                                         (const uint32_t*)(d_blob + o_roots), nr, nbs, nes, u, t, cp,
+                                                         comp ? 0 : 1, d_out, use_smem ? nullptr : d_scr);
+        rc = check_launch(ctx, "k_constraints");
+        if (rc == SG_OK && cudaStreamSynchronize(st) != cudaSuccess) {
+            set_error("constraints: execution failed");
+            rc = SG_ERR_CUDA;
+        }
+    }
+    if (d_scr) dev_free(ctx, st, d_scr, sb);
+    dev_free(ctx, st, d_blob, bb);
+    return rc;
+}
+
+int sg_decompose_d2(sg_ctx* c, void* stream, const uint64_t* d_h, uint64_t lde_rows, const uint64_t* d_inv_2x,
+                    uint64_t* d_out) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(c);
+    SG_CHECK_ARG(ctx, "null context");
+    SG_CHECK_ARG(lde_rows % 2 == 0, "even LDE size required");
+    const uint64_t n = lde_rows / 2;
+    if (n == 0) return SG_OK;
+    const uint64_t two_inv = (GL_P + 1) / 2;
+    k_decompose_d2<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(d_h, d_inv_2x, two_inv, n, d_out);
+    return check_launch(ctx, "k_decompose_d2");
+}
+
+}  // extern "C"

@@ -1,0 +1,708 @@
+// Round 2-4 kernels of the STARK prover for sm_100a: batch inversion and
+// inverse denominators, barycentric OOD sums, DEEP composition, FRI folding
+// with the next layer's leaves fused in, LogUp auxiliary columns, row gathers.
+//
+// Reference behaviour (CPU semantics the kernels reproduce):
+//  * inversion:   FieldElement::inplace_batch_inverse; denominators per
+//                 crypto/math-cuda/src/inverse.rs:226-300 (DenomSign).
+//  * barycentric: polynomial.rs:207-235 inner sum; barycentric.cu:210-323.
+//  * DEEP:        prover.rs:2400-2608 / deep.cu:30-115.
+//  * FRI:         fri/fri_functions.rs:15-61, FRI leaves keccak.cu:384.
+//  * LogUp:       lookup.rs:1660-1842 with the CSR descriptor of
+//                 crypto/math-cuda/src/logup.rs:26-44.
+// All layouts are row-major; ext3 values are 3 consecutive u64.
+#include <vector>
+
+#include "common.cuh"
+#include "gl.cuh"
+#include "keccak.cuh"
+
+namespace sg {
+
+using gl::fe3;
+
+__device__ __forceinline__ fe3 ld3(const uint64_t* p) { return fe3{p[0], p[1], p[2]}; }
+__device__ __forceinline__ void st3(uint64_t* p, fe3 v) {
+    p[0] = v.c0;
+    p[1] = v.c1;
+    p[2] = v.c2;
+}
+__device__ __forceinline__ fe3 one3() { return fe3{1, 0, 0}; }
+__device__ __forceinline__ fe3 zero3() { return fe3{0, 0, 0}; }
+__device__ __forceinline__ fe3 shfl_up3(fe3 v, int d) {
+    return fe3{__shfl_up_sync(0xffffffffu, v.c0, d), __shfl_up_sync(0xffffffffu, v.c1, d),
+               __shfl_up_sync(0xffffffffu, v.c2, d)};
+}
+__device__ __forceinline__ fe3 shfl_down3(fe3 v, int d) {
+    return fe3{__shfl_down_sync(0xffffffffu, v.c0, d), __shfl_down_sync(0xffffffffu, v.c1, d),
+               __shfl_down_sync(0xffffffffu, v.c2, d)};
+}
+__device__ __forceinline__ fe3 shfl3(fe3 v, int src) {
+    return fe3{__shfl_sync(0xffffffffu, v.c0, src), __shfl_sync(0xffffffffu, v.c1, src),
+               __shfl_sync(0xffffffffu, v.c2, src)};
+}
+__device__ __forceinline__ bool is_zero3(fe3 v) {
+    return gl::canon(v.c0) == 0 && gl::canon(v.c1) == 0 && gl::canon(v.c2) == 0;
+}
+
+// ---------------------------------------------------------------- batch inversion
+// Montgomery's trick in one pass: each thread owns BI_CH consecutive elements,
+// a warp prefix/suffix scan of the thread products gives every thread the
+// inverse of its own product from ONE Fp3 inversion per warp (lane 0), and the
+// thread then unwinds its chunk. No global scan, no second pass.
+#define BI_CH 4
+
+struct LoadPlain {
+    const uint64_t* in;
+    __device__ __forceinline__ fe3 operator()(uint64_t idx) const { return ld3(in + 3 * idx); }
+};
+// Denominators z_k - x_i (sign 0) or x_i - z_k (sign 1), element idx = k*n + i.
+struct LoadDenom {
+    const uint64_t* x;
+    const uint64_t* z;
+    uint64_t n;
+    int x_minus_z;
+    __device__ __forceinline__ fe3 operator()(uint64_t idx) const {
+        const uint64_t k = idx / n, i = idx - k * n;
+        const fe3 zk = ld3(z + 3 * k);
+        const uint64_t xi = x[i];
+        return x_minus_z ? fe3{gl::sub(xi, zk.c0), gl::neg(zk.c1), gl::neg(zk.c2)}
+                         : fe3{gl::sub(zk.c0, xi), zk.c1, zk.c2};
+    }
+};
+
+template <class Load>
+__global__ void __launch_bounds__(256) k_batch_inv(Load load, uint64_t total, uint64_t* out, unsigned* zero_flag) {
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t base = tid * BI_CH;
+    const int lane = threadIdx.x & 31;
+    fe3 a[BI_CH], p[BI_CH];
+#pragma unroll
+    for (int i = 0; i < BI_CH; ++i) a[i] = base + i < total ? load(base + i) : one3();
+    p[0] = a[0];
+#pragma unroll
+    for (int i = 1; i < BI_CH; ++i) p[i] = gl::mul3(p[i - 1], a[i]);
+    const fe3 tot = p[BI_CH - 1];
+    fe3 incl = tot, sinc = tot;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const fe3 v = shfl_up3(incl, off);
+        if (lane >= off) incl = gl::mul3(v, incl);
+        const fe3 w = shfl_down3(sinc, off);
+        if (lane + off < 32) sinc = gl::mul3(sinc, w);
+    }
+    fe3 excl = shfl_up3(incl, 1);
+    if (lane == 0) excl = one3();
+    fe3 sexcl = shfl_down3(sinc, 1);
+    if (lane == 31) sexcl = one3();
+    const fe3 T = shfl3(incl, 31);
+    fe3 Tinv = zero3();
+    if (lane == 0) {
+        if (is_zero3(T)) atomicOr(zero_flag, 1u);
+        Tinv = gl::inv3(T);
+    }
+    Tinv = shfl3(Tinv, 0);
+    // (excl * tot)^-1 = T^-1 * sexcl ; tot^-1 = that * excl
+    fe3 inv = gl::mul3(gl::mul3(Tinv, sexcl), excl);
+#pragma unroll
+    for (int i = BI_CH - 1; i >= 1; --i) {
+        const fe3 r = gl::mul3(inv, p[i - 1]);
+        if (base + i < total) st3(out + 3 * (base + i), gl::canon3(r));
+        inv = gl::mul3(inv, a[i]);
+    }
+    if (base < total) st3(out + 3 * base, gl::canon3(inv));
+}
+
+template <class Load>
+static int batch_inv_launch(Ctx* ctx, cudaStream_t st, Load load, uint64_t total, uint64_t* out, int* zero_out) {
+    if (total == 0) return SG_OK;
+    unsigned* d_flag = nullptr;
+    SG_TRY(dev_alloc(ctx, st, sizeof(unsigned), (void**)&d_flag));
+    int rc = SG_OK;
+    if (cudaMemsetAsync(d_flag, 0, sizeof(unsigned), st) != cudaSuccess) {
+        set_error("batch inverse: flag reset failed");
+        rc = SG_ERR_CUDA;
+    }
+    if (rc == SG_OK) {
+        const uint64_t threads = (total + BI_CH - 1) / BI_CH;
+        k_batch_inv<Load><<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(load, total, out, d_flag);
+        rc = check_launch(ctx, "k_batch_inv");
+    }
+    if (rc == SG_OK && zero_out) {
+        unsigned h = 0;
+        if (cudaMemcpyAsync(&h, d_flag, sizeof(unsigned), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) {
+            set_error("batch inverse: flag readback failed");
+            rc = SG_ERR_CUDA;
+        }
+        *zero_out = h ? 1 : 0;
+    }
+    int rf = dev_free(ctx, st, d_flag, sizeof(unsigned));
+    return rc != SG_OK ? rc : rf;
+}
+
+// ---------------------------------------------------------------- barycentric sums
+// out_partial[(chunk * K + k) * cols + c] = sum over the chunk's rows i of
+//   points[i] * col_c(row i*stride) * inv_denoms[k][i]
+#define BARY_MAX_K 8
+template <bool EXT3>
+__global__ void __launch_bounds__(128) k_bary(const uint64_t* data, uint64_t row_u64, uint64_t stride, uint64_t cols,
+                                              const uint64_t* points, const uint64_t* invd, uint64_t n, uint32_t K,
+                                              uint64_t chunk_len, uint64_t* partial) {
+    const uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t chunk = blockIdx.y;
+    if (c >= cols) return;
+    fe3 acc[BARY_MAX_K];
+#pragma unroll
+    for (int k = 0; k < BARY_MAX_K; ++k) acc[k] = zero3();
+    const uint64_t i0 = chunk * chunk_len, i1 = min(n, i0 + chunk_len);
+    for (uint64_t i = i0; i < i1; ++i) {
+        const uint64_t* row = data + i * stride * row_u64;
+        const uint64_t pt = __ldg(points + i);
+        fe3 pe;
+        if (EXT3) {
+            pe = gl::mulb3(ld3(row + 3 * c), pt);
+        } else {
+            pe = fe3{gl::mul(row[c], pt), 0, 0};
+        }
+#pragma unroll
+        for (int k = 0; k < BARY_MAX_K; ++k) {
+            if (k < (int)K) {
+                const fe3 d = fe3{__ldg(invd + 3 * (k * n + i)), __ldg(invd + 3 * (k * n + i) + 1),
+                                  __ldg(invd + 3 * (k * n + i) + 2)};
+                acc[k] = gl::add3(acc[k], EXT3 ? gl::mul3(pe, d) : gl::mulb3(d, pe.c0));
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < BARY_MAX_K; ++k)
+        if (k < (int)K) st3(partial + 3 * ((chunk * K + k) * cols + c), acc[k]);
+}
+
+__global__ void k_bary_combine(const uint64_t* partial, uint64_t chunks, uint64_t per_chunk, uint64_t* out) {
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= per_chunk) return;
+    fe3 s = zero3();
+    for (uint64_t ch = 0; ch < chunks; ++ch) s = gl::add3(s, ld3(partial + 3 * (ch * per_chunk + t)));
+    st3(out + 3 * t, gl::canon3(s));
+}
+
+// ---------------------------------------------------------------- DEEP
+// One warp per LDE row: lanes split the row's columns, so every load is a
+// coalesced row segment; per-lane partial sums are warp-reduced.
+//   result = inv_h * (sum_j g_j H_j(x) - c_h)
+//          + sum_k inv_t[k] * (sum_j g'_{jk} t_j(x) - c_k)
+// with c_h = sum_j g_j H_j(z^P) and c_k = sum_j g'_{jk} t_j(z w^k) folded on
+// the host: the same field value as summing g (t - t_ood) term by term.
+#define DEEP_MAX_K 8
+__global__ void __launch_bounds__(256) k_deep(const uint64_t* main, uint64_t m, const uint64_t* aux, uint64_t A,
+                                              const uint64_t* parts, uint64_t P, uint64_t rows, uint32_t log_rows,
+                                              const uint64_t* gam_h, const uint64_t* gam_tr, uint32_t K,
+                                              const uint64_t* consts, const uint64_t* inv_h, const uint64_t* inv_t,
+                                              int bitrev_out, uint64_t* out) {
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= rows) return;
+    const uint64_t i = warp;
+    fe3 sk[DEEP_MAX_K];
+#pragma unroll
+    for (int k = 0; k < DEEP_MAX_K; ++k) sk[k] = zero3();
+    fe3 sh = zero3();
+    const uint64_t* mrow = main + i * m;
+    for (uint64_t j = lane; j < m; j += 32) {
+        const uint64_t t = mrow[j];
+#pragma unroll
+        for (int k = 0; k < DEEP_MAX_K; ++k)
+            if (k < (int)K) sk[k] = gl::add3(sk[k], gl::mulb3(ld3(gam_tr + 3 * (j * K + k)), t));
+    }
+    const uint64_t* arow = aux + i * A * 3;
+    for (uint64_t j = lane; j < A; j += 32) {
+        const fe3 t = ld3(arow + 3 * j);
+#pragma unroll
+        for (int k = 0; k < DEEP_MAX_K; ++k)
+            if (k < (int)K) sk[k] = gl::add3(sk[k], gl::mul3(ld3(gam_tr + 3 * ((m + j) * K + k)), t));
+    }
+    const uint64_t* prow = parts + i * P * 3;
+    for (uint64_t j = lane; j < P; j += 32) sh = gl::add3(sh, gl::mul3(ld3(gam_h + 3 * j), ld3(prow + 3 * j)));
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) {
+        sh = gl::add3(sh, shfl_down3(sh, off));
+#pragma unroll
+        for (int k = 0; k < DEEP_MAX_K; ++k)
+            if (k < (int)K) sk[k] = gl::add3(sk[k], shfl_down3(sk[k], off));
+    }
+    if (lane == 0) {
+        fe3 r = gl::mul3(ld3(inv_h + 3 * i), gl::sub3(sh, ld3(consts)));
+#pragma unroll
+        for (int k = 0; k < DEEP_MAX_K; ++k)
+            if (k < (int)K)
+                r = gl::add3(r, gl::mul3(ld3(inv_t + 3 * (k * rows + i)), gl::sub3(sk[k], ld3(consts + 3 * (1 + k)))));
+        const uint64_t o = bitrev_out ? (log_rows ? (__brevll(i) >> (64 - log_rows)) : 0) : i;
+        st3(out + 3 * o, gl::canon3(r));
+    }
+}
+
+// ---------------------------------------------------------------- FRI
+// Fold one layer (evaluations in bit-reversed order, pairs (2j, 2j+1) are
+// x_j and -x_j) and, fused in the same pass, hash the folded layer's leaf
+// pairs and derive the next layer's inverse twiddles tw'[j] = tw[2j]^2.
+// Each thread produces folded outputs 2t and 2t+1, i.e. exactly leaf t.
+__device__ __forceinline__ fe3 fold_one(const uint64_t* in, uint64_t j, uint64_t tw, fe3 zeta) {
+    const fe3 lo = ld3(in + 6 * j), hi = ld3(in + 6 * j + 3);
+    return gl::add3(gl::add3(lo, hi), gl::mulb3(gl::mul3(zeta, gl::sub3(lo, hi)), tw));
+}
+
+__global__ void __launch_bounds__(128) k_fri_fold(const uint64_t* in, uint64_t h, const uint64_t* tw, uint64_t z0,
+                                                  uint64_t z1, uint64_t z2, uint64_t* out, uint64_t* tw_next,
+                                                  uint64_t* leaves) {
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const fe3 zeta{z0, z1, z2};
+    if (2 * t >= h) return;
+    const uint64_t tw0 = tw[2 * t];
+    const fe3 a = gl::canon3(fold_one(in, 2 * t, tw0, zeta));
+    st3(out + 6 * t, a);
+    if (2 * t + 1 < h) {
+        const fe3 b = gl::canon3(fold_one(in, 2 * t + 1, tw[2 * t + 1], zeta));
+        st3(out + 6 * t + 3, b);
+        if (tw_next) tw_next[t] = gl::canon(gl::sqr(tw0));
+        if (leaves) {
+            // Keccak-256 of 48 bytes: 6 big-endian lanes, pad at lane 6.
+            uint64_t s[25];
+#pragma unroll
+            for (int q = 0; q < 25; ++q) s[q] = 0;
+            s[0] = kc::bswap64(a.c0);
+            s[1] = kc::bswap64(a.c1);
+            s[2] = kc::bswap64(a.c2);
+            s[3] = kc::bswap64(b.c0);
+            s[4] = kc::bswap64(b.c1);
+            s[5] = kc::bswap64(b.c2);
+            s[6] = 0x01ULL;
+            s[16] = 0x8000000000000000ULL;
+            kc::permute(s);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) leaves[4 * t + q] = s[q];
+        }
+    }
+}
+
+// Leaves of an already-folded layer (pairs of consecutive ext3 values).
+__global__ void __launch_bounds__(128) k_fri_leaves(const uint64_t* ev, uint64_t nleaves, uint64_t* leaves) {
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nleaves) return;
+    uint64_t s[25];
+#pragma unroll
+    for (int q = 0; q < 25; ++q) s[q] = 0;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) s[q] = kc::bswap64(gl::canon(ev[6 * t + q]));
+    s[6] = 0x01ULL;
+    s[16] = 0x8000000000000000ULL;
+    kc::permute(s);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) leaves[4 * t + q] = s[q];
+}
+
+// ---------------------------------------------------------------- gathers
+// out[q * width + c] = data[rows[q] * row_u64 + col0 + c] for c < width.
+__global__ void k_gather_rows(const uint64_t* data, uint64_t row_u64, uint64_t nrows, uint64_t col0, uint64_t width,
+                              const uint32_t* rows, uint32_t nq, uint64_t* out) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= (uint64_t)nq * width) return;
+    const uint64_t q = g / width, c = g - q * width;
+    const uint64_t r = rows[q];
+    out[g] = r < nrows ? data[r * row_u64 + col0 + c] : 0;
+}
+
+// ---------------------------------------------------------------- LogUp
+// fingerprints fp[k*n + r] = z - (bus_id_k + sum_e alpha^{ai_e} (c_e + sum_t coef_t main[r][col_t]))
+struct LogupDesc {
+    uint32_t K;
+    const uint64_t* bus_ids;
+    const uint32_t* elem_off;
+    const uint32_t* elem_alpha;
+    const uint64_t* elem_const;
+    const uint32_t* term_off;
+    const uint64_t* term_coef;
+    const uint32_t* term_col;
+    uint32_t n_out;
+    const uint32_t* out_off;
+    const uint32_t* out_int;
+    const uint64_t* mult_const;
+    const uint32_t* mterm_off;
+    const uint64_t* mterm_coef;
+    const uint32_t* mterm_col;
+    uint32_t n_committed;
+    const uint64_t* alpha_pows;
+};
+
+__global__ void k_logup_fp(const uint64_t* main, uint64_t n, uint64_t m, LogupDesc d, uint64_t z0, uint64_t z1,
+                           uint64_t z2, uint64_t* fp) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= (uint64_t)d.K * n) return;
+    const uint32_t k = (uint32_t)(g / n);
+    const uint64_t r = g - (uint64_t)k * n;
+    const uint64_t* row = main + r * m;
+    fe3 lc{d.bus_ids[k], 0, 0};
+    for (uint32_t e = d.elem_off[k]; e < d.elem_off[k + 1]; ++e) {
+        uint64_t base = d.elem_const[e];
+        for (uint32_t t = d.term_off[e]; t < d.term_off[e + 1]; ++t)
+            base = gl::add(base, gl::mul(d.term_coef[t], row[d.term_col[t]]));
+        lc = gl::add3(lc, gl::mulb3(ld3(d.alpha_pows + 3 * d.elem_alpha[e]), base));
+    }
+    st3(fp + 3 * g, gl::sub3(fe3{z0, z1, z2}, lc));
+}
+
+// Terms per row: committed columns go to aux[r][c]; row sums to rsum[r].
+__global__ void k_logup_terms(const uint64_t* main, uint64_t n, uint64_t m, LogupDesc d, const uint64_t* recip,
+                              uint64_t* aux, uint64_t* rsum) {
+    const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const uint64_t* row = main + r * m;
+    const uint64_t W = (uint64_t)d.n_committed + 1;
+    fe3 s = zero3();
+    for (uint32_t c = 0; c < d.n_out; ++c) {
+        fe3 term = zero3();
+        for (uint32_t ki = d.out_off[c]; ki < d.out_off[c + 1]; ++ki) {
+            const uint32_t k = d.out_int[ki];
+            uint64_t mu = d.mult_const[k];
+            for (uint32_t t = d.mterm_off[k]; t < d.mterm_off[k + 1]; ++t)
+                mu = gl::add(mu, gl::mul(d.mterm_coef[t], row[d.mterm_col[t]]));
+            term = gl::add3(term, gl::mulb3(ld3(recip + 3 * ((uint64_t)k * n + r)), mu));
+        }
+        if (c < d.n_committed) st3(aux + 3 * (r * W + c), gl::canon3(term));
+        s = gl::add3(s, term);
+    }
+    st3(rsum + 3 * r, s);
+}
+
+// Segment sums of rsum over SEG rows.
+#define LG_SEG 1024
+__global__ void __launch_bounds__(256) k_seg_sum(const uint64_t* rsum, uint64_t n, uint64_t* seg) {
+    __shared__ uint64_t sh[3 * 8];
+    const uint64_t s0 = (uint64_t)blockIdx.x * LG_SEG;
+    fe3 acc = zero3();
+    for (uint64_t r = s0 + threadIdx.x; r < min(n, s0 + LG_SEG); r += blockDim.x) acc = gl::add3(acc, ld3(rsum + 3 * r));
+    for (int off = 16; off >= 1; off >>= 1) acc = gl::add3(acc, shfl_down3(acc, off));
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) st3(sh + 3 * w, acc);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        fe3 t = zero3();
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t = gl::add3(t, ld3(sh + 3 * q));
+        st3(seg + 3 * blockIdx.x, t);
+    }
+}
+
+// Exclusive prefix of the segment sums, total L and offset L/n (one thread:
+// at most n/1024 segments).
+__global__ void k_seg_scan(uint64_t* seg, uint64_t nseg, uint64_t ninv, uint64_t* L_off) {
+    if (threadIdx.x || blockIdx.x) return;
+    fe3 run = zero3();
+    for (uint64_t s = 0; s < nseg; ++s) {
+        const fe3 v = ld3(seg + 3 * s);
+        st3(seg + 3 * s, run);
+        run = gl::add3(run, v);
+    }
+    st3(L_off, gl::canon3(run));
+    st3(L_off + 3, gl::mulb3(run, ninv));
+}
+
+// acc[r] = (sum_{r' < r} rsum[r']) - r * (L / n), written to aux column W-1.
+__global__ void __launch_bounds__(1024) k_logup_acc(const uint64_t* rsum, uint64_t n, const uint64_t* seg,
+                                                    const uint64_t* L_off, uint64_t W, uint64_t* aux) {
+    __shared__ uint64_t wsum[3 * 32];
+    const uint64_t r = (uint64_t)blockIdx.x * LG_SEG + threadIdx.x;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    fe3 v = r < n ? ld3(rsum + 3 * r) : zero3();
+    fe3 incl = v;
+    for (int off = 1; off < 32; off <<= 1) {
+        const fe3 u = shfl_up3(incl, off);
+        if (lane >= off) incl = gl::add3(incl, u);
+    }
+    if (lane == 31) st3(wsum + 3 * w, incl);
+    __syncthreads();
+    if (w == 0) {
+        fe3 x = ld3(wsum + 3 * lane);
+        fe3 xi = x;
+        for (int off = 1; off < 32; off <<= 1) {
+            const fe3 u = shfl_up3(xi, off);
+            if (lane >= off) xi = gl::add3(xi, u);
+        }
+        st3(wsum + 3 * lane, gl::sub3(xi, x));  // exclusive warp prefix
+    }
+    __syncthreads();
+    if (r >= n) return;
+    const fe3 excl = gl::add3(gl::add3(ld3(seg + 3 * blockIdx.x), ld3(wsum + 3 * w)), gl::sub3(incl, v));
+    const fe3 off = ld3(L_off + 3);
+    st3(aux + 3 * (r * W + (W - 1)), gl::canon3(gl::sub3(excl, gl::mulb3(off, r % GL_P))));
+}
+
+}  // namespace sg
+
+using namespace sg;
+
+static Ctx* CX(sg_ctx* c) { return reinterpret_cast<Ctx*>(c); }
+
+extern "C" {
+
+int sg_batch_inverse_ext3(sg_ctx* c, void* stream, const uint64_t* d_in, uint64_t n, uint64_t* d_out,
+                          int* zero_found) {
+    SG_CHECK_ARG(c && (n == 0 || (d_in && d_out)), "null argument");
+    return batch_inv_launch(CX(c), (cudaStream_t)stream, LoadPlain{d_in}, n, d_out, zero_found);
+}
+
+int sg_inv_denoms_ext3(sg_ctx* c, void* stream, const uint64_t* d_x, uint64_t n, const uint64_t* z_host, uint32_t k,
+                       int x_minus_z, uint64_t* d_out, int* zero_found) {
+    SG_CHECK_ARG(c && z_host && (n == 0 || (d_x && d_out)), "null argument");
+    Ctx* ctx = CX(c);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (n == 0 || k == 0) return SG_OK;
+    uint64_t* d_z = nullptr;
+    SG_TRY(dev_alloc(ctx, st, 24ull * k, (void**)&d_z));
+    int rc = SG_OK;
+    if (cudaMemcpyAsync(d_z, z_host, 24ull * k, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+        set_error("inv_denoms: z upload failed");
+        rc = SG_ERR_CUDA;
+    }
+    if (rc == SG_OK) rc = batch_inv_launch(ctx, st, LoadDenom{d_x, d_z, n, x_minus_z}, n * k, d_out, zero_found);
+    int rf = dev_free(ctx, st, d_z, 24ull * k);
+    return rc != SG_OK ? rc : rf;
+}
+
+int sg_barycentric_sums(sg_ctx* c, void* stream, const uint64_t* d_data, uint64_t row_u64, uint64_t row_stride,
+                        int ext3, uint64_t cols, const uint64_t* d_points, const uint64_t* d_inv_denoms, uint64_t n,
+                        uint32_t k, uint64_t* d_out) {
+    SG_CHECK_ARG(c, "null context");
+    SG_CHECK_ARG(k >= 1 && k <= BARY_MAX_K, "1 <= k <= 8 evaluation points");
+    SG_CHECK_ARG(cols * (ext3 ? 3 : 1) <= row_u64, "columns exceed the row width");
+    Ctx* ctx = CX(c);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (cols == 0) return SG_OK;
+    if (n == 0) {
+        SG_CUDA(cudaMemsetAsync(d_out, 0, 24ull * k * cols, st));
+        return SG_OK;
+    }
+    const uint64_t ctiles = (cols + 127) / 128;
+    uint64_t chunks = (148 * 8 + ctiles - 1) / ctiles;
+    if (chunks > n) chunks = n;
+    if (chunks > 65535) chunks = 65535;
+    const uint64_t chunk_len = (n + chunks - 1) / chunks;
+    chunks = (n + chunk_len - 1) / chunk_len;
+    uint64_t* part = nullptr;
+    SG_TRY(dev_alloc(ctx, st, 24ull * chunks * k * cols, (void**)&part));
+    dim3 grid((unsigned)ctiles, (unsigned)chunks);
+    if (ext3)
+        k_bary<true><<<grid, 128, 0, st>>>(d_data, row_u64, row_stride, cols, d_points, d_inv_denoms, n, k, chunk_len,
+                                           part);
+    else
+        k_bary<false><<<grid, 128, 0, st>>>(d_data, row_u64, row_stride, cols, d_points, d_inv_denoms, n, k, chunk_len,
+                                            part);
+    int rc = check_launch(ctx, "k_bary");
+    if (rc == SG_OK) {
+        const uint64_t per = (uint64_t)k * cols;
+        k_bary_combine<<<(unsigned)((per + 255) / 256), 256, 0, st>>>(part, chunks, per, d_out);
+        rc = check_launch(ctx, "k_bary_combine");
+    }
+    int rf = dev_free(ctx, st, part, 24ull * chunks * k * cols);
+    return rc != SG_OK ? rc : rf;
+}
+
+int sg_deep_composition(sg_ctx* c, void* stream, const uint64_t* d_main, uint64_t m, const uint64_t* d_aux,
+                        uint64_t a, const uint64_t* d_parts, uint64_t p, uint64_t rows, const uint64_t* h_ood,
+                        const uint64_t* trace_ood, const uint64_t* gammas_h, const uint64_t* gammas_tr, uint32_t k,
+                        const uint64_t* d_inv_h, const uint64_t* d_inv_t, int bitrev_out, uint64_t* d_out) {
+    SG_CHECK_ARG(c && h_ood && trace_ood && gammas_h && gammas_tr, "null argument");
+    SG_CHECK_ARG(k <= DEEP_MAX_K, "at most 8 evaluation points");
+    const int lr = log2_exact(rows);
+    SG_CHECK_ARG(!bitrev_out || lr >= 0, "bit-reversed output needs a power-of-two row count");
+    Ctx* ctx = CX(c);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (rows == 0) return SG_OK;
+    // Host side: fold the OOD terms into constants c_h, c_k (field identities).
+    const uint64_t ng_h = 3 * p, ng_t = 3 * (m + a) * k;
+    auto mulc = [](const uint64_t* x, const uint64_t* y, uint64_t* o) { sg_host_fp3_mul(x, y, o); };
+    uint64_t ch[3] = {0, 0, 0};
+    for (uint64_t j = 0; j < p; ++j) {
+        uint64_t t[3];
+        mulc(gammas_h + 3 * j, h_ood + 3 * j, t);
+        sg_host_fp3_add(ch, t, ch);
+    }
+    std::vector<uint64_t> consts(3 * (1 + k), 0);
+    consts[0] = ch[0];
+    consts[1] = ch[1];
+    consts[2] = ch[2];
+    for (uint32_t kk = 0; kk < k; ++kk) {
+        uint64_t acc[3] = {0, 0, 0};
+        for (uint64_t j = 0; j < m + a; ++j) {
+            uint64_t t[3];
+            mulc(gammas_tr + 3 * (j * k + kk), trace_ood + 3 * (j * k + kk), t);
+            sg_host_fp3_add(acc, t, acc);
+        }
+        consts[3 * (1 + kk)] = acc[0];
+        consts[3 * (1 + kk) + 1] = acc[1];
+        consts[3 * (1 + kk) + 2] = acc[2];
+    }
+    uint64_t* d_g = nullptr;
+    const uint64_t gbytes = 8 * (ng_h + ng_t + consts.size());
+    SG_TRY(dev_alloc(ctx, st, gbytes, (void**)&d_g));
+    int rc = SG_OK;
+    if (cudaMemcpyAsync(d_g, gammas_h, 8 * ng_h, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(d_g + ng_h, gammas_tr, 8 * ng_t, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(d_g + ng_h + ng_t, consts.data(), 8 * consts.size(), cudaMemcpyHostToDevice, st) != cudaSuccess) {
+        set_error("deep: coefficient upload failed");
+        rc = SG_ERR_CUDA;
+    }
+    if (rc == SG_OK) {
+        const uint64_t threads = rows * 32;
+        k_deep<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(d_main, m, d_aux, a, d_parts, p, rows,
+                                                                  lr < 0 ? 0 : (uint32_t)lr, d_g, d_g + ng_h, k,
+                                                                  d_g + ng_h + ng_t, d_inv_h, d_inv_t, bitrev_out,
+                                                                  d_out);
+        rc = check_launch(ctx, "k_deep");
+        // keep host vectors alive until the copies have been consumed
+        if (rc == SG_OK && cudaStreamSynchronize(st) != cudaSuccess) {
+            set_error("deep: sync failed");
+            rc = SG_ERR_CUDA;
+        }
+    }
+    int rf = dev_free(ctx, st, d_g, gbytes);
+    return rc != SG_OK ? rc : rf;
+}
+
+int sg_fri_fold_layer(sg_ctx* c, void* stream, const uint64_t* d_in, uint64_t h, const uint64_t* d_inv_tw,
+                      const uint64_t zeta[3], uint64_t* d_out, uint64_t* d_inv_tw_next, uint8_t* d_leaves) {
+    SG_CHECK_ARG(c && zeta, "null argument");
+    SG_CHECK_ARG(!d_leaves || (h % 2 == 0), "leaves need an even folded length");
+    if (h == 0) return SG_OK;
+    const uint64_t threads = (h + 1) / 2;
+    k_fri_fold<<<(unsigned)((threads + 127) / 128), 128, 0, (cudaStream_t)stream>>>(
+        d_in, h, d_inv_tw, zeta[0], zeta[1], zeta[2], d_out, d_inv_tw_next, (uint64_t*)d_leaves);
+    return check_launch(CX(c), "k_fri_fold");
+}
+
+int sg_fri_leaves(sg_ctx* c, void* stream, const uint64_t* d_evals, uint64_t n, uint8_t* d_leaves) {
+    SG_CHECK_ARG(c, "null context");
+    SG_CHECK_ARG(n % 2 == 0, "FRI leaves hash pairs: even length required");
+    if (n == 0) return SG_OK;
+    k_fri_leaves<<<(unsigned)((n / 2 + 127) / 128), 128, 0, (cudaStream_t)stream>>>(d_evals, n / 2,
+                                                                                     (uint64_t*)d_leaves);
+    return check_launch(CX(c), "k_fri_leaves");
+}
+
+int sg_gather_rows(sg_ctx* c, void* stream, const uint64_t* d_data, uint64_t row_u64, uint64_t nrows, uint64_t col0,
+                   uint64_t width, const uint32_t* d_rows, uint32_t nq, uint64_t* d_out) {
+    SG_CHECK_ARG(c, "null context");
+    SG_CHECK_ARG(col0 + width <= row_u64, "column range exceeds the row");
+    const uint64_t tot = (uint64_t)nq * width;
+    if (tot == 0) return SG_OK;
+    k_gather_rows<<<(unsigned)((tot + 255) / 256), 256, 0, (cudaStream_t)stream>>>(d_data, row_u64, nrows, col0,
+                                                                                  width, d_rows, nq, d_out);
+    return check_launch(CX(c), "k_gather_rows");
+}
+
+int sg_logup_aux(sg_ctx* c, void* stream, const uint64_t* d_main, uint64_t n, uint64_t m, const sg_logup_desc* hd,
+                 const uint64_t* alpha_powers, uint32_t num_alpha, const uint64_t z[3], uint64_t* d_aux,
+                 uint64_t table_contribution[3]) {
+    SG_CHECK_ARG(c && hd && z && table_contribution, "null argument");
+    SG_CHECK_ARG(n >= 1, "n must be >= 1");
+    SG_CHECK_ARG(hd->num_committed <= hd->num_out_cols, "committed columns exceed output columns");
+    Ctx* ctx = CX(c);
+    cudaStream_t st = (cudaStream_t)stream;
+    const uint32_t K = hd->num_interactions, NO = hd->num_out_cols;
+    const uint32_t ne = K ? hd->elem_offsets[K] : 0, nt = ne ? hd->term_offsets[ne] : 0;
+    const uint32_t noi = NO ? hd->out_col_offsets[NO] : 0, nmt = K ? hd->mult_term_offsets[K] : 0;
+    // Validate CSR indices on the host: every column index must be < m and
+    // every interaction index < K, so the kernels never read out of bounds.
+    for (uint32_t t = 0; t < nt; ++t) SG_CHECK_ARG(hd->term_cols[t] < m, "fingerprint term column out of range");
+    for (uint32_t t = 0; t < nmt; ++t) SG_CHECK_ARG(hd->mult_term_cols[t] < m, "multiplicity column out of range");
+    for (uint32_t t = 0; t < noi; ++t) SG_CHECK_ARG(hd->out_col_interactions[t] < K, "interaction index out of range");
+    for (uint32_t e = 0; e < ne; ++e) SG_CHECK_ARG(hd->elem_alpha_idx[e] < num_alpha, "alpha power index out of range");
+    for (uint32_t k = 0; k < K; ++k) SG_CHECK_ARG(hd->elem_offsets[k] <= hd->elem_offsets[k + 1], "elem offsets");
+    for (uint32_t e = 0; e < ne; ++e) SG_CHECK_ARG(hd->term_offsets[e] <= hd->term_offsets[e + 1], "term offsets");
+    for (uint32_t o = 0; o < NO; ++o) SG_CHECK_ARG(hd->out_col_offsets[o] <= hd->out_col_offsets[o + 1], "out offsets");
+    for (uint32_t k = 0; k < K; ++k)
+        SG_CHECK_ARG(hd->mult_term_offsets[k] <= hd->mult_term_offsets[k + 1], "mult offsets");
+    // One device blob for the descriptor.
+    std::vector<uint64_t> blob;
+    auto put64 = [&](const uint64_t* p, size_t cnt) {
+        size_t o = blob.size();
+        blob.insert(blob.end(), p, p + cnt);
+        return o;
+    };
+    auto put32 = [&](const uint32_t* p, size_t cnt) {
+        size_t o = blob.size();
+        for (size_t i = 0; i < cnt; i += 2) {
+            uint64_t lo = p[i], hi = i + 1 < cnt ? p[i + 1] : 0;
+            blob.push_back(lo | (hi << 32));
+        }
+        if (cnt == 0) blob.push_back(0);
+        return o;
+    };
+    const uint32_t zero32[2] = {0, 0};
+    const size_t o_bus = put64(hd->bus_ids, K), o_eo = put32(K ? hd->elem_offsets : zero32, K + 1),
+                 o_ea = put32(hd->elem_alpha_idx, ne), o_ec = put64(hd->elem_consts, ne),
+                 o_to = put32(ne ? hd->term_offsets : zero32, ne + 1), o_tc = put64(hd->term_coefs, nt),
+                 o_tl = put32(hd->term_cols, nt), o_oo = put32(NO ? hd->out_col_offsets : zero32, NO + 1),
+                 o_oi = put32(hd->out_col_interactions, noi), o_mc = put64(hd->mult_consts, K),
+                 o_mo = put32(K ? hd->mult_term_offsets : zero32, K + 1), o_mk = put64(hd->mult_term_coefs, nmt),
+                 o_ml = put32(hd->mult_term_cols, nmt), o_al = put64(alpha_powers, 3ull * num_alpha);
+    blob.push_back(0);
+    const uint64_t W = (uint64_t)hd->num_committed + 1;
+    const uint64_t nseg = (n + LG_SEG - 1) / LG_SEG;
+    uint64_t *d_blob = nullptr, *d_fp = nullptr, *d_rs = nullptr, *d_seg = nullptr;
+    const uint64_t bb = 8 * blob.size(), fb = 24ull * (uint64_t)K * n + 24, rb = 24ull * n, sb = 24ull * (nseg + 2);
+    int rc = dev_alloc(ctx, st, bb, (void**)&d_blob);
+    if (rc == SG_OK) rc = dev_alloc(ctx, st, fb, (void**)&d_fp);
+    if (rc == SG_OK) rc = dev_alloc(ctx, st, rb, (void**)&d_rs);
+    if (rc == SG_OK) rc = dev_alloc(ctx, st, sb, (void**)&d_seg);
+    if (rc == SG_OK && cudaMemcpyAsync(d_blob, blob.data(), bb, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+        set_error("logup: descriptor upload failed");
+        rc = SG_ERR_CUDA;
+    }
+    if (rc == SG_OK) {
+        auto u32p = [&](size_t o) { return (const uint32_t*)(d_blob + o); };
+        LogupDesc d{K,          d_blob + o_bus, u32p(o_eo),     u32p(o_ea),     d_blob + o_ec,
+                    u32p(o_to), d_blob + o_tc,  u32p(o_tl),     NO,             u32p(o_oo),
+                    u32p(o_oi), d_blob + o_mc,  u32p(o_mo),     d_blob + o_mk,  u32p(o_ml),
+                    hd->num_committed, d_blob + o_al};
+        if (K) {
+            const uint64_t tot = (uint64_t)K * n;
+            k_logup_fp<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(d_main, n, m, d, z[0], z[1], z[2], d_fp);
+            rc = check_launch(ctx, "k_logup_fp");
+            int zf = 0;
+            if (rc == SG_OK) rc = batch_inv_launch(ctx, st, LoadPlain{d_fp}, tot, d_fp, &zf);
+            if (rc == SG_OK && zf) {
+                set_error("logup: a fingerprint is zero (challenge collides with a row value)");
+                rc = SG_ERR_INVALID;
+            }
+        }
+        if (rc == SG_OK) {
+            k_logup_terms<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(d_main, n, m, d, d_fp, d_aux, d_rs);
+            rc = check_launch(ctx, "k_logup_terms");
+        }
+        if (rc == SG_OK) {
+            k_seg_sum<<<(unsigned)nseg, 256, 0, st>>>(d_rs, n, d_seg + 6);
+            rc = check_launch(ctx, "k_seg_sum");
+        }
+        if (rc == SG_OK) {
+            const uint64_t ninv = sg_host_gl_inv(n % GL_P);
+            k_seg_scan<<<1, 32, 0, st>>>(d_seg + 6, nseg, ninv, d_seg);
+            rc = check_launch(ctx, "k_seg_scan");
+        }
+        if (rc == SG_OK) {
+            k_logup_acc<<<(unsigned)nseg, LG_SEG, 0, st>>>(d_rs, n, d_seg + 6, d_seg, W, d_aux);
+            rc = check_launch(ctx, "k_logup_acc");
+        }
+        if (rc == SG_OK && (cudaMemcpyAsync(table_contribution, d_seg, 24, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                            cudaStreamSynchronize(st) != cudaSuccess)) {
+            set_error("logup: contribution readback failed");
+            rc = SG_ERR_CUDA;
+        }
+    }
+    dev_free(ctx, st, d_seg, sb);
+    dev_free(ctx, st, d_rs, rb);
+    dev_free(ctx, st, d_fp, fb);
+    dev_free(ctx, st, d_blob, bb);
+    return rc;
+}
+
+}  // extern "C"

@@ -29,6 +29,28 @@ class LdeInfo(C.Structure):
 
 
 u64, u32, i32, vp = C.c_uint64, C.c_uint32, C.c_int, C.c_void_p
+
+
+class DeviceProgram(C.Structure):
+    _fields_ = [("nodes", C.c_void_p), ("num_nodes", C.c_uint32), ("base_consts", C.c_void_p),
+                ("num_base_consts", C.c_uint32), ("ext_consts", C.c_void_p), ("num_ext_consts", C.c_uint32),
+                ("roots", C.c_void_p), ("num_roots", C.c_uint32), ("num_base_slots", C.c_uint32),
+                ("num_ext_slots", C.c_uint32)]
+
+
+class Composition(C.Structure):
+    _fields_ = [("beta_trans", C.c_void_p), ("d_z_inv", C.c_void_p), ("z_len", C.c_uint64),
+                ("num_boundary", C.c_uint32), ("b_col", C.c_void_p), ("b_is_aux", C.c_void_p),
+                ("b_value", C.c_void_p), ("b_beta", C.c_void_p), ("d_b_z_inv", C.c_void_p)]
+
+
+class LogupDesc(C.Structure):
+    _fields_ = [("num_interactions", C.c_uint32), ("bus_ids", C.c_void_p), ("elem_offsets", C.c_void_p),
+                ("elem_alpha_idx", C.c_void_p), ("elem_consts", C.c_void_p), ("term_offsets", C.c_void_p),
+                ("term_coefs", C.c_void_p), ("term_cols", C.c_void_p), ("num_out_cols", C.c_uint32),
+                ("out_col_offsets", C.c_void_p), ("out_col_interactions", C.c_void_p), ("mult_consts", C.c_void_p),
+                ("mult_term_offsets", C.c_void_p), ("mult_term_coefs", C.c_void_p), ("mult_term_cols", C.c_void_p),
+                ("num_committed", C.c_uint32)]
 PROTOTYPES = {
     "sg_ctx_create": (i32, [i32, u64, C.POINTER(vp)]),
     "sg_ctx_destroy": (None, [vp]),
@@ -55,6 +77,29 @@ PROTOTYPES = {
     "sg_lde_free": (None, [vp, vp]),
     "sg_grind": (i32, [vp, vp, vp, C.c_uint8, C.POINTER(u64)]),
     "sg_coset_lde_static": (i32, [vp, vp, u64, u64, u32, vp, vp]),
+    "sg_transcript_new": (vp, [vp, u64]),
+    "sg_transcript_clone": (vp, [vp]),
+    "sg_transcript_free": (None, [vp]),
+    "sg_transcript_append": (None, [vp, vp, u64]),
+    "sg_transcript_append_base": (None, [vp, u64]),
+    "sg_transcript_append_ext3": (None, [vp, vp]),
+    "sg_transcript_sample": (None, [vp, vp]),
+    "sg_transcript_state": (None, [vp, vp]),
+    "sg_transcript_sample_base": (u64, [vp]),
+    "sg_transcript_sample_ext3": (None, [vp, vp]),
+    "sg_transcript_sample_u64": (u64, [vp, u64]),
+    "sg_transcript_sample_z_ood": (None, [vp, u64, u64, u64, vp]),
+    "sg_keccak256": (None, [vp, u64, vp]),
+    "sg_batch_inverse_ext3": (i32, [vp, vp, vp, u64, vp, C.POINTER(i32)]),
+    "sg_inv_denoms_ext3": (i32, [vp, vp, vp, u64, vp, u32, i32, vp, C.POINTER(i32)]),
+    "sg_barycentric_sums": (i32, [vp, vp, vp, u64, u64, i32, u64, vp, vp, u64, u32, vp]),
+    "sg_deep_composition": (i32, [vp, vp, vp, u64, vp, u64, vp, u64, u64, vp, vp, vp, vp, u32, vp, vp, i32, vp]),
+    "sg_fri_fold_layer": (i32, [vp, vp, vp, u64, vp, vp, vp, vp, vp]),
+    "sg_fri_leaves": (i32, [vp, vp, vp, u64, vp]),
+    "sg_gather_rows": (i32, [vp, vp, vp, u64, u64, u64, u64, vp, u32, vp]),
+    "sg_logup_aux": (i32, [vp, vp, vp, u64, u64, vp, vp, u32, vp, vp, vp]),
+    "sg_eval_constraints": (i32, [vp, vp, vp, vp, u32, vp, u32, vp, vp, u64, vp, u64, u64, u64, vp, vp]),
+    "sg_decompose_d2": (i32, [vp, vp, vp, u64, vp, vp]),
 }
 SG_STATIC_SCRATCH_BYTES = 32 << 20
 

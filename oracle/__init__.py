@@ -57,6 +57,12 @@ def lib():
             "or_grind": (u64, [vp, C.c_uint8, u64]),
             "or_fp3_batch_inverse": (C.c_int, [vp, u64]),
             "or_fri_fold": (None, [vp, u64, vp, vp, vp]),
+            "or_inv_denoms": (C.c_int, [vp, u64, vp, u64, C.c_int, vp]),
+            "or_barycentric_sums": (None, [vp, u64, u64, C.c_int, u64, vp, vp, u64, u64, vp]),
+            "or_deep": (None, [vp, u64, vp, u64, vp, u64, u64, vp, vp, vp, vp, vp, vp, u64, vp]),
+            "or_fri_leaves": (None, [vp, u64, vp]),
+            "or_logup_aux": (C.c_int, [vp, u64, u64, u32, vp, vp, vp, vp, vp, vp, vp, u32, vp, vp, vp, vp, vp, vp,
+                                       u32, vp, vp, vp, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -281,3 +287,63 @@ def fri_number_of_queries(blowup, security_bits=128, grinding=20):
     proximity = 1.0 - math.sqrt(rate) - 1.0 / 300.0
     bits_per_query = -math.log2(1.0 - proximity)
     return int(math.ceil((security_bits - grinding) / bits_per_query))
+
+
+def inv_denoms(x, z, x_minus_z):
+    x, z = _u64(x), _u64(z).reshape(-1)
+    n, K = x.size, z.size // 3
+    out = np.zeros(3 * n * K, np.uint64)
+    if lib().or_inv_denoms(_p(x), n, _p(z), K, 1 if x_minus_z else 0, _p(out)):
+        raise ZeroDivisionError("zero denominator")
+    return out
+
+
+def barycentric_sums(data, row_stride, ext3, cols, points, invd, n, K):
+    d = _u64(data)
+    ru = d.shape[1] if d.ndim == 2 else d.size
+    out = np.zeros(3 * K * cols, np.uint64)
+    lib().or_barycentric_sums(_p(d), ru, row_stride, 1 if ext3 else 0, cols, _p(_u64(points)), _p(_u64(invd)), n, K,
+                              _p(out))
+    return out
+
+
+def deep(main, aux, parts, h_ood, trace_ood, gammas_h, gammas_tr, inv_h, inv_t, K):
+    main, aux, parts = _u64(main), _u64(aux), _u64(parts)
+    rows = main.shape[0]
+    m = main.shape[1] if main.ndim == 2 else 0
+    A = (aux.shape[1] // 3) if aux.ndim == 2 else 0
+    Pp = (parts.shape[1] // 3) if parts.ndim == 2 else 0
+    out = np.zeros(3 * rows, np.uint64)
+    lib().or_deep(_p(main), m, _p(aux), A, _p(parts), Pp, rows, _p(_u64(h_ood)), _p(_u64(trace_ood)),
+                  _p(_u64(gammas_h)), _p(_u64(gammas_tr)), _p(_u64(inv_h)), _p(_u64(inv_t)), K, _p(out))
+    return out
+
+
+def fri_leaves(evals):
+    e = _u64(evals).reshape(-1)
+    h = e.size // 6
+    out = np.zeros((h, 32), np.uint8)
+    lib().or_fri_leaves(_p(e), h, _p(out))
+    return out
+
+
+def logup_aux(main, desc, alpha_pows, z):
+    """desc: dict of numpy arrays with the CSR descriptor fields."""
+    main = _u64(main)
+    n, m = main.shape
+    u32 = lambda a: np.ascontiguousarray(a, np.uint32)
+    d = {k: (u32(v) if v.dtype == np.uint32 else _u64(v)) if isinstance(v, np.ndarray) else v for k, v in desc.items()}
+    W = d["num_committed"] + 1
+    aux = np.zeros((n, 3 * W), np.uint64)
+    L = np.zeros(3, np.uint64)
+    keep = [d[k] for k in d if isinstance(d[k], np.ndarray)]
+    rc = lib().or_logup_aux(_p(main), n, m, d["num_interactions"], _p(d["bus_ids"]), _p(d["elem_offsets"]),
+                            _p(d["elem_alpha_idx"]), _p(d["elem_consts"]), _p(d["term_offsets"]),
+                            _p(d["term_coefs"]), _p(d["term_cols"]), d["num_out_cols"], _p(d["out_col_offsets"]),
+                            _p(d["out_col_interactions"]), _p(d["mult_consts"]), _p(d["mult_term_offsets"]),
+                            _p(d["mult_term_coefs"]), _p(d["mult_term_cols"]), d["num_committed"],
+                            _p(_u64(alpha_pows)), _p(_u64(z)), _p(aux), _p(L))
+    del keep
+    if rc:
+        raise ZeroDivisionError("zero fingerprint")
+    return aux, L

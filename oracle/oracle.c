@@ -574,3 +574,155 @@ void or_fri_fold(const uint64_t *evals, uint64_t h, const uint64_t *inv_tw, cons
         for (int k = 0; k < 3; k++) out[3 * j + k] = or_gl_add(s[k], or_gl_mul(inv_tw[j], zd[k]));
     }
 }
+
+/* ------------------------------------------------------------------ */
+/* Denominators for barycentric (R3) and DEEP (R4):                    */
+/* crypto/math-cuda/src/inverse.rs:226-300 (DenomSign), polynomial.rs   */
+/* barycentric_inv_denoms (z - x), prover.rs R4 (x - z).               */
+/* out[k*n + i] = sign ? x_i - z_k : z_k - x_i  (ext3, then inverted).  */
+/* ------------------------------------------------------------------ */
+int or_inv_denoms(const uint64_t *x, uint64_t n, const uint64_t *z, uint64_t K, int x_minus_z, uint64_t *out) {
+    for (uint64_t k = 0; k < K; k++)
+        for (uint64_t i = 0; i < n; i++) {
+            uint64_t *o = out + 3 * (k * n + i);
+            const uint64_t *zk = z + 3 * k;
+            if (x_minus_z) {
+                o[0] = or_gl_sub(x[i], zk[0]); o[1] = or_gl_neg(zk[1]); o[2] = or_gl_neg(zk[2]);
+            } else {
+                o[0] = or_gl_sub(zk[0], x[i]); o[1] = zk[1]; o[2] = zk[2];
+            }
+        }
+    return or_fp3_batch_inverse(out, K * n);
+}
+
+/* Barycentric sums (interpolate_coset_eval_ext_with_g_n_inv's inner sum,  */
+/* polynomial.rs:207-235; barycentric.cu:210-300):                        */
+/*   out[(k*cols + c)] = sum_i points[i] * col_c(row i*row_stride) * invd[k][i] */
+/* `data` is row-major (rows x row_u64); ext3 != 0 reads 3-u64 elements.   */
+void or_barycentric_sums(const uint64_t *data, uint64_t row_u64, uint64_t row_stride, int ext3, uint64_t cols,
+                         const uint64_t *points, const uint64_t *invd, uint64_t n, uint64_t K, uint64_t *out) {
+    #pragma omp parallel for schedule(static) if (cols * n > 65536)
+    for (int64_t c = 0; c < (int64_t)cols; c++) {
+        for (uint64_t k = 0; k < K; k++) {
+            uint64_t acc[3] = {0, 0, 0};
+            for (uint64_t i = 0; i < n; i++) {
+                const uint64_t *row = data + i * row_stride * row_u64;
+                uint64_t pe[3];
+                if (ext3) {
+                    for (int q = 0; q < 3; q++) pe[q] = or_gl_mul(points[i], row[3 * c + q]);
+                } else {
+                    pe[0] = or_gl_mul(points[i], row[c]); pe[1] = 0; pe[2] = 0;
+                }
+                uint64_t t[3];
+                or_fp3_mul(pe, invd + 3 * (k * n + i), t);
+                or_fp3_add(acc, t, acc);
+            }
+            for (int q = 0; q < 3; q++) out[3 * (k * cols + c) + q] = acc[q];
+        }
+    }
+}
+
+/* DEEP composition per LDE row (deep.cu:30-115, prover.rs:2400-2608):      */
+/*   r = sum_j g_j (H_j(x) - H_j(z^P)) inv_h[i]                               */
+/*     + sum_{j,k} g'_{jk} (t_j(x) - t_j(z w^k)) inv_t[k][i]                  */
+/* main: rows x m base; aux: rows x A ext3; parts: rows x P ext3 (row-major).  */
+/* out is written in natural order.                                          */
+void or_deep(const uint64_t *main, uint64_t m, const uint64_t *aux, uint64_t A, const uint64_t *parts, uint64_t P,
+             uint64_t rows, const uint64_t *h_ood, const uint64_t *trace_ood, const uint64_t *gammas_h,
+             const uint64_t *gammas_tr, const uint64_t *inv_h, const uint64_t *inv_t, uint64_t K, uint64_t *out) {
+    #pragma omp parallel for schedule(static) if (rows > 4096)
+    for (int64_t i = 0; i < (int64_t)rows; i++) {
+        uint64_t res[3] = {0, 0, 0}, t[3], u[3];
+        for (uint64_t j = 0; j < P; j++) {
+            or_fp3_sub(parts + 3 * ((uint64_t)i * P + j), h_ood + 3 * j, t);
+            or_fp3_mul(gammas_h + 3 * j, t, u);
+            or_fp3_mul(u, inv_h + 3 * i, t);
+            or_fp3_add(res, t, res);
+        }
+        for (uint64_t j = 0; j < m + A; j++) {
+            uint64_t tv[3];
+            if (j < m) { tv[0] = main[(uint64_t)i * m + j]; tv[1] = 0; tv[2] = 0; }
+            else memcpy(tv, aux + 3 * ((uint64_t)i * A + (j - m)), 24);
+            for (uint64_t k = 0; k < K; k++) {
+                uint64_t idx = 3 * (j * K + k);
+                or_fp3_sub(tv, trace_ood + idx, t);
+                or_fp3_mul(gammas_tr + idx, t, u);
+                or_fp3_mul(u, inv_t + 3 * (k * rows + (uint64_t)i), t);
+                or_fp3_add(res, t, res);
+            }
+        }
+        memcpy(out + 3 * i, res, 24);
+    }
+}
+
+/* FRI layer leaves: Keccak256(e[2j] || e[2j+1]), each ext3 as 3 canonical BE
+ * u64 (FieldElementPairBackend, field_element_vector.rs; keccak.cu:384). */
+void or_fri_leaves(const uint64_t *evals, uint64_t h, uint8_t *out) {
+    #pragma omp parallel for schedule(static) if (h > 4096)
+    for (int64_t j = 0; j < (int64_t)h; j++) {
+        uint8_t b[48];
+        for (int q = 0; q < 6; q++) {
+            uint64_t v = or_gl_canonical(evals[6 * j + q]);
+            for (int x = 0; x < 8; x++) b[8 * q + x] = (uint8_t)(v >> (8 * (7 - x)));
+        }
+        or_keccak256(b, 48, out + 32 * (uint64_t)j);
+    }
+}
+
+/* LogUp aux build: crypto/stark/src/lookup.rs:1660-1842 (term columns and the
+ * accumulated column) with the CSR descriptor of math-cuda/src/logup.rs:26-44.
+ * main: row-major n x m. aux out: row-major n x (n_committed + 1) ext3:
+ * term columns [0, n_committed) then the accumulated column.
+ * Returns the table contribution L in L_out. */
+int or_logup_aux(const uint64_t *main, uint64_t n, uint64_t m, uint32_t K, const uint64_t *bus_ids,
+                 const uint32_t *elem_off, const uint32_t *elem_alpha, const uint64_t *elem_const,
+                 const uint32_t *term_off, const uint64_t *term_coef, const uint32_t *term_col, uint32_t n_out,
+                 const uint32_t *out_off, const uint32_t *out_int, const uint64_t *mult_const,
+                 const uint32_t *mterm_off, const uint64_t *mterm_coef, const uint32_t *mterm_col,
+                 uint32_t n_committed, const uint64_t *alpha_pows, const uint64_t *z, uint64_t *aux, uint64_t *L_out) {
+    uint64_t *fp = (uint64_t *)malloc(3 * (uint64_t)K * n * sizeof(uint64_t) + 8);
+    uint64_t *rs = (uint64_t *)calloc(3 * n + 1, sizeof(uint64_t));
+    uint64_t W = n_committed + 1;
+    for (uint64_t r = 0; r < n; r++)
+        for (uint32_t k = 0; k < K; k++) {
+            uint64_t lc[3] = {bus_ids[k], 0, 0};
+            for (uint32_t e = elem_off[k]; e < elem_off[k + 1]; e++) {
+                uint64_t base = elem_const[e];
+                for (uint32_t t = term_off[e]; t < term_off[e + 1]; t++)
+                    base = or_gl_add(base, or_gl_mul(term_coef[t], main[r * m + term_col[t]]));
+                const uint64_t *a = alpha_pows + 3 * elem_alpha[e];
+                for (int q = 0; q < 3; q++) lc[q] = or_gl_add(lc[q], or_gl_mul(a[q], base));
+            }
+            uint64_t *f = fp + 3 * ((uint64_t)k * n + r);
+            or_fp3_sub(z, lc, f);
+        }
+    if (K && or_fp3_batch_inverse(fp, (uint64_t)K * n)) { free(fp); free(rs); return -1; }
+    for (uint64_t r = 0; r < n; r++)
+        for (uint32_t c = 0; c < n_out; c++) {
+            uint64_t term[3] = {0, 0, 0};
+            for (uint32_t ki = out_off[c]; ki < out_off[c + 1]; ki++) {
+                uint32_t k = out_int[ki];
+                uint64_t mu = mult_const[k];
+                for (uint32_t t = mterm_off[k]; t < mterm_off[k + 1]; t++)
+                    mu = or_gl_add(mu, or_gl_mul(mterm_coef[t], main[r * m + mterm_col[t]]));
+                const uint64_t *rc = fp + 3 * ((uint64_t)k * n + r);
+                for (int q = 0; q < 3; q++) term[q] = or_gl_add(term[q], or_gl_mul(rc[q], mu));
+            }
+            if (c < n_committed) memcpy(aux + 3 * (r * W + c), term, 24);
+            or_fp3_add(rs + 3 * r, term, rs + 3 * r);
+        }
+    uint64_t L[3] = {0, 0, 0};
+    for (uint64_t r = 0; r < n; r++) or_fp3_add(L, rs + 3 * r, L);
+    uint64_t ninv = or_gl_inv(n % GL_P), off[3];
+    for (int q = 0; q < 3; q++) off[q] = or_gl_mul(L[q], ninv);
+    uint64_t acc[3] = {0, 0, 0};
+    for (uint64_t r = 0; r < n; r++) {
+        memcpy(aux + 3 * (r * W + n_committed), acc, 24);
+        or_fp3_add(acc, rs + 3 * r, acc);
+        or_fp3_sub(acc, off, acc);
+    }
+    memcpy(L_out, L, 24);
+    free(fp);
+    free(rs);
+    return 0;
+}
