@@ -89,6 +89,8 @@ class DeviceBuffer:
             native.lib().sg_dev_free(self.be.h, self.stream, self.ptr, self.nbytes)
             self.ptr = 0
 
+    free = close
+
     def __del__(self):
         try:
             self.close()

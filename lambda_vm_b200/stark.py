@@ -1,0 +1,493 @@
+"""Multi-table STARK prover over the B200 kernels.
+
+Round structure follows IsStarkProver::multi_prove (crypto/stark/src/prover.rs:3299-4037)
+and prove_rounds_2_to_4 (prover.rs:4433-4620):
+  R1  per table: coset LDE of the main trace + row-pair Keccak commitment;
+      roots absorbed in table order; LogUp challenges [z, alpha] sampled once;
+      per-table transcript forks (clone + table index LE bytes when > 1 table).
+  aux LogUp aux columns built and committed, root absorbed.
+  R2  beta; coefficients beta^i (transition constraints first, then boundary);
+      composition H over the LDE; degree-2 split into two parts, each
+      extended to the LDE; parts committed, root absorbed.
+  R3  z = sample_z_ood; trace columns opened at z and z*w, the parts at z^2, by
+      barycentric interpolation over the trace coset; values absorbed.
+  R4  gamma; DEEP codeword; FRI commit (fri/mod.rs:27-151) with the terminal
+      polynomial; grinding nonce (grinding.rs); query indexes
+      sample_u64(lde/2); openings with Merkle paths.
+Every heavy step is a C-ABI call into libstarkgpu (the GPU backend below);
+the driver only moves challenges and small host values. The same driver runs
+over any backend with the same interface.
+
+Differences from the reference protocol, kept deliberately simple: every trace
+column is opened at z*w (the reference prunes next-row openings to the columns
+constraints read there), and the DEEP coefficients are successive powers of
+gamma (parts first, then trace columns column-major over the two points).
+"""
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import field as F
+from . import math_cuda as mc
+from . import native
+from .device import DeviceBuffer, backend as _backend
+from .ir import lower
+
+P = F.P
+
+
+class Options:
+    def __init__(self, blowup=2, coset_offset=3, grinding=20, final_log_degree=5, queries=None, security=128):
+        self.blowup = blowup
+        self.coset_offset = coset_offset
+        self.grinding = grinding
+        self.final_log_degree = final_log_degree
+        if queries is None:
+            rate = 1.0 / blowup
+            prox = 1.0 - math.sqrt(rate) - 1.0 / 300.0
+            queries = int(math.ceil((security - grinding) / -math.log2(1.0 - prox)))
+        self.queries = queries
+
+
+def fri_layout(lde_log, blowup_log, k):
+    """FriFoldLayout::new (fri/terminal.rs:45-55)."""
+    terminal_log = min(blowup_log + k, lde_log)
+    total = lde_log - terminal_log
+    return {"total_folds": total, "num_committed": max(total - 1, 0), "terminal_len": 1 << terminal_log,
+            "effective_k": terminal_log - blowup_log}
+
+
+def terminal_coeffs(codeword_br, terminal_offset, eff_k):
+    """coeffs_from_terminal_codeword (fri/terminal.rs:72-103): gather the
+    size-2^k sub-coset from the bit-reversed codeword and interpolate it on
+    the coset terminal_offset * <w^blowup> (small, on the host)."""
+    ln = len(codeword_br)
+    keep = 1 << eff_k
+    blow = ln // keep
+    lbits = ln.bit_length() - 1
+    sub = [F.f3(codeword_br[F.bitrev_int(mm * blow, lbits)]) for mm in range(keep)]
+    # evaluations at terminal_offset * w_keep^j ; coefficients by inverse DFT
+    w = F.root_of_unity(eff_k)
+    winv = F.inv_int(w) if keep > 1 else 1
+    kinv = F.inv_int(keep)
+    oinv = F.inv_int(terminal_offset)
+    coeffs = []
+    for i in range(keep):
+        acc = (0, 0, 0)
+        wi = pow(winv, i, P)
+        for j in range(keep):
+            acc = F.f3add(acc, F.f3scale(sub[j], pow(wi, j, P)))
+        coeffs.append(F.f3scale(acc, kinv * pow(oinv, i, P) % P))
+    return coeffs
+
+
+# ====================================================================== GPU backend
+class Mat:
+    """A row-major device matrix: rows x cols u64."""
+
+    def __init__(self, buf, rows, cols):
+        self.buf, self.rows, self.cols = buf, rows, cols
+
+    @property
+    def ptr(self):
+        return self.buf.ptr
+
+    def __len__(self):
+        return self.rows
+
+    def free(self):
+        self.buf.close()
+
+
+class Tree:
+    def __init__(self, buf, leaves_len):
+        self.buf, self.leaves_len = buf, leaves_len
+
+    def free(self):
+        self.buf.close()
+
+
+class GpuBackend:
+    name = "gpu"
+
+    def __init__(self, be=None, stream=None):
+        self.be = be or _backend()
+        self.L = native.lib()
+        self.st = stream
+
+    def _alloc(self, rows, cols):
+        return Mat(DeviceBuffer(max(8, 8 * rows * cols), self.be, self.st), rows, cols)
+
+    def transcript(self, label):
+        return mc.Transcript(label)
+
+    def upload(self, arr):
+        a = np.ascontiguousarray(arr, np.uint64)
+        if a.ndim == 1:
+            a = a.reshape(-1, 1)
+        m = self._alloc(a.shape[0], a.shape[1])
+        m.buf.upload(a)
+        return m
+
+    def to_host(self, mat):
+        return mat.buf.download(np.uint64, mat.rows * mat.cols).reshape(mat.rows, mat.cols)
+
+    def lde(self, mat, blowup, weights):
+        dw = DeviceBuffer.from_host(np.ascontiguousarray(weights, np.uint64), self.be, self.st)
+        out = self._alloc(mat.rows * blowup, mat.cols)
+        native.check(self.L.sg_coset_lde(self.be.h, self.st, mat.ptr, mat.rows, mat.cols, blowup, dw.ptr, out.ptr))
+        dw.close()
+        return out
+
+    def commit(self, mat, rows_per_leaf=2, little_endian=False):
+        nl = mat.rows // rows_per_leaf
+        tree = Tree(DeviceBuffer((2 * nl - 1) * 32, self.be, self.st), nl)
+        lay = native.LeafLayout(rows_per_leaf, 1 if little_endian else 0, 0, 0)
+        leaves = tree.buf.ptr + (nl - 1) * 32
+        native.check(self.L.sg_keccak_leaves(self.be.h, self.st, mat.ptr, mat.rows, mat.cols, C.byref(lay), leaves))
+        root = (C.c_uint8 * 32)()
+        native.check(self.L.sg_merkle_build(self.be.h, self.st, leaves, nl, tree.buf.ptr, root))
+        return tree, bytes(root)
+
+    def tree_from_leaves(self, leaves_buf, nl):
+        tree = Tree(DeviceBuffer((2 * nl - 1) * 32, self.be, self.st), nl)
+        root = (C.c_uint8 * 32)()
+        native.check(self.L.sg_merkle_build(self.be.h, self.st, leaves_buf.ptr, nl, tree.buf.ptr, root))
+        return tree, bytes(root)
+
+    def logup_aux(self, trace, desc, alpha_pows, z):
+        keep = {}
+
+        def arr(name, dt):
+            a = np.ascontiguousarray(desc[name], dt)
+            keep[name] = a if a.size else np.zeros(1, dt)
+            return keep[name].ctypes.data
+
+        d = native.LogupDesc()
+        d.num_interactions = desc["num_interactions"]
+        for nm, dt in (("bus_ids", np.uint64), ("elem_offsets", np.uint32), ("elem_alpha_idx", np.uint32),
+                       ("elem_consts", np.uint64), ("term_offsets", np.uint32), ("term_coefs", np.uint64),
+                       ("term_cols", np.uint32), ("out_col_offsets", np.uint32), ("out_col_interactions", np.uint32),
+                       ("mult_consts", np.uint64), ("mult_term_offsets", np.uint32), ("mult_term_coefs", np.uint64),
+                       ("mult_term_cols", np.uint32)):
+            setattr(d, nm, arr(nm, dt))
+        d.num_out_cols = desc["num_out_cols"]
+        d.num_committed = desc["num_committed"]
+        W = desc["num_committed"] + 1
+        al = np.ascontiguousarray(alpha_pows, np.uint64).reshape(-1)
+        zz = np.array(z, np.uint64)
+        aux = self._alloc(trace.rows, 3 * W)
+        L = np.zeros(3, np.uint64)
+        native.check(self.L.sg_logup_aux(self.be.h, self.st, trace.ptr, trace.rows, trace.cols, C.byref(d),
+                                         al.ctypes.data, al.size // 3, zz.ctypes.data, aux.ptr, L.ctypes.data))
+        return aux, F.f3(L)
+
+    def composition(self, program, lowered, main, aux, rap, alpha_pows, offset, next_step, beta, z_inv, boundary,
+                    b_z_inv):
+        keep = []
+        prog = mc._program_struct(lowered, keep)
+        c = native.Composition()
+        bt = np.ascontiguousarray(beta, np.uint64).reshape(-1)
+        dz = DeviceBuffer.from_host(np.ascontiguousarray(z_inv, np.uint64), self.be, self.st)
+        c.beta_trans, c.d_z_inv, c.z_len = bt.ctypes.data, dz.ptr, len(z_inv)
+        c.num_boundary = len(boundary)
+        cols = np.array([b[0] for b in boundary] or [0], np.uint64)
+        isa = np.array([1 if b[1] else 0 for b in boundary] or [0], np.uint64)
+        val = np.array([b[2] for b in boundary] or [(0, 0, 0)], np.uint64).reshape(-1)
+        bb = np.array([b[3] for b in boundary] or [(0, 0, 0)], np.uint64).reshape(-1)
+        c.b_col, c.b_is_aux, c.b_value, c.b_beta = cols.ctypes.data, isa.ctypes.data, val.ctypes.data, bb.ctypes.data
+        c.d_b_z_inv = b_z_inv.ptr if b_z_inv is not None else None
+        rap_a = np.ascontiguousarray(rap, np.uint64).reshape(-1)
+        al = np.ascontiguousarray(alpha_pows, np.uint64).reshape(-1)
+        off = np.array(offset, np.uint64)
+        out = self._alloc(main.rows, 3)
+        native.check(self.L.sg_eval_constraints(self.be.h, self.st, C.byref(prog), rap_a.ctypes.data, rap_a.size // 3,
+                                                al.ctypes.data, al.size // 3, off.ctypes.data, main.ptr, main.cols,
+                                                aux.ptr, aux.cols // 3, main.rows, next_step, C.byref(c), out.ptr))
+        dz.close()
+        return out
+
+    def decompose(self, h, inv2x):
+        out = self._alloc(h.rows // 2, 6)
+        native.check(self.L.sg_decompose_d2(self.be.h, self.st, h.ptr, h.rows, inv2x.ptr, out.ptr))
+        return out
+
+    def inv_base(self, x):
+        """Device vector of base inverses 1/x_i (x host)."""
+        x = np.ascontiguousarray(x, np.uint64)
+        e = np.zeros((x.size, 3), np.uint64)
+        e[:, 0] = x
+        m = self.upload(e)
+        zf = C.c_int(0)
+        native.check(self.L.sg_batch_inverse_ext3(self.be.h, self.st, m.ptr, x.size, m.ptr, C.byref(zf)))
+        if zf.value:
+            raise ZeroDivisionError("inverse of zero")
+        h = self.to_host(m)[:, 0].copy()
+        m.free()
+        return h
+
+    def inv_denoms(self, pts, zs, x_minus_z):
+        z = np.array(zs, np.uint64).reshape(-1)
+        k = len(zs)
+        out = self._alloc(pts.rows * k, 3)
+        zf = C.c_int(0)
+        native.check(self.L.sg_inv_denoms_ext3(self.be.h, self.st, pts.ptr, pts.rows, z.ctypes.data, k,
+                                               1 if x_minus_z else 0, out.ptr, C.byref(zf)))
+        if zf.value:
+            raise ZeroDivisionError("zero denominator")
+        return out
+
+    def bary(self, mat, stride, ext3, cols, pts, invd, n, k):
+        out = DeviceBuffer(24 * k * cols, self.be, self.st)
+        native.check(self.L.sg_barycentric_sums(self.be.h, self.st, mat.ptr, mat.cols, stride, 1 if ext3 else 0, cols,
+                                                pts.ptr, invd.ptr, n, k, out.ptr))
+        r = out.download(np.uint64, 3 * k * cols).reshape(k, cols, 3)
+        out.close()
+        return r
+
+    def deep(self, main, aux, parts, h_ood, trace_ood, gh, gt, inv_h, inv_t, k):
+        out = self._alloc(main.rows, 3)
+        arrs = [np.ascontiguousarray(np.array(x, np.uint64).reshape(-1)) for x in (h_ood, trace_ood, gh, gt)]
+        native.check(self.L.sg_deep_composition(self.be.h, self.st, main.ptr, main.cols, aux.ptr, aux.cols // 3,
+                                                parts.ptr, parts.cols // 3, main.rows, arrs[0].ctypes.data,
+                                                arrs[1].ctypes.data, arrs[2].ctypes.data, arrs[3].ctypes.data, k,
+                                                inv_h.ptr, inv_t.ptr, 1, out.ptr))
+        return out
+
+    def fri_fold(self, ev, tw, zeta, with_leaves):
+        h = ev.rows // 2
+        out = self._alloc(h, 3)
+        twn = self._alloc(max(1, h // 2), 1)
+        leaves = DeviceBuffer(32 * max(1, h // 2), self.be, self.st) if with_leaves else None
+        z = np.array(zeta, np.uint64)
+        native.check(self.L.sg_fri_fold_layer(self.be.h, self.st, ev.ptr, h, tw.ptr, z.ctypes.data, out.ptr, twn.ptr,
+                                              leaves.ptr if leaves else None))
+        return out, twn, leaves
+
+    def gather(self, mat, rows):
+        r = np.ascontiguousarray(rows, np.uint32)
+        dr = DeviceBuffer.from_host(r, self.be, self.st)
+        out = DeviceBuffer(8 * max(1, r.size * mat.cols), self.be, self.st)
+        native.check(self.L.sg_gather_rows(self.be.h, self.st, mat.ptr, mat.cols, mat.rows, 0, mat.cols, dr.ptr,
+                                           r.size, out.ptr))
+        h = out.download(np.uint64, r.size * mat.cols).reshape(r.size, mat.cols)
+        dr.close()
+        out.close()
+        return h
+
+    def paths(self, tree, positions):
+        pos = np.ascontiguousarray(positions, np.uint32)
+        depth = tree.leaves_len.bit_length() - 1
+        dp = DeviceBuffer.from_host(pos, self.be, self.st)
+        out = DeviceBuffer(max(32, pos.size * depth * 32), self.be, self.st)
+        native.check(self.L.sg_merkle_gather_paths(self.be.h, self.st, tree.buf.ptr, tree.leaves_len, dp.ptr,
+                                                   pos.size, out.ptr))
+        h = out.download(np.uint8, pos.size * depth * 32).reshape(pos.size, depth, 32)
+        dp.close()
+        out.close()
+        return h
+
+    def grind(self, state, g):
+        inner = mc.keccak256(bytes([0x01, 0x23, 0x45, 0x67, 0x89, 0xAB, 0xCD, 0xED]) + bytes(state) + bytes([g]))
+        return mc.generate_nonce_gpu(mc.inner_hash_lanes(inner), g, self.be)
+
+    def free(self, *objs):
+        for o in objs:
+            if o is not None:
+                o.free()
+
+
+# ====================================================================== the protocol
+def _u64le(i):
+    return int(i).to_bytes(8, "little")
+
+
+def _u64be(i):
+    return int(i).to_bytes(8, "big")
+
+
+def _ood_scale(z, n, g):
+    """(z^n - g^n) * (1/n) * g^-n  (interpolate_coset_eval_ext_with_g_n_inv, polynomial.rs:207-235)."""
+    gn = F.pow_int(g, n)
+    s = F.inv_int(n) * F.inv_int(gn) % P
+    return F.f3scale(F.f3sub(F.f3pow(z, n), (gn, 0, 0)), s)
+
+
+def prove_table(bk, air, lowered, trace_mat, main_lde, main_tree, t, challenges, alpha_pows, opts, stats=None):
+    """Aux build + rounds 2-4 for one table (prover.rs:3603-3977, 4433-4620)."""
+    n, N = air.n, air.n * opts.blowup
+    B, g = opts.blowup, opts.coset_offset
+    log_n, log_N = air.log_n, air.log_n + (B.bit_length() - 1)
+    weights = F.coset_weights(n, g)
+    proof = {}
+    # ---- aux
+    aux, Lc = bk.logup_aux(trace_mat, air.logup_descriptor(), alpha_pows, challenges[0])
+    aux_lde = bk.lde(aux, B, weights)
+    bk.free(aux)
+    aux_tree, aux_root = bk.commit(aux_lde)
+    t.append_bytes(aux_root)
+    proof["aux_root"] = aux_root
+    proof["table_contribution"] = Lc
+    # ---- R2
+    beta = F.f3(t.sample_ext3())
+    ncons = len(lowered["roots"]) + len(air.boundary)
+    coefs = [(1, 0, 0)]
+    for _ in range(ncons - 1):
+        coefs.append(F.f3mul(coefs[-1], beta))
+    beta_t, beta_b = coefs[:len(lowered["roots"])], coefs[len(lowered["roots"]):]
+    # zerofiers on the LDE coset x_k = g w_N^k: x^n = g^n w_B^k
+    gn = F.pow_int(g, n)
+    wB = F.root_of_unity(B.bit_length() - 1)
+    z_inv = bk.inv_base(np.array([(gn * pow(wB, k, P) - 1) % P for k in range(B)], np.uint64))
+    pts_N = F.coset_points(log_N, g)
+    b_z_inv_host = bk.inv_base(F.sub(pts_N, np.uint64(1)))  # acc boundary at row 0: 1/(x - 1)
+    b_z_inv = bk.upload(b_z_inv_host.reshape(1, -1))
+    offset = F.f3scale(Lc, F.inv_int(n))
+    boundary = [(col, is_aux, (0, 0, 0), beta_b[i]) for i, (col, is_aux, _row) in enumerate(air.boundary)]
+    H = bk.composition(air.program, lowered, main_lde, aux_lde, [challenges[0], challenges[1]], alpha_pows, offset, B, beta_t,
+                       z_inv, boundary, b_z_inv)
+    bk.free(b_z_inv)
+    inv2x = bk.upload(bk.inv_base(F.add(pts_N[: N // 2], pts_N[: N // 2])).reshape(-1, 1))
+    halves = bk.decompose(H, inv2x)
+    bk.free(H, inv2x)
+    parts_lde = bk.lde(halves, 2, F.composition_weights(N // 2, g))
+    bk.free(halves)
+    comp_tree, comp_root = bk.commit(parts_lde)
+    t.append_bytes(comp_root)
+    proof["comp_root"] = comp_root
+    # ---- R3
+    z = F.f3(t.sample_z_ood(n, N, g))
+    wn = F.root_of_unity(log_n)
+    zw = F.f3scale(z, wn)
+    z2 = F.f3mul(z, z)
+    pts_n = bk.upload(F.coset_points(log_n, g).reshape(-1, 1))
+    invd = bk.inv_denoms(pts_n, [z, zw, z2], False)
+    S_main = bk.bary(main_lde, B, False, air.width, pts_n, invd, n, 3)
+    S_aux = bk.bary(aux_lde, B, True, air.aux_width, pts_n, invd, n, 3)
+    S_parts = bk.bary(parts_lde, B, True, 2, pts_n, invd, n, 3)
+    bk.free(invd, pts_n)
+    sc = [_ood_scale(p, n, g) for p in (z, zw, z2)]
+    trace_ood = [[F.f3mul(sc[k], F.f3(S_main[k, c])) for c in range(air.width)] +
+                 [F.f3mul(sc[k], F.f3(S_aux[k, c])) for c in range(air.aux_width)] for k in range(2)]
+    parts_ood = [F.f3mul(sc[2], F.f3(S_parts[2, j])) for j in range(2)]
+    for k in range(2):
+        for v in trace_ood[k]:
+            t.append_ext3(v)
+    for v in parts_ood:
+        t.append_ext3(v)
+    proof["trace_ood"] = trace_ood
+    proof["parts_ood"] = parts_ood
+    # ---- R4: DEEP
+    gamma = F.f3(t.sample_ext3())
+    ncols = air.width + air.aux_width
+    gp = [(1, 0, 0)]
+    for _ in range(2 + 2 * ncols - 1):
+        gp.append(F.f3mul(gp[-1], gamma))
+    gh, gt = gp[:2], gp[2:]
+    trace_ood_jk = [trace_ood[k][j] for j in range(ncols) for k in range(2)]
+    ptsN = bk.upload(pts_N.reshape(-1, 1))
+    inv_h = bk.inv_denoms(ptsN, [z2], True)
+    inv_t = bk.inv_denoms(ptsN, [z, zw], True)
+    bk.free(ptsN)
+    deep = bk.deep(main_lde, aux_lde, parts_lde, parts_ood, trace_ood_jk, gh, gt, inv_h, inv_t, 2)
+    bk.free(inv_h, inv_t)
+    # ---- FRI commit (fri/mod.rs:27-151)
+    lay = fri_layout(log_N, B.bit_length() - 1, opts.final_log_degree)
+    half = N // 2
+    tw0 = bk.inv_base(F.coset_points(log_N, g)[:half][F.bitrev_indices(log_N - 1).astype(np.int64)])
+    tw = bk.upload(tw0.reshape(-1, 1))
+    ev = deep
+    layers, fri_roots = [], []
+    for _ in range(lay["num_committed"]):
+        zeta = F.f3(t.sample_ext3())
+        ev2, tw2, leaves = bk.fri_fold(ev, tw, zeta, True)
+        tree, root = bk.tree_from_leaves(leaves, len(ev2) // 2)
+        bk.free(leaves, tw)
+        layers.append((ev2, tree))
+        fri_roots.append(root)
+        t.append_bytes(root)
+        ev, tw = ev2, tw2
+    if lay["total_folds"] > 0:
+        zeta = F.f3(t.sample_ext3())
+        evf, twf, _ = bk.fri_fold(ev, tw, zeta, False)
+        bk.free(twf)
+        final = bk.to_host(evf)
+        bk.free(evf)
+    else:
+        final = bk.to_host(ev)
+    bk.free(tw)
+    term_off = F.pow_int(g, 1 << lay["total_folds"])
+    coeffs = terminal_coeffs(final, term_off, lay["effective_k"])
+    for c in coeffs:
+        t.append_ext3(c)
+    proof["fri_roots"] = fri_roots
+    proof["fri_final_coeffs"] = coeffs
+    # ---- grinding + queries
+    nonce = bk.grind(t.state(), opts.grinding) if opts.grinding else 0
+    if opts.grinding:
+        t.append_bytes(_u64be(nonce))
+    proof["nonce"] = nonce
+    iotas = [t.sample_u64(half) for _ in range(opts.queries)]
+    proof["iotas"] = iotas
+    # ---- openings: leaf iota of each trace-side tree covers rows br(2i), br(2i+1)
+    rows = []
+    for i in iotas:
+        rows += [F.bitrev_int(2 * i, log_N), F.bitrev_int(2 * i + 1, log_N)]
+    proof["open_main"] = bk.gather(main_lde, rows)
+    proof["open_aux"] = bk.gather(aux_lde, rows)
+    proof["open_parts"] = bk.gather(parts_lde, rows)
+    proof["path_main"] = bk.paths(main_tree, iotas)
+    proof["path_aux"] = bk.paths(aux_tree, iotas)
+    proof["path_parts"] = bk.paths(comp_tree, iotas)
+    fri_open, fri_paths = [], []
+    for li, (lev, ltree) in enumerate(layers):
+        pos = [i >> li for i in iotas]
+        leaf = [p >> 1 for p in pos]
+        rr = []
+        for lf in leaf:
+            rr += [2 * lf, 2 * lf + 1]
+        fri_open.append(bk.gather(lev, rr))
+        fri_paths.append(bk.paths(ltree, leaf))
+    proof["fri_open"] = fri_open
+    proof["fri_paths"] = fri_paths
+    bk.free(deep, aux_lde, parts_lde, aux_tree, comp_tree)
+    for lev, ltree in layers:
+        bk.free(lev, ltree)
+    return proof
+
+
+def multi_prove(airs, traces, opts=None, bk=None, label=b"lambda_vm_b200/synthetic-multi-table"):
+    """Prove all tables of one multi-table statement; returns the proof dict."""
+    opts = opts or Options()
+    bk = bk or GpuBackend()
+    t = bk.transcript(label)
+    B, g = opts.blowup, opts.coset_offset
+    tabs = []
+    for air, tr in zip(airs, traces):
+        tm = bk.upload(tr)
+        lde = bk.lde(tm, B, F.coset_weights(air.n, g))
+        tree, root = bk.commit(lde)
+        tabs.append((air, tm, lde, tree, root))
+    for _, _, _, _, root in tabs:
+        t.append_bytes(root)
+    challenges = [F.f3(t.sample_ext3()), F.f3(t.sample_ext3())]  # [z, alpha] (lookup.rs:1315-1322)
+    alpha = challenges[1]
+    max_alpha = max(a.max_alpha for a in airs)
+    alpha_pows = [(1, 0, 0)]
+    for _ in range(max_alpha - 1):
+        alpha_pows.append(F.f3mul(alpha_pows[-1], alpha))
+    forks = []
+    for i in range(len(tabs)):
+        ti = t.clone()
+        if len(tabs) > 1:
+            ti.append_bytes(_u64le(i))
+        forks.append(ti)
+    proofs = []
+    for i, (air, tm, lde, tree, root) in enumerate(tabs):
+        lowered = lower(air.program)
+        p = prove_table(bk, air, lowered, tm, lde, tree, forks[i], challenges, alpha_pows, opts)
+        p["main_root"] = root
+        proofs.append(p)
+        bk.free(tm, lde, tree)
+    return {"tables": proofs, "challenges": challenges}

@@ -102,6 +102,17 @@ def fp3_mul(a, b):
     return out
 
 
+def fp3_pow(a, e):
+    r = np.array([1, 0, 0], np.uint64)
+    b = _u64(a).copy()
+    while e:
+        if e & 1:
+            r = fp3_mul(r, b)
+        b = fp3_mul(b, b)
+        e >>= 1
+    return r
+
+
 def fp3_inv(a):
     a, out = _u64(a), np.zeros(3, np.uint64)
     if lib().or_fp3_inv(_p(a), _p(out)):
@@ -242,6 +253,19 @@ class Transcript:
 
     def sample_u64(self, upper: int) -> int:
         return lib().or_transcript_sample_u64(_p(self._buf), upper)
+
+    def sample_z_ood(self, trace_len, lde_len, offset):
+        """IsStarkTranscript::sample_z_ood_with_domain_params (is_transcript.rs:44-75)."""
+        off_pow = gl_pow(offset, lde_len)
+        blow = lde_len // trace_len
+        while True:
+            z = self.sample_ext3()
+            zt = fp3_pow(z, trace_len)
+            in_trace = list(map(int, canon_array(zt))) == [1, 0, 0]
+            zl = fp3_pow(zt, blow)
+            in_lde = list(map(int, canon_array(zl))) == [canonical(off_pow), 0, 0]
+            if not in_trace and not in_lde:
+                return z
 
 
 # ---------------- grinding / FRI / inversion ----------------

@@ -2,8 +2,8 @@
 
 * `random_program` builds a random constraint program in the reference's IR
   (crypto/stark/src/constraint_ir/ir.rs: Op nodes with Base/Ext dims);
-* `lower` restates DeviceProgram::lower (constraint_ir/device.rs:160-330):
-  uniform-leaf propagation, liveness slot reuse per dim class, pinned roots;
+* `lower` is the library's DeviceProgram::lower restatement (lambda_vm_b200.ir),
+  checked here only through the kernel against the unlowered evaluation;
 * `eval_rows` evaluates the UNLOWERED program row by row with the oracle's
   field arithmetic (constraint_ir/interp.rs semantics), plus the composition
   accumulation of constraints/evaluator.rs.
@@ -69,98 +69,7 @@ def random_program(rng, m, a, n_rap, n_alpha, n_nodes=60, n_roots=5, max_offset=
     return {"nodes": nodes, "dims": dims, "base_consts": base_consts, "ext_consts": ext_consts, "roots": roots}
 
 
-def _operands(node):
-    if node[0] in ("add", "sub", "mul"):
-        return [node[1], node[2]]
-    if node[0] in ("neg", "embed"):
-        return [node[1]]
-    return []
-
-
-def _uniform(node):
-    return node[0] in ("cb", "ce", "rap", "alpha", "off")
-
-
-def lower(prog):
-    """DeviceProgram::lower restated: returns dict of numpy arrays."""
-    nodes, dims, roots = prog["nodes"], prog["dims"], prog["roots"]
-    n = len(nodes)
-    used = [False] * n
-    last = [0] * n
-    for i, nd in enumerate(nodes):
-        for o in _operands(nd):
-            used[o] = True
-            last[o] = i
-    is_root = [False] * n
-    for r in roots:
-        is_root[r] = True
-        used[r] = True
-    emitted = [used[i] and (not _uniform(nodes[i]) or is_root[i]) for i in range(n)]
-
-    def enc_uniform(nd):
-        k = nd[0]
-        if k == "cb":
-            return (OPK_BASE_CONST << OPK_SHIFT) | nd[1]
-        if k == "ce":
-            return (OPK_EXT_CONST << OPK_SHIFT) | nd[1]
-        if k == "rap":
-            return (OPK_RAP << OPK_SHIFT) | nd[1]
-        if k == "alpha":
-            return (OPK_ALPHA << OPK_SHIFT) | nd[1]
-        return OPK_OFFSET << OPK_SHIFT
-
-    slot_of = [None] * n
-    free = {BASE: [], EXT: []}
-    count = {BASE: 0, EXT: 0}
-    out = []
-    for i in range(n):
-        if not emitted[i]:
-            continue
-        nd = nodes[i]
-
-        def enc(j):
-            if not emitted[j]:
-                return enc_uniform(nodes[j])
-            kind = OPK_BASE_SLOT if dims[j] == BASE else OPK_EXT_SLOT
-            return (kind << OPK_SHIFT) | slot_of[j]
-
-        k = nd[0]
-        if k == "cb":
-            t = (OP_CONST_BASE, nd[1], 0)
-        elif k == "ce":
-            t = (OP_CONST_EXT, nd[1], 0)
-        elif k == "var":
-            _, main, off, col = nd
-            t = (OP_VAR, col, (int(main) << 16) | (off << 8))
-        elif k == "rap":
-            t = (OP_RAP, nd[1], 0)
-        elif k == "alpha":
-            t = (OP_ALPHA, nd[1], 0)
-        elif k == "off":
-            t = (OP_OFFSET, 0, 0)
-        elif k in ("add", "sub", "mul"):
-            t = ({"add": OP_ADD, "sub": OP_SUB, "mul": OP_MUL}[k], enc(nd[1]), enc(nd[2]))
-        elif k == "neg":
-            t = (OP_NEG, enc(nd[1]), 0)
-        else:
-            t = (OP_EMBED, enc(nd[1]), 0)
-        for o in _operands(nd):
-            if emitted[o] and not is_root[o] and last[o] == i and slot_of[o] is not None:
-                free[dims[o]].append(slot_of[o])
-                slot_of[o] = None
-        d = dims[i]
-        if free[d]:
-            s = free[d].pop()
-        else:
-            s = count[d]
-            count[d] += 1
-        slot_of[i] = s
-        out.append((t[0], t[1], t[2], s | (RES_EXT_BIT if d == EXT else 0)))
-    root_enc = [slot_of[r] | (RES_EXT_BIT if dims[r] == EXT else 0) for r in roots]
-    return {"nodes": np.array(out, np.uint32).reshape(-1, 4), "roots": np.array(root_enc, np.uint32),
-            "base_consts": np.array(prog["base_consts"], np.uint64),
-            "ext_consts": np.array(prog["ext_consts"], np.uint64).reshape(-1, 3),
-            "num_base_slots": count[BASE], "num_ext_slots": count[EXT]}
+from lambda_vm_b200.ir import lower  # noqa: E402,F401  (DeviceProgram::lower restatement under test)
 
 
 # ---------------- reference evaluation (unlowered IR) ----------------
