@@ -70,6 +70,8 @@ SG_API void sg_ctx_destroy(sg_ctx* ctx);
 SG_API const char* sg_last_error(void);
 /* Bytes currently held by the context and the high-water mark. */
 SG_API int sg_ctx_memory(sg_ctx* ctx, uint64_t* in_use, uint64_t* peak);
+/* The context's HBM budget in bytes. */
+SG_API uint64_t sg_ctx_budget(sg_ctx* ctx);
 /* Kernels launched through this context so far (for launch accounting). */
 SG_API uint64_t sg_ctx_launches(sg_ctx* ctx);
 /* Test hook for host-side failure handling: the n-th device allocation from
@@ -82,6 +84,10 @@ SG_API int sg_dev_free(sg_ctx* ctx, void* stream, void* d_ptr, uint64_t bytes);
 SG_API int sg_memcpy_h2d(sg_ctx* ctx, void* stream, void* d_dst, const void* src, uint64_t bytes);
 SG_API int sg_memcpy_d2h(sg_ctx* ctx, void* stream, void* dst, const void* d_src, uint64_t bytes);
 SG_API int sg_stream_sync(sg_ctx* ctx, void* stream);
+/* Non-blocking CUDA streams owned by the caller (one per concurrent table driver,
+ * the reference's 32-stream pool, device.rs:139-143,500-503). */
+SG_API int sg_stream_create(sg_ctx* ctx, void** stream_out);
+SG_API int sg_stream_destroy(sg_ctx* ctx, void* stream);
 /* Page-locked host memory for fast transfers. */
 SG_API int sg_host_alloc(uint64_t bytes, void** out);
 SG_API int sg_host_free(void* p);
@@ -298,6 +304,13 @@ SG_API int sg_eval_constraints(sg_ctx* ctx, void* stream, const sg_device_progra
  *      d_out: lde_rows/2 rows of [H0, H1] (6 u64 per row). ---- */
 SG_API int sg_decompose_d2(sg_ctx* ctx, void* stream, const uint64_t* d_h, uint64_t lde_rows, const uint64_t* d_inv_2x,
                            uint64_t* d_out);
+
+/* ---- synthetic chip-table trace (benchmark input generator; no counterpart in the
+ *      reference, whose traces come from the VM executor): n x w row-major,
+ *      element (r, c) = splitmix64(splitmix64(seed) + r*w + c) mod p, column w-2 a
+ *      16-bit multiplicity, column w-1 = sum_{j<k} c_j(r) c_j(r+1 mod n). ---- */
+SG_API int sg_synth_trace(sg_ctx* ctx, void* stream, uint64_t* d_out, uint64_t n, uint64_t w, uint64_t seed,
+                          uint32_t k_checksum);
 
 #ifdef __cplusplus
 }

@@ -13,7 +13,8 @@ Constraints (all cyclic over the n rows, zerofier x^n - 1):
     absorbed into the accumulated column's constraint; fingerprints are
     fp = z - (bus + sum_i alpha^(i+1) v_i) (lookup.rs:2160-2183).
 Boundary: the accumulated column is 0 at row 0 (lookup.rs:1330-1340).
-Composition degree 3 -> two composition parts (needs blowup >= 4).
+Composition degree 3 -> two composition parts; H = C/Z has degree < 2n, so
+blowup 2 already gives enough evaluation points.
 """
 import numpy as np
 
@@ -22,6 +23,15 @@ from .ir import Builder
 
 P = F.P
 NEG_ONE = P - 1
+
+
+def splitmix64(x):
+    x = np.asarray(x, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        z = x + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
 
 
 def split_interactions(k):
@@ -138,6 +148,21 @@ class SynthTableAir:
 
     # ---------------------------------------------------------- trace
     def trace(self, seed):
+        """Counter-based synthetic trace (identical to sg_synth_trace on the device)."""
+        n, w = self.n, self.width
+        key = splitmix64(np.array([seed], np.uint64))[0]
+        with np.errstate(over="ignore"):
+            idx = key + np.arange(n * w, dtype=np.uint64)
+        v = splitmix64(idx).reshape(n, w)
+        t = F.canon(v)
+        t[:, self.mult_col] = v[:, self.mult_col] & np.uint64(0xFFFF)
+        s = np.zeros(n, np.uint64)
+        for j in range(self.k):
+            s = F.add(s, F.mul(t[:, j], np.roll(t[:, j], -1)))
+        t[:, self.sum_col] = s
+        return np.ascontiguousarray(t)
+
+    def trace_random(self, seed):
         rng = np.random.default_rng(seed)
         n, w = self.n, self.width
         t = rng.integers(0, 2**64, size=(n, w), dtype=np.uint64)

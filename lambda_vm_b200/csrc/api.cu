@@ -118,6 +118,8 @@ int sg_ctx_memory(sg_ctx* c, uint64_t* in_use, uint64_t* peak) {
 
 uint64_t sg_ctx_launches(sg_ctx* c) { return c ? C(c)->launches.load() : 0; }
 
+uint64_t sg_ctx_budget(sg_ctx* c) { return c ? C(c)->budget : 0; }
+
 int sg_ctx_fail_alloc_after(sg_ctx* c, int64_t n) {
     SG_CHECK_ARG(c && n >= 0, "bad argument");
     C(c)->fail_alloc_after.store(n == 0 ? -1 : n);
@@ -151,6 +153,20 @@ int sg_memcpy_d2h(sg_ctx* c, void* stream, void* dst, const void* src, uint64_t 
 int sg_stream_sync(sg_ctx* c, void* stream) {
     SG_CHECK_ARG(c, "null context");
     SG_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    return SG_OK;
+}
+
+int sg_stream_create(sg_ctx* c, void** out) {
+    SG_CHECK_ARG(c && out, "null argument");
+    cudaStream_t st;
+    SG_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    *out = (void*)st;
+    return SG_OK;
+}
+
+int sg_stream_destroy(sg_ctx* c, void* stream) {
+    SG_CHECK_ARG(c, "null context");
+    if (stream) SG_CUDA(cudaStreamDestroy((cudaStream_t)stream));
     return SG_OK;
 }
 

@@ -145,38 +145,72 @@ static int batch_inv_launch(Ctx* ctx, cudaStream_t st, Load load, uint64_t total
 // out_partial[(chunk * K + k) * cols + c] = sum over the chunk's rows i of
 //   points[i] * col_c(row i*stride) * inv_denoms[k][i]
 #define BARY_MAX_K 8
-template <bool EXT3>
-__global__ void __launch_bounds__(128) k_bary(const uint64_t* data, uint64_t row_u64, uint64_t stride, uint64_t cols,
-                                              const uint64_t* points, const uint64_t* invd, uint64_t n, uint32_t K,
-                                              uint64_t chunk_len, uint64_t* partial) {
-    const uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const uint64_t chunk = blockIdx.y;
-    if (c >= cols) return;
-    fe3 acc[BARY_MAX_K];
+// Block = RL row lanes x CT columns (thread t: lane t / CT, column t % CT of
+// the block's column tile). Lane r walks rows i0+r, i0+r+RL, ... of the
+// chunk, so narrow tables still fill the block and each warp reads whole
+// row segments. The lanes' sums meet in shared memory; one partial per
+// (chunk, k, column) goes to k_bary_combine.
+template <bool EXT3, int K>
+__global__ void __launch_bounds__(512) k_bary(const uint64_t* __restrict__ data, uint64_t row_u64, uint64_t stride,
+                                              uint64_t cols, uint32_t CT, uint32_t RL,
+                                              const uint64_t* __restrict__ points,
+                                              const uint64_t* __restrict__ invd, uint64_t n, uint64_t chunk_len,
+                                              uint64_t* __restrict__ partial) {
+    extern __shared__ uint64_t bary_sm[];  // [RL][CT][K] ext3
+    const uint32_t lane = threadIdx.x / CT, cl = threadIdx.x % CT;
+    const uint64_t c = (uint64_t)blockIdx.x * CT + cl;
+    const bool active = lane < RL && c < cols;
+    fe3 acc[K];
 #pragma unroll
-    for (int k = 0; k < BARY_MAX_K; ++k) acc[k] = zero3();
-    const uint64_t i0 = chunk * chunk_len, i1 = min(n, i0 + chunk_len);
-    for (uint64_t i = i0; i < i1; ++i) {
-        const uint64_t* row = data + i * stride * row_u64;
-        const uint64_t pt = __ldg(points + i);
-        fe3 pe;
-        if (EXT3) {
-            pe = gl::mulb3(ld3(row + 3 * c), pt);
-        } else {
-            pe = fe3{gl::mul(row[c], pt), 0, 0};
-        }
+    for (int k = 0; k < K; ++k) acc[k] = zero3();
+    const uint64_t i0 = blockIdx.y * chunk_len, i1 = min(n, i0 + chunk_len);
+    if (active) {
+#pragma unroll 4
+        for (uint64_t i = i0 + lane; i < i1; i += RL) {
+            const uint64_t* row = data + i * stride * row_u64;
+            const uint64_t pt = __ldg(points + i);
+            fe3 pe;
+            if (EXT3)
+                pe = gl::mulb3(fe3{__ldg(row + 3 * c), __ldg(row + 3 * c + 1), __ldg(row + 3 * c + 2)}, pt);
+            else
+                pe = fe3{gl::mul(__ldg(row + c), pt), 0, 0};
 #pragma unroll
-        for (int k = 0; k < BARY_MAX_K; ++k) {
-            if (k < (int)K) {
-                const fe3 d = fe3{__ldg(invd + 3 * (k * n + i)), __ldg(invd + 3 * (k * n + i) + 1),
-                                  __ldg(invd + 3 * (k * n + i) + 2)};
+            for (int k = 0; k < K; ++k) {
+                const uint64_t* dp = invd + 3 * (k * n + i);
+                const fe3 d{__ldg(dp), __ldg(dp + 1), __ldg(dp + 2)};
                 acc[k] = gl::add3(acc[k], EXT3 ? gl::mul3(pe, d) : gl::mulb3(d, pe.c0));
             }
         }
     }
+    if (lane < RL) {
 #pragma unroll
-    for (int k = 0; k < BARY_MAX_K; ++k)
-        if (k < (int)K) st3(partial + 3 * ((chunk * K + k) * cols + c), acc[k]);
+        for (int k = 0; k < K; ++k) st3(bary_sm + 3 * (((uint64_t)lane * CT + cl) * K + k), acc[k]);
+    }
+    __syncthreads();
+    if (lane == 0 && c < cols) {
+        for (uint32_t r = 1; r < RL; ++r) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) acc[k] = gl::add3(acc[k], ld3(bary_sm + 3 * (((uint64_t)r * CT + cl) * K + k)));
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k) st3(partial + 3 * ((blockIdx.y * (uint64_t)K + k) * cols + c), acc[k]);
+    }
+}
+
+typedef void (*bary_fn)(const uint64_t*, uint64_t, uint64_t, uint64_t, uint32_t, uint32_t, const uint64_t*,
+                        const uint64_t*, uint64_t, uint64_t, uint64_t*);
+template <bool EXT3>
+static bary_fn bary_kernel(uint32_t K) {
+    switch (K) {
+        case 1: return k_bary<EXT3, 1>;
+        case 2: return k_bary<EXT3, 2>;
+        case 3: return k_bary<EXT3, 3>;
+        case 4: return k_bary<EXT3, 4>;
+        case 5: return k_bary<EXT3, 5>;
+        case 6: return k_bary<EXT3, 6>;
+        case 7: return k_bary<EXT3, 7>;
+        default: return k_bary<EXT3, 8>;
+    }
 }
 
 __global__ void k_bary_combine(const uint64_t* partial, uint64_t chunks, uint64_t per_chunk, uint64_t* out) {
@@ -188,57 +222,71 @@ __global__ void k_bary_combine(const uint64_t* partial, uint64_t chunks, uint64_
 }
 
 // ---------------------------------------------------------------- DEEP
-// One warp per LDE row: lanes split the row's columns, so every load is a
-// coalesced row segment; per-lane partial sums are warp-reduced.
+// One thread per LDE row, templated on the number K of trace opening points:
 //   result = inv_h * (sum_j g_j H_j(x) - c_h)
 //          + sum_k inv_t[k] * (sum_j g'_{jk} t_j(x) - c_k)
 // with c_h = sum_j g_j H_j(z^P) and c_k = sum_j g'_{jk} t_j(z w^k) folded on
 // the host: the same field value as summing g (t - t_ood) term by term.
+// The coefficient loads are uniform across the warp (broadcast); each
+// thread streams its own row, whose 32-byte sectors stay in L1 across the
+// four consecutive column reads that share them.
 #define DEEP_MAX_K 8
-__global__ void __launch_bounds__(256) k_deep(const uint64_t* main, uint64_t m, const uint64_t* aux, uint64_t A,
-                                              const uint64_t* parts, uint64_t P, uint64_t rows, uint32_t log_rows,
-                                              const uint64_t* gam_h, const uint64_t* gam_tr, uint32_t K,
-                                              const uint64_t* consts, const uint64_t* inv_h, const uint64_t* inv_t,
-                                              int bitrev_out, uint64_t* out) {
-    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (warp >= rows) return;
-    const uint64_t i = warp;
-    fe3 sk[DEEP_MAX_K];
+template <int K>
+__global__ void __launch_bounds__(128) k_deep(const uint64_t* __restrict__ main, uint64_t m,
+                                              const uint64_t* __restrict__ aux, uint64_t A,
+                                              const uint64_t* __restrict__ parts, uint64_t P, uint64_t rows,
+                                              uint32_t log_rows, const uint64_t* __restrict__ gam_h,
+                                              const uint64_t* __restrict__ gam_tr, const uint64_t* __restrict__ consts,
+                                              const uint64_t* __restrict__ inv_h, const uint64_t* __restrict__ inv_t,
+                                              int bitrev_out, uint64_t* __restrict__ out) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= rows) return;
+    fe3 sk[K > 0 ? K : 1];
 #pragma unroll
-    for (int k = 0; k < DEEP_MAX_K; ++k) sk[k] = zero3();
-    fe3 sh = zero3();
+    for (int k = 0; k < K; ++k) sk[k] = zero3();
     const uint64_t* mrow = main + i * m;
-    for (uint64_t j = lane; j < m; j += 32) {
-        const uint64_t t = mrow[j];
+    for (uint64_t j = 0; j < m; ++j) {
+        const uint64_t t = __ldg(mrow + j);
+        const uint64_t* g = gam_tr + 3 * j * K;
 #pragma unroll
-        for (int k = 0; k < DEEP_MAX_K; ++k)
-            if (k < (int)K) sk[k] = gl::add3(sk[k], gl::mulb3(ld3(gam_tr + 3 * (j * K + k)), t));
+        for (int k = 0; k < K; ++k)
+            sk[k] = gl::add3(sk[k], gl::mulb3(fe3{__ldg(g + 3 * k), __ldg(g + 3 * k + 1), __ldg(g + 3 * k + 2)}, t));
     }
     const uint64_t* arow = aux + i * A * 3;
-    for (uint64_t j = lane; j < A; j += 32) {
-        const fe3 t = ld3(arow + 3 * j);
+    for (uint64_t j = 0; j < A; ++j) {
+        const fe3 t{__ldg(arow + 3 * j), __ldg(arow + 3 * j + 1), __ldg(arow + 3 * j + 2)};
+        const uint64_t* g = gam_tr + 3 * (m + j) * K;
 #pragma unroll
-        for (int k = 0; k < DEEP_MAX_K; ++k)
-            if (k < (int)K) sk[k] = gl::add3(sk[k], gl::mul3(ld3(gam_tr + 3 * ((m + j) * K + k)), t));
+        for (int k = 0; k < K; ++k)
+            sk[k] = gl::add3(sk[k], gl::mul3(fe3{__ldg(g + 3 * k), __ldg(g + 3 * k + 1), __ldg(g + 3 * k + 2)}, t));
     }
+    fe3 sh = zero3();
     const uint64_t* prow = parts + i * P * 3;
-    for (uint64_t j = lane; j < P; j += 32) sh = gl::add3(sh, gl::mul3(ld3(gam_h + 3 * j), ld3(prow + 3 * j)));
+    for (uint64_t j = 0; j < P; ++j)
+        sh = gl::add3(sh, gl::mul3(fe3{__ldg(gam_h + 3 * j), __ldg(gam_h + 3 * j + 1), __ldg(gam_h + 3 * j + 2)},
+                                   fe3{__ldg(prow + 3 * j), __ldg(prow + 3 * j + 1), __ldg(prow + 3 * j + 2)}));
+    fe3 r = gl::mul3(ld3(inv_h + 3 * i), gl::sub3(sh, ld3(consts)));
 #pragma unroll
-    for (int off = 16; off >= 1; off >>= 1) {
-        sh = gl::add3(sh, shfl_down3(sh, off));
-#pragma unroll
-        for (int k = 0; k < DEEP_MAX_K; ++k)
-            if (k < (int)K) sk[k] = gl::add3(sk[k], shfl_down3(sk[k], off));
-    }
-    if (lane == 0) {
-        fe3 r = gl::mul3(ld3(inv_h + 3 * i), gl::sub3(sh, ld3(consts)));
-#pragma unroll
-        for (int k = 0; k < DEEP_MAX_K; ++k)
-            if (k < (int)K)
-                r = gl::add3(r, gl::mul3(ld3(inv_t + 3 * (k * rows + i)), gl::sub3(sk[k], ld3(consts + 3 * (1 + k)))));
-        const uint64_t o = bitrev_out ? (log_rows ? (__brevll(i) >> (64 - log_rows)) : 0) : i;
-        st3(out + 3 * o, gl::canon3(r));
+    for (int k = 0; k < K; ++k)
+        r = gl::add3(r, gl::mul3(ld3(inv_t + 3 * (k * rows + i)), gl::sub3(sk[k], ld3(consts + 3 * (1 + k)))));
+    const uint64_t o = bitrev_out ? (log_rows ? (__brevll(i) >> (64 - log_rows)) : 0) : i;
+    st3(out + 3 * o, gl::canon3(r));
+}
+
+typedef void (*deep_fn)(const uint64_t*, uint64_t, const uint64_t*, uint64_t, const uint64_t*, uint64_t, uint64_t,
+                        uint32_t, const uint64_t*, const uint64_t*, const uint64_t*, const uint64_t*, const uint64_t*,
+                        int, uint64_t*);
+static deep_fn deep_kernel(uint32_t K) {
+    switch (K) {
+        case 0: return k_deep<0>;
+        case 1: return k_deep<1>;
+        case 2: return k_deep<2>;
+        case 3: return k_deep<3>;
+        case 4: return k_deep<4>;
+        case 5: return k_deep<5>;
+        case 6: return k_deep<6>;
+        case 7: return k_deep<7>;
+        default: return k_deep<8>;
     }
 }
 
@@ -481,21 +529,26 @@ int sg_barycentric_sums(sg_ctx* c, void* stream, const uint64_t* d_data, uint64_
         SG_CUDA(cudaMemsetAsync(d_out, 0, 24ull * k * cols, st));
         return SG_OK;
     }
-    const uint64_t ctiles = (cols + 127) / 128;
-    uint64_t chunks = (148 * 8 + ctiles - 1) / ctiles;
-    if (chunks > n) chunks = n;
+    // Column tile of at most 512 threads; row lanes fill the block to >= 256 threads.
+    const uint64_t ctiles = (cols + 511) / 512;
+    const uint32_t CT = (uint32_t)((cols + ctiles - 1) / ctiles);
+    const uint32_t RL = CT >= 256 ? 1u : 256u / CT;
+    const uint32_t threads = (RL * CT + 31) / 32 * 32;
+    const size_t smem = 24ull * k * RL * CT;
+    // About four blocks of work per SM in total, each chunk at least RL rows.
+    uint64_t chunks = (148 * 4 + ctiles - 1) / ctiles;
+    const uint64_t max_chunks = (n + RL - 1) / RL;
+    if (chunks > max_chunks) chunks = max_chunks;
     if (chunks > 65535) chunks = 65535;
     const uint64_t chunk_len = (n + chunks - 1) / chunks;
     chunks = (n + chunk_len - 1) / chunk_len;
     uint64_t* part = nullptr;
     SG_TRY(dev_alloc(ctx, st, 24ull * chunks * k * cols, (void**)&part));
     dim3 grid((unsigned)ctiles, (unsigned)chunks);
-    if (ext3)
-        k_bary<true><<<grid, 128, 0, st>>>(d_data, row_u64, row_stride, cols, d_points, d_inv_denoms, n, k, chunk_len,
-                                           part);
-    else
-        k_bary<false><<<grid, 128, 0, st>>>(d_data, row_u64, row_stride, cols, d_points, d_inv_denoms, n, k, chunk_len,
-                                            part);
+    bary_fn fn = ext3 ? bary_kernel<true>(k) : bary_kernel<false>(k);
+    if (smem > 48 * 1024) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    fn<<<grid, threads, smem, st>>>(d_data, row_u64, row_stride, cols, CT, RL, d_points, d_inv_denoms, n, chunk_len,
+                                    part);
     int rc = check_launch(ctx, "k_bary");
     if (rc == SG_OK) {
         const uint64_t per = (uint64_t)k * cols;
@@ -552,11 +605,10 @@ int sg_deep_composition(sg_ctx* c, void* stream, const uint64_t* d_main, uint64_
         rc = SG_ERR_CUDA;
     }
     if (rc == SG_OK) {
-        const uint64_t threads = rows * 32;
-        k_deep<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(d_main, m, d_aux, a, d_parts, p, rows,
-                                                                  lr < 0 ? 0 : (uint32_t)lr, d_g, d_g + ng_h, k,
-                                                                  d_g + ng_h + ng_t, d_inv_h, d_inv_t, bitrev_out,
-                                                                  d_out);
+        deep_kernel(k)<<<(unsigned)((rows + 127) / 128), 128, 0, st>>>(d_main, m, d_aux, a, d_parts, p, rows,
+                                                                        lr < 0 ? 0 : (uint32_t)lr, d_g, d_g + ng_h,
+                                                                        d_g + ng_h + ng_t, d_inv_h, d_inv_t,
+                                                                        bitrev_out, d_out);
         rc = check_launch(ctx, "k_deep");
         // keep host vectors alive until the copies have been consumed
         if (rc == SG_OK && cudaStreamSynchronize(st) != cudaSuccess) {

@@ -28,6 +28,9 @@ class Backend:
         native.check(native.lib().sg_ctx_memory(self.h, C.byref(a), C.byref(b)))
         return a.value, b.value
 
+    def budget(self) -> int:
+        return native.lib().sg_ctx_budget(self.h)
+
     def launches(self) -> int:
         return native.lib().sg_ctx_launches(self.h)
 

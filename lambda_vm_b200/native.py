@@ -57,12 +57,15 @@ PROTOTYPES = {
     "sg_last_error": (C.c_char_p, []),
     "sg_ctx_memory": (i32, [vp, C.POINTER(u64), C.POINTER(u64)]),
     "sg_ctx_launches": (u64, [vp]),
+    "sg_ctx_budget": (u64, [vp]),
     "sg_ctx_fail_alloc_after": (i32, [vp, C.c_int64]),
     "sg_dev_alloc": (i32, [vp, vp, u64, C.POINTER(vp)]),
     "sg_dev_free": (i32, [vp, vp, vp, u64]),
     "sg_memcpy_h2d": (i32, [vp, vp, vp, vp, u64]),
     "sg_memcpy_d2h": (i32, [vp, vp, vp, vp, u64]),
     "sg_stream_sync": (i32, [vp, vp]),
+    "sg_stream_create": (i32, [vp, C.POINTER(vp)]),
+    "sg_stream_destroy": (i32, [vp, vp]),
     "sg_host_alloc": (i32, [u64, C.POINTER(vp)]),
     "sg_host_free": (i32, [vp]),
     "sg_ntt_forward": (i32, [vp, vp, vp, u64, u64]),
@@ -100,6 +103,7 @@ PROTOTYPES = {
     "sg_logup_aux": (i32, [vp, vp, vp, u64, u64, vp, vp, u32, vp, vp, vp]),
     "sg_eval_constraints": (i32, [vp, vp, vp, vp, u32, vp, u32, vp, vp, u64, vp, u64, u64, u64, vp, vp]),
     "sg_decompose_d2": (i32, [vp, vp, vp, u64, vp, vp]),
+    "sg_synth_trace": (i32, [vp, vp, vp, u64, u64, u64, u32]),
 }
 SG_STATIC_SCRATCH_BYTES = 32 << 20
 

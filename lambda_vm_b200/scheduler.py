@@ -1,0 +1,155 @@
+"""Table scheduler: concurrent per-table drivers under an HBM budget.
+
+Restates the reference's scheduling (crypto/stark/src/prover.rs:620-790):
+heaviest-first ordering (`heaviest_first`, :785), k concurrent table drivers
+(`run_admitted`, :749-783) each admitted by a byte budget (`VramGate`,
+:697-747; estimate `estimate_table_vram_bytes`, :682-695). Each driver owns a
+non-blocking CUDA stream, so small tables overlap on the device instead of
+running one after another behind host round trips; ctypes releases the GIL
+during every C-ABI call, so drivers run concurrently on the host too.
+
+The protocol is unchanged: R1 commits run concurrently but their roots are
+absorbed in table order, and every table's rounds 2-4 run on its own
+transcript fork, so the proof is identical to the sequential prover's.
+"""
+import ctypes as C
+import threading
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+
+from . import field as F
+from . import native
+from .device import backend as _backend
+from .ir import lower
+from .stark import GpuBackend, Options, _gen_trace, _u64le, prove_table
+
+
+class VramGate:
+    def __init__(self, budget_bytes):
+        self.budget = budget_bytes
+        self.used = 0
+        self.cv = threading.Condition()
+
+    def acquire(self, nbytes):
+        with self.cv:
+            # an oversized table runs alone rather than deadlocking
+            while self.used > 0 and self.used + nbytes > self.budget:
+                self.cv.wait()
+            self.used += nbytes
+
+    def release(self, nbytes):
+        with self.cv:
+            self.used -= nbytes
+            self.cv.notify_all()
+
+
+def estimate_table_bytes(air, opts):
+    """Device bytes a table's rounds 2-4 allocate beyond its resident main LDE."""
+    N = air.n * opts.blowup
+    W = air.aux_width
+    per_row = 8 * (3 * W) + 8 * 6 + 24 + 24 + 24 + 24 + 24 + 48 + 24  # aux, parts, H, halves, DEEP, FRI, inv_t, inv_h
+    return N * per_row + air.n * 3 * W * 8
+
+
+def heaviest_first(airs, opts):
+    return sorted(range(len(airs)), key=lambda i: -(airs[i].n * opts.blowup * (airs[i].width + 3 * airs[i].aux_width)))
+
+
+class StreamPool:
+    def __init__(self, be, k):
+        self.be = be
+        L = native.lib()
+        self.streams = []
+        for _ in range(k):
+            s = C.c_void_p()
+            native.check(L.sg_stream_create(be.h, C.byref(s)))
+            self.streams.append(s.value)
+        self.free = [GpuBackend(be, s) for s in self.streams]
+        self.lock = threading.Lock()
+
+    def take(self):
+        with self.lock:
+            return self.free.pop()
+
+    def give(self, bk):
+        with self.lock:
+            self.free.append(bk)
+
+    def close(self):
+        L = native.lib()
+        for s in self.streams:
+            L.sg_stream_sync(self.be.h, s)
+            L.sg_stream_destroy(self.be.h, s)
+        self.streams = []
+
+
+def multi_prove_scheduled(airs, sources, opts=None, workers=8, budget_bytes=None, be=None,
+                          label=b"lambda_vm_b200/synthetic-multi-table"):
+    """Same proof as stark.multi_prove, with k concurrent table drivers."""
+    opts = opts or Options()
+    be = be or _backend()
+    B, g = opts.blowup, opts.coset_offset
+    base = GpuBackend(be)
+    for air in airs:  # warm the domain caches serially on the legacy stream
+        base.domain(air.log_n, B, g)
+    native.check(native.lib().sg_stream_sync(be.h, None))
+    pool = StreamPool(be, workers)
+    order = heaviest_first(airs, opts)
+    r1 = [None] * len(airs)
+
+    def commit(i):
+        bk = pool.take()
+        try:
+            tm = _gen_trace(bk, airs[i], sources[i])
+            lde = bk.lde(tm, B, bk.domain(airs[i].log_n, B, g).weights)
+            tree, root = bk.commit(lde)  # synchronizes this stream (root readback)
+            r1[i] = (tm, lde, tree, root)
+        finally:
+            pool.give(bk)
+
+    try:
+        with ThreadPoolExecutor(workers) as ex:
+            list(ex.map(commit, order))
+        t = base.transcript(label)
+        for i in range(len(airs)):
+            t.append_bytes(r1[i][3])
+        challenges = [F.f3(t.sample_ext3()), F.f3(t.sample_ext3())]
+        alpha = challenges[1]
+        alpha_pows = [(1, 0, 0)]
+        for _ in range(max(a.max_alpha for a in airs) - 1):
+            alpha_pows.append(F.f3mul(alpha_pows[-1], alpha))
+        forks = []
+        for i in range(len(airs)):
+            ti = t.clone()
+            if len(airs) > 1:
+                ti.append_bytes(_u64le(i))
+            forks.append(ti)
+        in_use, _ = be.memory()
+        budget = budget_bytes if budget_bytes is not None else be.budget() - in_use
+        gate = VramGate(max(budget, 1 << 30))
+        proofs = [None] * len(airs)
+
+        def rounds(i):
+            est = estimate_table_bytes(airs[i], opts)
+            gate.acquire(est)
+            bk = pool.take()
+            try:
+                tm, lde, tree, root = r1[i]
+                p = prove_table(bk, airs[i], lower(airs[i].program), tm, lde, tree, forks[i], challenges, alpha_pows,
+                                opts)
+                p["main_root"] = root
+                # The R1 buffers were allocated on another driver's stream and are
+                # released on that stream: finish this stream's use of them first.
+                native.check(bk.L.sg_stream_sync(bk.be.h, bk.st))
+                bk.free(tm, lde, tree)
+                proofs[i] = p
+            finally:
+                pool.give(bk)
+                gate.release(est)
+
+        with ThreadPoolExecutor(workers) as ex:
+            list(ex.map(rounds, order))
+        return {"tables": proofs, "challenges": challenges}
+    finally:
+        pool.close()

@@ -58,28 +58,43 @@ def fri_layout(lde_log, blowup_log, k):
             "effective_k": terminal_log - blowup_log}
 
 
+def _dft_int(a, w):
+    """Radix-2 DFT over Python ints: out[i] = sum_j a[j] w^(ij) mod p."""
+    n = len(a)
+    if n == 1:
+        return list(a)
+    w2 = w * w % P
+    ev, od = _dft_int(a[0::2], w2), _dft_int(a[1::2], w2)
+    out = [0] * n
+    t = 1
+    h = n // 2
+    for k in range(h):
+        x = od[k] * t % P
+        out[k] = (ev[k] + x) % P
+        out[k + h] = (ev[k] - x) % P
+        t = t * w % P
+    return out
+
+
 def terminal_coeffs(codeword_br, terminal_offset, eff_k):
     """coeffs_from_terminal_codeword (fri/terminal.rs:72-103): gather the
     size-2^k sub-coset from the bit-reversed codeword and interpolate it on
-    the coset terminal_offset * <w^blowup> (small, on the host)."""
+    the coset terminal_offset * <w^blowup>: c_i = o^-i / keep * sum_j v_j w^-ij."""
     ln = len(codeword_br)
     keep = 1 << eff_k
     blow = ln // keep
     lbits = ln.bit_length() - 1
-    sub = [F.f3(codeword_br[F.bitrev_int(mm * blow, lbits)]) for mm in range(keep)]
-    # evaluations at terminal_offset * w_keep^j ; coefficients by inverse DFT
-    w = F.root_of_unity(eff_k)
-    winv = F.inv_int(w) if keep > 1 else 1
-    kinv = F.inv_int(keep)
+    cw = np.asarray(codeword_br, np.uint64).reshape(-1, 3)
+    sub = [[int(v) % P for v in cw[F.bitrev_int(mm * blow, lbits)]] for mm in range(keep)]
+    winv = F.inv_int(F.root_of_unity(eff_k)) if keep > 1 else 1
     oinv = F.inv_int(terminal_offset)
-    coeffs = []
+    comps = [_dft_int([sub[j][c] for j in range(keep)], winv) for c in range(3)]
+    out = []
+    s = F.inv_int(keep)
     for i in range(keep):
-        acc = (0, 0, 0)
-        wi = pow(winv, i, P)
-        for j in range(keep):
-            acc = F.f3add(acc, F.f3scale(sub[j], pow(wi, j, P)))
-        coeffs.append(F.f3scale(acc, kinv * pow(oinv, i, P) % P))
-    return coeffs
+        out.append(tuple(comps[c][i] * s % P for c in range(3)))
+        s = s * oinv % P
+    return out
 
 
 # ====================================================================== GPU backend
@@ -108,6 +123,36 @@ class Tree:
         self.buf.close()
 
 
+_DOMAINS = {}
+_DOMAIN_LOCK = __import__("threading").Lock()
+
+
+class Domain:
+    pass
+
+
+def _build_domain(bk, log_n, B, g):
+    """Set-up vectors of one evaluation domain, as backend matrices."""
+    n = 1 << log_n
+    N = n * B
+    log_N = log_n + (B.bit_length() - 1)
+    d = Domain()
+    d.log_n, d.log_N, d.n, d.N = log_n, log_N, n, N
+    d.weights = bk.upload(F.coset_weights(n, g).reshape(-1, 1))
+    d.comp_weights = bk.upload(F.composition_weights(N // 2, g).reshape(-1, 1))
+    gn = F.pow_int(g, n)
+    wB = F.root_of_unity(B.bit_length() - 1)
+    d.z_inv = bk.inv_base(np.array([(gn * pow(wB, k, P) - 1) % P for k in range(B)], np.uint64))
+    pts_N = F.coset_points(log_N, g)
+    d.b_z_inv = bk.upload(bk.inv_base(F.sub(pts_N, np.uint64(1))).reshape(1, -1))  # 1/(x - 1)
+    d.inv2x = bk.upload(bk.inv_base(F.add(pts_N[: N // 2], pts_N[: N // 2])).reshape(-1, 1))
+    d.pts_N = bk.upload(pts_N.reshape(-1, 1))
+    d.pts_n = bk.upload(F.coset_points(log_n, g).reshape(-1, 1))
+    tw0 = bk.inv_base(pts_N[: N // 2][F.bitrev_indices(log_N - 1).astype(np.int64)])
+    d.tw0 = bk.upload(tw0.reshape(-1, 1))
+    return d
+
+
 class GpuBackend:
     name = "gpu"
 
@@ -134,11 +179,31 @@ class GpuBackend:
         return mat.buf.download(np.uint64, mat.rows * mat.cols).reshape(mat.rows, mat.cols)
 
     def lde(self, mat, blowup, weights):
-        dw = DeviceBuffer.from_host(np.ascontiguousarray(weights, np.uint64), self.be, self.st)
+        """Coset LDE; `weights` is a host array or a device Mat (cached domain weights)."""
+        dw = weights if isinstance(weights, Mat) else None
+        if dw is None:
+            dw = self.upload(np.ascontiguousarray(weights, np.uint64).reshape(-1, 1))
         out = self._alloc(mat.rows * blowup, mat.cols)
         native.check(self.L.sg_coset_lde(self.be.h, self.st, mat.ptr, mat.rows, mat.cols, blowup, dw.ptr, out.ptr))
-        dw.close()
+        if not isinstance(weights, Mat):
+            dw.free()
         return out
+
+    def domain(self, log_n, blowup, g):
+        """Per-domain set-up vectors, built once per (size, blowup, offset) and
+        shared by every table and proof on this context (the reference's
+        domain_and_twiddles cache, prover.rs:514-580)."""
+        key = (id(self.be), log_n, blowup, g)
+        with _DOMAIN_LOCK:
+            d = _DOMAINS.get(key)
+            if d is None:
+                saved, self.st = self.st, None  # build on the legacy stream, visible to all streams after sync
+                try:
+                    d = _build_domain(self, log_n, blowup, g)
+                finally:
+                    self.st = saved
+                _DOMAINS[key] = d
+            return d
 
     def commit(self, mat, rows_per_leaf=2, little_endian=False):
         nl = mat.rows // rows_per_leaf
@@ -314,16 +379,16 @@ def _ood_scale(z, n, g):
     return F.f3scale(F.f3sub(F.f3pow(z, n), (gn, 0, 0)), s)
 
 
-def prove_table(bk, air, lowered, trace_mat, main_lde, main_tree, t, challenges, alpha_pows, opts, stats=None):
+def prove_table(bk, air, lowered, trace_mat, main_lde, main_tree, t, challenges, alpha_pows, opts):
     """Aux build + rounds 2-4 for one table (prover.rs:3603-3977, 4433-4620)."""
     n, N = air.n, air.n * opts.blowup
     B, g = opts.blowup, opts.coset_offset
     log_n, log_N = air.log_n, air.log_n + (B.bit_length() - 1)
-    weights = F.coset_weights(n, g)
+    dom = bk.domain(log_n, B, g)
     proof = {}
     # ---- aux
     aux, Lc = bk.logup_aux(trace_mat, air.logup_descriptor(), alpha_pows, challenges[0])
-    aux_lde = bk.lde(aux, B, weights)
+    aux_lde = bk.lde(aux, B, dom.weights)
     bk.free(aux)
     aux_tree, aux_root = bk.commit(aux_lde)
     t.append_bytes(aux_root)
@@ -336,22 +401,13 @@ def prove_table(bk, air, lowered, trace_mat, main_lde, main_tree, t, challenges,
     for _ in range(ncons - 1):
         coefs.append(F.f3mul(coefs[-1], beta))
     beta_t, beta_b = coefs[:len(lowered["roots"])], coefs[len(lowered["roots"]):]
-    # zerofiers on the LDE coset x_k = g w_N^k: x^n = g^n w_B^k
-    gn = F.pow_int(g, n)
-    wB = F.root_of_unity(B.bit_length() - 1)
-    z_inv = bk.inv_base(np.array([(gn * pow(wB, k, P) - 1) % P for k in range(B)], np.uint64))
-    pts_N = F.coset_points(log_N, g)
-    b_z_inv_host = bk.inv_base(F.sub(pts_N, np.uint64(1)))  # acc boundary at row 0: 1/(x - 1)
-    b_z_inv = bk.upload(b_z_inv_host.reshape(1, -1))
     offset = F.f3scale(Lc, F.inv_int(n))
     boundary = [(col, is_aux, (0, 0, 0), beta_b[i]) for i, (col, is_aux, _row) in enumerate(air.boundary)]
-    H = bk.composition(air.program, lowered, main_lde, aux_lde, [challenges[0], challenges[1]], alpha_pows, offset, B, beta_t,
-                       z_inv, boundary, b_z_inv)
-    bk.free(b_z_inv)
-    inv2x = bk.upload(bk.inv_base(F.add(pts_N[: N // 2], pts_N[: N // 2])).reshape(-1, 1))
-    halves = bk.decompose(H, inv2x)
-    bk.free(H, inv2x)
-    parts_lde = bk.lde(halves, 2, F.composition_weights(N // 2, g))
+    H = bk.composition(air.program, lowered, main_lde, aux_lde, [challenges[0], challenges[1]], alpha_pows, offset, B,
+                       beta_t, dom.z_inv, boundary, dom.b_z_inv)
+    halves = bk.decompose(H, dom.inv2x)
+    bk.free(H)
+    parts_lde = bk.lde(halves, 2, dom.comp_weights)
     bk.free(halves)
     comp_tree, comp_root = bk.commit(parts_lde)
     t.append_bytes(comp_root)
@@ -361,12 +417,11 @@ def prove_table(bk, air, lowered, trace_mat, main_lde, main_tree, t, challenges,
     wn = F.root_of_unity(log_n)
     zw = F.f3scale(z, wn)
     z2 = F.f3mul(z, z)
-    pts_n = bk.upload(F.coset_points(log_n, g).reshape(-1, 1))
-    invd = bk.inv_denoms(pts_n, [z, zw, z2], False)
-    S_main = bk.bary(main_lde, B, False, air.width, pts_n, invd, n, 3)
-    S_aux = bk.bary(aux_lde, B, True, air.aux_width, pts_n, invd, n, 3)
-    S_parts = bk.bary(parts_lde, B, True, 2, pts_n, invd, n, 3)
-    bk.free(invd, pts_n)
+    invd = bk.inv_denoms(dom.pts_n, [z, zw, z2], False)
+    S_main = bk.bary(main_lde, B, False, air.width, dom.pts_n, invd, n, 3)
+    S_aux = bk.bary(aux_lde, B, True, air.aux_width, dom.pts_n, invd, n, 3)
+    S_parts = bk.bary(parts_lde, B, True, 2, dom.pts_n, invd, n, 3)
+    bk.free(invd)
     sc = [_ood_scale(p, n, g) for p in (z, zw, z2)]
     trace_ood = [[F.f3mul(sc[k], F.f3(S_main[k, c])) for c in range(air.width)] +
                  [F.f3mul(sc[k], F.f3(S_aux[k, c])) for c in range(air.aux_width)] for k in range(2)]
@@ -386,28 +441,26 @@ def prove_table(bk, air, lowered, trace_mat, main_lde, main_tree, t, challenges,
         gp.append(F.f3mul(gp[-1], gamma))
     gh, gt = gp[:2], gp[2:]
     trace_ood_jk = [trace_ood[k][j] for j in range(ncols) for k in range(2)]
-    ptsN = bk.upload(pts_N.reshape(-1, 1))
-    inv_h = bk.inv_denoms(ptsN, [z2], True)
-    inv_t = bk.inv_denoms(ptsN, [z, zw], True)
-    bk.free(ptsN)
+    inv_h = bk.inv_denoms(dom.pts_N, [z2], True)
+    inv_t = bk.inv_denoms(dom.pts_N, [z, zw], True)
     deep = bk.deep(main_lde, aux_lde, parts_lde, parts_ood, trace_ood_jk, gh, gt, inv_h, inv_t, 2)
     bk.free(inv_h, inv_t)
     # ---- FRI commit (fri/mod.rs:27-151)
     lay = fri_layout(log_N, B.bit_length() - 1, opts.final_log_degree)
-    half = N // 2
-    tw0 = bk.inv_base(F.coset_points(log_N, g)[:half][F.bitrev_indices(log_N - 1).astype(np.int64)])
-    tw = bk.upload(tw0.reshape(-1, 1))
+    tw, own_tw = dom.tw0, False
     ev = deep
     layers, fri_roots = [], []
     for _ in range(lay["num_committed"]):
         zeta = F.f3(t.sample_ext3())
         ev2, tw2, leaves = bk.fri_fold(ev, tw, zeta, True)
         tree, root = bk.tree_from_leaves(leaves, len(ev2) // 2)
-        bk.free(leaves, tw)
+        bk.free(leaves)
+        if own_tw:
+            bk.free(tw)
         layers.append((ev2, tree))
         fri_roots.append(root)
         t.append_bytes(root)
-        ev, tw = ev2, tw2
+        ev, tw, own_tw = ev2, tw2, True
     if lay["total_folds"] > 0:
         zeta = F.f3(t.sample_ext3())
         evf, twf, _ = bk.fri_fold(ev, tw, zeta, False)
@@ -416,7 +469,8 @@ def prove_table(bk, air, lowered, trace_mat, main_lde, main_tree, t, challenges,
         bk.free(evf)
     else:
         final = bk.to_host(ev)
-    bk.free(tw)
+    if own_tw:
+        bk.free(tw)
     term_off = F.pow_int(g, 1 << lay["total_folds"])
     coeffs = terminal_coeffs(final, term_off, lay["effective_k"])
     for c in coeffs:
@@ -428,7 +482,7 @@ def prove_table(bk, air, lowered, trace_mat, main_lde, main_tree, t, challenges,
     if opts.grinding:
         t.append_bytes(_u64be(nonce))
     proof["nonce"] = nonce
-    iotas = [t.sample_u64(half) for _ in range(opts.queries)]
+    iotas = [t.sample_u64(N // 2) for _ in range(opts.queries)]
     proof["iotas"] = iotas
     # ---- openings: leaf iota of each trace-side tree covers rows br(2i), br(2i+1)
     rows = []
@@ -457,16 +511,30 @@ def prove_table(bk, air, lowered, trace_mat, main_lde, main_tree, t, challenges,
     return proof
 
 
+def _gen_trace(bk, air, source):
+    """`source` is a host array, or an int seed for the counter-based synthetic
+    trace (generated on the device by the GPU backend, on the host otherwise)."""
+    if isinstance(source, (int, np.integer)):
+        if isinstance(bk, GpuBackend):
+            m = bk._alloc(air.n, air.width)
+            native.check(bk.L.sg_synth_trace(bk.be.h, bk.st, m.ptr, air.n, air.width, int(source), air.k))
+            return m
+        return bk.upload(air.trace(int(source)))
+    return bk.upload(source)
+
+
 def multi_prove(airs, traces, opts=None, bk=None, label=b"lambda_vm_b200/synthetic-multi-table"):
-    """Prove all tables of one multi-table statement; returns the proof dict."""
+    """Prove all tables of one multi-table statement, one table after another
+    (the plain form); returns the proof dict. `traces` holds host arrays or
+    int seeds of counter-based synthetic traces."""
     opts = opts or Options()
     bk = bk or GpuBackend()
     t = bk.transcript(label)
     B, g = opts.blowup, opts.coset_offset
     tabs = []
     for air, tr in zip(airs, traces):
-        tm = bk.upload(tr)
-        lde = bk.lde(tm, B, F.coset_weights(air.n, g))
+        tm = _gen_trace(bk, air, tr)
+        lde = bk.lde(tm, B, bk.domain(air.log_n, B, g).weights)
         tree, root = bk.commit(lde)
         tabs.append((air, tm, lde, tree, root))
     for _, _, _, _, root in tabs:

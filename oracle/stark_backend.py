@@ -71,6 +71,30 @@ class OracleBackend:
     def transcript(self, label):
         return O.Transcript(label)
 
+    def domain(self, log_n, blowup, g):
+        """Domain set-up vectors computed with the oracle (no cache)."""
+        class D:
+            pass
+        n, N = 1 << log_n, (1 << log_n) * blowup
+        log_N = N.bit_length() - 1
+        d = D()
+        d.weights = O.canon_array(O.coset_weights(n, g))
+        # composition weights g^-j / (N/2)
+        ginv, hinv = O.gl_inv(g), O.gl_inv(N // 2)
+        d.comp_weights = np.array([O.canonical(O.gl_mul(hinv, O.gl_pow(ginv, j))) for j in range(N // 2)], np.uint64)
+        wN, wn = O.root_of_unity(log_N), O.root_of_unity(log_n)
+        pts_N = np.array([O.canonical(O.gl_mul(g, O.gl_pow(wN, i))) for i in range(N)], np.uint64)
+        gn, wB = O.gl_pow(g, n), O.root_of_unity(blowup.bit_length() - 1)
+        d.z_inv = self.inv_base(np.array([O.gl_sub(O.gl_mul(gn, O.gl_pow(wB, k)), 1) for k in range(blowup)],
+                                         np.uint64))
+        d.b_z_inv = self.inv_base(np.array([O.gl_sub(int(x), 1) for x in pts_N], np.uint64)).reshape(1, -1)
+        d.inv2x = self.inv_base(np.array([O.gl_add(int(x), int(x)) for x in pts_N[: N // 2]], np.uint64)).reshape(-1, 1)
+        d.pts_N = pts_N.reshape(-1, 1)
+        d.pts_n = np.array([O.canonical(O.gl_mul(g, O.gl_pow(wn, i))) for i in range(n)], np.uint64).reshape(-1, 1)
+        br = [int(format(i, f"0{log_N - 1}b")[::-1], 2) if log_N > 1 else 0 for i in range(N // 2)]
+        d.tw0 = self.inv_base(pts_N[: N // 2][br]).reshape(-1, 1)
+        return d
+
     def upload(self, arr):
         a = np.ascontiguousarray(arr, np.uint64)
         return a.reshape(-1, 1).copy() if a.ndim == 1 else a.copy()
@@ -79,7 +103,7 @@ class OracleBackend:
         return m
 
     def lde(self, mat, blowup, weights):
-        return _c(O.coset_lde_row_major(mat, blowup, weights))
+        return _c(O.coset_lde_row_major(mat, blowup, np.asarray(weights).reshape(-1)))
 
     def commit(self, mat, rows_per_leaf=2, little_endian=False):
         nodes = O.merkle_nodes(O.leaves_row_major(mat, rows_per_leaf, little_endian))
