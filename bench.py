@@ -370,11 +370,19 @@ def main():
     # leaves read B*n*m*8 and write 32 B per leaf.
     alg = {"lde": (n * m + N * m) * 8, "leaves": N * m * 8 + nl * 32, "tree": (nl - 1) * 96}
     dom = max(med, key=med.get)
+    # DRAM bytes (read + written) of one LDE (its 4 k_dft launches), measured by
+    # ncu on the 2^20 x 16 x blowup-4 case and scaled by the column count;
+    # traffic grows in proportion to the columns (same passes, same tiles).
+    traffic, traffic_src = None, None
+    if dom == "lde" and a.log_n == 20 and B == 4:
+        traffic = round(2.105714944e9 * m / 16)
+        traffic_src = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the 4 k_dft launches of one "
+                       "2^20 x 16 blowup-4 LDE, x m/16 (profiles/k_dft_coset_lde_1048576x16_blowup4.md)")
     achieved = alg[dom] / (med[dom] * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": {"lde": "k_dft_pass (coset LDE, 4 launches)", "leaves": "k_leaves",
                                           "tree": "k_merkle_levels"}[dom],
                 "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
-                "peak_source": peak_src, "traffic": None,
+                "peak_source": peak_src, "traffic": traffic, "traffic_source": traffic_src,
                 "per_kernel_ms": {k: round(v, 3) for k, v in med.items()},
                 "per_kernel_gbs": {k: round(alg[k] / (med[k] * 1e-3) / 1e9, 1) for k in med},
                 "note": "Goldilocks butterflies and Keccak run on the INT pipes; see profiles/ for issue utilisation"}

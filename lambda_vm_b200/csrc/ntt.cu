@@ -117,15 +117,23 @@ struct PassArgs {
 };
 
 // Compile-time stage plan per tile length: radix exponents, columns per tile,
-// threads per CTA.
+// threads per CTA. A tile of 2^LOGL points runs NST register stages of at
+// most 2^QM points each (larger radices first).
+#ifndef SG_DFT_QMAX
+#define SG_DFT_QMAX 4
+#endif
+#ifndef SG_DFT_T10
+#define SG_DFT_T10 256
+#endif
 template <int LOGL>
 struct Plan {
-    static constexpr int NST = LOGL == 0 ? 0 : (LOGL <= 5 ? 1 : (LOGL <= 10 ? 2 : 3));
-    static constexpr int Q1 = NST == 1 ? LOGL : (NST == 2 ? (LOGL + 1) / 2 : 4);
-    static constexpr int Q2 = NST == 2 ? LOGL / 2 : (NST == 3 ? 4 : 0);
-    static constexpr int Q3 = NST == 3 ? LOGL - 8 : 0;
+    static constexpr int QM = SG_DFT_QMAX;
+    static constexpr int NST = LOGL == 0 ? 0 : (LOGL <= 5 ? 1 : ((LOGL + QM - 1) / QM < 2 ? 2 : (LOGL + QM - 1) / QM));
+    static constexpr int q(int s) { return NST == 0 ? 0 : LOGL / NST + (s < LOGL % NST ? 1 : 0); }
+    static constexpr int lgns(int s) { return s == 0 ? 0 : lgns(s - 1) + q(s - 1); }
+    static constexpr int Q1 = q(0);
     static constexpr int C = LOGL <= 7 ? 32 : (LOGL <= 9 ? 16 : (LOGL <= 11 ? 8 : 4));
-    static constexpr int T = LOGL >= 11 ? 512 : 256;
+    static constexpr int T = LOGL >= 11 ? 512 : (LOGL == 10 ? SG_DFT_T10 : 256);
     static constexpr uint32_t L = 1u << LOGL;
     static constexpr uint32_t CS0 = L + (NST > 1 ? (L >> Q1) : 0);
     static constexpr uint32_t CP = C < 16 ? C : 16;
@@ -135,6 +143,7 @@ struct Plan {
     static constexpr uint32_t WL_WORDS = NST > 1 ? L : 0;
     static constexpr uint32_t F_WORDS = NST > 1 ? L : 2 * L;  // one buffer reused for pre and post
     static constexpr size_t SMEM = (size_t)(S_WORDS + WL_WORDS + F_WORDS) * 8;
+    static_assert(NST < 2 || q(0) <= 5, "register stage wider than 32 points");
 };
 
 template <int LOGL>
@@ -174,6 +183,17 @@ __device__ __forceinline__ void mid_stage(uint64_t* S, const uint64_t* WL) {
         dit_reg<Q, INV>(v);
 #pragma unroll
         for (uint32_t r = 0; r < R; ++r) col[tpad<LOGL>(base + r * Ns)] = v[r];
+    }
+}
+
+// Stages 1 .. NST-2, each separated from the next by a barrier.
+template <int LOGL, int STG, bool INV>
+__device__ __forceinline__ void mid_stages(uint64_t* S, const uint64_t* WL) {
+    using PL = Plan<LOGL>;
+    if constexpr (STG < PL::NST - 1) {
+        if constexpr (STG > 1) __syncthreads();
+        mid_stage<LOGL, PL::q(STG), PL::lgns(STG), INV>(S, WL);
+        mid_stages<LOGL, STG + 1, INV>(S, WL);
     }
 }
 
@@ -259,12 +279,10 @@ __device__ __forceinline__ void tile_body(const PassArgs& a, uint64_t* S, const 
             for (uint32_t k = threadIdx.x; k < L; k += T)
                 Fpost[k] = a.weights[pt * a.out_ts + (uint64_t)k * a.out_ps + (uint64_t)rep * a.out_rs];
         }
-        if constexpr (PL::NST == 3) {
-            mid_stage<LOGL, PL::Q2, PL::Q1, INV>(S, WL);
-        }
+        mid_stages<LOGL, 1, INV>(S, WL);
         __syncthreads();
         // ---- last stage: smem -> registers -> HBM
-        constexpr int Q = PL::NST == 2 ? PL::Q2 : PL::Q3;
+        constexpr int Q = PL::q(PL::NST - 1);
         constexpr int LOGNS = LOGL - Q;
         constexpr uint32_t R = 1u << Q, Ns = 1u << LOGNS, items = C * Ns;
         for (uint32_t w = threadIdx.x; w < items; w += T) {
@@ -288,7 +306,7 @@ __device__ __forceinline__ void tile_body(const PassArgs& a, uint64_t* S, const 
 // One instantiation per (tile length, direction): each launch carries only the
 // butterfly code it runs, which keeps the unrolled networks in the I-cache.
 template <int LOGL, bool INV>
-__global__ void __launch_bounds__(Plan<LOGL>::T, Plan<LOGL>::T == 256 ? 2 : 1)
+__global__ void __launch_bounds__(Plan<LOGL>::T, Plan<LOGL>::T == 256 ? 2 : (LOGL == 10 ? 2 : 1))
     k_dft(PassArgs a, uint64_t ntiles, uint32_t ctiles) {
     using PL = Plan<LOGL>;
     extern __shared__ uint64_t sm[];
