@@ -157,6 +157,32 @@ SG_API int sg_lde_commit(sg_ctx* ctx, void* stream, const uint64_t* trace, int t
                   uint64_t* host_lde_out, sg_lde** out, uint8_t root_out[32]);
 SG_API int sg_lde_get_info(const sg_lde* lde, sg_lde_info* info);
 SG_API void sg_lde_free(sg_ctx* ctx, sg_lde* lde);
+/* Stream-ordered release of a handle: its memory returns to the pool after
+ * the work already queued on `stream`; no device-wide wait. */
+SG_API void sg_lde_free_async(sg_ctx* ctx, void* stream, sg_lde* lde);
+
+/* ---- batched commit: the batched form of the per-table commits that
+ *      crypto/stark/src/prover.rs:1132-1398 (commit_main_trace) runs through
+ *      coset_lde_row_major_with_merkle_tree_keep (crypto/math-cuda/src/lde.rs:674)
+ *      once per table, under the table scheduler (prover.rs:749-790).
+ *      Commits `count` tables in one call: heaviest first, spread over
+ *      `concurrency` internal streams that start after the work already on
+ *      `stream` and that `stream` waits for; returns when every root is on the
+ *      host. out_ldes[i] / roots_out[32*i] belong to tables[i], each identical
+ *      to what sg_lde_commit returns for that table alone. On failure no handle
+ *      is returned. ---- */
+typedef struct sg_table_desc {
+    const uint64_t* trace;   /* n x row_u64 row-major */
+    int trace_on_device;     /* nonzero: device pointer, else host */
+    uint64_t n;              /* power of two >= 2 */
+    uint64_t row_u64;
+    uint32_t blowup;         /* power of two */
+    int weights_on_device;   /* nonzero: device pointer, else host */
+    const uint64_t* weights; /* n coset weights g^i / n */
+    sg_leaf_layout layout;   /* rows_per_leaf == 0 selects {2, BE, all columns} */
+} sg_table_desc;
+SG_API int sg_batch_commit(sg_ctx* ctx, void* stream, const sg_table_desc* tables, uint32_t count,
+                           uint32_t concurrency, sg_lde** out_ldes, uint8_t* roots_out);
 
 /* ---- grinding: replaces grinding::generate_nonce_gpu (crypto/math-cuda/src/grinding.rs:29).
  *      inner_lanes: the 32-byte inner hash as four little-endian u64 lanes

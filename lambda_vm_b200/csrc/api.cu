@@ -2,7 +2,9 @@
 // The per-function reference correspondences are listed in include/starkgpu.h.
 #include <string.h>
 
+#include <algorithm>
 #include <string>
+#include <vector>
 
 #include "common.cuh"
 
@@ -247,13 +249,17 @@ int sg_merkle_build(sg_ctx* c, void* stream, const uint8_t* d_leaves, uint64_t n
     return SG_OK;
 }
 
-int sg_lde_commit(sg_ctx* c, void* stream, const uint64_t* trace, int trace_on_device, uint64_t n, uint64_t row_u64,
-                  uint32_t blowup, const uint64_t* weights, const sg_leaf_layout* layout, uint64_t* host_lde_out,
-                  sg_lde** out, uint8_t root_out[32]) {
-    SG_CHECK_ARG(c && out && trace && weights, "null argument");
+}  // extern "C"
+
+// Enqueue one table's commit on `st` without waiting on the host: weights and
+// trace upload (when given on the host), coset LDE, leaves, tree, and the root
+// copied to root_dst (pinned host memory, valid once `st` has drained). On
+// failure nothing stays allocated and *out is null.
+static int commit_enqueue(Ctx* ctx, cudaStream_t st, const uint64_t* trace, int trace_on_device, uint64_t n,
+                          uint64_t row_u64, uint32_t blowup, const uint64_t* weights, int weights_on_device,
+                          const sg_leaf_layout* layout, uint64_t* host_lde_out, sg_lde** out, uint8_t* root_dst) {
+    SG_CHECK_ARG(out && trace && weights, "null argument");
     *out = nullptr;
-    Ctx* ctx = C(c);
-    cudaStream_t st = (cudaStream_t)stream;
     SG_CHECK_ARG(n >= 2 && log2_exact(n) >= 0, "n must be a power of two >= 2");
     SG_CHECK_ARG(blowup >= 1 && log2_exact(blowup) >= 0, "blowup must be a power of two");
     SG_CHECK_ARG(row_u64 >= 1, "row width must be >= 1");
@@ -263,8 +269,7 @@ int sg_lde_commit(sg_ctx* c, void* stream, const uint64_t* trace, int trace_on_d
     SG_TRY(resolve_layout(layout, row_u64, &R, &le, &c0, &c1));
     const uint64_t lde_rows = n * blowup;
     SG_CHECK_ARG(lde_rows % R == 0, "rows_per_leaf must divide the LDE size");
-    const uint64_t num_leaves = lde_rows / R;
-    const uint64_t L = num_leaves;  // power of two
+    const uint64_t L = lde_rows / R;  // power of two
     sg_lde* h = new sg_lde();
     h->lde_rows = lde_rows;
     h->row_u64 = row_u64;
@@ -278,12 +283,16 @@ int sg_lde_commit(sg_ctx* c, void* stream, const uint64_t* trace, int trace_on_d
         if (rc) break;
         rc = dev_alloc(ctx, st, (2 * L - 1) * 32, (void**)&h->d_nodes);
         if (rc) break;
-        rc = dev_alloc(ctx, st, n * 8, (void**)&d_w);
-        if (rc) break;
-        if (cudaMemcpyAsync(d_w, weights, n * 8, cudaMemcpyHostToDevice, st) != cudaSuccess) {
-            set_error("weights upload failed");
-            rc = SG_ERR_CUDA;
-            break;
+        const uint64_t* w = weights;
+        if (!weights_on_device) {
+            rc = dev_alloc(ctx, st, n * 8, (void**)&d_w);
+            if (rc) break;
+            if (cudaMemcpyAsync(d_w, weights, n * 8, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+                set_error("weights upload failed");
+                rc = SG_ERR_CUDA;
+                break;
+            }
+            w = d_w;
         }
         const uint64_t* src = trace;
         if (!trace_on_device) {
@@ -296,13 +305,13 @@ int sg_lde_commit(sg_ctx* c, void* stream, const uint64_t* trace, int trace_on_d
             }
             src = d_trace;
         }
-        rc = coset_lde(ctx, st, src, n, row_u64, blowup, d_w, h->d_lde);
+        rc = coset_lde(ctx, st, src, n, row_u64, blowup, w, h->d_lde);
         if (rc) break;
         rc = leaves_row_major(ctx, st, h->d_lde, lde_rows, row_u64, c0, c1, R, le, h->d_nodes + (L - 1) * 32);
         if (rc) break;
         rc = merkle_inner(ctx, st, h->d_nodes, L);
         if (rc) break;
-        if (cudaMemcpyAsync(h->root, h->d_nodes, 32, cudaMemcpyDeviceToHost, st) != cudaSuccess) {
+        if (cudaMemcpyAsync(root_dst, h->d_nodes, 32, cudaMemcpyDeviceToHost, st) != cudaSuccess) {
             set_error("root download failed");
             rc = SG_ERR_CUDA;
             break;
@@ -313,13 +322,8 @@ int sg_lde_commit(sg_ctx* c, void* stream, const uint64_t* trace, int trace_on_d
             rc = SG_ERR_CUDA;
             break;
         }
-        cudaError_t e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) {
-            set_error(std::string("lde commit: ") + cudaGetErrorString(e));
-            rc = SG_ERR_CUDA;
-            break;
-        }
     } while (0);
+    // Stream-ordered frees: the memory returns to the pool after the kernels that read it.
     if (d_trace) dev_free(ctx, st, d_trace, trace_bytes);
     if (d_w) dev_free(ctx, st, d_w, n * 8);
     if (rc != SG_OK) {
@@ -328,9 +332,131 @@ int sg_lde_commit(sg_ctx* c, void* stream, const uint64_t* trace, int trace_on_d
         delete h;
         return rc;
     }
+    *out = h;
+    return SG_OK;
+}
+
+namespace {
+// Page-locked 32-byte root slots for asynchronous root copies.
+struct PinnedRoots {
+    uint8_t* p = nullptr;
+    ~PinnedRoots() {
+        if (p) cudaFreeHost(p);
+    }
+};
+}  // namespace
+
+extern "C" {
+
+int sg_lde_commit(sg_ctx* c, void* stream, const uint64_t* trace, int trace_on_device, uint64_t n, uint64_t row_u64,
+                  uint32_t blowup, const uint64_t* weights, const sg_leaf_layout* layout, uint64_t* host_lde_out,
+                  sg_lde** out, uint8_t root_out[32]) {
+    SG_CHECK_ARG(c && out, "null argument");
+    *out = nullptr;
+    Ctx* ctx = C(c);
+    cudaStream_t st = (cudaStream_t)stream;
+    PinnedRoots pr;
+    SG_CUDA(cudaMallocHost((void**)&pr.p, 32));
+    sg_lde* h = nullptr;
+    SG_TRY(commit_enqueue(ctx, st, trace, trace_on_device, n, row_u64, blowup, weights, 0, layout, host_lde_out, &h,
+                          pr.p));
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        set_error(std::string("lde commit: ") + cudaGetErrorString(e));
+        sg_lde_free(c, h);
+        return SG_ERR_CUDA;
+    }
+    memcpy(h->root, pr.p, 32);
     if (root_out) memcpy(root_out, h->root, 32);
     *out = h;
     return SG_OK;
+}
+
+int sg_batch_commit(sg_ctx* c, void* stream, const sg_table_desc* tables, uint32_t count, uint32_t concurrency,
+                    sg_lde** out_ldes, uint8_t* roots_out) {
+    SG_CHECK_ARG(c && (count == 0 || (tables && out_ldes)), "null argument");
+    for (uint32_t i = 0; i < count; ++i) out_ldes[i] = nullptr;
+    if (count == 0) return SG_OK;
+    Ctx* ctx = C(c);
+    cudaStream_t caller = (cudaStream_t)stream;
+    // Heaviest first (crypto/stark/src/prover.rs:785): the long tables start
+    // at once and the short ones fill the gaps behind them.
+    std::vector<uint32_t> order(count);
+    for (uint32_t i = 0; i < count; ++i) order[i] = i;
+    auto weight = [&](uint32_t i) { return (double)tables[i].n * tables[i].blowup * tables[i].row_u64; };
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return weight(x) > weight(y); });
+    uint32_t k = concurrency == 0 ? 1 : concurrency;
+    if (k > count) k = count;
+    if (k > 32) k = 32;
+    PinnedRoots pr;
+    SG_CUDA(cudaMallocHost((void**)&pr.p, 32ull * count));
+    std::vector<cudaStream_t> streams(k, nullptr);
+    std::vector<cudaEvent_t> done(k, nullptr);
+    cudaEvent_t start = nullptr;
+    int rc = SG_OK;
+    auto cuda_ok = [&](cudaError_t e, const char* what) {
+        if (e != cudaSuccess && rc == SG_OK) {
+            set_error(std::string("batch commit: ") + what + ": " + cudaGetErrorString(e));
+            rc = SG_ERR_CUDA;
+        }
+        return e == cudaSuccess;
+    };
+    if (cuda_ok(cudaEventCreateWithFlags(&start, cudaEventDisableTiming), "event") &&
+        cuda_ok(cudaEventRecord(start, caller), "event record")) {
+        for (uint32_t s = 0; s < k && rc == SG_OK; ++s) {
+            if (!cuda_ok(cudaStreamCreateWithFlags(&streams[s], cudaStreamNonBlocking), "stream")) break;
+            if (!cuda_ok(cudaEventCreateWithFlags(&done[s], cudaEventDisableTiming), "event")) break;
+            cuda_ok(cudaStreamWaitEvent(streams[s], start, 0), "stream wait");
+        }
+    }
+    for (uint32_t j = 0; j < count && rc == SG_OK; ++j) {
+        const uint32_t i = order[j];
+        const sg_table_desc& d = tables[i];
+        const sg_leaf_layout* lay = d.layout.rows_per_leaf ? &d.layout : nullptr;
+        rc = commit_enqueue(ctx, streams[j % k], d.trace, d.trace_on_device, d.n, d.row_u64, d.blowup, d.weights,
+                            d.weights_on_device, lay, nullptr, &out_ldes[i], pr.p + 32ull * i);
+    }
+    // Join: the caller's stream waits for every driver stream; the roots are
+    // host-visible once it drains.
+    for (uint32_t s = 0; s < k; ++s) {
+        if (streams[s] && done[s]) {
+            cuda_ok(cudaEventRecord(done[s], streams[s]), "event record");
+            cuda_ok(cudaStreamWaitEvent(caller, done[s], 0), "stream wait");
+        }
+    }
+    for (uint32_t s = 0; s < k; ++s)
+        if (streams[s]) cuda_ok(cudaStreamSynchronize(streams[s]), "sync");
+    cuda_ok(cudaStreamSynchronize(caller), "sync");
+    for (uint32_t s = 0; s < k; ++s) {
+        if (done[s]) cudaEventDestroy(done[s]);
+        if (streams[s]) cudaStreamDestroy(streams[s]);
+    }
+    if (start) cudaEventDestroy(start);
+    if (rc != SG_OK) {
+        for (uint32_t i = 0; i < count; ++i) {
+            if (out_ldes[i]) {
+                dev_free(ctx, caller, out_ldes[i]->d_lde, out_ldes[i]->lde_rows * out_ldes[i]->row_u64 * 8);
+                dev_free(ctx, caller, out_ldes[i]->d_nodes, (2 * out_ldes[i]->leaves_len - 1) * 32);
+                delete out_ldes[i];
+                out_ldes[i] = nullptr;
+            }
+        }
+        return rc;
+    }
+    for (uint32_t i = 0; i < count; ++i) {
+        memcpy(out_ldes[i]->root, pr.p + 32ull * i, 32);
+        if (roots_out) memcpy(roots_out + 32ull * i, out_ldes[i]->root, 32);
+    }
+    return SG_OK;
+}
+
+void sg_lde_free_async(sg_ctx* c, void* stream, sg_lde* h) {
+    if (!c || !h) return;
+    Ctx* ctx = C(c);
+    cudaStream_t st = (cudaStream_t)stream;
+    dev_free(ctx, st, h->d_lde, h->lde_rows * h->row_u64 * 8);
+    dev_free(ctx, st, h->d_nodes, (2 * h->leaves_len - 1) * 32);
+    delete h;
 }
 
 int sg_lde_get_info(const sg_lde* h, sg_lde_info* info) {

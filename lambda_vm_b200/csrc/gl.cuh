@@ -183,6 +183,61 @@ __device__ __forceinline__ fe3 mul3(fe3 a, fe3 b) {
                dot3(a.c0, b.c2, a.c1, b.c1, a.c2, b.c0)};
 }
 
+// ---------------------------------------------------------------- lazily reduced sums of products
+// A sum of up to 2^32 products of two u64 is exact in 160 bits; it is reduced
+// once at the end with 2^128 = -2^32 (mod p). One product then costs the
+// 32-bit partial products plus a 5-limb carry chain, instead of a full
+// reduction and a modular add.
+struct wacc {
+    uint32_t w0, w1, w2, w3, w4;
+};
+
+__device__ __forceinline__ wacc wzero() { return wacc{0, 0, 0, 0, 0}; }
+
+__device__ __forceinline__ void wmac(wacc& a, uint64_t x, uint64_t y) {
+    uint32_t t0, t1, t2, t3;
+    mul128(x, y, t0, t1, t2, t3);
+    asm("add.cc.u32 %0, %0, %5;\n\t"
+        "addc.cc.u32 %1, %1, %6;\n\t"
+        "addc.cc.u32 %2, %2, %7;\n\t"
+        "addc.cc.u32 %3, %3, %8;\n\t"
+        "addc.u32 %4, %4, 0;"
+        : "+r"(a.w0), "+r"(a.w1), "+r"(a.w2), "+r"(a.w3), "+r"(a.w4)
+        : "r"(t0), "r"(t1), "r"(t2), "r"(t3));
+}
+
+__device__ __forceinline__ uint64_t wreduce(const wacc& a) {
+    return sub(reduce128(a.w0, a.w1, a.w2, a.w3), pack(0u, a.w4));
+}
+
+struct wacc3 {
+    wacc c0, c1, c2;
+};
+
+__device__ __forceinline__ wacc3 wzero3() { return wacc3{wzero(), wzero(), wzero()}; }
+
+// acc += g * t (ext3 times base)
+__device__ __forceinline__ void wmacb3(wacc3& a, const fe3& g, uint64_t t) {
+    wmac(a.c0, g.c0, t);
+    wmac(a.c1, g.c1, t);
+    wmac(a.c2, g.c2, t);
+}
+
+// acc += x * y (ext3 times ext3, w^3 = 2); y2 = (2 y1, 2 y2) precomputed by the caller.
+__device__ __forceinline__ void wmac3(wacc3& a, const fe3& x, const fe3& y, uint64_t y1_2, uint64_t y2_2) {
+    wmac(a.c0, x.c0, y.c0);
+    wmac(a.c0, x.c1, y2_2);
+    wmac(a.c0, x.c2, y1_2);
+    wmac(a.c1, x.c0, y.c1);
+    wmac(a.c1, x.c1, y.c0);
+    wmac(a.c1, x.c2, y2_2);
+    wmac(a.c2, x.c0, y.c2);
+    wmac(a.c2, x.c1, y.c1);
+    wmac(a.c2, x.c2, y.c0);
+}
+
+__device__ __forceinline__ fe3 wreduce3(const wacc3& a) { return fe3{wreduce(a.c0), wreduce(a.c1), wreduce(a.c2)}; }
+
 // Norm-based inverse (extensions_goldilocks.rs:359-390). Returns 0 for 0.
 __device__ __forceinline__ fe3 inv3(fe3 a) {
     uint64_t a0s = sqr(a.c0), a1s = sqr(a.c1), a2s = sqr(a.c2);

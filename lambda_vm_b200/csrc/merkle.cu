@@ -120,6 +120,21 @@ __global__ void __launch_bounds__(128) k_merkle_levels(uint64_t* nodes, uint32_t
     }
 }
 
+// One tree level with one thread per parent: level jc (2^jc nodes) -> jc - 1.
+// Used for the wide bottom levels, where every thread of every warp has a
+// pair to hash; the fused kernel above takes over once a level is narrow.
+__global__ void __launch_bounds__(128) k_merkle_level(uint64_t* nodes, uint32_t jc) {
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t parents = 1ULL << (jc - 1);
+    if (t >= parents) return;
+    const uint64_t child = ((1ULL << jc) - 1) + 2 * t;
+    uint64_t d[4];
+    hash_pair(nodes + child * 4, nodes + (child + 1) * 4, d);
+    const uint64_t parent = (parents - 1) + t;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) nodes[parent * 4 + i] = d[i];
+}
+
 int leaves_row_major(Ctx* ctx, cudaStream_t st, const uint64_t* data, uint64_t num_rows, uint64_t row_u64,
                      uint64_t col_start, uint64_t col_end, uint32_t rows_per_leaf, int little_endian,
                      uint8_t* out) {
@@ -145,6 +160,13 @@ int merkle_inner(Ctx* ctx, cudaStream_t st, uint8_t* nodes, uint64_t L) {
     SG_CHECK_ARG(lg >= 0, "leaf count must be a power of two");
     SG_CHECK_ARG(((uintptr_t)nodes & 7) == 0, "node buffer must be 8-byte aligned");
     uint32_t jc = (uint32_t)lg;
+    // Levels with at least 2^14 parents: one full-width launch per level.
+    while (jc > 14) {
+        const uint64_t parents = 1ULL << (jc - 1);
+        k_merkle_level<<<(unsigned)((parents + 127) / 128), 128, 0, st>>>((uint64_t*)nodes, jc);
+        SG_TRY(check_launch(ctx, "k_merkle_level"));
+        --jc;
+    }
     while (jc > 0) {
         const uint32_t levels = jc < 8 ? jc : 8;
         const uint64_t ctas = 1ULL << (jc - levels);

@@ -160,28 +160,38 @@ __global__ void __launch_bounds__(512) k_bary(const uint64_t* __restrict__ data,
     const uint32_t lane = threadIdx.x / CT, cl = threadIdx.x % CT;
     const uint64_t c = (uint64_t)blockIdx.x * CT + cl;
     const bool active = lane < RL && c < cols;
-    fe3 acc[K];
+    // Row sums are accumulated unreduced (160-bit, at most 3n products each)
+    // and reduced once per thread.
+    gl::wacc3 wa[K];
 #pragma unroll
-    for (int k = 0; k < K; ++k) acc[k] = zero3();
+    for (int k = 0; k < K; ++k) wa[k] = gl::wzero3();
     const uint64_t i0 = blockIdx.y * chunk_len, i1 = min(n, i0 + chunk_len);
     if (active) {
 #pragma unroll 4
         for (uint64_t i = i0 + lane; i < i1; i += RL) {
             const uint64_t* row = data + i * stride * row_u64;
             const uint64_t pt = __ldg(points + i);
-            fe3 pe;
-            if (EXT3)
-                pe = gl::mulb3(fe3{__ldg(row + 3 * c), __ldg(row + 3 * c + 1), __ldg(row + 3 * c + 2)}, pt);
-            else
-                pe = fe3{gl::mul(__ldg(row + c), pt), 0, 0};
+            if (EXT3) {
+                const fe3 pe = gl::mulb3(fe3{__ldg(row + 3 * c), __ldg(row + 3 * c + 1), __ldg(row + 3 * c + 2)}, pt);
+                const uint64_t p1_2 = gl::add(pe.c1, pe.c1), p2_2 = gl::add(pe.c2, pe.c2);
 #pragma unroll
-            for (int k = 0; k < K; ++k) {
-                const uint64_t* dp = invd + 3 * (k * n + i);
-                const fe3 d{__ldg(dp), __ldg(dp + 1), __ldg(dp + 2)};
-                acc[k] = gl::add3(acc[k], EXT3 ? gl::mul3(pe, d) : gl::mulb3(d, pe.c0));
+                for (int k = 0; k < K; ++k) {
+                    const uint64_t* dp = invd + 3 * (k * n + i);
+                    gl::wmac3(wa[k], fe3{__ldg(dp), __ldg(dp + 1), __ldg(dp + 2)}, pe, p1_2, p2_2);
+                }
+            } else {
+                const uint64_t pe = gl::mul(__ldg(row + c), pt);
+#pragma unroll
+                for (int k = 0; k < K; ++k) {
+                    const uint64_t* dp = invd + 3 * (k * n + i);
+                    gl::wmacb3(wa[k], fe3{__ldg(dp), __ldg(dp + 1), __ldg(dp + 2)}, pe);
+                }
             }
         }
     }
+    fe3 acc[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] = gl::wreduce3(wa[k]);
     if (lane < RL) {
 #pragma unroll
         for (int k = 0; k < K; ++k) st3(bary_sm + 3 * (((uint64_t)lane * CT + cl) * K + k), acc[k]);
@@ -213,12 +223,20 @@ static bary_fn bary_kernel(uint32_t K) {
     }
 }
 
+// One warp per output: lanes sum strided chunk partials, then a shuffle tree.
 __global__ void k_bary_combine(const uint64_t* partial, uint64_t chunks, uint64_t per_chunk, uint64_t* out) {
-    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= per_chunk) return;
+    const uint64_t t = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32;
+    const uint32_t lane = threadIdx.x % 32;
+    if (t >= per_chunk) return;  // whole warp leaves together
     fe3 s = zero3();
-    for (uint64_t ch = 0; ch < chunks; ++ch) s = gl::add3(s, ld3(partial + 3 * (ch * per_chunk + t)));
-    st3(out + 3 * t, gl::canon3(s));
+    for (uint64_t ch = lane; ch < chunks; ch += 32) s = gl::add3(s, ld3(partial + 3 * (ch * per_chunk + t)));
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const fe3 o{__shfl_down_sync(0xffffffffu, s.c0, off), __shfl_down_sync(0xffffffffu, s.c1, off),
+                    __shfl_down_sync(0xffffffffu, s.c2, off)};
+        s = gl::add3(s, o);
+    }
+    if (lane == 0) st3(out + 3 * t, gl::canon3(s));
 }
 
 // ---------------------------------------------------------------- DEEP
@@ -241,30 +259,38 @@ __global__ void __launch_bounds__(128) k_deep(const uint64_t* __restrict__ main,
                                               int bitrev_out, uint64_t* __restrict__ out) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= rows) return;
-    fe3 sk[K > 0 ? K : 1];
+    // Column sums are accumulated unreduced (160-bit) and reduced once per row.
+    gl::wacc3 acc[K > 0 ? K : 1];
 #pragma unroll
-    for (int k = 0; k < K; ++k) sk[k] = zero3();
+    for (int k = 0; k < K; ++k) acc[k] = gl::wzero3();
     const uint64_t* mrow = main + i * m;
     for (uint64_t j = 0; j < m; ++j) {
         const uint64_t t = __ldg(mrow + j);
         const uint64_t* g = gam_tr + 3 * j * K;
 #pragma unroll
         for (int k = 0; k < K; ++k)
-            sk[k] = gl::add3(sk[k], gl::mulb3(fe3{__ldg(g + 3 * k), __ldg(g + 3 * k + 1), __ldg(g + 3 * k + 2)}, t));
+            gl::wmacb3(acc[k], fe3{__ldg(g + 3 * k), __ldg(g + 3 * k + 1), __ldg(g + 3 * k + 2)}, t);
     }
     const uint64_t* arow = aux + i * A * 3;
     for (uint64_t j = 0; j < A; ++j) {
         const fe3 t{__ldg(arow + 3 * j), __ldg(arow + 3 * j + 1), __ldg(arow + 3 * j + 2)};
+        const uint64_t t1_2 = gl::add(t.c1, t.c1), t2_2 = gl::add(t.c2, t.c2);
         const uint64_t* g = gam_tr + 3 * (m + j) * K;
 #pragma unroll
         for (int k = 0; k < K; ++k)
-            sk[k] = gl::add3(sk[k], gl::mul3(fe3{__ldg(g + 3 * k), __ldg(g + 3 * k + 1), __ldg(g + 3 * k + 2)}, t));
+            gl::wmac3(acc[k], fe3{__ldg(g + 3 * k), __ldg(g + 3 * k + 1), __ldg(g + 3 * k + 2)}, t, t1_2, t2_2);
     }
-    fe3 sh = zero3();
+    gl::wacc3 acch = gl::wzero3();
     const uint64_t* prow = parts + i * P * 3;
-    for (uint64_t j = 0; j < P; ++j)
-        sh = gl::add3(sh, gl::mul3(fe3{__ldg(gam_h + 3 * j), __ldg(gam_h + 3 * j + 1), __ldg(gam_h + 3 * j + 2)},
-                                   fe3{__ldg(prow + 3 * j), __ldg(prow + 3 * j + 1), __ldg(prow + 3 * j + 2)}));
+    for (uint64_t j = 0; j < P; ++j) {
+        const fe3 h{__ldg(prow + 3 * j), __ldg(prow + 3 * j + 1), __ldg(prow + 3 * j + 2)};
+        gl::wmac3(acch, fe3{__ldg(gam_h + 3 * j), __ldg(gam_h + 3 * j + 1), __ldg(gam_h + 3 * j + 2)}, h,
+                  gl::add(h.c1, h.c1), gl::add(h.c2, h.c2));
+    }
+    fe3 sk[K > 0 ? K : 1];
+#pragma unroll
+    for (int k = 0; k < K; ++k) sk[k] = gl::wreduce3(acc[k]);
+    const fe3 sh = gl::wreduce3(acch);
     fe3 r = gl::mul3(ld3(inv_h + 3 * i), gl::sub3(sh, ld3(consts)));
 #pragma unroll
     for (int k = 0; k < K; ++k)
@@ -552,7 +578,7 @@ int sg_barycentric_sums(sg_ctx* c, void* stream, const uint64_t* d_data, uint64_
     int rc = check_launch(ctx, "k_bary");
     if (rc == SG_OK) {
         const uint64_t per = (uint64_t)k * cols;
-        k_bary_combine<<<(unsigned)((per + 255) / 256), 256, 0, st>>>(part, chunks, per, d_out);
+        k_bary_combine<<<(unsigned)((per * 32 + 255) / 256), 256, 0, st>>>(part, chunks, per, d_out);
         rc = check_launch(ctx, "k_bary_combine");
     }
     int rf = dev_free(ctx, st, part, 24ull * chunks * k * cols);

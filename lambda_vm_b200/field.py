@@ -112,6 +112,29 @@ def bitrev_indices(log_n):
     return r
 
 
+def bitrev_vec(idx, bits):
+    """Bit-reversal of each index of `idx` (array-like) over `bits` bits."""
+    i = np.asarray(idx, dtype=np.uint64)
+    r = np.zeros_like(i)
+    for b in range(bits):
+        r |= ((i >> np.uint64(b)) & np.uint64(1)) << np.uint64(bits - 1 - b)
+    return r
+
+
+def f3mul_vec(a, b):
+    """Fp3 products of (..., 3) uint64 arrays, with broadcasting; canonical output."""
+    a = np.asarray(a, np.uint64)
+    b = np.asarray(b, np.uint64)
+    a0, a1, a2 = a[..., 0], a[..., 1], a[..., 2]
+    b0, b1, b2 = b[..., 0], b[..., 1], b[..., 2]
+    t = add(mul(a1, b2), mul(a2, b1))
+    c0 = add(mul(a0, b0), add(t, t))
+    u = mul(a2, b2)
+    c1 = add(add(mul(a0, b1), mul(a1, b0)), add(u, u))
+    c2 = add(add(mul(a0, b2), mul(a1, b1)), mul(a2, b0))
+    return canon(np.stack(np.broadcast_arrays(c0, c1, c2), axis=-1))
+
+
 # ---------------- scalar Fp3 helpers (Python ints) for the few host-side
 # extension-field values (challenges, OOD scalars, terminal polynomial).
 def f3(x):

@@ -245,6 +245,14 @@ class Transcript:
         a = _u64(v)
         native.lib().sg_transcript_append_ext3(self.h, a.ctypes.data)
 
+    def append_ext3_many(self, vals):
+        """Absorb a sequence of Fp3 elements in order: the same absorption as
+        append_ext3 on each (canonical c0 || c1 || c2, big-endian), in one update."""
+        a = np.asarray(vals, np.uint64).reshape(-1, 3)
+        p = np.uint64(0xFFFFFFFF00000001)
+        c = np.where(a >= p, a - p, a)
+        self.append_bytes(c.astype(">u8").tobytes())
+
     def sample(self) -> bytes:
         out = (C.c_uint8 * 32)()
         native.lib().sg_transcript_sample(self.h, out)

@@ -23,6 +23,12 @@ class LeafLayout(C.Structure):
                 ("col_start", C.c_uint64), ("col_end", C.c_uint64)]
 
 
+class TableDesc(C.Structure):
+    _fields_ = [("trace", C.c_void_p), ("trace_on_device", C.c_int), ("n", C.c_uint64), ("row_u64", C.c_uint64),
+                ("blowup", C.c_uint32), ("weights_on_device", C.c_int), ("weights", C.c_void_p),
+                ("layout", LeafLayout)]
+
+
 class LdeInfo(C.Structure):
     _fields_ = [("d_lde", C.c_void_p), ("lde_rows", C.c_uint64), ("row_u64", C.c_uint64),
                 ("d_nodes", C.c_void_p), ("leaves_len", C.c_uint64), ("root", C.c_uint8 * 32)]
@@ -78,6 +84,8 @@ PROTOTYPES = {
     "sg_lde_commit": (i32, [vp, vp, vp, i32, u64, u64, u32, vp, C.POINTER(LeafLayout), vp, C.POINTER(vp), vp]),
     "sg_lde_get_info": (i32, [vp, C.POINTER(LdeInfo)]),
     "sg_lde_free": (None, [vp, vp]),
+    "sg_lde_free_async": (None, [vp, vp, vp]),
+    "sg_batch_commit": (i32, [vp, vp, vp, u32, u32, vp, vp]),
     "sg_grind": (i32, [vp, vp, vp, C.c_uint8, C.POINTER(u64)]),
     "sg_coset_lde_static": (i32, [vp, vp, u64, u64, u32, vp, vp]),
     "sg_transcript_new": (vp, [vp, u64]),

@@ -8,8 +8,9 @@ non-blocking CUDA stream, so small tables overlap on the device instead of
 running one after another behind host round trips; ctypes releases the GIL
 during every C-ABI call, so drivers run concurrently on the host too.
 
-The protocol is unchanged: R1 commits run concurrently but their roots are
-absorbed in table order, and every table's rounds 2-4 run on its own
+R1 is one native call (sg_batch_commit): every table's LDE, leaves and tree,
+heaviest first over k internal streams. The protocol is unchanged: the roots
+are absorbed in table order, and every table's rounds 2-4 run on its own
 transcript fork, so the proof is identical to the sequential prover's.
 """
 import ctypes as C
@@ -98,19 +99,14 @@ def multi_prove_scheduled(airs, sources, opts=None, workers=8, budget_bytes=None
     order = heaviest_first(airs, opts)
     r1 = [None] * len(airs)
 
-    def commit(i):
-        bk = pool.take()
-        try:
-            tm = _gen_trace(bk, airs[i], sources[i])
-            lde = bk.lde(tm, B, bk.domain(airs[i].log_n, B, g).weights)
-            tree, root = bk.commit(lde)  # synchronizes this stream (root readback)
-            r1[i] = (tm, lde, tree, root)
-        finally:
-            pool.give(bk)
-
     try:
-        with ThreadPoolExecutor(workers) as ex:
-            list(ex.map(commit, order))
+        # R1: every table's trace, then one native batched commit (LDE + leaves
+        # + tree per table, heaviest first over `workers` streams).
+        tms = [_gen_trace(base, air, src) for air, src in zip(airs, sources)]
+        committed = base.batch_commit(tms, B, [base.domain(a.log_n, B, g).weights for a in airs], workers)
+        for i in range(len(airs)):
+            lde, tree, root, release = committed[i]
+            r1[i] = (tms[i], lde, tree, root, release)
         t = base.transcript(label)
         for i in range(len(airs)):
             t.append_bytes(r1[i][3])
@@ -134,17 +130,18 @@ def multi_prove_scheduled(airs, sources, opts=None, workers=8, budget_bytes=None
             est = estimate_table_bytes(airs[i], opts)
             gate.acquire(est)
             bk = pool.take()
+            tm, lde, tree, root, release = r1[i]
             try:
-                tm, lde, tree, root = r1[i]
                 p = prove_table(bk, airs[i], lower(airs[i].program), tm, lde, tree, forks[i], challenges, alpha_pows,
                                 opts)
                 p["main_root"] = root
-                # The R1 buffers were allocated on another driver's stream and are
-                # released on that stream: finish this stream's use of them first.
-                native.check(bk.L.sg_stream_sync(bk.be.h, bk.st))
-                bk.free(tm, lde, tree)
                 proofs[i] = p
             finally:
+                # The R1 buffers were allocated on other streams: finish this
+                # stream's use of them before they are released.
+                bk.L.sg_stream_sync(bk.be.h, bk.st)
+                bk.free(tm)
+                release(bk)
                 pool.give(bk)
                 gate.release(est)
 

@@ -1,0 +1,226 @@
+"""Proof serving: continuous admission of proof jobs under an HBM budget.
+
+A request loop in the shape of the reference's multi-table driver
+(crypto/stark/src/prover.rs:697-790, `VramGate` + `run_admitted`) lifted from
+tables to whole proofs: jobs (one multi-table proof each) arrive at any time,
+wait in a FIFO queue, and are admitted as soon as a job slot is free and the
+job's HBM estimate fits the remaining budget. Admitted jobs run concurrently
+(each on its own table drivers and CUDA streams), so a small proof that
+arrives behind a large one overlaps with it on the device instead of waiting
+for it. Every job's proof is the same as when it runs alone: jobs share no
+transcript or buffers, only the device.
+
+Latency of a job = completion time - submit time (queueing included);
+`ServeStats` reports p50/p99 beside proofs/s and proved rows/s.
+"""
+import threading
+import time
+from collections import deque
+
+from .scheduler import VramGate, estimate_table_bytes, multi_prove_scheduled
+from .stark import Options
+
+
+def estimate_job_bytes(airs, opts, drivers):
+    """Peak device bytes of one proof: every table's main trace, LDE and tree
+    stay resident from R1 until the table's rounds finish, plus rounds 2-4 of
+    `drivers` tables at once (crypto/stark/src/prover.rs:682-695)."""
+    resident = 0
+    for a in airs:
+        N = a.n * opts.blowup
+        resident += a.n * a.width * 8 + N * a.width * 8 + N * 32
+    per_table = sorted((estimate_table_bytes(a, opts) for a in airs), reverse=True)
+    return resident + sum(per_table[:max(1, drivers)])
+
+
+class Job:
+    __slots__ = ("id", "airs", "sources", "rows", "est", "t_submit", "t_start", "t_done", "proof", "error", "done")
+
+    def __init__(self, jid, airs, sources, est):
+        self.id = jid
+        self.airs = airs
+        self.sources = sources
+        self.rows = sum(a.n for a in airs)
+        self.est = est
+        self.t_submit = time.perf_counter()
+        self.t_start = None
+        self.t_done = None
+        self.proof = None
+        self.error = None
+        self.done = threading.Event()
+
+    @property
+    def latency(self):
+        return None if self.t_done is None else self.t_done - self.t_submit
+
+
+class ServeStats:
+    def __init__(self, jobs, t0, t1):
+        lat = sorted(j.latency for j in jobs if j.latency is not None)
+        self.jobs = len(jobs)
+        self.failed = sum(1 for j in jobs if j.error is not None)
+        self.wall_s = t1 - t0
+        self.proofs_per_s = len(lat) / self.wall_s if self.wall_s > 0 else 0.0
+        self.rows_per_s = sum(j.rows for j in jobs if j.error is None) / self.wall_s if self.wall_s > 0 else 0.0
+        self.p50_s = _quantile(lat, 0.50)
+        self.p99_s = _quantile(lat, 0.99)
+        self.mean_s = sum(lat) / len(lat) if lat else None
+
+    def as_dict(self):
+        r = lambda x: None if x is None else round(x * 1e3, 1)
+        return {"jobs": self.jobs, "failed": self.failed, "wall_s": round(self.wall_s, 3),
+                "proofs_per_s": round(self.proofs_per_s, 3), "rows_per_s": round(self.rows_per_s, 1),
+                "p50_ms": r(self.p50_s), "p99_ms": r(self.p99_s), "mean_ms": r(self.mean_s)}
+
+
+def _quantile(sorted_vals, q):
+    """Nearest-rank quantile."""
+    if not sorted_vals:
+        return None
+    k = max(0, min(len(sorted_vals) - 1, int(-(-q * len(sorted_vals) // 1)) - 1))
+    return sorted_vals[k]
+
+
+class ProofServer:
+    """FIFO job queue with slot + HBM-budget admission.
+
+    `max_jobs` concurrent proofs, each proved by `prove_fn(airs, sources, opts,
+    drivers, budget_bytes)` (default: the scheduled multi-table prover on the
+    process-wide device context) with `drivers` table drivers. A job whose
+    estimate exceeds the whole budget runs alone rather than never.
+    """
+
+    def __init__(self, budget_bytes, max_jobs=4, drivers=4, opts=None, prove_fn=None, be=None):
+        self.opts = opts or Options()
+        self.max_jobs = max_jobs
+        self.drivers = drivers
+        self.gate = VramGate(budget_bytes)
+        self.be = be
+        self.prove_fn = prove_fn or self._prove_gpu
+        self.queue = deque()
+        self.cv = threading.Condition()
+        self.running = 0
+        self.next_id = 0
+        self.jobs = []
+        self.closed = False
+        self.threads = []
+        self.dispatcher = threading.Thread(target=self._dispatch, daemon=True)
+        self.dispatcher.start()
+
+    def _prove_gpu(self, airs, sources, opts, drivers, budget_bytes):
+        return multi_prove_scheduled(airs, sources, opts, workers=drivers, budget_bytes=budget_bytes, be=self.be)
+
+    def submit(self, airs, sources):
+        with self.cv:
+            if self.closed:
+                raise RuntimeError("server is closed")
+            job = Job(self.next_id, airs, sources, estimate_job_bytes(airs, self.opts, self.drivers))
+            self.next_id += 1
+            self.jobs.append(job)
+            self.queue.append(job)
+            self.cv.notify_all()
+        return job
+
+    def _fits(self, job):
+        g = self.gate
+        return g.used == 0 or g.used + job.est <= g.budget
+
+    def _dispatch(self):
+        while True:
+            with self.cv:
+                while not self.closed and not (self.queue and self.running < self.max_jobs and
+                                               self._fits(self.queue[0])):
+                    self.cv.wait(0.05)
+                if self.closed and not self.queue:
+                    return
+                if not (self.queue and self.running < self.max_jobs and self._fits(self.queue[0])):
+                    continue
+                job = self.queue.popleft()
+                self.running += 1
+                self.gate.acquire(job.est)
+            t = threading.Thread(target=self._run, args=(job,), daemon=True)
+            self.threads.append(t)
+            t.start()
+
+    def _run(self, job):
+        job.t_start = time.perf_counter()
+        try:
+            # rounds 2-4 of this job may use what its resident R1 state leaves of its share
+            job.proof = self.prove_fn(job.airs, job.sources, self.opts, self.drivers, job.est)
+        except Exception as e:  # reported per job; the server keeps serving
+            job.error = e
+        finally:
+            job.t_done = time.perf_counter()
+            self.gate.release(job.est)
+            with self.cv:
+                self.running -= 1
+                self.cv.notify_all()
+            job.done.set()
+
+    def drain(self):
+        for j in list(self.jobs):
+            j.done.wait()
+
+    def close(self):
+        self.drain()
+        with self.cv:
+            self.closed = True
+            self.cv.notify_all()
+        self.dispatcher.join()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def serve_poisson(server, job_specs, rate, seed=0):
+    """Submit `job_specs` [(airs, sources)] with exponential inter-arrival
+    times of mean 1/rate (seeded); wait for all; return (jobs, ServeStats)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate, size=len(job_specs))
+    t0 = time.perf_counter()
+    due = t0
+    jobs = []
+    for (airs, sources), gap in zip(job_specs, gaps):
+        due += gap
+        now = time.perf_counter()
+        if due > now:
+            time.sleep(due - now)
+        jobs.append(server.submit(airs, sources))
+    for j in jobs:
+        j.done.wait()
+    t1 = max(j.t_done for j in jobs)
+    return jobs, ServeStats(jobs, t0, t1)
+
+
+def serve_sequential(job_specs, rate, prove_fn, seed=0):
+    """The one-at-a-time baseline: the same arrival stream, one proof at a
+    time in arrival order; latency includes the wait behind earlier jobs."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate, size=len(job_specs))
+    arrivals = []
+    t = 0.0
+    for gap in gaps:
+        t += gap
+        arrivals.append(t)
+    t0 = time.perf_counter()
+    jobs = []
+    for (airs, sources), at in zip(job_specs, arrivals):
+        now = time.perf_counter()
+        if t0 + at > now:
+            time.sleep(t0 + at - now)
+        j = Job(len(jobs), airs, sources, 0)
+        j.t_submit = t0 + at
+        j.t_start = time.perf_counter()
+        try:
+            j.proof = prove_fn(airs, sources)
+        except Exception as e:
+            j.error = e
+        j.t_done = time.perf_counter()
+        j.done.set()
+        jobs.append(j)
+    return jobs, ServeStats(jobs, t0, max(j.t_done for j in jobs))

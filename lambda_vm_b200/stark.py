@@ -115,6 +115,29 @@ class Mat:
         self.buf.close()
 
 
+class _Borrowed:
+    """Device memory owned by a library handle; closing the view frees nothing."""
+
+    def __init__(self, ptr):
+        self.ptr = ptr
+
+    def close(self):
+        pass
+
+
+class _Release:
+    """Stream-ordered release of an sg_lde handle (LDE + tree) on a backend's stream."""
+
+    def __init__(self, bk, handle):
+        self.bk, self.h = bk, handle
+
+    def __call__(self, bk=None):
+        if self.h:
+            b = bk or self.bk
+            b.L.sg_lde_free_async(b.be.h, b.st, self.h)
+            self.h = None
+
+
 class Tree:
     def __init__(self, buf, leaves_len):
         self.buf, self.leaves_len = buf, leaves_len
@@ -215,6 +238,27 @@ class GpuBackend:
         native.check(self.L.sg_merkle_build(self.be.h, self.st, leaves, nl, tree.buf.ptr, root))
         return tree, bytes(root)
 
+    def batch_commit(self, mats, blowup, weights, concurrency=8):
+        """Commit many main traces in one sg_batch_commit call (row-pair BE
+        leaves); returns [(lde Mat, Tree, root, release)] in table order, where
+        release() returns the LDE and tree memory on this backend's stream."""
+        n = len(mats)
+        descs = (native.TableDesc * n)()
+        for i, (m, w) in enumerate(zip(mats, weights)):
+            descs[i] = native.TableDesc(m.ptr, 1, m.rows, m.cols, blowup, 1, w.ptr, native.LeafLayout(2, 0, 0, 0))
+        handles = (C.c_void_p * n)()
+        roots = (C.c_uint8 * (32 * n))()
+        native.check(self.L.sg_batch_commit(self.be.h, self.st, descs, n, concurrency, handles, roots))
+        out = []
+        for i in range(n):
+            info = native.LdeInfo()
+            native.check(self.L.sg_lde_get_info(handles[i], C.byref(info)))
+            h = handles[i]
+            lde = Mat(_Borrowed(info.d_lde), info.lde_rows, info.row_u64)
+            tree = Tree(_Borrowed(info.d_nodes), info.leaves_len)
+            out.append((lde, tree, bytes(roots[32 * i:32 * i + 32]), _Release(self, h)))
+        return out
+
     def tree_from_leaves(self, leaves_buf, nl):
         tree = Tree(DeviceBuffer((2 * nl - 1) * 32, self.be, self.st), nl)
         root = (C.c_uint8 * 32)()
@@ -303,10 +347,11 @@ class GpuBackend:
             raise ZeroDivisionError("zero denominator")
         return out
 
-    def bary(self, mat, stride, ext3, cols, pts, invd, n, k):
+    def bary(self, mat, stride, ext3, cols, pts, invd, n, k, k0=0):
+        """Sums over the k denominator rows k0 .. k0+k-1 of `invd`."""
         out = DeviceBuffer(24 * k * cols, self.be, self.st)
         native.check(self.L.sg_barycentric_sums(self.be.h, self.st, mat.ptr, mat.cols, stride, 1 if ext3 else 0, cols,
-                                                pts.ptr, invd.ptr, n, k, out.ptr))
+                                                pts.ptr, invd.ptr + 24 * k0 * n, n, k, out.ptr))
         r = out.download(np.uint64, 3 * k * cols).reshape(k, cols, 3)
         out.close()
         return r
@@ -352,6 +397,43 @@ class GpuBackend:
         dp.close()
         out.close()
         return h
+
+    def open_many(self, reqs):
+        """Query openings in one round trip: reqs is a list of ("rows", Mat,
+        rows) and ("paths", Tree, positions); one upload of all indices, one
+        kernel per request into one output buffer, one download."""
+        idx = [np.ascontiguousarray(r[2], np.uint32) for r in reqs]
+        offs, sizes, tot_idx = [], [], 0
+        for (kind, obj, _), ix in zip(reqs, idx):
+            offs.append(tot_idx)
+            tot_idx += ix.size
+            sizes.append(ix.size * (obj.cols * 8 if kind == "rows" else (obj.leaves_len.bit_length() - 1) * 32))
+        allidx = np.concatenate(idx) if idx else np.zeros(1, np.uint32)
+        dix = DeviceBuffer.from_host(allidx if allidx.size else np.zeros(1, np.uint32), self.be, self.st)
+        ob = [0]
+        for sz in sizes:
+            ob.append(ob[-1] + (sz + 7) // 8 * 8)
+        out = DeviceBuffer(max(8, ob[-1]), self.be, self.st)
+        for (kind, obj, _), ix, off, o in zip(reqs, idx, offs, ob):
+            if ix.size == 0:
+                continue
+            if kind == "rows":
+                native.check(self.L.sg_gather_rows(self.be.h, self.st, obj.ptr, obj.cols, obj.rows, 0, obj.cols,
+                                                   dix.ptr + 4 * off, ix.size, out.ptr + o))
+            else:
+                native.check(self.L.sg_merkle_gather_paths(self.be.h, self.st, obj.buf.ptr, obj.leaves_len,
+                                                           dix.ptr + 4 * off, ix.size, out.ptr + o))
+        host = out.download(np.uint8, ob[-1]) if ob[-1] else np.zeros(0, np.uint8)
+        dix.close()
+        out.close()
+        res = []
+        for (kind, obj, _), ix, o, sz in zip(reqs, idx, ob, sizes):
+            b = host[o:o + sz]
+            if kind == "rows":
+                res.append(b.view(np.uint64).reshape(ix.size, obj.cols))
+            else:
+                res.append(b.reshape(ix.size, obj.leaves_len.bit_length() - 1, 32))
+        return res
 
     def grind(self, state, g):
         inner = mc.keccak256(bytes([0x01, 0x23, 0x45, 0x67, 0x89, 0xAB, 0xCD, 0xED]) + bytes(state) + bytes([g]))
@@ -418,19 +500,19 @@ def prove_table(bk, air, lowered, trace_mat, main_lde, main_tree, t, challenges,
     zw = F.f3scale(z, wn)
     z2 = F.f3mul(z, z)
     invd = bk.inv_denoms(dom.pts_n, [z, zw, z2], False)
-    S_main = bk.bary(main_lde, B, False, air.width, dom.pts_n, invd, n, 3)
-    S_aux = bk.bary(aux_lde, B, True, air.aux_width, dom.pts_n, invd, n, 3)
-    S_parts = bk.bary(parts_lde, B, True, 2, dom.pts_n, invd, n, 3)
+    # trace columns at z and z*w (denominator rows 0, 1); parts at z^2 (row 2)
+    S_main = bk.bary(main_lde, B, False, air.width, dom.pts_n, invd, n, 2)
+    S_aux = bk.bary(aux_lde, B, True, air.aux_width, dom.pts_n, invd, n, 2)
+    S_parts = bk.bary(parts_lde, B, True, 2, dom.pts_n, invd, n, 1, k0=2)
     bk.free(invd)
-    sc = [_ood_scale(p, n, g) for p in (z, zw, z2)]
-    trace_ood = [[F.f3mul(sc[k], F.f3(S_main[k, c])) for c in range(air.width)] +
-                 [F.f3mul(sc[k], F.f3(S_aux[k, c])) for c in range(air.aux_width)] for k in range(2)]
-    parts_ood = [F.f3mul(sc[2], F.f3(S_parts[2, j])) for j in range(2)]
-    for k in range(2):
-        for v in trace_ood[k]:
-            t.append_ext3(v)
-    for v in parts_ood:
-        t.append_ext3(v)
+    sc = np.array([_ood_scale(p, n, g) for p in (z, zw, z2)], np.uint64)
+    tood = np.concatenate([F.f3mul_vec(S_main[:2], sc[:2, None, :]), F.f3mul_vec(S_aux[:2], sc[:2, None, :])],
+                          axis=1)  # (2 points, main + aux columns, 3)
+    pood = F.f3mul_vec(S_parts[0], sc[2][None, :])  # (2 parts, 3)
+    t.append_ext3_many(tood)
+    t.append_ext3_many(pood)
+    trace_ood = [[tuple(v) for v in row] for row in tood.tolist()]
+    parts_ood = [tuple(v) for v in pood.tolist()]
     proof["trace_ood"] = trace_ood
     proof["parts_ood"] = parts_ood
     # ---- R4: DEEP
@@ -440,7 +522,7 @@ def prove_table(bk, air, lowered, trace_mat, main_lde, main_tree, t, challenges,
     for _ in range(2 + 2 * ncols - 1):
         gp.append(F.f3mul(gp[-1], gamma))
     gh, gt = gp[:2], gp[2:]
-    trace_ood_jk = [trace_ood[k][j] for j in range(ncols) for k in range(2)]
+    trace_ood_jk = tood.transpose(1, 0, 2).reshape(-1, 3)  # index j*2 + k
     inv_h = bk.inv_denoms(dom.pts_N, [z2], True)
     inv_t = bk.inv_denoms(dom.pts_N, [z, zw], True)
     deep = bk.deep(main_lde, aux_lde, parts_lde, parts_ood, trace_ood_jk, gh, gt, inv_h, inv_t, 2)
@@ -473,8 +555,7 @@ def prove_table(bk, air, lowered, trace_mat, main_lde, main_tree, t, challenges,
         bk.free(tw)
     term_off = F.pow_int(g, 1 << lay["total_folds"])
     coeffs = terminal_coeffs(final, term_off, lay["effective_k"])
-    for c in coeffs:
-        t.append_ext3(c)
+    t.append_ext3_many(coeffs)
     proof["fri_roots"] = fri_roots
     proof["fri_final_coeffs"] = coeffs
     # ---- grinding + queries
@@ -485,24 +566,19 @@ def prove_table(bk, air, lowered, trace_mat, main_lde, main_tree, t, challenges,
     iotas = [t.sample_u64(N // 2) for _ in range(opts.queries)]
     proof["iotas"] = iotas
     # ---- openings: leaf iota of each trace-side tree covers rows br(2i), br(2i+1)
-    rows = []
-    for i in iotas:
-        rows += [F.bitrev_int(2 * i, log_N), F.bitrev_int(2 * i + 1, log_N)]
-    proof["open_main"] = bk.gather(main_lde, rows)
-    proof["open_aux"] = bk.gather(aux_lde, rows)
-    proof["open_parts"] = bk.gather(parts_lde, rows)
-    proof["path_main"] = bk.paths(main_tree, iotas)
-    proof["path_aux"] = bk.paths(aux_tree, iotas)
-    proof["path_parts"] = bk.paths(comp_tree, iotas)
-    fri_open, fri_paths = [], []
+    it = np.asarray(iotas, np.uint64)
+    rows = F.bitrev_vec(np.stack([2 * it, 2 * it + 1], axis=1).reshape(-1), log_N).tolist()
+    reqs = [("rows", main_lde, rows), ("rows", aux_lde, rows), ("rows", parts_lde, rows),
+            ("paths", main_tree, iotas), ("paths", aux_tree, iotas), ("paths", comp_tree, iotas)]
     for li, (lev, ltree) in enumerate(layers):
-        pos = [i >> li for i in iotas]
-        leaf = [p >> 1 for p in pos]
-        rr = []
-        for lf in leaf:
-            rr += [2 * lf, 2 * lf + 1]
-        fri_open.append(bk.gather(lev, rr))
-        fri_paths.append(bk.paths(ltree, leaf))
+        leaf = (it >> np.uint64(li + 1)).tolist()
+        rr = np.stack([2 * np.asarray(leaf, np.uint64), 2 * np.asarray(leaf, np.uint64) + 1], axis=1).reshape(-1)
+        reqs += [("rows", lev, rr.tolist()), ("paths", ltree, leaf)]
+    opened = bk.open_many(reqs)
+    (proof["open_main"], proof["open_aux"], proof["open_parts"], proof["path_main"], proof["path_aux"],
+     proof["path_parts"]) = opened[:6]
+    fri_open = opened[6::2]
+    fri_paths = opened[7::2]
     proof["fri_open"] = fri_open
     proof["fri_paths"] = fri_paths
     bk.free(deep, aux_lde, parts_lde, aux_tree, comp_tree)

@@ -233,6 +233,11 @@ class Transcript:
         a = _u64(v)
         lib().or_transcript_append_ext3(_p(self._buf), _p(a))
 
+    def append_ext3_many(self, vals):
+        """One append_ext3 per element (default_transcript.rs append semantics)."""
+        for v in np.asarray(vals, np.uint64).reshape(-1, 3):
+            self.append_ext3(v)
+
     def sample(self) -> bytes:
         out = np.zeros(32, np.uint8)
         lib().or_transcript_sample(_p(self._buf), _p(out))

@@ -157,8 +157,9 @@ class OracleBackend:
     def inv_denoms(self, pts, zs, x_minus_z):
         return _c(O.inv_denoms(pts.reshape(-1), np.array(zs, np.uint64), x_minus_z)).reshape(-1, 3)
 
-    def bary(self, mat, stride, ext3, cols, pts, invd, n, k):
-        return _c(O.barycentric_sums(mat, stride, ext3, cols, pts.reshape(-1), invd.reshape(-1), n, k)).reshape(k, cols, 3)
+    def bary(self, mat, stride, ext3, cols, pts, invd, n, k, k0=0):
+        sel = np.ascontiguousarray(invd.reshape(-1, 3)[k0 * n:(k0 + k) * n])
+        return _c(O.barycentric_sums(mat, stride, ext3, cols, pts.reshape(-1), sel.reshape(-1), n, k)).reshape(k, cols, 3)
 
     def deep(self, main, aux, parts, h_ood, trace_ood, gh, gt, inv_h, inv_t, k):
         nat = _c(O.deep(main, aux, parts, np.array(h_ood, np.uint64), np.array(trace_ood, np.uint64),
@@ -184,6 +185,9 @@ class OracleBackend:
 
     def paths(self, tree, positions):
         return np.stack([O.merkle_path(tree, int(p)) for p in positions])
+
+    def open_many(self, reqs):
+        return [self.gather(obj, ix) if kind == "rows" else self.paths(obj, ix) for kind, obj, ix in reqs]
 
     def grind(self, state, g):
         return O.grind(bytes(state), g)

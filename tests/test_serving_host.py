@@ -1,0 +1,102 @@
+"""Serving loop host logic on the CPU with a stand-in prover: slot and HBM
+budget admission, FIFO order, per-job results and errors, latency quantiles."""
+import threading
+import time
+
+import pytest
+
+from lambda_vm_b200.air import SynthTableAir
+from lambda_vm_b200.serving import ProofServer, ServeStats, _quantile, estimate_job_bytes, serve_poisson
+from lambda_vm_b200.stark import Options
+
+
+class Recorder:
+    def __init__(self, delay=0.02, fail_ids=()):
+        self.lock = threading.Lock()
+        self.running = {}
+        self.max_running = 0
+        self.max_bytes = 0
+        self.starts = []
+        self.delay = delay
+        self.fail_ids = set(fail_ids)
+
+    def __call__(self, airs, sources, opts, drivers, budget):
+        key = sources[0]
+        with self.lock:
+            self.running[key] = budget
+            self.max_running = max(self.max_running, len(self.running))
+            self.max_bytes = max(self.max_bytes, sum(self.running.values()))
+            self.starts.append(key)
+        time.sleep(self.delay)
+        with self.lock:
+            del self.running[key]
+        if key in self.fail_ids:
+            raise ValueError(f"job {key} failed")
+        return {"job": key}
+
+
+def _spec(i, log_n=10, width=8):
+    return [SynthTableAir(log_n, width, 2)], [i]
+
+
+def test_slots_fifo_and_results():
+    rec = Recorder()
+    with ProofServer(budget_bytes=1 << 40, max_jobs=3, drivers=2, prove_fn=rec) as srv:
+        jobs = [srv.submit(*_spec(i)) for i in range(10)]
+        srv.drain()
+    assert rec.max_running <= 3
+    assert rec.starts == list(range(10))
+    assert [j.proof["job"] for j in jobs] == list(range(10))
+    assert all(j.latency is not None and j.latency >= 0 for j in jobs)
+
+
+def test_budget_admission_limits_concurrency():
+    opts = Options()
+    est = estimate_job_bytes(*_spec(0, 12, 40)[:1], opts, 2)
+    rec = Recorder()
+    # room for two such jobs at a time, not three
+    with ProofServer(budget_bytes=2 * est + est // 2, max_jobs=8, drivers=2, prove_fn=rec, opts=opts) as srv:
+        for i in range(6):
+            srv.submit(*_spec(i, 12, 40))
+        srv.drain()
+    assert rec.max_running == 2
+    assert rec.max_bytes <= 2 * est + est // 2
+
+
+def test_oversized_job_runs_alone():
+    rec = Recorder()
+    with ProofServer(budget_bytes=1, max_jobs=4, drivers=2, prove_fn=rec) as srv:
+        jobs = [srv.submit(*_spec(i)) for i in range(3)]
+        srv.drain()
+    assert rec.max_running == 1
+    assert all(j.error is None for j in jobs)
+
+
+def test_job_errors_are_per_job():
+    rec = Recorder(fail_ids={1})
+    with ProofServer(budget_bytes=1 << 40, max_jobs=2, drivers=2, prove_fn=rec) as srv:
+        jobs = [srv.submit(*_spec(i)) for i in range(4)]
+        srv.drain()
+    assert isinstance(jobs[1].error, ValueError)
+    assert [j.error is None for j in jobs] == [True, False, True, True]
+    st = ServeStats(jobs, min(j.t_submit for j in jobs), max(j.t_done for j in jobs))
+    assert st.failed == 1 and st.jobs == 4
+
+
+def test_poisson_stream_and_quantiles():
+    rec = Recorder(delay=0.005)
+    with ProofServer(budget_bytes=1 << 40, max_jobs=2, drivers=2, prove_fn=rec) as srv:
+        jobs, st = serve_poisson(srv, [_spec(i) for i in range(12)], rate=200.0, seed=3)
+    assert st.jobs == 12 and st.failed == 0
+    assert st.p50_s <= st.p99_s
+    assert _quantile([1, 2, 3, 4], 0.5) == 2
+    assert _quantile([1, 2, 3, 4], 0.99) == 4
+    assert _quantile(list(range(1, 101)), 0.99) == 99
+    assert _quantile([], 0.5) is None
+
+
+def test_closed_server_rejects():
+    srv = ProofServer(budget_bytes=1 << 30, prove_fn=Recorder())
+    srv.close()
+    with pytest.raises(RuntimeError):
+        srv.submit(*_spec(0))

@@ -68,3 +68,19 @@ def test_sample_z_ood_avoids_domains():
     o = O.Transcript(b"z-ood")
     z2 = o.sample_ext3()
     assert list(z) == list(z2)  # first candidate is accepted with overwhelming probability
+
+
+def test_bulk_ext3_absorb_equals_one_by_one():
+    rng = np.random.default_rng(11)
+    vals = rng.integers(0, 2**64, size=(37, 3), dtype=np.uint64)
+    vals[0] = [0xFFFFFFFF00000001, 0xFFFFFFFFFFFFFFFF, 5]  # non-canonical inputs are canonicalised
+    a, b, c = mc.Transcript(b"bulk"), mc.Transcript(b"bulk"), O.Transcript(b"bulk")
+    a.sample_ext3()
+    b.sample_ext3()
+    c.sample_ext3()
+    a.append_ext3_many(vals)
+    for v in vals:
+        b.append_ext3(v)
+        c.append_ext3(v)
+    assert a.sample() == b.sample() == c.sample()
+    assert [int(x) for x in a.sample_ext3()] == [int(x) for x in b.sample_ext3()] == [int(x) for x in c.sample_ext3()]
