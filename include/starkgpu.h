@@ -331,6 +331,86 @@ SG_API int sg_eval_constraints(sg_ctx* ctx, void* stream, const sg_device_progra
 SG_API int sg_decompose_d2(sg_ctx* ctx, void* stream, const uint64_t* d_h, uint64_t lde_rows, const uint64_t* d_inv_2x,
                            uint64_t* d_out);
 
+/* ---- one table's rounds 2-4 in one call: the per-table body of the prover
+ *      (crypto/stark/src/prover.rs:3603-3977 rounds 2-3, 4433-4620 round 4,
+ *      fri/mod.rs:27-205 FRI commit and queries) over the kernels above:
+ *      LogUp aux + commit, beta, composition + decomposition + parts commit,
+ *      z_ood, OOD values (main and aux at z and z*w, parts at z^2), gamma,
+ *      DEEP, FRI layers, terminal coefficients, grinding, query indexes and
+ *      openings. `t` is the table's transcript fork (advanced in place).
+ *      Row-pair big-endian leaves throughout; the table's boundary
+ *      constraints are described by (b_col, b_is_aux, b_value) with their
+ *      zerofier inverses in d_b_z_inv. ---- */
+typedef struct sg_table_job {
+    /* main trace and its R1 commitment (device) */
+    const uint64_t* d_trace;      /* n x m */
+    const uint64_t* d_main_lde;   /* N x m, N = n * blowup */
+    const uint8_t* d_main_nodes;  /* node array of the main tree */
+    uint64_t main_leaves_len;     /* N / 2 */
+    uint64_t n, m;
+    uint32_t blowup;
+    uint64_t coset_offset;
+    /* domain vectors (device) */
+    const uint64_t* d_weights;      /* n: g^i / n */
+    const uint64_t* d_comp_weights; /* N/2: g^-j / (N/2) */
+    const uint64_t* d_z_inv;        /* blowup: 1 / (x^n - 1), cyclic over rows */
+    const uint64_t* d_b_z_inv;      /* num_boundary x N: boundary zerofier inverses */
+    const uint64_t* d_inv2x;        /* N/2: 1 / (2 x_i) */
+    const uint64_t* d_pts_n;        /* n: g * w_n^i */
+    const uint64_t* d_pts_N;        /* N: g * w_N^i */
+    const uint64_t* d_tw0;          /* N/2: 1 / x over the bit-reversed first FRI layer */
+    /* AIR */
+    const sg_logup_desc* logup;
+    const sg_device_program* program;
+    uint32_t num_boundary;
+    const uint64_t* b_col;    /* host: num_boundary */
+    const uint64_t* b_is_aux; /* host: num_boundary */
+    const uint64_t* b_value;  /* host: num_boundary ext3 */
+    /* challenges shared by the tables of the proof (host) */
+    const uint64_t* lookup_challenges; /* 2 ext3: LogUp z, alpha */
+    const uint64_t* alpha_pows;
+    uint32_t n_alpha;
+    /* options */
+    uint32_t queries;
+    uint32_t grinding;
+    uint32_t final_log_degree;
+} sg_table_job;
+
+/* Sizes of a table proof: A = aux_cols ext3 columns, W = m + A, Q = queries,
+ * D = depth (log2 N - 1), F = fri_layers committed FRI layers. */
+typedef struct sg_proof_shape {
+    uint64_t aux_cols;
+    uint32_t total_folds;
+    uint32_t fri_layers;
+    uint32_t terminal_coeffs;
+    uint32_t depth;
+    uint64_t fri_path_bytes; /* sum over layers l < F of Q * (D - 1 - l) * 32 */
+} sg_proof_shape;
+SG_API int sg_table_proof_shape(const sg_table_job* job, sg_proof_shape* shape);
+
+/* Caller-allocated host outputs of sg_prove_table. */
+typedef struct sg_table_proof {
+    uint8_t* aux_root;            /* 32 */
+    uint8_t* comp_root;           /* 32 */
+    uint64_t* table_contribution; /* ext3 */
+    uint64_t* trace_ood;          /* 2 x W ext3: [point][column], main then aux */
+    uint64_t* parts_ood;          /* 2 ext3 */
+    uint8_t* fri_roots;           /* F x 32 */
+    uint64_t* fri_final;          /* terminal_coeffs ext3 */
+    uint64_t* nonce;              /* 1 */
+    uint64_t* iotas;              /* Q */
+    uint64_t* open_main;          /* 2Q x m */
+    uint64_t* open_aux;           /* 2Q x 3A */
+    uint64_t* open_parts;         /* 2Q x 6 */
+    uint8_t* path_main;           /* Q x D x 32 */
+    uint8_t* path_aux;            /* Q x D x 32 */
+    uint8_t* path_parts;          /* Q x D x 32 */
+    uint64_t* fri_open;           /* F x 2Q ext3 */
+    uint8_t* fri_paths;           /* layer after layer: Q x (D - 1 - l) x 32 */
+} sg_table_proof;
+SG_API int sg_prove_table(sg_ctx* ctx, void* stream, sg_transcript* t, const sg_table_job* job,
+                          sg_table_proof* out);
+
 /* ---- synthetic chip-table trace (benchmark input generator; no counterpart in the
  *      reference, whose traces come from the VM executor): n x w row-major,
  *      element (r, c) = splitmix64(splitmix64(seed) + r*w + c) mod p, column w-2 a

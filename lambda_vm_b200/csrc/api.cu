@@ -14,6 +14,31 @@ static thread_local std::string g_err;
 void set_error(const std::string& msg) { g_err = msg; }
 const char* last_error() { return g_err.c_str(); }
 
+// Capacity classes: 512-byte granularity up to 2 MiB, then eight classes per
+// power of two (at most 12.5 % slack), so freed blocks fit later requests of
+// nearby sizes.
+static uint64_t cap_of(uint64_t b) {
+    if (b <= (2ull << 20)) return (b + 511) & ~511ull;
+    const int lg = 63 - __builtin_clzll(b);
+    const uint64_t step = 1ull << (lg - 3);
+    return (b + step - 1) & ~(step - 1);
+}
+
+void trim_cache(Ctx* ctx) {
+    std::vector<Ctx::Cached> blocks;
+    {
+        std::lock_guard<std::mutex> g(ctx->cache_mu);
+        for (auto& kv : ctx->free_blocks) blocks.push_back(kv.second);
+        ctx->free_blocks.clear();
+        ctx->cached_bytes = 0;
+    }
+    for (auto& b : blocks) {
+        cudaEventSynchronize(b.ev);
+        cudaFree(b.p);
+        cudaEventDestroy(b.ev);
+    }
+}
+
 int dev_alloc(Ctx* ctx, cudaStream_t st, uint64_t bytes, void** out) {
     *out = nullptr;
     if (bytes == 0) return SG_OK;
@@ -34,24 +59,76 @@ int dev_alloc(Ctx* ctx, cudaStream_t st, uint64_t bytes, void** out) {
     uint64_t pk = ctx->peak.load();
     while (cur > pk && !ctx->peak.compare_exchange_weak(pk, cur)) {
     }
-    cudaError_t e = cudaMallocAsync(out, bytes, st);
+    const uint64_t cap = cap_of(bytes);
+    {
+        std::lock_guard<std::mutex> g(ctx->cache_mu);
+        auto it = ctx->free_blocks.lower_bound(cap);
+        if (it != ctx->free_blocks.end() && it->first <= cap + cap / 4) {
+            Ctx::Cached b = it->second;
+            ctx->free_blocks.erase(it);
+            ctx->cached_bytes -= b.cap;
+            ctx->live_cap[b.p] = b.cap;
+            // The block's last use was on the freeing stream: order this stream after it.
+            cudaError_t e = cudaStreamWaitEvent(st, b.ev, 0);
+            ctx->spare_events.push_back(b.ev);
+            if (e != cudaSuccess) {
+                ctx->live_cap.erase(b.p);
+                ctx->in_use.fetch_sub(bytes);
+                set_error(std::string("cudaStreamWaitEvent: ") + cudaGetErrorString(e));
+                return SG_ERR_CUDA;
+            }
+            *out = b.p;
+            return SG_OK;
+        }
+    }
+    cudaError_t e = cudaMallocAsync(out, cap, st);
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        trim_cache(ctx);
+        e = cudaMallocAsync(out, cap, st);
+    }
     if (e != cudaSuccess) {
         ctx->in_use.fetch_sub(bytes);
         *out = nullptr;
         set_error(std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
         return e == cudaErrorMemoryAllocation ? SG_ERR_OOM : SG_ERR_CUDA;
     }
+    std::lock_guard<std::mutex> g(ctx->cache_mu);
+    ctx->live_cap[*out] = cap;
     return SG_OK;
 }
 
 int dev_free(Ctx* ctx, cudaStream_t st, void* p, uint64_t bytes) {
     if (!p) return SG_OK;
-    cudaError_t e = cudaFreeAsync(p, st);
     ctx->in_use.fetch_sub(bytes);
+    cudaEvent_t ev = nullptr;
+    uint64_t cap = 0;
+    {
+        std::lock_guard<std::mutex> g(ctx->cache_mu);
+        auto it = ctx->live_cap.find(p);
+        if (it == ctx->live_cap.end()) {
+            set_error("dev_free: pointer not allocated by this context");
+            return SG_ERR_INVALID;
+        }
+        cap = it->second;
+        ctx->live_cap.erase(it);
+        if (!ctx->spare_events.empty()) {
+            ev = ctx->spare_events.back();
+            ctx->spare_events.pop_back();
+        }
+    }
+    cudaError_t e = ev ? cudaSuccess : cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(ev, st);
     if (e != cudaSuccess) {
-        set_error(std::string("cudaFreeAsync: ") + cudaGetErrorString(e));
+        // Without an event the block cannot be reused safely: hand it back to the pool.
+        if (ev) cudaEventDestroy(ev);
+        cudaError_t e2 = cudaFreeAsync(p, st);
+        set_error(std::string("dev_free: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
         return SG_ERR_CUDA;
     }
+    std::lock_guard<std::mutex> g(ctx->cache_mu);
+    ctx->free_blocks.insert({cap, Ctx::Cached{p, cap, ev}});
+    ctx->cached_bytes += cap;
     return SG_OK;
 }
 
@@ -107,6 +184,9 @@ void sg_ctx_destroy(sg_ctx* c) {
     Ctx* ctx = C(c);
     if (!ctx) return;
     cudaDeviceSynchronize();
+    trim_cache(ctx);
+    for (auto& kv : ctx->live_cap) cudaFree(kv.first);
+    for (auto ev : ctx->spare_events) cudaEventDestroy(ev);
     for (auto& kv : ctx->roots) cudaFree(kv.second);
     delete ctx;
 }
@@ -252,12 +332,12 @@ int sg_merkle_build(sg_ctx* c, void* stream, const uint8_t* d_leaves, uint64_t n
 }  // extern "C"
 
 // Enqueue one table's commit on `st` without waiting on the host: weights and
-// trace upload (when given on the host), coset LDE, leaves, tree, and the root
-// copied to root_dst (pinned host memory, valid once `st` has drained). On
-// failure nothing stays allocated and *out is null.
+// trace upload (when given on the host), coset LDE, leaves and tree; the root
+// is node 0 of the handle's node array. On failure nothing stays allocated and
+// *out is null.
 static int commit_enqueue(Ctx* ctx, cudaStream_t st, const uint64_t* trace, int trace_on_device, uint64_t n,
                           uint64_t row_u64, uint32_t blowup, const uint64_t* weights, int weights_on_device,
-                          const sg_leaf_layout* layout, uint64_t* host_lde_out, sg_lde** out, uint8_t* root_dst) {
+                          const sg_leaf_layout* layout, uint64_t* host_lde_out, sg_lde** out) {
     SG_CHECK_ARG(out && trace && weights, "null argument");
     *out = nullptr;
     SG_CHECK_ARG(n >= 2 && log2_exact(n) >= 0, "n must be a power of two >= 2");
@@ -311,11 +391,6 @@ static int commit_enqueue(Ctx* ctx, cudaStream_t st, const uint64_t* trace, int 
         if (rc) break;
         rc = merkle_inner(ctx, st, h->d_nodes, L);
         if (rc) break;
-        if (cudaMemcpyAsync(root_dst, h->d_nodes, 32, cudaMemcpyDeviceToHost, st) != cudaSuccess) {
-            set_error("root download failed");
-            rc = SG_ERR_CUDA;
-            break;
-        }
         if (host_lde_out &&
             cudaMemcpyAsync(host_lde_out, h->d_lde, lde_rows * row_u64 * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess) {
             set_error("LDE download failed");
@@ -336,15 +411,6 @@ static int commit_enqueue(Ctx* ctx, cudaStream_t st, const uint64_t* trace, int 
     return SG_OK;
 }
 
-namespace {
-// Page-locked 32-byte root slots for asynchronous root copies.
-struct PinnedRoots {
-    uint8_t* p = nullptr;
-    ~PinnedRoots() {
-        if (p) cudaFreeHost(p);
-    }
-};
-}  // namespace
 
 extern "C" {
 
@@ -355,18 +421,15 @@ int sg_lde_commit(sg_ctx* c, void* stream, const uint64_t* trace, int trace_on_d
     *out = nullptr;
     Ctx* ctx = C(c);
     cudaStream_t st = (cudaStream_t)stream;
-    PinnedRoots pr;
-    SG_CUDA(cudaMallocHost((void**)&pr.p, 32));
     sg_lde* h = nullptr;
-    SG_TRY(commit_enqueue(ctx, st, trace, trace_on_device, n, row_u64, blowup, weights, 0, layout, host_lde_out, &h,
-                          pr.p));
-    cudaError_t e = cudaStreamSynchronize(st);
+    SG_TRY(commit_enqueue(ctx, st, trace, trace_on_device, n, row_u64, blowup, weights, 0, layout, host_lde_out, &h));
+    cudaError_t e = cudaMemcpyAsync(h->root, h->d_nodes, 32, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
         set_error(std::string("lde commit: ") + cudaGetErrorString(e));
         sg_lde_free(c, h);
         return SG_ERR_CUDA;
     }
-    memcpy(h->root, pr.p, 32);
     if (root_out) memcpy(root_out, h->root, 32);
     *out = h;
     return SG_OK;
@@ -388,8 +451,10 @@ int sg_batch_commit(sg_ctx* c, void* stream, const sg_table_desc* tables, uint32
     uint32_t k = concurrency == 0 ? 1 : concurrency;
     if (k > count) k = count;
     if (k > 32) k = 32;
-    PinnedRoots pr;
-    SG_CUDA(cudaMallocHost((void**)&pr.p, 32ull * count));
+    // Roots are gathered on the device and read back with one copy after the join.
+    uint8_t* d_roots = nullptr;
+    SG_TRY(dev_alloc(ctx, caller, 32ull * count, (void**)&d_roots));
+    std::vector<uint8_t> roots(32ull * count);
     std::vector<cudaStream_t> streams(k, nullptr);
     std::vector<cudaEvent_t> done(k, nullptr);
     cudaEvent_t start = nullptr;
@@ -414,7 +479,11 @@ int sg_batch_commit(sg_ctx* c, void* stream, const sg_table_desc* tables, uint32
         const sg_table_desc& d = tables[i];
         const sg_leaf_layout* lay = d.layout.rows_per_leaf ? &d.layout : nullptr;
         rc = commit_enqueue(ctx, streams[j % k], d.trace, d.trace_on_device, d.n, d.row_u64, d.blowup, d.weights,
-                            d.weights_on_device, lay, nullptr, &out_ldes[i], pr.p + 32ull * i);
+                            d.weights_on_device, lay, nullptr, &out_ldes[i]);
+        if (rc == SG_OK)
+            cuda_ok(cudaMemcpyAsync(d_roots + 32ull * i, out_ldes[i]->d_nodes, 32, cudaMemcpyDeviceToDevice,
+                                    streams[j % k]),
+                    "root copy");
     }
     // Join: the caller's stream waits for every driver stream; the roots are
     // host-visible once it drains.
@@ -424,9 +493,12 @@ int sg_batch_commit(sg_ctx* c, void* stream, const sg_table_desc* tables, uint32
             cuda_ok(cudaStreamWaitEvent(caller, done[s], 0), "stream wait");
         }
     }
+    if (rc == SG_OK) cuda_ok(cudaMemcpyAsync(roots.data(), d_roots, 32ull * count, cudaMemcpyDeviceToHost, caller),
+                             "roots download");
     for (uint32_t s = 0; s < k; ++s)
         if (streams[s]) cuda_ok(cudaStreamSynchronize(streams[s]), "sync");
     cuda_ok(cudaStreamSynchronize(caller), "sync");
+    dev_free(ctx, caller, d_roots, 32ull * count);
     for (uint32_t s = 0; s < k; ++s) {
         if (done[s]) cudaEventDestroy(done[s]);
         if (streams[s]) cudaStreamDestroy(streams[s]);
@@ -444,7 +516,7 @@ int sg_batch_commit(sg_ctx* c, void* stream, const sg_table_desc* tables, uint32
         return rc;
     }
     for (uint32_t i = 0; i < count; ++i) {
-        memcpy(out_ldes[i]->root, pr.p + 32ull * i, 32);
+        memcpy(out_ldes[i]->root, roots.data() + 32ull * i, 32);
         if (roots_out) memcpy(roots_out + 32ull * i, out_ldes[i]->root, 32);
     }
     return SG_OK;

@@ -9,6 +9,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/starkgpu.h"
 
@@ -67,7 +68,25 @@ struct Ctx {
     // Fault injection for host-side failure tests: when > 0, the next
     // allocation that would bring the count to zero fails with SG_ERR_OOM.
     std::atomic<int64_t> fail_alloc_after{-1};
+    // Stream-ordered block cache: freed blocks stay with the context, keyed by
+    // capacity, each with the event recorded on the freeing stream; a later
+    // allocation on any stream waits on that event before reusing the block.
+    // Steady-state proofs then allocate without driver calls (growing the
+    // driver pool maps physical memory and can stall for hundreds of ms).
+    struct Cached {
+        void* p;
+        uint64_t cap;
+        cudaEvent_t ev;
+    };
+    std::mutex cache_mu;
+    std::multimap<uint64_t, Cached> free_blocks;
+    std::map<void*, uint64_t> live_cap;
+    std::vector<cudaEvent_t> spare_events;
+    uint64_t cached_bytes = 0;
 };
+
+// Return every cached block to the driver pool (on OOM, and at teardown).
+void trim_cache(Ctx* ctx);
 
 // Stream-ordered allocation charged against the context budget.
 int dev_alloc(Ctx* ctx, cudaStream_t st, uint64_t bytes, void** out);

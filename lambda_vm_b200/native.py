@@ -57,6 +57,30 @@ class LogupDesc(C.Structure):
                 ("out_col_offsets", C.c_void_p), ("out_col_interactions", C.c_void_p), ("mult_consts", C.c_void_p),
                 ("mult_term_offsets", C.c_void_p), ("mult_term_coefs", C.c_void_p), ("mult_term_cols", C.c_void_p),
                 ("num_committed", C.c_uint32)]
+class TableJob(C.Structure):
+    _fields_ = [("d_trace", C.c_void_p), ("d_main_lde", C.c_void_p), ("d_main_nodes", C.c_void_p),
+                ("main_leaves_len", C.c_uint64), ("n", C.c_uint64), ("m", C.c_uint64), ("blowup", C.c_uint32),
+                ("coset_offset", C.c_uint64), ("d_weights", C.c_void_p), ("d_comp_weights", C.c_void_p),
+                ("d_z_inv", C.c_void_p), ("d_b_z_inv", C.c_void_p), ("d_inv2x", C.c_void_p), ("d_pts_n", C.c_void_p),
+                ("d_pts_N", C.c_void_p), ("d_tw0", C.c_void_p), ("logup", C.c_void_p), ("program", C.c_void_p),
+                ("num_boundary", C.c_uint32), ("b_col", C.c_void_p), ("b_is_aux", C.c_void_p),
+                ("b_value", C.c_void_p), ("lookup_challenges", C.c_void_p), ("alpha_pows", C.c_void_p),
+                ("n_alpha", C.c_uint32), ("queries", C.c_uint32), ("grinding", C.c_uint32),
+                ("final_log_degree", C.c_uint32)]
+
+
+class ProofShape(C.Structure):
+    _fields_ = [("aux_cols", C.c_uint64), ("total_folds", C.c_uint32), ("fri_layers", C.c_uint32),
+                ("terminal_coeffs", C.c_uint32), ("depth", C.c_uint32), ("fri_path_bytes", C.c_uint64)]
+
+
+class TableProof(C.Structure):
+    _fields_ = [(nm, C.c_void_p) for nm in ("aux_root", "comp_root", "table_contribution", "trace_ood", "parts_ood",
+                                            "fri_roots", "fri_final", "nonce", "iotas", "open_main", "open_aux",
+                                            "open_parts", "path_main", "path_aux", "path_parts", "fri_open",
+                                            "fri_paths")]
+
+
 PROTOTYPES = {
     "sg_ctx_create": (i32, [i32, u64, C.POINTER(vp)]),
     "sg_ctx_destroy": (None, [vp]),
@@ -86,6 +110,8 @@ PROTOTYPES = {
     "sg_lde_free": (None, [vp, vp]),
     "sg_lde_free_async": (None, [vp, vp, vp]),
     "sg_batch_commit": (i32, [vp, vp, vp, u32, u32, vp, vp]),
+    "sg_table_proof_shape": (i32, [vp, vp]),
+    "sg_prove_table": (i32, [vp, vp, vp, vp, vp]),
     "sg_grind": (i32, [vp, vp, vp, C.c_uint8, C.POINTER(u64)]),
     "sg_coset_lde_static": (i32, [vp, vp, u64, u64, u32, vp, vp]),
     "sg_transcript_new": (vp, [vp, u64]),

@@ -167,6 +167,7 @@ def _build_domain(bk, log_n, B, g):
     wB = F.root_of_unity(B.bit_length() - 1)
     d.z_inv = bk.inv_base(np.array([(gn * pow(wB, k, P) - 1) % P for k in range(B)], np.uint64))
     pts_N = F.coset_points(log_N, g)
+    d.z_inv_dev = bk.upload(d.z_inv.reshape(-1, 1))
     d.b_z_inv = bk.upload(bk.inv_base(F.sub(pts_N, np.uint64(1))).reshape(1, -1))  # 1/(x - 1)
     d.inv2x = bk.upload(bk.inv_base(F.add(pts_N[: N // 2], pts_N[: N // 2])).reshape(-1, 1))
     d.pts_N = bk.upload(pts_N.reshape(-1, 1))
@@ -178,6 +179,7 @@ def _build_domain(bk, log_n, B, g):
 
 class GpuBackend:
     name = "gpu"
+    native_rounds = True
 
     def __init__(self, be=None, stream=None):
         self.be = be or _backend()
@@ -264,6 +266,80 @@ class GpuBackend:
         root = (C.c_uint8 * 32)()
         native.check(self.L.sg_merkle_build(self.be.h, self.st, leaves_buf.ptr, nl, tree.buf.ptr, root))
         return tree, bytes(root)
+
+    @staticmethod
+    def _logup_struct(desc, keep):
+        def arr(name, dt):
+            a = np.ascontiguousarray(desc[name], dt)
+            keep[name] = a if a.size else np.zeros(1, dt)
+            return keep[name].ctypes.data
+
+        d = native.LogupDesc()
+        d.num_interactions = desc["num_interactions"]
+        for nm, dt in (("bus_ids", np.uint64), ("elem_offsets", np.uint32), ("elem_alpha_idx", np.uint32),
+                       ("elem_consts", np.uint64), ("term_offsets", np.uint32), ("term_coefs", np.uint64),
+                       ("term_cols", np.uint32), ("out_col_offsets", np.uint32), ("out_col_interactions", np.uint32),
+                       ("mult_consts", np.uint64), ("mult_term_offsets", np.uint32), ("mult_term_coefs", np.uint64),
+                       ("mult_term_cols", np.uint32)):
+            setattr(d, nm, arr(nm, dt))
+        d.num_out_cols = desc["num_out_cols"]
+        d.num_committed = desc["num_committed"]
+        return d
+
+    def prove_table_native(self, air, lowered, trace_mat, main_lde, main_tree, t, challenges, alpha_pows, opts):
+        """Rounds 2-4 of one table in one library call (sg_prove_table); the
+        same proof fields, in the same format, as prove_table's step-by-step path."""
+        keep = {}
+        B, g = opts.blowup, opts.coset_offset
+        dom = self.domain(air.log_n, B, g)
+        ld = self._logup_struct(air.logup_descriptor(), keep)
+        kp = []
+        prog = mc._program_struct(lowered, kp)
+        nb = len(air.boundary)
+        bcol = np.array([b[0] for b in air.boundary] or [0], np.uint64)
+        bis = np.array([1 if b[1] else 0 for b in air.boundary] or [0], np.uint64)
+        bval = np.zeros(3 * max(nb, 1), np.uint64)
+        ch = np.array([challenges[0], challenges[1]], np.uint64).reshape(-1)
+        al = np.ascontiguousarray(alpha_pows, np.uint64).reshape(-1)
+        j = native.TableJob(trace_mat.ptr, main_lde.ptr, main_tree.buf.ptr, main_tree.leaves_len, air.n, air.width,
+                            B, g, dom.weights.ptr, dom.comp_weights.ptr, dom.z_inv_dev.ptr, dom.b_z_inv.ptr,
+                            dom.inv2x.ptr, dom.pts_n.ptr, dom.pts_N.ptr, dom.tw0.ptr, C.addressof(ld),
+                            C.addressof(prog), nb, bcol.ctypes.data, bis.ctypes.data, bval.ctypes.data,
+                            ch.ctypes.data, al.ctypes.data, len(alpha_pows), opts.queries, opts.grinding,
+                            opts.final_log_degree)
+        shp = native.ProofShape()
+        native.check(self.L.sg_table_proof_shape(C.byref(j), C.byref(shp)))
+        A, Q, D, Fl = shp.aux_cols, opts.queries, shp.depth, shp.fri_layers
+        W = air.width + A
+        u8, u64 = np.uint8, np.uint64
+        buf = {"aux_root": np.zeros(32, u8), "comp_root": np.zeros(32, u8), "table_contribution": np.zeros(3, u64),
+               "trace_ood": np.zeros((2, W, 3), u64), "parts_ood": np.zeros((2, 3), u64),
+               "fri_roots": np.zeros((max(Fl, 1), 32), u8), "fri_final": np.zeros((shp.terminal_coeffs, 3), u64),
+               "nonce": np.zeros(1, u64), "iotas": np.zeros(max(Q, 1), u64),
+               "open_main": np.zeros((2 * Q, air.width), u64), "open_aux": np.zeros((2 * Q, 3 * A), u64),
+               "open_parts": np.zeros((2 * Q, 6), u64), "path_main": np.zeros((Q, D, 32), u8),
+               "path_aux": np.zeros((Q, D, 32), u8), "path_parts": np.zeros((Q, D, 32), u8),
+               "fri_open": np.zeros((max(Fl, 1), 2 * Q, 3), u64), "fri_paths": np.zeros(max(1, shp.fri_path_bytes), u8)}
+        o = native.TableProof(*[buf[k].ctypes.data for k in (
+            "aux_root", "comp_root", "table_contribution", "trace_ood", "parts_ood", "fri_roots", "fri_final", "nonce",
+            "iotas", "open_main", "open_aux", "open_parts", "path_main", "path_aux", "path_parts", "fri_open",
+            "fri_paths")])
+        native.check(self.L.sg_prove_table(self.be.h, self.st, t.h, C.byref(j), C.byref(o)))
+        fri_paths, off = [], 0
+        for li in range(Fl):
+            d = D - 1 - li
+            fri_paths.append(buf["fri_paths"][off:off + Q * d * 32].reshape(Q, d, 32))
+            off += Q * d * 32
+        return {"aux_root": buf["aux_root"].tobytes(), "table_contribution": tuple(buf["table_contribution"].tolist()),
+                "comp_root": buf["comp_root"].tobytes(),
+                "trace_ood": [[tuple(v) for v in row] for row in buf["trace_ood"].tolist()],
+                "parts_ood": [tuple(v) for v in buf["parts_ood"].tolist()],
+                "fri_roots": [buf["fri_roots"][i].tobytes() for i in range(Fl)],
+                "fri_final_coeffs": [tuple(v) for v in buf["fri_final"].tolist()], "nonce": int(buf["nonce"][0]),
+                "iotas": buf["iotas"][:Q].tolist(), "open_main": buf["open_main"], "open_aux": buf["open_aux"],
+                "open_parts": buf["open_parts"], "path_main": buf["path_main"], "path_aux": buf["path_aux"],
+                "path_parts": buf["path_parts"], "fri_open": [buf["fri_open"][i] for i in range(Fl)],
+                "fri_paths": fri_paths}
 
     def logup_aux(self, trace, desc, alpha_pows, z):
         keep = {}
@@ -461,8 +537,15 @@ def _ood_scale(z, n, g):
     return F.f3scale(F.f3sub(F.f3pow(z, n), (gn, 0, 0)), s)
 
 
-def prove_table(bk, air, lowered, trace_mat, main_lde, main_tree, t, challenges, alpha_pows, opts):
-    """Aux build + rounds 2-4 for one table (prover.rs:3603-3977, 4433-4620)."""
+def prove_table(bk, air, lowered, trace_mat, main_lde, main_tree, t, challenges, alpha_pows, opts, native_rounds=None):
+    """Aux build + rounds 2-4 for one table (prover.rs:3603-3977, 4433-4620).
+    On the GPU backend the whole sequence runs as one library call
+    (sg_prove_table) unless native_rounds is False, which drives the same steps
+    one backend operation at a time from here."""
+    if native_rounds is None:
+        native_rounds = getattr(bk, "native_rounds", False)
+    if native_rounds:
+        return bk.prove_table_native(air, lowered, trace_mat, main_lde, main_tree, t, challenges, alpha_pows, opts)
     n, N = air.n, air.n * opts.blowup
     B, g = opts.blowup, opts.coset_offset
     log_n, log_N = air.log_n, air.log_n + (B.bit_length() - 1)

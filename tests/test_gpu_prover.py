@@ -51,3 +51,17 @@ def test_scheduled_prover_matches_plain_and_verifies(be):
     host = multi_prove(airs[:2], [a.trace(s) for a, s in zip(airs[:2], seeds[:2])], opts, GpuBackend(be))
     dev = multi_prove(airs[:2], seeds[:2], opts, GpuBackend(be))
     assert diff(host, dev) is None
+
+
+def test_native_table_driver_matches_step_by_step_driver(be):
+    """sg_prove_table (rounds 2-4 of a table in one library call) gives the
+    same proof as driving the same kernels one operation at a time."""
+    opts = Options(blowup=2, grinding=8, final_log_degree=3, queries=11)
+    airs = [SynthTableAir(9, 13, 4), SynthTableAir(6, 8, 2), SynthTableAir(10, 40, 6)]
+    seeds = [300 + i for i in range(len(airs))]
+    step = GpuBackend(be)
+    step.native_rounds = False
+    a = multi_prove(airs, seeds, opts, step)
+    b = multi_prove(airs, seeds, opts, GpuBackend(be))
+    assert diff(a, b) is None, diff(a, b)
+    assert verify(airs, b, opts) == (True, "ok")
