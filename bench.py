@@ -482,7 +482,7 @@ def main():
     # traffic grows in proportion to the columns (same passes, same tiles).
     traffic, traffic_src = None, None
     if dom == "lde" and a.log_n == 20 and B == 4:
-        traffic = round(2.105714944e9 * m / 16)
+        traffic = round(2.086977024e9 * m / 16)
         traffic_src = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the 4 k_dft launches of one "
                        "2^20 x 16 blowup-4 LDE, x m/16 (profiles/k_dft_coset_lde_1048576x16_blowup4.md)")
     achieved = alg[dom] / (med[dom] * 1e-3) / 1e9

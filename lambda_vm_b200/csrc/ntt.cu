@@ -122,8 +122,14 @@ struct PassArgs {
 #ifndef SG_DFT_QMAX
 #define SG_DFT_QMAX 4
 #endif
+#ifndef SG_DFT_C10
+#define SG_DFT_C10 16
+#endif
 #ifndef SG_DFT_T10
-#define SG_DFT_T10 256
+#define SG_DFT_T10 512
+#endif
+#ifndef SG_DFT_T11
+#define SG_DFT_T11 512
 #endif
 template <int LOGL>
 struct Plan {
@@ -132,8 +138,10 @@ struct Plan {
     static constexpr int q(int s) { return NST == 0 ? 0 : LOGL / NST + (s < LOGL % NST ? 1 : 0); }
     static constexpr int lgns(int s) { return s == 0 ? 0 : lgns(s - 1) + q(s - 1); }
     static constexpr int Q1 = q(0);
-    static constexpr int C = LOGL <= 7 ? 32 : (LOGL <= 9 ? 16 : (LOGL <= 11 ? 8 : 4));
-    static constexpr int T = LOGL >= 11 ? 512 : (LOGL == 10 ? SG_DFT_T10 : 256);
+    static constexpr int C = LOGL <= 7 ? 32 : (LOGL <= 9 ? 16 : (LOGL == 10 ? SG_DFT_C10 : (LOGL <= 11 ? 8 : 4)));
+    static constexpr int T = LOGL >= 12 ? 512 : (LOGL == 11 ? SG_DFT_T11 : (LOGL == 10 ? SG_DFT_T10 : 256));
+    // CTAs per SM the register allocation must allow (64K registers per SM).
+    static constexpr int MINB = T <= 256 ? 2 : (T <= 512 && LOGL == 10 ? 2 : 1);
     static constexpr uint32_t L = 1u << LOGL;
     static constexpr uint32_t CS0 = L + (NST > 1 ? (L >> Q1) : 0);
     static constexpr uint32_t CP = C < 16 ? C : 16;
@@ -306,7 +314,7 @@ __device__ __forceinline__ void tile_body(const PassArgs& a, uint64_t* S, const 
 // One instantiation per (tile length, direction): each launch carries only the
 // butterfly code it runs, which keeps the unrolled networks in the I-cache.
 template <int LOGL, bool INV>
-__global__ void __launch_bounds__(Plan<LOGL>::T, Plan<LOGL>::T == 256 ? 2 : (LOGL == 10 ? 2 : 1))
+__global__ void __launch_bounds__(Plan<LOGL>::T, Plan<LOGL>::MINB)
     k_dft(PassArgs a, uint64_t ntiles, uint32_t ctiles) {
     using PL = Plan<LOGL>;
     extern __shared__ uint64_t sm[];
