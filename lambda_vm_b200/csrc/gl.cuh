@@ -60,37 +60,31 @@ __device__ __forceinline__ uint64_t sub(uint64_t a, uint64_t b) {
     return r;
 }
 
-// Reduce the 128-bit value (x3:x2:x1:x0) mod p using 2^64 = EPS, 2^96 = -1.
+// Reduce the 128-bit value (x3:x2:x1:x0) mod p using 2^64 = EPS, 2^96 = -1:
+// V = (x1:x0) + x2 * EPS - x3. The x2 * EPS term is a 32x32 multiply-add on
+// the FMA pipe into the low word pair (S < 2^65, carry c); subtracting x3
+// leaves c' = c - borrow in {-1, 0, 1}, and V = s + c' * 2^64 = s + c' * EPS
+// with no further wrap (S <= 2^65 - 2^33, so s + EPS < 2^64 when c' = 1; and
+// c' = -1 only when s >= 2^64 - x3 > EPS). c' * EPS mod 2^64 has low word -c'
+// and high word sign(c').
 __device__ __forceinline__ uint64_t reduce128(uint32_t x0, uint32_t x1, uint32_t x2, uint32_t x3) {
-    // t0 = lo - hi_hi, folding a borrow as -EPS (cannot borrow twice).
-    uint32_t t0, t1, b;
-    asm("sub.cc.u32 %0, %3, %5;\n\t"
-        "subc.cc.u32 %1, %4, 0;\n\t"
-        "subc.u32 %2, 0, 0;"
-        : "=r"(t0), "=r"(t1), "=r"(b)
-        : "r"(x0), "r"(x1), "r"(x3));
-    asm("sub.cc.u32 %0, %0, %2;\n\t"
-        "subc.u32 %1, %1, 0;"
-        : "+r"(t0), "+r"(t1)
-        : "r"(b));
-    // u = hi_lo * EPS = (x2 << 32) - x2
-    uint32_t u0, u1;
-    asm("sub.cc.u32 %0, 0, %2;\n\t"
-        "subc.u32 %1, %2, 0;"
-        : "=r"(u0), "=r"(u1)
-        : "r"(x2));
-    // r = t + u, carry folds +EPS (cannot carry twice).
-    uint32_t c;
-    asm("add.cc.u32 %0, %0, %3;\n\t"
-        "addc.cc.u32 %1, %1, %4;\n\t"
+    uint32_t s0, s1, c;
+    asm("mad.lo.cc.u32 %0, %3, %5, %4;\n\t"
+        "madc.hi.cc.u32 %1, %3, %5, %6;\n\t"
         "addc.u32 %2, 0, 0;"
-        : "+r"(t0), "+r"(t1), "=r"(c)
-        : "r"(u0), "r"(u1));
+        : "=r"(s0), "=r"(s1), "=r"(c)
+        : "r"(x2), "r"(x0), "r"(0xFFFFFFFFu), "r"(x1));
+    asm("sub.cc.u32 %0, %0, %3;\n\t"
+        "subc.cc.u32 %1, %1, 0;\n\t"
+        "subc.u32 %2, %2, 0;"
+        : "+r"(s0), "+r"(s1), "+r"(c)
+        : "r"(x3));
+    const uint32_t lo = 0u - c, hi = (uint32_t)((int32_t)c >> 31);
     asm("add.cc.u32 %0, %0, %2;\n\t"
-        "addc.u32 %1, %1, 0;"
-        : "+r"(t0), "+r"(t1)
-        : "r"(0u - c));
-    return pack(t0, t1);
+        "addc.u32 %1, %1, %3;"
+        : "+r"(s0), "+r"(s1)
+        : "r"(lo), "r"(hi));
+    return pack(s0, s1);
 }
 
 // Full 64x64 -> 128 product as four 32-bit limbs.
