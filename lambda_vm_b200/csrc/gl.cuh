@@ -20,25 +20,28 @@ __device__ __forceinline__ uint64_t pack(uint32_t lo, uint32_t hi) {
 
 __device__ __forceinline__ uint64_t canon(uint64_t a) { return a >= GL_P ? a - GL_P : a; }
 
-// a + b mod p. One conditional EPS fold per carry; the second carry can only
-// occur when both inputs are >= p.
+// a + b mod p. The carry c of the 64-bit sum is folded as c * EPS with a
+// 32-bit multiply-add (FMA pipe), whose own carry w is folded the same way;
+// that second fold cannot carry (after a wrap the sum is < EPS - 1). The
+// additions and the two carry reads stay on the ALU pipe, which the
+// butterflies saturate, while the FMA pipe has room.
 __device__ __forceinline__ uint64_t add(uint64_t a, uint64_t b) {
-    uint32_t r0, r1, c;
+    uint32_t r0, r1, c, w;
     asm("add.cc.u32 %0, %3, %5;\n\t"
         "addc.cc.u32 %1, %4, %6;\n\t"
         "addc.u32 %2, 0, 0;"
         : "=r"(r0), "=r"(r1), "=r"(c)
         : "r"(lo32(a)), "r"(hi32(a)), "r"(lo32(b)), "r"(hi32(b)));
-    uint32_t fix = 0u - c;  // 0 or 0xFFFFFFFF == EPS
-    uint32_t c2;
-    asm("add.cc.u32 %0, %0, %3;\n\t"
-        "addc.cc.u32 %1, %1, 0;\n\t"
+    asm("mad.lo.cc.u32 %0, %3, %4, %0;\n\t"
+        "madc.hi.cc.u32 %1, %3, %4, %1;\n\t"
         "addc.u32 %2, 0, 0;"
-        : "+r"(r0), "+r"(r1), "=r"(c2)
-        : "r"(fix));
-    uint64_t r = pack(r0, r1);
-    if (c2) r += GL_EPS;  // r < EPS after a second wrap, so this cannot carry
-    return r;
+        : "+r"(r0), "+r"(r1), "=r"(w)
+        : "r"(c), "r"(0xFFFFFFFFu));
+    asm("mad.lo.cc.u32 %0, %2, %3, %0;\n\t"
+        "madc.hi.u32 %1, %2, %3, %1;"
+        : "+r"(r0), "+r"(r1)
+        : "r"(w), "r"(0xFFFFFFFFu));
+    return pack(r0, r1);
 }
 
 // a - b mod p.
