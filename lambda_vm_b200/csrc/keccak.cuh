@@ -52,43 +52,47 @@ __device__ __forceinline__ void permute(uint64_t s[25]) {
     // call sites; within a round every lane index is still a constant.
 #pragma unroll 1
     for (int round = 0; round < 24; ++round) {
-        uint64_t C[5], D[5];
+        // theta: A[x,y] ^= C[x-1] ^ rotl1(C[x+1]), written as one 3-input XOR
+        // per lane half (a single LOP3) instead of materialising D first.
+        uint64_t C[5], R[5];
 #pragma unroll
         for (int x = 0; x < 5; ++x) C[x] = xor5(s[x], s[x + 5], s[x + 10], s[x + 15], s[x + 20]);
 #pragma unroll
-        for (int x = 0; x < 5; ++x) D[x] = C[(x + 4) % 5] ^ rotl<1>(C[(x + 1) % 5]);
+        for (int x = 0; x < 5; ++x) R[x] = rotl<1>(C[x]);
+#define D(x) C[((x) + 4) % 5] ^ R[((x) + 1) % 5]
         uint64_t B[25];
         // B[y + 5*((2x+3y)%5)] = rot(A[x+5y] ^ D[x], r[x][y])
-        B[0] = s[0] ^ D[0];
-        B[10] = rotl<1>(s[1] ^ D[1]);
-        B[20] = rotl<62>(s[2] ^ D[2]);
-        B[5] = rotl<28>(s[3] ^ D[3]);
-        B[15] = rotl<27>(s[4] ^ D[4]);
-        B[16] = rotl<36>(s[5] ^ D[0]);
-        B[1] = rotl<44>(s[6] ^ D[1]);
-        B[11] = rotl<6>(s[7] ^ D[2]);
-        B[21] = rotl<55>(s[8] ^ D[3]);
-        B[6] = rotl<20>(s[9] ^ D[4]);
-        B[7] = rotl<3>(s[10] ^ D[0]);
-        B[17] = rotl<10>(s[11] ^ D[1]);
-        B[2] = rotl<43>(s[12] ^ D[2]);
-        B[12] = rotl<25>(s[13] ^ D[3]);
-        B[22] = rotl<39>(s[14] ^ D[4]);
-        B[23] = rotl<41>(s[15] ^ D[0]);
-        B[8] = rotl<45>(s[16] ^ D[1]);
-        B[18] = rotl<15>(s[17] ^ D[2]);
-        B[3] = rotl<21>(s[18] ^ D[3]);
-        B[13] = rotl<8>(s[19] ^ D[4]);
-        B[14] = rotl<18>(s[20] ^ D[0]);
-        B[24] = rotl<2>(s[21] ^ D[1]);
-        B[9] = rotl<61>(s[22] ^ D[2]);
-        B[19] = rotl<56>(s[23] ^ D[3]);
-        B[4] = rotl<14>(s[24] ^ D[4]);
+        B[0] = s[0] ^ D(0);
+        B[10] = rotl<1>(s[1] ^ D(1));
+        B[20] = rotl<62>(s[2] ^ D(2));
+        B[5] = rotl<28>(s[3] ^ D(3));
+        B[15] = rotl<27>(s[4] ^ D(4));
+        B[16] = rotl<36>(s[5] ^ D(0));
+        B[1] = rotl<44>(s[6] ^ D(1));
+        B[11] = rotl<6>(s[7] ^ D(2));
+        B[21] = rotl<55>(s[8] ^ D(3));
+        B[6] = rotl<20>(s[9] ^ D(4));
+        B[7] = rotl<3>(s[10] ^ D(0));
+        B[17] = rotl<10>(s[11] ^ D(1));
+        B[2] = rotl<43>(s[12] ^ D(2));
+        B[12] = rotl<25>(s[13] ^ D(3));
+        B[22] = rotl<39>(s[14] ^ D(4));
+        B[23] = rotl<41>(s[15] ^ D(0));
+        B[8] = rotl<45>(s[16] ^ D(1));
+        B[18] = rotl<15>(s[17] ^ D(2));
+        B[3] = rotl<21>(s[18] ^ D(3));
+        B[13] = rotl<8>(s[19] ^ D(4));
+        B[14] = rotl<18>(s[20] ^ D(0));
+        B[24] = rotl<2>(s[21] ^ D(1));
+        B[9] = rotl<61>(s[22] ^ D(2));
+        B[19] = rotl<56>(s[23] ^ D(3));
+        B[4] = rotl<14>(s[24] ^ D(4));
 #pragma unroll
         for (int y = 0; y < 5; ++y) {
 #pragma unroll
             for (int x = 0; x < 5; ++x) s[x + 5 * y] = chi(B[x + 5 * y], B[(x + 1) % 5 + 5 * y], B[(x + 2) % 5 + 5 * y]);
         }
+#undef D
         s[0] ^= RC[round];
     }
 }
