@@ -331,6 +331,52 @@ int sg_merkle_build(sg_ctx* c, void* stream, const uint8_t* d_leaves, uint64_t n
 
 }  // extern "C"
 
+// Host trace -> LDE with the upload overlapped: the columns go up in chunks
+// of kChunkCols on a copy stream (one strided copy each), and each chunk's
+// LDE starts on `st` as soon as its copy lands, so the PCIe transfer of the
+// later chunks runs under the DFT passes of the earlier ones. With a
+// page-locked host trace the copies are asynchronous; with pageable memory
+// they are staged by the driver and the overlap is lost, not the result.
+static constexpr uint64_t kChunkCols = 64;
+
+static int upload_and_lde(Ctx* ctx, cudaStream_t st, const uint64_t* h_trace, uint64_t* d_trace, uint64_t n,
+                          uint64_t m, uint64_t blowup, const uint64_t* d_w, uint64_t* d_lde) {
+    const uint64_t chunk = m >= 2 * kChunkCols ? kChunkCols : m;
+    const uint64_t nchunks = (m + chunk - 1) / chunk;
+    cudaStream_t cs = nullptr;
+    std::vector<cudaEvent_t> ev(nchunks + 1, nullptr);
+    int rc = SG_OK;
+    auto ok = [&](cudaError_t e, const char* what) {
+        if (e != cudaSuccess && rc == SG_OK) {
+            set_error(std::string("trace upload: ") + what + ": " + cudaGetErrorString(e));
+            rc = SG_ERR_CUDA;
+        }
+        return rc == SG_OK;
+    };
+    if (ok(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "stream")) {
+        for (auto& e : ev)
+            if (!ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event")) break;
+    }
+    // the copy stream starts after d_trace is valid in `st`'s order
+    if (rc == SG_OK && ok(cudaEventRecord(ev[nchunks], st), "record")) ok(cudaStreamWaitEvent(cs, ev[nchunks], 0), "wait");
+    for (uint64_t k = 0; k < nchunks && rc == SG_OK; ++k) {
+        const uint64_t c0 = k * chunk, w = m - c0 < chunk ? m - c0 : chunk;
+        if (!ok(cudaMemcpy2DAsync(d_trace + c0, m * 8, h_trace + c0, m * 8, w * 8, n, cudaMemcpyHostToDevice, cs),
+                "copy"))
+            break;
+        if (!ok(cudaEventRecord(ev[k], cs), "record") || !ok(cudaStreamWaitEvent(st, ev[k], 0), "wait")) break;
+        rc = coset_lde_ld(ctx, st, d_trace + c0, m, n, w, blowup, d_w, d_lde + c0, m);
+    }
+    // On success the copy stream's work is ordered before `st` through the
+    // events; after a failure part of it may not be, so drain it before the
+    // caller frees the buffers. Its resources are released once it completes.
+    if (cs && rc != SG_OK) cudaStreamSynchronize(cs);
+    if (cs) cudaStreamDestroy(cs);
+    for (auto e : ev)
+        if (e) cudaEventDestroy(e);
+    return rc;
+}
+
 // Enqueue one table's commit on `st` without waiting on the host: weights and
 // trace upload (when given on the host), coset LDE, leaves and tree; the root
 // is node 0 of the handle's node array. On failure nothing stays allocated and
@@ -374,18 +420,13 @@ static int commit_enqueue(Ctx* ctx, cudaStream_t st, const uint64_t* trace, int 
             }
             w = d_w;
         }
-        const uint64_t* src = trace;
-        if (!trace_on_device) {
+        if (trace_on_device) {
+            rc = coset_lde(ctx, st, trace, n, row_u64, blowup, w, h->d_lde);
+        } else {
             rc = dev_alloc(ctx, st, trace_bytes, (void**)&d_trace);
             if (rc) break;
-            if (cudaMemcpyAsync(d_trace, trace, trace_bytes, cudaMemcpyHostToDevice, st) != cudaSuccess) {
-                set_error("trace upload failed");
-                rc = SG_ERR_CUDA;
-                break;
-            }
-            src = d_trace;
+            rc = upload_and_lde(ctx, st, trace, d_trace, n, row_u64, blowup, w, h->d_lde);
         }
-        rc = coset_lde(ctx, st, src, n, row_u64, blowup, w, h->d_lde);
         if (rc) break;
         rc = leaves_row_major(ctx, st, h->d_lde, lde_rows, row_u64, c0, c1, R, le, h->d_nodes + (L - 1) * 32);
         if (rc) break;

@@ -119,6 +119,10 @@ int ntt_rows(Ctx* ctx, cudaStream_t st, uint64_t* d, uint64_t n, uint64_t m, int
 // Coset LDE: out ((B*n) x m, row-major, canonical) from trace (n x m) and coset weights.
 int coset_lde(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t n, uint64_t m, uint64_t blowup,
               const uint64_t* weights, uint64_t* out);
+// The same over m columns of wider row-major matrices: trace rows of trace_ld
+// u64, output rows of out_ld u64 (a column range of each, by pointer offset).
+int coset_lde_ld(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t trace_ld, uint64_t n, uint64_t m,
+                 uint64_t blowup, const uint64_t* weights, uint64_t* out, uint64_t out_ld);
 int leaves_row_major(Ctx* ctx, cudaStream_t st, const uint64_t* data, uint64_t num_rows, uint64_t row_u64,
                      uint64_t col_start, uint64_t col_end, uint32_t rows_per_leaf, int little_endian,
                      uint8_t* out);

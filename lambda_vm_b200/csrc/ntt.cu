@@ -99,7 +99,8 @@ __device__ __forceinline__ uint64_t tw_root(const Tw& t, uint32_t logM, uint64_t
 struct PassArgs {
     const uint64_t* in;
     uint64_t* out;
-    uint64_t m;  // columns == row stride in u64
+    uint64_t m;               // columns transformed
+    uint64_t in_ld, out_ld;   // row strides of in / out in u64 (>= m)
     uint32_t logL;
     uint32_t inverse;
     // row(tile, point, rep) = tile*ts + point*ps + rep*rs
@@ -231,9 +232,9 @@ __device__ __forceinline__ void tile_body(const PassArgs& a, uint64_t* S, const 
         }
     }
     __syncthreads();
-    const uint64_t* in = a.in + (pt * a.in_ts) * a.m + col0;
-    uint64_t* out = a.out + (pt * a.out_ts + (uint64_t)rep * a.out_rs) * a.m + col0;
-    const uint64_t ip = a.in_ps * a.m, op = a.out_ps * a.m;
+    const uint64_t* in = a.in + (pt * a.in_ts) * a.in_ld + col0;
+    uint64_t* out = a.out + (pt * a.out_ts + (uint64_t)rep * a.out_rs) * a.out_ld + col0;
+    const uint64_t ip = a.in_ps * a.in_ld, op = a.out_ps * a.out_ld;
     if constexpr (PL::NST == 0) {
         for (uint32_t c = threadIdx.x; c < C; c += T) {
             if (c < ncols) {
@@ -389,6 +390,8 @@ static PassArgs base_args(const uint64_t* in, uint64_t* out, uint64_t m, uint32_
     a.in = in;
     a.out = out;
     a.m = m;
+    a.in_ld = m;
+    a.out_ld = m;
     a.logL = logL;
     a.inverse = inv ? 1 : 0;
     a.reps = 1;
@@ -518,17 +521,20 @@ int ntt_rows(Ctx* ctx, cudaStream_t st, uint64_t* d, uint64_t n, uint64_t m, int
 
 // The LDE pass sequence over caller-provided scratch: coef (n x m) always,
 // tmp (n x m) when n > 4096.
-static int lde_passes(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t n, uint64_t m, uint64_t blowup,
-                      const uint64_t* weights, uint64_t* out, const Tw& tw, uint64_t* coef, uint64_t* tmp) {
+static int lde_passes(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t trace_ld, uint64_t n, uint64_t m,
+                      uint64_t blowup, const uint64_t* weights, uint64_t* out, uint64_t out_ld, const Tw& tw,
+                      uint64_t* coef, uint64_t* tmp) {
     const int logn = log2_exact(n), logN = (int)tw.logN;
     if (logn <= 12) {
         PassArgs I = base_args(trace, coef, m, logn, true, tw);
+        I.in_ld = trace_ld;
         I.in_ps = 1;
         I.out_ps = 1;
         I.post_kind = 2;
         I.weights = weights;
         SG_TRY(run_pass(ctx, st, I, 1));
         PassArgs F = base_args(coef, out, m, logn, false, tw);
+        F.out_ld = out_ld;
         F.in_ps = 1;
         F.reps = (uint32_t)blowup;
         F.pre_kind = 1;
@@ -541,6 +547,7 @@ static int lde_passes(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t
     const uint32_t l1 = logn / 2, l2 = logn - l1;
     const uint64_t N1 = 1ULL << l1, N2 = 1ULL << l2;
     PassArgs I1 = base_args(trace, tmp, m, l1, true, tw);
+    I1.in_ld = trace_ld;
     I1.in_ts = 1;
     I1.in_ps = N2;
     I1.out_ts = 1;
@@ -557,6 +564,7 @@ static int lde_passes(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t
     I2.weights = weights;
     SG_TRY(run_pass(ctx, st, I2, N1));
     PassArgs F1 = base_args(coef, out, m, l1, false, tw);
+    F1.out_ld = out_ld;
     F1.in_ts = 1;
     F1.in_ps = N2;
     F1.reps = (uint32_t)blowup;
@@ -569,6 +577,8 @@ static int lde_passes(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t
     F1.out_rs = 1;
     SG_TRY(run_pass(ctx, st, F1, N2));
     PassArgs F2 = base_args(out, out, m, l2, false, tw);
+    F2.in_ld = out_ld;
+    F2.out_ld = out_ld;
     F2.in_ts = 1;
     F2.in_ps = blowup * N1;
     F2.out_ts = 1;
@@ -579,7 +589,13 @@ static int lde_passes(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t
 
 int coset_lde(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t n, uint64_t m, uint64_t blowup,
               const uint64_t* weights, uint64_t* out) {
+    return coset_lde_ld(ctx, st, trace, m, n, m, blowup, weights, out, m);
+}
+
+int coset_lde_ld(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t trace_ld, uint64_t n, uint64_t m,
+                 uint64_t blowup, const uint64_t* weights, uint64_t* out, uint64_t out_ld) {
     if (n == 0 || m == 0) return SG_OK;
+    SG_CHECK_ARG(trace_ld >= m && out_ld >= m, "row stride smaller than the column count");
     const int logn = log2_exact(n), logB = log2_exact(blowup);
     SG_CHECK_ARG(logn >= 0, "n must be a power of two");
     SG_CHECK_ARG(logB >= 0, "blowup must be a power of two");
@@ -596,7 +612,7 @@ int coset_lde(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t n, uint
     SG_TRY(dev_alloc(ctx, st, n * m * 8, (void**)&coef));
     int rc = SG_OK;
     if (logn > 12) rc = dev_alloc(ctx, st, n * m * 8, (void**)&tmp);
-    if (rc == SG_OK) rc = lde_passes(ctx, st, trace, n, m, blowup, weights, out, tw, coef, tmp);
+    if (rc == SG_OK) rc = lde_passes(ctx, st, trace, trace_ld, n, m, blowup, weights, out, out_ld, tw, coef, tmp);
     int rf = dev_free(ctx, st, tmp, n * m * 8);
     int rf2 = dev_free(ctx, st, coef, n * m * 8);
     if (rc != SG_OK) return rc;
@@ -687,5 +703,5 @@ extern "C" int sg_coset_lde_static(void* stream, const uint64_t* d_trace, uint64
     SG_TRY(build_tw(ctx, st, (uint32_t)logN, scratch, &tw));
     uint64_t* coef = scratch + tw_region;
     uint64_t* tmp = coef + n * m;
-    return lde_passes(ctx, st, d_trace, n, m, blowup, d_weights, d_out, tw, coef, tmp);
+    return lde_passes(ctx, st, d_trace, m, n, m, blowup, d_weights, d_out, m, tw, coef, tmp);
 }
