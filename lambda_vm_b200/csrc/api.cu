@@ -339,11 +339,23 @@ int sg_merkle_build(sg_ctx* c, void* stream, const uint8_t* d_leaves, uint64_t n
 // they are staged by the driver and the overlap is lost, not the result.
 static constexpr uint64_t kChunkCols = 64;
 
+// When `leaves` is non-null the commit's leaves are one LDE row each over the
+// whole row: they are then absorbed window by window as the LDE columns
+// complete (whole 17-lane sponge blocks), so hashing also runs under the
+// upload, and the digests land in `leaves` when the last window is done.
+struct LeafSink {
+    uint8_t* leaves;
+    int little_endian;
+    uint64_t* state;  // 25 x lde_rows u64
+};
+
 static int upload_and_lde(Ctx* ctx, cudaStream_t st, const uint64_t* h_trace, uint64_t* d_trace, uint64_t n,
-                          uint64_t m, uint64_t blowup, const uint64_t* d_w, uint64_t* d_lde) {
+                          uint64_t m, uint64_t blowup, const uint64_t* d_w, uint64_t* d_lde,
+                          const LeafSink* sink = nullptr) {
     const uint64_t chunk = m >= 2 * kChunkCols ? kChunkCols : m;
     const uint64_t nchunks = (m + chunk - 1) / chunk;
     cudaStream_t cs = nullptr;
+    uint64_t absorbed = 0;  // leaf columns absorbed so far (a multiple of 17)
     std::vector<cudaEvent_t> ev(nchunks + 1, nullptr);
     int rc = SG_OK;
     auto ok = [&](cudaError_t e, const char* what) {
@@ -366,6 +378,16 @@ static int upload_and_lde(Ctx* ctx, cudaStream_t st, const uint64_t* h_trace, ui
             break;
         if (!ok(cudaEventRecord(ev[k], cs), "record") || !ok(cudaStreamWaitEvent(st, ev[k], 0), "wait")) break;
         rc = coset_lde_ld(ctx, st, d_trace + c0, m, n, w, blowup, d_w, d_lde + c0, m);
+        if (rc == SG_OK && sink) {
+            // absorb every whole sponge block now complete; the tail with the last chunk
+            const uint64_t done = (c0 + w == m) ? m : (c0 + w) / 17 * 17;
+            const uint64_t from = absorbed;
+            if (done > from || c0 + w == m) {
+                rc = leaves_window(ctx, st, d_lde, n * blowup, m, from, done - from, sink->little_endian,
+                                   sink->state, from == 0, c0 + w == m, sink->leaves);
+                absorbed = done;
+            }
+        }
     }
     // On success the copy stream's work is ordered before `st` through the
     // events; after a failure part of it may not be, so drain it before the
@@ -402,6 +424,7 @@ static int commit_enqueue(Ctx* ctx, cudaStream_t st, const uint64_t* trace, int 
     h->leaves_len = L;
     uint64_t* d_trace = nullptr;
     uint64_t* d_w = nullptr;
+    uint64_t* d_state = nullptr;
     const uint64_t trace_bytes = n * row_u64 * 8;
     int rc = SG_OK;
     do {
@@ -420,15 +443,26 @@ static int commit_enqueue(Ctx* ctx, cudaStream_t st, const uint64_t* trace, int 
             }
             w = d_w;
         }
+        uint8_t* leaf_out = h->d_nodes + (L - 1) * 32;
+        bool leaves_done = false;
         if (trace_on_device) {
             rc = coset_lde(ctx, st, trace, n, row_u64, blowup, w, h->d_lde);
         } else {
             rc = dev_alloc(ctx, st, trace_bytes, (void**)&d_trace);
             if (rc) break;
-            rc = upload_and_lde(ctx, st, trace, d_trace, n, row_u64, blowup, w, h->d_lde);
+            // one-row leaves over whole rows are hashed as the columns arrive
+            if (R == 1 && c0 == 0 && c1 == row_u64 && row_u64 >= 2 * kChunkCols) {
+                rc = dev_alloc(ctx, st, 25 * lde_rows * 8, (void**)&d_state);
+                if (rc) break;
+                LeafSink sink{leaf_out, le, d_state};
+                rc = upload_and_lde(ctx, st, trace, d_trace, n, row_u64, blowup, w, h->d_lde, &sink);
+                leaves_done = true;
+            } else {
+                rc = upload_and_lde(ctx, st, trace, d_trace, n, row_u64, blowup, w, h->d_lde);
+            }
         }
         if (rc) break;
-        rc = leaves_row_major(ctx, st, h->d_lde, lde_rows, row_u64, c0, c1, R, le, h->d_nodes + (L - 1) * 32);
+        if (!leaves_done) rc = leaves_row_major(ctx, st, h->d_lde, lde_rows, row_u64, c0, c1, R, le, leaf_out);
         if (rc) break;
         rc = merkle_inner(ctx, st, h->d_nodes, L);
         if (rc) break;
@@ -442,6 +476,7 @@ static int commit_enqueue(Ctx* ctx, cudaStream_t st, const uint64_t* trace, int 
     // Stream-ordered frees: the memory returns to the pool after the kernels that read it.
     if (d_trace) dev_free(ctx, st, d_trace, trace_bytes);
     if (d_w) dev_free(ctx, st, d_w, n * 8);
+    if (d_state) dev_free(ctx, st, d_state, 25 * lde_rows * 8);
     if (rc != SG_OK) {
         if (h->d_lde) dev_free(ctx, st, h->d_lde, lde_rows * row_u64 * 8);
         if (h->d_nodes) dev_free(ctx, st, h->d_nodes, (2 * L - 1) * 32);

@@ -127,6 +127,10 @@ int leaves_row_major(Ctx* ctx, cudaStream_t st, const uint64_t* data, uint64_t n
                      uint64_t col_start, uint64_t col_end, uint32_t rows_per_leaf, int little_endian,
                      uint8_t* out);
 int merkle_inner(Ctx* ctx, cudaStream_t st, uint8_t* nodes, uint64_t num_leaves_pow2);
+// One-row leaves absorbed in column windows [c0, c0 + w) with the sponge
+// state (25 x num_rows u64) kept in HBM between windows; see merkle.cu.
+int leaves_window(Ctx* ctx, cudaStream_t st, const uint64_t* data, uint64_t num_rows, uint64_t row_u64, uint64_t c0,
+                  uint64_t w, int little_endian, uint64_t* state, int first, int last, uint8_t* out);
 int pad_leaves(Ctx* ctx, cudaStream_t st, uint8_t* leaves, uint64_t n, uint64_t L);
 
 }  // namespace sg

@@ -68,6 +68,69 @@ __global__ void __launch_bounds__(128) k_leaves(const uint64_t* __restrict__ dat
     o[3] = s[3];
 }
 
+// Per-row leaves absorbed one column window at a time, for commits whose
+// columns arrive in chunks: window [c0, c0 + w) of every leaf's row is
+// absorbed into that leaf's sponge, which lives in HBM between windows
+// (structure of arrays: lane j of leaf i at state[j * L + i], so every load
+// and store is coalesced). Windows start on sponge-block boundaries (c0 a
+// multiple of 17 lanes); the last one absorbs the remainder, pads, permutes
+// and writes the digest. The absorbed byte stream, and so the digest, is the
+// one k_leaves produces for rows_per_leaf = 1.
+template <bool LE>
+__global__ void __launch_bounds__(128) k_leaves_window(const uint64_t* __restrict__ data, uint64_t row_u64,
+                                                       uint64_t c0, uint64_t w, uint32_t log_rows, uint64_t L,
+                                                       uint64_t* __restrict__ state, int first, int last,
+                                                       uint64_t* __restrict__ out) {
+    const uint64_t leaf = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (leaf >= L) return;
+    const uint64_t br = log_rows ? (__brevll(leaf) >> (64 - log_rows)) : 0;
+    const uint64_t* row = data + br * row_u64 + c0;
+    uint64_t s[25];
+#pragma unroll
+    for (int i = 0; i < 25; ++i) s[i] = first ? 0 : state[(uint64_t)i * L + leaf];
+    auto lane = [&](uint64_t c) {
+        const uint64_t v = gl::canon(__ldg(row + c));
+        return LE ? v : kc::bswap64(v);
+    };
+    const uint64_t full = w / 17;
+    for (uint64_t b = 0; b < full; ++b) {
+#pragma unroll
+        for (int i = 0; i < 17; ++i) s[i] ^= lane(b * 17 + i);
+        kc::permute(s);
+    }
+    if (last) {
+        const uint32_t rem = (uint32_t)(w % 17);
+#pragma unroll
+        for (int i = 0; i < 17; ++i) {
+            if ((uint32_t)i < rem) s[i] ^= lane(full * 17 + i);
+            if ((uint32_t)i == rem) s[i] ^= 0x01ULL;
+        }
+        s[16] ^= 0x8000000000000000ULL;
+        kc::permute(s);
+        uint64_t* o = out + leaf * 4;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) o[i] = s[i];
+    } else {
+#pragma unroll
+        for (int i = 0; i < 25; ++i) state[(uint64_t)i * L + leaf] = s[i];
+    }
+}
+
+int leaves_window(Ctx* ctx, cudaStream_t st, const uint64_t* data, uint64_t num_rows, uint64_t row_u64, uint64_t c0,
+                  uint64_t w, int little_endian, uint64_t* state, int first, int last, uint8_t* out) {
+    SG_CHECK_ARG(c0 % 17 == 0 && (last || w % 17 == 0), "leaf windows must cover whole sponge blocks");
+    const int lr = log2_exact(num_rows);
+    SG_CHECK_ARG(lr >= 0, "num_rows must be a power of two");
+    const unsigned grid = (unsigned)((num_rows + 127) / 128);
+    if (little_endian)
+        k_leaves_window<true><<<grid, 128, 0, st>>>(data, row_u64, c0, w, lr, num_rows, state, first, last,
+                                                   (uint64_t*)out);
+    else
+        k_leaves_window<false><<<grid, 128, 0, st>>>(data, row_u64, c0, w, lr, num_rows, state, first, last,
+                                                    (uint64_t*)out);
+    return check_launch(ctx, "k_leaves_window");
+}
+
 __device__ __forceinline__ void hash_pair(const uint64_t* l, const uint64_t* r, uint64_t* d) {
     uint64_t s[25];
 #pragma unroll
