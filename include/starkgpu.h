@@ -105,6 +105,18 @@ SG_API int sg_ntt_inverse(sg_ctx* ctx, void* stream, uint64_t* d_data, uint64_t 
  *      d_out: (blowup*n) x m row-major, natural order, canonical. ---- */
 SG_API int sg_coset_lde(sg_ctx* ctx, void* stream, const uint64_t* d_trace, uint64_t n, uint64_t m, uint32_t blowup,
                  const uint64_t* d_weights, uint64_t* d_out);
+/* ---- DFT tile autotuning (no reference counterpart: the reference fixes its
+ *      kernels' launch shapes). Each pass of 2^log_len points can run with
+ *      several compiled tile widths (columns per tile; 4/8/16 for lengths
+ *      2^8..2^10, 4/8 for 2^11). On a context's first pass of a length, every
+ *      width is timed on the same work and its time per column kept; a pass
+ *      over m columns then uses the width minimising ceil(m/C)*C*cost(C).
+ *      Results never depend on the width. sg_ctx_dft_tiles pins a width for a
+ *      length (cols = 0: automatic); sg_ctx_dft_tuning reports the widths and
+ *      their time per column (ms), timing them on `stream` first if needed. ---- */
+SG_API int sg_ctx_dft_tiles(sg_ctx* ctx, uint32_t log_len, uint32_t cols);
+SG_API int sg_ctx_dft_tuning(sg_ctx* ctx, void* stream, uint32_t log_len, uint32_t* cols, float* cost_per_col,
+                             uint32_t* count);
 
 /* ---- allocation-free coset LDE. No counterpart in the reference: an extra
  *      entry point for callers that cannot allocate device memory at call time

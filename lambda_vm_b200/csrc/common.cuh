@@ -83,6 +83,18 @@ struct Ctx {
     std::map<void*, uint64_t> live_cap;
     std::vector<cudaEvent_t> spare_events;
     uint64_t cached_bytes = 0;
+    // DFT tile widths per tile length 2^logL (ntt.cu): the compiled widths and
+    // their measured time per column, filled on first use; `forced` pins a
+    // width (0 = automatic). Contexts that must not allocate never tune.
+    struct TileTune {
+        int n = 0;
+        int cols[4] = {0, 0, 0, 0};
+        float cost[4] = {0, 0, 0, 0};
+        int forced = 0;
+    };
+    TileTune tiles[13];
+    std::mutex tune_mu;
+    bool autotune = true;
 };
 
 // Return every cached block to the driver pool (on OOM, and at teardown).

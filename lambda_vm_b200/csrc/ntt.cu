@@ -117,32 +117,28 @@ struct PassArgs {
     uint32_t canon_out;
 };
 
-// Compile-time stage plan per tile length: radix exponents, columns per tile,
-// threads per CTA. A tile of 2^LOGL points runs NST register stages of at
-// most 2^QM points each (larger radices first).
+// Compile-time stage plan per tile: 2^LOGL points x CC columns. A tile runs
+// NST register stages of at most 2^QM points each (larger radices first).
+// The column count is a tuning choice: several are compiled per tile length
+// and the context picks one per call (see pick_cols).
 #ifndef SG_DFT_QMAX
 #define SG_DFT_QMAX 4
 #endif
-#ifndef SG_DFT_C10
-#define SG_DFT_C10 16
-#endif
-#ifndef SG_DFT_T10
-#define SG_DFT_T10 512
-#endif
-#ifndef SG_DFT_T11
-#define SG_DFT_T11 512
-#endif
-template <int LOGL>
+// Default (and untuned) columns per tile for 2^logL-point passes.
+__host__ __device__ constexpr int default_cols(int logL) {
+    return logL <= 7 ? 32 : (logL <= 10 ? 16 : (logL == 11 ? 8 : 4));
+}
+template <int LOGL, int CC>
 struct Plan {
     static constexpr int QM = SG_DFT_QMAX;
     static constexpr int NST = LOGL == 0 ? 0 : (LOGL <= 5 ? 1 : ((LOGL + QM - 1) / QM < 2 ? 2 : (LOGL + QM - 1) / QM));
     static constexpr int q(int s) { return NST == 0 ? 0 : LOGL / NST + (s < LOGL % NST ? 1 : 0); }
     static constexpr int lgns(int s) { return s == 0 ? 0 : lgns(s - 1) + q(s - 1); }
     static constexpr int Q1 = q(0);
-    static constexpr int C = LOGL <= 7 ? 32 : (LOGL <= 9 ? 16 : (LOGL == 10 ? SG_DFT_C10 : (LOGL <= 11 ? 8 : 4)));
-    static constexpr int T = LOGL >= 12 ? 512 : (LOGL == 11 ? SG_DFT_T11 : (LOGL == 10 ? SG_DFT_T10 : 256));
+    static constexpr int C = CC;
+    static constexpr int T = LOGL >= 11 ? 512 : (LOGL == 10 && C >= 16 ? 512 : 256);
     // CTAs per SM the register allocation must allow (64K registers per SM).
-    static constexpr int MINB = T <= 256 ? 2 : (T <= 512 && LOGL == 10 ? 2 : 1);
+    static constexpr int MINB = T <= 256 ? (C <= 4 && LOGL >= 10 ? 4 : 2) : (LOGL == 10 ? 2 : 1);
     static constexpr uint32_t L = 1u << LOGL;
     static constexpr uint32_t CS0 = L + (NST > 1 ? (L >> Q1) : 0);
     static constexpr uint32_t CP = C < 16 ? C : 16;
@@ -155,9 +151,9 @@ struct Plan {
     static_assert(NST < 2 || q(0) <= 5, "register stage wider than 32 points");
 };
 
-template <int LOGL>
+template <int LOGL, int C>
 __device__ __forceinline__ uint32_t tpad(uint32_t p) {
-    using PL = Plan<LOGL>;
+    using PL = Plan<LOGL, C>;
     if constexpr (PL::NST > 1)
         return p + (p >> PL::Q1);
     else
@@ -173,9 +169,9 @@ __device__ __forceinline__ uint64_t finish(const PassArgs& a, uint64_t v, uint64
 }
 
 // Middle stage: in place in shared memory.
-template <int LOGL, int Q, int LOGNS, bool INV>
+template <int LOGL, int C_, int Q, int LOGNS, bool INV>
 __device__ __forceinline__ void mid_stage(uint64_t* S, const uint64_t* WL) {
-    using PL = Plan<LOGL>;
+    using PL = Plan<LOGL, C_>;
     constexpr uint32_t R = 1u << Q, Ns = 1u << LOGNS, per_col = PL::L >> Q;
     constexpr uint32_t items = PL::C * per_col;
     for (uint32_t w = threadIdx.x; w < items; w += PL::T) {
@@ -185,31 +181,31 @@ __device__ __forceinline__ void mid_stage(uint64_t* S, const uint64_t* WL) {
         uint64_t* col = S + c * PL::CS;
         uint64_t v[R];
 #pragma unroll
-        for (uint32_t r = 0; r < R; ++r) v[r] = col[tpad<LOGL>(base + r * Ns)];
+        for (uint32_t r = 0; r < R; ++r) v[r] = col[tpad<LOGL, C_>(base + r * Ns)];
         constexpr uint32_t sh = LOGL - LOGNS - Q;
 #pragma unroll
         for (uint32_t r = 1; r < R; ++r) v[r] = gl::mul(v[r], WL[(k * brev_q<Q>(r)) << sh]);
         dit_reg<Q, INV>(v);
 #pragma unroll
-        for (uint32_t r = 0; r < R; ++r) col[tpad<LOGL>(base + r * Ns)] = v[r];
+        for (uint32_t r = 0; r < R; ++r) col[tpad<LOGL, C_>(base + r * Ns)] = v[r];
     }
 }
 
 // Stages 1 .. NST-2, each separated from the next by a barrier.
-template <int LOGL, int STG, bool INV>
+template <int LOGL, int C_, int STG, bool INV>
 __device__ __forceinline__ void mid_stages(uint64_t* S, const uint64_t* WL) {
-    using PL = Plan<LOGL>;
+    using PL = Plan<LOGL, C_>;
     if constexpr (STG < PL::NST - 1) {
         if constexpr (STG > 1) __syncthreads();
-        mid_stage<LOGL, PL::q(STG), PL::lgns(STG), INV>(S, WL);
-        mid_stages<LOGL, STG + 1, INV>(S, WL);
+        mid_stage<LOGL, C_, PL::q(STG), PL::lgns(STG), INV>(S, WL);
+        mid_stages<LOGL, C_, STG + 1, INV>(S, WL);
     }
 }
 
-template <int LOGL, bool INV>
+template <int LOGL, int C_, bool INV>
 __device__ __forceinline__ void tile_body(const PassArgs& a, uint64_t* S, const uint64_t* WL, uint64_t* F,
                                           uint64_t pt, uint64_t col0, uint32_t ncols, uint32_t rep) {
-    using PL = Plan<LOGL>;
+    using PL = Plan<LOGL, C_>;
     constexpr uint32_t L = PL::L, C = PL::C, T = PL::T;
     uint64_t* Fpre = F;
     uint64_t* Fpost = PL::NST > 1 ? F : F + L;
@@ -273,7 +269,7 @@ __device__ __forceinline__ void tile_body(const PassArgs& a, uint64_t* S, const 
             } else {
                 uint64_t* col = S + c * PL::CS;
 #pragma unroll
-                for (uint32_t q = 0; q < R; ++q) col[tpad<LOGL>(j * R + q)] = v[q];
+                for (uint32_t q = 0; q < R; ++q) col[tpad<LOGL, C_>(j * R + q)] = v[q];
             }
         }
     }
@@ -288,7 +284,7 @@ __device__ __forceinline__ void tile_body(const PassArgs& a, uint64_t* S, const 
             for (uint32_t k = threadIdx.x; k < L; k += T)
                 Fpost[k] = a.weights[pt * a.out_ts + (uint64_t)k * a.out_ps + (uint64_t)rep * a.out_rs];
         }
-        mid_stages<LOGL, 1, INV>(S, WL);
+        mid_stages<LOGL, C_, 1, INV>(S, WL);
         __syncthreads();
         // ---- last stage: smem -> registers -> HBM
         constexpr int Q = PL::q(PL::NST - 1);
@@ -299,7 +295,7 @@ __device__ __forceinline__ void tile_body(const PassArgs& a, uint64_t* S, const 
             const uint64_t* col = S + c * PL::CS;
             uint64_t v[R];
 #pragma unroll
-            for (uint32_t r = 0; r < R; ++r) v[r] = col[tpad<LOGL>(k + r * Ns)];
+            for (uint32_t r = 0; r < R; ++r) v[r] = col[tpad<LOGL, C_>(k + r * Ns)];
 #pragma unroll
             for (uint32_t r = 1; r < R; ++r) v[r] = gl::mul(v[r], WL[k * brev_q<Q>(r)]);
             dit_reg<Q, INV>(v);
@@ -312,12 +308,13 @@ __device__ __forceinline__ void tile_body(const PassArgs& a, uint64_t* S, const 
     }
 }
 
-// One instantiation per (tile length, direction): each launch carries only the
-// butterfly code it runs, which keeps the unrolled networks in the I-cache.
-template <int LOGL, bool INV>
-__global__ void __launch_bounds__(Plan<LOGL>::T, Plan<LOGL>::MINB)
+// One instantiation per (tile length, columns, direction): each launch carries
+// only the butterfly code it runs, which keeps the unrolled networks in the
+// I-cache.
+template <int LOGL, int C_, bool INV>
+__global__ void __launch_bounds__(Plan<LOGL, C_>::T, Plan<LOGL, C_>::MINB)
     k_dft(PassArgs a, uint64_t ntiles, uint32_t ctiles) {
-    using PL = Plan<LOGL>;
+    using PL = Plan<LOGL, C_>;
     extern __shared__ uint64_t sm[];
     uint64_t* S = sm;
     uint64_t* WL = S + PL::S_WORDS;
@@ -332,24 +329,29 @@ __global__ void __launch_bounds__(Plan<LOGL>::T, Plan<LOGL>::MINB)
         const uint32_t ncols = (uint32_t)min((uint64_t)PL::C, a.m - col0);
         for (uint32_t rep = 0; rep < a.reps; ++rep) {
             __syncthreads();  // the previous tile is done with S and F
-            tile_body<LOGL, INV>(a, S, WL, F, pt, col0, ncols, rep);
+            tile_body<LOGL, C_, INV>(a, S, WL, F, pt, col0, ncols, rep);
         }
     }
 }
 
-template <int LOGL, bool INV>
+template <int LOGL, int C_, bool INV>
 static int launch_dft_dir(Ctx* ctx, cudaStream_t st, const PassArgs& a, uint64_t ntiles) {
-    using PL = Plan<LOGL>;
-    static int blocks_per_sm = 0;
-    static int num_sms = 0;
-    if (!blocks_per_sm) {
-        SG_CUDA(cudaFuncSetAttribute(k_dft<LOGL, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PL::SMEM));
+    using PL = Plan<LOGL, C_>;
+    static std::once_flag once;
+    static int blocks_per_sm = 0, num_sms = 0;
+    static cudaError_t init_err = cudaSuccess;
+    std::call_once(once, [] {
         int dev = 0;
-        SG_CUDA(cudaGetDevice(&dev));
-        SG_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
-        SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_dft<LOGL, INV>, PL::T, PL::SMEM));
+        init_err = cudaFuncSetAttribute(k_dft<LOGL, C_, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)PL::SMEM);
+        if (init_err == cudaSuccess) init_err = cudaGetDevice(&dev);
+        if (init_err == cudaSuccess) init_err = cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
+        if (init_err == cudaSuccess)
+            init_err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_dft<LOGL, C_, INV>, PL::T,
+                                                                     PL::SMEM);
         if (blocks_per_sm < 1) blocks_per_sm = 1;
-    }
+    });
+    SG_CUDA(init_err);
     const uint64_t ctiles = (a.m + PL::C - 1) / PL::C;
     if (ctiles > 0xffffffffULL) {
         set_error("too many columns");
@@ -357,32 +359,143 @@ static int launch_dft_dir(Ctx* ctx, cudaStream_t st, const PassArgs& a, uint64_t
     }
     const uint64_t total = ntiles * ctiles;
     const uint64_t grid = total < (uint64_t)num_sms * blocks_per_sm ? total : (uint64_t)num_sms * blocks_per_sm;
-    k_dft<LOGL, INV><<<(unsigned)grid, PL::T, PL::SMEM, st>>>(a, ntiles, (uint32_t)ctiles);
+    k_dft<LOGL, C_, INV><<<(unsigned)grid, PL::T, PL::SMEM, st>>>(a, ntiles, (uint32_t)ctiles);
     return check_launch(ctx, "k_dft");
 }
 
-template <int LOGL>
+template <int LOGL, int C_>
 static int launch_dft(Ctx* ctx, cudaStream_t st, const PassArgs& a, uint64_t ntiles) {
-    return a.inverse ? launch_dft_dir<LOGL, true>(ctx, st, a, ntiles) : launch_dft_dir<LOGL, false>(ctx, st, a, ntiles);
+    return a.inverse ? launch_dft_dir<LOGL, C_, true>(ctx, st, a, ntiles)
+                     : launch_dft_dir<LOGL, C_, false>(ctx, st, a, ntiles);
+}
+
+// Tile-width variants compiled per tile length (columns per tile).
+static int tile_variants(uint32_t logL, int* out) {
+    if (logL >= 8 && logL <= 10) {
+        out[0] = 4, out[1] = 8, out[2] = 16;
+        return 3;
+    }
+    if (logL == 11) {
+        out[0] = 4, out[1] = 8;
+        return 2;
+    }
+    out[0] = default_cols((int)logL);
+    return 1;
+}
+
+static int launch_cols(Ctx* ctx, cudaStream_t st, const PassArgs& a, uint64_t ntiles, int cols) {
+    switch (a.logL) {
+        case 0: return launch_dft<0, default_cols(0)>(ctx, st, a, ntiles);
+        case 1: return launch_dft<1, default_cols(1)>(ctx, st, a, ntiles);
+        case 2: return launch_dft<2, default_cols(2)>(ctx, st, a, ntiles);
+        case 3: return launch_dft<3, default_cols(3)>(ctx, st, a, ntiles);
+        case 4: return launch_dft<4, default_cols(4)>(ctx, st, a, ntiles);
+        case 5: return launch_dft<5, default_cols(5)>(ctx, st, a, ntiles);
+        case 6: return launch_dft<6, default_cols(6)>(ctx, st, a, ntiles);
+        case 7: return launch_dft<7, default_cols(7)>(ctx, st, a, ntiles);
+        case 8:
+            return cols == 4 ? launch_dft<8, 4>(ctx, st, a, ntiles)
+                             : (cols == 8 ? launch_dft<8, 8>(ctx, st, a, ntiles) : launch_dft<8, 16>(ctx, st, a, ntiles));
+        case 9:
+            return cols == 4 ? launch_dft<9, 4>(ctx, st, a, ntiles)
+                             : (cols == 8 ? launch_dft<9, 8>(ctx, st, a, ntiles) : launch_dft<9, 16>(ctx, st, a, ntiles));
+        case 10:
+            return cols == 4 ? launch_dft<10, 4>(ctx, st, a, ntiles)
+                             : (cols == 8 ? launch_dft<10, 8>(ctx, st, a, ntiles)
+                                          : launch_dft<10, 16>(ctx, st, a, ntiles));
+        case 11: return cols == 4 ? launch_dft<11, 4>(ctx, st, a, ntiles) : launch_dft<11, 8>(ctx, st, a, ntiles);
+        case 12: return launch_dft<12, default_cols(12)>(ctx, st, a, ntiles);
+        default: set_error("dft pass longer than 4096 points"); return SG_ERR_UNSUPPORTED;
+    }
+}
+
+static int ctx_tw(Ctx* ctx, cudaStream_t st, uint32_t logN, Tw* tw);
+static PassArgs base_args(const uint64_t* in, uint64_t* out, uint64_t m, uint32_t logL, bool inv, const Tw& tw);
+
+// Tile-width autotuner. The first pass of each tile length on a context times
+// every compiled width on the same work (2^logL points x 16 columns x 296
+// tiles, one forward pass, in place on a scratch buffer) and keeps each
+// width's time per column; a pass over m columns then uses the width that
+// minimises ceil(m / C) * C * cost(C), so narrow matrices (LogUp aux, the
+// composition parts) get narrow tiles and wide ones keep the 128-byte rows.
+// Widths only change how columns are grouped into tiles, never a value.
+static int tune_tiles(Ctx* ctx, cudaStream_t st, uint32_t logL) {
+    int vs[4];
+    const int nv = tile_variants(logL, vs);
+    Ctx::TileTune& tt = ctx->tiles[logL];
+    if (nv == 1) {
+        tt.n = 1, tt.cols[0] = vs[0], tt.cost[0] = 1.0f;
+        return SG_OK;
+    }
+    const uint64_t L = 1ULL << logL, m = 16, tiles = 296;
+    uint64_t* scratch = nullptr;
+    SG_TRY(dev_alloc(ctx, st, L * m * tiles * 8, (void**)&scratch));
+    int rc = SG_OK;
+    Tw tw;
+    rc = ctx_tw(ctx, st, logL, &tw);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (rc == SG_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)) {
+        set_error("tile tuning: event creation failed");
+        rc = SG_ERR_CUDA;
+    }
+    if (rc == SG_OK && cudaMemsetAsync(scratch, 0, L * m * tiles * 8, st) != cudaSuccess) {
+        set_error("tile tuning: memset failed");
+        rc = SG_ERR_CUDA;
+    }
+    for (int v = 0; v < nv && rc == SG_OK; ++v) {
+        PassArgs a = base_args(scratch, scratch, m, logL, false, tw);
+        a.in_ts = L, a.in_ps = 1, a.out_ts = L, a.out_ps = 1;
+        rc = launch_cols(ctx, st, a, tiles, vs[v]);  // warm-up (first launch sets up the kernel)
+        if (rc == SG_OK) cudaEventRecord(e0, st);
+        for (int r = 0; r < 3 && rc == SG_OK; ++r) rc = launch_cols(ctx, st, a, tiles, vs[v]);
+        if (rc == SG_OK) {
+            cudaEventRecord(e1, st);
+            float ms = 0;
+            if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+                set_error("tile tuning: timing failed");
+                rc = SG_ERR_CUDA;
+            }
+            tt.cols[v] = vs[v];
+            tt.cost[v] = ms / (3.0f * (float)m);
+        }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    int rf = dev_free(ctx, st, scratch, L * m * tiles * 8);
+    if (rc == SG_OK) tt.n = nv;
+    return rc != SG_OK ? rc : rf;
+}
+
+static int pick_cols(Ctx* ctx, cudaStream_t st, uint32_t logL, uint64_t m, int* cols) {
+    int vs[4];
+    const int nv = tile_variants(logL, vs);
+    *cols = default_cols((int)logL);
+    if (nv == 1 || !ctx->autotune) return SG_OK;
+    {
+        std::lock_guard<std::mutex> g(ctx->tune_mu);
+        const int forced = ctx->tiles[logL].forced;
+        if (forced) {
+            *cols = forced;
+            return SG_OK;
+        }
+    }
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) return SG_OK;
+    std::lock_guard<std::mutex> g(ctx->tune_mu);
+    Ctx::TileTune& tt = ctx->tiles[logL];
+    if (tt.n == 0) SG_TRY(tune_tiles(ctx, st, logL));
+    double best = 0;
+    for (int v = 0; v < tt.n; ++v) {
+        const double c = (double)((m + tt.cols[v] - 1) / tt.cols[v] * tt.cols[v]) * tt.cost[v];
+        if (v == 0 || c < best) best = c, *cols = tt.cols[v];
+    }
+    return SG_OK;
 }
 
 static int run_pass(Ctx* ctx, cudaStream_t st, const PassArgs& a, uint64_t ntiles) {
-    switch (a.logL) {
-        case 0: return launch_dft<0>(ctx, st, a, ntiles);
-        case 1: return launch_dft<1>(ctx, st, a, ntiles);
-        case 2: return launch_dft<2>(ctx, st, a, ntiles);
-        case 3: return launch_dft<3>(ctx, st, a, ntiles);
-        case 4: return launch_dft<4>(ctx, st, a, ntiles);
-        case 5: return launch_dft<5>(ctx, st, a, ntiles);
-        case 6: return launch_dft<6>(ctx, st, a, ntiles);
-        case 7: return launch_dft<7>(ctx, st, a, ntiles);
-        case 8: return launch_dft<8>(ctx, st, a, ntiles);
-        case 9: return launch_dft<9>(ctx, st, a, ntiles);
-        case 10: return launch_dft<10>(ctx, st, a, ntiles);
-        case 11: return launch_dft<11>(ctx, st, a, ntiles);
-        case 12: return launch_dft<12>(ctx, st, a, ntiles);
-        default: set_error("dft pass longer than 4096 points"); return SG_ERR_UNSUPPORTED;
-    }
+    int cols = 0;
+    SG_TRY(pick_cols(ctx, st, a.logL, a.m, &cols));
+    return launch_cols(ctx, st, a, ntiles, cols);
 }
 
 static PassArgs base_args(const uint64_t* in, uint64_t* out, uint64_t m, uint32_t logL, bool inv, const Tw& tw) {
@@ -649,7 +762,8 @@ namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_static_mu;
 uint64_t* g_static_scratch[kMaxDevices] = {};
-Ctx g_static_ctx;  // launch accounting only; it never allocates
+Ctx g_static_ctx;  // launch accounting only; it never allocates (so it never tunes tiles)
+const bool g_static_ctx_fixed = (g_static_ctx.autotune = false, true);
 
 int static_scratch(uint64_t** out) {
     int dev = 0;
@@ -704,4 +818,34 @@ extern "C" int sg_coset_lde_static(void* stream, const uint64_t* d_trace, uint64
     uint64_t* coef = scratch + tw_region;
     uint64_t* tmp = coef + n * m;
     return lde_passes(ctx, st, d_trace, m, n, m, blowup, d_weights, d_out, m, tw, coef, tmp);
+}
+
+extern "C" int sg_ctx_dft_tiles(sg_ctx* c, uint32_t log_len, uint32_t cols) {
+    using namespace sg;
+    SG_CHECK_ARG(c && log_len <= 12, "null context or tile length above 2^12");
+    int vs[4];
+    const int nv = tile_variants(log_len, vs);
+    bool ok = cols == 0;
+    for (int v = 0; v < nv; ++v) ok = ok || (int)cols == vs[v];
+    SG_CHECK_ARG(ok, "no compiled tile of that width for this length");
+    Ctx* ctx = reinterpret_cast<Ctx*>(c);
+    std::lock_guard<std::mutex> g(ctx->tune_mu);
+    ctx->tiles[log_len].forced = (int)cols;
+    return SG_OK;
+}
+
+extern "C" int sg_ctx_dft_tuning(sg_ctx* c, void* stream, uint32_t log_len, uint32_t* cols, float* cost_per_col,
+                                 uint32_t* count) {
+    using namespace sg;
+    SG_CHECK_ARG(c && cols && cost_per_col && count && log_len <= 12, "null argument or tile length above 2^12");
+    Ctx* ctx = reinterpret_cast<Ctx*>(c);
+    std::lock_guard<std::mutex> g(ctx->tune_mu);
+    Ctx::TileTune& tt = ctx->tiles[log_len];
+    if (tt.n == 0) SG_TRY(tune_tiles(ctx, (cudaStream_t)stream, log_len));
+    for (int v = 0; v < tt.n; ++v) {
+        cols[v] = (uint32_t)tt.cols[v];
+        cost_per_col[v] = tt.cost[v];
+    }
+    *count = (uint32_t)tt.n;
+    return SG_OK;
 }

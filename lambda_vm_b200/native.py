@@ -111,6 +111,8 @@ PROTOTYPES = {
     "sg_lde_free_async": (None, [vp, vp, vp]),
     "sg_batch_commit": (i32, [vp, vp, vp, u32, u32, vp, vp]),
     "sg_table_proof_shape": (i32, [vp, vp]),
+    "sg_ctx_dft_tiles": (i32, [vp, u32, u32]),
+    "sg_ctx_dft_tuning": (i32, [vp, vp, u32, vp, vp, vp]),
     "sg_prove_table": (i32, [vp, vp, vp, vp, vp]),
     "sg_grind": (i32, [vp, vp, vp, C.c_uint8, C.POINTER(u64)]),
     "sg_coset_lde_static": (i32, [vp, vp, u64, u64, u32, vp, vp]),

@@ -203,3 +203,36 @@ def test_injected_allocation_failure_is_reported(be):
     h, _ = mc.lde_commit(t, 64, 4, 2, w, be=be)  # context still usable
     assert h.root == O.merkle_root(O.leaves_row_major(O.coset_lde_row_major(t, 2, w), 2, False))
     h.free()
+
+
+@pytest.mark.parametrize("log_n", [16, 18, 20, 22])
+def test_every_dft_tile_width_gives_the_same_lde(be, log_n):
+    """The tile autotuner only regroups columns into tiles: every compiled
+    width of the pass length (2^(log_n/2) points) yields the identical LDE."""
+    import ctypes as C
+    from lambda_vm_b200 import native
+    L = native.lib()
+    log_len = log_n // 2
+    cols = (C.c_uint32 * 4)()
+    cost = (C.c_float * 4)()
+    cnt = C.c_uint32()
+    native.check(L.sg_ctx_dft_tuning(be.h, None, log_len, cols, cost, C.byref(cnt)))
+    widths = [cols[i] for i in range(cnt.value)]
+    assert cnt.value >= 2 and all(cost[i] > 0 for i in range(cnt.value))
+    rng = np.random.default_rng(log_n)
+    n, m = 1 << log_n, 7
+    t = rand_raw(rng, (n, m))
+    w = O.coset_weights(n, 3)
+    outs = []
+    try:
+        for c in widths + [0]:
+            native.check(L.sg_ctx_dft_tiles(be.h, log_len, c))
+            outs.append(mc.coset_lde_batch_base(t, 2, w, be=be))
+    finally:
+        native.check(L.sg_ctx_dft_tiles(be.h, log_len, 0))
+    for o in outs[1:]:
+        assert (o == outs[0]).all()
+    if log_n <= 18:
+        assert (outs[0] == O.canon_array(O.coset_lde_row_major(t, 2, w))).all()
+    with pytest.raises(native.SgError):
+        native.check(L.sg_ctx_dft_tiles(be.h, log_len, 5))
