@@ -5,6 +5,8 @@ records the pinned values those tests assert:
   * Keccak-256 vectors: crypto/ethrex-crypto/src/tests/keccak_tests.rs:57-79
   * transcript duplex KAT: crypto/crypto/src/tests/default_transcript_tests.rs:253-281
   * FRI query counts: crypto/stark/src/tests/proof_options_tests.rs:4-40
+  * grinding nonces: crypto/stark/src/tests/grinding_tests.rs (seed, nonce,
+    grinding factor, valid or not)
 The JSON is committed so tests never need the reference tree at run time.
 Usage: python tests/golden/extract_kats.py [REFERENCE_ROOT]
 """
@@ -61,12 +63,25 @@ def query_counts():
     return out
 
 
+def grinding_kats():
+    src = read("crypto/stark/src/tests/grinding_tests.rs")
+    out = []
+    for body in re.findall(r"#\[test\]\s*fn \w+\(\) \{(.*?)\n\}", src, re.S):
+        seed = [int(x) for x in re.findall(r"\d+", re.search(r"let seed = \[([^\]]+)\]", body).group(1))]
+        nonce = int(re.search(r"let nonce = (0x[0-9a-fA-F]+|\d+);", body).group(1), 0)
+        g = int(re.search(r"let grinding_factor = (\d+);", body).group(1))
+        valid = "assert!(!is_valid_nonce" not in body
+        out.append({"seed": seed, "nonce": nonce, "grinding_factor": g, "valid": valid})
+    return out
+
+
 def main():
     kats = {
         "source": "lambda_vm test sources (text-extracted by tests/golden/extract_kats.py)",
         "keccak256": keccak_kats(),
         "transcript": transcript_kat(),
         "fri_queries": query_counts(),
+        "grinding": grinding_kats(),
     }
     with open(OUT, "w") as f:
         json.dump(kats, f, indent=1)

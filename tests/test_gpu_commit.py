@@ -181,6 +181,24 @@ def test_grinding_smallest_nonce(be, g):
     assert nonce == O.grind(seed, g)
 
 
+def _grinding_kats():
+    import json
+    import os
+    d = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_kats.json")))
+    return [k for k in d["grinding"] if k["valid"] and k["grinding_factor"] <= 20]
+
+
+@pytest.mark.parametrize("kat", _grinding_kats(), ids=lambda k: f"g{k['grinding_factor']}")
+def test_grinding_reference_vectors(be, kat):
+    """grinding_tests.rs vectors: the device search returns the smallest valid
+    nonce, which is at most the reference test's valid nonce."""
+    seed, g = bytes(kat["seed"]), kat["grinding_factor"]
+    inner = O.grind_inner_hash(seed, g)
+    nonce = mc.generate_nonce_gpu(mc.inner_hash_lanes(inner), g, be)
+    assert nonce <= kat["nonce"] and O.grind_is_valid(inner, nonce, g)
+    assert nonce == O.grind(seed, g)
+
+
 # ---------------------------------------------------------------- errors
 def test_invalid_shapes_raise_status(be):
     from lambda_vm_b200.native import SgError

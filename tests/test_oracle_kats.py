@@ -219,3 +219,38 @@ def test_grinding_smallest_nonce():
     nonce = O.grind(seed, g)
     assert O.grind_is_valid(inner, nonce, g)
     assert not any(O.grind_is_valid(inner, k, g) for k in range(nonce))
+
+
+@pytest.mark.parametrize("kat", KATS["grinding"], ids=lambda k: f"g{k['grinding_factor']}-{k['nonce']}")
+def test_grinding_kat(kat):
+    """grinding_tests.rs: Hash(Hash(prefix || seed || g) || nonce_be) validity."""
+    inner = O.grind_inner_hash(bytes(kat["seed"]), kat["grinding_factor"])
+    assert O.grind_is_valid(inner, kat["nonce"], kat["grinding_factor"]) == kat["valid"]
+
+
+def test_grinding_search_returns_smallest_nonce_below_the_kat():
+    # the g = 10 vector's nonce is valid, so the smallest valid nonce is <= it
+    kat = next(k for k in KATS["grinding"] if k["grinding_factor"] == 10 and k["valid"])
+    seed, g = bytes(kat["seed"]), kat["grinding_factor"]
+    nonce = O.grind(seed, g)
+    inner = O.grind_inner_hash(seed, g)
+    assert nonce <= kat["nonce"] and O.grind_is_valid(inner, nonce, g)
+    assert not any(O.grind_is_valid(inner, k, g) for k in range(nonce))
+
+
+def test_terminal_roundtrip():
+    """terminal_tests.rs test_terminal_roundtrip: coefficients 1..8 evaluated on
+    the offset-3 coset of 16 points (FRI bit-reversed order) come back from
+    coeffs_from_terminal_codeword with k = 3."""
+    from lambda_vm_b200 import field as F
+    from lambda_vm_b200.stark import terminal_coeffs
+    P = F.P
+    w16 = F.root_of_unity(4)
+    evals = []
+    for i in range(16):
+        x = 3 * pow(w16, i, P) % P
+        evals.append(sum(c * pow(x, j, P) for j, c in enumerate(range(1, 9))) % P)
+    br = [evals[int(format(i, "04b")[::-1], 2)] for i in range(16)]
+    cw = np.zeros((16, 3), np.uint64)
+    cw[:, 0] = br
+    assert terminal_coeffs(cw, 3, 3) == [(c, 0, 0) for c in range(1, 9)]
