@@ -45,8 +45,8 @@ def parse():
     ap.add_argument("--workload", default="commit", choices=["commit", "proof", "serve"],
                     help="commit: LDE + Merkle commit of one trace (default); proof: multi-table proof, plain vs "
                          "scheduled; serve: Poisson stream of proof jobs, concurrent admission vs one at a time")
-    ap.add_argument("--rates", default="2,5,10,20", help="serve: arrival rates (jobs/s)")
-    ap.add_argument("--jobs", type=int, default=24, help="serve: jobs per rate")
+    ap.add_argument("--rates", default="2,5,10,20,50,100", help="serve: arrival rates (jobs/s)")
+    ap.add_argument("--jobs", type=int, default=40, help="serve: jobs per rate")
     ap.add_argument("--job-max-log-n", type=int, default=18, help="serve: largest job height (log2 cycles)")
     ap.add_argument("--max-jobs", type=int, default=4, help="serve: concurrent jobs")
     ap.add_argument("--tables", type=int, default=40)
@@ -304,24 +304,34 @@ def run_serve(a):
     p50/p99 latency (submit to proof, queueing included)."""
     import torch
     from lambda_vm_b200.device import backend
-    from lambda_vm_b200.serving import ProofServer, serve_poisson, serve_sequential
+    from lambda_vm_b200.scheduler import multi_prove_scheduled
+    from lambda_vm_b200.serving import ProofServer, serve_poisson, serve_sequential, warm_context
     from lambda_vm_b200.stark import GpuBackend, Options, multi_prove
     be = backend(0)
     opts = Options(blowup=2, grinding=20, final_log_degree=5)
     specs = serve_jobs(a)
     budget = min(160 * (1 << 30), be.budget())
-    for airs, srcs in specs[:3]:  # warm the domain caches and the allocator
+    warm_context(be, specs, opts)  # domains of every height, DFT tile timings
+    for airs, srcs in specs[:3]:  # and the allocator's block cache, through both provers
         multi_prove(airs, srcs, opts, GpuBackend(be))
+        multi_prove_scheduled(airs, srcs, opts, workers=4, be=be)
     torch.cuda.synchronize()
     sweep = []
-    for rate in [float(x) for x in a.rates.split(",")]:
-        with ProofServer(budget, max_jobs=a.max_jobs, drivers=4, opts=opts, be=be) as srv:
-            jobs, st = serve_poisson(srv, specs, rate, seed=int(rate * 1000))
-        _, st_seq = serve_sequential(specs, rate, lambda airs, srcs: multi_prove(airs, srcs, opts, GpuBackend(be)),
-                                     seed=int(rate * 1000))
-        same = all(j.proof is not None for j in jobs)
+    for i, rate in enumerate(float(x) for x in a.rates.split(",")):
+        def batched():
+            with ProofServer(budget, max_jobs=a.max_jobs, drivers=4, opts=opts, be=be) as srv:
+                return serve_poisson(srv, specs, rate, seed=int(rate * 1000))[1]
+
+        def one_at_a_time():
+            return serve_sequential(specs, rate, lambda airs, srcs: multi_prove(airs, srcs, opts, GpuBackend(be)),
+                                    seed=int(rate * 1000))[1]
+        # the two servers take turns going first
+        if i % 2 == 0:
+            st, st_seq = batched(), one_at_a_time()
+        else:
+            st_seq, st = one_at_a_time(), batched()
         sweep.append({"rate_jobs_per_s": rate, "batched": st.as_dict(), "one_at_a_time": st_seq.as_dict(),
-                      "all_proved": same})
+                      "all_proved": st.failed == 0 and st_seq.failed == 0})
     top = sweep[-1]
     rows = sum(sum(x.n for x in airs) for airs, _ in specs)
     line = {"metric": "proof serving: proved cycles/s and p50/p99 latency under Poisson arrivals",

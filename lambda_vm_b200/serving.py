@@ -175,6 +175,22 @@ class ProofServer:
         self.close()
 
 
+def warm_context(be, job_specs, opts):
+    """Start-up work a serving process does once, so no job pays for it: the
+    per-domain vectors of every trace height the jobs use, and the DFT tile
+    timings of every pass length."""
+    import ctypes as C
+    from . import native
+    from .stark import GpuBackend
+    bk = GpuBackend(be)
+    for log_n in sorted({a.log_n for airs, _ in job_specs for a in airs}):
+        bk.domain(log_n, opts.blowup, opts.coset_offset)
+    cols, cost, cnt = (C.c_uint32 * 4)(), (C.c_float * 4)(), C.c_uint32()
+    for log_len in range(8, 12):
+        native.check(native.lib().sg_ctx_dft_tuning(be.h, None, log_len, cols, cost, C.byref(cnt)))
+    native.check(native.lib().sg_stream_sync(be.h, None))
+
+
 def serve_poisson(server, job_specs, rate, seed=0):
     """Submit `job_specs` [(airs, sources)] with exponential inter-arrival
     times of mean 1/rate (seeded); wait for all; return (jobs, ServeStats)."""
