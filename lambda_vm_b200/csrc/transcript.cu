@@ -14,6 +14,7 @@
 #include <new>
 
 #include "../../include/starkgpu.h"
+#include "fs.cuh"
 
 typedef unsigned __int128 u128;
 static const uint64_t P = 0xFFFFFFFF00000001ULL;
@@ -116,70 +117,22 @@ void keccak_f(uint64_t* A) {
     }
 }
 
-struct Keccak256 {
-    uint64_t st[25];
-    uint8_t buf[136];
-    unsigned pos;
-    void reset() {
-        memset(st, 0, sizeof st);
-        pos = 0;
-    }
-    void block() {
-        for (int i = 0; i < 17; ++i) {
-            uint64_t v;
-            memcpy(&v, buf + 8 * i, 8);  // little-endian lanes
-            st[i] ^= v;
-        }
-        keccak_f(st);
-    }
-    void update(const uint8_t* d, size_t n) {
-        while (n) {
-            size_t t = 136 - pos;
-            if (t > n) t = n;
-            memcpy(buf + pos, d, t);
-            pos += (unsigned)t;
-            d += t;
-            n -= t;
-            if (pos == 136) {
-                block();
-                pos = 0;
-            }
-        }
-    }
-    void final(uint8_t out[32]) const {
-        Keccak256 k = *this;
-        memset(k.buf + k.pos, 0, 136 - k.pos);
-        k.buf[k.pos] ^= 0x01;
-        k.buf[135] ^= 0x80;
-        k.block();
-        memcpy(out, k.st, 32);
-    }
-};
-
 }  // namespace
 
-struct sg_transcript {
-    Keccak256 h;
-    uint8_t out_buf[32];
-    unsigned out_pos;
-};
+void fs::host_permute(uint64_t st[25]) { keccak_f(st); }
 
 extern "C" {
 
 void sg_keccak256(const uint8_t* data, uint64_t len, uint8_t out[32]) {
-    Keccak256 k;
-    k.reset();
-    k.update(data, len);
-    k.final(out);
+    fs::State k;
+    fs::init(k, data, len);
+    fs::final_digest(k, out);
 }
 
 sg_transcript* sg_transcript_new(const uint8_t* data, uint64_t len) {
     sg_transcript* t = new (std::nothrow) sg_transcript;
     if (!t) return nullptr;
-    t->h.reset();
-    memset(t->out_buf, 0, 32);
-    t->out_pos = 32;
-    if (len) t->h.update(data, len);
+    fs::init(t->s, data, len);
     return t;
 }
 
@@ -191,70 +144,21 @@ sg_transcript* sg_transcript_clone(const sg_transcript* t) {
 
 void sg_transcript_free(sg_transcript* t) { delete t; }
 
-void sg_transcript_append(sg_transcript* t, const uint8_t* data, uint64_t len) {
-    t->out_pos = 32;
-    t->h.update(data, len);
-}
+void sg_transcript_append(sg_transcript* t, const uint8_t* data, uint64_t len) { fs::append(t->s, data, len); }
 
-void sg_transcript_append_base(sg_transcript* t, uint64_t v) {
-    uint8_t b[8];
-    v = sg_host_gl_canon(v);
-    for (int i = 0; i < 8; ++i) b[i] = (uint8_t)(v >> (56 - 8 * i));
-    sg_transcript_append(t, b, 8);
-}
+void sg_transcript_append_base(sg_transcript* t, uint64_t v) { fs::append_u64_be(t->s, fs::canon(v)); }
 
-void sg_transcript_append_ext3(sg_transcript* t, const uint64_t v[3]) {
-    uint8_t b[24];
-    for (int k = 0; k < 3; ++k) {
-        uint64_t c = sg_host_gl_canon(v[k]);
-        for (int i = 0; i < 8; ++i) b[8 * k + i] = (uint8_t)(c >> (56 - 8 * i));
-    }
-    sg_transcript_append(t, b, 24);
-}
+void sg_transcript_append_ext3(sg_transcript* t, const uint64_t v[3]) { fs::append_ext3(t->s, v); }
 
-void sg_transcript_sample(sg_transcript* t, uint8_t out[32]) {
-    uint8_t d[32];
-    t->h.final(d);
-    for (int i = 0; i < 32; ++i) out[i] = d[31 - i];
-    t->h.reset();
-    t->h.update(out, 32);
-    t->out_pos = 32;
-}
+void sg_transcript_sample(sg_transcript* t, uint8_t out[32]) { fs::sample(t->s, out); }
 
-void sg_transcript_state(const sg_transcript* t, uint8_t out[32]) { t->h.final(out); }
+void sg_transcript_state(const sg_transcript* t, uint8_t out[32]) { fs::final_digest(t->s, out); }
 
-static uint64_t next_u64(sg_transcript* t) {
-    if (t->out_pos + 8 > 32) {
-        uint8_t s[32];
-        sg_transcript_sample(t, s);
-        memcpy(t->out_buf, s, 32);
-        t->out_pos = 0;
-    }
-    uint64_t v = 0;
-    for (int i = 0; i < 8; ++i) v = (v << 8) | t->out_buf[t->out_pos + i];
-    t->out_pos += 8;
-    return v;
-}
+uint64_t sg_transcript_sample_base(sg_transcript* t) { return fs::sample_base(t->s); }
 
-uint64_t sg_transcript_sample_base(sg_transcript* t) {
-    for (;;) {
-        uint64_t c = next_u64(t);
-        if (c < P) return c;
-    }
-}
+void sg_transcript_sample_ext3(sg_transcript* t, uint64_t out[3]) { fs::sample_ext3(t->s, out); }
 
-void sg_transcript_sample_ext3(sg_transcript* t, uint64_t out[3]) {
-    for (int i = 0; i < 3; ++i) out[i] = sg_transcript_sample_base(t);
-}
-
-uint64_t sg_transcript_sample_u64(sg_transcript* t, uint64_t upper) {
-    if (upper == 0) return 0;
-    const uint64_t thr = (0 - upper) % upper;
-    for (;;) {
-        uint64_t c = next_u64(t);
-        if (c >= thr) return c % upper;
-    }
-}
+uint64_t sg_transcript_sample_u64(sg_transcript* t, uint64_t upper) { return fs::sample_u64(t->s, upper); }
 
 void sg_transcript_sample_z_ood(sg_transcript* t, uint64_t trace_len, uint64_t lde_len, uint64_t coset_offset,
                                 uint64_t out[3]) {
