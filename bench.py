@@ -42,6 +42,8 @@ def parse():
     ap.add_argument("--leaf-layout", default="row-le", choices=["row-le", "pair-be"],
                     help="row-le: one row per leaf, LE bytes (this workload); pair-be: the prover's row-pair BE leaf")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-proof-summary", action="store_true",
+                    help="skip the multi-table proof summary the default line carries at N = 1")
     ap.add_argument("--workload", default="commit", choices=["commit", "proof", "serve"],
                     help="commit: LDE + Merkle commit of one trace (default); proof: multi-table proof, plain vs "
                          "scheduled; serve: Poisson stream of proof jobs, concurrent admission vs one at a time")
@@ -229,7 +231,25 @@ def run_proof_distributed(a, rank, world, local):
     dist.destroy_process_group()
 
 
+def proof_summary(a, steps=3, warmup=2):
+    """The multi-table proof workload, plain vs scheduled, as a compact dict
+    for the default bench line (N = 1)."""
+    import types
+    b = types.SimpleNamespace(tables=a.tables, max_log_n=a.max_log_n, workers=a.workers, steps=steps, warmup=warmup)
+    line = measure_proof(b)
+    return {"workload": line["config"]["workload"], "rows": line["config"]["rows"],
+            "plain_ms_per_proof": round(line["plain"]["ms_per_proof"], 1),
+            "scheduled_ms_per_proof": round(line["scheduled"]["ms_per_proof"], 1),
+            "scheduled_rows_per_s": round(line["value"], 1),
+            "scheduled_over_plain": round(line["scheduled_over_plain"], 3),
+            "same_first_root": line["same_first_root"]}
+
+
 def run_proof(a):
+    print(json.dumps(measure_proof(a)), flush=True)
+
+
+def measure_proof(a):
     """One multi-table proof (LDE + commit + LogUp aux + constraint evaluation +
     composition + OOD + DEEP + FRI to a degree-32 final polynomial + grinding +
     queries), plain form vs scheduled form; proved rows (cycles) per second."""
@@ -278,7 +298,7 @@ def run_proof(a):
                           "ms_per_proof": res["scheduled"]["s_per_proof"] * 1e3, "all_ms": res["scheduled"]["all_ms"]},
             "scheduled_over_plain": res["plain"]["s_per_proof"] / res["scheduled"]["s_per_proof"],
             "same_first_root": same}
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def serve_jobs(a, seed=77):
@@ -516,6 +536,13 @@ def main():
                     "path": "sg_lde_commit(host pinned trace) -> root"}}
     if not a.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(a, rpl, le)
+    if world == 1 and not a.no_proof_summary:
+        # the batched-vs-plain proof workload beside the primitive (not timed
+        # into `value`); a failure here is reported, never fatal to the line
+        try:
+            line["proof_workload"] = proof_summary(a)
+        except Exception as e:  # noqa: BLE001
+            line["proof_workload"] = {"error": f"{type(e).__name__}: {e}"}
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
