@@ -1,0 +1,271 @@
+"""STARK verifier for the multi-table proofs of lambda_vm_b200.stark.
+
+Restates the checks of crypto/stark/src/verifier.rs (multi_verify): per-table
+transcript replay, the bus balance of the LogUp contributions, the step-2
+composition check at the out-of-domain point (H(z) = H0(z^2) + z H1(z^2)
+against the constraints evaluated on the OOD frame), the step-3 FRI checks
+(layer openings and authentication paths, fold consistency, the terminal
+polynomial) and the grinding nonce, with the library's Keccak-256 and
+transcript and Python-integer field arithmetic on the host. Returns
+(ok, reason). `verify_bytes` takes a serialized proof (proof_io).
+"""
+import numpy as np
+
+from . import field as F
+from . import math_cuda as mc
+
+P = F.P
+GRIND_PREFIX = bytes([0x01, 0x23, 0x45, 0x67, 0x89, 0xAB, 0xCD, 0xED])  # grinding.rs:6
+
+
+def f3(x):
+    return tuple(int(v) % P for v in x)
+
+
+def add(a, b):
+    return tuple((a[i] + b[i]) % P for i in range(3))
+
+
+def sub(a, b):
+    return tuple((a[i] - b[i]) % P for i in range(3))
+
+
+def mul(a, b):
+    a0, a1, a2 = a
+    b0, b1, b2 = b
+    return ((a0 * b0 + 2 * (a1 * b2 + a2 * b1)) % P, (a0 * b1 + a1 * b0 + 2 * a2 * b2) % P,
+            (a0 * b2 + a1 * b1 + a2 * b0) % P)
+
+
+def scale(a, s):
+    return tuple(v * (s % P) % P for v in a)
+
+
+def fpow(a, e):
+    r, b = (1, 0, 0), f3(a)
+    while e:
+        if e & 1:
+            r = mul(r, b)
+        b = mul(b, b)
+        e >>= 1
+    return r
+
+
+def finv(a):
+    a0, a1, a2 = f3(a)
+    nrm = (a0 ** 3 + 2 * a1 ** 3 + 4 * a2 ** 3 - 6 * a0 * a1 * a2) % P
+    ni = pow(nrm, P - 2, P)
+    return ((a0 * a0 - 2 * a1 * a2) * ni % P, (2 * a2 * a2 - a0 * a1) * ni % P, (a1 * a1 - a0 * a2) * ni % P)
+
+
+def brev(i, bits):
+    return int(format(i, f"0{bits}b")[::-1], 2) if bits else 0
+
+
+def root(log_n):
+    return F.root_of_unity(log_n) % P
+
+
+def merkle_ok(leaf_hash, idx, path, rt):
+    h = leaf_hash
+    for sib in path:
+        s = bytes(sib)
+        h = mc.keccak256(h + s) if idx % 2 == 0 else mc.keccak256(s + h)
+        idx //= 2
+    return h == rt
+
+
+def row_pair_leaf(r0, r1):
+    b = b""
+    for row in (r0, r1):
+        for v in row:
+            b += (int(v) % P).to_bytes(8, "big")
+    return mc.keccak256(b)
+
+
+def eval_ood(prog, frame, rap, alpha, offset):
+    """Constraint roots at the OOD point; frame[off][col] over main || aux."""
+    v = []
+    m_main = frame["m"]
+    for nd in prog["nodes"]:
+        k = nd[0]
+        if k == "var":
+            _, is_main, off, col = nd
+            v.append(frame["vals"][off][col if is_main else m_main + col])
+        elif k == "cb":
+            v.append((prog["base_consts"][nd[1]] % P, 0, 0))
+        elif k == "ce":
+            v.append(f3(prog["ext_consts"][nd[1]]))
+        elif k == "rap":
+            v.append(f3(rap[nd[1]]))
+        elif k == "alpha":
+            v.append(f3(alpha[nd[1]]))
+        elif k == "off":
+            v.append(f3(offset))
+        elif k == "add":
+            v.append(add(v[nd[1]], v[nd[2]]))
+        elif k == "sub":
+            v.append(sub(v[nd[1]], v[nd[2]]))
+        elif k == "mul":
+            v.append(mul(v[nd[1]], v[nd[2]]))
+        elif k == "neg":
+            v.append(scale(v[nd[1]], P - 1))
+        else:
+            v.append(v[nd[1]])
+    return [v[r] for r in prog["roots"]]
+
+
+def verify(airs, proof, opts, label=b"lambda_vm_b200/synthetic-multi-table"):
+    T = mc.Transcript(label)
+    tabs = proof["tables"]
+    for tp in tabs:
+        T.append_bytes(tp["main_root"])
+    ch = [f3(T.sample_ext3()), f3(T.sample_ext3())]
+    alpha = ch[1]
+    apows = [(1, 0, 0)]
+    for _ in range(max(a.max_alpha for a in airs) - 1):
+        apows.append(mul(apows[-1], alpha))
+    total = (0, 0, 0)
+    for tp in tabs:
+        total = add(total, f3(tp["table_contribution"]))
+    if total != (0, 0, 0):
+        return False, "bus contributions do not balance"
+    B, g = opts.blowup, opts.coset_offset
+    for ti, (air, tp) in enumerate(zip(airs, tabs)):
+        t = T.clone()
+        if len(tabs) > 1:
+            t.append_bytes(int(ti).to_bytes(8, "little"))
+        n = air.n
+        N = n * B
+        logN = N.bit_length() - 1
+        t.append_bytes(tp["aux_root"])
+        beta = f3(t.sample_ext3())
+        prog = air.program
+        ncons = len(prog["roots"]) + len(air.boundary)
+        coefs = [(1, 0, 0)]
+        for _ in range(ncons - 1):
+            coefs.append(mul(coefs[-1], beta))
+        bt, bb = coefs[:len(prog["roots"])], coefs[len(prog["roots"]):]
+        t.append_bytes(tp["comp_root"])
+        z = f3(t.sample_z_ood(n, N, g))
+        wn = root(air.log_n)
+        zw = scale(z, wn)
+        z2 = mul(z, z)
+        tood = [[f3(v) for v in tp["trace_ood"][k]] for k in range(2)]
+        pood = [f3(v) for v in tp["parts_ood"]]
+        # step 2: composition identity at z
+        L = f3(tp["table_contribution"])
+        offset = scale(L, pow(n, P - 2, P))
+        frame = {"m": air.width, "vals": tood}
+        roots_v = eval_ood(prog, frame, ch, apows, offset)
+        acc = (0, 0, 0)
+        for c, cv in enumerate(roots_v):
+            acc = add(acc, mul(bt[c], cv))
+        zn1 = sub(fpow(z, n), (1, 0, 0))
+        h = mul(acc, finv(zn1))
+        for b, (col, is_aux, row) in enumerate(air.boundary):
+            cell = tood[0][air.width + col] if is_aux else tood[0][col]
+            h = add(h, mul(mul(bb[b], cell), finv(sub(z, (1, 0, 0)))))
+        if h != add(pood[0], mul(z, pood[1])):
+            return False, f"table {ti}: composition check failed"
+        for k in range(2):
+            for v in tood[k]:
+                t.append_ext3(np.array(v, np.uint64))
+        for v in pood:
+            t.append_ext3(np.array(v, np.uint64))
+        gamma = f3(t.sample_ext3())
+        ncols = air.width + air.aux_width
+        gp = [(1, 0, 0)]
+        for _ in range(2 + 2 * ncols - 1):
+            gp.append(mul(gp[-1], gamma))
+        gh, gt = gp[:2], gp[2:]
+        # FRI transcript replay
+        blog = B.bit_length() - 1
+        terminal_log = min(blog + opts.final_log_degree, logN)
+        total_folds = logN - terminal_log
+        num_committed = max(total_folds - 1, 0)
+        if len(tp["fri_roots"]) != num_committed:
+            return False, "wrong number of FRI layers"
+        zetas = []
+        for li in range(num_committed):
+            zetas.append(f3(t.sample_ext3()))
+            t.append_bytes(tp["fri_roots"][li])
+        if total_folds > 0:
+            zetas.append(f3(t.sample_ext3()))
+        coeffs = [f3(c) for c in tp["fri_final_coeffs"]]
+        if len(coeffs) != 1 << (terminal_log - blog):
+            return False, "wrong terminal length"
+        for c in coeffs:
+            t.append_ext3(np.array(c, np.uint64))
+        if opts.grinding:
+            inner = mc.keccak256(GRIND_PREFIX + t.state() + bytes([opts.grinding]))
+            head = int.from_bytes(mc.keccak256(inner + int(tp["nonce"]).to_bytes(8, "big"))[:8], "big")
+            if head >= 1 << (64 - opts.grinding):
+                return False, "grinding nonce invalid"
+            t.append_bytes(int(tp["nonce"]).to_bytes(8, "big"))
+        iotas = [t.sample_u64(N // 2) for _ in range(opts.queries)]
+        if list(iotas) != list(tp["iotas"]):
+            return False, "query indexes differ"
+        wN = root(logN)
+        term_off = pow(g, 1 << total_folds, P)
+        Tlen = 1 << terminal_log
+        wT = root(terminal_log)
+        for q, iota in enumerate(iotas):
+            r0, r1 = brev(2 * iota, logN), brev(2 * iota + 1, logN)
+            om, oa, op = tp["open_main"], tp["open_aux"], tp["open_parts"]
+            if not merkle_ok(row_pair_leaf(om[2 * q], om[2 * q + 1]), iota, tp["path_main"][q], tp["main_root"]):
+                return False, "main opening path"
+            if not merkle_ok(row_pair_leaf(oa[2 * q], oa[2 * q + 1]), iota, tp["path_aux"][q], tp["aux_root"]):
+                return False, "aux opening path"
+            if not merkle_ok(row_pair_leaf(op[2 * q], op[2 * q + 1]), iota, tp["path_parts"][q], tp["comp_root"]):
+                return False, "parts opening path"
+            dv = []
+            for rr, r in ((2 * q, r0), (2 * q + 1, r1)):
+                x = g * pow(wN, r, P) % P
+                ih = finv(sub((x, 0, 0), z2))
+                acc = (0, 0, 0)
+                for j in range(2):
+                    hx = f3(op[rr][3 * j:3 * j + 3])
+                    acc = add(acc, mul(mul(gh[j], sub(hx, pood[j])), ih))
+                for kk, pt in enumerate((z, zw)):
+                    it = finv(sub((x, 0, 0), pt))
+                    for j in range(ncols):
+                        tv = (int(om[rr][j]) % P, 0, 0) if j < air.width else f3(oa[rr][3 * (j - air.width):3 * (j - air.width) + 3])
+                        acc = add(acc, mul(mul(gt[2 * j + kk], sub(tv, tood[kk][j])), it))
+                dv.append(acc)
+            # fold chain
+            x0 = g * pow(wN, brev(iota, logN - 1), P) % P
+            if x0 != g * pow(wN, r0, P) % P:
+                return False, "query point mismatch"
+            v = add(add(dv[0], dv[1]), scale(mul(zetas[0], sub(dv[0], dv[1])), pow(x0, P - 2, P))) if total_folds else None
+            for li in range(num_committed):
+                f = li + 1
+                pos = iota >> li
+                leaf = pos >> 1
+                pair = tp["fri_open"][li][2 * q:2 * q + 2]
+                a, b = f3(pair[0]), f3(pair[1])
+                if (a, b)[pos & 1] != v:
+                    return False, f"FRI layer {f} value mismatch"
+                lb = b"".join((int(u) % P).to_bytes(8, "big") for u in list(pair[0]) + list(pair[1]))
+                if not merkle_ok(mc.keccak256(lb), leaf, tp["fri_paths"][li][q], tp["fri_roots"][li]):
+                    return False, f"FRI layer {f} path"
+                xj = pow(g * pow(wN, brev(leaf << f, logN - 1), P) % P, 1 << f, P)
+                v = add(add(a, b), scale(mul(zetas[f], sub(a, b)), pow(xj, P - 2, P)))
+            if total_folds:
+                p_term = iota >> (total_folds - 1)
+                xt = term_off * pow(wT, brev(p_term, terminal_log), P) % P
+                ev = (0, 0, 0)
+                for c in reversed(coeffs):
+                    ev = add(scale(ev, xt), c)
+                if ev != v:
+                    return False, "terminal polynomial mismatch"
+    return True, "ok"
+
+
+def verify_bytes(airs, blob, opts, label=b"lambda_vm_b200/synthetic-multi-table"):
+    from .proof_io import deserialize
+    try:
+        proof = deserialize(blob)
+    except ValueError as e:
+        return False, f"malformed proof: {e}"
+    return verify(airs, proof, opts, label)

@@ -25,6 +25,11 @@ def test_gpu_proof_identical_to_oracle_and_verifies(be, shapes, opts):
     op = multi_prove(airs, trs, opts, OracleBackend())
     assert diff(gp, op) is None, diff(gp, op)
     assert verify(airs, gp, opts) == (True, "ok")
+    # byte-identical canonical serialization; the library-side verifier accepts
+    from lambda_vm_b200.proof_io import serialize
+    from lambda_vm_b200.verifier import verify_bytes
+    assert serialize(gp) == serialize(op)
+    assert verify_bytes(airs, serialize(gp), opts) == (True, "ok")
 
 
 def test_gpu_prover_larger_table_verifies(be):
