@@ -169,6 +169,15 @@ SG_API int sg_lde_commit(sg_ctx* ctx, void* stream, const uint64_t* trace, int t
                   uint64_t* host_lde_out, sg_lde** out, uint8_t root_out[32]);
 SG_API int sg_lde_get_info(const sg_lde* lde, sg_lde_info* info);
 SG_API void sg_lde_free(sg_ctx* ctx, sg_lde* lde);
+/* ---- split commitment: replaces coset_lde_row_major_split_trees
+ *      (crypto/math-cuda/src/lde.rs:726): one LDE, two row-pair big-endian trees,
+ *      columns [split_col, row_u64) in the returned handle (root_out) and, when
+ *      build_pre != 0, the precomputed columns [0, split_col) into the caller's
+ *      device node buffer d_pre_nodes ((blowup*n - 1) * 32 bytes; root_pre_out). ---- */
+SG_API int sg_lde_commit_split(sg_ctx* ctx, void* stream, const uint64_t* trace, int trace_on_device, uint64_t n,
+                               uint64_t row_u64, uint32_t blowup, const uint64_t* weights, uint64_t split_col,
+                               int build_pre, uint64_t* host_lde_out, sg_lde** out, uint8_t root_out[32],
+                               uint8_t* d_pre_nodes, uint8_t root_pre_out[32]);
 /* Stream-ordered release of a handle: its memory returns to the pool after
  * the work already queued on `stream`; no device-wide wait. */
 SG_API void sg_lde_free_async(sg_ctx* ctx, void* stream, sg_lde* lde);
@@ -260,6 +269,24 @@ SG_API int sg_deep_composition(sg_ctx* ctx, void* stream, const uint64_t* d_main
  *      Merkle leaves Keccak(out[2j] || out[2j+1]) (h/2 x 32 bytes). ---- */
 SG_API int sg_fri_fold_layer(sg_ctx* ctx, void* stream, const uint64_t* d_in, uint64_t h, const uint64_t* d_inv_tw,
                              const uint64_t zeta[3], uint64_t* d_out, uint64_t* d_inv_tw_next, uint8_t* d_leaves);
+/* ---- stateful FRI commit phase: replaces FriCommitState (crypto/math-cuda/src/fri.rs:48-255).
+ *      sg_fri_begin (FriCommitState::new / new_dev): the bit-reversed layer-0 ext3
+ *      evaluations (3*n0 u64; a device buffer is borrowed, a host one copied) and
+ *      their inverse twiddles (n0/2 u64).
+ *      sg_fri_fold_commit_layer (fold_and_commit_layer): fold with zeta, commit the
+ *      ext3 pair leaves, root to root_out, optionally the folded evaluations to
+ *      host_evals_out (want_host). sg_fri_fold_final: the last fold, uncommitted.
+ *      Every committed layer stays resident (sg_fri_layer) until sg_fri_free. ---- */
+typedef struct sg_fri sg_fri;
+SG_API int sg_fri_begin(sg_ctx* ctx, void* stream, const uint64_t* evals, int evals_on_device, const uint64_t* inv_tw,
+                        int tw_on_device, uint64_t n0, sg_fri** out);
+SG_API int sg_fri_fold_commit_layer(sg_fri* fri, const uint64_t zeta[3], uint8_t root_out[32],
+                                    uint64_t* host_evals_out);
+SG_API int sg_fri_fold_final(sg_fri* fri, const uint64_t zeta[3], uint64_t* host_evals_out);
+SG_API uint32_t sg_fri_num_layers(const sg_fri* fri);
+SG_API int sg_fri_layer(const sg_fri* fri, uint32_t layer, const uint64_t** d_evals, uint64_t* n,
+                        const uint8_t** d_nodes, uint64_t* leaves_len);
+SG_API void sg_fri_free(sg_fri* fri);
 /* FRI layer leaves over n ext3 evaluations (keccak_fri_leaves_ext3, keccak.cu:384). */
 SG_API int sg_fri_leaves(sg_ctx* ctx, void* stream, const uint64_t* d_evals, uint64_t n, uint8_t* d_leaves);
 /* ---- row gathers for query openings: replaces barycentric::gather_rows_{base,ext3}_on_device

@@ -511,6 +511,44 @@ int sg_lde_commit(sg_ctx* c, void* stream, const uint64_t* trace, int trace_on_d
     return SG_OK;
 }
 
+int sg_lde_commit_split(sg_ctx* c, void* stream, const uint64_t* trace, int trace_on_device, uint64_t n,
+                        uint64_t row_u64, uint32_t blowup, const uint64_t* weights, uint64_t split_col, int build_pre,
+                        uint64_t* host_lde_out, sg_lde** out, uint8_t root_out[32], uint8_t* d_pre_nodes,
+                        uint8_t root_pre_out[32]) {
+    SG_CHECK_ARG(c && out, "null argument");
+    *out = nullptr;
+    SG_CHECK_ARG(split_col > 0 && split_col < row_u64, "split inside the row");
+    SG_CHECK_ARG(!build_pre || d_pre_nodes, "the precomputed tree needs a node buffer");
+    Ctx* ctx = C(c);
+    cudaStream_t st = (cudaStream_t)stream;
+    const sg_leaf_layout main_cols{2, 0, split_col, row_u64};
+    sg_lde* h = nullptr;
+    SG_TRY(commit_enqueue(ctx, st, trace, trace_on_device, n, row_u64, blowup, weights, 0, &main_cols, host_lde_out,
+                          &h));
+    int rc = SG_OK;
+    const uint64_t L = h->leaves_len;
+    if (build_pre) {
+        rc = leaves_row_major(ctx, st, h->d_lde, h->lde_rows, row_u64, 0, split_col, 2, 0, d_pre_nodes + (L - 1) * 32);
+        if (rc == SG_OK) rc = merkle_inner(ctx, st, d_pre_nodes, L);
+    }
+    uint8_t pre[32];
+    cudaError_t e = rc == SG_OK ? cudaMemcpyAsync(h->root, h->d_nodes, 32, cudaMemcpyDeviceToHost, st) : cudaSuccess;
+    if (rc == SG_OK && e == cudaSuccess && build_pre) e = cudaMemcpyAsync(pre, d_pre_nodes, 32, cudaMemcpyDeviceToHost, st);
+    if (rc == SG_OK && e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (rc == SG_OK && e != cudaSuccess) {
+        set_error(std::string("lde commit split: ") + cudaGetErrorString(e));
+        rc = SG_ERR_CUDA;
+    }
+    if (rc != SG_OK) {
+        sg_lde_free(c, h);
+        return rc;
+    }
+    if (root_out) memcpy(root_out, h->root, 32);
+    if (build_pre && root_pre_out) memcpy(root_pre_out, pre, 32);
+    *out = h;
+    return SG_OK;
+}
+
 int sg_batch_commit(sg_ctx* c, void* stream, const sg_table_desc* tables, uint32_t count, uint32_t concurrency,
                     sg_lde** out_ldes, uint8_t* roots_out) {
     SG_CHECK_ARG(c && (count == 0 || (tables && out_ldes)), "null argument");

@@ -784,3 +784,146 @@ int sg_logup_aux(sg_ctx* c, void* stream, const uint64_t* d_main, uint64_t n, ui
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- FRI commit state
+// The stateful form of the FRI commit phase (FriCommitState, crypto/math-cuda/src/fri.rs:48-255):
+// it owns the current codeword and twiddles, and every committed layer's
+// evaluations and Merkle tree stay resident for the query phase.
+struct sg_fri {
+    sg::Ctx* ctx;
+    cudaStream_t st;
+    uint64_t* cur;      // current evaluations (3 * n u64)
+    uint64_t n;
+    bool own_cur;       // false while cur is the caller's layer-0 buffer
+    uint64_t* tw;       // inverse twiddles of the current layer (n / 2 u64)
+    struct Layer {
+        uint64_t* evals;
+        uint64_t n;
+        uint8_t* nodes;
+        uint64_t leaves;
+    };
+    std::vector<Layer> layers;
+    uint64_t* final_evals = nullptr;
+    uint64_t final_n = 0;
+};
+
+extern "C" {
+
+int sg_fri_begin(sg_ctx* c, void* stream, const uint64_t* evals, int evals_on_device, const uint64_t* inv_tw,
+                 int tw_on_device, uint64_t n0, sg_fri** out) {
+    using namespace sg;
+    SG_CHECK_ARG(c && evals && inv_tw && out, "null argument");
+    SG_CHECK_ARG(n0 >= 2 && log2_exact(n0) >= 0, "n0 must be a power of two >= 2");
+    *out = nullptr;
+    Ctx* ctx = CX(c);
+    cudaStream_t st = (cudaStream_t)stream;
+    sg_fri* f = new sg_fri{ctx, st, nullptr, n0, false, nullptr, {}};
+    int rc = SG_OK;
+    if (evals_on_device) {
+        f->cur = const_cast<uint64_t*>(evals);
+    } else {
+        rc = dev_alloc(ctx, st, 24 * n0, (void**)&f->cur);
+        f->own_cur = rc == SG_OK;
+        if (rc == SG_OK && cudaMemcpyAsync(f->cur, evals, 24 * n0, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+            set_error("fri: evaluations upload failed");
+            rc = SG_ERR_CUDA;
+        }
+    }
+    if (rc == SG_OK) rc = dev_alloc(ctx, st, 8 * (n0 / 2), (void**)&f->tw);
+    if (rc == SG_OK && cudaMemcpyAsync(f->tw, inv_tw, 8 * (n0 / 2),
+                                       tw_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                       st) != cudaSuccess) {
+        set_error("fri: twiddles upload failed");
+        rc = SG_ERR_CUDA;
+    }
+    if (rc != SG_OK) {
+        sg_fri_free(f);
+        return rc;
+    }
+    *out = f;
+    return SG_OK;
+}
+
+static int fri_fold_step(sg_fri* f, const uint64_t zeta[3], bool commit, uint8_t root_out[32],
+                         uint64_t* host_evals_out) {
+    using namespace sg;
+    SG_CHECK_ARG(f && zeta, "null argument");
+    SG_CHECK_ARG(!f->final_evals, "the final fold has been taken");
+    const uint64_t h = f->n / 2;
+    SG_CHECK_ARG(h >= (commit ? 2u : 1u), "codeword too short for another fold");
+    Ctx* ctx = f->ctx;
+    uint64_t *out = nullptr, *twn = nullptr;
+    uint8_t* nodes = nullptr;
+    const uint64_t nl = h / 2;
+    int rc = dev_alloc(ctx, f->st, 24 * h, (void**)&out);
+    if (rc == SG_OK) rc = dev_alloc(ctx, f->st, 8 * (nl ? nl : 1), (void**)&twn);
+    if (rc == SG_OK && commit) rc = dev_alloc(ctx, f->st, (2 * nl - 1) * 32, (void**)&nodes);
+    if (rc == SG_OK)
+        rc = sg_fri_fold_layer(reinterpret_cast<sg_ctx*>(ctx), f->st, f->cur, h, f->tw, zeta, out, twn,
+                               commit ? nodes + (nl - 1) * 32 : nullptr);
+    if (rc == SG_OK && commit) rc = merkle_inner(ctx, f->st, nodes, nl);
+    cudaError_t e = cudaSuccess;
+    if (rc == SG_OK && commit && root_out) e = cudaMemcpyAsync(root_out, nodes, 32, cudaMemcpyDeviceToHost, f->st);
+    if (rc == SG_OK && e == cudaSuccess && host_evals_out)
+        e = cudaMemcpyAsync(host_evals_out, out, 24 * h, cudaMemcpyDeviceToHost, f->st);
+    if (rc == SG_OK && e == cudaSuccess) e = cudaStreamSynchronize(f->st);
+    if (rc == SG_OK && e != cudaSuccess) {
+        set_error(std::string("fri fold: ") + cudaGetErrorString(e));
+        rc = SG_ERR_CUDA;
+    }
+    if (rc != SG_OK) {
+        dev_free(ctx, f->st, out, 24 * h);
+        dev_free(ctx, f->st, twn, 8 * (nl ? nl : 1));
+        dev_free(ctx, f->st, nodes, (2 * nl - 1) * 32);
+        return rc;
+    }
+    if (f->own_cur && f->layers.empty()) dev_free(ctx, f->st, f->cur, 24 * f->n);  // the uploaded layer 0
+    dev_free(ctx, f->st, f->tw, 8 * (f->n / 2 ? f->n / 2 : 1));
+    f->tw = twn;
+    if (commit) {
+        f->layers.push_back({out, h, nodes, nl});
+    } else {
+        f->final_evals = out;
+        f->final_n = h;
+    }
+    f->cur = out;
+    f->n = h;
+    return SG_OK;
+}
+
+int sg_fri_fold_commit_layer(sg_fri* f, const uint64_t zeta[3], uint8_t root_out[32], uint64_t* host_evals_out) {
+    return fri_fold_step(f, zeta, true, root_out, host_evals_out);
+}
+
+int sg_fri_fold_final(sg_fri* f, const uint64_t zeta[3], uint64_t* host_evals_out) {
+    return fri_fold_step(f, zeta, false, nullptr, host_evals_out);
+}
+
+uint32_t sg_fri_num_layers(const sg_fri* f) { return f ? (uint32_t)f->layers.size() : 0; }
+
+int sg_fri_layer(const sg_fri* f, uint32_t layer, const uint64_t** d_evals, uint64_t* n, const uint8_t** d_nodes,
+                 uint64_t* leaves_len) {
+    SG_CHECK_ARG(f && layer < f->layers.size(), "no such FRI layer");
+    const auto& L = f->layers[layer];
+    if (d_evals) *d_evals = L.evals;
+    if (n) *n = L.n;
+    if (d_nodes) *d_nodes = L.nodes;
+    if (leaves_len) *leaves_len = L.leaves;
+    return SG_OK;
+}
+
+void sg_fri_free(sg_fri* f) {
+    using namespace sg;
+    if (!f) return;
+    Ctx* ctx = f->ctx;
+    for (auto& L : f->layers) {
+        dev_free(ctx, f->st, L.evals, 24 * L.n);
+        dev_free(ctx, f->st, L.nodes, (2 * L.leaves - 1) * 32);
+    }
+    if (f->final_evals) dev_free(ctx, f->st, f->final_evals, 24 * f->final_n);
+    if (f->own_cur && f->layers.empty() && !f->final_evals) dev_free(ctx, f->st, f->cur, 24 * f->n);
+    if (f->tw) dev_free(ctx, f->st, f->tw, 8 * (f->n / 2 ? f->n / 2 : 1));
+    delete f;
+}
+
+}  // extern "C"

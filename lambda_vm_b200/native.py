@@ -109,6 +109,13 @@ PROTOTYPES = {
     "sg_lde_get_info": (i32, [vp, C.POINTER(LdeInfo)]),
     "sg_lde_free": (None, [vp, vp]),
     "sg_lde_free_async": (None, [vp, vp, vp]),
+    "sg_lde_commit_split": (i32, [vp, vp, vp, i32, u64, u64, u32, vp, u64, i32, vp, vp, vp, vp, vp]),
+    "sg_fri_begin": (i32, [vp, vp, vp, i32, vp, i32, u64, vp]),
+    "sg_fri_fold_commit_layer": (i32, [vp, vp, vp, vp]),
+    "sg_fri_fold_final": (i32, [vp, vp, vp]),
+    "sg_fri_num_layers": (u32, [vp]),
+    "sg_fri_layer": (i32, [vp, u32, vp, vp, vp, vp]),
+    "sg_fri_free": (None, [vp]),
     "sg_batch_commit": (i32, [vp, vp, vp, u32, u32, vp, vp]),
     "sg_table_proof_shape": (i32, [vp, vp]),
     "sg_ctx_dft_tiles": (i32, [vp, u32, u32]),

@@ -140,3 +140,69 @@ def test_logup_aux_matches_oracle(be, n, m, K, n_out, n_comm):
     want_aux, want_L = O.logup_aux(main, desc, alpha, z)
     assert (aux == O.canon_array(want_aux)).all()
     assert (L == O.canon_array(want_L)).all()
+
+
+@pytest.mark.parametrize("n0,layers", [(64, 3), (1024, 7), (1 << 14, 5)])
+def test_fri_commit_state_matches_oracle_chain(be, n0, layers):
+    """sg_fri (FriCommitState): each committed layer's evaluations, leaves and
+    root follow the oracle's fold chain, the twiddles square from layer to
+    layer, and the final fold matches."""
+    import ctypes as C
+    from lambda_vm_b200 import native
+    L = native.lib()
+    rng = np.random.default_rng(n0)
+    ev = rf(rng, (n0, 3)).reshape(-1)
+    tw = rf(rng, (n0 // 2,))
+    f = C.c_void_p()
+    native.check(L.sg_fri_begin(be.h, None, ev.ctypes.data, 0, tw.ctypes.data, 0, n0, C.byref(f)))
+    try:
+        cur, ctw = O.canon_array(ev), tw.copy()
+        for li in range(layers):
+            zeta = rf(rng, (3,))
+            root = (C.c_uint8 * 32)()
+            host = np.zeros(3 * (len(cur) // 6), np.uint64)
+            native.check(L.sg_fri_fold_commit_layer(f, zeta.ctypes.data, root, host.ctypes.data))
+            want = O.canon_array(O.fri_fold(cur, ctw, zeta))
+            assert (host == want.reshape(-1)).all()
+            nodes = O.merkle_nodes(O.fri_leaves(want))
+            assert bytes(root) == nodes[0].tobytes()
+            d_ev, n, d_nodes, nl = C.c_void_p(), C.c_uint64(), C.c_void_p(), C.c_uint64()
+            native.check(L.sg_fri_layer(f, li, C.byref(d_ev), C.byref(n), C.byref(d_nodes), C.byref(nl)))
+            assert n.value == len(want.reshape(-1)) // 3 and nl.value == n.value // 2
+            cur = want.reshape(-1)
+            ctw = np.array([O.canonical(O.gl_mul(int(ctw[2 * j]), int(ctw[2 * j]))) for j in range(len(ctw) // 2)],
+                           np.uint64)
+        assert L.sg_fri_num_layers(f) == layers
+        zeta = rf(rng, (3,))
+        fin = np.zeros(3 * (len(cur) // 6), np.uint64)
+        native.check(L.sg_fri_fold_final(f, zeta.ctypes.data, fin.ctypes.data))
+        assert (fin == O.canon_array(O.fri_fold(cur, ctw, zeta)).reshape(-1)).all()
+        assert L.sg_fri_fold_final(f, zeta.ctypes.data, None) == native.SG_ERR_INVALID
+    finally:
+        L.sg_fri_free(f)
+
+
+def test_split_commit_matches_two_column_range_trees(be):
+    """sg_lde_commit_split (coset_lde_row_major_split_trees): one LDE, a main
+    tree over columns [split, m) and a precomputed tree over [0, split)."""
+    import ctypes as C
+    from lambda_vm_b200 import native
+    L = native.lib()
+    rng = np.random.default_rng(77)
+    n, m, B, split = 1 << 9, 11, 4, 4
+    t = rf(rng, (n, m))
+    w = O.coset_weights(n, 3)
+    Lv = n * B // 2
+    pre = C.c_void_p()
+    native.check(L.sg_dev_alloc(be.h, None, (2 * Lv - 1) * 32, C.byref(pre)))
+    h = C.c_void_p()
+    root, root_pre = (C.c_uint8 * 32)(), (C.c_uint8 * 32)()
+    host = np.zeros((n * B, m), np.uint64)
+    native.check(L.sg_lde_commit_split(be.h, None, t.ctypes.data, 0, n, m, B, w.ctypes.data, split, 1,
+                                       host.ctypes.data, C.byref(h), root, pre, root_pre))
+    lde = O.canon_array(O.coset_lde_row_major(t, B, w))
+    assert (host == lde).all()
+    assert bytes(root) == O.merkle_nodes(O.leaves_row_major(lde, 2, False, col_range=(split, m)))[0].tobytes()
+    assert bytes(root_pre) == O.merkle_nodes(O.leaves_row_major(lde, 2, False, col_range=(0, split)))[0].tobytes()
+    L.sg_lde_free(be.h, h)
+    L.sg_dev_free(be.h, None, pre, (2 * Lv - 1) * 32)
