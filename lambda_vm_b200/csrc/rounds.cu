@@ -927,3 +927,48 @@ void sg_fri_free(sg_fri* f) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- field self-test
+// Element-wise Goldilocks / Fp3 operations on device vectors, for checking the
+// device arithmetic (add, sub, mul, reduce, Fp3 mul / inverse, the lazily
+// reduced sums) against exact integer arithmetic on the host. Ops:
+//   0 add, 1 sub, 2 mul, 3 canon(a), 4 neg(a), 5 inv(a), 6 sqr(a),
+//   7 Fp3 mul (a, b, out: 3 u64 per element), 8 Fp3 inverse (a),
+//   9 reduce128 of (a = low 64 bits, b = high 64 bits),
+//   10 sum of a[i] * b[j] for j < 16 accumulated unreduced (wacc) then reduced.
+namespace sg {
+__global__ void k_field_ops(uint32_t op, const uint64_t* a, const uint64_t* b, uint64_t* out, uint64_t n) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    switch (op) {
+        case 0: out[i] = gl::add(a[i], b[i]); break;
+        case 1: out[i] = gl::sub(a[i], b[i]); break;
+        case 2: out[i] = gl::mul(a[i], b[i]); break;
+        case 3: out[i] = gl::canon(a[i]); break;
+        case 4: out[i] = gl::neg(a[i]); break;
+        case 5: out[i] = gl::inv(gl::canon(a[i])); break;
+        case 6: out[i] = gl::sqr(a[i]); break;
+        case 7: st3(out + 3 * i, gl::mul3(ld3(a + 3 * i), ld3(b + 3 * i))); break;
+        case 8: st3(out + 3 * i, gl::inv3(ld3(a + 3 * i))); break;
+        case 9:
+            out[i] = gl::reduce128((uint32_t)a[i], (uint32_t)(a[i] >> 32), (uint32_t)b[i], (uint32_t)(b[i] >> 32));
+            break;
+        case 10: {
+            gl::wacc w = gl::wzero();
+            for (uint64_t j = 0; j < 16; ++j) gl::wmac(w, a[i], b[(i + j) % n]);
+            out[i] = gl::wreduce(w);
+            break;
+        }
+        default: break;
+    }
+}
+}  // namespace sg
+
+extern "C" int sg_field_ops(sg_ctx* c, void* stream, uint32_t op, const uint64_t* d_a, const uint64_t* d_b,
+                            uint64_t* d_out, uint64_t n) {
+    using namespace sg;
+    SG_CHECK_ARG(c && op <= 10, "null context or unknown op");
+    if (n == 0) return SG_OK;
+    k_field_ops<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(op, d_a, d_b, d_out, n);
+    return check_launch(CX(c), "k_field_ops");
+}
