@@ -337,7 +337,7 @@ int sg_merkle_build(sg_ctx* c, void* stream, const uint8_t* d_leaves, uint64_t n
 // later chunks runs under the DFT passes of the earlier ones. With a
 // page-locked host trace the copies are asynchronous; with pageable memory
 // they are staged by the driver and the overlap is lost, not the result.
-static constexpr uint64_t kChunkCols = 64;
+static constexpr uint64_t kChunkCols = 32;  // fastest of 16/24/32/48/64 at 2^20 x 256
 
 // When `leaves` is non-null the commit's leaves are one LDE row each over the
 // whole row: they are then absorbed window by window as the LDE columns

@@ -122,9 +122,10 @@ def test_merkle_tree_matches_oracle(be, n):
 @pytest.mark.parametrize("log_n,m,blowup,R,le", [
     (3, 4, 2, 2, False), (8, 7, 4, 2, False), (10, 64, 2, 2, False), (13, 32, 4, 1, True),
     (14, 12, 2, 2, False), (12, 256, 4, 1, True), (11, 3 * 5, 2, 2, False),
-    # host traces of >= 128 columns are uploaded in 64-column chunks; one-row
+    # host traces of >= 64 columns are uploaded in 32-column chunks; one-row
     # leaves are then absorbed in 17-lane windows as the chunks complete
-    (10, 300, 2, 1, False), (9, 130, 4, 1, True), (11, 200, 2, 2, False), (8, 128, 8, 1, False)])
+    (10, 300, 2, 1, False), (9, 130, 4, 1, True), (11, 200, 2, 2, False), (8, 128, 8, 1, False),
+    (10, 64, 2, 1, False), (9, 63, 2, 1, True), (10, 97, 2, 1, True), (9, 65, 4, 2, False)])
 def test_lde_commit_root_matches_oracle(be, log_n, m, blowup, R, le):
     """merkle_root_parity.rs: GPU LDE + leaves + tree root == CPU row-major
     LDE + commit_rows_bit_reversed."""
