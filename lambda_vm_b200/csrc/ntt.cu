@@ -714,6 +714,7 @@ int coset_lde_ld(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t trac
     SG_CHECK_ARG(logB >= 0, "blowup must be a power of two");
     const int logN = logn + logB;
     SG_CHECK_ARG(logN <= 32, "LDE size must be <= 2^32 (TWO_ADICITY)");
+    SG_CHECK_ARG(trace_ld <= (~0ULL / 8) >> logn && out_ld <= (~0ULL / 8) >> logN, "matrix size overflows 64 bits");
     if (logn > 24) {
         set_error("traces longer than 2^24 rows are not supported by the two-pass kernel");
         return SG_ERR_UNSUPPORTED;
@@ -796,11 +797,14 @@ extern "C" int sg_coset_lde_static(void* stream, const uint64_t* d_trace, uint64
     const int logN = logn + logB;
     SG_CHECK_ARG(logN <= 32 && logn <= 24, "LDE size out of range");
     const uint64_t N = 1ULL << logN;
-    const uint64_t need = N + 2 * n * m;  // u64 words: omega table + coefficients + four-step intermediate
-    if (need > SG_STATIC_SCRATCH_BYTES / sizeof(uint64_t)) {
-        set_error("sg_coset_lde_static: needs " + std::to_string(need * 8) +
-                  " bytes of scratch ((blowup*n + 2*n*m) * 8) but the static scratch holds " +
-                  std::to_string((unsigned long long)SG_STATIC_SCRATCH_BYTES) + "; use sg_coset_lde");
+    // u64 words needed: omega table (N) + coefficients + four-step intermediate
+    // (n x m each). Bounded by division, so no m wraps N + 2*n*m into range.
+    const uint64_t cap = SG_STATIC_SCRATCH_BYTES / sizeof(uint64_t);
+    if (N > cap || m > (cap - N) / (2 * n)) {
+        set_error("sg_coset_lde_static: n=" + std::to_string(n) + " m=" + std::to_string(m) +
+                  " blowup=" + std::to_string(blowup) +
+                  " needs (blowup*n + 2*n*m) * 8 bytes of scratch, more than the static scratch holds (" +
+                  std::to_string((unsigned long long)SG_STATIC_SCRATCH_BYTES) + " bytes); use sg_coset_lde");
         return SG_ERR_INVALID;
     }
     uint64_t* scratch = nullptr;

@@ -3,11 +3,14 @@ grinding through the C ABI, bit-exact against the CPU oracle (canonical
 values; digests byte for byte). Modelled on crypto/math-cuda/tests/{ntt.rs,
 ntt_known.rs, lde.rs, lde_batch.rs, keccak_leaves.rs, merkle_tree.rs,
 merkle_root_parity.rs, merkle_gather.rs, grinding.rs}."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
 import oracle as O
 from lambda_vm_b200 import math_cuda as mc
+from lambda_vm_b200 import native
 
 pytestmark = pytest.mark.gpu
 P = O.P
@@ -255,3 +258,13 @@ def test_every_dft_tile_width_gives_the_same_lde(be, log_n):
         assert (outs[0] == O.canon_array(O.coset_lde_row_major(t, 2, w))).all()
     with pytest.raises(native.SgError):
         native.check(L.sg_ctx_dft_tiles(be.h, log_len, 5))
+
+
+def test_lde_rejects_sizes_that_overflow(be):
+    """A column count whose matrix size wraps 64 bits is an argument error,
+    raised before any allocation or launch."""
+    L = native.lib()
+    for m in (1 << 61, (1 << 64) - 1):
+        rc = L.sg_coset_lde(be.h, None, C.c_void_p(16), 1 << 10, m, 4, C.c_void_p(16), C.c_void_p(16))
+        assert rc == native.SG_ERR_INVALID
+        assert b"overflows" in L.sg_last_error()

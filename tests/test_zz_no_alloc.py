@@ -63,3 +63,8 @@ def test_static_lde_rejects_oversized_requests(be):
     rc = L.sg_coset_lde_static(None, C.c_void_p(16), n, m, blowup, C.c_void_p(16), C.c_void_p(16))
     assert rc == native.SG_ERR_INVALID
     assert b"static scratch" in L.sg_last_error()
+    # a column count whose scratch size wraps 64 bits is rejected too, before any launch
+    for m in (1 << 63, (1 << 64) - 1, (1 << 64) // (2 << 10) + 1):
+        rc = L.sg_coset_lde_static(None, C.c_void_p(16), 1 << 10, m, 2, C.c_void_p(16), C.c_void_p(16))
+        assert rc == native.SG_ERR_INVALID
+        assert b"static scratch" in L.sg_last_error()
