@@ -335,6 +335,11 @@ def run_serve(a):
     for airs, srcs in specs[:3]:  # and the allocator's block cache, through both provers
         multi_prove(airs, srcs, opts, GpuBackend(be))
         multi_prove_scheduled(airs, srcs, opts, workers=4, be=be)
+    # one burst of every job at once, so the block cache reaches the working
+    # set of max_jobs overlapping proofs before any latency is measured
+    with ProofServer(budget, max_jobs=a.max_jobs, drivers=4, opts=opts, be=be) as srv:
+        for airs, srcs in specs:
+            srv.submit(airs, srcs)
     torch.cuda.synchronize()
     sweep = []
     for i, rate in enumerate(float(x) for x in a.rates.split(",")):
