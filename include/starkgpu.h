@@ -454,8 +454,9 @@ SG_API int sg_prove_table(sg_ctx* ctx, void* stream, sg_transcript* t, const sg_
  *      fuzzes its host field code): d_out[i] = op(d_a[i], d_b[i]) for op
  *      0 add, 1 sub, 2 mul, 3 canon, 4 neg, 5 inv, 6 sqr, 7 Fp3 mul, 8 Fp3 inverse
  *      (3 u64 per element for 7 and 8), 9 reduce of the 128-bit (d_b[i]:d_a[i]),
- *      10 sum_{j<16} d_a[i] * d_b[(i+j) mod n] accumulated unreduced. Outputs are
- *      reduced mod p but not necessarily canonical (except 3). ---- */
+ *      10 sum_{j<16} d_a[i] * d_b[(i+j) mod n] accumulated unreduced, 11 d_a[i] *
+ *      2^(d_b[i] mod 96) by the shift-and-reduce product the DFT butterflies use.
+ *      Outputs are reduced mod p but not necessarily canonical (except 3). ---- */
 SG_API int sg_field_ops(sg_ctx* ctx, void* stream, uint32_t op, const uint64_t* d_a, const uint64_t* d_b,
                         uint64_t* d_out, uint64_t n);
 

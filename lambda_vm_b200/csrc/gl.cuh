@@ -113,6 +113,77 @@ __device__ __forceinline__ uint64_t mul(uint64_t a, uint64_t b) {
     return reduce128(r0, r1, r2, r3);
 }
 
+// Reduce the 96-bit value (w2:w1:w0) mod p: S = (w1:w0) + w2 * EPS < 2^65
+// (2^64 = EPS) as multiply-adds, then its carry c folded as c * EPS, which
+// cannot wrap again (S - 2^64 <= 2^64 - 2^33 when c = 1). Every step but the
+// carry read is a 32-bit multiply-add (FMA pipe).
+__device__ __forceinline__ uint64_t reduce96(uint32_t w0, uint32_t w1, uint32_t w2) {
+    uint32_t s0, s1, c;
+    asm("mad.lo.cc.u32 %0, %3, %5, %4;\n\t"
+        "madc.hi.cc.u32 %1, %3, %5, %6;\n\t"
+        "addc.u32 %2, 0, 0;"
+        : "=r"(s0), "=r"(s1), "=r"(c)
+        : "r"(w2), "r"(w0), "r"(0xFFFFFFFFu), "r"(w1));
+    asm("mad.lo.cc.u32 %0, %2, %3, %0;\n\t"
+        "madc.hi.u32 %1, %2, %3, %1;"
+        : "+r"(s0), "+r"(s1)
+        : "r"(c), "r"(0xFFFFFFFFu));
+    return pack(s0, s1);
+}
+
+
+// (w2:w1:w0) = x * k exactly, for a 32-bit k (four multiply-adds).
+__device__ __forceinline__ void mul_wide_k32(uint64_t x, uint32_t k, uint32_t& w0, uint32_t& w1, uint32_t& w2) {
+    asm("mul.lo.u32 %0, %3, %5;\n\t"
+        "mul.hi.u32 %1, %3, %5;\n\t"
+        "mad.lo.cc.u32 %1, %4, %5, %1;\n\t"
+        "madc.hi.u32 %2, %4, %5, 0;"
+        : "=r"(w0), "=r"(w1), "=r"(w2)
+        : "r"(lo32(x)), "r"(hi32(x)), "r"(k));
+}
+
+// x * k mod p for a 32-bit k: the 96-bit product, reduced.
+__device__ __forceinline__ uint64_t mul_k32(uint64_t x, uint32_t k) {
+    uint32_t w0, w1, w2;
+    mul_wide_k32(x, k, w0, w1, w2);
+    return reduce96(w0, w1, w2);
+}
+
+// x * 2^S mod p for a compile-time 0 <= S < 96 (2^96 = -1, so every power of
+// two is +-2^S with S in this range), from y = x * 2^(S mod 32) as three
+// exact words (w2:w1:w0) placed S div 32 words up:
+//   S < 32:  reduce96(w0, w1, w2)
+//   S < 64:  words (w2:w1:w0:0): reduce128
+//   S >= 64: w0 2^64 + w1 2^96 + w2 2^128 = w0 EPS - (w2:w1)
+// (2^64 = EPS, 2^96 = -1, 2^128 = -2^32). Of the forms measured in the DFT's
+// register butterflies, this mix of FMA-pipe and ALU-pipe work was fastest.
+template <int S>
+__device__ __forceinline__ uint64_t mul_2exp(uint64_t x) {
+    static_assert(S >= 0 && S < 96, "exponent out of range");
+    if constexpr (S == 0) {
+        return x;
+    } else if constexpr (S == 32) {
+        return reduce96(0, lo32(x), hi32(x));
+    } else if constexpr (S == 64) {
+        return mul_k32(x, 0xFFFFFFFFu);
+    } else {
+        uint32_t w0, w1, w2;
+        mul_wide_k32(x, 1u << (S % 32), w0, w1, w2);
+        if constexpr (S < 32) {
+            return reduce96(w0, w1, w2);
+        } else if constexpr (S < 64) {
+            return reduce128(0, w0, w1, w2);
+        } else {
+            uint32_t t0, t1;
+            asm("mul.lo.u32 %0, %2, %3;\n\t"
+                "mul.hi.u32 %1, %2, %3;"
+                : "=r"(t0), "=r"(t1)
+                : "r"(w0), "r"(0xFFFFFFFFu));
+            return sub(pack(t0, t1), pack(w1, w2));
+        }
+    }
+}
+
 __device__ __forceinline__ uint64_t sqr(uint64_t a) { return mul(a, a); }
 
 __device__ __forceinline__ uint64_t neg(uint64_t a) {
@@ -277,6 +348,16 @@ constexpr uint64_t root(uint32_t log_n) {
     uint64_t r = 1753635133440165772ULL;
     for (uint32_t i = 0; i < 32 - log_n; i++) r = mul(r, r);
     return log_n == 0 ? 1 : r;
+}
+// The S in [0, 192) with 2^S = v (2 has order 192), or -1 when v is not a
+// power of two. Every 64th root of unity is one: omega_64 is 2^39 here.
+constexpr int log2_of(uint64_t v) {
+    uint64_t c = 1;
+    for (int s = 0; s < 192; ++s) {
+        if (c == v) return s;
+        c = mul(c, 2);
+    }
+    return -1;
 }
 constexpr uint64_t inv(uint64_t a) { return pow(a, P - 2); }
 }  // namespace glc

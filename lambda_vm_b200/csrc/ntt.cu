@@ -28,44 +28,57 @@
 // c_i * w_{Bn}^{ij} (steps F1, F2). F1 writes its B outputs straight into the
 // LDE buffer at the rows F2 later reads and overwrites, so F2 runs in place and
 // the LDE needs no scratch beyond two n x m buffers.
+#include <utility>
+
 #include "common.cuh"
 #include "gl.cuh"
 
 namespace sg {
 
-struct W64 {
-    uint64_t v[64];
-    constexpr W64() : v() {
-        uint64_t w = glc::root(6), c = 1;
-        for (int i = 0; i < 64; ++i) {
-            v[i] = c;
-            c = glc::mul(c, w);
-        }
+// f(integral_constant<int, 0>) ... f(integral_constant<int, N-1>), so loop
+// indices are compile-time constants inside f.
+template <typename F, int... I>
+__device__ __forceinline__ void static_for_(F&& f, std::integer_sequence<int, I...>) {
+    (f(std::integral_constant<int, I>{}), ...);
+}
+template <int N, typename F>
+__device__ __forceinline__ void static_for(F&& f) {
+    static_for_(f, std::make_integer_sequence<int, N>{});
+}
+
+// One radix-2 butterfly (a, t) -> (a + w t, a - w t) with w = omega_64^E.
+// Every 64th root of unity is +-2^S (S < 96), so w t is a shift-and-reduce
+// product of 32-bit constants (gl::mul_2exp) instead of a full 64x64
+// multiply, and a negative w swaps the two outputs instead of negating.
+template <int E>
+__device__ __forceinline__ void bfly_w64(uint64_t& x, uint64_t& y) {
+    constexpr int S = glc::log2_of(glc::pow(glc::root(6), (uint64_t)E));
+    static_assert(S >= 0, "64th roots of unity are powers of two");
+    const uint64_t a = x, t = gl::mul_2exp<S % 96>(y);
+    if constexpr (S >= 96) {
+        x = gl::sub(a, t);
+        y = gl::add(a, t);
+    } else {
+        x = gl::add(a, t);
+        y = gl::sub(a, t);
     }
-};
-// omega_64^e with omega_64 derived from the reference's two-adic generator.
-__constant__ W64 c_w64 = W64();
+}
 
 // 2^Q-point DFT on registers: bit-reversed input order, natural output order.
 template <int Q, bool INVD>
 __device__ __forceinline__ void dit_reg(uint64_t* v) {
     constexpr int R = 1 << Q;
-#pragma unroll
-    for (int h = 1; h < R; h <<= 1) {
-#pragma unroll
-        for (int b = 0; b < R; b += 2 * h) {
-#pragma unroll
-            for (int j = 0; j < h; ++j) {
-                uint64_t a = v[b + j], t = v[b + j + h];
-                if (j != 0) {
-                    const int e = j * (64 / (2 * h));
-                    t = gl::mul(t, INVD ? c_w64.v[(64 - e) & 63] : c_w64.v[e]);
-                }
-                v[b + j] = gl::add(a, t);
-                v[b + j + h] = gl::sub(a, t);
-            }
-        }
-    }
+    static_for<Q>([&](auto lh) {
+        constexpr int h = 1 << decltype(lh)::value;
+        static_for<R / (2 * h)>([&](auto bi) {
+            constexpr int b = decltype(bi)::value * 2 * h;
+            static_for<h>([&](auto ji) {
+                constexpr int j = decltype(ji)::value;
+                constexpr int e = j * (64 / (2 * h));
+                bfly_w64<INVD ? (64 - e) & 63 : e>(v[b + j], v[b + j + h]);
+            });
+        });
+    });
 }
 
 template <int Q>

@@ -937,6 +937,15 @@ void sg_fri_free(sg_fri* f) {
 //   9 reduce128 of (a = low 64 bits, b = high 64 bits),
 //   10 sum of a[i] * b[j] for j < 16 accumulated unreduced (wacc) then reduced.
 namespace sg {
+// gl::mul_2exp<S> for a runtime S < 96 (a chain of compile-time cases).
+template <int S>
+__device__ __forceinline__ uint64_t mul_2exp_rt(uint64_t x, uint32_t s) {
+    if constexpr (S == 96)
+        return 0;
+    else
+        return s == S ? gl::mul_2exp<S>(x) : mul_2exp_rt<S + 1>(x, s);
+}
+
 __global__ void k_field_ops(uint32_t op, const uint64_t* a, const uint64_t* b, uint64_t* out, uint64_t n) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -959,6 +968,7 @@ __global__ void k_field_ops(uint32_t op, const uint64_t* a, const uint64_t* b, u
             out[i] = gl::wreduce(w);
             break;
         }
+        case 11: out[i] = mul_2exp_rt<0>(a[i], (uint32_t)(b[i] % 96)); break;
         default: break;
     }
 }
@@ -967,7 +977,7 @@ __global__ void k_field_ops(uint32_t op, const uint64_t* a, const uint64_t* b, u
 extern "C" int sg_field_ops(sg_ctx* c, void* stream, uint32_t op, const uint64_t* d_a, const uint64_t* d_b,
                             uint64_t* d_out, uint64_t n) {
     using namespace sg;
-    SG_CHECK_ARG(c && op <= 10, "null context or unknown op");
+    SG_CHECK_ARG(c && op <= 11, "null context or unknown op");
     if (n == 0) return SG_OK;
     k_field_ops<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(op, d_a, d_b, d_out, n);
     return check_launch(CX(c), "k_field_ops");

@@ -66,6 +66,17 @@ def test_reduce128(be):
         assert g <= M64 and g % P == (x + (y << 64)) % P
 
 
+def test_mul_by_power_of_two(be):
+    # every exponent 0..95 (2^96 = -1 covers the rest), each on the edge values
+    # and on random words; the DFT butterflies multiply by these constants
+    rng = np.random.default_rng(8)
+    xs = EDGE + [int(v) for v in rng.integers(0, 2**64, size=40, dtype=np.uint64)]
+    a = [x for x in xs for _ in range(96)]
+    b = [s for _ in xs for s in range(96)]
+    for g, x, s in zip(_run(be, 11, a, b), a, b):
+        assert g <= M64 and g % P == (x << s) % P, (hex(x), s, hex(g))
+
+
 def test_unreduced_sums(be):
     rng = np.random.default_rng(6)
     a = [int(v) for v in rng.integers(2**63, 2**64, size=512, dtype=np.uint64)] + EDGE
