@@ -110,8 +110,9 @@ SG_API int sg_coset_lde(sg_ctx* ctx, void* stream, const uint64_t* d_trace, uint
  *      several compiled tile widths (columns per tile; 4/8/16 for lengths
  *      2^8..2^10, 4/8 for 2^11). On a context's first pass of a length, every
  *      width is timed on the same work and its time per column kept; a pass
- *      over m columns then uses the width minimising ceil(m/C)*C*cost(C).
- *      Results never depend on the width. sg_ctx_dft_tiles pins a width for a
+ *      over m columns then uses the width minimising ceil(m/C)*C*cost(C),
+ *      keeping the default width (16 up to 2^10, 8 at 2^11) unless another is
+ *      at least 3 % cheaper. Results never depend on the width. sg_ctx_dft_tiles pins a width for a
  *      length (cols = 0: automatic); sg_ctx_dft_tuning reports the widths and
  *      their time per column (ms), timing them on `stream` first if needed. ---- */
 SG_API int sg_ctx_dft_tiles(sg_ctx* ctx, uint32_t log_len, uint32_t cols);

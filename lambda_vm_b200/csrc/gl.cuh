@@ -131,7 +131,6 @@ __device__ __forceinline__ uint64_t reduce96(uint32_t w0, uint32_t w1, uint32_t 
     return pack(s0, s1);
 }
 
-
 // (w2:w1:w0) = x * k exactly, for a 32-bit k (four multiply-adds).
 __device__ __forceinline__ void mul_wide_k32(uint64_t x, uint32_t k, uint32_t& w0, uint32_t& w1, uint32_t& w2) {
     asm("mul.lo.u32 %0, %3, %5;\n\t"
@@ -167,8 +166,10 @@ __device__ __forceinline__ uint64_t mul_2exp(uint64_t x) {
     } else if constexpr (S == 64) {
         return mul_k32(x, 0xFFFFFFFFu);
     } else {
-        uint32_t w0, w1, w2;
-        mul_wide_k32(x, 1u << (S % 32), w0, w1, w2);
+        // y = x * 2^r as three words by funnel shifts (ALU pipe: this form
+        // measured 1 % faster in the DFT than four multiply-adds)
+        constexpr int r = S % 32;
+        const uint32_t w0 = lo32(x) << r, w1 = __funnelshift_l(lo32(x), hi32(x), r), w2 = hi32(x) >> (32 - r);
         if constexpr (S < 32) {
             return reduce96(w0, w1, w2);
         } else if constexpr (S < 64) {
