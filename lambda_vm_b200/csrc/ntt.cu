@@ -131,19 +131,20 @@ struct PassArgs {
 };
 
 // Compile-time stage plan per tile: 2^LOGL points x CC columns. A tile runs
-// NST register stages of at most 2^QM points each (larger radices first).
+// NST register stages of at most 2^QM points each (larger radices first):
+// 2^5 where a thread may hold 128 registers (tiles of 8+ columns; a 2^10
+// pass is then 2^5 x 2^5, one shared-memory round trip and 31/32 general
+// twiddle products a point instead of 2^4 x 2^3 x 2^3 with 7/4), 2^4 for
+// the 4-column tiles, whose 64-register budget a 32-point stage would spill.
 // The column count is a tuning choice: several are compiled per tile length
 // and the context picks one per call (see pick_cols).
-#ifndef SG_DFT_QMAX
-#define SG_DFT_QMAX 4
-#endif
 // Default (and untuned) columns per tile for 2^logL-point passes.
 __host__ __device__ constexpr int default_cols(int logL) {
     return logL <= 7 ? 32 : (logL <= 10 ? 16 : (logL == 11 ? 8 : 4));
 }
 template <int LOGL, int CC>
 struct Plan {
-    static constexpr int QM = SG_DFT_QMAX;
+    static constexpr int QM = CC <= 4 ? 4 : 5;
     static constexpr int NST = LOGL == 0 ? 0 : (LOGL <= 5 ? 1 : ((LOGL + QM - 1) / QM < 2 ? 2 : (LOGL + QM - 1) / QM));
     static constexpr int q(int s) { return NST == 0 ? 0 : LOGL / NST + (s < LOGL % NST ? 1 : 0); }
     static constexpr int lgns(int s) { return s == 0 ? 0 : lgns(s - 1) + q(s - 1); }
@@ -151,7 +152,10 @@ struct Plan {
     static constexpr int C = CC;
     static constexpr int T = LOGL >= 11 ? 512 : (LOGL == 10 && C >= 16 ? 512 : 256);
     // CTAs per SM the register allocation must allow (64K registers per SM).
-    static constexpr int MINB = T <= 256 ? (C <= 4 && LOGL >= 10 ? 4 : 2) : (LOGL == 10 ? 2 : 1);
+    // 512-thread tiles are planned at one CTA per SM (up to 128 registers a
+    // thread); the 2^10-point ones hold 155 KB of shared memory, so a second
+    // CTA would not fit beside them in any case.
+    static constexpr int MINB = T <= 256 ? (C <= 4 && LOGL >= 10 ? 4 : 2) : 1;
     static constexpr uint32_t L = 1u << LOGL;
     static constexpr uint32_t CS0 = L + (NST > 1 ? (L >> Q1) : 0);
     static constexpr uint32_t CP = C < 16 ? C : 16;
