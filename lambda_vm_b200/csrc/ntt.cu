@@ -135,7 +135,9 @@ struct PassArgs {
 // 2^5 where a thread may hold 128 registers (tiles of 8+ columns; a 2^10
 // pass is then 2^5 x 2^5, one shared-memory round trip and 31/32 general
 // twiddle products a point instead of 2^4 x 2^3 x 2^3 with 7/4), 2^4 for
-// the 4-column tiles, whose 64-register budget a 32-point stage would spill.
+// the 4-column tiles, planned at four 256-thread CTAs per SM (64 registers):
+// 2^5 stages at two CTAs per SM measured slower on the narrow LDEs those
+// tiles serve (2^20 x 3 columns, blowup 2: 0.42 against 0.35 ms).
 // The column count is a tuning choice: several are compiled per tile length
 // and the context picks one per call (see pick_cols).
 // Default (and untuned) columns per tile for 2^logL-point passes.
@@ -226,8 +228,10 @@ __device__ __forceinline__ void tile_body(const PassArgs& a, uint64_t* S, const 
     constexpr uint32_t L = PL::L, C = PL::C, T = PL::T;
     uint64_t* Fpre = F;
     uint64_t* Fpost = PL::NST > 1 ? F : F + L;
+    // coset-shift pre factors omega^(row * rep): rep 0 scales by omega^0 = 1
+    const bool pre = a.pre_kind == 1 && rep != 0;
     // ---- pre factors
-    if (a.pre_kind == 1) {
+    if (pre) {
         const uint64_t pmask = (1ULL << a.pre_log) - 1;
         for (uint32_t i = threadIdx.x; i < L; i += T) {
             const uint64_t row = pt * a.in_ts + (uint64_t)i * a.in_ps;
@@ -252,7 +256,7 @@ __device__ __forceinline__ void tile_body(const PassArgs& a, uint64_t* S, const 
         for (uint32_t c = threadIdx.x; c < C; c += T) {
             if (c < ncols) {
                 uint64_t v = in[c];
-                if (a.pre_kind == 1) v = gl::mul(v, Fpre[0]);
+                if (pre) v = gl::mul(v, Fpre[0]);
                 out[c] = finish(a, v, Fpost[0]);
             }
         }
@@ -269,7 +273,7 @@ __device__ __forceinline__ void tile_body(const PassArgs& a, uint64_t* S, const 
                 const uint64_t* src = in + (uint64_t)jb * ip + c;
 #pragma unroll
                 for (uint32_t r = 0; r < R; ++r) v[r] = __ldg(src + (uint64_t)(brev_q<Q>(r) * per_col) * ip);
-                if (a.pre_kind == 1) {
+                if (pre) {
 #pragma unroll
                     for (uint32_t r = 0; r < R; ++r) v[r] = gl::mul(v[r], Fpre[jb + brev_q<Q>(r) * per_col]);
                 }
