@@ -202,7 +202,27 @@ __device__ __forceinline__ uint64_t pow(uint64_t a, uint64_t e) {
     return r;
 }
 
-__device__ __forceinline__ uint64_t inv(uint64_t a) { return pow(a, GL_P - 2); }
+// x^(2^n) by n squarings.
+__device__ __forceinline__ uint64_t sqn(uint64_t x, int n) {
+    for (int i = 0; i < n; ++i) x = mul(x, x);
+    return x;
+}
+
+// a^(p-2) = a^-1 (0 -> 0) by an addition chain: p - 2 = (2^31 - 1) 2^33 +
+// (2^32 - 1), and t_k = a^(2^k - 1) doubles as t_{j+k} = t_j^(2^k) t_k. 64
+// squarings and 9 products against 127 for square-and-multiply: the inverse
+// is a single dependent chain, so its length is its latency.
+__device__ __forceinline__ uint64_t inv(uint64_t a) {
+    const uint64_t t2 = mul(sqr(a), a);           // 2^2 - 1
+    const uint64_t t3 = mul(sqr(t2), a);          // 2^3 - 1
+    const uint64_t t6 = mul(sqn(t3, 3), t3);      // 2^6 - 1
+    const uint64_t t12 = mul(sqn(t6, 6), t6);     // 2^12 - 1
+    const uint64_t t24 = mul(sqn(t12, 12), t12);  // 2^24 - 1
+    const uint64_t t30 = mul(sqn(t24, 6), t6);    // 2^30 - 1
+    const uint64_t t31 = mul(sqr(t30), a);        // 2^31 - 1
+    const uint64_t t32 = mul(sqr(t31), a);        // 2^32 - 1
+    return mul(sqn(t31, 33), t32);                // (2^31 - 1) 2^33 + 2^32 - 1
+}
 
 // ---------------------------------------------------------------- Fp3
 struct fe3 {
