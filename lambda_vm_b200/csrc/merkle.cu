@@ -312,6 +312,29 @@ extern "C" int sg_merkle_gather_paths(sg_ctx* c, void* stream, const uint8_t* d_
     return check_launch(ctx, "k_gather_paths");
 }
 
+// Grid of the grinding search: exactly the CTAs that are resident at once.
+// The search must return the smallest valid nonce, so it can only stop once
+// every smaller nonce is checked; CTAs beyond the resident ones would start
+// late on the low nonces of each sweep and hold the whole search open.
+static int grind_grid(unsigned* grid) {
+    static std::once_flag once;
+    static unsigned g = 0;
+    static cudaError_t err = cudaSuccess;
+    std::call_once(once, [] {
+        int dev = 0, sms = 0, per_sm = 0;
+        err = cudaGetDevice(&dev);
+        if (err == cudaSuccess) err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (err == cudaSuccess) err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_grind, 256, 0);
+        g = (unsigned)(sms > 0 ? sms : 1) * (unsigned)(per_sm > 0 ? per_sm : 1);
+    });
+    if (err != cudaSuccess) {
+        set_error(std::string("grind: occupancy query: ") + cudaGetErrorString(err));
+        return SG_ERR_CUDA;
+    }
+    *grid = g;
+    return SG_OK;
+}
+
 extern "C" int sg_grind(sg_ctx* c, void* stream, const uint64_t inner_lanes[4], uint8_t grinding_factor,
                         uint64_t* nonce_out) {
     Ctx* ctx = reinterpret_cast<Ctx*>(c);
@@ -321,6 +344,8 @@ extern "C" int sg_grind(sg_ctx* c, void* stream, const uint64_t inner_lanes[4], 
     const uint64_t limit = grinding_factor == 64 ? 1ULL : (1ULL << (64 - grinding_factor));
     const uint64_t expected = grinding_factor >= 63 ? ~0ULL : (1ULL << grinding_factor);
     uint64_t count = expected > (1ULL << 25) ? (1ULL << 28) : (expected * 8 < (1ULL << 20) ? (1ULL << 20) : expected * 8);
+    unsigned grid = 0;
+    SG_TRY(grind_grid(&grid));
     unsigned long long* d_best = nullptr;
     SG_TRY(dev_alloc(ctx, st, 8, (void**)&d_best));
     int rc = SG_OK;
@@ -331,7 +356,7 @@ extern "C" int sg_grind(sg_ctx* c, void* stream, const uint64_t inner_lanes[4], 
         unsigned long long host = 0;
         cudaError_t e = cudaMemcpyAsync(d_best, &init, 8, cudaMemcpyHostToDevice, st);
         if (e == cudaSuccess) {
-            k_grind<<<148 * 8, 256, 0, st>>>(inner_lanes[0], inner_lanes[1], inner_lanes[2], inner_lanes[3], limit,
+            k_grind<<<grid, 256, 0, st>>>(inner_lanes[0], inner_lanes[1], inner_lanes[2], inner_lanes[3], limit,
                                                base, count, d_best);
             rc = check_launch(ctx, "k_grind");
             if (rc != SG_OK) break;
