@@ -168,17 +168,20 @@ static int batch_inv_launch(Ctx* ctx, cudaStream_t st, Load load, uint64_t total
 //   points[i] * col_c(row i*stride) * inv_denoms[k][i]
 #define BARY_MAX_K 8
 // Block = RL row lanes x CT columns (thread t: lane t / CT, column t % CT of
-// the block's column tile). Lane r walks rows i0+r, i0+r+RL, ... of the
-// chunk, so narrow tables still fill the block and each warp reads whole
-// row segments. The lanes' sums meet in shared memory; one partial per
-// (chunk, k, column) goes to k_bary_combine.
+// the block's column tile). The chunk's rows go in batches of RB: the block
+// first forms the row weights W[r][k] = points[i] * inv_denoms[k][i] of the
+// batch in shared memory (coalesced loads, one product per row instead of one
+// per cell), then lane r walks rows r, r+RL, ... of the batch, so narrow tables
+// still fill the block and each warp reads whole row segments. The lanes'
+// sums meet in the same shared memory; one partial per (chunk, k, column)
+// goes to k_bary_combine.
 template <bool EXT3, int K>
 __global__ void __launch_bounds__(512) k_bary(const uint64_t* __restrict__ data, uint64_t row_u64, uint64_t stride,
-                                              uint64_t cols, uint32_t CT, uint32_t RL,
+                                              uint64_t cols, uint32_t CT, uint32_t RL, uint32_t RB,
                                               const uint64_t* __restrict__ points,
                                               const uint64_t* __restrict__ invd, uint64_t n, uint64_t chunk_len,
                                               uint64_t* __restrict__ partial) {
-    extern __shared__ uint64_t bary_sm[];  // [RL][CT][K] ext3
+    extern __shared__ uint64_t bary_sm[];  // batch weights [RB][K] ext3, then lane sums [RL][CT][K] ext3
     const uint32_t lane = threadIdx.x / CT, cl = threadIdx.x % CT;
     const uint64_t c = (uint64_t)blockIdx.x * CT + cl;
     const bool active = lane < RL && c < cols;
@@ -188,25 +191,30 @@ __global__ void __launch_bounds__(512) k_bary(const uint64_t* __restrict__ data,
 #pragma unroll
     for (int k = 0; k < K; ++k) wa[k] = gl::wzero3();
     const uint64_t i0 = blockIdx.y * chunk_len, i1 = min(n, i0 + chunk_len);
-    if (active) {
+    for (uint64_t b0 = i0; b0 < i1; b0 += RB) {
+        const uint32_t nb = (uint32_t)min((uint64_t)RB, i1 - b0);
+        __syncthreads();  // the previous batch's weights are consumed
+        for (uint32_t e = threadIdx.x; e < nb * K; e += blockDim.x) {
+            const uint32_t r = e / K, k = e % K;
+            const uint64_t i = b0 + r;
+            const uint64_t* dp = invd + 3 * (k * n + i);
+            st3(bary_sm + 3 * e, gl::mulb3(fe3{__ldg(dp), __ldg(dp + 1), __ldg(dp + 2)}, __ldg(points + i)));
+        }
+        __syncthreads();
+        if (active) {
 #pragma unroll 4
-        for (uint64_t i = i0 + lane; i < i1; i += RL) {
-            const uint64_t* row = data + i * stride * row_u64;
-            const uint64_t pt = __ldg(points + i);
-            if (EXT3) {
-                const fe3 pe = gl::mulb3(fe3{__ldg(row + 3 * c), __ldg(row + 3 * c + 1), __ldg(row + 3 * c + 2)}, pt);
-                const uint64_t p1_2 = gl::add(pe.c1, pe.c1), p2_2 = gl::add(pe.c2, pe.c2);
+            for (uint32_t r = lane; r < nb; r += RL) {
+                const uint64_t* row = data + (b0 + r) * stride * row_u64;
+                const uint64_t* wr = bary_sm + 3 * ((uint64_t)r * K);
+                if (EXT3) {
+                    const fe3 t{__ldg(row + 3 * c), __ldg(row + 3 * c + 1), __ldg(row + 3 * c + 2)};
+                    const uint64_t t1_2 = gl::add(t.c1, t.c1), t2_2 = gl::add(t.c2, t.c2);
 #pragma unroll
-                for (int k = 0; k < K; ++k) {
-                    const uint64_t* dp = invd + 3 * (k * n + i);
-                    gl::wmac3(wa[k], fe3{__ldg(dp), __ldg(dp + 1), __ldg(dp + 2)}, pe, p1_2, p2_2);
-                }
-            } else {
-                const uint64_t pe = gl::mul(__ldg(row + c), pt);
+                    for (int k = 0; k < K; ++k) gl::wmac3(wa[k], ld3(wr + 3 * k), t, t1_2, t2_2);
+                } else {
+                    const uint64_t t = __ldg(row + c);
 #pragma unroll
-                for (int k = 0; k < K; ++k) {
-                    const uint64_t* dp = invd + 3 * (k * n + i);
-                    gl::wmacb3(wa[k], fe3{__ldg(dp), __ldg(dp + 1), __ldg(dp + 2)}, pe);
+                    for (int k = 0; k < K; ++k) gl::wmacb3(wa[k], ld3(wr + 3 * k), t);
                 }
             }
         }
@@ -214,6 +222,7 @@ __global__ void __launch_bounds__(512) k_bary(const uint64_t* __restrict__ data,
     fe3 acc[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) acc[k] = gl::wreduce3(wa[k]);
+    __syncthreads();  // the weights are consumed; the buffer takes the lane sums
     if (lane < RL) {
 #pragma unroll
         for (int k = 0; k < K; ++k) st3(bary_sm + 3 * (((uint64_t)lane * CT + cl) * K + k), acc[k]);
@@ -229,8 +238,8 @@ __global__ void __launch_bounds__(512) k_bary(const uint64_t* __restrict__ data,
     }
 }
 
-typedef void (*bary_fn)(const uint64_t*, uint64_t, uint64_t, uint64_t, uint32_t, uint32_t, const uint64_t*,
-                        const uint64_t*, uint64_t, uint64_t, uint64_t*);
+typedef void (*bary_fn)(const uint64_t*, uint64_t, uint64_t, uint64_t, uint32_t, uint32_t, uint32_t,
+                        const uint64_t*, const uint64_t*, uint64_t, uint64_t, uint64_t*);
 template <bool EXT3>
 static bary_fn bary_kernel(uint32_t K) {
     switch (K) {
@@ -582,7 +591,9 @@ int sg_barycentric_sums(sg_ctx* c, void* stream, const uint64_t* d_data, uint64_
     const uint32_t CT = (uint32_t)((cols + ctiles - 1) / ctiles);
     const uint32_t RL = CT >= 256 ? 1u : 256u / CT;
     const uint32_t threads = (RL * CT + 31) / 32 * 32;
-    const size_t smem = 24ull * k * RL * CT;
+    // weight batches of at least 64 rows, a whole number of row lanes
+    const uint32_t RB = RL >= 64 ? RL : (64 + RL - 1) / RL * RL;
+    const size_t smem = 24ull * k * (RB > RL * CT ? RB : RL * CT);
     // About four blocks of work per SM in total, each chunk at least RL rows.
     uint64_t chunks = (148 * 4 + ctiles - 1) / ctiles;
     const uint64_t max_chunks = (n + RL - 1) / RL;
@@ -595,7 +606,7 @@ int sg_barycentric_sums(sg_ctx* c, void* stream, const uint64_t* d_data, uint64_
     dim3 grid((unsigned)ctiles, (unsigned)chunks);
     bary_fn fn = ext3 ? bary_kernel<true>(k) : bary_kernel<false>(k);
     if (smem > 48 * 1024) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    fn<<<grid, threads, smem, st>>>(d_data, row_u64, row_stride, cols, CT, RL, d_points, d_inv_denoms, n, chunk_len,
+    fn<<<grid, threads, smem, st>>>(d_data, row_u64, row_stride, cols, CT, RL, RB, d_points, d_inv_denoms, n, chunk_len,
                                     part);
     int rc = check_launch(ctx, "k_bary");
     if (rc == SG_OK) {
