@@ -278,7 +278,9 @@ __global__ void k_bary_combine(const uint64_t* partial, uint64_t chunks, uint64_
 // the host: the same field value as summing g (t - t_ood) term by term.
 // The coefficient loads are uniform across the warp (broadcast); each
 // thread streams its own row, whose 32-byte sectors stay in L1 across the
-// four consecutive column reads that share them.
+// consecutive column reads that share them. The row is read two columns per
+// 16-byte load where it is 16-byte aligned: a warp's load touches 32 rows'
+// sectors either way, so pairs halve the L1 lookups, which bound this kernel.
 #define DEEP_MAX_K 8
 template <int K>
 __global__ void __launch_bounds__(128) k_deep(const uint64_t* __restrict__ main, uint64_t m,
@@ -295,13 +297,20 @@ __global__ void __launch_bounds__(128) k_deep(const uint64_t* __restrict__ main,
 #pragma unroll
     for (int k = 0; k < K; ++k) acc[k] = gl::wzero3();
     const uint64_t* mrow = main + i * m;
-    for (uint64_t j = 0; j < m; ++j) {
-        const uint64_t t = __ldg(mrow + j);
+    auto col = [&](uint64_t j, uint64_t t) {
         const uint64_t* g = gam_tr + 3 * j * K;
 #pragma unroll
         for (int k = 0; k < K; ++k)
             gl::wmacb3(acc[k], fe3{__ldg(g + 3 * k), __ldg(g + 3 * k + 1), __ldg(g + 3 * k + 2)}, t);
+    };
+    uint64_t j = 0;
+    if (m > 0 && ((uintptr_t)mrow & 15)) col(j++, __ldg(mrow));
+    for (; j + 1 < m; j += 2) {
+        const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(mrow + j));
+        col(j, v.x);
+        col(j + 1, v.y);
     }
+    if (j < m) col(j, __ldg(mrow + j));
     const uint64_t* arow = aux + i * A * 3;
     for (uint64_t j = 0; j < A; ++j) {
         const fe3 t{__ldg(arow + 3 * j), __ldg(arow + 3 * j + 1), __ldg(arow + 3 * j + 2)};

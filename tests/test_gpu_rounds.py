@@ -57,7 +57,8 @@ def test_barycentric_sums_match_oracle(be, rows, ru, cols, ext3, stride, k):
 
 
 @pytest.mark.parametrize("rows,m,a,p,k", [(32, 3, 1, 1, 1), (256, 17, 2, 2, 2), (1024, 64, 5, 2, 3),
-                                          (4096, 300, 0, 2, 2), (2048, 8, 40, 1, 8)])
+                                          (4096, 300, 0, 2, 2), (2048, 8, 40, 1, 8), (64, 1, 1, 1, 2),
+                                          (128, 2, 1, 2, 2)])
 def test_deep_matches_oracle(be, rows, m, a, p, k):
     rng = np.random.default_rng(rows + m + a)
     main = rf(rng, (rows, m))
