@@ -231,7 +231,7 @@ def run_proof_distributed(a, rank, world, local):
     dist.destroy_process_group()
 
 
-def proof_summary(a, steps=3, warmup=2):
+def proof_summary(a, steps=5, warmup=2):
     """The multi-table proof workload, plain vs scheduled, as a compact dict
     for the default bench line (N = 1)."""
     import types
@@ -539,15 +539,20 @@ def main():
             "e2e": {"value": world * n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": n * m * 8 + n * 8,
                     "d2h_bytes_per_step": 32, "ms_per_step": e2e_s * 1e3,
                     "path": "sg_lde_commit(host pinned trace) -> root"}}
-    if not a.no_cpu_baseline and world == 1:
-        line["cpu_baseline"] = cpu_baseline(a, rpl, le)
     if world == 1 and not a.no_proof_summary:
         # the batched-vs-plain proof workload beside the primitive (not timed
-        # into `value`); a failure here is reported, never fatal to the line
+        # into `value`); a failure here is reported, never fatal to the line.
+        # It runs before the CPU baseline, whose OpenMP threads would compete
+        # with the scheduled form's host-side table drivers.
+        import torch
+        del d_trace, d_out, d_nodes
+        torch.cuda.empty_cache()
         try:
             line["proof_workload"] = proof_summary(a)
         except Exception as e:  # noqa: BLE001
             line["proof_workload"] = {"error": f"{type(e).__name__}: {e}"}
+    if not a.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline(a, rpl, le)
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
