@@ -44,9 +44,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-proof-summary", action="store_true",
                     help="skip the multi-table proof summary the default line carries at N = 1")
-    ap.add_argument("--workload", default="commit", choices=["commit", "proof", "serve"],
+    ap.add_argument("--workload", default="commit", choices=["commit", "proof", "serve", "rounds"],
                     help="commit: LDE + Merkle commit of one trace (default); proof: multi-table proof, plain vs "
-                         "scheduled; serve: Poisson stream of proof jobs, concurrent admission vs one at a time")
+                         "scheduled; serve: Poisson stream of proof jobs, concurrent admission vs one at a time; "
+                         "rounds: the round-2..4 kernels of one large table, one by one")
     ap.add_argument("--rates", default="2,5,10,20,50,100", help="serve: arrival rates (jobs/s)")
     ap.add_argument("--jobs", type=int, default=40, help="serve: jobs per rate")
     ap.add_argument("--job-max-log-n", type=int, default=18, help="serve: largest job height (log2 cycles)")
@@ -371,6 +372,66 @@ def run_serve(a):
     print(json.dumps(line), flush=True)
 
 
+def run_rounds(a):
+    """The round-2..4 kernels of one large table, each timed alone with CUDA
+    events (median of `steps` after `warmup`): the DEEP denominators'
+    batch inversion (2^22 points x 3 opening points, x - z), the DEEP
+    composition (2^20 LDE rows: 256 base, 3 aux and 2 part ext3 columns, 2
+    points) and the OOD barycentric sums (2^20 points read at stride 2 from a
+    2^21-row LDE, 256 and 9 base columns, 2 points). Inputs are seeded
+    uniform words; the sums' values are not checked here (the tests do)."""
+    import ctypes as C
+    import torch
+    from lambda_vm_b200 import native
+    from lambda_vm_b200.device import backend
+    L = native.lib()
+    be = backend(0)
+    s = torch.cuda.current_stream()
+    sp = C.c_void_p(s.cuda_stream)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(11)
+    R = lambda k: torch.randint(0, 2**62, (k,), dtype=torch.int64, device="cuda", generator=g)
+    rng = np.random.default_rng(11)
+    H = lambda k: (C.c_uint64 * k)(*[int(x) for x in rng.integers(0, 2**62, size=k, dtype=np.uint64)])
+
+    def timed(fn):
+        ts = []
+        for it in range(a.warmup + a.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            fn()
+            e1.record(s)
+            torch.cuda.synchronize()
+            if it >= a.warmup:
+                ts.append(e0.elapsed_time(e1))
+        return round(statistics.median(ts), 3)
+
+    out = {}
+    n, k = 1 << 22, 3
+    x, z, inv = R(n), H(3 * k), torch.empty(3 * n * k, dtype=torch.int64, device="cuda")
+    out["batch_inverse_2^22x3_ms"] = timed(lambda: native.check(
+        L.sg_inv_denoms_ext3(be.h, sp, x.data_ptr(), n, z, k, 1, inv.data_ptr(), None)))
+    del x, inv
+    rows, m, A, P, K = 1 << 20, 256, 3, 2, 2
+    main, aux, parts = R(rows * m), R(rows * 3 * A), R(rows * 3 * P)
+    inv_h, inv_t, dout = R(3 * rows), R(3 * K * rows), torch.empty(3 * rows, dtype=torch.int64, device="cuda")
+    h_ood, t_ood, gh, gt = H(3 * P), H(3 * (m + A) * K), H(3 * P), H(3 * (m + A) * K)
+    out["deep_2^20x256_ms"] = timed(lambda: native.check(L.sg_deep_composition(
+        be.h, sp, main.data_ptr(), m, aux.data_ptr(), A, parts.data_ptr(), P, rows, h_ood, t_ood, gh, gt, K,
+        inv_h.data_ptr(), inv_t.data_ptr(), 1, dout.data_ptr())))
+    del main, aux, parts, inv_h, inv_t, dout
+    npts = 1 << 20
+    pts, invd = R(npts), R(3 * K * npts)
+    for cols in (256, 9):
+        data, bout = R(2 * npts * cols), torch.empty(3 * K * cols, dtype=torch.int64, device="cuda")
+        out[f"barycentric_2^20x{cols}_ms"] = timed(lambda: native.check(L.sg_barycentric_sums(
+            be.h, sp, data.data_ptr(), cols, 2, 0, cols, pts.data_ptr(), invd.data_ptr(), npts, K, bout.data_ptr())))
+        del data, bout
+    print(json.dumps({"metric": "round-2..4 kernel times (one large table)", "unit": "ms", "n_gpus": 1,
+                      "steps": a.steps, "warmup": a.warmup, "higher_is_better": False,
+                      "data": "synthetic (seeded uniform words)", "kernels": out}), flush=True)
+
+
 def main():
     a = parse()
     if a.workload == "proof" and a.impl == "ours":
@@ -382,6 +443,9 @@ def main():
         return
     if a.workload == "serve" and a.impl == "ours":
         run_serve(a)
+        return
+    if a.workload == "rounds" and a.impl == "ours":
+        run_rounds(a)
         return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
