@@ -33,7 +33,9 @@ def test_batch_inverse_reports_zero(be):
         mc.batch_inverse_ext3(a, be)
 
 
-@pytest.mark.parametrize("n,k,sign", [(1, 1, 0), (64, 2, 0), (1000, 3, 1), (4096, 8, 1), (50000, 2, 0)])
+@pytest.mark.parametrize("n,k,sign", [(1, 1, 0), (64, 2, 0), (1000, 3, 1), (4096, 8, 1), (50000, 2, 0),
+                                      # a thread's chunk of 12 denominators wraps across several points
+                                      (1, 8, 1), (5, 7, 0), (11, 3, 1)])
 def test_inv_denoms_match_oracle(be, n, k, sign):
     rng = np.random.default_rng(n + k)
     x = rf(rng, (n,))
@@ -44,7 +46,9 @@ def test_inv_denoms_match_oracle(be, n, k, sign):
 
 @pytest.mark.parametrize("rows,ru,cols,ext3,stride,k", [
     (64, 5, 5, False, 1, 1), (256, 7, 7, False, 2, 3), (1024, 12, 4, True, 4, 2), (4096, 300, 300, False, 2, 8),
-    (2048, 30, 10, True, 2, 5), (16384, 16, 16, False, 4, 2)])
+    (2048, 30, 10, True, 2, 5), (16384, 16, 16, False, 4, 2),
+    # point counts that end inside a weight batch and inside a prefetch group
+    (3000, 9, 9, False, 3, 2), (96, 9, 3, True, 1, 8), (1000, 600, 600, False, 1, 1)])
 def test_barycentric_sums_match_oracle(be, rows, ru, cols, ext3, stride, k):
     rng = np.random.default_rng(rows + cols)
     data = rf(rng, (rows, ru))
