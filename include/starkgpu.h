@@ -126,11 +126,13 @@ SG_API int sg_ctx_dft_tuning(sg_ctx* ctx, void* stream, uint32_t log_len, uint32
  *      no context object). Same arguments and result as sg_coset_lde, but no
  *      context and no allocation: its scratch is a static device array of
  *      SG_STATIC_SCRATCH_BYTES per GPU, held until the process exits. Requires
- *      (blowup*n + 2*n*m) * 8 <= SG_STATIC_SCRATCH_BYTES, else SG_ERR_INVALID.
- *      The first call on a device (with that device current) looks up the
- *      array's device address; make it before any stream capture. Calls share
- *      the array, so calls that overlap on the GPU race and must be serialized
- *      by the caller. ---- */
+ *      (max(blowup*n, 3) + 2*n*m) * 8 <= SG_STATIC_SCRATCH_BYTES, else
+ *      SG_ERR_INVALID. It runs on the calling thread's current device; each
+ *      GPU has its own array, and the first call on a device (with that device
+ *      current) looks up that array's device address and sets the DFT kernels'
+ *      shared-memory limit there, so make it before any stream capture. Calls
+ *      share the array, so calls that overlap on the GPU race and must be
+ *      serialized by the caller. ---- */
 #define SG_STATIC_SCRATCH_BYTES (32ull << 20)
 SG_API int sg_coset_lde_static(void* stream, const uint64_t* d_trace, uint64_t n, uint64_t m, uint32_t blowup,
                                const uint64_t* d_weights, uint64_t* d_out);

@@ -132,6 +132,28 @@ int dev_free(Ctx* ctx, cudaStream_t st, void* p, uint64_t bytes) {
     return SG_OK;
 }
 
+int kernel_info(const void* fn, size_t smem, int threads, KernelInfo* out) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, KernelInfo> cache;
+    int dev = 0;
+    SG_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> g(mu);
+    auto it = cache.find({fn, dev});
+    if (it != cache.end()) {
+        *out = it->second;
+        return SG_OK;
+    }
+    KernelInfo k;
+    if (smem > 48 * 1024) SG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    SG_CUDA(cudaDeviceGetAttribute(&k.sms, cudaDevAttrMultiProcessorCount, dev));
+    SG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k.blocks_per_sm, fn, threads, smem));
+    if (k.sms < 1) k.sms = 1;
+    if (k.blocks_per_sm < 1) k.blocks_per_sm = 1;
+    cache[{fn, dev}] = k;
+    *out = k;
+    return SG_OK;
+}
+
 }  // namespace sg
 
 using namespace sg;
@@ -183,6 +205,7 @@ int sg_ctx_create(int device, uint64_t budget, sg_ctx** out) {
 void sg_ctx_destroy(sg_ctx* c) {
     Ctx* ctx = C(c);
     if (!ctx) return;
+    enter(ctx);  // best effort: teardown continues either way
     cudaDeviceSynchronize();
     trim_cache(ctx);
     for (auto& kv : ctx->live_cap) cudaFree(kv.first);
@@ -193,6 +216,7 @@ void sg_ctx_destroy(sg_ctx* c) {
 
 int sg_ctx_memory(sg_ctx* c, uint64_t* in_use, uint64_t* peak) {
     SG_CHECK_ARG(c, "null context");
+    SG_ENTER(ctx_of(c));
     if (in_use) *in_use = C(c)->in_use.load();
     if (peak) *peak = C(c)->peak.load();
     return SG_OK;
@@ -204,22 +228,26 @@ uint64_t sg_ctx_budget(sg_ctx* c) { return c ? C(c)->budget : 0; }
 
 int sg_ctx_fail_alloc_after(sg_ctx* c, int64_t n) {
     SG_CHECK_ARG(c && n >= 0, "bad argument");
+    SG_ENTER(ctx_of(c));
     C(c)->fail_alloc_after.store(n == 0 ? -1 : n);
     return SG_OK;
 }
 
 int sg_dev_alloc(sg_ctx* c, void* stream, uint64_t bytes, void** d_out) {
     SG_CHECK_ARG(c && d_out, "null argument");
+    SG_ENTER(ctx_of(c));
     return dev_alloc(C(c), (cudaStream_t)stream, bytes, d_out);
 }
 
 int sg_dev_free(sg_ctx* c, void* stream, void* p, uint64_t bytes) {
     SG_CHECK_ARG(c, "null context");
+    SG_ENTER(ctx_of(c));
     return dev_free(C(c), (cudaStream_t)stream, p, bytes);
 }
 
 int sg_memcpy_h2d(sg_ctx* c, void* stream, void* dst, const void* src, uint64_t bytes) {
     SG_CHECK_ARG(c, "null context");
+    SG_ENTER(ctx_of(c));
     if (!bytes) return SG_OK;
     SG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, (cudaStream_t)stream));
     return SG_OK;
@@ -227,6 +255,7 @@ int sg_memcpy_h2d(sg_ctx* c, void* stream, void* dst, const void* src, uint64_t 
 
 int sg_memcpy_d2h(sg_ctx* c, void* stream, void* dst, const void* src, uint64_t bytes) {
     SG_CHECK_ARG(c, "null context");
+    SG_ENTER(ctx_of(c));
     if (!bytes) return SG_OK;
     SG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, (cudaStream_t)stream));
     return SG_OK;
@@ -234,12 +263,14 @@ int sg_memcpy_d2h(sg_ctx* c, void* stream, void* dst, const void* src, uint64_t 
 
 int sg_stream_sync(sg_ctx* c, void* stream) {
     SG_CHECK_ARG(c, "null context");
+    SG_ENTER(ctx_of(c));
     SG_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
     return SG_OK;
 }
 
 int sg_stream_create(sg_ctx* c, void** out) {
     SG_CHECK_ARG(c && out, "null argument");
+    SG_ENTER(ctx_of(c));
     cudaStream_t st;
     SG_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     *out = (void*)st;
@@ -248,6 +279,7 @@ int sg_stream_create(sg_ctx* c, void** out) {
 
 int sg_stream_destroy(sg_ctx* c, void* stream) {
     SG_CHECK_ARG(c, "null context");
+    SG_ENTER(ctx_of(c));
     if (stream) SG_CUDA(cudaStreamDestroy((cudaStream_t)stream));
     return SG_OK;
 }
@@ -265,17 +297,20 @@ int sg_host_free(void* p) {
 
 int sg_ntt_forward(sg_ctx* c, void* stream, uint64_t* d, uint64_t n, uint64_t m) {
     SG_CHECK_ARG(c, "null context");
+    SG_ENTER(ctx_of(c));
     return ntt_rows(C(c), (cudaStream_t)stream, d, n, m, 0, 0);
 }
 
 int sg_ntt_inverse(sg_ctx* c, void* stream, uint64_t* d, uint64_t n, uint64_t m) {
     SG_CHECK_ARG(c, "null context");
+    SG_ENTER(ctx_of(c));
     return ntt_rows(C(c), (cudaStream_t)stream, d, n, m, 1, 1);
 }
 
 int sg_coset_lde(sg_ctx* c, void* stream, const uint64_t* d_trace, uint64_t n, uint64_t m, uint32_t blowup,
                  const uint64_t* d_weights, uint64_t* d_out) {
     SG_CHECK_ARG(c, "null context");
+    SG_ENTER(ctx_of(c));
     SG_CHECK_ARG(blowup >= 1, "blowup must be >= 1");
     if (n == 0 || m == 0) return SG_OK;
     SG_CHECK_ARG(d_trace && d_weights && d_out, "null buffer");
@@ -298,6 +333,7 @@ static int resolve_layout(const sg_leaf_layout* lay, uint64_t row_u64, uint32_t*
 int sg_keccak_leaves(sg_ctx* c, void* stream, const uint64_t* d_data, uint64_t num_rows, uint64_t row_u64,
                      const sg_leaf_layout* layout, uint8_t* d_out) {
     SG_CHECK_ARG(c, "null context");
+    SG_ENTER(ctx_of(c));
     if (num_rows == 0) return SG_OK;
     uint32_t R;
     int le;
@@ -315,6 +351,7 @@ uint64_t sg_merkle_leaves_len(uint64_t num_leaves) {
 int sg_merkle_build(sg_ctx* c, void* stream, const uint8_t* d_leaves, uint64_t num_leaves, uint8_t* d_nodes,
                     uint8_t root_out[32]) {
     SG_CHECK_ARG(c, "null context");
+    SG_ENTER(ctx_of(c));
     SG_CHECK_ARG(num_leaves > 0, "empty leaf set");
     cudaStream_t st = (cudaStream_t)stream;
     const uint64_t L = sg_merkle_leaves_len(num_leaves);
@@ -494,6 +531,7 @@ int sg_lde_commit(sg_ctx* c, void* stream, const uint64_t* trace, int trace_on_d
                   uint32_t blowup, const uint64_t* weights, const sg_leaf_layout* layout, uint64_t* host_lde_out,
                   sg_lde** out, uint8_t root_out[32]) {
     SG_CHECK_ARG(c && out, "null argument");
+    SG_ENTER(ctx_of(c));
     *out = nullptr;
     Ctx* ctx = C(c);
     cudaStream_t st = (cudaStream_t)stream;
@@ -516,6 +554,7 @@ int sg_lde_commit_split(sg_ctx* c, void* stream, const uint64_t* trace, int trac
                         uint64_t* host_lde_out, sg_lde** out, uint8_t root_out[32], uint8_t* d_pre_nodes,
                         uint8_t root_pre_out[32]) {
     SG_CHECK_ARG(c && out, "null argument");
+    SG_ENTER(ctx_of(c));
     *out = nullptr;
     SG_CHECK_ARG(split_col > 0 && split_col < row_u64, "split inside the row");
     SG_CHECK_ARG(!build_pre || d_pre_nodes, "the precomputed tree needs a node buffer");
@@ -552,6 +591,7 @@ int sg_lde_commit_split(sg_ctx* c, void* stream, const uint64_t* trace, int trac
 int sg_batch_commit(sg_ctx* c, void* stream, const sg_table_desc* tables, uint32_t count, uint32_t concurrency,
                     sg_lde** out_ldes, uint8_t* roots_out) {
     SG_CHECK_ARG(c && (count == 0 || (tables && out_ldes)), "null argument");
+    SG_ENTER(ctx_of(c));
     for (uint32_t i = 0; i < count; ++i) out_ldes[i] = nullptr;
     if (count == 0) return SG_OK;
     Ctx* ctx = C(c);
@@ -639,6 +679,7 @@ int sg_batch_commit(sg_ctx* c, void* stream, const sg_table_desc* tables, uint32
 void sg_lde_free_async(sg_ctx* c, void* stream, sg_lde* h) {
     if (!c || !h) return;
     Ctx* ctx = C(c);
+    enter(ctx);  // best effort: the handle is released either way
     cudaStream_t st = (cudaStream_t)stream;
     dev_free(ctx, st, h->d_lde, h->lde_rows * h->row_u64 * 8);
     dev_free(ctx, st, h->d_nodes, (2 * h->leaves_len - 1) * 32);
@@ -659,6 +700,7 @@ int sg_lde_get_info(const sg_lde* h, sg_lde_info* info) {
 void sg_lde_free(sg_ctx* c, sg_lde* h) {
     if (!c || !h) return;
     Ctx* ctx = C(c);
+    enter(ctx);  // best effort: the handle is released either way
     // Freed on the legacy stream: ordered after all prior work that used the handle.
     cudaDeviceSynchronize();
     dev_free(ctx, nullptr, h->d_lde, h->lde_rows * h->row_u64 * 8);

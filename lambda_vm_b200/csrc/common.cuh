@@ -114,6 +114,35 @@ inline int log2_exact(uint64_t n) {
     return l;
 }
 
+// Make the context's GPU current on the calling thread. CUDA's current device
+// is per host thread and a thread that never chose one runs on device 0, so
+// every entry point that takes a context calls this before any CUDA call:
+// worker threads of a table scheduler or a proof server then launch on the
+// context's GPU whichever thread they are. Cheap when it is already current.
+inline Ctx* ctx_of(sg_ctx* c) { return reinterpret_cast<Ctx*>(c); }
+inline int enter(Ctx* ctx) {
+    int cur = -1;
+    if (cudaGetDevice(&cur) == cudaSuccess && cur == ctx->device) return SG_OK;
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) {
+        set_error(std::string("cudaSetDevice(") + std::to_string(ctx->device) + "): " + cudaGetErrorString(e));
+        return SG_ERR_CUDA;
+    }
+    return SG_OK;
+}
+#define SG_ENTER(ctx) SG_TRY(::sg::enter(ctx))
+
+// Launch facts of one kernel on the current device: its SM count and how many
+// CTAs of `threads` threads and `smem` dynamic shared memory bytes fit on one
+// SM. The first query per (kernel, device) also raises the kernel's dynamic
+// shared-memory limit when smem exceeds 48 KB; that attribute is per device,
+// so each GPU of a process gets it on its first launch there.
+struct KernelInfo {
+    int sms = 0;
+    int blocks_per_sm = 0;
+};
+int kernel_info(const void* fn, size_t smem, int threads, KernelInfo* out);
+
 inline int check_launch(Ctx* ctx, const char* what) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {

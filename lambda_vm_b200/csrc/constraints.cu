@@ -289,6 +289,7 @@ int sg_eval_constraints(sg_ctx* c, void* stream, const sg_device_program* prog, 
                         uint64_t next_step, const sg_composition* comp, uint64_t* d_out) {
     Ctx* ctx = reinterpret_cast<Ctx*>(c);
     SG_CHECK_ARG(ctx && prog && table_offset, "null argument");
+    SG_ENTER(ctx);
     SG_CHECK_ARG(rows >= 1 && next_step < rows, "bad row count / frame step");
     cudaStream_t st = (cudaStream_t)stream;
     const uint32_t nn = prog->num_nodes, nr = prog->num_roots;
@@ -410,6 +411,7 @@ int sg_decompose_d2(sg_ctx* c, void* stream, const uint64_t* d_h, uint64_t lde_r
                     uint64_t* d_out) {
     Ctx* ctx = reinterpret_cast<Ctx*>(c);
     SG_CHECK_ARG(ctx, "null context");
+    SG_ENTER(ctx);
     SG_CHECK_ARG(lde_rows % 2 == 0, "even LDE size required");
     const uint64_t n = lde_rows / 2;
     if (n == 0) return SG_OK;

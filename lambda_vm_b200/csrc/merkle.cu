@@ -303,6 +303,7 @@ extern "C" int sg_merkle_gather_paths(sg_ctx* c, void* stream, const uint8_t* d_
                                       const uint32_t* d_positions, uint32_t num_queries, uint8_t* d_out) {
     Ctx* ctx = reinterpret_cast<Ctx*>(c);
     SG_CHECK_ARG(ctx, "null context");
+    SG_ENTER(ctx);
     const int lg = log2_exact(leaves_len);
     SG_CHECK_ARG(lg >= 0, "leaves_len must be a power of two");
     if (num_queries == 0 || lg == 0) return SG_OK;
@@ -317,21 +318,9 @@ extern "C" int sg_merkle_gather_paths(sg_ctx* c, void* stream, const uint8_t* d_
 // every smaller nonce is checked; CTAs beyond the resident ones would start
 // late on the low nonces of each sweep and hold the whole search open.
 static int grind_grid(unsigned* grid) {
-    static std::once_flag once;
-    static unsigned g = 0;
-    static cudaError_t err = cudaSuccess;
-    std::call_once(once, [] {
-        int dev = 0, sms = 0, per_sm = 0;
-        err = cudaGetDevice(&dev);
-        if (err == cudaSuccess) err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (err == cudaSuccess) err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_grind, 256, 0);
-        g = (unsigned)(sms > 0 ? sms : 1) * (unsigned)(per_sm > 0 ? per_sm : 1);
-    });
-    if (err != cudaSuccess) {
-        set_error(std::string("grind: occupancy query: ") + cudaGetErrorString(err));
-        return SG_ERR_CUDA;
-    }
-    *grid = g;
+    KernelInfo ki;
+    SG_TRY(kernel_info((const void*)k_grind, 0, 256, &ki));
+    *grid = (unsigned)ki.sms * (unsigned)ki.blocks_per_sm;
     return SG_OK;
 }
 
@@ -339,6 +328,7 @@ extern "C" int sg_grind(sg_ctx* c, void* stream, const uint64_t inner_lanes[4], 
                         uint64_t* nonce_out) {
     Ctx* ctx = reinterpret_cast<Ctx*>(c);
     SG_CHECK_ARG(ctx && inner_lanes && nonce_out, "null argument");
+    SG_ENTER(ctx);
     SG_CHECK_ARG(grinding_factor >= 1 && grinding_factor <= 64, "grinding factor must be in 1..=64");
     cudaStream_t st = (cudaStream_t)stream;
     const uint64_t limit = grinding_factor == 64 ? 1ULL : (1ULL << (64 - grinding_factor));

@@ -358,21 +358,9 @@ __global__ void __launch_bounds__(Plan<LOGL, C_>::T, Plan<LOGL, C_>::MINB)
 template <int LOGL, int C_, bool INV>
 static int launch_dft_dir(Ctx* ctx, cudaStream_t st, const PassArgs& a, uint64_t ntiles) {
     using PL = Plan<LOGL, C_>;
-    static std::once_flag once;
-    static int blocks_per_sm = 0, num_sms = 0;
-    static cudaError_t init_err = cudaSuccess;
-    std::call_once(once, [] {
-        int dev = 0;
-        init_err = cudaFuncSetAttribute(k_dft<LOGL, C_, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)PL::SMEM);
-        if (init_err == cudaSuccess) init_err = cudaGetDevice(&dev);
-        if (init_err == cudaSuccess) init_err = cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
-        if (init_err == cudaSuccess)
-            init_err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_dft<LOGL, C_, INV>, PL::T,
-                                                                     PL::SMEM);
-        if (blocks_per_sm < 1) blocks_per_sm = 1;
-    });
-    SG_CUDA(init_err);
+    KernelInfo ki;
+    SG_TRY(kernel_info((const void*)k_dft<LOGL, C_, INV>, PL::SMEM, PL::T, &ki));
+    const int blocks_per_sm = ki.blocks_per_sm, num_sms = ki.sms;
     const uint64_t ctiles = (a.m + PL::C - 1) / PL::C;
     if (ctiles > 0xffffffffULL) {
         set_error("too many columns");
@@ -836,13 +824,15 @@ extern "C" int sg_coset_lde_static(void* stream, const uint64_t* d_trace, uint64
     const int logN = logn + logB;
     SG_CHECK_ARG(logN <= 32 && logn <= 24, "LDE size out of range");
     const uint64_t N = 1ULL << logN;
-    // u64 words needed: omega table (N) + coefficients + four-step intermediate
-    // (n x m each). Bounded by division, so no m wraps N + 2*n*m into range.
+    // u64 words needed: the two-level root tables (tw_words(logN) <= max(N, 3))
+    // + coefficients + four-step intermediate (n x m each). Bounded by
+    // division, so no m wraps tw_region + 2*n*m into range.
+    const uint64_t tw_region = N > 3 ? N : 3;
     const uint64_t cap = SG_STATIC_SCRATCH_BYTES / sizeof(uint64_t);
-    if (N > cap || m > (cap - N) / (2 * n)) {
+    if (tw_region > cap || m > (cap - tw_region) / (2 * n)) {
         set_error("sg_coset_lde_static: n=" + std::to_string(n) + " m=" + std::to_string(m) +
                   " blowup=" + std::to_string(blowup) +
-                  " needs (blowup*n + 2*n*m) * 8 bytes of scratch, more than the static scratch holds (" +
+                  " needs (max(blowup*n, 3) + 2*n*m) * 8 bytes of scratch, more than the static scratch holds (" +
                   std::to_string((unsigned long long)SG_STATIC_SCRATCH_BYTES) + " bytes); use sg_coset_lde");
         return SG_ERR_INVALID;
     }
@@ -851,11 +841,6 @@ extern "C" int sg_coset_lde_static(void* stream, const uint64_t* d_trace, uint64
     cudaStream_t st = (cudaStream_t)stream;
     Ctx* ctx = &g_static_ctx;
     // Scratch layout: [root tables | coefficients (n x m) | four-step intermediate (n x m)].
-    const uint64_t tw_region = tw_words((uint32_t)logN) > N ? tw_words((uint32_t)logN) : N;
-    if (tw_region + 2 * n * m > SG_STATIC_SCRATCH_BYTES / sizeof(uint64_t)) {
-        set_error("sg_coset_lde_static: request does not fit the static scratch; use sg_coset_lde");
-        return SG_ERR_INVALID;
-    }
     Tw tw;
     SG_TRY(build_tw(ctx, st, (uint32_t)logN, scratch, &tw));
     uint64_t* coef = scratch + tw_region;
@@ -866,6 +851,7 @@ extern "C" int sg_coset_lde_static(void* stream, const uint64_t* d_trace, uint64
 extern "C" int sg_ctx_dft_tiles(sg_ctx* c, uint32_t log_len, uint32_t cols) {
     using namespace sg;
     SG_CHECK_ARG(c && log_len <= 12, "null context or tile length above 2^12");
+    SG_ENTER(ctx_of(c));
     int vs[4];
     const int nv = tile_variants(log_len, vs);
     bool ok = cols == 0;
@@ -881,6 +867,7 @@ extern "C" int sg_ctx_dft_tuning(sg_ctx* c, void* stream, uint32_t log_len, uint
                                  uint32_t* count) {
     using namespace sg;
     SG_CHECK_ARG(c && cols && cost_per_col && count && log_len <= 12, "null argument or tile length above 2^12");
+    SG_ENTER(ctx_of(c));
     Ctx* ctx = reinterpret_cast<Ctx*>(c);
     std::lock_guard<std::mutex> g(ctx->tune_mu);
     Ctx::TileTune& tt = ctx->tiles[log_len];

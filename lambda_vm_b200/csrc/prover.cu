@@ -172,6 +172,7 @@ extern "C" int sg_table_proof_shape(const sg_table_job* j, sg_proof_shape* s) {
 
 extern "C" int sg_prove_table(sg_ctx* c, void* stream, sg_transcript* t, const sg_table_job* j, sg_table_proof* o) {
     SG_CHECK_ARG(c && t && j && o && j->logup && j->program, "null argument");
+    SG_ENTER(ctx_of(c));
     Ctx* ctx = reinterpret_cast<Ctx*>(c);
     cudaStream_t st = (cudaStream_t)stream;
     sg_proof_shape shp;

@@ -578,12 +578,14 @@ extern "C" {
 int sg_batch_inverse_ext3(sg_ctx* c, void* stream, const uint64_t* d_in, uint64_t n, uint64_t* d_out,
                           int* zero_found) {
     SG_CHECK_ARG(c && (n == 0 || (d_in && d_out)), "null argument");
+    SG_ENTER(ctx_of(c));
     return batch_inv_launch(CX(c), (cudaStream_t)stream, LoadPlain{d_in}, n, d_out, zero_found);
 }
 
 int sg_inv_denoms_ext3(sg_ctx* c, void* stream, const uint64_t* d_x, uint64_t n, const uint64_t* z_host, uint32_t k,
                        int x_minus_z, uint64_t* d_out, int* zero_found) {
     SG_CHECK_ARG(c && z_host && (n == 0 || (d_x && d_out)), "null argument");
+    SG_ENTER(ctx_of(c));
     Ctx* ctx = CX(c);
     cudaStream_t st = (cudaStream_t)stream;
     if (n == 0 || k == 0) return SG_OK;
@@ -603,6 +605,7 @@ int sg_barycentric_sums(sg_ctx* c, void* stream, const uint64_t* d_data, uint64_
                         int ext3, uint64_t cols, const uint64_t* d_points, const uint64_t* d_inv_denoms, uint64_t n,
                         uint32_t k, uint64_t* d_out) {
     SG_CHECK_ARG(c, "null context");
+    SG_ENTER(ctx_of(c));
     SG_CHECK_ARG(k >= 1 && k <= BARY_MAX_K, "1 <= k <= 8 evaluation points");
     SG_CHECK_ARG(cols * (ext3 ? 3 : 1) <= row_u64, "columns exceed the row width");
     Ctx* ctx = CX(c);
@@ -649,6 +652,7 @@ int sg_deep_composition(sg_ctx* c, void* stream, const uint64_t* d_main, uint64_
                         const uint64_t* trace_ood, const uint64_t* gammas_h, const uint64_t* gammas_tr, uint32_t k,
                         const uint64_t* d_inv_h, const uint64_t* d_inv_t, int bitrev_out, uint64_t* d_out) {
     SG_CHECK_ARG(c && h_ood && trace_ood && gammas_h && gammas_tr, "null argument");
+    SG_ENTER(ctx_of(c));
     SG_CHECK_ARG(k <= DEEP_MAX_K, "at most 8 evaluation points");
     const int lr = log2_exact(rows);
     SG_CHECK_ARG(!bitrev_out || lr >= 0, "bit-reversed output needs a power-of-two row count");
@@ -708,6 +712,7 @@ int sg_deep_composition(sg_ctx* c, void* stream, const uint64_t* d_main, uint64_
 int sg_fri_fold_layer(sg_ctx* c, void* stream, const uint64_t* d_in, uint64_t h, const uint64_t* d_inv_tw,
                       const uint64_t zeta[3], uint64_t* d_out, uint64_t* d_inv_tw_next, uint8_t* d_leaves) {
     SG_CHECK_ARG(c && zeta, "null argument");
+    SG_ENTER(ctx_of(c));
     SG_CHECK_ARG(!d_leaves || (h % 2 == 0), "leaves need an even folded length");
     if (h == 0) return SG_OK;
     const uint64_t threads = (h + 1) / 2;
@@ -718,6 +723,7 @@ int sg_fri_fold_layer(sg_ctx* c, void* stream, const uint64_t* d_in, uint64_t h,
 
 int sg_fri_leaves(sg_ctx* c, void* stream, const uint64_t* d_evals, uint64_t n, uint8_t* d_leaves) {
     SG_CHECK_ARG(c, "null context");
+    SG_ENTER(ctx_of(c));
     SG_CHECK_ARG(n % 2 == 0, "FRI leaves hash pairs: even length required");
     if (n == 0) return SG_OK;
     k_fri_leaves<<<(unsigned)((n / 2 + 127) / 128), 128, 0, (cudaStream_t)stream>>>(d_evals, n / 2,
@@ -728,6 +734,7 @@ int sg_fri_leaves(sg_ctx* c, void* stream, const uint64_t* d_evals, uint64_t n, 
 int sg_gather_rows(sg_ctx* c, void* stream, const uint64_t* d_data, uint64_t row_u64, uint64_t nrows, uint64_t col0,
                    uint64_t width, const uint32_t* d_rows, uint32_t nq, uint64_t* d_out) {
     SG_CHECK_ARG(c, "null context");
+    SG_ENTER(ctx_of(c));
     SG_CHECK_ARG(col0 + width <= row_u64, "column range exceeds the row");
     const uint64_t tot = (uint64_t)nq * width;
     if (tot == 0) return SG_OK;
@@ -740,6 +747,7 @@ int sg_logup_aux(sg_ctx* c, void* stream, const uint64_t* d_main, uint64_t n, ui
                  const uint64_t* alpha_powers, uint32_t num_alpha, const uint64_t z[3], uint64_t* d_aux,
                  uint64_t table_contribution[3]) {
     SG_CHECK_ARG(c && hd && z && table_contribution, "null argument");
+    SG_ENTER(ctx_of(c));
     SG_CHECK_ARG(n >= 1, "n must be >= 1");
     SG_CHECK_ARG(hd->num_committed <= hd->num_out_cols, "committed columns exceed output columns");
     Ctx* ctx = CX(c);
@@ -872,6 +880,7 @@ int sg_fri_begin(sg_ctx* c, void* stream, const uint64_t* evals, int evals_on_de
                  int tw_on_device, uint64_t n0, sg_fri** out) {
     using namespace sg;
     SG_CHECK_ARG(c && evals && inv_tw && out, "null argument");
+    SG_ENTER(ctx_of(c));
     SG_CHECK_ARG(n0 >= 2 && log2_exact(n0) >= 0, "n0 must be a power of two >= 2");
     *out = nullptr;
     Ctx* ctx = CX(c);
@@ -911,6 +920,7 @@ static int fri_fold_step(sg_fri* f, const uint64_t zeta[3], bool commit, uint8_t
     const uint64_t h = f->n / 2;
     SG_CHECK_ARG(h >= (commit ? 2u : 1u), "codeword too short for another fold");
     Ctx* ctx = f->ctx;
+    SG_ENTER(ctx);
     uint64_t *out = nullptr, *twn = nullptr;
     uint8_t* nodes = nullptr;
     const uint64_t nl = h / 2;
@@ -975,6 +985,7 @@ void sg_fri_free(sg_fri* f) {
     using namespace sg;
     if (!f) return;
     Ctx* ctx = f->ctx;
+    enter(ctx);  // best effort: the layers are released either way
     for (auto& L : f->layers) {
         dev_free(ctx, f->st, L.evals, 24 * L.n);
         dev_free(ctx, f->st, L.nodes, (2 * L.leaves - 1) * 32);
@@ -1037,6 +1048,7 @@ extern "C" int sg_field_ops(sg_ctx* c, void* stream, uint32_t op, const uint64_t
                             uint64_t* d_out, uint64_t n) {
     using namespace sg;
     SG_CHECK_ARG(c && op <= 11, "null context or unknown op");
+    SG_ENTER(ctx_of(c));
     if (n == 0) return SG_OK;
     k_field_ops<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(op, d_a, d_b, d_out, n);
     return check_launch(CX(c), "k_field_ops");

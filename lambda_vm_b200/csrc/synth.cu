@@ -45,6 +45,7 @@ extern "C" int sg_synth_trace(sg_ctx* c, void* stream, uint64_t* d_out, uint64_t
                               uint32_t k_checksum) {
     Ctx* ctx = reinterpret_cast<Ctx*>(c);
     SG_CHECK_ARG(ctx && d_out, "null argument");
+    SG_ENTER(ctx);
     SG_CHECK_ARG(w >= 3 && k_checksum <= w - 2, "width must be >= 3 and k <= width - 2");
     if (n == 0) return SG_OK;
     cudaStream_t st = (cudaStream_t)stream;

@@ -8,14 +8,17 @@ records the pinned values those tests assert:
   * grinding nonces: crypto/stark/src/tests/grinding_tests.rs (seed, nonce,
     grinding factor, valid or not)
 The JSON is committed so tests never need the reference tree at run time.
-Usage: python tests/golden/extract_kats.py [REFERENCE_ROOT]
+Usage: python tests/golden/extract_kats.py REFERENCE_ROOT
+(REFERENCE_ROOT: the root of a lambda_vm checkout.)
 """
 import json
 import os
 import re
 import sys
 
-ROOT = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: python tests/golden/extract_kats.py REFERENCE_ROOT  (the root of a lambda_vm checkout)")
+ROOT = sys.argv[1]
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_kats.json")
 
 
