@@ -7,6 +7,7 @@ import glob
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -30,15 +31,23 @@ def build(force=False, verbose=False, extra=()):
     os.makedirs(OBJ, exist_ok=True)
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
     hdrs = sorted(glob.glob(os.path.join(CSRC, "*.cuh"))) + [os.path.join(ROOT, "include", "starkgpu.h")]
-    objs = []
+    objs, jobs = [], []
     for s in srcs:
         o = os.path.join(OBJ, os.path.basename(s)[:-3] + ".o")
         objs.append(o)
         if force or _stale(o, [s] + hdrs):
-            cmd = [NVCC] + ARCH + FLAGS + list(extra) + ["-dc" if False else "-c", s, "-o", o]
+            jobs.append((s, [NVCC] + ARCH + FLAGS + list(extra) + ["-c", s, "-o", o]))
+
+    def compile_one(job):
+        s, cmd = job
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        return s, cmd, r
+
+    # the translation units are independent: compile them in parallel
+    with ThreadPoolExecutor(max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for s, cmd, r in ex.map(compile_one, jobs):
             if verbose:
                 print(" ".join(cmd), flush=True)
-            r = subprocess.run(cmd, capture_output=True, text=True)
             if r.returncode != 0:
                 raise RuntimeError(f"nvcc failed for {s}:\n{r.stderr}")
             if verbose and r.stderr:
