@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--jobs", type=int, default=40, help="serve: jobs per rate")
     ap.add_argument("--job-max-log-n", type=int, default=18, help="serve: largest job height (log2 cycles)")
     ap.add_argument("--max-jobs", type=int, default=4, help="serve: concurrent jobs")
+    ap.add_argument("--policy", default="backfill", choices=["backfill", "fifo"], help="serve: admission policy")
+    ap.add_argument("--no-serve-summary", action="store_true",
+                    help="skip the serving summary the default line carries at N = 1")
     ap.add_argument("--tables", type=int, default=40)
     ap.add_argument("--max-log-n", type=int, default=22)
     ap.add_argument("--workers", type=int, default=8)
@@ -350,10 +353,14 @@ def serve_jobs(a, seed=77):
 
 
 def run_serve(a):
+    print(json.dumps(measure_serve(a)), flush=True)
+
+
+def measure_serve(a):
     """Serving: the same Poisson arrival stream served (1) by the admission
-    loop (up to --max-jobs concurrent proofs under a 160 GB HBM budget) and
-    (2) one proof at a time in arrival order; per rate: proofs/s, rows/s,
-    p50/p99 latency (submit to proof, queueing included)."""
+    loop (up to --max-jobs concurrent proofs under a 160 GB HBM budget, policy
+    --policy) and (2) one proof at a time in arrival order; per rate: proofs/s,
+    rows/s, p50/p99 latency (submit to proof, queueing included)."""
     import torch
     from lambda_vm_b200.device import backend
     from lambda_vm_b200.scheduler import multi_prove_scheduled
@@ -369,14 +376,14 @@ def run_serve(a):
         multi_prove_scheduled(airs, srcs, opts, workers=4, be=be)
     # one burst of every job at once, so the block cache reaches the working
     # set of max_jobs overlapping proofs before any latency is measured
-    with ProofServer(budget, max_jobs=a.max_jobs, drivers=4, opts=opts, be=be) as srv:
+    with ProofServer(budget, max_jobs=a.max_jobs, drivers=4, opts=opts, be=be, policy="fifo") as srv:
         for airs, srcs in specs:
             srv.submit(airs, srcs)
     torch.cuda.synchronize()
     sweep = []
     for i, rate in enumerate(float(x) for x in a.rates.split(",")):
         def batched():
-            with ProofServer(budget, max_jobs=a.max_jobs, drivers=4, opts=opts, be=be) as srv:
+            with ProofServer(budget, max_jobs=a.max_jobs, drivers=4, opts=opts, be=be, policy=a.policy) as srv:
                 return serve_poisson(srv, specs, rate, seed=int(rate * 1000))[1]
 
         def one_at_a_time():
@@ -388,7 +395,8 @@ def run_serve(a):
         else:
             st_seq, st = one_at_a_time(), batched()
         sweep.append({"rate_jobs_per_s": rate, "batched": st.as_dict(), "one_at_a_time": st_seq.as_dict(),
-                      "all_proved": st.failed == 0 and st_seq.failed == 0})
+                      "all_proved": st.failed == 0 and st_seq.failed == 0,
+                      "p99_batched_le_one_at_a_time": st.p99_s <= st_seq.p99_s})
     top = sweep[-1]
     rows = sum(sum(x.n for x in airs) for airs, _ in specs)
     line = {"metric": "proof serving: proved cycles/s and p50/p99 latency under Poisson arrivals",
@@ -398,9 +406,27 @@ def run_serve(a):
             "data": "synthetic chip-table proofs (no VM front-end: job sizes stand in for the guests' cycle counts)",
             "config": {"workload": f"{a.jobs} proof jobs per rate, cycles log-uniform 2^10..2^{a.job_max_log_n}, "
                                    f"2-4 tables each, blowup 2, 219 queries, grinding 20",
-                       "rows_total": rows, "hbm_budget_bytes": budget, "max_concurrent_jobs": a.max_jobs},
+                       "rows_total": rows, "hbm_budget_bytes": budget, "max_concurrent_jobs": a.max_jobs,
+                       "policy": a.policy},
             "p50_ms": top["batched"]["p50_ms"], "p99_ms": top["batched"]["p99_ms"], "sweep": sweep}
-    print(json.dumps(line), flush=True)
+    return line
+
+
+def serve_summary(a):
+    """A bounded serving run for the default bench line: two arrival rates,
+    24 jobs each, admission server against one proof at a time."""
+    import types
+    b = types.SimpleNamespace(jobs=24, job_max_log_n=a.job_max_log_n, max_jobs=a.max_jobs, rates="5,50",
+                              policy=a.policy)
+    line = measure_serve(b)
+    return {"workload": line["config"]["workload"], "policy": a.policy,
+            "rates": [{"rate_jobs_per_s": s["rate_jobs_per_s"],
+                       "p50_ms": s["batched"]["p50_ms"], "p99_ms": s["batched"]["p99_ms"],
+                       "proofs_per_s": s["batched"]["proofs_per_s"],
+                       "one_at_a_time_p50_ms": s["one_at_a_time"]["p50_ms"],
+                       "one_at_a_time_p99_ms": s["one_at_a_time"]["p99_ms"],
+                       "one_at_a_time_proofs_per_s": s["one_at_a_time"]["proofs_per_s"],
+                       "all_proved": s["all_proved"]} for s in line["sweep"]]}
 
 
 def run_rounds(a):
@@ -662,6 +688,11 @@ def main():
             line["proof_workload"] = proof_summary(a)
         except Exception as e:  # noqa: BLE001
             line["proof_workload"] = {"error": f"{type(e).__name__}: {e}"}
+    if world == 1 and not a.no_serve_summary:
+        try:
+            line["serving"] = serve_summary(a)
+        except Exception as e:  # noqa: BLE001
+            line["serving"] = {"error": f"{type(e).__name__}: {e}"}
     if not a.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(a, rpl, le)
     print(json.dumps(line), flush=True)

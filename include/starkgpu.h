@@ -88,6 +88,14 @@ SG_API int sg_stream_sync(sg_ctx* ctx, void* stream);
  * the reference's 32-stream pool, device.rs:139-143,500-503). */
 SG_API int sg_stream_create(sg_ctx* ctx, void** stream_out);
 SG_API int sg_stream_destroy(sg_ctx* ctx, void* stream);
+/* The same with a scheduling priority (lower numbers run first; the device's
+ * range comes from sg_stream_priority_range, greatest = the most urgent). The
+ * proof server gives its large jobs the urgent end so that small jobs running
+ * beside them fill gaps instead of stretching them. Streams a call creates
+ * internally (batched commits, host-trace uploads) take the caller stream's
+ * priority. No counterpart in the reference (its stream pool has one level). */
+SG_API int sg_stream_create_priority(sg_ctx* ctx, int priority, void** stream_out);
+SG_API int sg_stream_priority_range(sg_ctx* ctx, int* least, int* greatest);
 /* Page-locked host memory for fast transfers. */
 SG_API int sg_host_alloc(uint64_t bytes, void** out);
 SG_API int sg_host_free(void* p);

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "common.cuh"
@@ -211,6 +212,9 @@ void sg_ctx_destroy(sg_ctx* c) {
     for (auto& kv : ctx->live_cap) cudaFree(kv.first);
     for (auto ev : ctx->spare_events) cudaEventDestroy(ev);
     for (auto& kv : ctx->roots) cudaFree(kv.second);
+    for (auto e : ctx->stage_free)
+        if (e) cudaEventDestroy(e);
+    if (ctx->stage) cudaFreeHost(ctx->stage);
     delete ctx;
 }
 
@@ -274,6 +278,22 @@ int sg_stream_create(sg_ctx* c, void** out) {
     cudaStream_t st;
     SG_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     *out = (void*)st;
+    return SG_OK;
+}
+
+int sg_stream_create_priority(sg_ctx* c, int priority, void** out) {
+    SG_CHECK_ARG(c && out, "null argument");
+    SG_ENTER(ctx_of(c));
+    cudaStream_t st;
+    SG_CUDA(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, priority));
+    *out = (void*)st;
+    return SG_OK;
+}
+
+int sg_stream_priority_range(sg_ctx* c, int* least, int* greatest) {
+    SG_CHECK_ARG(c && least && greatest, "null argument");
+    SG_ENTER(ctx_of(c));
+    SG_CUDA(cudaDeviceGetStreamPriorityRange(least, greatest));
     return SG_OK;
 }
 
@@ -376,6 +396,51 @@ int sg_merkle_build(sg_ctx* c, void* stream, const uint8_t* d_leaves, uint64_t n
 // they are staged by the driver and the overlap is lost, not the result.
 static constexpr uint64_t kChunkCols = 32;  // fastest of 16/24/32/48/64 at 2^20 x 256
 
+// A non-blocking stream with the scheduling priority of `like` (the legacy
+// default stream counts as the default priority).
+static cudaError_t new_stream_like(cudaStream_t like, cudaStream_t* out) {
+    int prio = 0;
+    if (like && cudaStreamGetPriority(like, &prio) != cudaSuccess) prio = 0;
+    return cudaStreamCreateWithPriority(out, cudaStreamNonBlocking, prio);
+}
+
+// Copy columns [c0, c0 + w) of an n x m row-major host matrix into a dense
+// n x w buffer, rows split across host threads (each row is one w*8-byte copy).
+static void gather_columns(uint64_t* dst, const uint64_t* src, uint64_t n, uint64_t m, uint64_t c0, uint64_t w) {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const uint64_t T = std::max<uint64_t>(1, std::min<uint64_t>({hw ? hw : 1u, 16u, (n + 4095) / 4096}));
+    auto part = [&](uint64_t t) {
+        const uint64_t r0 = n * t / T, r1 = n * (t + 1) / T;
+        for (uint64_t r = r0; r < r1; ++r) memcpy(dst + r * w, src + r * m + c0, w * 8);
+    };
+    std::vector<std::thread> th;
+    for (uint64_t t = 1; t < T; ++t) th.emplace_back(part, t);
+    part(0);
+    for (auto& x : th) x.join();
+}
+
+// Page-locked staging for host traces in pageable memory: two halves of at
+// least `half_bytes`, kept by the context and reused by later calls. The
+// DMA engine can read only page-locked memory, so a pageable copy is staged
+// by the driver one small bounce buffer at a time (2 GiB took 350 ms); here
+// host threads gather a column chunk into one half while the previous chunk
+// goes up from the other. Called with ctx->stage_mu held.
+static int stage_reserve(Ctx* ctx, uint64_t half_bytes) {
+    if (ctx->stage && ctx->stage_bytes >= half_bytes) return SG_OK;
+    for (auto& e : ctx->stage_free)
+        if (e) SG_CUDA(cudaEventSynchronize(e));
+    if (ctx->stage) {
+        cudaFreeHost(ctx->stage);
+        ctx->stage = nullptr;
+        ctx->stage_bytes = 0;
+    }
+    SG_CUDA(cudaMallocHost(&ctx->stage, 2 * half_bytes));
+    ctx->stage_bytes = half_bytes;
+    for (auto& e : ctx->stage_free)
+        if (!e) SG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    return SG_OK;
+}
+
 // When `leaves` is non-null the commit's leaves are one LDE row each over the
 // whole row: they are then absorbed window by window as the LDE columns
 // complete (whole 17-lane sponge blocks), so hashing also runs under the
@@ -402,17 +467,37 @@ static int upload_and_lde(Ctx* ctx, cudaStream_t st, const uint64_t* h_trace, ui
         }
         return rc == SG_OK;
     };
-    if (ok(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "stream")) {
+    if (ok(new_stream_like(st, &cs), "stream")) {
         for (auto& e : ev)
             if (!ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event")) break;
     }
     // the copy stream starts after d_trace is valid in `st`'s order
     if (rc == SG_OK && ok(cudaEventRecord(ev[nchunks], st), "record")) ok(cudaStreamWaitEvent(cs, ev[nchunks], 0), "wait");
+    // pageable host memory goes through the context's page-locked staging
+    cudaPointerAttributes pa;
+    const bool pageable = cudaPointerGetAttributes(&pa, h_trace) != cudaSuccess || pa.type == cudaMemoryTypeUnregistered;
+    cudaGetLastError();
+    std::unique_lock<std::mutex> stage_lock(ctx->stage_mu, std::defer_lock);
+    if (pageable && rc == SG_OK) {
+        stage_lock.lock();
+        rc = stage_reserve(ctx, n * chunk * 8);
+    }
     for (uint64_t k = 0; k < nchunks && rc == SG_OK; ++k) {
         const uint64_t c0 = k * chunk, w = m - c0 < chunk ? m - c0 : chunk;
-        if (!ok(cudaMemcpy2DAsync(d_trace + c0, m * 8, h_trace + c0, m * 8, w * 8, n, cudaMemcpyHostToDevice, cs),
-                "copy"))
+        if (pageable) {
+            // wait until the half's previous copy (this call's or an earlier one's) has left it
+            uint64_t* half = (uint64_t*)ctx->stage + (k & 1) * (ctx->stage_bytes / 8);
+            if (!ok(cudaEventSynchronize(ctx->stage_free[k & 1]), "staging wait")) break;
+            gather_columns(half, h_trace, n, m, c0, w);
+            if (!ok(cudaMemcpy2DAsync(d_trace + c0, m * 8, half, w * 8, w * 8, n, cudaMemcpyHostToDevice, cs),
+                    "copy") ||
+                !ok(cudaEventRecord(ctx->stage_free[k & 1], cs), "record"))
+                break;
+        } else if (!ok(cudaMemcpy2DAsync(d_trace + c0, m * 8, h_trace + c0, m * 8, w * 8, n, cudaMemcpyHostToDevice,
+                                         cs),
+                       "copy")) {
             break;
+        }
         if (!ok(cudaEventRecord(ev[k], cs), "record") || !ok(cudaStreamWaitEvent(st, ev[k], 0), "wait")) break;
         rc = coset_lde_ld(ctx, st, d_trace + c0, m, n, w, blowup, d_w, d_lde + c0, m);
         if (rc == SG_OK && sink) {
@@ -623,7 +708,7 @@ int sg_batch_commit(sg_ctx* c, void* stream, const sg_table_desc* tables, uint32
     if (cuda_ok(cudaEventCreateWithFlags(&start, cudaEventDisableTiming), "event") &&
         cuda_ok(cudaEventRecord(start, caller), "event record")) {
         for (uint32_t s = 0; s < k && rc == SG_OK; ++s) {
-            if (!cuda_ok(cudaStreamCreateWithFlags(&streams[s], cudaStreamNonBlocking), "stream")) break;
+            if (!cuda_ok(new_stream_like(caller, &streams[s]), "stream")) break;
             if (!cuda_ok(cudaEventCreateWithFlags(&done[s], cudaEventDisableTiming), "event")) break;
             cuda_ok(cudaStreamWaitEvent(streams[s], start, 0), "stream wait");
         }

@@ -95,6 +95,12 @@ struct Ctx {
     TileTune tiles[13];
     std::mutex tune_mu;
     bool autotune = true;
+    // Page-locked staging for uploads from pageable host memory (api.cu): two
+    // halves of stage_bytes, each with the event of the copy that last read it.
+    std::mutex stage_mu;
+    void* stage = nullptr;
+    uint64_t stage_bytes = 0;
+    cudaEvent_t stage_free[2] = {nullptr, nullptr};
 };
 
 // Return every cached block to the driver pool (on OOM, and at teardown).

@@ -95,6 +95,8 @@ PROTOTYPES = {
     "sg_memcpy_d2h": (i32, [vp, vp, vp, vp, u64]),
     "sg_stream_sync": (i32, [vp, vp]),
     "sg_stream_create": (i32, [vp, C.POINTER(vp)]),
+    "sg_stream_create_priority": (i32, [vp, C.c_int, C.POINTER(vp)]),
+    "sg_stream_priority_range": (i32, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "sg_stream_destroy": (i32, [vp, vp]),
     "sg_host_alloc": (i32, [u64, C.POINTER(vp)]),
     "sg_host_free": (i32, [vp]),

@@ -58,13 +58,20 @@ def heaviest_first(airs, opts):
 
 
 class StreamPool:
-    def __init__(self, be, k):
+    """k non-blocking streams, each wrapped in a GpuBackend for one table
+    driver. `priority` (None: the default) is a CUDA stream priority, lower
+    numbers first (sg_stream_priority_range)."""
+
+    def __init__(self, be, k, priority=None):
         self.be = be
         L = native.lib()
         self.streams = []
         for _ in range(k):
             s = C.c_void_p()
-            native.check(L.sg_stream_create(be.h, C.byref(s)))
+            if priority is None:
+                native.check(L.sg_stream_create(be.h, C.byref(s)))
+            else:
+                native.check(L.sg_stream_create_priority(be.h, int(priority), C.byref(s)))
             self.streams.append(s.value)
         self.free = [GpuBackend(be, s) for s in self.streams]
         self.lock = threading.Lock()
@@ -85,13 +92,26 @@ class StreamPool:
         self.streams = []
 
 
+def stream_priority_range(be):
+    """(least, greatest) CUDA stream priority of the context's device."""
+    lo, hi = C.c_int(), C.c_int()
+    native.check(native.lib().sg_stream_priority_range(be.h, C.byref(lo), C.byref(hi)))
+    return lo.value, hi.value
+
+
 def multi_prove_scheduled(airs, sources, opts=None, workers=8, budget_bytes=None, be=None,
-                          label=b"lambda_vm_b200/synthetic-multi-table"):
-    """Same proof as stark.multi_prove, with k concurrent table drivers."""
+                          label=b"lambda_vm_b200/synthetic-multi-table", priority=None):
+    """Same proof as stark.multi_prove, with k concurrent table drivers (on
+    streams of CUDA priority `priority`, None: the default)."""
     opts = opts or Options()
     be = be or _backend()
     B, g = opts.blowup, opts.coset_offset
     base = GpuBackend(be)
+    r1_stream = None
+    if priority is not None:
+        s = C.c_void_p()
+        native.check(native.lib().sg_stream_create_priority(be.h, int(priority), C.byref(s)))
+        r1_stream = s.value
     for air in airs:  # warm the domain caches serially on the legacy stream
         base.domain(air.log_n, B, g)
     # time the DFT tile widths now, while nothing else runs, rather than
@@ -100,15 +120,18 @@ def multi_prove_scheduled(airs, sources, opts=None, workers=8, budget_bytes=None
     for log_len in range(8, 12):
         native.check(native.lib().sg_ctx_dft_tuning(be.h, None, log_len, cols, cost, C.byref(cnt)))
     native.check(native.lib().sg_stream_sync(be.h, None))
-    pool = StreamPool(be, workers)
+    pool = StreamPool(be, workers, priority)
+    # R1 runs on a stream of the job's priority (its batched commit's internal
+    # streams inherit it); the legacy stream when no priority is asked for
+    r1b = GpuBackend(be, r1_stream) if r1_stream is not None else base
     order = heaviest_first(airs, opts)
     r1 = [None] * len(airs)
 
     try:
         # R1: every table's trace, then one native batched commit (LDE + leaves
         # + tree per table, heaviest first over `workers` streams).
-        tms = [_gen_trace(base, air, src) for air, src in zip(airs, sources)]
-        committed = base.batch_commit(tms, B, [base.domain(a.log_n, B, g).weights for a in airs], workers)
+        tms = [_gen_trace(r1b, air, src) for air, src in zip(airs, sources)]
+        committed = r1b.batch_commit(tms, B, [base.domain(a.log_n, B, g).weights for a in airs], workers)
         for i in range(len(airs)):
             lde, tree, root, release = committed[i]
             r1[i] = (tms[i], lde, tree, root, release)
@@ -155,3 +178,6 @@ def multi_prove_scheduled(airs, sources, opts=None, workers=8, budget_bytes=None
         return {"tables": proofs, "challenges": challenges}
     finally:
         pool.close()
+        if r1_stream is not None:
+            native.lib().sg_stream_sync(be.h, r1_stream)
+            native.lib().sg_stream_destroy(be.h, r1_stream)

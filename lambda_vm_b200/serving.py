@@ -33,14 +33,23 @@ def estimate_job_bytes(airs, opts, drivers):
     return resident + sum(per_table[:max(1, drivers)])
 
 
-class Job:
-    __slots__ = ("id", "airs", "sources", "rows", "est", "t_submit", "t_start", "t_done", "proof", "error", "done")
+def job_cells(airs):
+    """Trace cells of a job (main + 3 per aux column, every table): the size
+    its device time grows with."""
+    return sum(a.n * (a.width + 3 * a.aux_width) for a in airs)
 
-    def __init__(self, jid, airs, sources, est):
+
+class Job:
+    __slots__ = ("id", "airs", "sources", "rows", "cells", "big", "est", "t_submit", "t_start", "t_done", "proof",
+                 "error", "done")
+
+    def __init__(self, jid, airs, sources, est, big_cells=None):
         self.id = jid
         self.airs = airs
         self.sources = sources
         self.rows = sum(a.n for a in airs)
+        self.cells = job_cells(airs)
+        self.big = big_cells is not None and self.cells >= big_cells
         self.est = est
         self.t_submit = time.perf_counter()
         self.t_start = None
@@ -82,24 +91,50 @@ def _quantile(sorted_vals, q):
 
 
 class ProofServer:
-    """FIFO job queue with slot + HBM-budget admission.
+    """Job queue with slot + HBM-budget admission.
 
     `max_jobs` concurrent proofs, each proved by `prove_fn(airs, sources, opts,
     drivers, budget_bytes)` (default: the scheduled multi-table prover on the
-    process-wide device context) with `drivers` table drivers. A job whose
-    estimate exceeds the whole budget runs alone rather than never.
+    process-wide device context). A job whose estimate exceeds the whole budget
+    runs alone rather than never.
+
+    policy "fifo": jobs start in arrival order as slots and memory allow, each
+    with `drivers` table drivers.
+
+    policy "backfill" (default): a job of at least `big_cells` trace cells is
+    large. Large jobs start in arrival order and never overlap one another, so a
+    large proof is never stretched by another large one (what made the FIFO
+    server's tail worse than one-at-a-time at low load). Small jobs start as
+    soon as a slot and memory are free, also past a large job that waits for
+    the running one (backfilling): they keep one slot and the waiting job's
+    memory free, so the large job still starts the moment the running large
+    job ends. Large jobs get `drivers` table drivers on streams of the
+    device's most urgent priority, small jobs at most `small_drivers` on
+    default-priority streams, so a small proof fills gaps in a large one
+    instead of lengthening it.
     """
 
-    def __init__(self, budget_bytes, max_jobs=4, drivers=4, opts=None, prove_fn=None, be=None):
+    def __init__(self, budget_bytes, max_jobs=4, drivers=4, opts=None, prove_fn=None, be=None, policy="backfill",
+                 big_cells=1 << 23, small_drivers=2):
+        if policy not in ("fifo", "backfill"):
+            raise ValueError(f"unknown admission policy {policy!r}")
         self.opts = opts or Options()
         self.max_jobs = max_jobs
         self.drivers = drivers
+        self.small_drivers = small_drivers
+        self.policy = policy
+        self.big_cells = big_cells if policy == "backfill" else None
         self.gate = VramGate(budget_bytes)
         self.be = be
+        self.urgent = None
+        if prove_fn is None and policy == "backfill" and be is not None:
+            from .scheduler import stream_priority_range
+            self.urgent = stream_priority_range(be)[1]
         self.prove_fn = prove_fn or self._prove_gpu
         self.queue = deque()
         self.cv = threading.Condition()
         self.running = 0
+        self.big_running = 0
         self.next_id = 0
         self.jobs = []
         self.closed = False
@@ -107,46 +142,77 @@ class ProofServer:
         self.dispatcher = threading.Thread(target=self._dispatch, daemon=True)
         self.dispatcher.start()
 
-    def _prove_gpu(self, airs, sources, opts, drivers, budget_bytes):
-        return multi_prove_scheduled(airs, sources, opts, workers=drivers, budget_bytes=budget_bytes, be=self.be)
+    def _prove_gpu(self, airs, sources, opts, drivers, budget_bytes, priority=None):
+        return multi_prove_scheduled(airs, sources, opts, workers=drivers, budget_bytes=budget_bytes, be=self.be,
+                                     priority=priority)
+
+    def _drivers(self, job):
+        return self.drivers if (self.policy == "fifo" or job.big) else max(1, min(self.small_drivers, self.drivers))
 
     def submit(self, airs, sources):
         with self.cv:
             if self.closed:
                 raise RuntimeError("server is closed")
-            job = Job(self.next_id, airs, sources, estimate_job_bytes(airs, self.opts, self.drivers))
+            probe = Job(self.next_id, airs, sources, 0, self.big_cells)
+            est = estimate_job_bytes(airs, self.opts, self.drivers if self.policy == "fifo" or probe.big
+                                     else max(1, min(self.small_drivers, self.drivers)))
+            job = Job(self.next_id, airs, sources, est, self.big_cells)
             self.next_id += 1
             self.jobs.append(job)
             self.queue.append(job)
             self.cv.notify_all()
         return job
 
-    def _fits(self, job):
+    def _fits(self, job, reserve=0):
         g = self.gate
-        return g.used == 0 or g.used + job.est <= g.budget
+        return g.used == 0 or g.used + job.est + reserve <= g.budget
+
+    def _pick(self):
+        """The queued job to start now, or None (called with the lock held)."""
+        if not self.queue or self.running >= self.max_jobs:
+            return None
+        if self.policy == "fifo":
+            return self.queue[0] if self._fits(self.queue[0]) else None
+        head = self.queue[0]
+        if self._fits(head) and not (head.big and self.big_running):
+            return head
+        # The head waits (a large job behind the running large one, or memory):
+        # a small job may pass it if it leaves the head a slot and its memory.
+        if self.running >= self.max_jobs - 1:
+            return None
+        for j in list(self.queue)[1:]:
+            if not j.big and self._fits(j, reserve=head.est):
+                return j
+        return None
 
     def _dispatch(self):
         while True:
             with self.cv:
-                while not self.closed and not (self.queue and self.running < self.max_jobs and
-                                               self._fits(self.queue[0])):
+                job = self._pick()
+                while not self.closed and job is None:
                     self.cv.wait(0.05)
+                    job = self._pick()
                 if self.closed and not self.queue:
                     return
-                if not (self.queue and self.running < self.max_jobs and self._fits(self.queue[0])):
+                if job is None:
                     continue
-                job = self.queue.popleft()
+                self.queue.remove(job)
                 self.running += 1
+                self.big_running += job.big
+                job.t_start = time.perf_counter()
                 self.gate.acquire(job.est)
             t = threading.Thread(target=self._run, args=(job,), daemon=True)
             self.threads.append(t)
             t.start()
 
     def _run(self, job):
-        job.t_start = time.perf_counter()
         try:
             # rounds 2-4 of this job may use what its resident R1 state leaves of its share
-            job.proof = self.prove_fn(job.airs, job.sources, self.opts, self.drivers, job.est)
+            if self.prove_fn == self._prove_gpu:
+                job.proof = self._prove_gpu(job.airs, job.sources, self.opts, self._drivers(job), job.est,
+                                            self.urgent if job.big else None)
+            else:
+                job.proof = self.prove_fn(job.airs, job.sources, self.opts, self._drivers(job), job.est)
         except Exception as e:  # reported per job; the server keeps serving
             job.error = e
         finally:
@@ -154,6 +220,7 @@ class ProofServer:
             self.gate.release(job.est)
             with self.cv:
                 self.running -= 1
+                self.big_running -= job.big
                 self.cv.notify_all()
             job.done.set()
 

@@ -100,3 +100,68 @@ def test_closed_server_rejects():
     srv.close()
     with pytest.raises(RuntimeError):
         srv.submit(*_spec(0))
+
+
+class SizedRecorder(Recorder):
+    """Stand-in prover whose run time grows with the job (large jobs 0.2 s,
+    small ones 0.02 s), recording when each job starts and ends."""
+
+    def __init__(self, big_cells):
+        super().__init__()
+        self.big_cells = big_cells
+        self.spans = {}
+        self.t0 = time.perf_counter()
+
+    def __call__(self, airs, sources, opts, drivers, budget):
+        from lambda_vm_b200.serving import job_cells
+        big = job_cells(airs) >= self.big_cells
+        self.delay = 0.2 if big else 0.02
+        start = time.perf_counter() - self.t0
+        out = super().__call__(airs, sources, opts, drivers, budget)
+        with self.lock:
+            self.spans[sources[0]] = (start, time.perf_counter() - self.t0, big, drivers)
+        return out
+
+
+def test_backfill_large_jobs_never_overlap_small_jobs_pass_them():
+    """Large jobs run one at a time in arrival order; small jobs that arrive
+    behind a waiting large job start at once (leaving it a slot), and the
+    large job starts as soon as the running large job ends."""
+    big = _spec(0, 14, 300)[0]
+    small = _spec(0, 10, 8)[0]
+    from lambda_vm_b200.serving import job_cells
+    cut = job_cells(big)
+    assert job_cells(small) < cut
+    rec = SizedRecorder(cut)
+    with ProofServer(budget_bytes=1 << 40, max_jobs=4, drivers=4, prove_fn=rec, big_cells=cut,
+                     small_drivers=2) as srv:
+        srv.submit(big, [0])
+        srv.submit(big, [1])
+        for i in range(2, 6):
+            srv.submit(small, [i])
+        srv.drain()
+    sp = rec.spans
+    a, b = sp[0], sp[1]
+    assert a[2] and b[2] and not any(sp[i][2] for i in range(2, 6))
+    assert b[0] >= a[1] - 1e-3  # the two large jobs never overlap
+    assert b[0] - a[1] < 0.05  # and the second starts as the first ends
+    # small jobs started while the first large job ran, ahead of the second
+    assert sum(1 for i in range(2, 6) if sp[i][0] < a[1]) >= 2
+    # one slot stays free for the waiting large job: at most 3 ran at once
+    assert rec.max_running <= 4
+    assert a[3] == 4 and all(sp[i][3] == 2 for i in range(2, 6))
+
+
+def test_fifo_policy_keeps_arrival_order():
+    big = _spec(0, 14, 300)[0]
+    from lambda_vm_b200.serving import job_cells
+    rec = SizedRecorder(job_cells(big))
+    with ProofServer(budget_bytes=1 << 40, max_jobs=1, drivers=3, prove_fn=rec, policy="fifo") as srv:
+        srv.submit(big, [0])
+        for i in range(1, 4):
+            srv.submit(_spec(0, 10, 8)[0], [i])
+        srv.drain()
+    assert rec.starts == [0, 1, 2, 3]
+    assert all(v[3] == 3 for v in rec.spans.values())
+    with pytest.raises(ValueError):
+        ProofServer(budget_bytes=1, prove_fn=rec, policy="lifo")
