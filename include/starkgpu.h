@@ -478,6 +478,58 @@ SG_API int sg_field_ops(sg_ctx* ctx, void* stream, uint32_t op, const uint64_t* 
 SG_API int sg_synth_trace(sg_ctx* ctx, void* stream, uint64_t* d_out, uint64_t n, uint64_t w, uint64_t seed,
                           uint32_t k_checksum);
 
+/* ---- DFT pass log: the autotuner's measurements. No counterpart in the
+ *      reference (its NTT has one fixed plan). While enabled, every DFT pass
+ *      launched through the context is bracketed by CUDA events; _read waits for
+ *      them and returns one record per pass (its shape, the tile width used and
+ *      its device time), oldest first, then clears the log. ---- */
+typedef struct {
+    uint32_t log_len;  /* points per tile, log2 */
+    uint32_t cols;     /* tile width (columns per tile) */
+    uint32_t inverse;  /* 1: inverse transform */
+    uint32_t reps;     /* coset repetitions per tile (blowup for the LDE's first forward pass) */
+    uint32_t pre;      /* 1: per-point coset-shift factors before the transform */
+    uint32_t post;     /* 0 none, 1 four-step twiddles, 2 coset weights, 3 scalar */
+    uint32_t canon;    /* 1: canonical output */
+    uint32_t pad_;
+    uint64_t tiles;    /* point tiles (each is log_len points x all columns) */
+    uint64_t m;        /* columns */
+    float ms;          /* device time of the launch */
+    float pad2_;
+} sg_pass_record;
+SG_API int sg_ctx_pass_log(sg_ctx* ctx, int enable);
+SG_API int sg_ctx_pass_log_read(sg_ctx* ctx, sg_pass_record* out, uint32_t capacity, uint32_t* count);
+
+/* ---- learned pass-cost model. No counterpart in the reference. A small MLP
+ *      (SG_MLP_IN inputs, two hidden layers of SG_MLP_HIDDEN ReLU units, one
+ *      output) predicts log(ms) of a DFT pass from its shape and tile width;
+ *      trained on the GPU by these kernels from pass-log measurements, it then
+ *      chooses each pass's tile width in place of the timing probe.
+ *      Parameters are fp32, laid out W1[H][IN], b1[H], W2[H][H], b2[H], w3[H], b3.
+ *      _loss_grad: mean squared error over n samples (x: n x SG_MLP_IN row-major,
+ *      y: n targets) and its gradient, one forward and backward pass, reduced in a
+ *      fixed order (deterministic). _train: `steps` Adam steps on the full batch
+ *      (lr, beta1 0.9, beta2 0.999, eps 1e-8), params updated in place; the final
+ *      loss is written to loss_out. _predict: y = model(x). All device pointers.
+ *      sg_ctx_set_pass_model installs host-side parameters in the context (count
+ *      = SG_MLP_PARAMS; count 0 removes them): pass tile widths are then the
+ *      model's choice, and the timing probe never runs. ---- */
+#define SG_MLP_IN 16
+#define SG_MLP_HIDDEN 32
+#define SG_MLP_PARAMS (SG_MLP_HIDDEN * SG_MLP_IN + SG_MLP_HIDDEN + SG_MLP_HIDDEN * SG_MLP_HIDDEN + SG_MLP_HIDDEN + \
+                       SG_MLP_HIDDEN + 1)
+SG_API int sg_mlp_loss_grad(sg_ctx* ctx, void* stream, const float* d_x, const float* d_y, uint32_t n,
+                            const float* d_params, float* d_grad, float* d_loss);
+SG_API int sg_mlp_train(sg_ctx* ctx, void* stream, const float* d_x, const float* d_y, uint32_t n, float* d_params,
+                        uint32_t steps, float lr, float* loss_out);
+SG_API int sg_mlp_predict(sg_ctx* ctx, void* stream, const float* d_x, uint32_t n, const float* d_params,
+                          float* d_out);
+/* Feature vector of one DFT pass with tile width `cols` (host function; the
+ * same features the model is trained on). */
+SG_API void sg_pass_features(uint32_t log_len, uint64_t tiles, uint64_t m, uint32_t cols, uint32_t reps,
+                             uint32_t inverse, uint32_t pre, uint32_t post, uint32_t canon, float out[SG_MLP_IN]);
+SG_API int sg_ctx_set_pass_model(sg_ctx* ctx, const float* params, uint32_t count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -101,7 +101,20 @@ struct Ctx {
     void* stage = nullptr;
     uint64_t stage_bytes = 0;
     cudaEvent_t stage_free[2] = {nullptr, nullptr};
+    // DFT pass log (ntt.cu, sg_ctx_pass_log): each pass with its events while on.
+    struct PassLog {
+        sg_pass_record rec;
+        cudaEvent_t e0, e1;
+    };
+    std::atomic<bool> passlog_on{false};
+    std::mutex passlog_mu;
+    std::vector<PassLog> passlog;
+    // Learned pass-cost model (mlp.cu): when set, DFT tile widths are its choice.
+    std::vector<float> pass_model;
 };
+
+// Host-side prediction of the pass-cost model (mlp.cu): log(ms) for features x.
+float mlp_predict_host(const float* params, const float* x);
 
 // Return every cached block to the driver pool (on OOM, and at teardown).
 void trim_cache(Ctx* ctx);

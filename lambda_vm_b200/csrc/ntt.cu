@@ -487,7 +487,9 @@ static int tune_tiles(Ctx* ctx, cudaStream_t st, uint32_t logL) {
     return rc != SG_OK ? rc : rf;
 }
 
-static int pick_cols(Ctx* ctx, cudaStream_t st, uint32_t logL, uint64_t m, int* cols) {
+static int pick_cols(Ctx* ctx, cudaStream_t st, const PassArgs& a, uint64_t ntiles, int* cols) {
+    const uint32_t logL = a.logL;
+    const uint64_t m = a.m;
     int vs[4];
     const int nv = tile_variants(logL, vs);
     *cols = default_cols((int)logL);
@@ -497,6 +499,20 @@ static int pick_cols(Ctx* ctx, cudaStream_t st, uint32_t logL, uint64_t m, int* 
         const int forced = ctx->tiles[logL].forced;
         if (forced) {
             *cols = forced;
+            return SG_OK;
+        }
+        // With a learned pass-cost model installed, each compiled width's pass
+        // time is predicted from the pass's shape and the fastest is taken; no
+        // timing probe runs.
+        if (!ctx->pass_model.empty()) {
+            float best = 0;
+            for (int v = 0; v < nv; ++v) {
+                float x[SG_MLP_IN];
+                sg_pass_features(logL, ntiles, m, (uint32_t)vs[v], a.reps, a.inverse, a.pre_kind ? 1 : 0,
+                                 a.post_kind, a.canon_out, x);
+                const float t = mlp_predict_host(ctx->pass_model.data(), x);
+                if (v == 0 || t < best) best = t, *cols = vs[v];
+            }
             return SG_OK;
         }
     }
@@ -521,8 +537,27 @@ static int pick_cols(Ctx* ctx, cudaStream_t st, uint32_t logL, uint64_t m, int* 
 
 static int run_pass(Ctx* ctx, cudaStream_t st, const PassArgs& a, uint64_t ntiles) {
     int cols = 0;
-    SG_TRY(pick_cols(ctx, st, a.logL, a.m, &cols));
-    return launch_cols(ctx, st, a, ntiles, cols);
+    SG_TRY(pick_cols(ctx, st, a, ntiles, &cols));
+    if (!ctx->passlog_on.load(std::memory_order_relaxed)) return launch_cols(ctx, st, a, ntiles, cols);
+    // pass log: the launch between two events, read back by sg_ctx_pass_log_read
+    Ctx::PassLog r{};
+    r.rec.log_len = a.logL, r.rec.cols = (uint32_t)cols, r.rec.inverse = a.inverse, r.rec.reps = a.reps;
+    r.rec.pre = a.pre_kind ? 1 : 0, r.rec.post = a.post_kind, r.rec.canon = a.canon_out;
+    r.rec.tiles = ntiles, r.rec.m = a.m;
+    SG_CUDA(cudaEventCreate(&r.e0));
+    cudaError_t e = cudaEventCreate(&r.e1);
+    if (e == cudaSuccess) e = cudaEventRecord(r.e0, st);
+    int rc = e == cudaSuccess ? launch_cols(ctx, st, a, ntiles, cols) : SG_ERR_CUDA;
+    if (rc == SG_OK) e = cudaEventRecord(r.e1, st);
+    if (e != cudaSuccess || rc != SG_OK) {
+        if (e != cudaSuccess) set_error(std::string("pass log: ") + cudaGetErrorString(e));
+        cudaEventDestroy(r.e0);
+        if (r.e1) cudaEventDestroy(r.e1);
+        return rc != SG_OK ? rc : SG_ERR_CUDA;
+    }
+    std::lock_guard<std::mutex> g(ctx->passlog_mu);
+    ctx->passlog.push_back(r);
+    return SG_OK;
 }
 
 static PassArgs base_args(const uint64_t* in, uint64_t* out, uint64_t m, uint32_t logL, bool inv, const Tw& tw) {
@@ -846,6 +881,47 @@ extern "C" int sg_coset_lde_static(void* stream, const uint64_t* d_trace, uint64
     uint64_t* coef = scratch + tw_region;
     uint64_t* tmp = coef + n * m;
     return lde_passes(ctx, st, d_trace, m, n, m, blowup, d_weights, d_out, m, tw, coef, tmp);
+}
+
+extern "C" int sg_ctx_pass_log(sg_ctx* c, int enable) {
+    using namespace sg;
+    SG_CHECK_ARG(c, "null context");
+    reinterpret_cast<Ctx*>(c)->passlog_on.store(enable != 0);
+    return SG_OK;
+}
+
+extern "C" int sg_ctx_pass_log_read(sg_ctx* c, sg_pass_record* out, uint32_t capacity, uint32_t* count) {
+    using namespace sg;
+    SG_CHECK_ARG(c && count && (out || capacity == 0), "null argument");
+    SG_ENTER(ctx_of(c));
+    Ctx* ctx = reinterpret_cast<Ctx*>(c);
+    std::vector<Ctx::PassLog> log;
+    {
+        std::lock_guard<std::mutex> g(ctx->passlog_mu);
+        log.swap(ctx->passlog);
+    }
+    int rc = SG_OK;
+    uint32_t k = 0;
+    for (auto& r : log) {
+        float ms = 0;
+        if (rc == SG_OK) {
+            cudaError_t e = cudaEventSynchronize(r.e1);
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, r.e0, r.e1);
+            if (e != cudaSuccess) {
+                set_error(std::string("pass log: ") + cudaGetErrorString(e));
+                rc = SG_ERR_CUDA;
+            }
+        }
+        if (rc == SG_OK && k < capacity) {
+            out[k] = r.rec;
+            out[k].ms = ms;
+            ++k;
+        }
+        cudaEventDestroy(r.e0);
+        cudaEventDestroy(r.e1);
+    }
+    *count = k;
+    return rc;
 }
 
 extern "C" int sg_ctx_dft_tiles(sg_ctx* c, uint32_t log_len, uint32_t cols) {

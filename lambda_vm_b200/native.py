@@ -29,6 +29,12 @@ class TableDesc(C.Structure):
                 ("layout", LeafLayout)]
 
 
+class PassRecord(C.Structure):
+    _fields_ = [("log_len", C.c_uint32), ("cols", C.c_uint32), ("inverse", C.c_uint32), ("reps", C.c_uint32),
+                ("pre", C.c_uint32), ("post", C.c_uint32), ("canon", C.c_uint32), ("pad_", C.c_uint32),
+                ("tiles", C.c_uint64), ("m", C.c_uint64), ("ms", C.c_float), ("pad2_", C.c_float)]
+
+
 class LdeInfo(C.Structure):
     _fields_ = [("d_lde", C.c_void_p), ("lde_rows", C.c_uint64), ("row_u64", C.c_uint64),
                 ("d_nodes", C.c_void_p), ("leaves_len", C.c_uint64), ("root", C.c_uint8 * 32)]
@@ -150,7 +156,16 @@ PROTOTYPES = {
     "sg_eval_constraints": (i32, [vp, vp, vp, vp, u32, vp, u32, vp, vp, u64, vp, u64, u64, u64, vp, vp]),
     "sg_decompose_d2": (i32, [vp, vp, vp, u64, vp, vp]),
     "sg_synth_trace": (i32, [vp, vp, vp, u64, u64, u64, u32]),
+    "sg_ctx_pass_log": (i32, [vp, i32]),
+    "sg_ctx_pass_log_read": (i32, [vp, C.POINTER(PassRecord), u32, C.POINTER(u32)]),
+    "sg_mlp_loss_grad": (i32, [vp, vp, vp, vp, u32, vp, vp, vp]),
+    "sg_mlp_train": (i32, [vp, vp, vp, vp, u32, vp, u32, C.c_float, C.POINTER(C.c_float)]),
+    "sg_mlp_predict": (i32, [vp, vp, vp, u32, vp, vp]),
+    "sg_pass_features": (None, [u32, u64, u64, u32, u32, u32, u32, u32, u32, C.POINTER(C.c_float)]),
+    "sg_ctx_set_pass_model": (i32, [vp, C.POINTER(C.c_float), u32]),
 }
+MLP_IN, MLP_HIDDEN = 16, 32
+MLP_PARAMS = MLP_HIDDEN * MLP_IN + MLP_HIDDEN + MLP_HIDDEN * MLP_HIDDEN + MLP_HIDDEN + MLP_HIDDEN + 1
 SG_STATIC_SCRATCH_BYTES = 32 << 20
 
 _lib = None

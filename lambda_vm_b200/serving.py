@@ -297,7 +297,7 @@ def serve_sequential(job_specs, rate, prove_fn, seed=0):
         if t0 + at > now:
             time.sleep(t0 + at - now)
         j = Job(len(jobs), airs, sources, 0)
-        j.t_submit = t0 + at
+        j.t_submit = t0 + float(at)
         j.t_start = time.perf_counter()
         try:
             j.proof = prove_fn(airs, sources)

@@ -37,7 +37,8 @@ def _functions(src):
 
 
 # Entry points that take a context but never touch the device.
-NO_CUDA = {"sg_ctx_launches", "sg_ctx_budget", "sg_ctx_fail_alloc_after", "sg_ctx_dft_tiles", "sg_ctx_memory"}
+NO_CUDA = {"sg_ctx_launches", "sg_ctx_budget", "sg_ctx_fail_alloc_after", "sg_ctx_dft_tiles", "sg_ctx_memory",
+           "sg_ctx_pass_log", "sg_ctx_set_pass_model"}
 
 
 def test_every_context_entry_point_enters_its_device():
