@@ -143,8 +143,29 @@ def collect(be, configs=None, repeats=3, seed=5):
             b.close()
     records = []
     for (shape, cols_, cfg), (rec, ms) in recs.items():
-        records.append(dict(rec, cols=cols_, ms=float(np.median(ms)), lde=list(cfg)))
+        records.append(dict(rec, cols=cols_, ms=round(float(np.median(ms)), 5), lde=list(cfg)))
     return {"records": records, "probe": {str(k): {str(c): v for c, v in d.items()} for k, d in probe.items()}}
+
+
+FIELDS = SHAPE_KEYS + ("cols", "ms", "lde_log_n", "lde_m", "lde_blowup")
+
+
+def save_dataset(data, path=DATASET):
+    """Compact JSON: one row of numbers per pass record."""
+    rows = [[r[k] for k in SHAPE_KEYS] + [r["cols"], r["ms"]] + list(r["lde"]) for r in data["records"]]
+    os.makedirs(os.path.dirname(path), exist_ok=True)
+    with open(path, "w") as f:
+        json.dump({"fields": list(FIELDS), "rows": rows, "probe": data["probe"]}, f, separators=(",", ":"))
+
+
+def load_dataset(path=DATASET):
+    d = json.load(open(path))
+    recs = []
+    for row in d["rows"]:
+        r = dict(zip(d["fields"], row))
+        r["lde"] = [r.pop("lde_log_n"), r.pop("lde_m"), r.pop("lde_blowup")]
+        recs.append(r)
+    return {"records": recs, "probe": d["probe"]}
 
 
 # ---------------------------------------------------------------- split, features
@@ -304,8 +325,8 @@ def main():
     from .device import backend
     be = backend(0)
     data = collect(be)
-    os.makedirs(os.path.dirname(DATASET), exist_ok=True)
-    json.dump(data, open(DATASET, "w"))
+    save_dataset(data)
+    data = load_dataset()
     tr, te = split(data["records"])
     X, y = design(tr)
     params, loss = train(be, X, y)

@@ -761,6 +761,123 @@ int sg_batch_commit(sg_ctx* c, void* stream, const sg_table_desc* tables, uint32
     return SG_OK;
 }
 
+int sg_batch_commit_fused(sg_ctx* c, void* stream, const sg_table_desc* tables, uint32_t count, sg_lde** out_ldes,
+                          uint8_t* roots_out) {
+    SG_CHECK_ARG(c && (count == 0 || (tables && out_ldes)), "null argument");
+    SG_ENTER(ctx_of(c));
+    for (uint32_t i = 0; i < count; ++i) out_ldes[i] = nullptr;
+    if (count == 0) return SG_OK;
+    Ctx* ctx = C(c);
+    cudaStream_t st = (cudaStream_t)stream;
+    struct Held {
+        uint64_t* coef = nullptr;
+        uint64_t* tmp = nullptr;
+        uint64_t* w = nullptr;
+        uint64_t coef_b = 0, w_b = 0;
+    };
+    std::vector<Held> held(count);
+    std::vector<LdeJob> jobs(count);
+    uint8_t* d_roots = nullptr;
+    int rc = SG_OK;
+    for (uint32_t i = 0; i < count && rc == SG_OK; ++i) {
+        const sg_table_desc& d = tables[i];
+        SG_CHECK_ARG(d.trace && d.weights, "null trace or weights");
+        SG_CHECK_ARG(d.trace_on_device, "the fused batch commit takes device-resident traces");
+        SG_CHECK_ARG(d.n >= 2 && log2_exact(d.n) >= 0, "n must be a power of two >= 2");
+        SG_CHECK_ARG(d.blowup >= 1 && log2_exact(d.blowup) >= 0, "blowup must be a power of two");
+        SG_CHECK_ARG(d.row_u64 >= 1, "row width must be >= 1");
+        uint32_t R;
+        int le;
+        uint64_t c0, c1;
+        const sg_leaf_layout* lay = d.layout.rows_per_leaf ? &d.layout : nullptr;
+        SG_TRY(resolve_layout(lay, d.row_u64, &R, &le, &c0, &c1));
+        const uint64_t lde_rows = d.n * d.blowup;
+        SG_CHECK_ARG(lde_rows % R == 0, "rows_per_leaf must divide the LDE size");
+        SG_CHECK_ARG(d.row_u64 <= (~0ULL / 8) / lde_rows, "matrix size overflows 64 bits");
+    }
+    for (uint32_t i = 0; i < count && rc == SG_OK; ++i) {
+        const sg_table_desc& d = tables[i];
+        const uint64_t lde_rows = d.n * d.blowup;
+        const uint32_t R = d.layout.rows_per_leaf ? d.layout.rows_per_leaf : 2;
+        const uint64_t L = lde_rows / R;
+        sg_lde* h = new sg_lde();
+        h->lde_rows = lde_rows;
+        h->row_u64 = d.row_u64;
+        h->leaves_len = L;
+        out_ldes[i] = h;
+        rc = dev_alloc(ctx, st, lde_rows * d.row_u64 * 8, (void**)&h->d_lde);
+        if (rc == SG_OK) rc = dev_alloc(ctx, st, (2 * L - 1) * 32, (void**)&h->d_nodes);
+        Held& hd = held[i];
+        hd.coef_b = d.n * d.row_u64 * 8;
+        if (rc == SG_OK) rc = dev_alloc(ctx, st, hd.coef_b, (void**)&hd.coef);
+        if (rc == SG_OK && d.n > 4096) rc = dev_alloc(ctx, st, hd.coef_b, (void**)&hd.tmp);
+        const uint64_t* w = d.weights;
+        if (rc == SG_OK && !d.weights_on_device) {
+            hd.w_b = d.n * 8;
+            rc = dev_alloc(ctx, st, hd.w_b, (void**)&hd.w);
+            if (rc == SG_OK && cudaMemcpyAsync(hd.w, d.weights, hd.w_b, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+                set_error("fused batch commit: weights upload failed");
+                rc = SG_ERR_CUDA;
+            }
+            w = hd.w;
+        }
+        jobs[i] = LdeJob{d.trace, d.row_u64, d.n, d.row_u64, d.blowup, w, h->d_lde, d.row_u64, hd.coef, hd.tmp};
+    }
+    if (rc == SG_OK) rc = dev_alloc(ctx, st, 32ull * count, (void**)&d_roots);
+    // every table's LDE: one multi-table launch per pass group
+    if (rc == SG_OK) rc = lde_multi(ctx, st, jobs.data(), count);
+    for (uint32_t i = 0; i < count && rc == SG_OK; ++i) {
+        const sg_table_desc& d = tables[i];
+        sg_lde* h = out_ldes[i];
+        uint32_t R;
+        int le;
+        uint64_t c0, c1;
+        const sg_leaf_layout* lay = d.layout.rows_per_leaf ? &d.layout : nullptr;
+        rc = resolve_layout(lay, d.row_u64, &R, &le, &c0, &c1);
+        if (rc == SG_OK)
+            rc = leaves_row_major(ctx, st, h->d_lde, h->lde_rows, d.row_u64, c0, c1, R, le,
+                                  h->d_nodes + (h->leaves_len - 1) * 32);
+        if (rc == SG_OK) rc = merkle_inner(ctx, st, h->d_nodes, h->leaves_len);
+        if (rc == SG_OK &&
+            cudaMemcpyAsync(d_roots + 32ull * i, h->d_nodes, 32, cudaMemcpyDeviceToDevice, st) != cudaSuccess) {
+            set_error("fused batch commit: root copy failed");
+            rc = SG_ERR_CUDA;
+        }
+    }
+    std::vector<uint8_t> roots(32ull * count);
+    if (rc == SG_OK) {
+        cudaError_t e = cudaMemcpyAsync(roots.data(), d_roots, 32ull * count, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            set_error(std::string("fused batch commit: ") + cudaGetErrorString(e));
+            rc = SG_ERR_CUDA;
+        }
+    }
+    for (uint32_t i = 0; i < count; ++i) {
+        dev_free(ctx, st, held[i].coef, held[i].coef_b);
+        dev_free(ctx, st, held[i].tmp, held[i].coef_b);
+        dev_free(ctx, st, held[i].w, held[i].w_b);
+    }
+    dev_free(ctx, st, d_roots, 32ull * count);
+    if (rc != SG_OK) {
+        cudaStreamSynchronize(st);
+        for (uint32_t i = 0; i < count; ++i) {
+            sg_lde* h = out_ldes[i];
+            if (!h) continue;
+            dev_free(ctx, st, h->d_lde, h->lde_rows * h->row_u64 * 8);
+            dev_free(ctx, st, h->d_nodes, (2 * h->leaves_len - 1) * 32);
+            delete h;
+            out_ldes[i] = nullptr;
+        }
+        return rc;
+    }
+    for (uint32_t i = 0; i < count; ++i) {
+        memcpy(out_ldes[i]->root, roots.data() + 32ull * i, 32);
+        if (roots_out) memcpy(roots_out + 32ull * i, out_ldes[i]->root, 32);
+    }
+    return SG_OK;
+}
+
 void sg_lde_free_async(sg_ctx* c, void* stream, sg_lde* h) {
     if (!c || !h) return;
     Ctx* ctx = C(c);

@@ -183,6 +183,19 @@ int coset_lde(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t n, uint
 // u64, output rows of out_ld u64 (a column range of each, by pointer offset).
 int coset_lde_ld(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t trace_ld, uint64_t n, uint64_t m,
                  uint64_t blowup, const uint64_t* weights, uint64_t* out, uint64_t out_ld);
+// One table's LDE for lde_multi: its input, output and scratch (coef n x m,
+// tmp n x m when n > 4096).
+struct LdeJob {
+    const uint64_t* trace;
+    uint64_t trace_ld, n, m, blowup;
+    const uint64_t* weights;
+    uint64_t* out;
+    uint64_t out_ld;
+    uint64_t* coef;
+    uint64_t* tmp;
+};
+// The LDEs of many tables with one multi-table launch per pass group.
+int lde_multi(Ctx* ctx, cudaStream_t st, const LdeJob* jobs, uint32_t count);
 int leaves_row_major(Ctx* ctx, cudaStream_t st, const uint64_t* data, uint64_t num_rows, uint64_t row_u64,
                      uint64_t col_start, uint64_t col_end, uint32_t rows_per_leaf, int little_endian,
                      uint8_t* out);

@@ -28,6 +28,7 @@
 // c_i * w_{Bn}^{ij} (steps F1, F2). F1 writes its B outputs straight into the
 // LDE buffer at the rows F2 later reads and overwrites, so F2 runs in place and
 // the LDE needs no scratch beyond two n x m buffers.
+#include <algorithm>
 #include <utility>
 
 #include "common.cuh"
@@ -355,6 +356,78 @@ __global__ void __launch_bounds__(Plan<LOGL, C_>::T, Plan<LOGL, C_>::MINB)
     }
 }
 
+// Passes of many tables that share a tile length, width and direction, in one
+// persistent launch. Descriptor d owns the global tiles [first, first +
+// ntiles * ctiles); a CTA finds the descriptor of each tile it takes by binary
+// search and keeps its arguments in shared memory while it works on tiles of
+// the same descriptor (the grid walks descriptors in order, so a CTA switches
+// rarely). Small tables then share the persistent grid with large ones
+// instead of running as launches of a few CTAs each.
+struct PassDesc {
+    PassArgs a;
+    uint64_t ntiles;
+    uint64_t first;
+    uint32_t ctiles;
+};
+
+template <int LOGL, int C_, bool INV>
+__global__ void __launch_bounds__(Plan<LOGL, C_>::T, Plan<LOGL, C_>::MINB)
+    k_dft_multi(const PassDesc* __restrict__ descs, uint32_t count, uint64_t total) {
+    using PL = Plan<LOGL, C_>;
+    extern __shared__ uint64_t sm[];
+    __shared__ PassArgs sa;
+    uint64_t* S = sm;
+    uint64_t* WL = S + PL::S_WORDS;
+    uint64_t* F = WL + PL::WL_WORDS;
+    if constexpr (PL::NST > 1) {
+        // omega_{2^LOGL} is the same from every table's root table
+        const Tw tw = descs[0].a.tw;
+        for (uint32_t e = threadIdx.x; e < PL::L; e += PL::T) WL[e] = tw_root(tw, LOGL, e, INV);
+    }
+    uint32_t cur = count;  // the descriptor whose arguments are in `sa`
+    for (uint64_t t = blockIdx.x; t < total; t += gridDim.x) {
+        uint32_t lo = 0, hi = count;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) / 2;
+            if (descs[mid].first <= t)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        if (lo != cur) {
+            __syncthreads();  // every thread is done with the previous descriptor's arguments
+            if (threadIdx.x == 0) sa = descs[lo].a;
+            cur = lo;
+            __syncthreads();
+        }
+        const uint64_t lt = t - descs[lo].first;
+        const uint32_t ctiles = descs[lo].ctiles;
+        const uint64_t pt = lt / ctiles;
+        const uint64_t col0 = (lt % ctiles) * PL::C;
+        const uint32_t ncols = (uint32_t)min((uint64_t)PL::C, sa.m - col0);
+        for (uint32_t rep = 0; rep < sa.reps; ++rep) {
+            __syncthreads();  // the previous tile is done with S and F
+            tile_body<LOGL, C_, INV>(sa, S, WL, F, pt, col0, ncols, rep);
+        }
+    }
+}
+
+template <int LOGL, int C_, bool INV>
+static int launch_multi_dir(Ctx* ctx, cudaStream_t st, const PassDesc* d, uint32_t count, uint64_t total) {
+    using PL = Plan<LOGL, C_>;
+    KernelInfo ki;
+    SG_TRY(kernel_info((const void*)k_dft_multi<LOGL, C_, INV>, PL::SMEM, PL::T, &ki));
+    const uint64_t cap = (uint64_t)ki.sms * ki.blocks_per_sm;
+    k_dft_multi<LOGL, C_, INV><<<(unsigned)(total < cap ? total : cap), PL::T, PL::SMEM, st>>>(d, count, total);
+    return check_launch(ctx, "k_dft_multi");
+}
+
+template <int LOGL, int C_>
+static int launch_multi(Ctx* ctx, cudaStream_t st, bool inv, const PassDesc* d, uint32_t count, uint64_t total) {
+    return inv ? launch_multi_dir<LOGL, C_, true>(ctx, st, d, count, total)
+               : launch_multi_dir<LOGL, C_, false>(ctx, st, d, count, total);
+}
+
 template <int LOGL, int C_, bool INV>
 static int launch_dft_dir(Ctx* ctx, cudaStream_t st, const PassArgs& a, uint64_t ntiles) {
     using PL = Plan<LOGL, C_>;
@@ -414,6 +487,37 @@ static int launch_cols(Ctx* ctx, cudaStream_t st, const PassArgs& a, uint64_t nt
                                           : launch_dft<10, 16>(ctx, st, a, ntiles));
         case 11: return cols == 4 ? launch_dft<11, 4>(ctx, st, a, ntiles) : launch_dft<11, 8>(ctx, st, a, ntiles);
         case 12: return launch_dft<12, default_cols(12)>(ctx, st, a, ntiles);
+        default: set_error("dft pass longer than 4096 points"); return SG_ERR_UNSUPPORTED;
+    }
+}
+
+static int launch_multi_cols(Ctx* ctx, cudaStream_t st, uint32_t logL, int cols, bool inv, const PassDesc* d,
+                             uint32_t count, uint64_t total) {
+    switch (logL) {
+        case 0: return launch_multi<0, default_cols(0)>(ctx, st, inv, d, count, total);
+        case 1: return launch_multi<1, default_cols(1)>(ctx, st, inv, d, count, total);
+        case 2: return launch_multi<2, default_cols(2)>(ctx, st, inv, d, count, total);
+        case 3: return launch_multi<3, default_cols(3)>(ctx, st, inv, d, count, total);
+        case 4: return launch_multi<4, default_cols(4)>(ctx, st, inv, d, count, total);
+        case 5: return launch_multi<5, default_cols(5)>(ctx, st, inv, d, count, total);
+        case 6: return launch_multi<6, default_cols(6)>(ctx, st, inv, d, count, total);
+        case 7: return launch_multi<7, default_cols(7)>(ctx, st, inv, d, count, total);
+        case 8:
+            return cols == 4 ? launch_multi<8, 4>(ctx, st, inv, d, count, total)
+                             : (cols == 8 ? launch_multi<8, 8>(ctx, st, inv, d, count, total)
+                                          : launch_multi<8, 16>(ctx, st, inv, d, count, total));
+        case 9:
+            return cols == 4 ? launch_multi<9, 4>(ctx, st, inv, d, count, total)
+                             : (cols == 8 ? launch_multi<9, 8>(ctx, st, inv, d, count, total)
+                                          : launch_multi<9, 16>(ctx, st, inv, d, count, total));
+        case 10:
+            return cols == 4 ? launch_multi<10, 4>(ctx, st, inv, d, count, total)
+                             : (cols == 8 ? launch_multi<10, 8>(ctx, st, inv, d, count, total)
+                                          : launch_multi<10, 16>(ctx, st, inv, d, count, total));
+        case 11:
+            return cols == 4 ? launch_multi<11, 4>(ctx, st, inv, d, count, total)
+                             : launch_multi<11, 8>(ctx, st, inv, d, count, total);
+        case 12: return launch_multi<12, default_cols(12)>(ctx, st, inv, d, count, total);
         default: set_error("dft pass longer than 4096 points"); return SG_ERR_UNSUPPORTED;
     }
 }
@@ -695,10 +799,14 @@ int ntt_rows(Ctx* ctx, cudaStream_t st, uint64_t* d, uint64_t n, uint64_t m, int
 }
 
 // The LDE pass sequence over caller-provided scratch: coef (n x m) always,
-// tmp (n x m) when n > 4096.
-static int lde_passes(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t trace_ld, uint64_t n, uint64_t m,
-                      uint64_t blowup, const uint64_t* weights, uint64_t* out, uint64_t out_ld, const Tw& tw,
-                      uint64_t* coef, uint64_t* tmp) {
+// tmp (n x m) when n > 4096. Each pass goes to `emit(step, args, ntiles)`,
+// which runs it now (one table) or plans it for the multi-table launcher.
+// Steps 0..3 are I1, I2, F1, F2 (a single-pass LDE uses steps 1 and 3);
+// passes of one step of different tables never depend on each other.
+template <typename Emit>
+static int lde_passes_to(Emit&& emit, const uint64_t* trace, uint64_t trace_ld, uint64_t n, uint64_t m,
+                         uint64_t blowup, const uint64_t* weights, uint64_t* out, uint64_t out_ld, const Tw& tw,
+                         uint64_t* coef, uint64_t* tmp) {
     const int logn = log2_exact(n), logN = (int)tw.logN;
     if (logn <= 12) {
         PassArgs I = base_args(trace, coef, m, logn, true, tw);
@@ -707,7 +815,7 @@ static int lde_passes(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t
         I.out_ps = 1;
         I.post_kind = 2;
         I.weights = weights;
-        SG_TRY(run_pass(ctx, st, I, 1));
+        SG_TRY(emit(1, I, 1));
         PassArgs F = base_args(coef, out, m, logn, false, tw);
         F.out_ld = out_ld;
         F.in_ps = 1;
@@ -717,7 +825,7 @@ static int lde_passes(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t
         F.out_ps = blowup;
         F.out_rs = 1;
         F.canon_out = 1;
-        return run_pass(ctx, st, F, 1);
+        return emit(3, F, 1);
     }
     const uint32_t l1 = logn / 2, l2 = logn - l1;
     const uint64_t N1 = 1ULL << l1, N2 = 1ULL << l2;
@@ -729,7 +837,7 @@ static int lde_passes(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t
     I1.out_ps = N2;
     I1.post_kind = 1;
     I1.post_log = logn;
-    SG_TRY(run_pass(ctx, st, I1, N2));
+    SG_TRY(emit(0, I1, N2));
     PassArgs I2 = base_args(tmp, coef, m, l2, true, tw);
     I2.in_ts = N2;
     I2.in_ps = 1;
@@ -737,7 +845,7 @@ static int lde_passes(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t
     I2.out_ps = N1;
     I2.post_kind = 2;
     I2.weights = weights;
-    SG_TRY(run_pass(ctx, st, I2, N1));
+    SG_TRY(emit(1, I2, N1));
     PassArgs F1 = base_args(coef, out, m, l1, false, tw);
     F1.out_ld = out_ld;
     F1.in_ts = 1;
@@ -750,7 +858,7 @@ static int lde_passes(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t
     F1.out_ts = blowup * N1;
     F1.out_ps = blowup;
     F1.out_rs = 1;
-    SG_TRY(run_pass(ctx, st, F1, N2));
+    SG_TRY(emit(2, F1, N2));
     PassArgs F2 = base_args(out, out, m, l2, false, tw);
     F2.in_ld = out_ld;
     F2.out_ld = out_ld;
@@ -759,7 +867,14 @@ static int lde_passes(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t
     F2.out_ts = 1;
     F2.out_ps = blowup * N1;
     F2.canon_out = 1;
-    return run_pass(ctx, st, F2, N1 * blowup);
+    return emit(3, F2, N1 * blowup);
+}
+
+static int lde_passes(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t trace_ld, uint64_t n, uint64_t m,
+                      uint64_t blowup, const uint64_t* weights, uint64_t* out, uint64_t out_ld, const Tw& tw,
+                      uint64_t* coef, uint64_t* tmp) {
+    auto now = [&](int, const PassArgs& a, uint64_t ntiles) { return run_pass(ctx, st, a, ntiles); };
+    return lde_passes_to(now, trace, trace_ld, n, m, blowup, weights, out, out_ld, tw, coef, tmp);
 }
 
 int coset_lde(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t n, uint64_t m, uint64_t blowup,
@@ -793,6 +908,78 @@ int coset_lde_ld(Ctx* ctx, cudaStream_t st, const uint64_t* trace, uint64_t trac
     int rf2 = dev_free(ctx, st, coef, n * m * 8);
     if (rc != SG_OK) return rc;
     return rf != SG_OK ? rf : rf2;
+}
+
+// The LDEs of many tables, the passes of each step grouped by (tile length,
+// width, direction) into one multi-table launch each: 4 steps x a few
+// groups of launches for any number of tables. Every job brings its own
+// scratch (coef always, tmp when n > 4096) and its output buffer.
+int lde_multi(Ctx* ctx, cudaStream_t st, const LdeJob* jobs, uint32_t count) {
+    struct Planned {
+        int step, cols;
+        PassArgs a;
+        uint64_t ntiles;
+    };
+    std::vector<Planned> plan;
+    for (uint32_t i = 0; i < count; ++i) {
+        const LdeJob& j = jobs[i];
+        if (j.n == 0 || j.m == 0) continue;
+        const int logn = log2_exact(j.n), logB = log2_exact(j.blowup);
+        SG_CHECK_ARG(logn >= 0 && logB >= 0 && logn <= 24 && logn + logB <= 32, "LDE size out of range");
+        SG_CHECK_ARG(j.n <= 4096 || j.tmp, "a four-step LDE needs its tmp scratch");
+        Tw tw;
+        SG_TRY(ctx_tw(ctx, st, (uint32_t)(logn + logB), &tw));
+        auto record = [&](int step, const PassArgs& a, uint64_t ntiles) {
+            int cols = 0;
+            SG_TRY(pick_cols(ctx, st, a, ntiles, &cols));
+            plan.push_back({step, cols, a, ntiles});
+            return SG_OK;
+        };
+        SG_TRY(lde_passes_to(record, j.trace, j.trace_ld, j.n, j.m, j.blowup, j.weights, j.out, j.out_ld, tw, j.coef,
+                             j.tmp));
+    }
+    if (plan.empty()) return SG_OK;
+    std::stable_sort(plan.begin(), plan.end(), [](const Planned& x, const Planned& y) {
+        if (x.step != y.step) return x.step < y.step;
+        if (x.a.logL != y.a.logL) return x.a.logL < y.a.logL;
+        if (x.cols != y.cols) return x.cols < y.cols;
+        return x.a.inverse < y.a.inverse;
+    });
+    // one descriptor array for every group, uploaded once before any launch
+    std::vector<PassDesc> descs(plan.size());
+    struct Group {
+        size_t begin, end;
+        uint64_t total;
+    };
+    std::vector<Group> groups;
+    for (size_t i = 0; i < plan.size(); ++i) {
+        const Planned& p = plan[i];
+        if (groups.empty() || p.step != plan[groups.back().begin].step || p.a.logL != plan[groups.back().begin].a.logL ||
+            p.cols != plan[groups.back().begin].cols || p.a.inverse != plan[groups.back().begin].a.inverse)
+            groups.push_back({i, i, 0});
+        Group& g = groups.back();
+        const uint64_t ctiles = (p.a.m + (uint64_t)p.cols - 1) / (uint64_t)p.cols;
+        SG_CHECK_ARG(ctiles <= 0xffffffffULL, "too many columns");
+        descs[i] = PassDesc{p.a, p.ntiles, g.total, (uint32_t)ctiles};
+        g.total += p.ntiles * ctiles;
+        g.end = i + 1;
+    }
+    PassDesc* d_descs = nullptr;
+    const uint64_t bytes = descs.size() * sizeof(PassDesc);
+    SG_TRY(dev_alloc(ctx, st, bytes, (void**)&d_descs));
+    int rc = SG_OK;
+    if (cudaMemcpyAsync(d_descs, descs.data(), bytes, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+        set_error("multi-table DFT: descriptor upload failed");
+        rc = SG_ERR_CUDA;
+    }
+    for (const Group& g : groups) {
+        if (rc != SG_OK) break;
+        const Planned& p = plan[g.begin];
+        rc = launch_multi_cols(ctx, st, p.a.logL, p.cols, p.a.inverse != 0, d_descs + g.begin,
+                               (uint32_t)(g.end - g.begin), g.total);
+    }
+    const int rf = dev_free(ctx, st, d_descs, bytes);
+    return rc != SG_OK ? rc : rf;
 }
 
 }  // namespace sg

@@ -8,8 +8,9 @@ non-blocking CUDA stream, so small tables overlap on the device instead of
 running one after another behind host round trips; ctypes releases the GIL
 during every C-ABI call, so drivers run concurrently on the host too.
 
-R1 is one native call (sg_batch_commit): every table's LDE, leaves and tree,
-heaviest first over k internal streams. The protocol is unchanged: the roots
+R1 is one native call (sg_batch_commit_fused): every table's LDE passes run
+in shared multi-table DFT launches (one persistent launch per pass step,
+length, width and direction), then each table's leaves and tree. The protocol is unchanged: the roots
 are absorbed in table order, and every table's rounds 2-4 run on its own
 transcript fork, so the proof is identical to the sequential prover's.
 """
@@ -100,9 +101,12 @@ def stream_priority_range(be):
 
 
 def multi_prove_scheduled(airs, sources, opts=None, workers=8, budget_bytes=None, be=None,
-                          label=b"lambda_vm_b200/synthetic-multi-table", priority=None):
+                          label=b"lambda_vm_b200/synthetic-multi-table", priority=None, fused_r1=True):
     """Same proof as stark.multi_prove, with k concurrent table drivers (on
-    streams of CUDA priority `priority`, None: the default)."""
+    streams of CUDA priority `priority`, None: the default). R1 commits every
+    table at once: with fused_r1 (default) through sg_batch_commit_fused, whose
+    multi-table DFT launches cover all tables' passes, else sg_batch_commit's
+    per-table launches over `workers` streams."""
     opts = opts or Options()
     be = be or _backend()
     B, g = opts.blowup, opts.coset_offset
@@ -128,10 +132,11 @@ def multi_prove_scheduled(airs, sources, opts=None, workers=8, budget_bytes=None
     r1 = [None] * len(airs)
 
     try:
-        # R1: every table's trace, then one native batched commit (LDE + leaves
-        # + tree per table, heaviest first over `workers` streams).
+        # R1: every table's trace, then one native batched commit of all tables
+        # (LDEs in multi-table DFT launches, then leaves and trees).
         tms = [_gen_trace(r1b, air, src) for air, src in zip(airs, sources)]
-        committed = r1b.batch_commit(tms, B, [base.domain(a.log_n, B, g).weights for a in airs], workers)
+        committed = r1b.batch_commit(tms, B, [base.domain(a.log_n, B, g).weights for a in airs], workers,
+                                     fused=fused_r1)
         for i in range(len(airs)):
             lde, tree, root, release = committed[i]
             r1[i] = (tms[i], lde, tree, root, release)

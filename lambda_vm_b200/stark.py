@@ -240,17 +240,22 @@ class GpuBackend:
         native.check(self.L.sg_merkle_build(self.be.h, self.st, leaves, nl, tree.buf.ptr, root))
         return tree, bytes(root)
 
-    def batch_commit(self, mats, blowup, weights, concurrency=8):
+    def batch_commit(self, mats, blowup, weights, concurrency=8, fused=False):
         """Commit many main traces in one sg_batch_commit call (row-pair BE
-        leaves); returns [(lde Mat, Tree, root, release)] in table order, where
-        release() returns the LDE and tree memory on this backend's stream."""
+        leaves), or with fused=True in one sg_batch_commit_fused call (every
+        table's DFT passes in shared multi-table launches); returns [(lde Mat,
+        Tree, root, release)] in table order, where release() returns the LDE
+        and tree memory on this backend's stream."""
         n = len(mats)
         descs = (native.TableDesc * n)()
         for i, (m, w) in enumerate(zip(mats, weights)):
             descs[i] = native.TableDesc(m.ptr, 1, m.rows, m.cols, blowup, 1, w.ptr, native.LeafLayout(2, 0, 0, 0))
         handles = (C.c_void_p * n)()
         roots = (C.c_uint8 * (32 * n))()
-        native.check(self.L.sg_batch_commit(self.be.h, self.st, descs, n, concurrency, handles, roots))
+        if fused:
+            native.check(self.L.sg_batch_commit_fused(self.be.h, self.st, descs, n, handles, roots))
+        else:
+            native.check(self.L.sg_batch_commit(self.be.h, self.st, descs, n, concurrency, handles, roots))
         out = []
         for i in range(n):
             info = native.LdeInfo()

@@ -50,7 +50,7 @@ def test_probe_rule_restates_the_tile_chooser():
 @pytest.mark.skipif(not os.path.exists(CM.MODEL), reason="no committed model")
 def test_committed_model_beats_the_probe_on_heldout_shapes():
     params, meta = CM.load_model()
-    data = json.load(open(CM.DATASET))
+    data = CM.load_dataset()
     _, test = CM.split(data["records"])
     ev = CM.evaluate(test, params, data["probe"])
     assert ev["shapes"] >= 50

@@ -1,6 +1,7 @@
 """sg_batch_commit: many tables committed in one call (heaviest first over
 internal streams) give, table by table, exactly what sg_lde_commit gives for
-that table alone: the same root, LDE and node array."""
+that table alone: the same root, LDE and node array. sg_batch_commit_fused
+(every table's DFT passes in shared multi-table launches) gives the same."""
 import ctypes as C
 
 import numpy as np
@@ -40,11 +41,19 @@ def _single(be, tr, n, m, B, rpl, le):
     return bytes(root), lde, nodes
 
 
-@pytest.mark.parametrize("on_device", [False, True])
-def test_batch_commit_equals_single_commits(be, on_device):
+SHAPES = [(1 << 12, 7, 2, 2, 0), (1 << 6, 33, 4, 1, 1), (1 << 14, 20, 2, 2, 0), (4, 3, 8, 2, 0),
+          (1 << 10, 64, 2, 1, 1), (1 << 13, 1, 4, 2, 0), (1 << 9, 300, 2, 2, 0)]
+# many tables of shared and distinct pass lengths, widths 1..300, both
+# directions' tile widths, single-pass and four-step LDEs, odd and even log n
+FUSED_SHAPES = SHAPES + [(1 << 14, 9, 2, 2, 0), (1 << 14, 6, 2, 2, 0), (1 << 16, 40, 2, 2, 0), (1 << 15, 3, 4, 2, 0),
+                         (1 << 17, 12, 2, 2, 0), (1 << 20, 16, 2, 2, 0), (1 << 21, 5, 2, 2, 0), (1 << 11, 100, 2, 2, 0),
+                         (2, 4, 2, 2, 0), (1 << 18, 33, 4, 2, 0), (1 << 16, 40, 2, 2, 0)]
+
+
+@pytest.mark.parametrize("on_device,fused", [(False, False), (True, False), (True, True)])
+def test_batch_commit_equals_single_commits(be, on_device, fused):
     rng = np.random.default_rng(5)
-    shapes = [(1 << 12, 7, 2, 2, 0), (1 << 6, 33, 4, 1, 1), (1 << 14, 20, 2, 2, 0), (4, 3, 8, 2, 0),
-              (1 << 10, 64, 2, 1, 1), (1 << 13, 1, 4, 2, 0), (1 << 9, 300, 2, 2, 0)]
+    shapes = FUSED_SHAPES if fused else SHAPES
     tabs = _tables(rng, shapes)
     L = native.lib()
     keep = []
@@ -60,7 +69,10 @@ def test_batch_commit_equals_single_commits(be, on_device):
             descs[i] = native.TableDesc(tr.ctypes.data, 0, n, m, B, 0, w.ctypes.data, native.LeafLayout(rpl, le, 0, 0))
     handles = (C.c_void_p * len(tabs))()
     roots = (C.c_uint8 * (32 * len(tabs)))()
-    native.check(L.sg_batch_commit(be.h, None, descs, len(tabs), 3, handles, roots))
+    if fused:
+        native.check(L.sg_batch_commit_fused(be.h, None, descs, len(tabs), handles, roots))
+    else:
+        native.check(L.sg_batch_commit(be.h, None, descs, len(tabs), 3, handles, roots))
     for i, t in enumerate(tabs):
         root, lde, nodes = _single(be, *t)
         assert bytes(roots[32 * i:32 * i + 32]) == root
@@ -97,3 +109,8 @@ def test_batch_commit_rejects_bad_table_and_leaks_nothing(be):
     native.check(L.sg_stream_sync(be.h, None))
     after, _ = be.memory()
     assert after == before
+    # the fused form rejects host traces and bad shapes before allocating anything
+    rc = L.sg_batch_commit_fused(be.h, None, descs, 2, handles, None)
+    assert rc == native.SG_ERR_INVALID and not handles[0] and not handles[1]
+    native.check(L.sg_stream_sync(be.h, None))
+    assert be.memory()[0] == before

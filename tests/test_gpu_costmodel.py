@@ -54,7 +54,7 @@ def test_training_reduces_the_loss(be):
 
 @pytest.mark.skipif(not os.path.exists(CM.DATASET), reason="no committed pass timings")
 def test_model_trained_here_beats_the_probe_on_heldout_shapes(be):
-    data = json.load(open(CM.DATASET))
+    data = CM.load_dataset()
     train, test = CM.split(data["records"])
     X, y = CM.design(train)
     params, loss = CM.train(be, X, y)
