@@ -659,7 +659,7 @@ def main():
     # traffic grows in proportion to the columns (same passes, same tiles).
     traffic, traffic_src = None, None
     if dom == "lde" and a.log_n == 20 and B == 4:
-        traffic = round(2.08152e9 * m / 16)
+        traffic = round(2.0781e9 * m / 16)
         traffic_src = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the 4 k_dft launches of one "
                        "2^20 x 16 blowup-4 LDE, x m/16 (profiles/k_dft_coset_lde_1048576x16_blowup4.md)")
     achieved = alg[dom] / (med[dom] * 1e-3) / 1e9
@@ -670,8 +670,10 @@ def main():
                 "per_kernel_ms": {k: round(v, 3) for k, v in med.items()},
                 "per_kernel_gbs": {k: round(alg[k] / (med[k] * 1e-3) / 1e9, 1) for k in med},
                 "note": "Goldilocks butterflies and Keccak run on the INT pipes; see profiles/ for issue utilisation",
-                "int_pipes": {"issue_active_frac": 0.55, "alu_pipe_frac": 0.57, "fma_pipe_frac": 0.22,
-                              "source": "ncu, the 4 k_dft launches of a 2^20 x 16 blowup-4 LDE "
+                "int_pipes": {"issue_active_frac": 0.545, "alu_pipe_frac": 0.57, "fmaheavy_pipe_frac": 0.56,
+                              "fma_instr_frac": 0.22, "thread_instr_per_point": {"I1": 206, "I2": 203, "F1": 230,
+                                                                                  "F2": 181},
+                              "source": "ncu, the 4 k_dft launches of a 2^20 x 16 blowup-4 LDE, time-weighted "
                                         "(profiles/k_dft_coset_lde_1048576x16_blowup4.md)"}}
     value = world * n / (ms * 1e-3)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,

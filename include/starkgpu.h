@@ -219,10 +219,11 @@ SG_API int sg_batch_commit(sg_ctx* ctx, void* stream, const sg_table_desc* table
  * goes into one persistent multi-table DFT launch per (step, pass length,
  * tile width, direction), so small tables share the grid with large ones
  * instead of running as launches of a few CTAs (4 steps x a few launches in
- * all, against 4 per table). Leaves and trees follow per table on `stream`.
+ * all, against 4 per table). Each table's leaves and tree follow, heaviest
+ * first over `concurrency` streams that start when the LDEs are done.
  * Traces must be device-resident. Same handles and roots as sg_batch_commit. */
 SG_API int sg_batch_commit_fused(sg_ctx* ctx, void* stream, const sg_table_desc* tables, uint32_t count,
-                                 sg_lde** out_ldes, uint8_t* roots_out);
+                                 uint32_t concurrency, sg_lde** out_ldes, uint8_t* roots_out);
 
 /* ---- grinding: replaces grinding::generate_nonce_gpu (crypto/math-cuda/src/grinding.rs:29).
  *      inner_lanes: the 32-byte inner hash as four little-endian u64 lanes

@@ -761,8 +761,8 @@ int sg_batch_commit(sg_ctx* c, void* stream, const sg_table_desc* tables, uint32
     return SG_OK;
 }
 
-int sg_batch_commit_fused(sg_ctx* c, void* stream, const sg_table_desc* tables, uint32_t count, sg_lde** out_ldes,
-                          uint8_t* roots_out) {
+int sg_batch_commit_fused(sg_ctx* c, void* stream, const sg_table_desc* tables, uint32_t count, uint32_t concurrency,
+                          sg_lde** out_ldes, uint8_t* roots_out) {
     SG_CHECK_ARG(c && (count == 0 || (tables && out_ldes)), "null argument");
     SG_ENTER(ctx_of(c));
     for (uint32_t i = 0; i < count; ++i) out_ldes[i] = nullptr;
@@ -826,7 +826,37 @@ int sg_batch_commit_fused(sg_ctx* c, void* stream, const sg_table_desc* tables, 
     if (rc == SG_OK) rc = dev_alloc(ctx, st, 32ull * count, (void**)&d_roots);
     // every table's LDE: one multi-table launch per pass group
     if (rc == SG_OK) rc = lde_multi(ctx, st, jobs.data(), count);
-    for (uint32_t i = 0; i < count && rc == SG_OK; ++i) {
+    // then each table's leaves and tree, heaviest first over k streams that
+    // start after the LDEs (the hashing of small tables overlaps the large ones)
+    uint32_t k = concurrency == 0 ? 1 : (concurrency > 32 ? 32 : concurrency);
+    if (k > count) k = count;
+    std::vector<cudaStream_t> streams(k, nullptr);
+    std::vector<cudaEvent_t> done(k, nullptr);
+    cudaEvent_t lde_done = nullptr;
+    auto cuda_ok = [&](cudaError_t e, const char* what) {
+        if (e != cudaSuccess && rc == SG_OK) {
+            set_error(std::string("fused batch commit: ") + what + ": " + cudaGetErrorString(e));
+            rc = SG_ERR_CUDA;
+        }
+        return rc == SG_OK;
+    };
+    if (rc == SG_OK && cuda_ok(cudaEventCreateWithFlags(&lde_done, cudaEventDisableTiming), "event") &&
+        cuda_ok(cudaEventRecord(lde_done, st), "event record")) {
+        for (uint32_t s = 0; s < k && rc == SG_OK; ++s) {
+            if (!cuda_ok(new_stream_like(st, &streams[s]), "stream")) break;
+            if (!cuda_ok(cudaEventCreateWithFlags(&done[s], cudaEventDisableTiming), "event")) break;
+            cuda_ok(cudaStreamWaitEvent(streams[s], lde_done, 0), "stream wait");
+        }
+    }
+    std::vector<uint32_t> order(count);
+    for (uint32_t i = 0; i < count; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
+        return (double)tables[x].n * tables[x].blowup * tables[x].row_u64 >
+               (double)tables[y].n * tables[y].blowup * tables[y].row_u64;
+    });
+    for (uint32_t j = 0; j < count && rc == SG_OK; ++j) {
+        const uint32_t i = order[j];
+        cudaStream_t ss = streams[j % k];
         const sg_table_desc& d = tables[i];
         sg_lde* h = out_ldes[i];
         uint32_t R;
@@ -835,13 +865,21 @@ int sg_batch_commit_fused(sg_ctx* c, void* stream, const sg_table_desc* tables, 
         const sg_leaf_layout* lay = d.layout.rows_per_leaf ? &d.layout : nullptr;
         rc = resolve_layout(lay, d.row_u64, &R, &le, &c0, &c1);
         if (rc == SG_OK)
-            rc = leaves_row_major(ctx, st, h->d_lde, h->lde_rows, d.row_u64, c0, c1, R, le,
+            rc = leaves_row_major(ctx, ss, h->d_lde, h->lde_rows, d.row_u64, c0, c1, R, le,
                                   h->d_nodes + (h->leaves_len - 1) * 32);
-        if (rc == SG_OK) rc = merkle_inner(ctx, st, h->d_nodes, h->leaves_len);
-        if (rc == SG_OK &&
-            cudaMemcpyAsync(d_roots + 32ull * i, h->d_nodes, 32, cudaMemcpyDeviceToDevice, st) != cudaSuccess) {
-            set_error("fused batch commit: root copy failed");
-            rc = SG_ERR_CUDA;
+        if (rc == SG_OK) rc = merkle_inner(ctx, ss, h->d_nodes, h->leaves_len);
+        if (rc == SG_OK)
+            cuda_ok(cudaMemcpyAsync(d_roots + 32ull * i, h->d_nodes, 32, cudaMemcpyDeviceToDevice, ss), "root copy");
+    }
+    // join: `st` waits for every hashing stream
+    for (uint32_t s = 0; s < k; ++s) {
+        if (streams[s] && done[s]) {
+            cudaError_t e = cudaEventRecord(done[s], streams[s]);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(st, done[s], 0);
+            if (e != cudaSuccess) {
+                cudaStreamSynchronize(streams[s]);
+                cuda_ok(e, "join");
+            }
         }
     }
     std::vector<uint8_t> roots(32ull * count);
@@ -853,6 +891,14 @@ int sg_batch_commit_fused(sg_ctx* c, void* stream, const sg_table_desc* tables, 
             rc = SG_ERR_CUDA;
         }
     }
+    for (uint32_t s = 0; s < k; ++s) {
+        if (streams[s]) {
+            if (rc != SG_OK) cudaStreamSynchronize(streams[s]);
+            cudaStreamDestroy(streams[s]);
+        }
+        if (done[s]) cudaEventDestroy(done[s]);
+    }
+    if (lde_done) cudaEventDestroy(lde_done);
     for (uint32_t i = 0; i < count; ++i) {
         dev_free(ctx, st, held[i].coef, held[i].coef_b);
         dev_free(ctx, st, held[i].tmp, held[i].coef_b);

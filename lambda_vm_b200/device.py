@@ -22,6 +22,7 @@ class Backend:
         native.check(L.sg_ctx_create(device, budget_bytes, C.byref(h)))
         self.h = h
         self.device = device
+        self.pass_model = None  # parameters of the installed DFT pass-cost model, if any
 
     def memory(self):
         a, b = C.c_uint64(), C.c_uint64()
@@ -47,11 +48,20 @@ class Backend:
 
 
 def backend(device: int = 0) -> Backend:
-    """Process-wide context for `device` (device::backend())."""
+    """Process-wide context for `device` (device::backend()). The committed
+    DFT pass-cost model (costmodel.py) chooses its tile widths, unless the
+    environment sets SG_PASS_MODEL=0 (the timing probe then decides)."""
+    import os
     with _lock:
         b = _backends.get(device)
         if b is None:
             b = Backend(device)
+            if os.environ.get("SG_PASS_MODEL", "1") != "0":
+                from . import costmodel
+                if os.path.exists(costmodel.MODEL):
+                    params, _ = costmodel.load_model()
+                    costmodel.install(b, params)
+                    b.pass_model = params
             _backends[device] = b
         return b
 

@@ -126,7 +126,7 @@ PROTOTYPES = {
     "sg_fri_free": (None, [vp]),
     "sg_field_ops": (i32, [vp, vp, u32, vp, vp, vp, u64]),
     "sg_batch_commit": (i32, [vp, vp, vp, u32, u32, vp, vp]),
-    "sg_batch_commit_fused": (i32, [vp, vp, vp, u32, vp, vp]),
+    "sg_batch_commit_fused": (i32, [vp, vp, vp, u32, u32, vp, vp]),
     "sg_table_proof_shape": (i32, [vp, vp]),
     "sg_ctx_dft_tiles": (i32, [vp, u32, u32]),
     "sg_ctx_dft_tuning": (i32, [vp, vp, u32, vp, vp, vp]),

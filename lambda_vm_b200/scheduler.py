@@ -118,10 +118,11 @@ def multi_prove_scheduled(airs, sources, opts=None, workers=8, budget_bytes=None
         r1_stream = s.value
     for air in airs:  # warm the domain caches serially on the legacy stream
         base.domain(air.log_n, B, g)
-    # time the DFT tile widths now, while nothing else runs, rather than
-    # inside the first concurrent pass (a no-op once the context has them)
+    # without a pass-cost model, time the DFT tile widths now, while nothing
+    # else runs, rather than inside the first concurrent pass (a no-op once
+    # the context has them)
     cols, cost, cnt = (C.c_uint32 * 4)(), (C.c_float * 4)(), C.c_uint32()
-    for log_len in range(8, 12):
+    for log_len in range(8, 12) if getattr(be, "pass_model", None) is None else ():
         native.check(native.lib().sg_ctx_dft_tuning(be.h, None, log_len, cols, cost, C.byref(cnt)))
     native.check(native.lib().sg_stream_sync(be.h, None))
     pool = StreamPool(be, workers, priority)

@@ -108,20 +108,23 @@ class ProofServer:
     soon as a slot and memory are free, also past a large job that waits for
     the running one (backfilling): they keep one slot and the waiting job's
     memory free, so the large job still starts the moment the running large
-    job ends. Large jobs get `drivers` table drivers on streams of the
-    device's most urgent priority, small jobs at most `small_drivers` on
-    default-priority streams, so a small proof fills gaps in a large one
-    instead of lengthening it.
+    job ends. While a large job runs, at most `beside_big` small jobs run
+    beside it, which bounds how much they can stretch it; with no large job
+    running, small jobs use every slot. Large jobs get `drivers` table drivers
+    on streams of the device's most urgent priority, small jobs at most
+    `small_drivers` on default-priority streams, so a small proof fills gaps in
+    a large one instead of lengthening it.
     """
 
     def __init__(self, budget_bytes, max_jobs=4, drivers=4, opts=None, prove_fn=None, be=None, policy="backfill",
-                 big_cells=1 << 23, small_drivers=2):
+                 big_cells=1 << 23, small_drivers=2, beside_big=1):
         if policy not in ("fifo", "backfill"):
             raise ValueError(f"unknown admission policy {policy!r}")
         self.opts = opts or Options()
         self.max_jobs = max_jobs
         self.drivers = drivers
         self.small_drivers = small_drivers
+        self.beside_big = beside_big
         self.policy = policy
         self.big_cells = big_cells if policy == "backfill" else None
         self.gate = VramGate(budget_bytes)
@@ -167,6 +170,13 @@ class ProofServer:
         g = self.gate
         return g.used == 0 or g.used + job.est + reserve <= g.budget
 
+    def _can_start(self, job, reserve=0):
+        if not self._fits(job, reserve):
+            return False
+        if job.big:
+            return not self.big_running
+        return not self.big_running or self.running - self.big_running < self.beside_big
+
     def _pick(self):
         """The queued job to start now, or None (called with the lock held)."""
         if not self.queue or self.running >= self.max_jobs:
@@ -174,14 +184,14 @@ class ProofServer:
         if self.policy == "fifo":
             return self.queue[0] if self._fits(self.queue[0]) else None
         head = self.queue[0]
-        if self._fits(head) and not (head.big and self.big_running):
+        if self._can_start(head):
             return head
         # The head waits (a large job behind the running large one, or memory):
         # a small job may pass it if it leaves the head a slot and its memory.
         if self.running >= self.max_jobs - 1:
             return None
         for j in list(self.queue)[1:]:
-            if not j.big and self._fits(j, reserve=head.est):
+            if not j.big and self._can_start(j, reserve=head.est):
                 return j
         return None
 
@@ -253,7 +263,7 @@ def warm_context(be, job_specs, opts):
     for log_n in sorted({a.log_n for airs, _ in job_specs for a in airs}):
         bk.domain(log_n, opts.blowup, opts.coset_offset)
     cols, cost, cnt = (C.c_uint32 * 4)(), (C.c_float * 4)(), C.c_uint32()
-    for log_len in range(8, 12):
+    for log_len in range(8, 12) if getattr(be, "pass_model", None) is None else ():
         native.check(native.lib().sg_ctx_dft_tuning(be.h, None, log_len, cols, cost, C.byref(cnt)))
     native.check(native.lib().sg_stream_sync(be.h, None))
 

@@ -253,7 +253,7 @@ class GpuBackend:
         handles = (C.c_void_p * n)()
         roots = (C.c_uint8 * (32 * n))()
         if fused:
-            native.check(self.L.sg_batch_commit_fused(self.be.h, self.st, descs, n, handles, roots))
+            native.check(self.L.sg_batch_commit_fused(self.be.h, self.st, descs, n, concurrency, handles, roots))
         else:
             native.check(self.L.sg_batch_commit(self.be.h, self.st, descs, n, concurrency, handles, roots))
         out = []

@@ -70,7 +70,7 @@ def test_batch_commit_equals_single_commits(be, on_device, fused):
     handles = (C.c_void_p * len(tabs))()
     roots = (C.c_uint8 * (32 * len(tabs)))()
     if fused:
-        native.check(L.sg_batch_commit_fused(be.h, None, descs, len(tabs), handles, roots))
+        native.check(L.sg_batch_commit_fused(be.h, None, descs, len(tabs), 4, handles, roots))
     else:
         native.check(L.sg_batch_commit(be.h, None, descs, len(tabs), 3, handles, roots))
     for i, t in enumerate(tabs):
@@ -110,7 +110,7 @@ def test_batch_commit_rejects_bad_table_and_leaks_nothing(be):
     after, _ = be.memory()
     assert after == before
     # the fused form rejects host traces and bad shapes before allocating anything
-    rc = L.sg_batch_commit_fused(be.h, None, descs, 2, handles, None)
+    rc = L.sg_batch_commit_fused(be.h, None, descs, 2, 2, handles, None)
     assert rc == native.SG_ERR_INVALID and not handles[0] and not handles[1]
     native.check(L.sg_stream_sync(be.h, None))
     assert be.memory()[0] == before

@@ -165,3 +165,21 @@ def test_fifo_policy_keeps_arrival_order():
     assert all(v[3] == 3 for v in rec.spans.values())
     with pytest.raises(ValueError):
         ProofServer(budget_bytes=1, prove_fn=rec, policy="lifo")
+
+
+def test_at_most_beside_big_small_jobs_run_beside_a_large_one():
+    big = _spec(0, 14, 300)[0]
+    from lambda_vm_b200.serving import job_cells
+    cut = job_cells(big)
+    rec = SizedRecorder(cut)
+    with ProofServer(budget_bytes=1 << 40, max_jobs=4, drivers=4, prove_fn=rec, big_cells=cut,
+                     beside_big=1) as srv:
+        srv.submit(big, [0])
+        for i in range(1, 7):
+            srv.submit(_spec(0, 10, 8)[0], [i])
+        srv.drain()
+    a = rec.spans[0]
+    smalls = [rec.spans[i] for i in range(1, 7)]
+    # while the large job ran, the small jobs beside it never overlapped one another
+    during = sorted((max(s, a[0]), min(e, a[1])) for s, e, _, _ in smalls if s < a[1] and e > a[0])
+    assert during and all(x[1] <= y[0] + 1e-3 for x, y in zip(during, during[1:]))
