@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--no-serve-summary", action="store_true",
                     help="skip the serving summary the default line carries at N = 1")
     ap.add_argument("--tables", type=int, default=40)
+    ap.add_argument("--host-verify", action="store_true",
+                    help="proof: also verify the benchmarked proof entirely on the host (slow) and time it")
     ap.add_argument("--max-log-n", type=int, default=22)
     ap.add_argument("--workers", type=int, default=8)
     ap.add_argument("--cpu-sample-log-n", type=int, default=None,
@@ -270,7 +272,8 @@ def proof_summary(a, steps=5, warmup=2):
                 "scheduled_ms_per_proof": round(line["scheduled"]["ms_per_proof"], 1),
                 "scheduled_rows_per_s": round(line["value"], 1),
                 "scheduled_over_plain": round(line["scheduled_over_plain"], 3),
-                "identical_proofs": line["identical_proofs"], "verified": line["verified"]}
+                "identical_proofs": line["identical_proofs"], "verified": line["verified"],
+                "verify_ms": line["verify_ms_gpu_queries"]}
     out = one(a.max_log_n)
     # The same number of tables, all small (2^10..2^14 rows, as most chip
     # tables of a real VM proof are): per-table launches and Fiat-Shamir
@@ -318,13 +321,21 @@ def measure_proof(a):
     res = {f: {"s_per_proof": statistics.median(times[f]), "all_ms": [round(x * 1e3, 1) for x in times[f]]}
            for f in times}
     # The benchmarked proofs themselves: the two forms' serialized proofs are
-    # compared byte for byte, and the library's verifier checks one of them.
+    # compared byte for byte, and the library's verifier checks one of them
+    # (transcript replay on the host, every query on the GPU in one launch;
+    # with --host-verify also entirely on the host, for comparison).
     from lambda_vm_b200.proof_io import serialize
     from lambda_vm_b200.verifier import verify
     same = serialize(last["plain"]) == serialize(last["scheduled"])
+    verify(airs, last["scheduled"], opts, device=be)  # warm
     tv = time.perf_counter()
-    verdict = verify(airs, last["scheduled"], opts)
+    verdict = verify(airs, last["scheduled"], opts, device=be)
     verify_s = time.perf_counter() - tv
+    host = None
+    if getattr(a, "host_verify", False):
+        tv = time.perf_counter()
+        hv = verify(airs, last["scheduled"], opts)
+        host = {"verified": hv[0] is True, "verify_s": round(time.perf_counter() - tv, 2)}
     del last
     line = {"metric": "proved cycles/s (multi-table proof, trace rows proved per second)",
             "value": rows / res["scheduled"]["s_per_proof"], "unit": "rows/s", "n_gpus": 1, "steps": a.steps,
@@ -340,7 +351,9 @@ def measure_proof(a):
                           "ms_per_proof": res["scheduled"]["s_per_proof"] * 1e3, "all_ms": res["scheduled"]["all_ms"]},
             "scheduled_over_plain": res["plain"]["s_per_proof"] / res["scheduled"]["s_per_proof"],
             "identical_proofs": same, "verified": verdict[0] is True, "verify_result": verdict[1],
-            "verify_s": round(verify_s, 2)}
+            "verify_ms_gpu_queries": round(verify_s * 1e3, 1)}
+    if host is not None:
+        line["host_verify"] = host
     return line
 
 

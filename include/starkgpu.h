@@ -487,6 +487,42 @@ SG_API int sg_field_ops(sg_ctx* ctx, void* stream, uint32_t op, const uint64_t* 
 SG_API int sg_synth_trace(sg_ctx* ctx, void* stream, uint64_t* d_out, uint64_t n, uint64_t w, uint64_t seed,
                           uint32_t k_checksum);
 
+/* ---- batched proof verification on the GPU: the query phase of
+ *      crypto/stark/src/verifier.rs (multi_verify, :1178-1430) for many tables
+ *      of many proofs in one launch, one thread per (table, query). The host
+ *      replays each table's transcript first (challenges, the composition
+ *      identity at z, grinding, the query indexes) and passes the values below;
+ *      the kernel checks, per query: the main, aux and composition openings'
+ *      Merkle paths (row-pair big-endian leaves), the DEEP values at both
+ *      opened rows, every FRI layer's opened value and path, and the terminal
+ *      polynomial. Ext3 constants are 3 u64 each; every pointer inside the
+ *      descriptor is a device pointer. status_out (host) gets one word per
+ *      (table, query) in order: 0 = accepted, else code | layer << 8 with code
+ *      1 main path, 2 aux path, 3 composition path, 4 FRI value, 5 FRI path,
+ *      6 terminal polynomial. ---- */
+typedef struct {
+    uint32_t log_n, log_N;         /* trace and LDE sizes, log2 */
+    uint32_t m, aux_cols;          /* main columns (base), aux columns (ext3) */
+    uint32_t queries, fri_layers;  /* committed FRI layers */
+    uint32_t total_folds, terminal_log, num_coeffs, pad_;
+    uint64_t coset_offset, omega_N, terminal_offset, omega_T;
+    /* ext3 constants, packed: z, z*w, z^2, gh[2], pood[2], gt[2*(m+A)] (column
+     * major: gt[2j+k]), tood[2][m+A] (point major), zetas[total_folds], coeffs */
+    const uint64_t* consts;
+    const uint8_t* roots;          /* main, aux, composition, then fri_layers roots, 32 bytes each */
+    const uint64_t* iotas;         /* queries */
+    const uint64_t* open_main;     /* 2Q x m */
+    const uint64_t* open_aux;      /* 2Q x 3A */
+    const uint64_t* open_parts;    /* 2Q x 6 */
+    const uint8_t* path_main;      /* Q x (log_N - 1) x 32, leaf first */
+    const uint8_t* path_aux;
+    const uint8_t* path_parts;
+    const uint64_t* fri_open;      /* fri_layers x 2Q x 3 */
+    const uint8_t* fri_paths;      /* layer after layer: Q x (log_N - 2 - l) x 32 */
+} sg_verify_table;
+SG_API int sg_verify_queries(sg_ctx* ctx, void* stream, const sg_verify_table* tables, uint32_t count,
+                             uint32_t* status_out);
+
 /* ---- DFT pass log: the autotuner's measurements. No counterpart in the
  *      reference (its NTT has one fixed plan). While enabled, every DFT pass
  *      launched through the context is bracketed by CUDA events; _read waits for

@@ -35,6 +35,17 @@ class PassRecord(C.Structure):
                 ("tiles", C.c_uint64), ("m", C.c_uint64), ("ms", C.c_float), ("pad2_", C.c_float)]
 
 
+class VerifyTable(C.Structure):
+    _fields_ = [("log_n", C.c_uint32), ("log_N", C.c_uint32), ("m", C.c_uint32), ("aux_cols", C.c_uint32),
+                ("queries", C.c_uint32), ("fri_layers", C.c_uint32), ("total_folds", C.c_uint32),
+                ("terminal_log", C.c_uint32), ("num_coeffs", C.c_uint32), ("pad_", C.c_uint32),
+                ("coset_offset", C.c_uint64), ("omega_N", C.c_uint64), ("terminal_offset", C.c_uint64),
+                ("omega_T", C.c_uint64), ("consts", C.c_void_p), ("roots", C.c_void_p), ("iotas", C.c_void_p),
+                ("open_main", C.c_void_p), ("open_aux", C.c_void_p), ("open_parts", C.c_void_p),
+                ("path_main", C.c_void_p), ("path_aux", C.c_void_p), ("path_parts", C.c_void_p),
+                ("fri_open", C.c_void_p), ("fri_paths", C.c_void_p)]
+
+
 class LdeInfo(C.Structure):
     _fields_ = [("d_lde", C.c_void_p), ("lde_rows", C.c_uint64), ("row_u64", C.c_uint64),
                 ("d_nodes", C.c_void_p), ("leaves_len", C.c_uint64), ("root", C.c_uint8 * 32)]
@@ -158,6 +169,7 @@ PROTOTYPES = {
     "sg_decompose_d2": (i32, [vp, vp, vp, u64, vp, vp]),
     "sg_synth_trace": (i32, [vp, vp, vp, u64, u64, u64, u32]),
     "sg_ctx_pass_log": (i32, [vp, i32]),
+    "sg_verify_queries": (i32, [vp, vp, C.POINTER(VerifyTable), u32, vp]),
     "sg_ctx_pass_log_read": (i32, [vp, C.POINTER(PassRecord), u32, C.POINTER(u32)]),
     "sg_mlp_loss_grad": (i32, [vp, vp, vp, vp, u32, vp, vp, vp]),
     "sg_mlp_train": (i32, [vp, vp, vp, vp, u32, vp, u32, C.c_float, C.POINTER(C.c_float)]),
