@@ -44,10 +44,12 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-proof-summary", action="store_true",
                     help="skip the multi-table proof summary the default line carries at N = 1")
-    ap.add_argument("--workload", default="commit", choices=["commit", "proof", "serve", "rounds"],
+    ap.add_argument("--workload", default="commit", choices=["commit", "proof", "serve", "rounds", "vm"],
                     help="commit: LDE + Merkle commit of one trace (default); proof: multi-table proof, plain vs "
                          "scheduled; serve: Poisson stream of proof jobs, concurrent admission vs one at a time; "
-                         "rounds: the round-2..4 kernels of one large table, one by one")
+                         "rounds: the round-2..4 kernels of one large table, one by one; vm: the Fibonacci RV64 "
+                         "guest executed and its execution proved")
+    ap.add_argument("--fib-n", type=int, default=30000, help="vm: Fibonacci loop iterations (5 cycles each)")
     ap.add_argument("--rates", default="2,5,10,20,50,100", help="serve: arrival rates (jobs/s)")
     ap.add_argument("--jobs", type=int, default=40, help="serve: jobs per rate")
     ap.add_argument("--job-max-log-n", type=int, default=18, help="serve: largest job height (log2 cycles)")
@@ -450,6 +452,52 @@ def serve_summary(a):
                        "all_proved": s["all_proved"]} for s in line["sweep"]]}
 
 
+def measure_vm(a, steps=3, warmup=1):
+    """The Fibonacci RV64 guest (add/mv/mv/addi/bnez loop, n iterations):
+    execute it, build its CPU and RANGE tables, prove the execution on the GPU
+    (blowup 2, 128-bit security, grinding 20), verify. Proved cycles/s =
+    executed instructions / wall time of execute + tables + prove."""
+    import torch
+    from lambda_vm_b200 import rv64
+    from lambda_vm_b200 import rv64_air as RA
+    from lambda_vm_b200.device import backend
+    from lambda_vm_b200.stark import GpuBackend, Options, multi_prove
+    be = backend(0)
+    opts = Options(blowup=2, grinding=20, final_log_degree=5)
+    words = rv64.fib_program(a.fib_n)
+    tb, tp = [], []
+    for it in range(warmup + steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        airs, traces, pub = RA.build(words)
+        t1 = time.perf_counter()
+        proof = multi_prove(airs, traces, opts, GpuBackend(be), label=pub["label"])
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        if it >= warmup:
+            tb.append(t1 - t0)
+            tp.append(t2 - t1)
+    tv = time.perf_counter()
+    verdict = RA.verify(words, pub["counts"], pub["output"], proof, opts, device=be)
+    verify_s = time.perf_counter() - tv
+    b_s, p_s = statistics.median(tb), statistics.median(tp)
+    cyc = pub["cycles"]
+    return {"metric": "proved cycles/s (RV64 Fibonacci guest: execute + trace tables + prove)",
+            "value": cyc / (b_s + p_s), "unit": "cycles/s", "cycles": cyc,
+            "workload": f"Fibonacci guest, {a.fib_n} iterations, {cyc} cycles; CPU table 2^{airs[0].log_n} x "
+                        f"{airs[0].width}, RANGE table 2^16 x 3; blowup 2, {opts.queries} queries, grinding 20",
+            "execute_and_tables_ms": round(b_s * 1e3, 1), "prove_ms": round(p_s * 1e3, 1),
+            "prove_only_cycles_per_s": round(cyc / p_s, 1), "output_ok": pub["output"] == rv64.fib_reference(a.fib_n),
+            "verified": verdict[0] is True, "verify_ms": round(verify_s * 1e3, 1)}
+
+
+def run_vm(a):
+    line = measure_vm(a)
+    line.update({"n_gpus": 1, "steps": 3, "warmup": 1, "higher_is_better": True, "scaling": "weak",
+                 "vs_baseline": None, "dtype": "u64 (Goldilocks) / Fp3", "data": "generated RV64 guest"})
+    print(json.dumps(line), flush=True)
+
+
 def run_rounds(a):
     """The round-2..4 kernels of one large table, each timed alone with CUDA
     events (median of `steps` after `warmup`): the DEEP denominators'
@@ -524,6 +572,9 @@ def main():
         return
     if a.workload == "rounds" and a.impl == "ours":
         run_rounds(a)
+        return
+    if a.workload == "vm" and a.impl == "ours":
+        run_vm(a)
         return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -711,6 +762,11 @@ def main():
             line["proof_workload"] = proof_summary(a)
         except Exception as e:  # noqa: BLE001
             line["proof_workload"] = {"error": f"{type(e).__name__}: {e}"}
+    if world == 1 and not a.no_proof_summary:
+        try:
+            line["vm_workload"] = measure_vm(a)
+        except Exception as e:  # noqa: BLE001
+            line["vm_workload"] = {"error": f"{type(e).__name__}: {e}"}
     if world == 1 and not a.no_serve_summary:
         try:
             line["serving"] = serve_summary(a)

@@ -115,10 +115,25 @@ def eval_ood(prog, frame, rap, alpha, offset):
     return [v[r] for r in prog["roots"]]
 
 
-def verify(airs, proof, opts, label=b"lambda_vm_b200/synthetic-multi-table", device=None):
+def public_sum(terms, z, apows):
+    """The verifier's side of LogUp buses with public content (a program's
+    instructions and execution counts, a claimed output): sum of m / (z -
+    (bus + sum_i alpha^(i+1) v_i)) over (bus, values, signed m) terms."""
+    s = (0, 0, 0)
+    for bus, vals, m in terms:
+        fp = sub(z, (bus % P, 0, 0))
+        for i, v in enumerate(vals):
+            fp = sub(fp, scale(apows[i + 1], int(v)))
+        s = add(s, scale(finv(fp), m % P))
+    return s
+
+
+def verify(airs, proof, opts, label=b"lambda_vm_b200/synthetic-multi-table", device=None, public_terms=()):
     """Verify a multi-table proof: (ok, reason). With `device` (a context from
-    device.backend()) the query phase runs on the GPU (sg_verify_queries)."""
-    ok, reason, prep = _replay(airs, proof, opts, label)
+    device.backend()) the query phase runs on the GPU (sg_verify_queries).
+    `public_terms` are bus terms whose content the statement fixes
+    (public_sum); they join the tables' contributions in the bus balance."""
+    ok, reason, prep = _replay(airs, proof, opts, label, public_terms)
     if not ok:
         return ok, reason
     if device is not None:
@@ -130,7 +145,7 @@ def verify(airs, proof, opts, label=b"lambda_vm_b200/synthetic-multi-table", dev
     return True, "ok"
 
 
-def _replay(airs, proof, opts, label):
+def _replay(airs, proof, opts, label, public_terms=()):
     """Transcript replay and every check that needs it (bus balance, the
     composition identity at z, FRI layer count, terminal length, grinding,
     query indexes); returns (ok, reason, per-table values for the query phase)."""
@@ -143,7 +158,7 @@ def _replay(airs, proof, opts, label):
     apows = [(1, 0, 0)]
     for _ in range(max(a.max_alpha for a in airs) - 1):
         apows.append(mul(apows[-1], alpha))
-    total = (0, 0, 0)
+    total = public_sum(public_terms, ch[0], apows)
     for tp in tabs:
         total = add(total, f3(tp["table_contribution"]))
     if total != (0, 0, 0):
@@ -373,12 +388,15 @@ def verify_queries_gpu(preps, be):
 
 
 def verify_many(items, opts, be, label=b"lambda_vm_b200/synthetic-multi-table"):
-    """Batched verification: [(airs, proof)] -> [(ok, reason)]; every proof's
-    transcript is replayed on the host, then all their queries are checked in
-    one GPU launch."""
+    """Batched verification: [(airs, proof)] or [(airs, proof, label,
+    public_terms)] -> [(ok, reason)]; every proof's transcript is replayed on
+    the host, then all their queries are checked in one GPU launch."""
     results, preps, idx = [], [], []
-    for airs, proof in items:
-        ok, reason, prep = _replay(airs, proof, opts, label)
+    for item in items:
+        airs, proof = item[0], item[1]
+        lab = item[2] if len(item) > 2 else label
+        pub = item[3] if len(item) > 3 else ()
+        ok, reason, prep = _replay(airs, proof, opts, lab, pub)
         results.append((ok, reason))
         if ok:
             idx.append(len(results) - 1)

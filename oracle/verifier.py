@@ -110,7 +110,20 @@ def eval_ood(prog, frame, rap, alpha, offset):
     return [v[r] for r in prog["roots"]]
 
 
-def verify(airs, proof, opts, label=b"lambda_vm_b200/synthetic-multi-table"):
+def public_sum(terms, z, apows):
+    """The verifier's side of LogUp buses with public content (a program's
+    instructions and execution counts, a claimed output): sum of m / (z -
+    (bus + sum_i alpha^(i+1) v_i)) over (bus, values, signed m) terms."""
+    s = (0, 0, 0)
+    for bus, vals, m in terms:
+        fp = sub(z, (bus % P, 0, 0))
+        for i, v in enumerate(vals):
+            fp = sub(fp, scale(apows[i + 1], int(v)))
+        s = add(s, scale(finv(fp), m % P))
+    return s
+
+
+def verify(airs, proof, opts, label=b"lambda_vm_b200/synthetic-multi-table", public_terms=()):
     T = O.Transcript(label)
     tabs = proof["tables"]
     for tp in tabs:
@@ -120,7 +133,7 @@ def verify(airs, proof, opts, label=b"lambda_vm_b200/synthetic-multi-table"):
     apows = [(1, 0, 0)]
     for _ in range(max(a.max_alpha for a in airs) - 1):
         apows.append(mul(apows[-1], alpha))
-    total = (0, 0, 0)
+    total = public_sum(public_terms, ch[0], apows)
     for tp in tabs:
         total = add(total, f3(tp["table_contribution"]))
     if total != (0, 0, 0):
