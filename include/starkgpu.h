@@ -523,6 +523,20 @@ typedef struct {
 SG_API int sg_verify_queries(sg_ctx* ctx, void* stream, const sg_verify_table* tables, uint32_t count,
                              uint32_t* status_out);
 
+/* ---- RV64 front-end (host): execute a guest of RV64I-subset words (ADD, SUB,
+ *      ADDI, LUI, BEQ, BNE, ECALL-exit with a7 = 93; executor/src/vm semantics)
+ *      from pc 0, at most max_steps instructions. *cycles_out gets the executed
+ *      instruction count and *a0_out the final a0. With trace_out, also writes
+ *      the CPU table of the execution's proof (n_rows x SG_RV64_CPU_WIDTH u64,
+ *      row-major, host memory; rows past the halt repeat the halting row, the
+ *      last row ends the cycle) and counts_out[i] (nwords entries) = how many
+ *      table rows execute instruction i. The layout is lambda_vm_b200/rv64_air.py's.
+ *      No counterpart in the reference's math-cuda (it is the executor and
+ *      trace builder of the VM crates, restricted to this subset). ---- */
+#define SG_RV64_CPU_WIDTH 188
+SG_API int sg_rv64_trace(const uint32_t* words, uint32_t nwords, uint64_t max_steps, uint64_t n_rows,
+                         uint64_t* trace_out, uint64_t* counts_out, uint64_t* a0_out, uint64_t* cycles_out);
+
 /* ---- DFT pass log: the autotuner's measurements. No counterpart in the
  *      reference (its NTT has one fixed plan). While enabled, every DFT pass
  *      launched through the context is bracketed by CUDA events; _read waits for

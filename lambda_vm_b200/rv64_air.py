@@ -151,6 +151,23 @@ CPU_WIDTH = X0 + 62
 TWO16, TWO32 = 1 << 16, 1 << 32
 
 
+def _batch_inverse(vals):
+    """Inverses mod p of a list of ints (0 -> 0) with one exponentiation
+    (prefix products, Montgomery's trick)."""
+    nz = [v for v in vals if v]
+    pre, acc = [], 1
+    for v in nz:
+        pre.append(acc)
+        acc = acc * v % P
+    inv = pow(acc, P - 2, P) if nz else 1
+    out_nz = [0] * len(nz)
+    for i in range(len(nz) - 1, -1, -1):
+        out_nz[i] = inv * pre[i] % P
+        inv = inv * nz[i] % P
+    it = iter(out_nz)
+    return [next(it) if v else 0 for v in vals]
+
+
 def xlo(k):
     return X0 + 2 * (k - 1)
 
@@ -279,33 +296,32 @@ class CpuAir(BusAir):
         by column with numpy."""
         n, T = self.n, len(rows)
         assert 1 <= T <= n, "the execution does not fit the table"
-        pad = [rows[-1]] * (n - T)
-        allr = rows + pad
-        u64 = lambda f: np.array([f(r) for r in allr], dtype=np.uint64)
-        pc, rd, rs1, rs2 = u64(lambda r: r[0]), u64(lambda r: r[2]), u64(lambda r: r[3]), u64(lambda r: r[4])
-        imm_s = [r[5] for r in allr]
-        imm_u = np.array([v & MASK64 for v in imm_s], dtype=np.uint64)
-        a, bv, r = u64(lambda r: r[6]), u64(lambda r: r[7]), u64(lambda r: r[8])
-        ops = [r[1] for r in allr]
+        cols = list(zip(*rows))
+        ext = lambda c: np.concatenate([c, np.full(n - T, c[-1], dtype=c.dtype)])
+        pc, rd, rs1, rs2 = (ext(np.array(cols[i], dtype=np.uint64)) for i in (0, 2, 3, 4))
+        imm_i = ext(np.array(cols[5], dtype=np.int64))
+        imm_u = imm_i.view(np.uint64)
+        a, bv, r = (ext(np.array(cols[i], dtype=np.uint64)) for i in (6, 7, 8))
+        op_of = {o: OP_ID[o] for o in OPS}
+        op = ext(np.array([op_of[o] for o in cols[1]], dtype=np.int64))
         m32, s32 = np.uint64(0xFFFFFFFF), np.uint64(32)
-        t = np.zeros((n, CPU_WIDTH), dtype=np.uint64)
-        t[:, PC] = pc
-        t[:, STEP] = 1
-        t[n - 1, STEP] = 0
-        opcol = np.array([SEL[o] for o in ops], dtype=np.int64)
+        t = np.zeros((CPU_WIDTH, n), dtype=np.uint64)  # column-major while filling
+        t[PC] = pc
+        t[STEP] = 1
+        t[STEP, n - 1] = 0
+        opcol = 2 + op - 1  # SEL columns follow OPS order, ids start at 1
         idx = np.arange(n)
-        t[idx, opcol] = 1
-        t[idx, RD0 + rd.astype(np.int64)] = 1
-        t[idx, RS10 + rs1.astype(np.int64)] = 1
-        t[idx, RS20 + rs2.astype(np.int64)] = 1
-        t[:, IMM_LO], t[:, IMM_HI] = imm_u & m32, imm_u >> s32
-        t[:, IMM_F] = np.array([v % P for v in imm_s], dtype=np.uint64)
-        t[:, A_LO], t[:, A_HI] = a & m32, a >> s32
-        t[:, B_LO], t[:, B_HI] = bv & m32, bv >> s32
-        t[:, R_LO], t[:, R_HI] = r & m32, r >> s32
+        t[opcol, idx] = 1
+        t[RD0 + rd.astype(np.int64), idx] = 1
+        t[RS10 + rs1.astype(np.int64), idx] = 1
+        t[RS20 + rs2.astype(np.int64), idx] = 1
+        t[IMM_LO], t[IMM_HI] = imm_u & m32, imm_u >> s32
+        t[IMM_F] = np.where(imm_i < 0, np.uint64(P) - (-imm_i).astype(np.uint64), imm_u)
+        t[A_LO], t[A_HI] = a & m32, a >> s32
+        t[B_LO], t[B_HI] = bv & m32, bv >> s32
+        t[R_LO], t[R_HI] = r & m32, r >> s32
         for j in range(4):
-            t[:, R16 + j] = (r >> np.uint64(16 * j)) & np.uint64(0xFFFF)
-        op = np.array([OP_ID[o] for o in ops])
+            t[R16 + j] = (r >> np.uint64(16 * j)) & np.uint64(0xFFFF)
         is_add = (op == OP_ID["add"]) | (op == OP_ID["addi"])
         o = np.where(op == OP_ID["add"], bv, imm_u)
         c0 = ((a & m32) + (o & m32)) >> s32
@@ -313,17 +329,17 @@ class CpuAir(BusAir):
         sb = op == OP_ID["sub"]
         b0 = ((a & m32) < (bv & m32)).astype(np.uint64)
         b1 = ((a >> s32) < (bv >> s32) + b0).astype(np.uint64)
-        t[:, C0] = np.where(is_add, c0, np.where(sb, b0, 0))
-        t[:, C1] = np.where(is_add, c1, np.where(sb, b1, 0))
+        t[C0] = np.where(is_add, c0, np.where(sb, b0, 0))
+        t[C1] = np.where(is_add, c1, np.where(sb, b1, 0))
         # branch rows: per-limb difference, its inverse, the flags
         br_rows = np.nonzero((op == OP_ID["beq"]) | (op == OP_ID["bne"]))[0]
-        for lo_hi, (ac, bc, ic, ec) in enumerate(((A_LO, B_LO, INV_LO, E_LO), (A_HI, B_HI, INV_HI, E_HI))):
-            d = [(int(t[i, ac]) - int(t[i, bc])) % P for i in br_rows]
-            t[br_rows, ic] = np.array([pow(x, P - 2, P) if x else 0 for x in d], dtype=np.uint64)
-            t[br_rows, ec] = np.array([1 if x else 0 for x in d], dtype=np.uint64)
-        ne = t[:, E_LO] | t[:, E_HI]
-        t[:, NE] = ne
-        t[:, BR] = np.where(op == OP_ID["bne"], ne, np.where(op == OP_ID["beq"], 1 - ne, 0))
+        for ac, bc, ic, ec in ((A_LO, B_LO, INV_LO, E_LO), (A_HI, B_HI, INV_HI, E_HI)):
+            d = [(x - y) % P for x, y in zip(t[ac, br_rows].tolist(), t[bc, br_rows].tolist())]
+            t[ic, br_rows] = np.array(_batch_inverse(d), dtype=np.uint64)
+            t[ec, br_rows] = np.array([1 if x else 0 for x in d], dtype=np.uint64)
+        ne = t[E_LO] | t[E_HI]
+        t[NE] = ne
+        t[BR] = np.where(op == OP_ID["bne"], ne, np.where(op == OP_ID["beq"], 1 - ne, 0))
         # register file before each row: the last value written below it
         writes = np.isin(op, [OP_ID[x] for x in ("add", "sub", "addi", "lui")]) & (rd != 0) & (idx < T)
         for k in range(1, 32):
@@ -331,15 +347,15 @@ class CpuAir(BusAir):
             last = np.maximum.accumulate(wk)
             before = np.concatenate(([-1], last[:-1]))
             val = np.where(before >= 0, r[np.maximum(before, 0)], np.uint64(0))
-            t[:, xlo(k)], t[:, xhi(k)] = val & m32, val >> s32
-        return t
+            t[xlo(k)], t[xhi(k)] = val & m32, val >> s32
+        return np.ascontiguousarray(t.T)
 
     def counts(self, rows):
         """Execution count of every program instruction over the n table rows."""
-        c = [0] * len(self.prog)
-        for i in range(self.n):
-            c[(rows[i] if i < len(rows) else rows[-1])[0] // 4] += 1
-        return c
+        pcs = np.array([r[0] for r in rows], dtype=np.int64) // 4
+        c = np.bincount(pcs, minlength=len(self.prog))
+        c[pcs[-1]] += self.n - len(rows)  # the repeated halting row
+        return [int(v) for v in c]
 
     def public_terms(self, counts, output):
         """The verifier's side of the ROM and END buses: (bus, tuple, signed
@@ -394,18 +410,32 @@ def statement_label(words, counts, output):
     return b"lambda_vm_b200/rv64/" + keccak256(blob)
 
 
+def native_trace(words, max_steps=1 << 32):
+    """Execute and build the CPU table in the library (sg_rv64_trace, C++):
+    (table, counts, a0, cycles)."""
+    import ctypes as C
+    from . import native
+    L = native.lib()
+    w = np.ascontiguousarray(np.asarray(words, dtype=np.uint32))
+    a0, cyc = C.c_uint64(), C.c_uint64()
+    native.check(L.sg_rv64_trace(w.ctypes.data, len(w), max_steps, 0, None, None, C.byref(a0), C.byref(cyc)))
+    n = 1 << max(1, (cyc.value - 1).bit_length())
+    t = np.empty((n, CPU_WIDTH), np.uint64)
+    counts = np.zeros(len(w), np.uint64)
+    native.check(L.sg_rv64_trace(w.ctypes.data, len(w), max_steps, n, t.ctypes.data, counts.ctypes.data,
+                                 C.byref(a0), C.byref(cyc)))
+    return t, [int(c) for c in counts], a0.value, cyc.value
+
+
 def build(words):
-    """Execute a program and build its tables: (airs, traces, public) with
-    public = {"words", "counts", "output", "cycles", "label", "terms"}."""
-    rows, regs = execute(words)
-    log_n = max(1, (len(rows) - 1).bit_length())
-    cpu = CpuAir(words, log_n)
+    """Execute a program and build its tables (the CPU table by the library's
+    native executor): (airs, traces, public) with public = {"words", "counts",
+    "output", "cycles", "label", "terms"}."""
+    ct, counts, out, cycles = native_trace(words)
+    cpu = CpuAir(words, ct.shape[0].bit_length() - 1)
     rng = RangeAir()
-    ct = cpu.trace(rows)
     rt = rng.trace(ct)
-    counts = cpu.counts(rows)
-    out = regs[10]
-    pub = {"words": list(words), "counts": counts, "output": out, "cycles": len(rows),
+    pub = {"words": list(words), "counts": counts, "output": out, "cycles": cycles,
            "label": statement_label(words, counts, out), "terms": cpu.public_terms(counts, out)}
     return [cpu, rng], [ct, rt], pub
 

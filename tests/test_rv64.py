@@ -36,6 +36,19 @@ def test_fibonacci_guest_runs(n):
     assert len(rows) == 2 + (1 if n < 2048 else 2) + 5 * n + 3
 
 
+@pytest.mark.parametrize("n", [1, 7, 30, 2047, 2048, 5000])
+def test_native_trace_equals_the_python_table(n):
+    """sg_rv64_trace (the library's C++ executor and table writer) against the
+    Python executor and table builder, cell for cell."""
+    words = rv64.fib_program(n)
+    rows, regs = rv64.execute(words)
+    ct, counts, out, cycles = RA.native_trace(words)
+    cpu = RA.CpuAir(words, ct.shape[0].bit_length() - 1)
+    assert cycles == len(rows) and out == regs[10]
+    assert np.array_equal(ct, cpu.trace(rows))
+    assert counts == cpu.counts(rows)
+
+
 def _aux_and_apows(airs, z, alpha):
     apows = [(1, 0, 0)]
     for _ in range(max(a.max_alpha for a in airs) - 1):
