@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--job-max-log-n", type=int, default=18, help="serve: largest job height (log2 cycles)")
     ap.add_argument("--max-jobs", type=int, default=4, help="serve: concurrent jobs")
     ap.add_argument("--policy", default="backfill", choices=["backfill", "fifo"], help="serve: admission policy")
+    ap.add_argument("--job-kind", default="mix", choices=["mix", "synth"],
+                    help="serve: Fibonacci guests and synthetic chip tables alternating, or synthetic only")
     ap.add_argument("--no-serve-summary", action="store_true",
                     help="skip the serving summary the default line carries at N = 1")
     ap.add_argument("--tables", type=int, default=40)
@@ -360,18 +362,26 @@ def measure_proof(a):
 
 
 def serve_jobs(a, seed=77):
-    """Proof requests of a serving stream: each job's cycle count c is
-    log-uniform in 2^10..2^job_max_log_n and its trace is 2-4 chip tables of
-    c, c/2, c/4, ... rows (widths uniform 8..300, 2-6 LogUp interactions),
-    with trace seeds of its own."""
+    """Proof requests of a serving stream. Even jobs are Fibonacci RV64 guests
+    (executed and tabled up front) of c cycles, odd jobs stand in for the
+    Keccak guests, whose chips are not built: 2-4 synthetic chip tables of c,
+    c/2, c/4, ... rows (widths uniform 8..300, 2-6 LogUp interactions) with
+    trace seeds of their own; c log-uniform in 2^10..2^job_max_log_n.
+    Each spec is (airs, sources, transcript label)."""
+    from lambda_vm_b200 import rv64
+    from lambda_vm_b200 import rv64_air as RA
     from lambda_vm_b200.air import SynthTableAir
     rng = np.random.default_rng(seed)
     specs = []
     for j in range(a.jobs):
         k = int(rng.integers(10, a.job_max_log_n + 1))
+        if j % 2 == 0 and getattr(a, "job_kind", "mix") == "mix":
+            airs, traces, pub = RA.build(rv64.fib_program(max(1, ((1 << k) - 6) // 5)))
+            specs.append((airs, traces, pub["label"]))
+            continue
         nt = int(rng.integers(2, 5))
         airs = [SynthTableAir(max(6, k - t), int(rng.integers(8, 301)), int(rng.choice([2, 4, 6]))) for t in range(nt)]
-        specs.append((airs, [100000 + 100 * j + t for t in range(nt)]))
+        specs.append((airs, [100000 + 100 * j + t for t in range(nt)], b"lambda_vm_b200/synthetic-multi-table"))
     return specs
 
 
@@ -394,14 +404,14 @@ def measure_serve(a):
     specs = serve_jobs(a)
     budget = min(160 * (1 << 30), be.budget())
     warm_context(be, specs, opts)  # domains of every height, DFT tile timings
-    for airs, srcs in specs[:3]:  # and the allocator's block cache, through both provers
-        multi_prove(airs, srcs, opts, GpuBackend(be))
-        multi_prove_scheduled(airs, srcs, opts, workers=4, be=be)
+    for airs, srcs, label in specs[:3]:  # and the allocator's block cache, through both provers
+        multi_prove(airs, srcs, opts, GpuBackend(be), label=label)
+        multi_prove_scheduled(airs, srcs, opts, workers=4, be=be, label=label)
     # one burst of every job at once, so the block cache reaches the working
     # set of max_jobs overlapping proofs before any latency is measured
     with ProofServer(budget, max_jobs=a.max_jobs, drivers=4, opts=opts, be=be, policy="fifo") as srv:
-        for airs, srcs in specs:
-            srv.submit(airs, srcs)
+        for spec in specs:
+            srv.submit(*spec)
     torch.cuda.synchronize()
     sweep = []
     for i, rate in enumerate(float(x) for x in a.rates.split(",")):
@@ -410,7 +420,8 @@ def measure_serve(a):
                 return serve_poisson(srv, specs, rate, seed=int(rate * 1000))[1]
 
         def one_at_a_time():
-            return serve_sequential(specs, rate, lambda airs, srcs: multi_prove(airs, srcs, opts, GpuBackend(be)),
+            return serve_sequential(specs, rate, lambda airs, srcs, label: multi_prove(airs, srcs, opts, GpuBackend(be),
+                                                                                      label=label),
                                     seed=int(rate * 1000))[1]
         # the two servers take turns going first
         if i % 2 == 0:
@@ -421,14 +432,18 @@ def measure_serve(a):
                       "all_proved": st.failed == 0 and st_seq.failed == 0,
                       "p99_batched_le_one_at_a_time": bool(st.p99_s <= st_seq.p99_s)})
     top = sweep[-1]
-    rows = sum(sum(x.n for x in airs) for airs, _ in specs)
+    rows = sum(sum(x.n for x in spec[0]) for spec in specs)
     line = {"metric": "proof serving: proved cycles/s and p50/p99 latency under Poisson arrivals",
             "value": top["batched"]["rows_per_s"], "unit": "rows/s", "n_gpus": 1, "steps": a.jobs, "warmup": 3,
             "ms_per_step": top["batched"]["mean_ms"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64 (Goldilocks) / Fp3",
-            "data": "synthetic chip-table proofs (no VM front-end: job sizes stand in for the guests' cycle counts)",
+            "data": ("Fibonacci RV64 guests executed and tabled up front, alternating with synthetic chip-table "
+                     "proofs standing in for the Keccak guests" if a.job_kind == "mix" else
+                     "synthetic chip-table proofs (job sizes stand in for the guests' cycle counts)"),
             "config": {"workload": f"{a.jobs} proof jobs per rate, cycles log-uniform 2^10..2^{a.job_max_log_n}, "
-                                   f"2-4 tables each, blowup 2, 219 queries, grinding 20",
+                                   + ("even jobs Fibonacci guests (CPU + RANGE tables), odd jobs "
+                                      if a.job_kind == "mix" else "")
+                                   + "2-4 synthetic tables each, blowup 2, 219 queries, grinding 20",
                        "rows_total": rows, "hbm_budget_bytes": budget, "max_concurrent_jobs": a.max_jobs,
                        "policy": a.policy},
             "p50_ms": top["batched"]["p50_ms"], "p99_ms": top["batched"]["p99_ms"], "sweep": sweep}
@@ -440,7 +455,7 @@ def serve_summary(a):
     24 jobs each, admission server against one proof at a time."""
     import types
     b = types.SimpleNamespace(jobs=24, job_max_log_n=a.job_max_log_n, max_jobs=a.max_jobs, rates="5,50",
-                              policy=a.policy)
+                              policy=a.policy, job_kind=getattr(a, "job_kind", "mix"))
     line = measure_serve(b)
     return {"workload": line["config"]["workload"], "policy": a.policy,
             "rates": [{"rate_jobs_per_s": s["rate_jobs_per_s"],

@@ -120,7 +120,9 @@ SG_API int sg_coset_lde(sg_ctx* ctx, void* stream, const uint64_t* d_trace, uint
  *      width is timed on the same work and its time per column kept; a pass
  *      over m columns then uses the width minimising ceil(m/C)*C*cost(C),
  *      keeping the default width (16 up to 2^10, 8 at 2^11) unless another is
- *      at least 3 % cheaper. Results never depend on the width. sg_ctx_dft_tiles pins a width for a
+ *      at least 3 % cheaper; a context with a learned pass-cost model
+ *      (sg_ctx_set_pass_model, below) predicts each width's pass time instead
+ *      and never times. Results never depend on the width. sg_ctx_dft_tiles pins a width for a
  *      length (cols = 0: automatic); sg_ctx_dft_tuning reports the widths and
  *      their time per column (ms), timing them on `stream` first if needed. ---- */
 SG_API int sg_ctx_dft_tiles(sg_ctx* ctx, uint32_t log_len, uint32_t cols);

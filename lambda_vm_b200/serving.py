@@ -40,13 +40,14 @@ def job_cells(airs):
 
 
 class Job:
-    __slots__ = ("id", "airs", "sources", "rows", "cells", "big", "est", "t_submit", "t_start", "t_done", "proof",
-                 "error", "done")
+    __slots__ = ("id", "airs", "sources", "label", "rows", "cells", "big", "est", "t_submit", "t_start", "t_done",
+                 "proof", "error", "done")
 
-    def __init__(self, jid, airs, sources, est, big_cells=None):
+    def __init__(self, jid, airs, sources, est, big_cells=None, label=None):
         self.id = jid
         self.airs = airs
         self.sources = sources
+        self.label = label
         self.rows = sum(a.n for a in airs)
         self.cells = job_cells(airs)
         self.big = big_cells is not None and self.cells >= big_cells
@@ -145,21 +146,24 @@ class ProofServer:
         self.dispatcher = threading.Thread(target=self._dispatch, daemon=True)
         self.dispatcher.start()
 
-    def _prove_gpu(self, airs, sources, opts, drivers, budget_bytes, priority=None):
+    def _prove_gpu(self, airs, sources, opts, drivers, budget_bytes, priority=None, label=None):
+        kw = {} if label is None else {"label": label}
         return multi_prove_scheduled(airs, sources, opts, workers=drivers, budget_bytes=budget_bytes, be=self.be,
-                                     priority=priority)
+                                     priority=priority, **kw)
 
     def _drivers(self, job):
         return self.drivers if (self.policy == "fifo" or job.big) else max(1, min(self.small_drivers, self.drivers))
 
-    def submit(self, airs, sources):
+    def submit(self, airs, sources, label=None):
+        """Queue one proof job: its tables and their traces (host arrays or
+        synthetic-trace seeds), and its statement's transcript label."""
         with self.cv:
             if self.closed:
                 raise RuntimeError("server is closed")
             probe = Job(self.next_id, airs, sources, 0, self.big_cells)
             est = estimate_job_bytes(airs, self.opts, self.drivers if self.policy == "fifo" or probe.big
                                      else max(1, min(self.small_drivers, self.drivers)))
-            job = Job(self.next_id, airs, sources, est, self.big_cells)
+            job = Job(self.next_id, airs, sources, est, self.big_cells, label)
             self.next_id += 1
             self.jobs.append(job)
             self.queue.append(job)
@@ -220,7 +224,7 @@ class ProofServer:
             # rounds 2-4 of this job may use what its resident R1 state leaves of its share
             if self.prove_fn == self._prove_gpu:
                 job.proof = self._prove_gpu(job.airs, job.sources, self.opts, self._drivers(job), job.est,
-                                            self.urgent if job.big else None)
+                                            self.urgent if job.big else None, job.label)
             else:
                 job.proof = self.prove_fn(job.airs, job.sources, self.opts, self._drivers(job), job.est)
         except Exception as e:  # reported per job; the server keeps serving
@@ -260,7 +264,7 @@ def warm_context(be, job_specs, opts):
     from . import native
     from .stark import GpuBackend
     bk = GpuBackend(be)
-    for log_n in sorted({a.log_n for airs, _ in job_specs for a in airs}):
+    for log_n in sorted({a.log_n for spec in job_specs for a in spec[0]}):
         bk.domain(log_n, opts.blowup, opts.coset_offset)
     cols, cost, cnt = (C.c_uint32 * 4)(), (C.c_float * 4)(), C.c_uint32()
     for log_len in range(8, 12) if getattr(be, "pass_model", None) is None else ():
@@ -269,7 +273,7 @@ def warm_context(be, job_specs, opts):
 
 
 def serve_poisson(server, job_specs, rate, seed=0):
-    """Submit `job_specs` [(airs, sources)] with exponential inter-arrival
+    """Submit `job_specs` [(airs, sources[, label])] with exponential inter-arrival
     times of mean 1/rate (seeded); wait for all; return (jobs, ServeStats)."""
     import numpy as np
     rng = np.random.default_rng(seed)
@@ -277,12 +281,12 @@ def serve_poisson(server, job_specs, rate, seed=0):
     t0 = time.perf_counter()
     due = t0
     jobs = []
-    for (airs, sources), gap in zip(job_specs, gaps):
+    for spec, gap in zip(job_specs, gaps):
         due += gap
         now = time.perf_counter()
         if due > now:
             time.sleep(due - now)
-        jobs.append(server.submit(airs, sources))
+        jobs.append(server.submit(*spec))
     for j in jobs:
         j.done.wait()
     t1 = max(j.t_done for j in jobs)
@@ -302,15 +306,15 @@ def serve_sequential(job_specs, rate, prove_fn, seed=0):
         arrivals.append(t)
     t0 = time.perf_counter()
     jobs = []
-    for (airs, sources), at in zip(job_specs, arrivals):
+    for spec, at in zip(job_specs, arrivals):
         now = time.perf_counter()
         if t0 + at > now:
             time.sleep(t0 + at - now)
-        j = Job(len(jobs), airs, sources, 0)
+        j = Job(len(jobs), spec[0], spec[1], 0)
         j.t_submit = t0 + float(at)
         j.t_start = time.perf_counter()
         try:
-            j.proof = prove_fn(airs, sources)
+            j.proof = prove_fn(*spec)
         except Exception as e:
             j.error = e
         j.t_done = time.perf_counter()
