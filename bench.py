@@ -47,9 +47,12 @@ def parse():
     ap.add_argument("--workload", default="commit", choices=["commit", "proof", "serve", "rounds", "vm"],
                     help="commit: LDE + Merkle commit of one trace (default); proof: multi-table proof, plain vs "
                          "scheduled; serve: Poisson stream of proof jobs, concurrent admission vs one at a time; "
-                         "rounds: the round-2..4 kernels of one large table, one by one; vm: the Fibonacci RV64 "
-                         "guest executed and its execution proved")
+                         "rounds: the round-2..4 kernels of one large table, one by one; vm: an RV64 guest (--guest) "
+                         "executed and its execution proved")
     ap.add_argument("--fib-n", type=int, default=30000, help="vm: Fibonacci loop iterations (5 cycles each)")
+    ap.add_argument("--guest", default="fib", choices=["fib", "keccak"], help="vm: which guest")
+    ap.add_argument("--keccak-bytes", type=int, default=136 * 7710,
+                    help="vm: the Keccak guest's buffer (a multiple of 136; default 1048560, about 1 MiB)")
     ap.add_argument("--rates", default="2,5,10,20,50,100", help="serve: arrival rates (jobs/s)")
     ap.add_argument("--jobs", type=int, default=40, help="serve: jobs per rate")
     ap.add_argument("--job-max-log-n", type=int, default=18, help="serve: largest job height (log2 cycles)")
@@ -467,47 +470,74 @@ def serve_summary(a):
                        "all_proved": s["all_proved"]} for s in line["sweep"]]}
 
 
-def measure_vm(a, steps=3, warmup=1):
-    """The Fibonacci RV64 guest (add/mv/mv/addi/bnez loop, n iterations):
-    execute it, build its CPU and RANGE tables, prove the execution on the GPU
-    (blowup 2, 128-bit security, grinding 20), verify. Proved cycles/s =
+def measure_vm(a, guest="fib", steps=3, warmup=1):
+    """An RV64 guest executed and its execution proved on the GPU (blowup 2,
+    128-bit security, grinding 20), then verified. fib: the Fibonacci guest
+    (add/mv/mv/addi/bnez loop, --fib-n iterations; CPU and RANGE tables).
+    keccak: the Keccak guest (a --keccak-bytes buffer filled by xorshift64,
+    hashed in 136-byte blocks through the keccak ecall, the digests XOR-folded
+    with load/store loops; CPU, RANGE, BITWISE, SHIFT, MEMORY and KECCAK
+    tables), proved by the plain per-table prover and by the batched one
+    (multi-table R1 launches, concurrent table drivers). Proved cycles/s =
     executed instructions / wall time of execute + tables + prove."""
     import torch
     from lambda_vm_b200 import rv64
     from lambda_vm_b200 import rv64_air as RA
     from lambda_vm_b200.device import backend
+    from lambda_vm_b200.scheduler import multi_prove_scheduled
     from lambda_vm_b200.stark import GpuBackend, Options, multi_prove
     be = backend(0)
     opts = Options(blowup=2, grinding=20, final_log_degree=5)
-    words = rv64.fib_program(a.fib_n)
-    tb, tp = [], []
+    if guest == "fib":
+        words, expect = rv64.fib_program(a.fib_n), rv64.fib_reference(a.fib_n)
+        forms = {"plain": lambda airs, tr, lb: multi_prove(airs, tr, opts, GpuBackend(be), label=lb)}
+    else:
+        words, expect = rv64.keccak_program(a.keccak_bytes), rv64.keccak_reference(a.keccak_bytes)
+        forms = {"plain": lambda airs, tr, lb: multi_prove(airs, tr, opts, GpuBackend(be), label=lb),
+                 "batched": lambda airs, tr, lb: multi_prove_scheduled(airs, tr, opts, workers=a.workers, be=be,
+                                                                       label=lb)}
+    times = {f: ([], []) for f in forms}
+    proofs = {}
     for it in range(warmup + steps):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        airs, traces, pub = RA.build(words)
-        t1 = time.perf_counter()
-        proof = multi_prove(airs, traces, opts, GpuBackend(be), label=pub["label"])
-        torch.cuda.synchronize()
-        t2 = time.perf_counter()
-        if it >= warmup:
-            tb.append(t1 - t0)
-            tp.append(t2 - t1)
+        for f, prove in forms.items():
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            airs, traces, pub = RA.build(words)
+            t1 = time.perf_counter()
+            proofs[f] = prove(airs, traces, pub["label"])
+            torch.cuda.synchronize()
+            t2 = time.perf_counter()
+            del traces
+            if it >= warmup:
+                times[f][0].append(t1 - t0)
+                times[f][1].append(t2 - t1)
     tv = time.perf_counter()
-    verdict = RA.verify(words, pub["counts"], pub["output"], proof, opts, device=be)
+    verdict = RA.verify(words, pub["counts"], pub["output"], proofs["plain"], opts, device=be,
+                        heights=pub["heights"])
     verify_s = time.perf_counter() - tv
-    b_s, p_s = statistics.median(tb), statistics.median(tp)
+    b_s, p_s = statistics.median(times["plain"][0]), statistics.median(times["plain"][1])
     cyc = pub["cycles"]
-    return {"metric": "proved cycles/s (RV64 Fibonacci guest: execute + trace tables + prove)",
+    tables = ", ".join(f"{type(t).__name__[:-3].upper()} 2^{t.log_n} x {t.width}" for t in airs)
+    name = "Fibonacci" if guest == "fib" else "Keccak"
+    size = f"{a.fib_n} iterations" if guest == "fib" else f"{a.keccak_bytes}-byte buffer"
+    line = {"metric": f"proved cycles/s (RV64 {name} guest: execute + trace tables + prove)",
             "value": cyc / (b_s + p_s), "unit": "cycles/s", "cycles": cyc,
-            "workload": f"Fibonacci guest, {a.fib_n} iterations, {cyc} cycles; CPU table 2^{airs[0].log_n} x "
-                        f"{airs[0].width}, RANGE table 2^16 x 3; blowup 2, {opts.queries} queries, grinding 20",
+            "workload": f"{name} guest, {size}, {cyc} cycles; {tables}; blowup 2, {opts.queries} queries, grinding 20",
             "execute_and_tables_ms": round(b_s * 1e3, 1), "prove_ms": round(p_s * 1e3, 1),
-            "prove_only_cycles_per_s": round(cyc / p_s, 1), "output_ok": pub["output"] == rv64.fib_reference(a.fib_n),
+            "prove_only_cycles_per_s": round(cyc / p_s, 1), "output_ok": pub["output"] == expect,
             "verified": verdict[0] is True, "verify_ms": round(verify_s * 1e3, 1)}
+    if "batched" in forms:
+        from lambda_vm_b200.proof_io import serialize
+        bb, bp = statistics.median(times["batched"][0]), statistics.median(times["batched"][1])
+        line.update({"batched_cycles_per_s": cyc / (bb + bp), "batched_prove_ms": round(bp * 1e3, 1),
+                     "batched_over_plain": round((b_s + p_s) / (bb + bp), 3),
+                     "batched_prove_over_plain_prove": round(p_s / bp, 3),
+                     "batched_equals_plain": serialize(proofs["batched"]) == serialize(proofs["plain"])})
+    return line
 
 
 def run_vm(a):
-    line = measure_vm(a)
+    line = measure_vm(a, a.guest)
     line.update({"n_gpus": 1, "steps": 3, "warmup": 1, "higher_is_better": True, "scaling": "weak",
                  "vs_baseline": None, "dtype": "u64 (Goldilocks) / Fp3", "data": "generated RV64 guest"})
     print(json.dumps(line), flush=True)

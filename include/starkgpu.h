@@ -526,18 +526,31 @@ SG_API int sg_verify_queries(sg_ctx* ctx, void* stream, const sg_verify_table* t
                              uint32_t* status_out);
 
 /* ---- RV64 front-end (host): execute a guest of RV64I-subset words (ADD, SUB,
- *      ADDI, LUI, BEQ, BNE, ECALL-exit with a7 = 93; executor/src/vm semantics)
- *      from pc 0, at most max_steps instructions. *cycles_out gets the executed
- *      instruction count and *a0_out the final a0. With trace_out, also writes
- *      the CPU table of the execution's proof (n_rows x SG_RV64_CPU_WIDTH u64,
- *      row-major, host memory; rows past the halt repeat the halting row, the
- *      last row ends the cycle) and counts_out[i] (nwords entries) = how many
- *      table rows execute instruction i. The layout is lambda_vm_b200/rv64_air.py's.
- *      No counterpart in the reference's math-cuda (it is the executor and
- *      trace builder of the VM crates, restricted to this subset). ---- */
-#define SG_RV64_CPU_WIDTH 188
-SG_API int sg_rv64_trace(const uint32_t* words, uint32_t nwords, uint64_t max_steps, uint64_t n_rows,
-                         uint64_t* trace_out, uint64_t* counts_out, uint64_t* a0_out, uint64_t* cycles_out);
+ *      XOR, OR, AND, ADDI, XORI, ORI, ANDI, SLLI, SRLI, LUI, LD, SD, BEQ, BNE,
+ *      ECALL: a7 = 93 exits, a7 = 2^64 - 2 applies keccak-f[1600] to the 25
+ *      lanes at a0; executor/src/vm semantics, the keccak ecall as
+ *      executor/src/vm/instruction/execution.rs:649-670) from pc 0 with zeroed
+ *      data memory, at most max_steps instructions. Fills *info (executed
+ *      instructions, final a0, shifts executed, memory cells touched, keccak
+ *      ecalls). With cpu_out, also writes the CPU table of the execution's
+ *      proof (n_rows x SG_RV64_CPU_WIDTH u64, row-major, host memory; rows past
+ *      the halt repeat the halting row, the last row ends the cycle; the layout
+ *      is lambda_vm_b200/rv64_air.py's) and counts_out[i] (nwords entries) =
+ *      how many table rows execute instruction i. Each optional event array
+ *      gets one record per event: shifts_out (dir, a, amount), cells_out
+ *      (address, final value, final timestamp; ascending addresses),
+ *      keccak_out (timestamp, state address, 25 input lanes, the 25 cells'
+ *      previous timestamps). Size them from a first call without outputs.
+ *      reserved must be NULL. No counterpart in the reference's math-cuda (it
+ *      is the executor and trace builder of the VM crates, restricted to this
+ *      subset). ---- */
+#define SG_RV64_CPU_WIDTH 234
+typedef struct {
+    uint64_t cycles, a0, shifts, cells, keccak_calls;
+} sg_rv64_info;
+SG_API int sg_rv64_run(const uint32_t* words, uint32_t nwords, uint64_t max_steps, uint64_t n_rows,
+                       uint64_t* cpu_out, uint64_t* counts_out, uint64_t* shifts_out, uint64_t* cells_out,
+                       uint64_t* keccak_out, void* reserved, sg_rv64_info* info);
 
 /* ---- DFT pass log: the autotuner's measurements. No counterpart in the
  *      reference (its NTT has one fixed plan). While enabled, every DFT pass

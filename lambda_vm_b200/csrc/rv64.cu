@@ -1,15 +1,24 @@
 // RV64 front-end on the host: execute a guest of the supported RV64I subset
-// and write the CPU table its proof needs, in one pass.
+// and write the CPU table its proof needs, in one pass, together with the
+// events the chip tables are built from (shifts, the touched memory cells,
+// the Keccak ecalls).
 //
-// The same machine and the same table as lambda_vm_b200/rv64.py (execute)
-// and rv64_air.py (CpuAir.trace), which the tests compare this against: ADD,
-// SUB, ADDI, LUI, BEQ, BNE and ECALL-exit (a7 = 93) on 64-bit registers with
-// x0 hard-wired to zero (executor/src/vm semantics for these opcodes). One
-// table row per executed instruction, padded to n rows by repeating the
-// halting ECALL; the last row carries STEP = 0. Writing the 188-column rows as
-// the machine runs keeps the whole front-end at memory speed on the host.
+// The same machine and the same table as lambda_vm_b200/rv64.py (run) and
+// rv64_air.py (CpuAir.trace), which the tests compare this against cell for
+// cell: ADD, SUB, XOR, OR, AND, ADDI, XORI, ORI, ANDI, SLLI, SRLI, LUI, LD, SD,
+// BEQ, BNE and ECALL (a7 = 93 exit, a7 = 2^64 - 2 keccak-f[1600] on the 25
+// lanes at a0) on 64-bit registers with x0 hard-wired to zero (executor/src/vm
+// semantics for these opcodes; the keccak ecall as
+// executor/src/vm/instruction/execution.rs:649-670). Data memory starts
+// zeroed; loads and stores are doublewords at 8-byte-aligned addresses below
+// 2^32. One table row per executed instruction (row t has timestamp t + 1),
+// padded to n rows by repeating the halting ECALL; the last row carries
+// STEP = 0. Writing the rows as the machine runs keeps the front-end at
+// memory speed on the host.
 #include <string.h>
 
+#include <algorithm>
+#include <unordered_map>
 #include <vector>
 
 #include "common.cuh"
@@ -17,11 +26,18 @@
 namespace {
 
 constexpr uint64_t P = 0xFFFFFFFF00000001ULL;
-enum Op { ADD = 1, SUB, ADDI, LUI, BEQ, BNE, ECALL };  // the ROM tuple's opcode ids
-// Column layout of the CPU table (rv64_air.py).
-constexpr int PC = 0, STEP = 1, SEL0 = 2, RD0 = 9, RS10 = 41, RS20 = 73, IMM_LO = 105, IMM_HI = 106, IMM_F = 107,
-              A_LO = 108, A_HI = 109, B_LO = 110, B_HI = 111, R_LO = 112, R_HI = 113, R16 = 114, C0 = 118, C1 = 119,
-              INV_LO = 120, INV_HI = 121, E_LO = 122, E_HI = 123, NE = 124, BR = 125, X0 = 126;
+constexpr uint64_t M32 = 0xFFFFFFFFULL;
+constexpr uint64_t KECCAK_CALL = ~0ULL - 1;  // a7 of the keccak ecall
+constexpr uint64_t EXIT_CALL = 93;
+// the ROM tuple's opcode ids (rv64.py OPS order, from 1)
+enum Op { ADD = 1, SUB, ADDI, LUI, BEQ, BNE, ECALL, XOR, OR, AND, XORI, ORI, ANDI, SLLI, SRLI, LD, SD };
+// Column layout of the CPU table (rv64_air.py); SEL0 + id - 1 is an opcode's
+// selector, SEL_KECCAK the keccak ecall's.
+constexpr int PC = 0, STEP = 1, CLK = 2, SEL0 = 3, SEL_KECCAK = 20, RD0 = 21, RS10 = 53, RS20 = 85, IMM_LO = 117,
+              IMM_HI = 118, IMM_F = 119, A_LO = 120, A_HI = 121, B_LO = 122, B_HI = 123, R_LO = 124, R_HI = 125,
+              R16 = 126, C0 = 130, C1 = 131, INV_LO = 132, INV_HI = 133, E_LO = 134, E_HI = 135, NE = 136, BR = 137,
+              AB0 = 138, BB0 = 146, RB0 = 154, MA = 162, MW0 = 163, MW1 = 164, MV_LO = 165, MV_HI = 166, MT = 167,
+              MD0 = 168, MD1 = 169, NV_LO = 170, NV_HI = 171, X0 = 172;
 static_assert(X0 + 62 == SG_RV64_CPU_WIDTH, "CPU table width");
 
 struct Ins {
@@ -39,10 +55,25 @@ bool decode(uint32_t w, Ins* o) {
     const uint32_t opc = w & 0x7F, rd = bits(w, 11, 7), f3 = bits(w, 14, 12), rs1 = bits(w, 19, 15),
                    rs2 = bits(w, 24, 20), f7 = bits(w, 31, 25);
     *o = Ins{0, (int)rd, (int)rs1, (int)rs2, 0};
-    if (opc == 0x33 && f3 == 0 && (f7 == 0 || f7 == 0x20)) {
-        o->op = f7 ? SUB : ADD;
-    } else if (opc == 0x13 && f3 == 0) {
-        *o = Ins{ADDI, (int)rd, (int)rs1, 0, sext(w >> 20, 12)};
+    if (opc == 0x33) {
+        if (f3 == 0 && (f7 == 0 || f7 == 0x20)) o->op = f7 ? SUB : ADD;
+        else if (f7 == 0 && f3 == 4) o->op = XOR;
+        else if (f7 == 0 && f3 == 6) o->op = OR;
+        else if (f7 == 0 && f3 == 7) o->op = AND;
+        else return false;
+    } else if (opc == 0x13) {
+        if (f3 == 1 || f3 == 5) {
+            if (bits(w, 31, 26) != 0) return false;
+            *o = Ins{f3 == 1 ? SLLI : SRLI, (int)rd, (int)rs1, 0, (int64_t)bits(w, 25, 20)};
+        } else {
+            const int op = f3 == 0 ? ADDI : f3 == 4 ? XORI : f3 == 6 ? ORI : f3 == 7 ? ANDI : 0;
+            if (!op) return false;
+            *o = Ins{op, (int)rd, (int)rs1, 0, sext(w >> 20, 12)};
+        }
+    } else if (opc == 0x03 && f3 == 3) {
+        *o = Ins{LD, (int)rd, (int)rs1, 0, sext(w >> 20, 12)};
+    } else if (opc == 0x23 && f3 == 3) {
+        *o = Ins{SD, 0, (int)rs1, (int)rs2, sext((f7 << 5) | rd, 12)};
     } else if (opc == 0x37) {
         *o = Ins{LUI, (int)rd, 0, 0, sext(w >> 12, 20) * 4096};
     } else if (opc == 0x63 && (f3 == 0 || f3 == 1)) {
@@ -56,72 +87,179 @@ bool decode(uint32_t w, Ins* o) {
     return true;
 }
 
+// keccak-f[1600] on the host, its round constants and rotation offsets
+// derived from their definitions in FIPS 202 (the rc(t) LFSR over
+// x^8 + x^6 + x^5 + x^4 + 1, the (x, y) -> (y, 2x + 3y) walk).
+struct KeccakTables {
+    uint64_t rc[24];
+    int rot[25];  // by lane x + 5y
+    KeccakTables() {
+        auto rc_bit = [](int t) {
+            if (t % 255 == 0) return 1u;
+            unsigned r = 1;
+            for (int i = 0; i < t % 255; ++i) {
+                r <<= 1;
+                if (r & 0x100) r ^= 0x171;
+            }
+            return r & 1u;
+        };
+        for (int ir = 0; ir < 24; ++ir) {
+            uint64_t c = 0;
+            for (int j = 0; j < 7; ++j) c |= (uint64_t)rc_bit(j + 7 * ir) << ((1 << j) - 1);
+            rc[ir] = c;
+        }
+        rot[0] = 0;
+        int x = 1, y = 0;
+        for (int t = 0; t < 24; ++t) {
+            rot[x + 5 * y] = ((t + 1) * (t + 2) / 2) % 64;
+            const int nx = y, ny = (2 * x + 3 * y) % 5;
+            x = nx, y = ny;
+        }
+    }
+};
+const KeccakTables& ktab() {
+    static const KeccakTables t;
+    return t;
+}
+uint64_t rotl(uint64_t v, int r) { return r ? (v << r) | (v >> (64 - r)) : v; }
+void keccak_f(uint64_t a[25]) {
+    const KeccakTables& k = ktab();
+    for (int ir = 0; ir < 24; ++ir) {
+        uint64_t c[5], d[5], b[25];
+        for (int x = 0; x < 5; ++x) c[x] = a[x] ^ a[x + 5] ^ a[x + 10] ^ a[x + 15] ^ a[x + 20];
+        for (int x = 0; x < 5; ++x) d[x] = c[(x + 4) % 5] ^ rotl(c[(x + 1) % 5], 1);
+        for (int x = 0; x < 5; ++x)
+            for (int y = 0; y < 5; ++y) b[y + 5 * ((2 * x + 3 * y) % 5)] = rotl(a[x + 5 * y] ^ d[x], k.rot[x + 5 * y]);
+        for (int x = 0; x < 5; ++x)
+            for (int y = 0; y < 5; ++y)
+                a[x + 5 * y] = b[x + 5 * y] ^ (~b[(x + 1) % 5 + 5 * y] & b[(x + 2) % 5 + 5 * y]);
+        a[0] ^= k.rc[ir];
+    }
+}
+
+struct Cell {
+    uint64_t value, stamp;
+};
+
 }  // namespace
 
 using namespace sg;
 
-extern "C" int sg_rv64_trace(const uint32_t* words, uint32_t nwords, uint64_t max_steps, uint64_t n_rows,
-                             uint64_t* trace_out, uint64_t* counts_out, uint64_t* a0_out, uint64_t* cycles_out) {
-    SG_CHECK_ARG(words && nwords && cycles_out && a0_out, "null argument");
-    SG_CHECK_ARG(!trace_out || (n_rows >= 2 && (n_rows & (n_rows - 1)) == 0), "n_rows must be a power of two >= 2");
+extern "C" int sg_rv64_run(const uint32_t* words, uint32_t nwords, uint64_t max_steps, uint64_t n_rows,
+                           uint64_t* cpu_out, uint64_t* counts_out, uint64_t* shifts_out, uint64_t* cells_out,
+                           uint64_t* keccak_out, void* reserved, sg_rv64_info* info) {
+    SG_CHECK_ARG(words && nwords && info && !reserved, "null argument");
+    SG_CHECK_ARG(!cpu_out || (n_rows >= 2 && (n_rows & (n_rows - 1)) == 0), "n_rows must be a power of two >= 2");
     std::vector<Ins> prog(nwords);
     for (uint32_t i = 0; i < nwords; ++i) SG_CHECK_ARG(decode(words[i], &prog[i]), "unsupported instruction word");
     if (counts_out) memset(counts_out, 0, nwords * sizeof(uint64_t));
     uint64_t x[32] = {0};
-    uint64_t pc = 0, t = 0;
+    uint64_t pc = 0, t = 0, nshift = 0, ncall = 0;
     const uint64_t W = SG_RV64_CPU_WIDTH;
-    auto row_of = [&](uint64_t r) { return trace_out + r * W; };
+    auto row_of = [&](uint64_t r) { return cpu_out + r * W; };
+    std::unordered_map<uint64_t, Cell> mem;
+    mem.reserve(1 << 16);
+    auto cell = [&](uint64_t addr, Cell** c) {
+        if (addr % 8 || addr >> 32) return false;
+        *c = &mem[addr];  // a new cell starts as (0, timestamp 0)
+        return true;
+    };
     bool halted = false;
     uint64_t halt_row = 0;
     while (!halted) {
         SG_CHECK_ARG(t < max_steps, "the program did not halt within max_steps");
         SG_CHECK_ARG(pc % 4 == 0 && pc / 4 < nwords, "pc outside the program");
         const Ins& in = prog[pc / 4];
-        const uint64_t a = x[in.rs1], b = x[in.rs2];
-        uint64_t r = 0, npc = pc + 4;
+        const uint64_t a = x[in.rs1], b = x[in.rs2], iu = (uint64_t)in.imm, clk = t + 1;
+        uint64_t r = 0, npc = pc + 4, ma = 0, mv = 0, mt = 0;
+        bool keccak = false;
         switch (in.op) {
             case ADD: r = a + b; break;
             case SUB: r = a - b; break;
-            case ADDI: r = a + (uint64_t)in.imm; break;
-            case LUI: r = (uint64_t)in.imm; break;
-            case BEQ: npc = a == b ? pc + (uint64_t)in.imm : pc + 4; break;
-            case BNE: npc = a != b ? pc + (uint64_t)in.imm : pc + 4; break;
+            case XOR: r = a ^ b; break;
+            case OR: r = a | b; break;
+            case AND: r = a & b; break;
+            case ADDI: r = a + iu; break;
+            case XORI: r = a ^ iu; break;
+            case ORI: r = a | iu; break;
+            case ANDI: r = a & iu; break;
+            case SLLI: r = a << in.imm; break;
+            case SRLI: r = a >> in.imm; break;
+            case LUI: r = iu; break;
+            case LD:
+            case SD: {
+                ma = a + iu;
+                Cell* c;
+                SG_CHECK_ARG(cell(ma, &c), "load / store address unaligned or outside the data space");
+                mv = c->value, mt = c->stamp;
+                if (in.op == LD) r = mv;
+                *c = Cell{in.op == LD ? mv : b, clk};
+                break;
+            }
+            case BEQ: npc = a == b ? pc + iu : pc + 4; break;
+            case BNE: npc = a != b ? pc + iu : pc + 4; break;
             case ECALL:
-                SG_CHECK_ARG(x[17] == 93, "only the exit ecall (a7 = 93) is supported");
-                halted = true;
-                npc = pc;
+                if (x[17] == EXIT_CALL) {
+                    halted = true;
+                    npc = pc;
+                } else {
+                    SG_CHECK_ARG(x[17] == KECCAK_CALL, "unsupported ecall (a7 is neither 93 nor 2^64 - 2)");
+                    keccak = true;
+                    ma = x[10];
+                    uint64_t lanes[25];
+                    Cell* cs[25];
+                    for (int i = 0; i < 25; ++i) {
+                        SG_CHECK_ARG(cell(ma + 8 * (uint64_t)i, &cs[i]), "keccak state unaligned or outside the data space");
+                        lanes[i] = cs[i]->value;
+                    }
+                    if (keccak_out) {
+                        uint64_t* k = keccak_out + 52 * ncall;
+                        k[0] = clk, k[1] = ma;
+                        for (int i = 0; i < 25; ++i) k[2 + i] = lanes[i], k[27 + i] = cs[i]->stamp;
+                    }
+                    keccak_f(lanes);
+                    for (int i = 0; i < 25; ++i) *cs[i] = Cell{lanes[i], clk};
+                    ++ncall;
+                }
                 break;
         }
-        if (trace_out) {
+        if (in.op == SLLI || in.op == SRLI) {
+            if (shifts_out) {
+                uint64_t* s = shifts_out + 3 * nshift;
+                s[0] = in.op == SRLI, s[1] = a, s[2] = iu;
+            }
+            ++nshift;
+        }
+        if (cpu_out) {
             SG_CHECK_ARG(t < n_rows, "the execution does not fit n_rows");
             uint64_t* row = row_of(t);
             memset(row, 0, W * 8);
             row[PC] = pc;
             row[STEP] = 1;
-            row[SEL0 + in.op - 1] = 1;
+            row[CLK] = clk;
+            row[keccak ? SEL_KECCAK : SEL0 + in.op - 1] = 1;
             row[RD0 + in.rd] = 1;
             row[RS10 + in.rs1] = 1;
             row[RS20 + in.rs2] = 1;
-            const uint64_t iu = (uint64_t)in.imm;
-            row[IMM_LO] = iu & 0xFFFFFFFFULL;
+            row[IMM_LO] = iu & M32;
             row[IMM_HI] = iu >> 32;
             row[IMM_F] = in.imm < 0 ? P - (uint64_t)(-in.imm) : iu;
-            row[A_LO] = a & 0xFFFFFFFFULL, row[A_HI] = a >> 32;
-            row[B_LO] = b & 0xFFFFFFFFULL, row[B_HI] = b >> 32;
-            row[R_LO] = r & 0xFFFFFFFFULL, row[R_HI] = r >> 32;
+            row[A_LO] = a & M32, row[A_HI] = a >> 32;
+            row[B_LO] = b & M32, row[B_HI] = b >> 32;
+            row[R_LO] = r & M32, row[R_HI] = r >> 32;
             for (int j = 0; j < 4; ++j) row[R16 + j] = (r >> (16 * j)) & 0xFFFF;
-            if (in.op == ADD || in.op == ADDI) {
+            if (in.op == ADD || in.op == ADDI || in.op == LD || in.op == SD) {
                 const uint64_t o = in.op == ADD ? b : iu;
-                const uint64_t c0 = ((a & 0xFFFFFFFFULL) + (o & 0xFFFFFFFFULL)) >> 32;
+                const uint64_t c0 = ((a & M32) + (o & M32)) >> 32;
                 row[C0] = c0;
                 row[C1] = ((a >> 32) + (o >> 32) + c0) >> 32;
             } else if (in.op == SUB) {
-                const uint64_t b0 = (a & 0xFFFFFFFFULL) < (b & 0xFFFFFFFFULL);
+                const uint64_t b0 = (a & M32) < (b & M32);
                 row[C0] = b0;
                 row[C1] = (a >> 32) < (b >> 32) + b0;
             }
             if (in.op == BEQ || in.op == BNE) {
-                const uint64_t dl = ((a & 0xFFFFFFFFULL) + P - (b & 0xFFFFFFFFULL)) % P;
+                const uint64_t dl = ((a & M32) + P - (b & M32)) % P;
                 const uint64_t dh = ((a >> 32) + P - (b >> 32)) % P;
                 row[INV_LO] = dl ? sg_host_gl_inv(dl) : 0;
                 row[INV_HI] = dh ? sg_host_gl_inv(dh) : 0;
@@ -130,24 +268,61 @@ extern "C" int sg_rv64_trace(const uint32_t* words, uint32_t nwords, uint64_t ma
                 row[NE] = ne;
                 row[BR] = in.op == BNE ? ne : 1 - ne;
             }
+            if (in.op >= XOR && in.op <= ANDI) {
+                const uint64_t second = in.op <= AND ? b : iu;
+                for (int i = 0; i < 8; ++i) {
+                    row[AB0 + i] = (a >> (8 * i)) & 0xFF;
+                    row[BB0 + i] = (second >> (8 * i)) & 0xFF;
+                    row[RB0 + i] = (r >> (8 * i)) & 0xFF;
+                }
+            }
+            if (in.op == LD || in.op == SD || keccak) {
+                row[MA] = ma;
+                row[MW0] = (ma >> 3) & 0xFFFF;
+                row[MW1] = ma >> 19;
+            }
+            if (in.op == LD || in.op == SD) {
+                row[MV_LO] = mv & M32, row[MV_HI] = mv >> 32;
+                row[MT] = mt;
+                const uint64_t gap = clk - mt - 1;
+                row[MD0] = gap & 0xFFFF, row[MD1] = gap >> 16;
+                const uint64_t nv = in.op == LD ? mv : b;
+                row[NV_LO] = nv & M32, row[NV_HI] = nv >> 32;
+            }
             for (int k = 1; k < 32; ++k) {
-                row[X0 + 2 * (k - 1)] = x[k] & 0xFFFFFFFFULL;
+                row[X0 + 2 * (k - 1)] = x[k] & M32;
                 row[X0 + 2 * (k - 1) + 1] = x[k] >> 32;
             }
         }
         if (counts_out) counts_out[pc / 4] += 1;
-        if (in.rd && (in.op == ADD || in.op == SUB || in.op == ADDI || in.op == LUI)) x[in.rd] = r;
+        const bool writes = !(in.op == BEQ || in.op == BNE || in.op == ECALL || in.op == SD);
+        if (in.rd && writes) x[in.rd] = r;
         halt_row = t;
         pc = npc;
         ++t;
     }
-    *cycles_out = t;
-    *a0_out = x[10];
-    if (trace_out) {
+    info->cycles = t;
+    info->a0 = x[10];
+    info->shifts = nshift;
+    info->cells = mem.size();
+    info->keccak_calls = ncall;
+    if (cpu_out) {
         // the halting row repeats to fill the table; the last row ends the cycle
-        for (uint64_t r = t; r < n_rows; ++r) memcpy(row_of(r), row_of(halt_row), W * 8);
+        for (uint64_t r = t; r < n_rows; ++r) {
+            memcpy(row_of(r), row_of(halt_row), W * 8);
+            row_of(r)[CLK] = r + 1;
+        }
         if (counts_out) counts_out[pc / 4] += n_rows - t;
         row_of(n_rows - 1)[STEP] = 0;
+    }
+    if (cells_out) {
+        std::vector<std::pair<uint64_t, Cell>> cs(mem.begin(), mem.end());
+        std::sort(cs.begin(), cs.end(), [](const auto& u, const auto& v) { return u.first < v.first; });
+        for (size_t i = 0; i < cs.size(); ++i) {
+            cells_out[3 * i] = cs[i].first;
+            cells_out[3 * i + 1] = cs[i].second.value;
+            cells_out[3 * i + 2] = cs[i].second.stamp;
+        }
     }
     return SG_OK;
 }

@@ -35,6 +35,11 @@ class PassRecord(C.Structure):
                 ("tiles", C.c_uint64), ("m", C.c_uint64), ("ms", C.c_float), ("pad2_", C.c_float)]
 
 
+class Rv64Info(C.Structure):
+    _fields_ = [("cycles", C.c_uint64), ("a0", C.c_uint64), ("shifts", C.c_uint64), ("cells", C.c_uint64),
+                ("keccak_calls", C.c_uint64)]
+
+
 class VerifyTable(C.Structure):
     _fields_ = [("log_n", C.c_uint32), ("log_N", C.c_uint32), ("m", C.c_uint32), ("aux_cols", C.c_uint32),
                 ("queries", C.c_uint32), ("fri_layers", C.c_uint32), ("total_folds", C.c_uint32),
@@ -169,7 +174,7 @@ PROTOTYPES = {
     "sg_decompose_d2": (i32, [vp, vp, vp, u64, vp, vp]),
     "sg_synth_trace": (i32, [vp, vp, vp, u64, u64, u64, u32]),
     "sg_ctx_pass_log": (i32, [vp, i32]),
-    "sg_rv64_trace": (i32, [vp, u32, u64, u64, vp, vp, C.POINTER(u64), C.POINTER(u64)]),
+    "sg_rv64_run": (i32, [vp, u32, u64, u64, vp, vp, vp, vp, vp, vp, vp]),
     "sg_verify_queries": (i32, [vp, vp, C.POINTER(VerifyTable), u32, vp]),
     "sg_ctx_pass_log_read": (i32, [vp, C.POINTER(PassRecord), u32, C.POINTER(u32)]),
     "sg_mlp_loss_grad": (i32, [vp, vp, vp, vp, u32, vp, vp, vp]),

@@ -1,30 +1,47 @@
-"""AIRs of the RV64 front-end: the CPU table and the 16-bit range table.
+"""AIRs of the RV64 front-end: the CPU table and the chips beside it.
 
-One CPU row per executed instruction (rv64.execute). The register file is
-carried in the row (x1..x31 as two 32-bit limbs each; x0 is zero and has no
-column), so register reads are one-hot dot products and writes are one-hot
-updates of the next row: no memory argument is needed for this ISA subset
-(ADD, SUB, ADDI, LUI, BEQ, BNE, ECALL). Every value written is range-checked
-limb by limb (four 16-bit pieces looked up in the RANGE table), so every
-register limb is below 2^32 and the 64-bit additions with boolean carries are
-exact integer identities in the field.
+Tables (a chip is present in a proof only when the execution uses it):
+
+* CPU: one row per executed instruction (rv64.run). The register file is
+  carried in the row (x1..x31 as two 32-bit limbs each; x0 is zero and has no
+  column), so register reads are one-hot dot products and writes are one-hot
+  updates of the next row. Every value written to a register is range-checked
+  limb by limb (four 16-bit pieces looked up in the RANGE table), so every
+  register limb is below 2^32 and 64-bit additions with boolean carries are
+  exact integer identities in the field.
+* RANGE: the values 0..2^16-1 with multiplicities.
+* BITWISE: every pair of bytes (x, y) with x XOR y, x OR y, x AND y; the CPU
+  looks up the eight byte triples of a bitwise instruction.
+* SHIFT: one row per executed shift (SLLI, SRLI): the operand's 64 bits and
+  the result of shifting them in two stages (by k mod 8 bits, then by k div 8
+  bytes).
+* MEMORY: one row per data-memory cell the run touches, sorted by address:
+  the cell's initial zero and its final value and timestamp. Offline memory
+  checking: every access receives the cell's (address, value, timestamp) as
+  the access before it left it and sends its own; a range check keeps each
+  previous timestamp below the access's.
+* KECCAK: 24 rows per keccak-f[1600] ecall, one per round, with the bits of
+  theta's column parities and output; it reads the 25 lanes from memory on
+  its first row and writes them back on its last.
 
 The prover's transition constraints are cyclic (they also link the last row
-to row 0). A STEP flag column marks the one row whose successor is not its
-next instruction: that row must be the halting ECALL (pc = the program's halt
-pc) and the row after it (cyclically: row 0) must hold the initial state
-(pc 0, every register zero). Its multiplicity (1 - STEP) on the END bus, which
-the verifier balances against one public (a0) tuple, makes it exactly one
-row. So the trace is one execution from the initial state to the halt, whose
-a0 is the claimed output.
+to row 0). A STEP flag column in the CPU table marks the one row whose
+successor is not its next instruction: that row must be an exit ECALL
+(a7 = 93, so the machine halts there) and the row after it (cyclically: row 0) must
+hold the initial state (pc 0, every register zero, timestamp 1). Its
+multiplicity (1 - STEP) on the END bus, which the verifier balances against
+one public (a0) tuple, makes it exactly one row. So the CPU table is one
+execution from the initial state to the halt, whose a0 is the claimed output.
 
 Buses (LogUp, lookup.rs conventions: fingerprint z - (bus + sum alpha^(i+1)
-v_i), senders +m, receivers -m): ROM (bus 1): each CPU row sends its
-instruction tuple (pc, opcode id, rd, rs1, rs2, imm low and high 32-bit limbs,
-imm as a field element); the verifier receives every instruction of the
-public program with its execution count. RANGE (bus 2): CPU rows send the four
-16-bit pieces of the written value, the RANGE table receives 0..2^16-1 with
-multiplicities. END (bus 3): see above. The public program, counts and output
+v_i), senders +m, receivers -m): ROM (1): each CPU row sends its instruction
+tuple (pc, opcode id, rd, rs1, rs2, imm low and high 32-bit limbs, imm as a
+field element); the verifier receives every instruction of the public
+program with its execution count. RANGE (2), END (3), BITWISE (4): (kind,
+x, y, result), SHIFT (5): (direction, a low, a high, amount, r low, r high),
+MEM (6): (address, value low, value high, timestamp), KECCAK (7): (timestamp,
+state address), WRAP (8): the one row of the MEMORY table whose successor is
+not the next address. The public program, counts, output and table heights
 are absorbed into the transcript label before any challenge is drawn.
 """
 import numpy as np
@@ -32,11 +49,15 @@ import numpy as np
 from . import field as F
 from .air import split_interactions
 from .ir import Builder
-from .rv64 import MASK64, OP_ID, OPS, decode, execute
+from .rv64 import EXIT, KECCAK, KECCAK_RC, KECCAK_ROT, MASK64, OP_ID, OPS, decode, run
 
 P = F.P
 NEG_ONE = P - 1
-BUS_ROM, BUS_RANGE, BUS_END = 1, 2, 3
+BUS_ROM, BUS_RANGE, BUS_END, BUS_BITWISE, BUS_SHIFT, BUS_MEM, BUS_KECCAK, BUS_WRAP = 1, 2, 3, 4, 5, 6, 7, 8
+TWO16, TWO32 = 1 << 16, 1 << 32
+MIN_LOG_N = 6
+CHIPS = ("bitwise", "shift", "memory", "keccak")
+_PROGRAMS = {}  # constraint programs by (table, parameters): a table's program depends on neither its height nor its trace
 
 
 class BusAir:
@@ -52,6 +73,11 @@ class BusAir:
         self.max_alpha = 1 + max(len(it["elems"]) for it in interactions)
         self.boundary = [(self.acc_col, True, 0)]
         self.num_parts = 2
+
+    def _program(self, key):
+        if key not in _PROGRAMS:
+            _PROGRAMS[key] = self._build_program()
+        return _PROGRAMS[key]
 
     @staticmethod
     def _lin(b, lin, offset=0):
@@ -134,10 +160,50 @@ class BusAir:
                 "num_committed": self.num_committed}
 
 
+def _col(c, coef=1):
+    return (0, [(coef, c)])
+
+
+def _sum_of(cols, coefs=None):
+    return (0, [(1 if coefs is None else coefs[i], c) for i, c in enumerate(cols)])
+
+
+class _Expr:
+    """Helpers over a Builder: sums, scaling, booleans, XOR of bits."""
+
+    def __init__(self, b):
+        self.b = b
+        self.one = b.const_base(1)
+        self.zero = b.const_base(0)
+
+    def total(self, es):
+        s = None
+        for e in es:
+            s = e if s is None else self.b.add(s, e)
+        return s if s is not None else self.zero
+
+    def scaled(self, k, e):
+        return e if k % P == 1 else self.b.mul(self.b.const_base(k % P), e)
+
+    def boolean(self, e):
+        self.b.emit(self.b.mul(e, self.b.sub(e, self.one)))
+
+    def xor2(self, x, y):
+        b = self.b
+        return b.sub(b.add(x, y), self.scaled(2, b.mul(x, y)))
+
+    def xor3(self, x, y, z):
+        """x ^ y ^ z of bits: x + y + z - 2(xy + yz + xz) + 4xyz."""
+        b = self.b
+        pairs = b.add(b.add(b.mul(x, y), b.mul(y, z)), b.mul(x, z))
+        return b.add(b.sub(b.add(b.add(x, y), z), self.scaled(2, pairs)), self.scaled(4, b.mul(b.mul(x, y), z)))
+
+
 # ---------------------------------------------------------------- CPU table columns
-PC, STEP = 0, 1
-SEL = {op: 2 + i for i, op in enumerate(OPS)}   # one-hot opcode selectors
-RD0 = 2 + len(OPS)                                # rd one-hot, 32 columns
+CPU_OPS = OPS + ("keccak",)   # the keccak ecall has a selector of its own; its ROM opcode is ECALL's
+PC, STEP, CLK = 0, 1, 2
+SEL = {op: 3 + i for i, op in enumerate(CPU_OPS)}  # one-hot opcode selectors
+RD0 = 3 + len(CPU_OPS)                            # rd one-hot, 32 columns
 RS10 = RD0 + 32                                   # rs1 one-hot
 RS20 = RS10 + 32                                  # rs2 one-hot
 IMM_LO, IMM_HI, IMM_F = RS20 + 32, RS20 + 33, RS20 + 34
@@ -146,9 +212,21 @@ R_LO, R_HI = B_HI + 1, B_HI + 2
 R16 = R_HI + 1                                    # four 16-bit pieces of the written value
 C0, C1 = R16 + 4, R16 + 5
 INV_LO, INV_HI, E_LO, E_HI, NE, BR = C1 + 1, C1 + 2, C1 + 3, C1 + 4, C1 + 5, C1 + 6
-X0 = BR + 1                                       # x1..x31: lo at X0 + 2(k-1), hi next
+AB0 = BR + 1                                      # bytes of a, of the second operand, of the result
+BB0 = AB0 + 8
+RB0 = BB0 + 8
+MA = RB0 + 8                                      # memory address (ld / sd / keccak state)
+MW0, MW1 = MA + 1, MA + 2                         # MA = 8 MW0 + 2^19 MW1
+MV_LO, MV_HI, MT = MA + 3, MA + 4, MA + 5         # the cell's value and timestamp before the access
+MD0, MD1 = MA + 6, MA + 7                         # CLK - MT - 1 in 16-bit pieces
+NV_LO, NV_HI = MA + 8, MA + 9                     # the value the access leaves
+X0 = NV_HI + 1                                    # x1..x31: lo at X0 + 2(k-1), hi next
 CPU_WIDTH = X0 + 62
-TWO16, TWO32 = 1 << 16, 1 << 32
+WRITES = ("add", "sub", "addi", "lui", "xor", "or", "and", "xori", "ori", "andi", "slli", "srli", "ld")
+BIT_REG, BIT_IMM = ("xor", "or", "and"), ("xori", "ori", "andi")
+BIT_KIND = {"xor": 1, "xori": 1, "or": 2, "ori": 2, "and": 3, "andi": 3}
+NEEDS = {"xor": "bitwise", "or": "bitwise", "and": "bitwise", "xori": "bitwise", "ori": "bitwise",
+         "andi": "bitwise", "slli": "shift", "srli": "shift", "ld": "memory", "sd": "memory"}
 
 
 def _batch_inverse(vals):
@@ -182,66 +260,95 @@ def rom_tuple(pc, op, rd, rs1, rs2, imm):
     return (pc, OP_ID[op], rd, rs1, rs2, u & 0xFFFFFFFF, u >> 32, imm % P)
 
 
+def _log2_rows(k):
+    return max(MIN_LOG_N, (max(k, 1) - 1).bit_length())
+
+
 class CpuAir(BusAir):
-    def __init__(self, words, log_n):
+    """The CPU table. `chips` names the chips the proof carries; the CPU's
+    lookups into a chip are part of the table only when the chip is, and an
+    instruction whose chip is absent cannot occur."""
+
+    def __init__(self, words, log_n, chips=()):
         self.words = list(words)
         self.prog = [decode(w) for w in self.words]
-        self.halt_pc = 4 * next(i for i, ins in enumerate(self.prog) if ins[0] == "ecall")
+        assert any(ins[0] == "ecall" for ins in self.prog), "a program halts by an ecall"
         self.log_n, self.n, self.width = log_n, 1 << log_n, CPU_WIDTH
-        self._logup_setup([
+        self.chips = tuple(c for c in CHIPS if c in chips)
+        rom_op = [(OP_ID["ecall" if o == "keccak" else o], SEL[o]) for o in CPU_OPS]
+        its = [
             {"bus": BUS_ROM, "sender": True, "mult": (1, []),
-             "elems": [(0, [(1, PC)]), (0, [(OP_ID[o], SEL[o]) for o in OPS]), (0, [(k, RD0 + k) for k in range(1, 32)]),
+             "elems": [_col(PC), (0, rom_op), (0, [(k, RD0 + k) for k in range(1, 32)]),
                        (0, [(k, RS10 + k) for k in range(1, 32)]), (0, [(k, RS20 + k) for k in range(1, 32)]),
-                       (0, [(1, IMM_LO)]), (0, [(1, IMM_HI)]), (0, [(1, IMM_F)])]},
-        ] + [{"bus": BUS_RANGE, "sender": True, "mult": (1, []), "elems": [(0, [(1, R16 + i)])]} for i in range(4)] + [
+                       _col(IMM_LO), _col(IMM_HI), _col(IMM_F)]},
+        ] + [{"bus": BUS_RANGE, "sender": True, "mult": (1, []), "elems": [_col(R16 + i)]} for i in range(4)] + [
             {"bus": BUS_END, "sender": True, "mult": (1, [(NEG_ONE, STEP)]),
-             "elems": [(0, [(1, xlo(10))]), (0, [(1, xhi(10))])]},
-        ])
-        self.program = self._build_program()
+             "elems": [_col(xlo(10)), _col(xhi(10))]},
+        ]
+        if "bitwise" in self.chips:
+            kind = (0, [(BIT_KIND[o], SEL[o]) for o in BIT_REG + BIT_IMM])
+            mult = _sum_of([SEL[o] for o in BIT_REG + BIT_IMM])
+            its += [{"bus": BUS_BITWISE, "sender": True, "mult": mult,
+                     "elems": [kind, _col(AB0 + i), _col(BB0 + i), _col(RB0 + i)]} for i in range(8)]
+        if "shift" in self.chips:
+            its.append({"bus": BUS_SHIFT, "sender": True, "mult": _sum_of([SEL["slli"], SEL["srli"]]),
+                        "elems": [_col(SEL["srli"]), _col(A_LO), _col(A_HI), _col(IMM_LO), _col(R_LO),
+                                  _col(R_HI)]})
+        if "memory" in self.chips:
+            smem = _sum_of([SEL["ld"], SEL["sd"]])
+            saddr = _sum_of([SEL["ld"], SEL["sd"], SEL["keccak"]])
+            its += [
+                {"bus": BUS_MEM, "sender": False, "mult": smem,
+                 "elems": [_col(MA), _col(MV_LO), _col(MV_HI), _col(MT)]},
+                {"bus": BUS_MEM, "sender": True, "mult": smem,
+                 "elems": [_col(MA), _col(NV_LO), _col(NV_HI), _col(CLK)]},
+                {"bus": BUS_RANGE, "sender": True, "mult": saddr, "elems": [_col(MW0)]},
+                {"bus": BUS_RANGE, "sender": True, "mult": saddr, "elems": [_col(MW1, 8)]},
+                {"bus": BUS_RANGE, "sender": True, "mult": smem, "elems": [_col(MD0)]},
+                {"bus": BUS_RANGE, "sender": True, "mult": smem, "elems": [_col(MD1)]},
+            ]
+        if "keccak" in self.chips:
+            its.append({"bus": BUS_KECCAK, "sender": True, "mult": _col(SEL["keccak"]),
+                        "elems": [_col(CLK), _col(MA)]})
+        self._logup_setup(its)
+        self.program = self._program(("cpu", self.chips))
 
     def _build_program(self):
         b = Builder()
+        x = _Expr(b)
         M = lambda c: b.main(0, c)
         N = lambda c: b.main(1, c)
-        one = b.const_base(1)
+        one = x.one
         k32 = b.const_base(TWO32)
+        k16 = b.const_base(TWO16)
         sel = {o: M(c) for o, c in SEL.items()}
+        sel_sum = lambda ops: x.total([sel[o] for o in ops])
         step = M(STEP)
         nstep = b.sub(one, step)
-
-        def boolean(e):
-            b.emit(b.mul(e, b.sub(e, one)))
-
-        def total(cols):
-            s = M(cols[0])
-            for c in cols[1:]:
-                s = b.add(s, M(c))
-            return s
+        has = lambda chip: chip in self.chips
 
         # one-hot selections and booleans
         for c in [STEP, C0, C1] + list(SEL.values()) + [RD0 + k for k in range(32)] + \
                 [RS10 + k for k in range(32)] + [RS20 + k for k in range(32)]:
-            boolean(M(c))
+            x.boolean(M(c))
         for group in (list(SEL.values()), [RD0 + k for k in range(32)], [RS10 + k for k in range(32)],
                       [RS20 + k for k in range(32)]):
-            b.emit(b.sub(total(group), one))
+            b.emit(b.sub(x.total([M(c) for c in group]), one))
+        # an instruction whose chip the proof does not carry cannot occur
+        for o, chip in list(NEEDS.items()) + [("keccak", "keccak")]:
+            if not has(chip) or (o == "keccak" and not has("memory")):
+                b.emit(sel[o])
 
         # operand reads: a = x[rs1], b = x[rs2] (x0 = 0 has no column)
         def read(base, limb):
-            s = None
-            for k in range(1, 32):
-                t = b.mul(M(base + k), M(xlo(k) if limb == 0 else xhi(k)))
-                s = t if s is None else b.add(s, t)
-            return s
+            return x.total([b.mul(M(base + k), M(xlo(k) if limb == 0 else xhi(k))) for k in range(1, 32)])
         b.emit(b.sub(M(A_LO), read(RS10, 0)))
         b.emit(b.sub(M(A_HI), read(RS10, 1)))
         b.emit(b.sub(M(B_LO), read(RS20, 0)))
         b.emit(b.sub(M(B_HI), read(RS20, 1)))
         # written value in 16-bit pieces (each one looked up in the RANGE table)
-        k16 = b.const_base(TWO16)
         b.emit(b.sub(M(R_LO), b.add(M(R16), b.mul(k16, M(R16 + 1)))))
         b.emit(b.sub(M(R_HI), b.add(M(R16 + 2), b.mul(k16, M(R16 + 3)))))
-        # results per opcode, with 32-bit carries
         rl, rh, al, ah, bl, bh, c0, c1 = (M(c) for c in (R_LO, R_HI, A_LO, A_HI, B_LO, B_HI, C0, C1))
         il, ih = M(IMM_LO), M(IMM_HI)
         # add / addi: r + c*2^32 = a + b (limb by limb, carry c0 into the high limb)
@@ -254,11 +361,11 @@ class CpuAir(BusAir):
         # lui: r = imm
         b.emit(b.mul(sel["lui"], b.sub(rl, il)))
         b.emit(b.mul(sel["lui"], b.sub(rh, ih)))
-        # no value for branches and ecall; no carries where none is used
-        nores = b.add(b.add(sel["beq"], sel["bne"]), sel["ecall"])
+        # no value for branches, ecalls and stores; carries only where an addition uses them
+        nores = sel_sum(("beq", "bne", "ecall", "keccak", "sd"))
         b.emit(b.mul(nores, rl))
         b.emit(b.mul(nores, rh))
-        nocarry = b.add(nores, sel["lui"])
+        nocarry = b.sub(one, sel_sum(("add", "addi", "sub", "ld", "sd")))
         b.emit(b.mul(nocarry, c0))
         b.emit(b.mul(nocarry, c1))
         # on branch rows, a != b: e = d * inv, d (1 - e) = 0 per limb; ne = e_lo
@@ -271,18 +378,56 @@ class CpuAir(BusAir):
         el, eh, ne = M(E_LO), M(E_HI), M(NE)
         b.emit(b.sub(ne, b.sub(b.add(el, eh), b.mul(el, eh))))
         b.emit(b.sub(M(BR), b.add(b.mul(sel["beq"], b.sub(one, ne)), b.mul(sel["bne"], ne))))
-        # transitions (rows with STEP = 1): next pc and the register file
+        # ecalls: exit with a7 = 93, keccak with a7 = 2^64 - 2
+        b.emit(b.mul(sel["ecall"], b.sub(M(xlo(17)), b.const_base(EXIT))))
+        b.emit(b.mul(sel["ecall"], M(xhi(17))))
+        b.emit(b.mul(sel["keccak"], b.sub(M(xlo(17)), b.const_base(KECCAK & 0xFFFFFFFF))))
+        b.emit(b.mul(sel["keccak"], b.sub(M(xhi(17)), b.const_base(KECCAK >> 32))))
+
+        if has("bitwise"):
+            # the operands and the result as bytes (each triple looked up in BITWISE)
+            def bytes_of(first, lo):
+                return x.total([x.scaled(1 << (8 * i), M(first + i + (0 if lo else 4))) for i in range(4)])
+            sreg, simm = sel_sum(BIT_REG), sel_sum(BIT_IMM)
+            sbit = b.add(sreg, simm)
+            for lo, (a_, b_, i_, r_) in ((True, (al, bl, il, rl)), (False, (ah, bh, ih, rh))):
+                b.emit(b.mul(sbit, b.sub(a_, bytes_of(AB0, lo))))
+                ob = bytes_of(BB0, lo)
+                b.emit(b.add(b.mul(sreg, b.sub(b_, ob)), b.mul(simm, b.sub(i_, ob))))
+                b.emit(b.mul(sbit, b.sub(r_, bytes_of(RB0, lo))))
+        if has("memory"):
+            smem = b.add(sel["ld"], sel["sd"])
+            saddr = b.add(smem, sel["keccak"])
+            ma = M(MA)
+            # ld / sd: address = a + imm below 2^32 (the high limbs' sum is 0 or 2^32)
+            b.emit(b.mul(smem, b.sub(b.add(ma, b.mul(c0, k32)), b.add(al, il))))
+            b.emit(b.mul(smem, b.sub(b.mul(c1, k32), b.add(b.add(ah, ih), c0))))
+            # keccak: the state address is a0, below 2^32
+            b.emit(b.mul(sel["keccak"], b.sub(ma, M(xlo(10)))))
+            b.emit(b.mul(sel["keccak"], M(xhi(10))))
+            # 8-byte aligned, below 2^32: MA = 8 MW0 + 2^19 MW1, MW0 and 8 MW1 in RANGE
+            b.emit(b.mul(saddr, b.sub(ma, b.add(x.scaled(8, M(MW0)), x.scaled(1 << 19, M(MW1))))))
+            # the previous access is earlier: CLK - MT - 1 = MD0 + 2^16 MD1
+            gap = b.sub(b.sub(M(CLK), M(MT)), one)
+            b.emit(b.mul(smem, b.sub(gap, b.add(M(MD0), b.mul(k16, M(MD1))))))
+            for nv, mv, bv, r_ in ((NV_LO, MV_LO, B_LO, rl), (NV_HI, MV_HI, B_HI, rh)):
+                b.emit(b.mul(sel["ld"], b.sub(M(nv), M(mv))))
+                b.emit(b.mul(sel["sd"], b.sub(M(nv), M(bv))))
+                b.emit(b.mul(sel["ld"], b.sub(r_, M(mv))))
+
+        # transitions (rows with STEP = 1): next pc, timestamp and register file
         four = b.const_base(4)
         adv = b.add(b.mul(four, b.sub(one, sel["ecall"])), b.mul(M(BR), b.sub(M(IMM_F), four)))
         b.emit(b.mul(step, b.sub(N(PC), b.add(M(PC), adv))))
+        b.emit(b.mul(step, b.sub(N(CLK), b.add(M(CLK), one))))
         for k in range(1, 32):
             for col, r in ((xlo(k), rl), (xhi(k), rh)):
                 upd = b.mul(M(RD0 + k), b.sub(r, M(col)))
                 b.emit(b.mul(step, b.sub(N(col), b.add(M(col), upd))))
-        # the END row (STEP = 0): the halting ECALL, followed by the initial state
-        b.emit(b.mul(nstep, b.sub(M(PC), b.const_base(self.halt_pc))))
+        # the END row (STEP = 0): an exit ECALL (a7 = 93, above), followed by the initial state
         b.emit(b.mul(nstep, b.sub(one, sel["ecall"])))
         b.emit(b.mul(nstep, N(PC)))
+        b.emit(b.mul(nstep, b.sub(N(CLK), one)))
         for k in range(1, 32):
             b.emit(b.mul(nstep, N(xlo(k))))
             b.emit(b.mul(nstep, N(xhi(k))))
@@ -290,28 +435,37 @@ class CpuAir(BusAir):
         return b.program()
 
     # ---------------------------------------------------------- trace
-    def trace(self, rows):
-        """CPU table of an execution (rv64.execute rows), padded to n rows by
-        repeating the halting ECALL; the last row is the END row. Built column
-        by column with numpy."""
+    def trace(self, rows, keccak_rows=()):
+        """CPU table of an execution (rv64.run rows; keccak_rows: the row
+        indices of Keccak ecalls), padded to n rows by repeating the halting
+        ECALL; the last row is the END row. Built column by column with numpy."""
         n, T = self.n, len(rows)
         assert 1 <= T <= n, "the execution does not fit the table"
         cols = list(zip(*rows))
         ext = lambda c: np.concatenate([c, np.full(n - T, c[-1], dtype=c.dtype)])
-        pc, rd, rs1, rs2 = (ext(np.array(cols[i], dtype=np.uint64)) for i in (0, 2, 3, 4))
+        u64 = lambda i: ext(np.array(cols[i], dtype=np.uint64))
+        pc, rd, rs1, rs2 = u64(0), u64(2), u64(3), u64(4)
         imm_i = ext(np.array(cols[5], dtype=np.int64))
         imm_u = imm_i.view(np.uint64)
-        a, bv, r = (ext(np.array(cols[i], dtype=np.uint64)) for i in (6, 7, 8))
-        op_of = {o: OP_ID[o] for o in OPS}
-        op = ext(np.array([op_of[o] for o in cols[1]], dtype=np.int64))
+        a, bv, r = u64(6), u64(7), u64(8)
+        if len(cols) > 9:
+            ma, mv, mt = u64(9), u64(10), u64(11)
+        else:
+            ma = mv = mt = np.zeros(n, np.uint64)
+        op = ext(np.array([OP_ID[o] for o in cols[1]], dtype=np.int64))
+        kecc = np.zeros(n, bool)
+        kecc[list(keccak_rows)] = True
+        is_op = lambda *names: np.isin(op, [OP_ID[o] for o in names])
         m32, s32 = np.uint64(0xFFFFFFFF), np.uint64(32)
+        idx = np.arange(n)
         t = np.zeros((CPU_WIDTH, n), dtype=np.uint64)  # column-major while filling
         t[PC] = pc
         t[STEP] = 1
         t[STEP, n - 1] = 0
-        opcol = 2 + op - 1  # SEL columns follow OPS order, ids start at 1
-        idx = np.arange(n)
-        t[opcol, idx] = 1
+        t[CLK] = idx + 1
+        selcol = np.array([SEL[o] for o in OPS])[op - 1]
+        selcol[kecc] = SEL["keccak"]
+        t[selcol, idx] = 1
         t[RD0 + rd.astype(np.int64), idx] = 1
         t[RS10 + rs1.astype(np.int64), idx] = 1
         t[RS20 + rs2.astype(np.int64), idx] = 1
@@ -322,7 +476,8 @@ class CpuAir(BusAir):
         t[R_LO], t[R_HI] = r & m32, r >> s32
         for j in range(4):
             t[R16 + j] = (r >> np.uint64(16 * j)) & np.uint64(0xFFFF)
-        is_add = (op == OP_ID["add"]) | (op == OP_ID["addi"])
+        # carries of the additions: add / addi / ld / sd (a + operand), sub's borrows
+        is_add = is_op("add", "addi", "ld", "sd")
         o = np.where(op == OP_ID["add"], bv, imm_u)
         c0 = ((a & m32) + (o & m32)) >> s32
         c1 = ((a >> s32) + (o >> s32) + c0) >> s32
@@ -332,16 +487,34 @@ class CpuAir(BusAir):
         t[C0] = np.where(is_add, c0, np.where(sb, b0, 0))
         t[C1] = np.where(is_add, c1, np.where(sb, b1, 0))
         # branch rows: per-limb difference, its inverse, the flags
-        br_rows = np.nonzero((op == OP_ID["beq"]) | (op == OP_ID["bne"]))[0]
+        br_rows = np.nonzero(is_op("beq", "bne"))[0]
         for ac, bc, ic, ec in ((A_LO, B_LO, INV_LO, E_LO), (A_HI, B_HI, INV_HI, E_HI)):
-            d = [(x - y) % P for x, y in zip(t[ac, br_rows].tolist(), t[bc, br_rows].tolist())]
+            d = [(x_ - y_) % P for x_, y_ in zip(t[ac, br_rows].tolist(), t[bc, br_rows].tolist())]
             t[ic, br_rows] = np.array(_batch_inverse(d), dtype=np.uint64)
-            t[ec, br_rows] = np.array([1 if x else 0 for x in d], dtype=np.uint64)
+            t[ec, br_rows] = np.array([1 if v else 0 for v in d], dtype=np.uint64)
         ne = t[E_LO] | t[E_HI]
         t[NE] = ne
         t[BR] = np.where(op == OP_ID["bne"], ne, np.where(op == OP_ID["beq"], 1 - ne, 0))
+        # bitwise rows: bytes of a, of the second operand, of the result
+        bit = is_op(*BIT_REG, *BIT_IMM)
+        second = np.where(is_op(*BIT_REG), bv, imm_u)
+        for first, v in ((AB0, a), (BB0, second), (RB0, r)):
+            for i in range(8):
+                t[first + i] = np.where(bit, (v >> np.uint64(8 * i)) & np.uint64(0xFF), 0)
+        # memory rows
+        mem = is_op("ld", "sd")
+        addr = mem | kecc
+        t[MA] = np.where(addr, ma, 0)
+        t[MW0] = np.where(addr, (ma >> np.uint64(3)) & np.uint64(0xFFFF), 0)
+        t[MW1] = np.where(addr, ma >> np.uint64(19), 0)
+        t[MV_LO], t[MV_HI] = np.where(mem, mv & m32, 0), np.where(mem, mv >> s32, 0)
+        t[MT] = np.where(mem, mt, 0)
+        gap = np.where(mem, (idx + 1).astype(np.uint64) - mt - np.uint64(1), np.uint64(0))
+        t[MD0], t[MD1] = gap & np.uint64(0xFFFF), gap >> np.uint64(16)
+        nv = np.where(op == OP_ID["ld"], mv, np.where(op == OP_ID["sd"], bv, 0))
+        t[NV_LO], t[NV_HI] = nv & m32, nv >> s32
         # register file before each row: the last value written below it
-        writes = np.isin(op, [OP_ID[x] for x in ("add", "sub", "addi", "lui")]) & (rd != 0) & (idx < T)
+        writes = is_op(*WRITES) & (rd != 0) & (idx < T)
         for k in range(1, 32):
             wk = np.where(writes & (rd == k), idx, -1)
             last = np.maximum.accumulate(wk)
@@ -352,19 +525,21 @@ class CpuAir(BusAir):
 
     def counts(self, rows):
         """Execution count of every program instruction over the n table rows."""
-        pcs = np.array([r[0] for r in rows], dtype=np.int64) // 4
+        pcs = np.array([r_[0] for r_ in rows], dtype=np.int64) // 4
         c = np.bincount(pcs, minlength=len(self.prog))
         c[pcs[-1]] += self.n - len(rows)  # the repeated halting row
         return [int(v) for v in c]
 
     def public_terms(self, counts, output):
-        """The verifier's side of the ROM and END buses: (bus, tuple, signed
-        multiplicity), receivers negative."""
+        """The verifier's side of the ROM and END buses (and of WRAP with the
+        memory chip): (bus, tuple, signed multiplicity), receivers negative."""
         terms = []
         for i, (op, rd, rs1, rs2, imm) in enumerate(self.prog):
             if counts[i]:
                 terms.append((BUS_ROM, rom_tuple(4 * i, op, rd, rs1, rs2, imm), -counts[i]))
         terms.append((BUS_END, (output & 0xFFFFFFFF, output >> 32), -1))
+        if "memory" in self.chips:
+            terms.append((BUS_WRAP, (1,), -1))
         return terms
 
 
@@ -374,12 +549,12 @@ class RangeAir(BusAir):
     cycle of 2^16 rows the V increments sum to zero, so W is 1 on exactly one
     row, where V = 2^16 - 1: V takes every value of 0..2^16-1 once."""
 
+    V, W, M = 0, 1, 2
+
     def __init__(self):
         self.log_n, self.n, self.width = 16, 1 << 16, 3
-        self.V, self.W, self.M = 0, 1, 2
-        self._logup_setup([{"bus": BUS_RANGE, "sender": False, "mult": (0, [(1, self.M)]),
-                            "elems": [(0, [(1, self.V)])]}])
-        self.program = self._build_program()
+        self._logup_setup([{"bus": BUS_RANGE, "sender": False, "mult": _col(self.M), "elems": [_col(self.V)]}])
+        self.program = self._program(("range",))
 
     def _build_program(self):
         b = Builder()
@@ -391,61 +566,549 @@ class RangeAir(BusAir):
         self._emit_logup(b)
         return b.program()
 
-    def trace(self, cpu_trace):
+    def trace(self, lookups):
+        """lookups: arrays of the 16-bit values looked up (with repetition)."""
         t = np.zeros((self.n, 3), np.uint64)
         t[:, self.V] = np.arange(self.n, dtype=np.uint64)
         t[self.n - 1, self.W] = 1
-        vals = cpu_trace[:, R16:R16 + 4].reshape(-1).astype(np.int64)
-        t[:, self.M] = np.bincount(vals, minlength=self.n).astype(np.uint64)
+        m = np.zeros(self.n, np.int64)
+        for v in lookups:
+            v = np.asarray(v).reshape(-1).astype(np.int64)
+            assert v.size == 0 or (v.min() >= 0 and v.max() < self.n), "a range lookup outside 0..2^16-1"
+            m += np.bincount(v, minlength=self.n)
+        t[:, self.M] = m.astype(np.uint64)
         return t
 
 
-def statement_label(words, counts, output):
+class BitwiseAir(BusAir):
+    """Every pair of bytes (x, y) with x XOR y, x OR y and x AND y, each with
+    a multiplicity: x and y are sums of boolean bit columns, so the table holds
+    bytes only, and each result is the bitwise identity over those bits."""
+
+    XB, YB, XOR, OR, AND, MX, MO, MAN = 0, 8, 16, 17, 18, 19, 20, 21
+
+    def __init__(self):
+        self.log_n, self.n, self.width = 16, 1 << 16, 22
+        xs = _sum_of([self.XB + i for i in range(8)], [1 << i for i in range(8)])
+        ys = _sum_of([self.YB + i for i in range(8)], [1 << i for i in range(8)])
+        self._logup_setup([{"bus": BUS_BITWISE, "sender": False, "mult": _col(m), "elems": [(k, []), xs, ys, _col(r)]}
+                           for k, r, m in ((1, self.XOR, self.MX), (2, self.OR, self.MO), (3, self.AND, self.MAN))])
+        self.program = self._program(("bitwise",))
+
+    def _build_program(self):
+        b = Builder()
+        x = _Expr(b)
+        M = lambda c: b.main(0, c)
+        xb = [M(self.XB + i) for i in range(8)]
+        yb = [M(self.YB + i) for i in range(8)]
+        for e in xb + yb:
+            x.boolean(e)
+        both = [b.mul(xb[i], yb[i]) for i in range(8)]
+        b.emit(b.sub(M(self.AND), x.total([x.scaled(1 << i, both[i]) for i in range(8)])))
+        b.emit(b.sub(M(self.XOR), x.total([x.scaled(1 << i, b.sub(b.add(xb[i], yb[i]), x.scaled(2, both[i])))
+                                           for i in range(8)])))
+        b.emit(b.sub(M(self.OR), x.total([x.scaled(1 << i, b.sub(b.add(xb[i], yb[i]), both[i]))
+                                          for i in range(8)])))
+        self._emit_logup(b)
+        return b.program()
+
+    def trace(self, cpu_trace):
+        t = np.zeros((self.n, self.width), np.uint64)
+        v = np.arange(self.n, dtype=np.uint64)
+        xv, yv = v >> np.uint64(8), v & np.uint64(0xFF)
+        for i in range(8):
+            t[:, self.XB + i] = (xv >> np.uint64(i)) & np.uint64(1)
+            t[:, self.YB + i] = (yv >> np.uint64(i)) & np.uint64(1)
+        t[:, self.XOR], t[:, self.OR], t[:, self.AND] = xv ^ yv, xv | yv, xv & yv
+        kind = np.zeros(cpu_trace.shape[0], np.int64)
+        for o, k in BIT_KIND.items():
+            kind[cpu_trace[:, SEL[o]] == 1] = k
+        for k, mcol in ((1, self.MX), (2, self.MO), (3, self.MAN)):
+            rows = kind == k
+            keys = (cpu_trace[rows, AB0:AB0 + 8].astype(np.int64) << 8) | cpu_trace[rows, BB0:BB0 + 8].astype(np.int64)
+            t[:, mcol] = np.bincount(keys.reshape(-1), minlength=self.n).astype(np.uint64)
+        return t
+
+
+class ShiftAir(BusAir):
+    """One row per executed shift: DIR (0 left, 1 right), the operand's 64
+    bits, the amount k = s + 8q as one-hot s (0..7) and q (0..7), the operand
+    shifted by s bits (TB), and the result's limbs: TB_j = sum_s S_s a_(j-+s),
+    r_i = sum_q Q_q TB_(i-+8q), bits shifted in are zero."""
+
+    DIR, AB, S, Q, TB, R_LO, R_HI, M = 0, 1, 65, 73, 81, 145, 146, 147
+
+    def __init__(self, log_n):
+        self.log_n, self.n, self.width = log_n, 1 << log_n, 148
+        k = (0, [(s, self.S + s) for s in range(1, 8)] + [(8 * q, self.Q + q) for q in range(1, 8)])
+        alo = _sum_of([self.AB + i for i in range(32)], [1 << i for i in range(32)])
+        ahi = _sum_of([self.AB + 32 + i for i in range(32)], [1 << i for i in range(32)])
+        self._logup_setup([{"bus": BUS_SHIFT, "sender": False, "mult": _col(self.M),
+                            "elems": [_col(self.DIR), alo, ahi, k, _col(self.R_LO), _col(self.R_HI)]}])
+        self.program = self._program(("shift",))
+
+    def _build_program(self):
+        b = Builder()
+        x = _Expr(b)
+        M = lambda c: b.main(0, c)
+        d = M(self.DIR)
+        nd = b.sub(x.one, d)
+        a = [M(self.AB + i) for i in range(64)]
+        s = [M(self.S + i) for i in range(8)]
+        q = [M(self.Q + i) for i in range(8)]
+        tb = [M(self.TB + i) for i in range(64)]
+        for e in [d] + a + s + q:
+            x.boolean(e)
+        b.emit(b.sub(x.total(s), x.one))
+        b.emit(b.sub(x.total(q), x.one))
+
+        def shifted(src, j, k_):
+            """Bit j of src shifted by k_ in the row's direction (None: zero either way)."""
+            parts = []
+            if j - k_ >= 0:
+                parts.append(b.mul(nd, src[j - k_]))
+            if j + k_ < 64:
+                parts.append(b.mul(d, src[j + k_]))
+            return x.total(parts) if parts else None
+
+        for j in range(64):
+            terms = [b.mul(s[k_], e) for k_ in range(8) if (e := shifted(a, j, k_)) is not None]
+            b.emit(b.sub(tb[j], x.total(terms)))
+        for limb, col in ((0, self.R_LO), (1, self.R_HI)):
+            acc = []
+            for i in range(32 * limb, 32 * limb + 32):
+                terms = [b.mul(q[k_], e) for k_ in range(8) if (e := shifted(tb, i, 8 * k_)) is not None]
+                if terms:
+                    acc.append(x.scaled(1 << (i - 32 * limb), x.total(terms)))
+            b.emit(b.sub(M(col), x.total(acc)))
+        self._emit_logup(b)
+        return b.program()
+
+    def trace(self, shifts):
+        """shifts: (dir, a, k) per executed shift."""
+        n = self.n
+        assert len(shifts) <= n, "the shifts do not fit the table"
+        t = np.zeros((n, self.width), np.uint64)
+        t[:, self.S] = 1
+        t[:, self.Q] = 1
+        if len(shifts) == 0:
+            return t
+        sh = np.asarray(shifts, dtype=np.uint64).reshape(-1, 3)
+        dr, av, kv = sh[:, 0], sh[:, 1], sh[:, 2]
+        m = sh.shape[0]
+        rows = np.arange(m)
+        t[:m, self.DIR] = dr
+        for i in range(64):
+            t[:m, self.AB + i] = (av >> np.uint64(i)) & np.uint64(1)
+        sv, qv = kv & np.uint64(7), kv >> np.uint64(3)
+        t[:m, self.S] = 0
+        t[:m, self.Q] = 0
+        t[rows, self.S + sv.astype(np.int64)] = 1
+        t[rows, self.Q + qv.astype(np.int64)] = 1
+        tv = np.where(dr == 1, av >> sv, av << sv)
+        for j in range(64):
+            t[:m, self.TB + j] = (tv >> np.uint64(j)) & np.uint64(1)
+        rv = np.where(dr == 1, av >> kv, av << kv)
+        t[:m, self.R_LO], t[:m, self.R_HI] = rv & np.uint64(0xFFFFFFFF), rv >> np.uint64(32)
+        t[:m, self.M] = 1
+        return t
+
+
+class MemoryAir(BusAir):
+    """One row per data-memory cell touched, addresses strictly increasing
+    down the table (ADDR(next) = ADDR + 8 + 8 (D0 + 2^16 D1), D0 and D1 in
+    RANGE) except on the one row where NW = 0 (the WRAP bus holds exactly one
+    such row against the verifier's public tuple), so no address has two rows.
+    Active rows send the cell's initial (address, 0, 0, timestamp 0) and
+    receive its final (address, value, timestamp); padding rows (ACT = 0)
+    continue the addresses."""
+
+    ADDR, V_LO, V_HI, T, ACT, NW, D0, D1 = range(8)
+
+    def __init__(self, log_n):
+        self.log_n, self.n, self.width = log_n, 1 << log_n, 8
+        self._logup_setup([
+            {"bus": BUS_MEM, "sender": True, "mult": _col(self.ACT),
+             "elems": [_col(self.ADDR), (0, []), (0, []), (0, [])]},
+            {"bus": BUS_MEM, "sender": False, "mult": _col(self.ACT),
+             "elems": [_col(self.ADDR), _col(self.V_LO), _col(self.V_HI), _col(self.T)]},
+            {"bus": BUS_RANGE, "sender": True, "mult": (1, []), "elems": [_col(self.D0)]},
+            {"bus": BUS_RANGE, "sender": True, "mult": (1, []), "elems": [_col(self.D1)]},
+            {"bus": BUS_WRAP, "sender": True, "mult": (1, [(NEG_ONE, self.NW)]), "elems": [(1, [])]},
+        ])
+        self.program = self._program(("memory",))
+
+    def _build_program(self):
+        b = Builder()
+        x = _Expr(b)
+        M = lambda c: b.main(0, c)
+        x.boolean(M(self.ACT))
+        x.boolean(M(self.NW))
+        step = b.add(b.const_base(8), b.add(x.scaled(8, M(self.D0)), x.scaled(8 << 16, M(self.D1))))
+        b.emit(b.mul(M(self.NW), b.sub(b.main(1, self.ADDR), b.add(M(self.ADDR), step))))
+        self._emit_logup(b)
+        return b.program()
+
+    def trace(self, addrs, values, stamps):
+        """The touched cells, sorted by address, with final values and timestamps."""
+        n = self.n
+        addrs = np.asarray(addrs, np.uint64)
+        k = addrs.size
+        assert 1 <= k <= n, "the memory cells do not fit the table"
+        t = np.zeros((n, self.width), np.uint64)
+        col = np.concatenate([addrs, addrs[-1] + np.uint64(8) * np.arange(1, n - k + 1, dtype=np.uint64)])
+        t[:, self.ADDR] = col
+        vals = np.asarray(values, np.uint64)
+        t[:k, self.V_LO], t[:k, self.V_HI] = vals & np.uint64(0xFFFFFFFF), vals >> np.uint64(32)
+        t[:k, self.T] = np.asarray(stamps, np.uint64)
+        t[:k, self.ACT] = 1
+        t[:n - 1, self.NW] = 1
+        d = (col[1:] - col[:-1] - np.uint64(8)) >> np.uint64(3)
+        t[:n - 1, self.D0], t[:n - 1, self.D1] = d & np.uint64(0xFFFF), d >> np.uint64(16)
+        return t
+
+
+# ---------------------------------------------------------------- KECCAK table columns
+def _lane(x, y):
+    return x + 5 * y
+
+
+KR = 0                  # round flags R_0..R_23
+KA = KR + 24            # the round's input lanes, 4 x 16-bit limbs each
+KC = KA + 100           # bits of theta's column parities C[x][z]
+KCP = KC + 320          # bits of C'[x][z] = C[x] ^ C[x-1] ^ rot(C[x+1], 1)
+KAP = KCP + 320         # bits of theta's output A'[x + 5y][z]
+KOUT = KAP + 1600       # the round's output lanes as limbs (lane 0 after iota)
+KB00 = KOUT + 100       # bits of lane 0 after chi, before iota
+KBASE = KB00 + 64       # state address
+KCLK = KBASE + 1        # the ecall's timestamp
+KTOLD = KCLK + 1        # previous timestamps of the 25 cells (first row)
+KTD = KTOLD + 25        # KCLK - KTOLD_i - 1 in 16-bit pieces (first row)
+KECCAK_WIDTH = KTD + 50
+
+
+class KeccakAir(BusAir):
+    """keccak-f[1600], one round per row, 24 rows per ecall (FIPS 202
+    theta, rho, pi, chi, iota on lanes A[x + 5y]).
+
+    Constraints: A's limbs are the bits A' ^ C ^ C'; for every (x, z) the
+    five A'[x][y][z] and C'[x][z] have even parity, so C is A's column parity
+    and A' = theta(A); OUT's limbs are chi of rho-pi of A' (lane 0: the stored
+    bits, then XOR the round constant selected by the flags); a row that is
+    not a permutation's last passes OUT on as the next row's A. The first row
+    of a permutation (R_0) takes (timestamp, address) from the CPU's ecall and
+    reads the 25 lanes from memory at earlier timestamps; the last (R_23)
+    writes them back at the ecall's timestamp. Rows outside permutations hold
+    the all-zero state with no flag set (every constraint holds on them)."""
+
+    def __init__(self, log_n):
+        self.log_n, self.n, self.width = log_n, 1 << log_n, KECCAK_WIDTH
+        lo = lambda base, i: (0, [(1, base + 4 * i), (TWO16, base + 4 * i + 1)])
+        hi = lambda base, i: (0, [(1, base + 4 * i + 2), (TWO16, base + 4 * i + 3)])
+        its = [{"bus": BUS_KECCAK, "sender": False, "mult": _col(KR), "elems": [_col(KCLK), _col(KBASE)]}]
+        for i in range(25):
+            addr = (8 * i, [(1, KBASE)])
+            its.append({"bus": BUS_MEM, "sender": False, "mult": _col(KR),
+                        "elems": [addr, lo(KA, i), hi(KA, i), _col(KTOLD + i)]})
+            its.append({"bus": BUS_MEM, "sender": True, "mult": _col(KR + 23),
+                        "elems": [addr, lo(KOUT, i), hi(KOUT, i), _col(KCLK)]})
+        for j in range(50):
+            its.append({"bus": BUS_RANGE, "sender": True, "mult": _col(KR), "elems": [_col(KTD + j)]})
+        self._logup_setup(its)
+        self.program = self._program(("keccak",))
+
+    def _build_program(self):
+        b = Builder()
+        e = _Expr(b)
+        M = lambda c: b.main(0, c)
+        N = lambda c: b.main(1, c)
+        one = e.one
+        r = [M(KR + i) for i in range(24)]
+        for f in r:
+            e.boolean(f)
+        e.boolean(e.total(r))
+        C = [[M(KC + 64 * x + z) for z in range(64)] for x in range(5)]
+        CP = [[M(KCP + 64 * x + z) for z in range(64)] for x in range(5)]
+        AP = [[[M(KAP + 64 * _lane(x, y) + z) for z in range(64)] for y in range(5)] for x in range(5)]
+        B00 = [M(KB00 + z) for z in range(64)]
+        for x in range(5):
+            for z in range(64):
+                e.boolean(C[x][z])
+                e.boolean(CP[x][z])
+                for y in range(5):
+                    e.boolean(AP[x][y][z])
+        for z in range(64):
+            e.boolean(B00[z])
+        # theta
+        two, four = b.const_base(2), b.const_base(4)
+        for x in range(5):
+            for z in range(64):
+                b.emit(b.sub(CP[x][z], e.xor3(C[x][z], C[(x - 1) % 5][z], C[(x + 1) % 5][(z - 1) % 64])))
+                t = b.sub(e.total([AP[x][y][z] for y in range(5)]), CP[x][z])
+                b.emit(b.mul(b.mul(t, b.sub(t, two)), b.sub(t, four)))
+        for x in range(5):
+            for y in range(5):
+                for l in range(4):
+                    bits = [e.xor3(AP[x][y][z], C[x][z], CP[x][z]) for z in range(16 * l, 16 * l + 16)]
+                    b.emit(b.sub(M(KA + 4 * _lane(x, y) + l), e.total([e.scaled(1 << i, v) for i, v in enumerate(bits)])))
+        # rho and pi: Bm[y][2x + 3y] = rot(A'[x][y], r[x][y])
+        Bm = [[None] * 5 for _ in range(5)]
+        for x in range(5):
+            for y in range(5):
+                rr = KECCAK_ROT[x][y]
+                Bm[y][(2 * x + 3 * y) % 5] = [AP[x][y][(z - rr) % 64] for z in range(64)]
+
+        def chi(x, y, z):
+            b0, b1, b2 = Bm[x][y][z], Bm[(x + 1) % 5][y][z], Bm[(x + 2) % 5][y][z]
+            return e.xor2(b0, b.mul(b.sub(one, b1), b2))
+        for x in range(5):
+            for y in range(5):
+                if (x, y) == (0, 0):
+                    continue
+                for l in range(4):
+                    v = e.total([e.scaled(1 << i, chi(x, y, z)) for i, z in enumerate(range(16 * l, 16 * l + 16))])
+                    b.emit(b.sub(M(KOUT + 4 * _lane(x, y) + l), v))
+        for z in range(64):
+            b.emit(b.sub(B00[z], chi(0, 0, z)))
+        # iota on lane 0: the round constant's bit z is the sum of the flags whose constant has it
+        for l in range(4):
+            acc = []
+            for i, z in enumerate(range(16 * l, 16 * l + 16)):
+                fl = [r[ir] for ir in range(24) if (KECCAK_RC[ir] >> z) & 1]
+                acc.append(e.scaled(1 << i, e.xor2(B00[z], e.total(fl)) if fl else B00[z]))
+            b.emit(b.sub(M(KOUT + l), e.total(acc)))
+        # transitions inside a permutation
+        for i in range(23):
+            b.emit(b.sub(N(KR + i + 1), r[i]))
+        g = e.total(r[:23])
+        for c in range(100):
+            b.emit(b.mul(g, b.sub(N(KA + c), M(KOUT + c))))
+        b.emit(b.mul(g, b.sub(N(KBASE), M(KBASE))))
+        b.emit(b.mul(g, b.sub(N(KCLK), M(KCLK))))
+        # reads are of earlier timestamps: KCLK - KTOLD_i - 1 = KTD_2i + 2^16 KTD_2i+1
+        for i in range(25):
+            gap = b.sub(b.sub(M(KCLK), M(KTOLD + i)), one)
+            v = b.add(M(KTD + 2 * i), e.scaled(TWO16, M(KTD + 2 * i + 1)))
+            b.emit(b.mul(r[0], b.sub(gap, v)))
+        self._emit_logup(b)
+        return b.program()
+
+    def trace(self, clocks, bases, lanes, told):
+        """One permutation per ecall: its timestamp, state address, the 25
+        input lanes and the cells' previous timestamps (arrays, one row per
+        ecall)."""
+        n = self.n
+        clk = np.asarray(clocks, np.uint64).reshape(-1)
+        Pn = clk.size
+        assert 24 * Pn <= n, "the permutations do not fit the table"
+        t = np.zeros((n, KECCAK_WIDTH), np.uint64)
+        if not Pn:
+            return t
+        sh = np.arange(64, dtype=np.uint64)
+        bits = lambda v: (v[..., None] >> sh) & np.uint64(1)
+
+        def rotl(v, k):
+            k %= 64
+            return v if k == 0 else (v << np.uint64(k)) | (v >> np.uint64(64 - k))
+
+        a = np.asarray(lanes, np.uint64).reshape(Pn, 25)
+        base = np.asarray(bases, np.uint64).reshape(-1)
+        told = np.asarray(told, np.uint64).reshape(Pn, 25)
+        rows0 = 24 * np.arange(Pn)
+        for ir in range(24):
+            rows = rows0 + ir
+            t[rows, KR + ir] = 1
+            t[rows, KBASE] = base
+            t[rows, KCLK] = clk
+            for l in range(4):
+                t[rows, KA + l:KA + 100:4] = (a >> np.uint64(16 * l)) & np.uint64(0xFFFF)
+            c = a[:, 0:5] ^ a[:, 5:10] ^ a[:, 10:15] ^ a[:, 15:20] ^ a[:, 20:25]
+            d = np.stack([c[:, (x - 1) % 5] ^ rotl(c[:, (x + 1) % 5], 1) for x in range(5)], axis=1)
+            ap = a ^ np.tile(d, (1, 5))
+            t[rows, KC:KC + 320] = bits(c).reshape(Pn, 320)
+            t[rows, KCP:KCP + 320] = bits(c ^ d).reshape(Pn, 320)
+            t[rows, KAP:KAP + 1600] = bits(ap).reshape(Pn, 1600)
+            bm = np.zeros_like(a)
+            for x in range(5):
+                for y in range(5):
+                    bm[:, _lane(y, (2 * x + 3 * y) % 5)] = rotl(ap[:, _lane(x, y)], KECCAK_ROT[x][y])
+            out = np.zeros_like(a)
+            for x in range(5):
+                for y in range(5):
+                    out[:, _lane(x, y)] = bm[:, _lane(x, y)] ^ (~bm[:, _lane((x + 1) % 5, y)] &
+                                                               bm[:, _lane((x + 2) % 5, y)])
+            t[rows, KB00:KB00 + 64] = bits(out[:, 0])
+            out[:, 0] ^= np.uint64(KECCAK_RC[ir])
+            for l in range(4):
+                t[rows, KOUT + l:KOUT + 100:4] = (out >> np.uint64(16 * l)) & np.uint64(0xFFFF)
+            a = out
+        t[rows0, KTOLD:KTOLD + 25] = told
+        gap = clk[:, None] - told - np.uint64(1)
+        t[rows0, KTD:KTD + 50:2] = gap & np.uint64(0xFFFF)
+        t[rows0, KTD + 1:KTD + 50:2] = gap >> np.uint64(16)
+        return t
+
+
+# ---------------------------------------------------------------- statements
+def statement_label(words, counts, output, heights=None):
     """Transcript label binding the public statement (program words, counts,
-    output) before any challenge is drawn."""
+    output and, with chips beside the CPU table, the chips' heights) before
+    any challenge is drawn."""
     from .math_cuda import keccak256
     blob = b"".join(int(w).to_bytes(4, "little") for w in words)
     blob += b"".join(int(c).to_bytes(8, "little") for c in counts)
     blob += int(output).to_bytes(8, "little")
+    if heights and any(c in heights for c in CHIPS):
+        blob += bytes(int(heights.get(c, 0)) for c in CHIPS)
     return b"lambda_vm_b200/rv64/" + keccak256(blob)
 
 
-def native_trace(words, max_steps=1 << 32):
-    """Execute and build the CPU table in the library (sg_rv64_trace, C++):
-    (table, counts, a0, cycles)."""
+def chips_of(heights):
+    return tuple(c for c in CHIPS if c in (heights or {}))
+
+
+def airs_for(words, counts, heights=None):
+    """The verifier's tables of a statement (it never executes the program):
+    the CPU table has one row per counted instruction execution; the chips'
+    heights (log2 rows) are part of the statement."""
+    heights = heights or {}
+    n = sum(int(c) for c in counts)
+    assert n >= 2 and n & (n - 1) == 0, "the counts must cover a power-of-two table"
+    chips = chips_of(heights)
+    airs = [CpuAir(words, n.bit_length() - 1, chips), RangeAir()]
+    if "bitwise" in chips:
+        airs.append(BitwiseAir())
+    if "shift" in chips:
+        airs.append(ShiftAir(heights["shift"]))
+    if "memory" in chips:
+        airs.append(MemoryAir(heights["memory"]))
+    if "keccak" in chips:
+        airs.append(KeccakAir(heights["keccak"]))
+    return airs
+
+
+class Events:
+    """What the chips need from a run, as arrays: the CPU table, counts, a0,
+    cycles; shifts (dir, a, k); the touched cells (sorted addresses, final
+    values, final timestamps); Keccak ecalls (timestamps, addresses, input
+    lanes, previous timestamps)."""
+
+    def __init__(self, cpu_trace, counts, output, cycles, shifts, cells, keccak):
+        self.cpu_trace, self.counts, self.output, self.cycles = cpu_trace, counts, output, cycles
+        self.shifts, self.cells, self.keccak = shifts, cells, keccak
+
+
+def python_events(words, max_steps=1 << 26, log_n=None):
+    """Events of a run of the Python executor (rv64.run) with the CPU table
+    built in numpy."""
+    ex = run(words, max_steps)
+    rows = ex.rows
+    T = len(rows)
+    chips = _chips_used(rows, ex)
+    cpu = CpuAir(words, log_n or max(1, (T - 1).bit_length()), chips)
+    ct = cpu.trace(rows, [k[0] for k in ex.keccak])
+    shifts = np.array([(1 if r_[1] == "srli" else 0, r_[6], r_[5]) for r_ in rows if r_[1] in ("slli", "srli")],
+                      np.uint64).reshape(-1, 3)
+    addrs = sorted(ex.memory)
+    cells = (np.array(addrs, np.uint64), np.array([ex.memory[a][0] for a in addrs], np.uint64),
+             np.array([ex.memory[a][1] for a in addrs], np.uint64))
+    kc = (np.array([k[0] + 1 for k in ex.keccak], np.uint64), np.array([k[1] for k in ex.keccak], np.uint64),
+          np.array([k[2] for k in ex.keccak], np.uint64).reshape(-1, 25),
+          np.array([k[3] for k in ex.keccak], np.uint64).reshape(-1, 25))
+    return Events(ct, cpu.counts(rows), ex.regs[10], T, shifts, cells, kc)
+
+
+def _chips_used(rows, ex):
+    ops = {r_[1] for r_ in rows}
+    used = {NEEDS[o] for o in ops if o in NEEDS}
+    if ex.keccak:
+        used |= {"keccak", "memory"}
+    return tuple(c for c in CHIPS if c in used)
+
+
+def tables_from_events(words, ev):
+    """(airs, traces, public) of a run's events: public = {"words", "counts",
+    "output", "cycles", "heights", "label", "terms"}."""
+    ct = ev.cpu_trace
+    heights = {"cpu": ct.shape[0].bit_length() - 1, "range": 16}
+    bit = any(ct[:, SEL[o]].any() for o in BIT_REG + BIT_IMM)
+    if bit:
+        heights["bitwise"] = 16
+    if len(ev.shifts):
+        heights["shift"] = _log2_rows(len(ev.shifts))
+    if len(ev.cells[0]):
+        heights["memory"] = _log2_rows(len(ev.cells[0]))
+    if len(ev.keccak[0]):
+        heights["keccak"] = _log2_rows(24 * len(ev.keccak[0]))
+    chips = chips_of(heights)
+    cpu = CpuAir(words, heights["cpu"], chips)
+    airs, traces = [cpu, RangeAir()], [ct, None]
+    look = [ct[:, R16:R16 + 4]]
+    if "bitwise" in chips:
+        a = BitwiseAir()
+        airs.append(a)
+        traces.append(a.trace(ct))
+    if "shift" in chips:
+        a = ShiftAir(heights["shift"])
+        airs.append(a)
+        traces.append(a.trace(ev.shifts))
+    if "memory" in chips:
+        a = MemoryAir(heights["memory"])
+        mt = a.trace(*ev.cells)
+        airs.append(a)
+        traces.append(mt)
+        addr = (ct[:, SEL["ld"]] + ct[:, SEL["sd"]] + ct[:, SEL["keccak"]]) == 1
+        mem = (ct[:, SEL["ld"]] + ct[:, SEL["sd"]]) == 1
+        look += [ct[addr, MW0], np.uint64(8) * ct[addr, MW1], ct[mem, MD0], ct[mem, MD1],
+                 mt[:, MemoryAir.D0], mt[:, MemoryAir.D1]]
+    if "keccak" in chips:
+        a = KeccakAir(heights["keccak"])
+        kt = a.trace(*ev.keccak)
+        airs.append(a)
+        traces.append(kt)
+        look.append(kt[kt[:, KR] == 1, KTD:KTD + 50])
+    traces[1] = airs[1].trace(look)
+    pub = {"words": list(words), "counts": ev.counts, "output": ev.output, "cycles": ev.cycles,
+           "heights": heights, "label": statement_label(words, ev.counts, ev.output, heights),
+           "terms": cpu.public_terms(ev.counts, ev.output)}
+    return airs, traces, pub
+
+
+def native_events(words, max_steps=1 << 32):
+    """Events of a run of the library's C++ executor (sg_rv64_run), which
+    writes the CPU table as it runs."""
     import ctypes as C
     from . import native
     L = native.lib()
     w = np.ascontiguousarray(np.asarray(words, dtype=np.uint32))
-    a0, cyc = C.c_uint64(), C.c_uint64()
-    native.check(L.sg_rv64_trace(w.ctypes.data, len(w), max_steps, 0, None, None, C.byref(a0), C.byref(cyc)))
-    n = 1 << max(1, (cyc.value - 1).bit_length())
-    t = np.empty((n, CPU_WIDTH), np.uint64)
+    info = native.Rv64Info()
+    native.check(L.sg_rv64_run(w.ctypes.data, len(w), max_steps, 0, None, None, None, None, None, None,
+                               C.byref(info)))
+    n = 1 << max(1, (info.cycles - 1).bit_length())
+    ct = np.empty((n, CPU_WIDTH), np.uint64)
     counts = np.zeros(len(w), np.uint64)
-    native.check(L.sg_rv64_trace(w.ctypes.data, len(w), max_steps, n, t.ctypes.data, counts.ctypes.data,
-                                 C.byref(a0), C.byref(cyc)))
-    return t, [int(c) for c in counts], a0.value, cyc.value
+    shifts = np.empty((info.shifts, 3), np.uint64)
+    cells = np.empty((info.cells, 3), np.uint64)
+    kc = np.empty((info.keccak_calls, 52), np.uint64)
+    ptr = lambda a: a.ctypes.data if a.size else None
+    native.check(L.sg_rv64_run(w.ctypes.data, len(w), max_steps, n, ct.ctypes.data, counts.ctypes.data,
+                               ptr(shifts), ptr(cells), ptr(kc), None, C.byref(info)))
+    return Events(ct, [int(c) for c in counts], info.a0, info.cycles, shifts,
+                  (cells[:, 0].copy(), cells[:, 1].copy(), cells[:, 2].copy()),
+                  (kc[:, 0].copy(), kc[:, 1].copy(), kc[:, 2:27].copy(), kc[:, 27:52].copy()))
 
 
-def build(words):
-    """Execute a program and build its tables (the CPU table by the library's
-    native executor): (airs, traces, public) with public = {"words", "counts",
-    "output", "cycles", "label", "terms"}."""
-    ct, counts, out, cycles = native_trace(words)
-    cpu = CpuAir(words, ct.shape[0].bit_length() - 1)
-    rng = RangeAir()
-    rt = rng.trace(ct)
-    pub = {"words": list(words), "counts": counts, "output": out, "cycles": cycles,
-           "label": statement_label(words, counts, out), "terms": cpu.public_terms(counts, out)}
-    return [cpu, rng], [ct, rt], pub
+def build(words, native_exec=True):
+    """Execute a program and build its tables (by default with the library's
+    native executor): (airs, traces, public)."""
+    ev = native_events(words) if native_exec else python_events(words)
+    return tables_from_events(words, ev)
 
 
-def airs_for(words, counts):
-    """The verifier's tables of a statement (it never executes the program):
-    the CPU table has one row per counted instruction execution."""
-    n = sum(int(c) for c in counts)
-    assert n >= 2 and n & (n - 1) == 0, "the counts must cover a power-of-two table"
-    return [CpuAir(words, n.bit_length() - 1), RangeAir()]
+def native_trace(words, max_steps=1 << 32):
+    """(CPU table, counts, a0, cycles) of a run of the native executor."""
+    ev = native_events(words, max_steps)
+    return ev.cpu_trace, ev.counts, ev.output, ev.cycles
 
 
 def prove(words, opts, bk):
@@ -457,11 +1120,12 @@ def prove(words, opts, bk):
     return proof, pub
 
 
-def verify(words, counts, output, proof, opts, device=None):
+def verify(words, counts, output, proof, opts, device=None, heights=None):
     """Verify that `words` run from the initial state halts with a0 = output,
-    having executed each instruction counts[i] times: (ok, reason)."""
+    having executed each instruction counts[i] times, with the chips'
+    heights of the statement: (ok, reason)."""
     from . import verifier
-    airs = airs_for(words, counts)
+    airs = airs_for(words, counts, heights)
     cpu = airs[0]
-    return verifier.verify(airs, proof, opts, label=statement_label(words, counts, output), device=device,
+    return verifier.verify(airs, proof, opts, label=statement_label(words, counts, output, heights), device=device,
                            public_terms=cpu.public_terms(counts, output))

@@ -31,3 +31,38 @@ def test_fibonacci_execution_proof_verifies(be, n):
     bad[3] += 1
     bad[0] -= 1
     assert RA.verify(words, bad, out, proof, OPTS)[0] is False
+
+
+@pytest.mark.parametrize("blocks", [1, 9])
+def test_keccak_guest_proof_verifies(be, blocks):
+    """The Keccak guest (xorshift buffer, keccak-f ecalls, load/store
+    XOR-folds): CPU, RANGE, BITWISE, SHIFT, MEMORY and KECCAK tables proved on
+    the GPU; accepted by the library's verifier (host and GPU query phase) and
+    by the oracle's, given the statement with the chips' heights; a wrong
+    output or a wrong height is rejected."""
+    words = rv64.keccak_program(136 * blocks)
+    proof, pub = RA.prove(words, OPTS, GpuBackend(be))
+    assert pub["output"] == rv64.keccak_reference(136 * blocks)
+    counts, out, h = pub["counts"], pub["output"], pub["heights"]
+    assert set(h) == {"cpu", "range", "bitwise", "shift", "memory", "keccak"}
+    assert RA.verify(words, counts, out, proof, OPTS, heights=h) == (True, "ok")
+    assert RA.verify(words, counts, out, proof, OPTS, device=be, heights=h) == (True, "ok")
+    airs = RA.airs_for(words, counts, h)
+    assert oracle_verify(airs, proof, OPTS, label=RA.statement_label(words, counts, out, h),
+                         public_terms=airs[0].public_terms(counts, out)) == (True, "ok")
+    assert RA.verify(words, counts, out ^ 1, proof, OPTS, heights=h)[0] is False
+    bad_h = dict(h)
+    bad_h["shift"] += 1
+    assert RA.verify(words, counts, out, proof, OPTS, heights=bad_h)[0] is False
+
+
+def test_keccak_guest_scheduled_proof_equals_plain(be):
+    """The batched prover (multi-table R1 launches, concurrent table drivers)
+    gives the plain prover's proof for the six-table statement."""
+    from lambda_vm_b200.scheduler import multi_prove_scheduled
+    from lambda_vm_b200.stark import multi_prove
+    from proofcmp import diff
+    airs, traces, pub = RA.build(rv64.keccak_program(136 * 4))
+    plain = multi_prove(airs, traces, OPTS, GpuBackend(be), label=pub["label"])
+    sched = multi_prove_scheduled(airs, traces, OPTS, workers=4, be=be, label=pub["label"])
+    assert diff(sched, plain) is None, diff(sched, plain)

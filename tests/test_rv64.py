@@ -1,12 +1,13 @@
-"""The RV64 front-end on the CPU: encodings, execution of the Fibonacci guest,
-and the CPU and RANGE table AIRs — every constraint vanishes on every row of
-an honest trace and the buses balance with the public statement, while a
-tampered trace or statement breaks a constraint or the balance."""
+"""The RV64 front-end on the CPU: encodings, execution of the Fibonacci and
+Keccak guests (Python and the library's native executor, cell for cell), and
+the AIRs of the CPU table and its chips — every constraint vanishes on the
+rows of an honest trace and the buses balance with the public statement,
+while a tampered trace or statement breaks a constraint or the balance."""
 import numpy as np
 import pytest
 
 import oracle as O
-from oracle.stark_backend import eval_program_row
+from vm_eval import bad_constraints
 from lambda_vm_b200 import rv64
 from lambda_vm_b200 import rv64_air as RA
 from lambda_vm_b200.verifier import public_sum
@@ -17,14 +18,24 @@ P = O.P
 def test_encodings_round_trip():
     cases = [("add", 7, 5, 6, 0), ("sub", 1, 2, 3, 0), ("addi", 10, 10, 0, -1), ("addi", 5, 0, 0, 2047),
              ("lui", 10, 0, 0, -(1 << 31)), ("lui", 3, 0, 0, 0x7FFFF << 12), ("beq", 0, 1, 2, -4096),
-             ("bne", 0, 10, 0, 4094), ("ecall", 0, 0, 0, 0)]
+             ("bne", 0, 10, 0, 4094), ("ecall", 0, 0, 0, 0), ("xor", 5, 6, 7, 0), ("or", 31, 1, 2, 0),
+             ("and", 9, 10, 11, 0), ("xori", 5, 6, 0, -1), ("ori", 8, 9, 0, 2047), ("andi", 1, 2, 0, -2048),
+             ("slli", 6, 5, 0, 13), ("slli", 6, 5, 0, 63), ("srli", 6, 5, 0, 7), ("srli", 6, 5, 0, 0),
+             ("ld", 6, 8, 0, -8), ("ld", 6, 8, 0, 2040), ("sd", 0, 18, 6, -2048), ("sd", 0, 18, 6, 136)]
     for op, rd, rs1, rs2, imm in cases:
         w = rv64.encode(op, rd, rs1, rs2, imm >> 12 if op == "lui" else imm)
         assert rv64.decode(w) == (op, rd, rs1, rs2, imm)
-    # standard encodings of the guest's first instructions
+    # standard encodings
     assert rv64.encode("addi", 10, 0, 0, 10) == 0x00A00513
     assert rv64.encode("add", 7, 5, 6) == 0x006283B3
     assert rv64.encode("ecall") == 0x00000073
+    assert rv64.encode("xor", 10, 11, 12) == 0x00C5C533
+    assert rv64.encode("slli", 5, 5, 0, 13) == 0x00D29293
+    assert rv64.encode("srli", 5, 5, 0, 7) == 0x0072D293
+    assert rv64.encode("ld", 10, 2, 0, 8) == 0x00813503
+    assert rv64.encode("sd", 0, 2, 10, 8) == 0x00A13423
+    with pytest.raises(ValueError):
+        rv64.decode(0x4072D293)  # srai: not in the subset
 
 
 @pytest.mark.parametrize("n", [1, 5, 300, 30000])
@@ -36,17 +47,65 @@ def test_fibonacci_guest_runs(n):
     assert len(rows) == 2 + (1 if n < 2048 else 2) + 5 * n + 3
 
 
-@pytest.mark.parametrize("n", [1, 7, 30, 2047, 2048, 5000])
-def test_native_trace_equals_the_python_table(n):
-    """sg_rv64_trace (the library's C++ executor and table writer) against the
-    Python executor and table builder, cell for cell."""
-    words = rv64.fib_program(n)
-    rows, regs = rv64.execute(words)
-    ct, counts, out, cycles = RA.native_trace(words)
-    cpu = RA.CpuAir(words, ct.shape[0].bit_length() - 1)
-    assert cycles == len(rows) and out == regs[10]
-    assert np.array_equal(ct, cpu.trace(rows))
-    assert counts == cpu.counts(rows)
+def test_keccak_f_known_answers():
+    """keccak-f[1600] of the zero state (its first lane is the published
+    0xF1258F7940E1DDE7), and Keccak-256 built on it as a sponge (rate 136,
+    pad 0x01 .. 0x80) against the oracle's Keccak-256."""
+    assert rv64.keccak_f([0] * 25)[0] == 0xF1258F7940E1DDE7
+    rng = np.random.default_rng(5)
+    for ln in (0, 1, 135, 136, 137, 300):
+        msg = bytes(rng.integers(0, 256, ln, dtype=np.uint8))
+        padded = bytearray(msg + b"\x01" + b"\0" * ((-len(msg) - 1) % 136))
+        padded[-1] |= 0x80
+        st = [0] * 25
+        for off in range(0, len(padded), 136):
+            blk = padded[off:off + 136]
+            for i in range(17):
+                st[i] ^= int.from_bytes(blk[8 * i:8 * i + 8], "little")
+            st = rv64.keccak_f(st)
+        digest = b"".join(v.to_bytes(8, "little") for v in st[:4])
+        assert digest == O.keccak256(msg)
+
+
+@pytest.mark.parametrize("blocks", [1, 3, 20])
+def test_keccak_guest_runs(blocks):
+    ex = rv64.run(rv64.keccak_program(136 * blocks))
+    assert ex.regs[10] == rv64.keccak_reference(136 * blocks)
+    assert len(ex.keccak) == blocks
+    words = 17 * blocks
+    # li buf (lui + addi), li count, li seed (lui + addi); 10 per word; li buf,
+    # li count, li state, li acc (two words each but the count), li a7; 63 per
+    # block; ld + 3 x (ld, xor); li a7, ecall
+    assert len(ex.rows) == 5 + 10 * words + 8 + 63 * blocks + 7 + 2
+    # every cell touched: the buffer, the 25 state lanes, the 4 accumulator lanes
+    assert len(ex.memory) == words + 25 + 4
+
+
+def test_executor_errors():
+    bad_addr = rv64.assemble([("li", "t0", 4), ("ld", "t1", 0, "t0"), ("li", "a7", 93), ("ecall",)])
+    with pytest.raises(ValueError, match="unaligned"):
+        rv64.run(bad_addr)
+    bad_call = rv64.assemble([("li", "a7", 7), ("ecall",)])
+    with pytest.raises(ValueError, match="ecall"):
+        rv64.run(bad_call)
+    # the library's executor refuses the same programs
+    for w in (bad_addr, bad_call):
+        with pytest.raises(Exception):
+            RA.native_events(w)
+
+
+@pytest.mark.parametrize("prog", ["fib7", "fib2047", "fib5000", "keccak1", "keccak9"])
+def test_native_events_equal_the_python_tables(prog):
+    """sg_rv64_run (the library's C++ executor and CPU-table writer) against
+    the Python executor and table builder: the CPU table cell for cell, the
+    counts, the output and every chip event."""
+    words = rv64.fib_program(int(prog[3:])) if prog.startswith("fib") else rv64.keccak_program(136 * int(prog[6:]))
+    pe, ne = RA.python_events(words), RA.native_events(words)
+    assert np.array_equal(pe.cpu_trace, ne.cpu_trace)
+    assert (pe.counts, pe.output, pe.cycles) == (ne.counts, ne.output, ne.cycles)
+    assert np.array_equal(pe.shifts, ne.shifts)
+    for a, b in zip(pe.cells + pe.keccak, ne.cells + ne.keccak):
+        assert np.array_equal(a, b)
 
 
 def _aux_and_apows(airs, z, alpha):
@@ -56,61 +115,130 @@ def _aux_and_apows(airs, z, alpha):
     return apows
 
 
-def _bad_roots(air, tr, z, alpha, apows, rows=None):
-    aux, L = O.logup_aux(tr, air.logup_descriptor(), np.array(apows, np.uint64), np.array(z, np.uint64))
-    L = [int(v) for v in L]
-    offset = [int(v) for v in O.fp3_mul(np.array(L, np.uint64), np.array([O.gl_inv(air.n), 0, 0], np.uint64))]
-    bad = set()
-    for r in (range(air.n) if rows is None else rows):
-        vals = eval_program_row(air.program, r, tr, aux, [z, alpha], apows, offset, 1)
-        bad |= {(ci, r) for ci, v in enumerate(vals) if any(int(x) % P for x in v)}
-    return bad, L
+def _check(airs, traces, pub, rows_limit=256, terms=None):
+    """(every table's failing (constraint, row) set, bus total with the public
+    terms) under fixed challenges."""
+    apows = _aux_and_apows(airs, Z, ALPHA)
+    total = public_sum(pub["terms"] if terms is None else terms, Z, apows)
+    bad = {}
+    for air, tr in zip(airs, traces):
+        aux, L = O.logup_aux(tr, air.logup_descriptor(), np.array(apows, np.uint64), np.array(Z, np.uint64))
+        L = [int(v) for v in L]
+        offset = [int(v) for v in O.fp3_mul(np.array(L, np.uint64), np.array([O.gl_inv(air.n), 0, 0], np.uint64))]
+        rows = range(air.n) if air.n <= rows_limit else \
+            list(range(rows_limit // 2)) + list(range(air.n - rows_limit // 2, air.n))
+        bad[type(air).__name__] = bad_constraints(air.program, tr, aux, [Z, ALPHA], apows, offset, list(rows))
+        total = tuple((total[i] + L[i]) % P for i in range(3))
+    return bad, total
 
 
 Z, ALPHA = (0x1234567, 0xABCDEF, 0x13579), (0x2468ACE, 0x1111, 0x777)
 
 
-def test_honest_trace_satisfies_every_constraint_and_the_buses_balance():
-    airs, traces, pub = RA.build(rv64.fib_program(12))
-    apows = _aux_and_apows(airs, Z, ALPHA)
-    total = public_sum(pub["terms"], Z, apows)
-    for air, tr in zip(airs, traces):
-        rows = None if air.n <= 128 else list(range(64)) + list(range(air.n - 64, air.n))
-        bad, L = _bad_roots(air, tr, Z, ALPHA, apows, rows)
-        assert not bad, (type(air).__name__, sorted(bad)[:5])
-        total = tuple((total[i] + L[i]) % P for i in range(3))
+@pytest.mark.parametrize("prog", ["fib12", "keccak2"])
+def test_honest_trace_satisfies_every_constraint_and_the_buses_balance(prog):
+    words = rv64.fib_program(12) if prog == "fib12" else rv64.keccak_program(272)
+    airs, traces, pub = RA.build(words)
+    bad, total = _check(airs, traces, pub)
+    assert not any(bad.values()), {k: sorted(v)[:5] for k, v in bad.items() if v}
     assert total == (0, 0, 0)
-    assert pub["output"] == rv64.fib_reference(12)
     assert sum(pub["counts"]) == airs[0].n
+    if prog == "keccak2":
+        assert [type(a).__name__ for a in airs] == ["CpuAir", "RangeAir", "BitwiseAir", "ShiftAir", "MemoryAir",
+                                                    "KeccakAir"]
+        assert pub["output"] == rv64.keccak_reference(272)
+    else:
+        assert len(airs) == 2 and pub["output"] == rv64.fib_reference(12)
+
+
+def _tampered(airs, traces, pub, table, fn, terms=None):
+    trs = [t.copy() for t in traces]
+    k = [type(a).__name__ for a in airs].index(table)
+    fn(trs[k])
+    bad, total = _check(airs, trs, pub, terms=terms)
+    return any(bad.values()) or total != (0, 0, 0)
 
 
 def test_tampering_breaks_a_constraint_or_the_balance():
     airs, traces, pub = RA.build(rv64.fib_program(6))
-    cpu, ct = airs[0], traces[0]
-    apows = _aux_and_apows(airs, Z, ALPHA)
-    # a register value changed mid-run
-    bad_tr = ct.copy()
-    bad_tr[9, RA.xlo(6)] = (int(bad_tr[9, RA.xlo(6)]) + 1) % P
-    assert _bad_roots(cpu, bad_tr, Z, ALPHA, apows)[0]
-    # an addition with a wrong result (and its range pieces adjusted)
-    row = next(i for i in range(cpu.n) if ct[i, RA.SEL["add"]] == 1)
-    bad_tr = ct.copy()
-    bad_tr[row, RA.R_LO] = int(bad_tr[row, RA.R_LO]) + 1
-    bad_tr[row, RA.R16] = int(bad_tr[row, RA.R16]) + 1
-    assert _bad_roots(cpu, bad_tr, Z, ALPHA, apows)[0]
-    # a second END row
-    bad_tr = ct.copy()
-    bad_tr[cpu.n // 2, RA.STEP] = 0
-    assert _bad_roots(cpu, bad_tr, Z, ALPHA, apows)[0]
-    # a different claimed output: the END bus no longer balances
-    _, L0 = _bad_roots(cpu, ct, Z, ALPHA, apows)
-    _, L1 = _bad_roots(airs[1], traces[1], Z, ALPHA, apows, rows=[0])
-    for out in (pub["output"] + 1,):
-        ps = public_sum(cpu.public_terms(pub["counts"], out), Z, apows)
-        assert tuple((L0[i] + L1[i] + ps[i]) % P for i in range(3)) != (0, 0, 0)
-    # different execution counts: the ROM bus no longer balances
+    ct = traces[0]
+
+    def reg(t):  # a register value changed mid-run
+        t[9, RA.xlo(6)] = (int(t[9, RA.xlo(6)]) + 1) % P
+    assert _tampered(airs, traces, pub, "CpuAir", reg)
+    row = next(i for i in range(ct.shape[0]) if ct[i, RA.SEL["add"]] == 1)
+
+    def add(t):  # an addition with a wrong result (range pieces adjusted)
+        t[row, RA.R_LO] += 1
+        t[row, RA.R16] += 1
+    assert _tampered(airs, traces, pub, "CpuAir", add)
+
+    def end(t):  # a second END row
+        t[t.shape[0] // 2, RA.STEP] = 0
+    assert _tampered(airs, traces, pub, "CpuAir", end)
+    cpu = airs[0]
+    # a different claimed output, or different execution counts
+    assert _tampered(airs, traces, pub, "CpuAir", lambda t: None,
+                     terms=cpu.public_terms(pub["counts"], pub["output"] + 1))
     counts = list(pub["counts"])
     counts[3] += 1
     counts[4] -= 1
-    ps = public_sum(cpu.public_terms(counts, pub["output"]), Z, apows)
-    assert tuple((L0[i] + L1[i] + ps[i]) % P for i in range(3)) != (0, 0, 0)
+    assert _tampered(airs, traces, pub, "CpuAir", lambda t: None, terms=cpu.public_terms(counts, pub["output"]))
+    assert not _tampered(airs, traces, pub, "CpuAir", lambda t: None)
+
+
+def test_tampered_chips_are_caught():
+    """Each chip's own relation, and its link to the CPU table, is enforced:
+    a flipped theta bit, a wrong Keccak output lane, a wrong shift result, a
+    load returning a value that was never stored, a second row for one memory
+    cell, a wrong XOR byte, a store whose previous timestamp is not earlier."""
+    airs, traces, pub = RA.build(rv64.keccak_program(272))
+    ct = traces[0]
+    assert not _tampered(airs, traces, pub, "CpuAir", lambda t: None)
+
+    def theta(t):
+        t[5, RA.KAP + 77] ^= 1
+    assert _tampered(airs, traces, pub, "KeccakAir", theta)
+
+    def out(t):
+        t[23, RA.KOUT + 9] += 1
+    assert _tampered(airs, traces, pub, "KeccakAir", out)
+
+    def shift(t):
+        t[0, RA.ShiftAir.R_LO] += 1
+    assert _tampered(airs, traces, pub, "ShiftAir", shift)
+    ld = next(i for i in range(ct.shape[0]) if ct[i, RA.SEL["ld"]] == 1 and ct[i, RA.MV_LO] < 1000)
+
+    def load(t):  # value read, written to the register and range pieces all changed together
+        for c in (RA.MV_LO, RA.NV_LO, RA.R_LO, RA.R16):
+            t[ld, c] += 1
+    assert _tampered(airs, traces, pub, "CpuAir", load)
+
+    def dup(t):  # the second cell takes the first one's address
+        t[1, RA.MemoryAir.ADDR] = t[0, RA.MemoryAir.ADDR]
+    assert _tampered(airs, traces, pub, "MemoryAir", dup)
+    xr = next(i for i in range(ct.shape[0]) if ct[i, RA.SEL["xor"]] == 1)
+
+    def xor_byte(t):
+        t[xr, RA.RB0] ^= 1
+        t[xr, RA.R_LO] ^= 1
+        t[xr, RA.R16] ^= 1
+    assert _tampered(airs, traces, pub, "CpuAir", xor_byte)
+    sd = next(i for i in range(ct.shape[0]) if ct[i, RA.SEL["sd"]] == 1 and ct[i, RA.MT] > 0)
+
+    def stamp(t):  # claims the cell's previous access is this one's own timestamp
+        t[sd, RA.MT] = t[sd, RA.CLK]
+    assert _tampered(airs, traces, pub, "CpuAir", stamp)
+
+
+def test_statement_binds_the_chip_heights():
+    words = rv64.keccak_program(272)
+    _, _, pub = RA.build(words)
+    h = dict(pub["heights"])
+    assert RA.statement_label(words, pub["counts"], pub["output"], h) == pub["label"]
+    h["keccak"] += 1
+    assert RA.statement_label(words, pub["counts"], pub["output"], h) != pub["label"]
+    # the Fibonacci statement (no chips) keeps its label
+    fw = rv64.fib_program(9)
+    _, _, fp = RA.build(fw)
+    assert fp["label"] == RA.statement_label(fw, fp["counts"], fp["output"])
