@@ -59,7 +59,7 @@ def parse():
     ap.add_argument("--max-jobs", type=int, default=4, help="serve: concurrent jobs")
     ap.add_argument("--policy", default="backfill", choices=["backfill", "fifo"], help="serve: admission policy")
     ap.add_argument("--job-kind", default="mix", choices=["mix", "synth"],
-                    help="serve: Fibonacci guests and synthetic chip tables alternating, or synthetic only")
+                    help="serve: Fibonacci and Keccak guests alternating, or synthetic chip tables only")
     ap.add_argument("--no-serve-summary", action="store_true",
                     help="skip the serving summary the default line carries at N = 1")
     ap.add_argument("--tables", type=int, default=40)
@@ -365,12 +365,13 @@ def measure_proof(a):
 
 
 def serve_jobs(a, seed=77):
-    """Proof requests of a serving stream. Even jobs are Fibonacci RV64 guests
-    (executed and tabled up front) of c cycles, odd jobs stand in for the
-    Keccak guests, whose chips are not built: 2-4 synthetic chip tables of c,
-    c/2, c/4, ... rows (widths uniform 8..300, 2-6 LogUp interactions) with
-    trace seeds of their own; c log-uniform in 2^10..2^job_max_log_n.
-    Each spec is (airs, sources, transcript label)."""
+    """Proof requests of a serving stream, each of about c cycles, c
+    log-uniform in 2^10..2^job_max_log_n. mix (default): Fibonacci RV64 guests
+    (even jobs) and Keccak guests (odd jobs; a buffer of about c / 14 bytes,
+    whole 136-byte blocks, so 4 KiB at c = 2^16), executed and tabled up front.
+    synth: 2-4 synthetic chip tables of c, c/2, c/4, ... rows (widths uniform
+    8..300, 2-6 LogUp interactions) with trace seeds of their own. Each spec
+    is (airs, sources, transcript label)."""
     from lambda_vm_b200 import rv64
     from lambda_vm_b200 import rv64_air as RA
     from lambda_vm_b200.air import SynthTableAir
@@ -378,8 +379,12 @@ def serve_jobs(a, seed=77):
     specs = []
     for j in range(a.jobs):
         k = int(rng.integers(10, a.job_max_log_n + 1))
-        if j % 2 == 0 and getattr(a, "job_kind", "mix") == "mix":
-            airs, traces, pub = RA.build(rv64.fib_program(max(1, ((1 << k) - 6) // 5)))
+        if getattr(a, "job_kind", "mix") == "mix":
+            if j % 2 == 0:
+                words = rv64.fib_program(max(1, ((1 << k) - 6) // 5))
+            else:
+                words = rv64.keccak_program(136 * max(1, (1 << k) // (14 * 136)))
+            airs, traces, pub = RA.build(words)
             specs.append((airs, traces, pub["label"]))
             continue
         nt = int(rng.integers(2, 5))
@@ -440,13 +445,14 @@ def measure_serve(a):
             "value": top["batched"]["rows_per_s"], "unit": "rows/s", "n_gpus": 1, "steps": a.jobs, "warmup": 3,
             "ms_per_step": top["batched"]["mean_ms"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64 (Goldilocks) / Fp3",
-            "data": ("Fibonacci RV64 guests executed and tabled up front, alternating with synthetic chip-table "
-                     "proofs standing in for the Keccak guests" if a.job_kind == "mix" else
+            "data": ("Fibonacci and Keccak RV64 guests, alternating, executed and tabled up front"
+                     if a.job_kind == "mix" else
                      "synthetic chip-table proofs (job sizes stand in for the guests' cycle counts)"),
             "config": {"workload": f"{a.jobs} proof jobs per rate, cycles log-uniform 2^10..2^{a.job_max_log_n}, "
-                                   + ("even jobs Fibonacci guests (CPU + RANGE tables), odd jobs "
-                                      if a.job_kind == "mix" else "")
-                                   + "2-4 synthetic tables each, blowup 2, 219 queries, grinding 20",
+                                   + ("even jobs Fibonacci guests (CPU + RANGE tables), odd jobs Keccak guests "
+                                      "(CPU, RANGE, BITWISE, SHIFT, MEMORY, KECCAK tables)" if a.job_kind == "mix"
+                                      else "2-4 synthetic tables each")
+                                   + ", blowup 2, 219 queries, grinding 20",
                        "rows_total": rows, "hbm_budget_bytes": budget, "max_concurrent_jobs": a.max_jobs,
                        "policy": a.policy},
             "p50_ms": top["batched"]["p50_ms"], "p99_ms": top["batched"]["p99_ms"], "sweep": sweep}

@@ -551,6 +551,16 @@ typedef struct {
 SG_API int sg_rv64_run(const uint32_t* words, uint32_t nwords, uint64_t max_steps, uint64_t n_rows,
                        uint64_t* cpu_out, uint64_t* counts_out, uint64_t* shifts_out, uint64_t* cells_out,
                        uint64_t* keccak_out, void* reserved, sg_rv64_info* info);
+/* Chip tables written on the device from sg_rv64_run's events (host arrays),
+ * so the host neither builds nor uploads them: d_out gets the KECCAK table
+ * (n_rows x 2605: 24 rows per ecall, the rest zero) from `count` 52-word ecall
+ * records, or the SHIFT table (n_rows x 148, padding rows shift 0 by 0) from
+ * `count` 3-word shift records. Layouts: lambda_vm_b200/rv64_air.py's
+ * KeccakAir and ShiftAir. Asynchronous on `stream`. */
+SG_API int sg_rv64_keccak_table(sg_ctx* ctx, void* stream, const uint64_t* calls, uint64_t count, uint64_t n_rows,
+                                uint64_t* d_out);
+SG_API int sg_rv64_shift_table(sg_ctx* ctx, void* stream, const uint64_t* shifts, uint64_t count, uint64_t n_rows,
+                               uint64_t* d_out);
 
 /* ---- DFT pass log: the autotuner's measurements. No counterpart in the
  *      reference (its NTT has one fixed plan). While enabled, every DFT pass

@@ -326,3 +326,170 @@ extern "C" int sg_rv64_run(const uint32_t* words, uint32_t nwords, uint64_t max_
     }
     return SG_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Chip tables expanded on the device from the run's compact events, so the
+// host never writes or uploads them: the KECCAK table (24 rows x 2605 columns
+// per ecall from 52 words of event) and the SHIFT table (148 columns per
+// shift from 3 words). Layouts: rv64_air.py's KeccakAir and ShiftAir.
+namespace {
+
+constexpr int KW = 2605;  // KECCAK table columns
+constexpr int K_A = 24, K_C = 124, K_CP = 444, K_AP = 764, K_OUT = 2364, K_B00 = 2464, K_BASE = 2528, K_CLK = 2529,
+              K_TOLD = 2530, K_TD = 2555;
+constexpr int K_SLOTS = 86;  // per round: A[25], C[5], C'[5], A'[25], OUT[25], chi lane 0 before iota
+
+struct KeccakConsts {
+    uint64_t rc[24];
+    int rot[25];
+};
+
+// One CTA per ecall: thread 0 runs the 24 rounds into shared memory, then the
+// CTA writes the ecall's 24 rows, consecutive threads on consecutive columns.
+__global__ void k_keccak_rows(const uint64_t* __restrict__ calls, uint64_t count, KeccakConsts kc,
+                              uint64_t* __restrict__ out) {
+    __shared__ uint64_t s[24][K_SLOTS];
+    for (uint64_t p = blockIdx.x; p < count; p += gridDim.x) {
+        const uint64_t* ev = calls + 52 * p;
+        if (threadIdx.x == 0) {
+            uint64_t a[25];
+            for (int i = 0; i < 25; ++i) a[i] = ev[2 + i];
+            for (int r = 0; r < 24; ++r) {
+                uint64_t* o = s[r];
+                uint64_t c[5], d[5], b[25];
+                for (int x = 0; x < 5; ++x) c[x] = a[x] ^ a[x + 5] ^ a[x + 10] ^ a[x + 15] ^ a[x + 20];
+                for (int x = 0; x < 5; ++x) {
+                    const uint64_t n1 = c[(x + 1) % 5];
+                    d[x] = c[(x + 4) % 5] ^ ((n1 << 1) | (n1 >> 63));
+                }
+                for (int i = 0; i < 25; ++i) {
+                    o[i] = a[i];
+                    o[55 + i] = 0;
+                }
+                for (int x = 0; x < 5; ++x) o[25 + x] = c[x], o[30 + x] = c[x] ^ d[x];
+                for (int x = 0; x < 5; ++x)
+                    for (int y = 0; y < 5; ++y) {
+                        const uint64_t v = a[x + 5 * y] ^ d[x];
+                        o[35 + x + 5 * y] = v;
+                        const int rr = kc.rot[x + 5 * y];
+                        b[y + 5 * ((2 * x + 3 * y) % 5)] = rr ? (v << rr) | (v >> (64 - rr)) : v;
+                    }
+                for (int x = 0; x < 5; ++x)
+                    for (int y = 0; y < 5; ++y)
+                        a[x + 5 * y] = b[x + 5 * y] ^ (~b[(x + 1) % 5 + 5 * y] & b[(x + 2) % 5 + 5 * y]);
+                o[85] = a[0];
+                a[0] ^= kc.rc[r];
+                for (int i = 0; i < 25; ++i) o[60 + i] = a[i];
+            }
+        }
+        __syncthreads();
+        const uint64_t clk = ev[0], base = ev[1];
+        uint64_t* rows = out + 24 * p * (uint64_t)KW;
+        for (uint32_t idx = threadIdx.x; idx < 24u * KW; idx += blockDim.x) {
+            const uint32_t r = idx / KW, c = idx % KW;
+            const uint64_t* o = s[r];
+            uint64_t v;
+            if (c < K_A) v = c == r;
+            else if (c < K_C) v = (o[(c - K_A) / 4] >> (16 * ((c - K_A) % 4))) & 0xFFFF;
+            else if (c < K_CP) v = (o[25 + (c - K_C) / 64] >> ((c - K_C) % 64)) & 1;
+            else if (c < K_AP) v = (o[30 + (c - K_CP) / 64] >> ((c - K_CP) % 64)) & 1;
+            else if (c < K_OUT) v = (o[35 + (c - K_AP) / 64] >> ((c - K_AP) % 64)) & 1;
+            else if (c < K_B00) v = (o[60 + (c - K_OUT) / 4] >> (16 * ((c - K_OUT) % 4))) & 0xFFFF;
+            else if (c < K_BASE) v = (o[85] >> (c - K_B00)) & 1;
+            else if (c == K_BASE) v = base;
+            else if (c == K_CLK) v = clk;
+            else if (c < K_TD) v = r == 0 ? ev[27 + (c - K_TOLD)] : 0;
+            else {
+                const uint32_t j = c - K_TD;
+                const uint64_t gap = clk - ev[27 + j / 2] - 1;
+                v = r == 0 ? ((j & 1) ? gap >> 16 : gap & 0xFFFF) : 0;
+            }
+            rows[idx] = v;
+        }
+        __syncthreads();
+    }
+}
+
+constexpr int SW = 148;  // SHIFT table columns: DIR, bits of a (64), S (8), Q (8), bits of a >>/<< s (64), R_LO, R_HI, M
+
+__global__ void k_shift_rows(const uint64_t* __restrict__ ev, uint64_t count, uint64_t n_rows,
+                             uint64_t* __restrict__ out) {
+    const uint64_t total = n_rows * SW;
+    for (uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t row = idx / SW;
+        const uint32_t c = (uint32_t)(idx % SW);
+        uint64_t v;
+        if (row >= count) {
+            v = (c == 65 || c == 73);  // padding: a = 0, k = 0
+        } else {
+            const uint64_t dir = ev[3 * row], a = ev[3 * row + 1], k = ev[3 * row + 2];
+            const uint64_t sb = k & 7, q = k >> 3;
+            const uint64_t t = dir ? a >> sb : a << sb, res = dir ? a >> k : a << k;
+            if (c == 0) v = dir;
+            else if (c < 65) v = (a >> (c - 1)) & 1;
+            else if (c < 73) v = (c - 65) == sb;
+            else if (c < 81) v = (c - 73) == q;
+            else if (c < 145) v = (t >> (c - 81)) & 1;
+            else if (c == 145) v = res & M32;
+            else if (c == 146) v = res >> 32;
+            else v = 1;
+        }
+        out[idx] = v;
+    }
+}
+
+int upload_events(Ctx* ctx, cudaStream_t st, const uint64_t* host, uint64_t words, uint64_t** d) {
+    SG_TRY(dev_alloc(ctx, st, 8 * words, (void**)d));
+    if (cudaMemcpyAsync(*d, host, 8 * words, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+        dev_free(ctx, st, *d, 8 * words);
+        set_error("rv64: event upload failed");
+        return SG_ERR_CUDA;
+    }
+    return SG_OK;
+}
+
+}  // namespace
+
+extern "C" int sg_rv64_keccak_table(sg_ctx* c, void* stream, const uint64_t* calls, uint64_t count, uint64_t n_rows,
+                                    uint64_t* d_out) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(c);
+    SG_CHECK_ARG(ctx && d_out && (calls || !count), "null argument");
+    SG_ENTER(ctx);
+    SG_CHECK_ARG(count <= n_rows / 24, "the ecalls do not fit n_rows");
+    cudaStream_t st = (cudaStream_t)stream;
+    const uint64_t used = 24 * count;
+    if (used < n_rows && cudaMemsetAsync(d_out + used * KW, 0, (n_rows - used) * KW * 8, st) != cudaSuccess) {
+        set_error("rv64: padding fill failed");
+        return SG_ERR_CUDA;
+    }
+    if (!count) return SG_OK;
+    KeccakConsts kc;
+    for (int i = 0; i < 24; ++i) kc.rc[i] = ktab().rc[i];
+    for (int i = 0; i < 25; ++i) kc.rot[i] = ktab().rot[i];
+    uint64_t* d_ev = nullptr;
+    SG_TRY(upload_events(ctx, st, calls, 52 * count, &d_ev));
+    const unsigned grid = (unsigned)std::min<uint64_t>(count, 148ull * 16);
+    k_keccak_rows<<<grid, 256, 0, st>>>(d_ev, count, kc, d_out);
+    const int rc = check_launch(ctx, "k_keccak_rows");
+    dev_free(ctx, st, d_ev, 8 * 52 * count);
+    return rc;
+}
+
+extern "C" int sg_rv64_shift_table(sg_ctx* c, void* stream, const uint64_t* shifts, uint64_t count, uint64_t n_rows,
+                                   uint64_t* d_out) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(c);
+    SG_CHECK_ARG(ctx && d_out && (shifts || !count), "null argument");
+    SG_ENTER(ctx);
+    SG_CHECK_ARG(count <= n_rows, "the shifts do not fit n_rows");
+    for (uint64_t i = 0; i < count; ++i) SG_CHECK_ARG(shifts[3 * i] <= 1 && shifts[3 * i + 2] < 64, "bad shift event");
+    cudaStream_t st = (cudaStream_t)stream;
+    uint64_t* d_ev = nullptr;
+    if (count) SG_TRY(upload_events(ctx, st, shifts, 3 * count, &d_ev));
+    const uint64_t total = n_rows * SW;
+    const unsigned grid = (unsigned)std::min<uint64_t>((total + 255) / 256, 148ull * 32);
+    k_shift_rows<<<grid, 256, 0, st>>>(d_ev, count, n_rows, d_out);
+    const int rc = check_launch(ctx, "k_shift_rows");
+    if (d_ev) dev_free(ctx, st, d_ev, 8 * 3 * count);
+    return rc;
+}

@@ -1026,9 +1026,58 @@ def _chips_used(rows, ex):
     return tuple(c for c in CHIPS if c in used)
 
 
-def tables_from_events(words, ev):
+class ShiftSource:
+    """The SHIFT table of a run's shift events (dir, a, k): written on the
+    device by the GPU backend (sg_rv64_shift_table), built with numpy
+    otherwise."""
+
+    def __init__(self, shifts):
+        self.shifts = np.ascontiguousarray(np.asarray(shifts, np.uint64).reshape(-1, 3))
+
+    def host_trace(self, air):
+        return air.trace(self.shifts)
+
+    def device_trace(self, bk, air):
+        from . import native
+        m = bk._alloc(air.n, air.width)
+        native.check(bk.L.sg_rv64_shift_table(bk.be.h, bk.st, self.shifts.ctypes.data if self.shifts.size else None,
+                                              self.shifts.shape[0], air.n, m.ptr))
+        return m
+
+
+class KeccakSource:
+    """The KECCAK table of a run's ecalls (timestamp, address, 25 input lanes,
+    25 previous timestamps): written on the device by the GPU backend
+    (sg_rv64_keccak_table), built with numpy otherwise."""
+
+    def __init__(self, clocks, bases, lanes, told):
+        clk = np.asarray(clocks, np.uint64).reshape(-1, 1)
+        self.calls = np.ascontiguousarray(np.hstack([clk, np.asarray(bases, np.uint64).reshape(-1, 1),
+                                                     np.asarray(lanes, np.uint64).reshape(-1, 25),
+                                                     np.asarray(told, np.uint64).reshape(-1, 25)]))
+
+    def host_trace(self, air):
+        c = self.calls
+        return air.trace(c[:, 0], c[:, 1], c[:, 2:27], c[:, 27:52])
+
+    def device_trace(self, bk, air):
+        from . import native
+        m = bk._alloc(air.n, air.width)
+        native.check(bk.L.sg_rv64_keccak_table(bk.be.h, bk.st, self.calls.ctypes.data if self.calls.size else None,
+                                               self.calls.shape[0], air.n, m.ptr))
+        return m
+
+    def range_lookups(self):
+        """The 16-bit pieces of each read's timestamp gap (the table's RANGE lookups)."""
+        gap = self.calls[:, :1] - self.calls[:, 27:52] - np.uint64(1)
+        return [gap & np.uint64(0xFFFF), gap >> np.uint64(16)]
+
+
+def tables_from_events(words, ev, host_tables=False):
     """(airs, traces, public) of a run's events: public = {"words", "counts",
-    "output", "cycles", "heights", "label", "terms"}."""
+    "output", "cycles", "heights", "label", "terms"}. The SHIFT and KECCAK
+    entries of traces are table sources the GPU backend expands on the device
+    (stark._gen_trace), or numpy tables with host_tables."""
     ct = ev.cpu_trace
     heights = {"cpu": ct.shape[0].bit_length() - 1, "range": 16}
     bit = any(ct[:, SEL[o]].any() for o in BIT_REG + BIT_IMM)
@@ -1050,8 +1099,9 @@ def tables_from_events(words, ev):
         traces.append(a.trace(ct))
     if "shift" in chips:
         a = ShiftAir(heights["shift"])
+        src = ShiftSource(ev.shifts)
         airs.append(a)
-        traces.append(a.trace(ev.shifts))
+        traces.append(src.host_trace(a) if host_tables else src)
     if "memory" in chips:
         a = MemoryAir(heights["memory"])
         mt = a.trace(*ev.cells)
@@ -1063,10 +1113,10 @@ def tables_from_events(words, ev):
                  mt[:, MemoryAir.D0], mt[:, MemoryAir.D1]]
     if "keccak" in chips:
         a = KeccakAir(heights["keccak"])
-        kt = a.trace(*ev.keccak)
+        src = KeccakSource(*ev.keccak)
         airs.append(a)
-        traces.append(kt)
-        look.append(kt[kt[:, KR] == 1, KTD:KTD + 50])
+        traces.append(src.host_trace(a) if host_tables else src)
+        look += src.range_lookups()
     traces[1] = airs[1].trace(look)
     pub = {"words": list(words), "counts": ev.counts, "output": ev.output, "cycles": ev.cycles,
            "heights": heights, "label": statement_label(words, ev.counts, ev.output, heights),
@@ -1098,11 +1148,12 @@ def native_events(words, max_steps=1 << 32):
                   (kc[:, 0].copy(), kc[:, 1].copy(), kc[:, 2:27].copy(), kc[:, 27:52].copy()))
 
 
-def build(words, native_exec=True):
+def build(words, native_exec=True, host_tables=False):
     """Execute a program and build its tables (by default with the library's
-    native executor): (airs, traces, public)."""
+    native executor; the SHIFT and KECCAK tables as device-written sources
+    unless host_tables): (airs, traces, public)."""
     ev = native_events(words) if native_exec else python_events(words)
-    return tables_from_events(words, ev)
+    return tables_from_events(words, ev, host_tables)
 
 
 def native_trace(words, max_steps=1 << 32):

@@ -676,8 +676,12 @@ def prove_table(bk, air, lowered, trace_mat, main_lde, main_tree, t, challenges,
 
 
 def _gen_trace(bk, air, source):
-    """`source` is a host array, or an int seed for the counter-based synthetic
-    trace (generated on the device by the GPU backend, on the host otherwise)."""
+    """`source` is a host array, an int seed for the counter-based synthetic
+    trace (generated on the device by the GPU backend, on the host otherwise),
+    or a table source with device_trace(bk, air) (the GPU backend writes the
+    table on the device) and host_trace(air)."""
+    if hasattr(source, "device_trace"):
+        return source.device_trace(bk, air) if isinstance(bk, GpuBackend) else bk.upload(source.host_trace(air))
     if isinstance(source, (int, np.integer)):
         if isinstance(bk, GpuBackend):
             m = bk._alloc(air.n, air.width)

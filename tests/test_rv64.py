@@ -138,7 +138,7 @@ Z, ALPHA = (0x1234567, 0xABCDEF, 0x13579), (0x2468ACE, 0x1111, 0x777)
 @pytest.mark.parametrize("prog", ["fib12", "keccak2"])
 def test_honest_trace_satisfies_every_constraint_and_the_buses_balance(prog):
     words = rv64.fib_program(12) if prog == "fib12" else rv64.keccak_program(272)
-    airs, traces, pub = RA.build(words)
+    airs, traces, pub = RA.build(words, host_tables=True)
     bad, total = _check(airs, traces, pub)
     assert not any(bad.values()), {k: sorted(v)[:5] for k, v in bad.items() if v}
     assert total == (0, 0, 0)
@@ -192,7 +192,7 @@ def test_tampered_chips_are_caught():
     a flipped theta bit, a wrong Keccak output lane, a wrong shift result, a
     load returning a value that was never stored, a second row for one memory
     cell, a wrong XOR byte, a store whose previous timestamp is not earlier."""
-    airs, traces, pub = RA.build(rv64.keccak_program(272))
+    airs, traces, pub = RA.build(rv64.keccak_program(272), host_tables=True)
     ct = traces[0]
     assert not _tampered(airs, traces, pub, "CpuAir", lambda t: None)
 
