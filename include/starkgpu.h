@@ -525,34 +525,50 @@ typedef struct {
 SG_API int sg_verify_queries(sg_ctx* ctx, void* stream, const sg_verify_table* tables, uint32_t count,
                              uint32_t* status_out);
 
-/* ---- RV64 front-end (host): execute a guest of RV64I-subset words (ADD, SUB,
- *      XOR, OR, AND, ADDI, XORI, ORI, ANDI, SLLI, SRLI, LUI, LD, SD, BEQ, BNE,
- *      ECALL: a7 = 93 exits, a7 = 2^64 - 2 applies keccak-f[1600] to the 25
- *      lanes at a0; executor/src/vm semantics, the keccak ecall as
+/* ---- RV64 front-end: execute a guest of RV64I-subset words (ADD, SUB, XOR,
+ *      OR, AND, ADDI, XORI, ORI, ANDI, SLLI, SRLI, LUI, LD, SD, BEQ, BNE, ECALL:
+ *      a7 = 93 exits, a7 = 2^64 - 2 applies keccak-f[1600] to the 25 lanes at
+ *      a0; executor/src/vm semantics, the keccak ecall as
  *      executor/src/vm/instruction/execution.rs:649-670) from pc 0 with zeroed
- *      data memory, at most max_steps instructions. Fills *info (executed
- *      instructions, final a0, shifts executed, memory cells touched, keccak
- *      ecalls). With cpu_out, also writes the CPU table of the execution's
- *      proof (n_rows x SG_RV64_CPU_WIDTH u64, row-major, host memory; rows past
- *      the halt repeat the halting row, the last row ends the cycle; the layout
- *      is lambda_vm_b200/rv64_air.py's) and counts_out[i] (nwords entries) =
- *      how many table rows execute instruction i. Each optional event array
- *      gets one record per event: shifts_out (dir, a, amount), cells_out
- *      (address, final value, final timestamp; ascending addresses),
- *      keccak_out (timestamp, state address, 25 input lanes, the 25 cells'
- *      previous timestamps). Size them from a first call without outputs.
- *      reserved must be NULL. No counterpart in the reference's math-cuda (it
- *      is the executor and trace builder of the VM crates, restricted to this
- *      subset). ---- */
+ *      data memory, at most max_steps instructions, on the host. Fills *info
+ *      (executed instructions, final a0, shifts executed, memory cells
+ *      touched, keccak ecalls, SG_RV64_CHIP_* bits of the chips the run
+ *      needs). Each optional output gets one record per event (size them from
+ *      a first call without outputs): rows_out (8 words per executed
+ *      instruction: pc | op << 32 | rd << 40 | rs1 << 48 | rs2 << 56, imm, a,
+ *      b, r, memory address, the cell's previous value and timestamp; op is
+ *      the ROM opcode id, 18 for a keccak ecall), regs_out (the 32 registers
+ *      before every SG_RV64_REG_CHUNK-th row of an n_rows table, the final
+ *      registers past the halt), counts_out (nwords: how many rows of an
+ *      n_rows table execute instruction i, the halting ECALL repeated to the
+ *      end), shifts_out (dir, a, amount), cells_out (address, final value,
+ *      final timestamp; ascending addresses), keccak_out (timestamp, state
+ *      address, 25 input lanes, the 25 cells' previous timestamps). No
+ *      counterpart in the reference's math-cuda (it is the executor and trace
+ *      builder of the VM crates, restricted to this subset). ---- */
+#define SG_RV64_CPU_CORE_WIDTH 200
 #define SG_RV64_CPU_WIDTH 234
+#define SG_RV64_REG_CHUNK 64
+#define SG_RV64_CHIP_BITWISE 1u
+#define SG_RV64_CHIP_SHIFT 2u
+#define SG_RV64_CHIP_MEMORY 4u
+#define SG_RV64_CHIP_KECCAK 8u
 typedef struct {
     uint64_t cycles, a0, shifts, cells, keccak_calls;
+    uint32_t chips, reserved;
 } sg_rv64_info;
 SG_API int sg_rv64_run(const uint32_t* words, uint32_t nwords, uint64_t max_steps, uint64_t n_rows,
-                       uint64_t* cpu_out, uint64_t* counts_out, uint64_t* shifts_out, uint64_t* cells_out,
-                       uint64_t* keccak_out, void* reserved, sg_rv64_info* info);
-/* Chip tables written on the device from sg_rv64_run's events (host arrays),
- * so the host neither builds nor uploads them: d_out gets the KECCAK table
+                       uint64_t* rows_out, uint64_t* regs_out, uint64_t* counts_out, uint64_t* shifts_out,
+                       uint64_t* cells_out, uint64_t* keccak_out, sg_rv64_info* info);
+/* The CPU table (n_rows x width u64, row-major, into device memory) written on
+ * the device from sg_rv64_run's `count` row records and register snapshots
+ * (host arrays): width SG_RV64_CPU_CORE_WIDTH (no chip instruction executed)
+ * or SG_RV64_CPU_WIDTH; rows past the execution repeat the halting row, the
+ * last row ends the cycle. Layout: lambda_vm_b200/rv64_air.py's CpuAir. */
+SG_API int sg_rv64_cpu_table(sg_ctx* ctx, void* stream, const uint64_t* rows, uint64_t count, const uint64_t* regs,
+                             uint64_t n_rows, uint32_t width, uint64_t* d_out);
+/* The chip tables written on the device from sg_rv64_run's events (host
+ * arrays), so the host neither builds nor uploads them: d_out gets the KECCAK table
  * (n_rows x 2605: 24 rows per ecall, the rest zero) from `count` 52-word ecall
  * records, or the SHIFT table (n_rows x 148, padding rows shift 0 by 0) from
  * `count` 3-word shift records. Layouts: lambda_vm_b200/rv64_air.py's

@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "gl.cuh"
 
 namespace {
 
@@ -31,14 +32,17 @@ constexpr uint64_t KECCAK_CALL = ~0ULL - 1;  // a7 of the keccak ecall
 constexpr uint64_t EXIT_CALL = 93;
 // the ROM tuple's opcode ids (rv64.py OPS order, from 1)
 enum Op { ADD = 1, SUB, ADDI, LUI, BEQ, BNE, ECALL, XOR, OR, AND, XORI, ORI, ANDI, SLLI, SRLI, LD, SD };
-// Column layout of the CPU table (rv64_air.py); SEL0 + id - 1 is an opcode's
-// selector, SEL_KECCAK the keccak ecall's.
-constexpr int PC = 0, STEP = 1, CLK = 2, SEL0 = 3, SEL_KECCAK = 20, RD0 = 21, RS10 = 53, RS20 = 85, IMM_LO = 117,
-              IMM_HI = 118, IMM_F = 119, A_LO = 120, A_HI = 121, B_LO = 122, B_HI = 123, R_LO = 124, R_HI = 125,
-              R16 = 126, C0 = 130, C1 = 131, INV_LO = 132, INV_HI = 133, E_LO = 134, E_HI = 135, NE = 136, BR = 137,
-              AB0 = 138, BB0 = 146, RB0 = 154, MA = 162, MW0 = 163, MW1 = 164, MV_LO = 165, MV_HI = 166, MT = 167,
-              MD0 = 168, MD1 = 169, NV_LO = 170, NV_HI = 171, X0 = 172;
-static_assert(X0 + 62 == SG_RV64_CPU_WIDTH, "CPU table width");
+// Column layout of the CPU table (rv64_air.py): the core columns and the
+// register file (SG_RV64_CPU_CORE_WIDTH), then the chips' columns (to
+// SG_RV64_CPU_WIDTH). SEL0 + op - 1 is an opcode's selector (KECCAK_OP: the
+// keccak ecall's).
+constexpr int KECCAK_OP = 18;
+constexpr int PC = 0, STEP = 1, CLK = 2, SEL0 = 3, RD0 = 21, RS10 = 53, RS20 = 85, IMM_LO = 117, IMM_HI = 118,
+              IMM_F = 119, A_LO = 120, A_HI = 121, B_LO = 122, B_HI = 123, R_LO = 124, R_HI = 125, R16 = 126, C0 = 130,
+              C1 = 131, INV_LO = 132, INV_HI = 133, E_LO = 134, E_HI = 135, NE = 136, BR = 137, X0 = 138, AB0 = 200,
+              BB0 = 208, RB0 = 216, MA = 224, MW0 = 225, MW1 = 226, MV_LO = 227, MV_HI = 228, MT = 229, MD0 = 230,
+              MD1 = 231, NV_LO = 232, NV_HI = 233;
+static_assert(X0 + 62 == SG_RV64_CPU_CORE_WIDTH && NV_HI + 1 == SG_RV64_CPU_WIDTH, "CPU table widths");
 
 struct Ins {
     int op, rd, rs1, rs2;
@@ -146,17 +150,16 @@ struct Cell {
 using namespace sg;
 
 extern "C" int sg_rv64_run(const uint32_t* words, uint32_t nwords, uint64_t max_steps, uint64_t n_rows,
-                           uint64_t* cpu_out, uint64_t* counts_out, uint64_t* shifts_out, uint64_t* cells_out,
-                           uint64_t* keccak_out, void* reserved, sg_rv64_info* info) {
-    SG_CHECK_ARG(words && nwords && info && !reserved, "null argument");
-    SG_CHECK_ARG(!cpu_out || (n_rows >= 2 && (n_rows & (n_rows - 1)) == 0), "n_rows must be a power of two >= 2");
+                           uint64_t* rows_out, uint64_t* regs_out, uint64_t* counts_out, uint64_t* shifts_out,
+                           uint64_t* cells_out, uint64_t* keccak_out, sg_rv64_info* info) {
+    SG_CHECK_ARG(words && nwords && info, "null argument");
+    SG_CHECK_ARG(!rows_out || (n_rows >= 2 && (n_rows & (n_rows - 1)) == 0), "n_rows must be a power of two >= 2");
     std::vector<Ins> prog(nwords);
     for (uint32_t i = 0; i < nwords; ++i) SG_CHECK_ARG(decode(words[i], &prog[i]), "unsupported instruction word");
     if (counts_out) memset(counts_out, 0, nwords * sizeof(uint64_t));
     uint64_t x[32] = {0};
     uint64_t pc = 0, t = 0, nshift = 0, ncall = 0;
-    const uint64_t W = SG_RV64_CPU_WIDTH;
-    auto row_of = [&](uint64_t r) { return cpu_out + r * W; };
+    uint32_t chips = 0;
     std::unordered_map<uint64_t, Cell> mem;
     mem.reserve(1 << 16);
     auto cell = [&](uint64_t addr, Cell** c) {
@@ -165,14 +168,15 @@ extern "C" int sg_rv64_run(const uint32_t* words, uint32_t nwords, uint64_t max_
         return true;
     };
     bool halted = false;
-    uint64_t halt_row = 0;
     while (!halted) {
         SG_CHECK_ARG(t < max_steps, "the program did not halt within max_steps");
         SG_CHECK_ARG(pc % 4 == 0 && pc / 4 < nwords, "pc outside the program");
+        SG_CHECK_ARG(!rows_out || t < n_rows, "the execution does not fit n_rows");
+        if (regs_out && t % SG_RV64_REG_CHUNK == 0) memcpy(regs_out + 32 * (t / SG_RV64_REG_CHUNK), x, 256);
         const Ins& in = prog[pc / 4];
         const uint64_t a = x[in.rs1], b = x[in.rs2], iu = (uint64_t)in.imm, clk = t + 1;
         uint64_t r = 0, npc = pc + 4, ma = 0, mv = 0, mt = 0;
-        bool keccak = false;
+        int op = in.op;
         switch (in.op) {
             case ADD: r = a + b; break;
             case SUB: r = a - b; break;
@@ -204,7 +208,7 @@ extern "C" int sg_rv64_run(const uint32_t* words, uint32_t nwords, uint64_t max_
                     npc = pc;
                 } else {
                     SG_CHECK_ARG(x[17] == KECCAK_CALL, "unsupported ecall (a7 is neither 93 nor 2^64 - 2)");
-                    keccak = true;
+                    op = KECCAK_OP;
                     ma = x[10];
                     uint64_t lanes[25];
                     Cell* cs[25];
@@ -223,81 +227,28 @@ extern "C" int sg_rv64_run(const uint32_t* words, uint32_t nwords, uint64_t max_
                 }
                 break;
         }
-        if (in.op == SLLI || in.op == SRLI) {
+        if (op == SLLI || op == SRLI) {
             if (shifts_out) {
-                uint64_t* s = shifts_out + 3 * nshift;
-                s[0] = in.op == SRLI, s[1] = a, s[2] = iu;
+                uint64_t* sh = shifts_out + 3 * nshift;
+                sh[0] = op == SRLI, sh[1] = a, sh[2] = iu;
             }
             ++nshift;
+            chips |= SG_RV64_CHIP_SHIFT;
+        } else if (op >= XOR && op <= ANDI) {
+            chips |= SG_RV64_CHIP_BITWISE;
+        } else if (op == LD || op == SD) {
+            chips |= SG_RV64_CHIP_MEMORY;
+        } else if (op == KECCAK_OP) {
+            chips |= SG_RV64_CHIP_MEMORY | SG_RV64_CHIP_KECCAK;
         }
-        if (cpu_out) {
-            SG_CHECK_ARG(t < n_rows, "the execution does not fit n_rows");
-            uint64_t* row = row_of(t);
-            memset(row, 0, W * 8);
-            row[PC] = pc;
-            row[STEP] = 1;
-            row[CLK] = clk;
-            row[keccak ? SEL_KECCAK : SEL0 + in.op - 1] = 1;
-            row[RD0 + in.rd] = 1;
-            row[RS10 + in.rs1] = 1;
-            row[RS20 + in.rs2] = 1;
-            row[IMM_LO] = iu & M32;
-            row[IMM_HI] = iu >> 32;
-            row[IMM_F] = in.imm < 0 ? P - (uint64_t)(-in.imm) : iu;
-            row[A_LO] = a & M32, row[A_HI] = a >> 32;
-            row[B_LO] = b & M32, row[B_HI] = b >> 32;
-            row[R_LO] = r & M32, row[R_HI] = r >> 32;
-            for (int j = 0; j < 4; ++j) row[R16 + j] = (r >> (16 * j)) & 0xFFFF;
-            if (in.op == ADD || in.op == ADDI || in.op == LD || in.op == SD) {
-                const uint64_t o = in.op == ADD ? b : iu;
-                const uint64_t c0 = ((a & M32) + (o & M32)) >> 32;
-                row[C0] = c0;
-                row[C1] = ((a >> 32) + (o >> 32) + c0) >> 32;
-            } else if (in.op == SUB) {
-                const uint64_t b0 = (a & M32) < (b & M32);
-                row[C0] = b0;
-                row[C1] = (a >> 32) < (b >> 32) + b0;
-            }
-            if (in.op == BEQ || in.op == BNE) {
-                const uint64_t dl = ((a & M32) + P - (b & M32)) % P;
-                const uint64_t dh = ((a >> 32) + P - (b >> 32)) % P;
-                row[INV_LO] = dl ? sg_host_gl_inv(dl) : 0;
-                row[INV_HI] = dh ? sg_host_gl_inv(dh) : 0;
-                row[E_LO] = dl != 0, row[E_HI] = dh != 0;
-                const uint64_t ne = row[E_LO] | row[E_HI];
-                row[NE] = ne;
-                row[BR] = in.op == BNE ? ne : 1 - ne;
-            }
-            if (in.op >= XOR && in.op <= ANDI) {
-                const uint64_t second = in.op <= AND ? b : iu;
-                for (int i = 0; i < 8; ++i) {
-                    row[AB0 + i] = (a >> (8 * i)) & 0xFF;
-                    row[BB0 + i] = (second >> (8 * i)) & 0xFF;
-                    row[RB0 + i] = (r >> (8 * i)) & 0xFF;
-                }
-            }
-            if (in.op == LD || in.op == SD || keccak) {
-                row[MA] = ma;
-                row[MW0] = (ma >> 3) & 0xFFFF;
-                row[MW1] = ma >> 19;
-            }
-            if (in.op == LD || in.op == SD) {
-                row[MV_LO] = mv & M32, row[MV_HI] = mv >> 32;
-                row[MT] = mt;
-                const uint64_t gap = clk - mt - 1;
-                row[MD0] = gap & 0xFFFF, row[MD1] = gap >> 16;
-                const uint64_t nv = in.op == LD ? mv : b;
-                row[NV_LO] = nv & M32, row[NV_HI] = nv >> 32;
-            }
-            for (int k = 1; k < 32; ++k) {
-                row[X0 + 2 * (k - 1)] = x[k] & M32;
-                row[X0 + 2 * (k - 1) + 1] = x[k] >> 32;
-            }
+        if (rows_out) {
+            uint64_t* q = rows_out + 8 * t;
+            q[0] = pc | ((uint64_t)op << 32) | ((uint64_t)in.rd << 40) | ((uint64_t)in.rs1 << 48) | ((uint64_t)in.rs2 << 56);
+            q[1] = iu, q[2] = a, q[3] = b, q[4] = r, q[5] = ma, q[6] = mv, q[7] = mt;
         }
         if (counts_out) counts_out[pc / 4] += 1;
         const bool writes = !(in.op == BEQ || in.op == BNE || in.op == ECALL || in.op == SD);
         if (in.rd && writes) x[in.rd] = r;
-        halt_row = t;
         pc = npc;
         ++t;
     }
@@ -306,14 +257,14 @@ extern "C" int sg_rv64_run(const uint32_t* words, uint32_t nwords, uint64_t max_
     info->shifts = nshift;
     info->cells = mem.size();
     info->keccak_calls = ncall;
-    if (cpu_out) {
-        // the halting row repeats to fill the table; the last row ends the cycle
-        for (uint64_t r = t; r < n_rows; ++r) {
-            memcpy(row_of(r), row_of(halt_row), W * 8);
-            row_of(r)[CLK] = r + 1;
-        }
+    info->chips = chips;
+    if (rows_out) {
+        // the halting row repeats to fill the table, with the final registers
         if (counts_out) counts_out[pc / 4] += n_rows - t;
-        row_of(n_rows - 1)[STEP] = 0;
+        if (regs_out)
+            for (uint64_t r = (t + SG_RV64_REG_CHUNK - 1) / SG_RV64_REG_CHUNK * SG_RV64_REG_CHUNK; r < n_rows;
+                 r += SG_RV64_REG_CHUNK)
+                memcpy(regs_out + 32 * (r / SG_RV64_REG_CHUNK), x, 256);
     }
     if (cells_out) {
         std::vector<std::pair<uint64_t, Cell>> cs(mem.begin(), mem.end());
@@ -439,6 +390,114 @@ __global__ void k_shift_rows(const uint64_t* __restrict__ ev, uint64_t count, ui
     }
 }
 
+// (a - b) mod p of two values below 2^32
+__device__ __forceinline__ uint64_t sub_small(uint64_t a, uint64_t b) { return a >= b ? a - b : GL_P - (b - a); }
+
+// One cell of the CPU table outside the register file, from the row's record.
+__device__ uint64_t cpu_cell(uint32_t c, uint64_t row, uint64_t n_rows, uint32_t op, uint64_t pc, uint32_t rd,
+                             uint32_t rs1, uint32_t rs2, uint64_t imm, uint64_t a, uint64_t b, uint64_t r, uint64_t ma,
+                             uint64_t mv, uint64_t mt) {
+    if (c == PC) return pc;
+    if (c == STEP) return row + 1 != n_rows;
+    if (c == CLK) return row + 1;
+    if (c < RD0) return c - SEL0 + 1 == op;
+    if (c < RS10) return c - RD0 == rd;
+    if (c < RS20) return c - RS10 == rs1;
+    if (c < IMM_LO) return c - RS20 == rs2;
+    switch (c) {
+        case IMM_LO: return imm & M32;
+        case IMM_HI: return imm >> 32;
+        case IMM_F: return (int64_t)imm < 0 ? GL_P - (uint64_t)(-(int64_t)imm) : imm;
+        case A_LO: return a & M32;
+        case A_HI: return a >> 32;
+        case B_LO: return b & M32;
+        case B_HI: return b >> 32;
+        case R_LO: return r & M32;
+        case R_HI: return r >> 32;
+        case R16: case R16 + 1: case R16 + 2: case R16 + 3: return (r >> (16 * (c - R16))) & 0xFFFF;
+        case C0: case C1: {
+            if (op == ADD || op == ADDI || op == LD || op == SD) {
+                const uint64_t o = op == ADD ? b : imm;
+                const uint64_t c0 = ((a & M32) + (o & M32)) >> 32;
+                return c == C0 ? c0 : ((a >> 32) + (o >> 32) + c0) >> 32;
+            }
+            if (op == SUB) {
+                const uint64_t b0 = (a & M32) < (b & M32);
+                return c == C0 ? b0 : (uint64_t)((a >> 32) < (b >> 32) + b0);
+            }
+            return 0;
+        }
+        default: break;
+    }
+    if (c <= BR) {  // INV_LO .. BR: the branch witnesses
+        if (op != BEQ && op != BNE) return 0;
+        const uint64_t dl = sub_small(a & M32, b & M32), dh = sub_small(a >> 32, b >> 32);
+        const uint64_t ne = (dl != 0) | (dh != 0);
+        switch (c) {
+            case INV_LO: return dl ? gl::canon(gl::inv(dl)) : 0;
+            case INV_HI: return dh ? gl::canon(gl::inv(dh)) : 0;
+            case E_LO: return dl != 0;
+            case E_HI: return dh != 0;
+            case NE: return ne;
+            default: return op == BNE ? ne : 1 - ne;
+        }
+    }
+    if (c < MA) {  // bytes of a, of the second operand and of the result (bitwise ops)
+        if (op < XOR || op > ANDI) return 0;
+        const uint32_t i = (c - AB0) % 8;
+        const uint64_t v = c < BB0 ? a : c < RB0 ? (op <= AND ? b : imm) : r;
+        return (v >> (8 * i)) & 0xFF;
+    }
+    const bool mem = op == LD || op == SD;
+    switch (c) {
+        case MA: return mem || op == KECCAK_OP ? ma : 0;
+        case MW0: return mem || op == KECCAK_OP ? (ma >> 3) & 0xFFFF : 0;
+        case MW1: return mem || op == KECCAK_OP ? ma >> 19 : 0;
+        case MV_LO: return mem ? mv & M32 : 0;
+        case MV_HI: return mem ? mv >> 32 : 0;
+        case MT: return mem ? mt : 0;
+        case MD0: return mem ? (row - mt) & 0xFFFF : 0;  // (row + 1) - mt - 1
+        case MD1: return mem ? (row - mt) >> 16 : 0;
+        case NV_LO: return op == LD ? mv & M32 : op == SD ? b & M32 : 0;
+        default: return op == LD ? mv >> 32 : op == SD ? b >> 32 : 0;  // NV_HI
+    }
+}
+
+// One warp per chunk of SG_RV64_REG_CHUNK rows: lane k holds register x_k
+// (from the chunk's snapshot) and the warp walks the chunk's rows in order,
+// writing each row's register columns by shuffles and its other columns
+// lane-strided, then applying the row's register write. Rows past the
+// execution repeat the halting row's record with their own timestamps.
+__global__ void k_cpu_rows(const uint64_t* __restrict__ recs, uint64_t T, const uint64_t* __restrict__ regs,
+                           uint64_t n_rows, uint32_t width, uint64_t* __restrict__ out) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const uint64_t nchunks = (n_rows + SG_RV64_REG_CHUNK - 1) / SG_RV64_REG_CHUNK;
+    const uint32_t k1 = lane / 2 + 1, k2 = lane < 30 ? (lane + 32) / 2 + 1 : 31;
+    for (uint64_t ch = warp; ch < nchunks; ch += nwarps) {
+        uint64_t xr = regs[32 * ch + lane];
+        const uint64_t r0 = ch * SG_RV64_REG_CHUNK;
+        const uint64_t r1 = r0 + SG_RV64_REG_CHUNK < n_rows ? r0 + SG_RV64_REG_CHUNK : n_rows;
+        for (uint64_t row = r0; row < r1; ++row) {
+            const uint64_t* q = recs + 8 * (row < T ? row : T - 1);
+            const uint64_t w0 = q[0], imm = q[1], a = q[2], b = q[3], r = q[4], ma = q[5], mv = q[6], mt = q[7];
+            const uint32_t op = (uint32_t)(w0 >> 32) & 0xFF, rd = (uint32_t)(w0 >> 40) & 0xFF,
+                           rs1 = (uint32_t)(w0 >> 48) & 0xFF, rs2 = (uint32_t)(w0 >> 56);
+            uint64_t* o = out + row * width;
+            const uint64_t v1 = __shfl_sync(0xFFFFFFFFu, xr, k1), v2 = __shfl_sync(0xFFFFFFFFu, xr, k2);
+            o[X0 + lane] = (lane & 1) ? v1 >> 32 : v1 & M32;
+            if (lane < 30) o[X0 + 32 + lane] = (lane & 1) ? v2 >> 32 : v2 & M32;
+            for (uint32_t c = lane; c < width; c += 32) {
+                if (c >= (uint32_t)X0 && c < (uint32_t)X0 + 62) continue;
+                o[c] = cpu_cell(c, row, n_rows, op, w0 & M32, rd, rs1, rs2, imm, a, b, r, ma, mv, mt);
+            }
+            const bool writes = row < T && !(op == BEQ || op == BNE || op == ECALL || op == SD || op == KECCAK_OP);
+            if (writes && rd != 0 && lane == rd) xr = r;
+        }
+    }
+}
+
 int upload_events(Ctx* ctx, cudaStream_t st, const uint64_t* host, uint64_t words, uint64_t** d) {
     SG_TRY(dev_alloc(ctx, st, 8 * words, (void**)d));
     if (cudaMemcpyAsync(*d, host, 8 * words, cudaMemcpyHostToDevice, st) != cudaSuccess) {
@@ -450,6 +509,36 @@ int upload_events(Ctx* ctx, cudaStream_t st, const uint64_t* host, uint64_t word
 }
 
 }  // namespace
+
+extern "C" int sg_rv64_cpu_table(sg_ctx* c, void* stream, const uint64_t* rows, uint64_t count, const uint64_t* regs,
+                                 uint64_t n_rows, uint32_t width, uint64_t* d_out) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(c);
+    SG_CHECK_ARG(ctx && d_out && rows && regs, "null argument");
+    SG_ENTER(ctx);
+    SG_CHECK_ARG(count >= 1 && count <= n_rows, "the execution does not fit n_rows");
+    SG_CHECK_ARG(width == SG_RV64_CPU_CORE_WIDTH || width == SG_RV64_CPU_WIDTH, "width is the core or the full width");
+    for (uint64_t i = 0; i < count; ++i) {
+        const uint64_t w0 = rows[8 * i];
+        const uint32_t op = (uint32_t)(w0 >> 32) & 0xFF;
+        SG_CHECK_ARG(op >= 1 && op <= KECCAK_OP && ((w0 >> 40) & 0xFF) < 32 && ((w0 >> 48) & 0xFF) < 32 &&
+                         (w0 >> 56) < 32, "bad row record");
+        SG_CHECK_ARG(width == SG_RV64_CPU_WIDTH || op < XOR || op == SLLI || op == SRLI,
+                     "a chip instruction in a table without the chips' columns");
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const uint64_t nchunks = (n_rows + SG_RV64_REG_CHUNK - 1) / SG_RV64_REG_CHUNK;
+    uint64_t *d_rows = nullptr, *d_regs = nullptr;
+    SG_TRY(upload_events(ctx, st, rows, 8 * count, &d_rows));
+    int rc = upload_events(ctx, st, regs, 32 * nchunks, &d_regs);
+    if (rc == SG_OK) {
+        const uint64_t warps = nchunks < 148ull * 64 ? nchunks : 148ull * 64;
+        k_cpu_rows<<<(unsigned)((warps + 7) / 8), 256, 0, st>>>(d_rows, count, d_regs, n_rows, width, d_out);
+        rc = check_launch(ctx, "k_cpu_rows");
+        dev_free(ctx, st, d_regs, 8 * 32 * nchunks);
+    }
+    dev_free(ctx, st, d_rows, 8 * 8 * count);
+    return rc;
+}
 
 extern "C" int sg_rv64_keccak_table(sg_ctx* c, void* stream, const uint64_t* calls, uint64_t count, uint64_t n_rows,
                                     uint64_t* d_out) {

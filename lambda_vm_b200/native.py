@@ -37,7 +37,7 @@ class PassRecord(C.Structure):
 
 class Rv64Info(C.Structure):
     _fields_ = [("cycles", C.c_uint64), ("a0", C.c_uint64), ("shifts", C.c_uint64), ("cells", C.c_uint64),
-                ("keccak_calls", C.c_uint64)]
+                ("keccak_calls", C.c_uint64), ("chips", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 class VerifyTable(C.Structure):
@@ -175,6 +175,7 @@ PROTOTYPES = {
     "sg_synth_trace": (i32, [vp, vp, vp, u64, u64, u64, u32]),
     "sg_ctx_pass_log": (i32, [vp, i32]),
     "sg_rv64_run": (i32, [vp, u32, u64, u64, vp, vp, vp, vp, vp, vp, vp]),
+    "sg_rv64_cpu_table": (i32, [vp, vp, vp, u64, vp, u64, u32, vp]),
     "sg_rv64_keccak_table": (i32, [vp, vp, vp, u64, u64, vp]),
     "sg_rv64_shift_table": (i32, [vp, vp, vp, u64, u64, vp]),
     "sg_verify_queries": (i32, [vp, vp, C.POINTER(VerifyTable), u32, vp]),

@@ -212,7 +212,9 @@ R_LO, R_HI = B_HI + 1, B_HI + 2
 R16 = R_HI + 1                                    # four 16-bit pieces of the written value
 C0, C1 = R16 + 4, R16 + 5
 INV_LO, INV_HI, E_LO, E_HI, NE, BR = C1 + 1, C1 + 2, C1 + 3, C1 + 4, C1 + 5, C1 + 6
-AB0 = BR + 1                                      # bytes of a, of the second operand, of the result
+X0 = BR + 1                                       # x1..x31: lo at X0 + 2(k-1), hi next
+CPU_CORE_WIDTH = X0 + 62                          # the table of a run that needs no chip ends here
+AB0 = CPU_CORE_WIDTH                              # bytes of a, of the second operand, of the result
 BB0 = AB0 + 8
 RB0 = BB0 + 8
 MA = RB0 + 8                                      # memory address (ld / sd / keccak state)
@@ -220,8 +222,9 @@ MW0, MW1 = MA + 1, MA + 2                         # MA = 8 MW0 + 2^19 MW1
 MV_LO, MV_HI, MT = MA + 3, MA + 4, MA + 5         # the cell's value and timestamp before the access
 MD0, MD1 = MA + 6, MA + 7                         # CLK - MT - 1 in 16-bit pieces
 NV_LO, NV_HI = MA + 8, MA + 9                     # the value the access leaves
-X0 = NV_HI + 1                                    # x1..x31: lo at X0 + 2(k-1), hi next
-CPU_WIDTH = X0 + 62
+CPU_WIDTH = NV_HI + 1
+KECCAK_OP = len(OPS) + 1                          # the keccak ecall's op in a row record
+REG_CHUNK = 64                                    # register snapshots every REG_CHUNK rows
 WRITES = ("add", "sub", "addi", "lui", "xor", "or", "and", "xori", "ori", "andi", "slli", "srli", "ld")
 BIT_REG, BIT_IMM = ("xor", "or", "and"), ("xori", "ori", "andi")
 BIT_KIND = {"xor": 1, "xori": 1, "or": 2, "ori": 2, "and": 3, "andi": 3}
@@ -273,8 +276,9 @@ class CpuAir(BusAir):
         self.words = list(words)
         self.prog = [decode(w) for w in self.words]
         assert any(ins[0] == "ecall" for ins in self.prog), "a program halts by an ecall"
-        self.log_n, self.n, self.width = log_n, 1 << log_n, CPU_WIDTH
         self.chips = tuple(c for c in CHIPS if c in chips)
+        self.log_n, self.n = log_n, 1 << log_n
+        self.width = CPU_WIDTH if self.chips else CPU_CORE_WIDTH
         rom_op = [(OP_ID["ecall" if o == "keccak" else o], SEL[o]) for o in CPU_OPS]
         its = [
             {"bus": BUS_ROM, "sender": True, "mult": (1, []),
@@ -435,40 +439,34 @@ class CpuAir(BusAir):
         return b.program()
 
     # ---------------------------------------------------------- trace
-    def trace(self, rows, keccak_rows=()):
-        """CPU table of an execution (rv64.run rows; keccak_rows: the row
-        indices of Keccak ecalls), padded to n rows by repeating the halting
-        ECALL; the last row is the END row. Built column by column with numpy."""
-        n, T = self.n, len(rows)
+    def trace(self, records):
+        """CPU table of an execution from its row records (T x 8 u64, the
+        layout sg_rv64_run writes: pc | op << 32 | rd << 40 | rs1 << 48 |
+        rs2 << 56, imm, a, b, r, memory address, the cell's previous value and
+        timestamp), padded to n rows by repeating the halting ECALL; the last
+        row is the END row. Built column by column with numpy."""
+        rec = np.asarray(records, np.uint64).reshape(-1, 8)
+        n, T = self.n, rec.shape[0]
         assert 1 <= T <= n, "the execution does not fit the table"
-        cols = list(zip(*rows))
-        ext = lambda c: np.concatenate([c, np.full(n - T, c[-1], dtype=c.dtype)])
-        u64 = lambda i: ext(np.array(cols[i], dtype=np.uint64))
-        pc, rd, rs1, rs2 = u64(0), u64(2), u64(3), u64(4)
-        imm_i = ext(np.array(cols[5], dtype=np.int64))
-        imm_u = imm_i.view(np.uint64)
-        a, bv, r = u64(6), u64(7), u64(8)
-        if len(cols) > 9:
-            ma, mv, mt = u64(9), u64(10), u64(11)
-        else:
-            ma = mv = mt = np.zeros(n, np.uint64)
-        op = ext(np.array([OP_ID[o] for o in cols[1]], dtype=np.int64))
-        kecc = np.zeros(n, bool)
-        kecc[list(keccak_rows)] = True
-        is_op = lambda *names: np.isin(op, [OP_ID[o] for o in names])
+        rec = np.concatenate([rec, np.repeat(rec[-1:], n - T, axis=0)])
+        w0 = rec[:, 0]
+        pc = w0 & np.uint64(0xFFFFFFFF)
+        op = ((w0 >> np.uint64(32)) & np.uint64(0xFF)).astype(np.int64)
+        rd, rs1, rs2 = (((w0 >> np.uint64(s_)) & np.uint64(0xFF)).astype(np.int64) for s_ in (40, 48, 56))
+        imm_u, a, bv, r, ma, mv, mt = (rec[:, i] for i in range(1, 8))
+        imm_i = imm_u.view(np.int64)
+        is_op = lambda *names: np.isin(op, [KECCAK_OP if o == "keccak" else OP_ID[o] for o in names])
         m32, s32 = np.uint64(0xFFFFFFFF), np.uint64(32)
         idx = np.arange(n)
-        t = np.zeros((CPU_WIDTH, n), dtype=np.uint64)  # column-major while filling
+        t = np.zeros((self.width, n), dtype=np.uint64)  # column-major while filling
         t[PC] = pc
         t[STEP] = 1
         t[STEP, n - 1] = 0
         t[CLK] = idx + 1
-        selcol = np.array([SEL[o] for o in OPS])[op - 1]
-        selcol[kecc] = SEL["keccak"]
-        t[selcol, idx] = 1
-        t[RD0 + rd.astype(np.int64), idx] = 1
-        t[RS10 + rs1.astype(np.int64), idx] = 1
-        t[RS20 + rs2.astype(np.int64), idx] = 1
+        t[SEL["add"] + op - 1, idx] = 1
+        t[RD0 + rd, idx] = 1
+        t[RS10 + rs1, idx] = 1
+        t[RS20 + rs2, idx] = 1
         t[IMM_LO], t[IMM_HI] = imm_u & m32, imm_u >> s32
         t[IMM_F] = np.where(imm_i < 0, np.uint64(P) - (-imm_i).astype(np.uint64), imm_u)
         t[A_LO], t[A_HI] = a & m32, a >> s32
@@ -495,24 +493,6 @@ class CpuAir(BusAir):
         ne = t[E_LO] | t[E_HI]
         t[NE] = ne
         t[BR] = np.where(op == OP_ID["bne"], ne, np.where(op == OP_ID["beq"], 1 - ne, 0))
-        # bitwise rows: bytes of a, of the second operand, of the result
-        bit = is_op(*BIT_REG, *BIT_IMM)
-        second = np.where(is_op(*BIT_REG), bv, imm_u)
-        for first, v in ((AB0, a), (BB0, second), (RB0, r)):
-            for i in range(8):
-                t[first + i] = np.where(bit, (v >> np.uint64(8 * i)) & np.uint64(0xFF), 0)
-        # memory rows
-        mem = is_op("ld", "sd")
-        addr = mem | kecc
-        t[MA] = np.where(addr, ma, 0)
-        t[MW0] = np.where(addr, (ma >> np.uint64(3)) & np.uint64(0xFFFF), 0)
-        t[MW1] = np.where(addr, ma >> np.uint64(19), 0)
-        t[MV_LO], t[MV_HI] = np.where(mem, mv & m32, 0), np.where(mem, mv >> s32, 0)
-        t[MT] = np.where(mem, mt, 0)
-        gap = np.where(mem, (idx + 1).astype(np.uint64) - mt - np.uint64(1), np.uint64(0))
-        t[MD0], t[MD1] = gap & np.uint64(0xFFFF), gap >> np.uint64(16)
-        nv = np.where(op == OP_ID["ld"], mv, np.where(op == OP_ID["sd"], bv, 0))
-        t[NV_LO], t[NV_HI] = nv & m32, nv >> s32
         # register file before each row: the last value written below it
         writes = is_op(*WRITES) & (rd != 0) & (idx < T)
         for k in range(1, 32):
@@ -521,13 +501,35 @@ class CpuAir(BusAir):
             before = np.concatenate(([-1], last[:-1]))
             val = np.where(before >= 0, r[np.maximum(before, 0)], np.uint64(0))
             t[xlo(k)], t[xhi(k)] = val & m32, val >> s32
+        if self.width == CPU_WIDTH:
+            # bitwise rows: bytes of a, of the second operand, of the result
+            bit = is_op(*BIT_REG, *BIT_IMM)
+            second = np.where(is_op(*BIT_REG), bv, imm_u)
+            for first, v in ((AB0, a), (BB0, second), (RB0, r)):
+                for i in range(8):
+                    t[first + i] = np.where(bit, (v >> np.uint64(8 * i)) & np.uint64(0xFF), 0)
+            # memory rows
+            mem = is_op("ld", "sd")
+            addr = mem | is_op("keccak")
+            t[MA] = np.where(addr, ma, 0)
+            t[MW0] = np.where(addr, (ma >> np.uint64(3)) & np.uint64(0xFFFF), 0)
+            t[MW1] = np.where(addr, ma >> np.uint64(19), 0)
+            t[MV_LO], t[MV_HI] = np.where(mem, mv & m32, 0), np.where(mem, mv >> s32, 0)
+            t[MT] = np.where(mem, mt, 0)
+            gap = np.where(mem, (idx + 1).astype(np.uint64) - mt - np.uint64(1), np.uint64(0))
+            t[MD0], t[MD1] = gap & np.uint64(0xFFFF), gap >> np.uint64(16)
+            nv = np.where(op == OP_ID["ld"], mv, np.where(op == OP_ID["sd"], bv, 0))
+            t[NV_LO], t[NV_HI] = nv & m32, nv >> s32
+        else:
+            assert not is_op(*NEEDS, "keccak").any(), "a chip instruction in a table without the chips' columns"
         return np.ascontiguousarray(t.T)
 
-    def counts(self, rows):
+    def counts(self, records):
         """Execution count of every program instruction over the n table rows."""
-        pcs = np.array([r_[0] for r_ in rows], dtype=np.int64) // 4
+        rec = np.asarray(records, np.uint64).reshape(-1, 8)
+        pcs = ((rec[:, 0] & np.uint64(0xFFFFFFFF)) // np.uint64(4)).astype(np.int64)
         c = np.bincount(pcs, minlength=len(self.prog))
-        c[pcs[-1]] += self.n - len(rows)  # the repeated halting row
+        c[pcs[-1]] += self.n - rec.shape[0]  # the repeated halting row
         return [int(v) for v in c]
 
     def public_terms(self, counts, output):
@@ -612,7 +614,9 @@ class BitwiseAir(BusAir):
         self._emit_logup(b)
         return b.program()
 
-    def trace(self, cpu_trace):
+    def trace(self, records):
+        """The table with the multiplicities of the byte triples the CPU's
+        bitwise rows (row records, as CpuAir.trace) look up."""
         t = np.zeros((self.n, self.width), np.uint64)
         v = np.arange(self.n, dtype=np.uint64)
         xv, yv = v >> np.uint64(8), v & np.uint64(0xFF)
@@ -620,13 +624,17 @@ class BitwiseAir(BusAir):
             t[:, self.XB + i] = (xv >> np.uint64(i)) & np.uint64(1)
             t[:, self.YB + i] = (yv >> np.uint64(i)) & np.uint64(1)
         t[:, self.XOR], t[:, self.OR], t[:, self.AND] = xv ^ yv, xv | yv, xv & yv
-        kind = np.zeros(cpu_trace.shape[0], np.int64)
-        for o, k in BIT_KIND.items():
-            kind[cpu_trace[:, SEL[o]] == 1] = k
+        rec = np.asarray(records, np.uint64).reshape(-1, 8)
+        op = ((rec[:, 0] >> np.uint64(32)) & np.uint64(0xFF)).astype(np.int64)
+        sh = np.arange(0, 64, 8, dtype=np.uint64)
         for k, mcol in ((1, self.MX), (2, self.MO), (3, self.MAN)):
-            rows = kind == k
-            keys = (cpu_trace[rows, AB0:AB0 + 8].astype(np.int64) << 8) | cpu_trace[rows, BB0:BB0 + 8].astype(np.int64)
-            t[:, mcol] = np.bincount(keys.reshape(-1), minlength=self.n).astype(np.uint64)
+            reg = np.isin(op, [OP_ID[o] for o in BIT_REG if BIT_KIND[o] == k])
+            imm = np.isin(op, [OP_ID[o] for o in BIT_IMM if BIT_KIND[o] == k])
+            rows = reg | imm
+            a = rec[rows, 2]
+            second = np.where(reg[rows], rec[rows, 3], rec[rows, 1])
+            keys = (((a[:, None] >> sh) & np.uint64(0xFF)) << np.uint64(8)) | ((second[:, None] >> sh) & np.uint64(0xFF))
+            t[:, mcol] = np.bincount(keys.reshape(-1).astype(np.int64), minlength=self.n).astype(np.uint64)
         return t
 
 
@@ -988,42 +996,83 @@ def airs_for(words, counts, heights=None):
 
 
 class Events:
-    """What the chips need from a run, as arrays: the CPU table, counts, a0,
-    cycles; shifts (dir, a, k); the touched cells (sorted addresses, final
-    values, final timestamps); Keccak ecalls (timestamps, addresses, input
-    lanes, previous timestamps)."""
+    """What the tables need from a run, as arrays: row records (T x 8, as
+    CpuAir.trace takes them), register snapshots (32 registers before every
+    REG_CHUNK-th row of the CPU table), counts, a0, cycles, the chips used;
+    shifts (dir, a, k); the touched cells (sorted addresses, final values,
+    final timestamps); Keccak ecalls (timestamps, addresses, input lanes,
+    previous timestamps)."""
 
-    def __init__(self, cpu_trace, counts, output, cycles, shifts, cells, keccak):
-        self.cpu_trace, self.counts, self.output, self.cycles = cpu_trace, counts, output, cycles
-        self.shifts, self.cells, self.keccak = shifts, cells, keccak
+    def __init__(self, records, regs, counts, output, cycles, chips, shifts, cells, keccak):
+        self.records, self.regs, self.counts, self.output, self.cycles = records, regs, counts, output, cycles
+        self.chips, self.shifts, self.cells, self.keccak = chips, shifts, cells, keccak
 
 
-def python_events(words, max_steps=1 << 26, log_n=None):
-    """Events of a run of the Python executor (rv64.run) with the CPU table
-    built in numpy."""
+def _chips_used(ops):
+    used = {NEEDS[o] for o in ops if o in NEEDS}
+    if "keccak" in ops:
+        used |= {"keccak", "memory"}
+    return tuple(c for c in CHIPS if c in used)
+
+
+def python_events(words, max_steps=1 << 26):
+    """Events of a run of the Python executor (rv64.run)."""
     ex = run(words, max_steps)
     rows = ex.rows
     T = len(rows)
-    chips = _chips_used(rows, ex)
-    cpu = CpuAir(words, log_n or max(1, (T - 1).bit_length()), chips)
-    ct = cpu.trace(rows, [k[0] for k in ex.keccak])
+    n = 1 << max(1, (T - 1).bit_length())
+    kecc = {k[0] for k in ex.keccak}
+    ops = [("keccak" if i in kecc else r_[1]) for i, r_ in enumerate(rows)]
+    rec = np.zeros((T, 8), np.uint64)
+    opid = np.array([KECCAK_OP if o == "keccak" else OP_ID[o] for o in ops], np.uint64)
+    f = lambda i: np.array([r_[i] for r_ in rows], np.uint64)
+    rec[:, 0] = f(0) | (opid << np.uint64(32)) | (f(2) << np.uint64(40)) | (f(3) << np.uint64(48)) | \
+        (f(4) << np.uint64(56))
+    rec[:, 1] = np.array([r_[5] for r_ in rows], np.int64).view(np.uint64)
+    for i in range(2, 8):
+        rec[:, i] = f(i + 4)
+    # register snapshots: replay the writes
+    regs = np.zeros(((n + REG_CHUNK - 1) // REG_CHUNK, 32), np.uint64)
+    x = [0] * 32
+    for t, r_ in enumerate(rows):
+        if t % REG_CHUNK == 0:
+            regs[t // REG_CHUNK] = x
+        if r_[2] and ops[t] in WRITES:
+            x[r_[2]] = r_[8]
+    for c in range((T + REG_CHUNK - 1) // REG_CHUNK, regs.shape[0]):
+        regs[c] = x
+    pcs = f(0).astype(np.int64) // 4
+    counts = np.bincount(pcs, minlength=len(words))
+    counts[pcs[-1]] += n - T
     shifts = np.array([(1 if r_[1] == "srli" else 0, r_[6], r_[5]) for r_ in rows if r_[1] in ("slli", "srli")],
                       np.uint64).reshape(-1, 3)
     addrs = sorted(ex.memory)
-    cells = (np.array(addrs, np.uint64), np.array([ex.memory[a][0] for a in addrs], np.uint64),
-             np.array([ex.memory[a][1] for a in addrs], np.uint64))
+    cells = (np.array(addrs, np.uint64), np.array([ex.memory[a_][0] for a_ in addrs], np.uint64),
+             np.array([ex.memory[a_][1] for a_ in addrs], np.uint64))
     kc = (np.array([k[0] + 1 for k in ex.keccak], np.uint64), np.array([k[1] for k in ex.keccak], np.uint64),
           np.array([k[2] for k in ex.keccak], np.uint64).reshape(-1, 25),
           np.array([k[3] for k in ex.keccak], np.uint64).reshape(-1, 25))
-    return Events(ct, cpu.counts(rows), ex.regs[10], T, shifts, cells, kc)
+    return Events(rec, regs, [int(c) for c in counts], ex.regs[10], T, _chips_used(set(ops)), shifts, cells, kc)
 
 
-def _chips_used(rows, ex):
-    ops = {r_[1] for r_ in rows}
-    used = {NEEDS[o] for o in ops if o in NEEDS}
-    if ex.keccak:
-        used |= {"keccak", "memory"}
-    return tuple(c for c in CHIPS if c in used)
+class CpuSource:
+    """The CPU table of a run's row records and register snapshots: written
+    on the device by the GPU backend (sg_rv64_cpu_table), built with numpy
+    otherwise."""
+
+    def __init__(self, records, regs):
+        self.records = np.ascontiguousarray(records, np.uint64)
+        self.regs = np.ascontiguousarray(regs, np.uint64)
+
+    def host_trace(self, air):
+        return air.trace(self.records)
+
+    def device_trace(self, bk, air):
+        from . import native
+        m = bk._alloc(air.n, air.width)
+        native.check(bk.L.sg_rv64_cpu_table(bk.be.h, bk.st, self.records.ctypes.data, self.records.shape[0],
+                                            self.regs.ctypes.data, air.n, air.width, m.ptr))
+        return m
 
 
 class ShiftSource:
@@ -1075,28 +1124,35 @@ class KeccakSource:
 
 def tables_from_events(words, ev, host_tables=False):
     """(airs, traces, public) of a run's events: public = {"words", "counts",
-    "output", "cycles", "heights", "label", "terms"}. The SHIFT and KECCAK
-    entries of traces are table sources the GPU backend expands on the device
-    (stark._gen_trace), or numpy tables with host_tables."""
-    ct = ev.cpu_trace
-    heights = {"cpu": ct.shape[0].bit_length() - 1, "range": 16}
-    bit = any(ct[:, SEL[o]].any() for o in BIT_REG + BIT_IMM)
-    if bit:
+    "output", "cycles", "heights", "label", "terms"}. The CPU, SHIFT and
+    KECCAK entries of traces are table sources the GPU backend writes on the
+    device (stark._gen_trace), or numpy tables with host_tables."""
+    rec = ev.records
+    T = rec.shape[0]
+    heights = {"cpu": max(1, (T - 1).bit_length()), "range": 16}
+    n = 1 << heights["cpu"]
+    if "bitwise" in ev.chips:
         heights["bitwise"] = 16
-    if len(ev.shifts):
+    if "shift" in ev.chips:
         heights["shift"] = _log2_rows(len(ev.shifts))
-    if len(ev.cells[0]):
+    if "memory" in ev.chips:
         heights["memory"] = _log2_rows(len(ev.cells[0]))
-    if len(ev.keccak[0]):
+    if "keccak" in ev.chips:
         heights["keccak"] = _log2_rows(24 * len(ev.keccak[0]))
     chips = chips_of(heights)
     cpu = CpuAir(words, heights["cpu"], chips)
-    airs, traces = [cpu, RangeAir()], [ct, None]
-    look = [ct[:, R16:R16 + 4]]
+    csrc = CpuSource(rec, ev.regs)
+    airs, traces = [cpu, RangeAir()], [csrc.host_trace(cpu) if host_tables else csrc, None]
+    # the CPU's RANGE lookups: the result's four 16-bit pieces on every row
+    # (rows past the halt repeat its zero result), the address and timestamp
+    # pieces of memory rows
+    op = ((rec[:, 0] >> np.uint64(32)) & np.uint64(0xFF)).astype(np.int64)
+    r = rec[:, 4]
+    look = [(r[:, None] >> np.arange(0, 64, 16, dtype=np.uint64)) & np.uint64(0xFFFF), np.zeros(4 * (n - T), np.uint64)]
     if "bitwise" in chips:
         a = BitwiseAir()
         airs.append(a)
-        traces.append(a.trace(ct))
+        traces.append(a.trace(rec))
     if "shift" in chips:
         a = ShiftAir(heights["shift"])
         src = ShiftSource(ev.shifts)
@@ -1107,10 +1163,12 @@ def tables_from_events(words, ev, host_tables=False):
         mt = a.trace(*ev.cells)
         airs.append(a)
         traces.append(mt)
-        addr = (ct[:, SEL["ld"]] + ct[:, SEL["sd"]] + ct[:, SEL["keccak"]]) == 1
-        mem = (ct[:, SEL["ld"]] + ct[:, SEL["sd"]]) == 1
-        look += [ct[addr, MW0], np.uint64(8) * ct[addr, MW1], ct[mem, MD0], ct[mem, MD1],
-                 mt[:, MemoryAir.D0], mt[:, MemoryAir.D1]]
+        mem = np.isin(op, [OP_ID["ld"], OP_ID["sd"]])
+        addr = mem | (op == KECCAK_OP)
+        ma = rec[addr, 5]
+        gap = np.nonzero(mem)[0].astype(np.uint64) - rec[mem, 7]   # (row + 1) - mt - 1
+        look += [(ma >> np.uint64(3)) & np.uint64(0xFFFF), np.uint64(8) * (ma >> np.uint64(19)),
+                 gap & np.uint64(0xFFFF), gap >> np.uint64(16), mt[:, MemoryAir.D0], mt[:, MemoryAir.D1]]
     if "keccak" in chips:
         a = KeccakAir(heights["keccak"])
         src = KeccakSource(*ev.keccak)
@@ -1125,8 +1183,7 @@ def tables_from_events(words, ev, host_tables=False):
 
 
 def native_events(words, max_steps=1 << 32):
-    """Events of a run of the library's C++ executor (sg_rv64_run), which
-    writes the CPU table as it runs."""
+    """Events of a run of the library's C++ executor (sg_rv64_run)."""
     import ctypes as C
     from . import native
     L = native.lib()
@@ -1135,15 +1192,17 @@ def native_events(words, max_steps=1 << 32):
     native.check(L.sg_rv64_run(w.ctypes.data, len(w), max_steps, 0, None, None, None, None, None, None,
                                C.byref(info)))
     n = 1 << max(1, (info.cycles - 1).bit_length())
-    ct = np.empty((n, CPU_WIDTH), np.uint64)
+    rec = np.empty((info.cycles, 8), np.uint64)
+    regs = np.empty(((n + REG_CHUNK - 1) // REG_CHUNK, 32), np.uint64)
     counts = np.zeros(len(w), np.uint64)
     shifts = np.empty((info.shifts, 3), np.uint64)
     cells = np.empty((info.cells, 3), np.uint64)
     kc = np.empty((info.keccak_calls, 52), np.uint64)
     ptr = lambda a: a.ctypes.data if a.size else None
-    native.check(L.sg_rv64_run(w.ctypes.data, len(w), max_steps, n, ct.ctypes.data, counts.ctypes.data,
-                               ptr(shifts), ptr(cells), ptr(kc), None, C.byref(info)))
-    return Events(ct, [int(c) for c in counts], info.a0, info.cycles, shifts,
+    native.check(L.sg_rv64_run(w.ctypes.data, len(w), max_steps, n, rec.ctypes.data, regs.ctypes.data,
+                               counts.ctypes.data, ptr(shifts), ptr(cells), ptr(kc), C.byref(info)))
+    chips = tuple(c for i, c in enumerate(CHIPS) if info.chips >> i & 1)
+    return Events(rec, regs, [int(c) for c in counts], info.a0, info.cycles, chips, shifts,
                   (cells[:, 0].copy(), cells[:, 1].copy(), cells[:, 2].copy()),
                   (kc[:, 0].copy(), kc[:, 1].copy(), kc[:, 2:27].copy(), kc[:, 27:52].copy()))
 
@@ -1157,9 +1216,10 @@ def build(words, native_exec=True, host_tables=False):
 
 
 def native_trace(words, max_steps=1 << 32):
-    """(CPU table, counts, a0, cycles) of a run of the native executor."""
+    """(CPU table built on the host, counts, a0, cycles) of a run of the native executor."""
     ev = native_events(words, max_steps)
-    return ev.cpu_trace, ev.counts, ev.output, ev.cycles
+    cpu = CpuAir(words, max(1, (ev.cycles - 1).bit_length()), ev.chips)
+    return cpu.trace(ev.records), ev.counts, ev.output, ev.cycles
 
 
 def prove(words, opts, bk):

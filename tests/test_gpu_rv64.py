@@ -69,10 +69,12 @@ def test_keccak_guest_scheduled_proof_equals_plain(be):
 
 
 def test_device_chip_tables_equal_the_host_tables(be):
-    """sg_rv64_keccak_table and sg_rv64_shift_table (tables written on the
-    device from the run's events) against the numpy builders, cell for cell:
-    the Keccak guest's own events, then random lanes and timestamps and every
-    shift amount in both directions, with padding rows."""
+    """sg_rv64_cpu_table, sg_rv64_keccak_table and sg_rv64_shift_table
+    (tables written on the device from the run's events) against the numpy
+    builders, cell for cell: the Keccak guest (full CPU width), the Fibonacci
+    guest (core width), a branch on low limbs 2^32 - 1 and 0, then random
+    lanes and timestamps and every shift amount in both directions, with
+    padding rows."""
     import numpy as np
     bk = GpuBackend(be)
 
@@ -82,16 +84,19 @@ def test_device_chip_tables_equal_the_host_tables(be):
         bk.free(m)
         assert np.array_equal(got, host)
 
-    words = rv64.keccak_program(136 * 11)
-    ev = RA.native_events(words)
-    airs, srcs, _ = RA.tables_from_events(words, ev)
-    _, host, _ = RA.tables_from_events(words, ev, host_tables=True)
-    checked = 0
-    for air, s, h in zip(airs, srcs, host):
-        if hasattr(s, "device_trace"):
-            same(s, air, h)
-            checked += 1
-    assert checked == 2
+    wrap = rv64.assemble([("li", "t0", -1), ("srli", "t0", "t0", 32), ("li", "t1", 0),
+                          ("beq", "t0", "t1", "end"), ("bne", "t0", "t1", "end"), ("li", "t1", 5),
+                          "end:", ("li", "a7", 93), ("ecall",)])
+    for words, expect in ((rv64.keccak_program(136 * 11), 3), (rv64.fib_program(3000), 1), (wrap, 2)):
+        ev = RA.native_events(words)
+        airs, srcs, _ = RA.tables_from_events(words, ev)
+        _, host, _ = RA.tables_from_events(words, ev, host_tables=True)
+        checked = 0
+        for air, s, h in zip(airs, srcs, host):
+            if hasattr(s, "device_trace"):
+                same(s, air, h)
+                checked += 1
+        assert checked == expect
     rng = np.random.default_rng(3)
     P_ = 7
     lanes = rng.integers(0, 2**64, size=(P_, 25), dtype=np.uint64)

@@ -94,18 +94,33 @@ def test_executor_errors():
             RA.native_events(w)
 
 
-@pytest.mark.parametrize("prog", ["fib7", "fib2047", "fib5000", "keccak1", "keccak9"])
-def test_native_events_equal_the_python_tables(prog):
-    """sg_rv64_run (the library's C++ executor and CPU-table writer) against
-    the Python executor and table builder: the CPU table cell for cell, the
-    counts, the output and every chip event."""
-    words = rv64.fib_program(int(prog[3:])) if prog.startswith("fib") else rv64.keccak_program(136 * int(prog[6:]))
+@pytest.mark.parametrize("prog", ["fib7", "fib2047", "fib5000", "keccak1", "keccak9", "wrap"])
+def test_native_events_equal_the_python_events(prog):
+    """sg_rv64_run (the library's C++ executor) against the Python executor:
+    row records, register snapshots, counts, output, chips and every chip
+    event; and the CPU table built from them. "wrap": a branch whose operands'
+    low limbs are 2^32 - 1 and 0, the corner of the limb differences."""
+    if prog == "wrap":
+        words = rv64.assemble([("li", "t0", -1), ("srli", "t0", "t0", 32), ("li", "t1", 0),
+                               ("beq", "t0", "t1", "end"), ("bne", "t0", "t1", "end"), ("li", "t1", 5),
+                               "end:", ("li", "a7", 93), ("ecall",)])
+    elif prog.startswith("fib"):
+        words = rv64.fib_program(int(prog[3:]))
+    else:
+        words = rv64.keccak_program(136 * int(prog[6:]))
     pe, ne = RA.python_events(words), RA.native_events(words)
-    assert np.array_equal(pe.cpu_trace, ne.cpu_trace)
-    assert (pe.counts, pe.output, pe.cycles) == (ne.counts, ne.output, ne.cycles)
+    assert np.array_equal(pe.records, ne.records)
+    assert np.array_equal(pe.regs, ne.regs)
+    assert (pe.counts, pe.output, pe.cycles, pe.chips) == (ne.counts, ne.output, ne.cycles, ne.chips)
     assert np.array_equal(pe.shifts, ne.shifts)
     for a, b in zip(pe.cells + pe.keccak, ne.cells + ne.keccak):
         assert np.array_equal(a, b)
+    airs, traces, pub = RA.tables_from_events(words, ne, host_tables=True)
+    if prog == "wrap":
+        bad, total = _check(airs, traces, pub)
+        assert not any(bad.values()) and total == (0, 0, 0)
+    else:
+        assert airs[0].width == (RA.CPU_CORE_WIDTH if prog.startswith("fib") else RA.CPU_WIDTH)
 
 
 def _aux_and_apows(airs, z, alpha):
@@ -160,7 +175,7 @@ def _tampered(airs, traces, pub, table, fn, terms=None):
 
 
 def test_tampering_breaks_a_constraint_or_the_balance():
-    airs, traces, pub = RA.build(rv64.fib_program(6))
+    airs, traces, pub = RA.build(rv64.fib_program(6), host_tables=True)
     ct = traces[0]
 
     def reg(t):  # a register value changed mid-run
