@@ -51,6 +51,8 @@ def parse():
                          "executed and its execution proved")
     ap.add_argument("--fib-n", type=int, default=30000, help="vm: Fibonacci loop iterations (5 cycles each)")
     ap.add_argument("--guest", default="fib", choices=["fib", "keccak"], help="vm: which guest")
+    ap.add_argument("--vm-steps", type=int, default=3, help="vm: timed proofs per form")
+    ap.add_argument("--vm-warmup", type=int, default=1, help="vm: untimed proofs per form first")
     ap.add_argument("--keccak-bytes", type=int, default=136 * 7710,
                     help="vm: the Keccak guest's buffer (a multiple of 136; default 1048560, about 1 MiB)")
     ap.add_argument("--rates", default="2,5,10,20,50,100", help="serve: arrival rates (jobs/s)")
@@ -543,8 +545,8 @@ def measure_vm(a, guest="fib", steps=3, warmup=1):
 
 
 def run_vm(a):
-    line = measure_vm(a, a.guest)
-    line.update({"n_gpus": 1, "steps": 3, "warmup": 1, "higher_is_better": True, "scaling": "weak",
+    line = measure_vm(a, a.guest, a.vm_steps, a.vm_warmup)
+    line.update({"n_gpus": 1, "steps": a.vm_steps, "warmup": a.vm_warmup, "higher_is_better": True, "scaling": "weak",
                  "vs_baseline": None, "dtype": "u64 (Goldilocks) / Fp3", "data": "generated RV64 guest"})
     print(json.dumps(line), flush=True)
 
