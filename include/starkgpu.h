@@ -347,7 +347,13 @@ SG_API int sg_logup_aux(sg_ctx* ctx, void* stream, const uint64_t* d_main, uint6
 
 /* Lowered constraint program (DeviceProgram, crypto/stark/src/constraint_ir/device.rs):
  * nodes are {op, a, b, res} u32 quadruples with the reference's OP_* tags,
- * operand encoding (kind << 29 | payload) and RES_EXT_BIT slot packing. */
+ * operand encoding (kind << 29 | payload) and RES_EXT_BIT slot packing.
+ * node_roots NULL: the reference's shape (each constraint's value pinned in
+ * the slot `roots` names until the walk ends). node_roots set (num_nodes
+ * entries): a streaming program, as lambda_vm_b200/ir.py lowers by default —
+ * node_roots[i] is the constraint instruction i completes (0xFFFFFFFF: none;
+ * each constraint exactly once; `roots` unused), and operands may also be
+ * trace reads, kind 7 with payload aux << 28 | frame offset << 20 | column. */
 typedef struct {
     const uint32_t* nodes;
     uint32_t num_nodes;
@@ -359,6 +365,7 @@ typedef struct {
     uint32_t num_roots;
     uint32_t num_base_slots;
     uint32_t num_ext_slots;
+    const uint32_t* node_roots; /* NULL, or num_nodes entries (streaming program) */
 } sg_device_program;
 
 /* Composition accumulation (CompositionAccum, crypto/math-cuda/src/constraint_interp.rs:157). */

@@ -17,6 +17,15 @@
 // laid out slot-major so a warp's accesses to one slot are consecutive.
 // The reference keeps these slots in global memory, where their traffic
 // dominates the walk. Trace reads come from the row-major resident LDEs.
+//
+// Streaming programs (lambda_vm_b200/ir.py lower(stream=True), node_roots
+// set): trace values are OPK_VAR operands read where they are used instead of
+// OP_VAR nodes holding a slot each, and every instruction that completes a
+// constraint folds it into the row's composition sum (or writes it, in the
+// per-constraint mode) at once, so no constraint holds a slot to the end of
+// the walk. The slot file then holds only intermediates: a 2605-column AIR
+// with 3434 constraints needs 101 words a row instead of 5719, which fits
+// shared memory.
 #include <vector>
 
 #include "common.cuh"
@@ -46,8 +55,13 @@ using gl::fe3;
 #define OPK_RAP 4u
 #define OPK_ALPHA 5u
 #define OPK_OFFSET 6u
+#define OPK_VAR 7u
+#define VAR_AUX_BIT (1u << 28)
+#define VAR_OFF_SHIFT 20u
+#define VAR_COL_MASK 0xFFFFFu
 #define RES_EXT_BIT 0x80000000u
 #define RES_SLOT_MASK 0x7FFFFFFFu
+#define NO_ROOT 0xFFFFFFFFu
 
 struct Uni {
     const uint64_t* base_consts;
@@ -75,27 +89,6 @@ struct SlotFile {
     }
 };
 
-__device__ __forceinline__ bool is_base_kind(uint32_t enc) {
-    const uint32_t k = enc >> OPK_SHIFT;
-    return k == OPK_BASE_SLOT || k == OPK_BASE_CONST;
-}
-__device__ __forceinline__ uint64_t base_op(uint32_t enc, const SlotFile& f, const Uni& u) {
-    const uint32_t p = enc & OPK_PAYLOAD_MASK;
-    return (enc >> OPK_SHIFT) == OPK_BASE_SLOT ? f.gb(p) : __ldg(u.base_consts + p);
-}
-__device__ __forceinline__ fe3 ext_op(uint32_t enc, const SlotFile& f, const Uni& u) {
-    const uint32_t p = enc & OPK_PAYLOAD_MASK;
-    switch (enc >> OPK_SHIFT) {
-        case OPK_BASE_SLOT: return fe3{f.gb(p), 0, 0};
-        case OPK_EXT_SLOT: return f.ge(p);
-        case OPK_BASE_CONST: return fe3{__ldg(u.base_consts + p), 0, 0};
-        case OPK_EXT_CONST: return fe3{__ldg(u.ext_consts + 3 * p), __ldg(u.ext_consts + 3 * p + 1), __ldg(u.ext_consts + 3 * p + 2)};
-        case OPK_RAP: return fe3{__ldg(u.rap + 3 * p), __ldg(u.rap + 3 * p + 1), __ldg(u.rap + 3 * p + 2)};
-        case OPK_ALPHA: return fe3{__ldg(u.alpha + 3 * p), __ldg(u.alpha + 3 * p + 1), __ldg(u.alpha + 3 * p + 2)};
-        default: return u.offset;
-    }
-}
-
 struct Trace {
     const uint64_t* main;
     uint64_t m;
@@ -105,8 +98,54 @@ struct Trace {
     uint64_t next_step;
 };
 
+__device__ __forceinline__ bool is_base_kind(uint32_t enc) {
+    const uint32_t k = enc >> OPK_SHIFT;
+    return k == OPK_BASE_SLOT || k == OPK_BASE_CONST || (k == OPK_VAR && !(enc & VAR_AUX_BIT));
+}
+// frame row of an OPK_VAR operand
+__device__ __forceinline__ uint64_t var_row(uint32_t p, const Trace& t, uint64_t row) {
+    uint64_t r = row + (uint64_t)((p >> VAR_OFF_SHIFT) & 0xFFu) * t.next_step;
+    return r >= t.rows ? r - t.rows : r;
+}
+__device__ __forceinline__ uint64_t base_op(uint32_t enc, const SlotFile& f, const Uni& u, const Trace& t,
+                                            uint64_t row) {
+    const uint32_t p = enc & OPK_PAYLOAD_MASK;
+    switch (enc >> OPK_SHIFT) {
+        case OPK_BASE_SLOT: return f.gb(p);
+        case OPK_VAR: return t.main[var_row(p, t, row) * t.m + (p & VAR_COL_MASK)];
+        default: return __ldg(u.base_consts + p);
+    }
+}
+__device__ __forceinline__ fe3 ext_op(uint32_t enc, const SlotFile& f, const Uni& u, const Trace& t, uint64_t row) {
+    const uint32_t p = enc & OPK_PAYLOAD_MASK;
+    switch (enc >> OPK_SHIFT) {
+        case OPK_BASE_SLOT: return fe3{f.gb(p), 0, 0};
+        case OPK_EXT_SLOT: return f.ge(p);
+        case OPK_BASE_CONST: return fe3{__ldg(u.base_consts + p), 0, 0};
+        case OPK_EXT_CONST: return fe3{__ldg(u.ext_consts + 3 * p), __ldg(u.ext_consts + 3 * p + 1), __ldg(u.ext_consts + 3 * p + 2)};
+        case OPK_RAP: return fe3{__ldg(u.rap + 3 * p), __ldg(u.rap + 3 * p + 1), __ldg(u.rap + 3 * p + 2)};
+        case OPK_ALPHA: return fe3{__ldg(u.alpha + 3 * p), __ldg(u.alpha + 3 * p + 1), __ldg(u.alpha + 3 * p + 2)};
+        case OPK_VAR: {
+            const uint64_t r = var_row(p, t, row);
+            if (!(p & VAR_AUX_BIT)) return fe3{t.main[r * t.m + (p & VAR_COL_MASK)], 0, 0};
+            const uint64_t* q = t.aux + (r * t.A + (p & VAR_COL_MASK)) * 3;
+            return fe3{q[0], q[1], q[2]};
+        }
+        default: return u.offset;
+    }
+}
+
+// Where a streaming walk puts each completed constraint: mode 0 folds
+// beta_c * C_c into *sum; mode 1 writes C_c to out[c * rows + row].
+struct Sink {
+    const uint32_t* node_roots;  // null: roots pinned, combined after the walk
+    const uint64_t* beta;
+    int mode;
+    uint64_t* out;
+};
+
 __device__ __forceinline__ void walk(const uint4* nodes, uint32_t num_nodes, const Uni& u, const SlotFile& f,
-                                     const Trace& t, uint64_t row) {
+                                     const Trace& t, uint64_t row, const Sink& sk, fe3* sum) {
     for (uint32_t i = 0; i < num_nodes; ++i) {
         const uint4 nd = __ldg(nodes + i);
         const uint32_t slot = nd.w & RES_SLOT_MASK;
@@ -127,55 +166,70 @@ __device__ __forceinline__ void walk(const uint4* nodes, uint32_t num_nodes, con
             }
             case OP_ADD:
                 if (!rx)
-                    f.pb(slot, gl::add(base_op(nd.y, f, u), base_op(nd.z, f, u)));
+                    f.pb(slot, gl::add(base_op(nd.y, f, u, t, row), base_op(nd.z, f, u, t, row)));
                 else if (is_base_kind(nd.y)) {
-                    const uint64_t x = base_op(nd.y, f, u);
-                    const fe3 y = ext_op(nd.z, f, u);
+                    const uint64_t x = base_op(nd.y, f, u, t, row);
+                    const fe3 y = ext_op(nd.z, f, u, t, row);
                     f.pe(slot, fe3{gl::add(x, y.c0), y.c1, y.c2});
                 } else if (is_base_kind(nd.z)) {
-                    const fe3 x = ext_op(nd.y, f, u);
-                    f.pe(slot, fe3{gl::add(x.c0, base_op(nd.z, f, u)), x.c1, x.c2});
+                    const fe3 x = ext_op(nd.y, f, u, t, row);
+                    f.pe(slot, fe3{gl::add(x.c0, base_op(nd.z, f, u, t, row)), x.c1, x.c2});
                 } else
-                    f.pe(slot, gl::add3(ext_op(nd.y, f, u), ext_op(nd.z, f, u)));
+                    f.pe(slot, gl::add3(ext_op(nd.y, f, u, t, row), ext_op(nd.z, f, u, t, row)));
                 break;
             case OP_SUB:
                 if (!rx)
-                    f.pb(slot, gl::sub(base_op(nd.y, f, u), base_op(nd.z, f, u)));
+                    f.pb(slot, gl::sub(base_op(nd.y, f, u, t, row), base_op(nd.z, f, u, t, row)));
                 else if (is_base_kind(nd.y)) {
-                    const uint64_t x = base_op(nd.y, f, u);
-                    const fe3 y = ext_op(nd.z, f, u);
+                    const uint64_t x = base_op(nd.y, f, u, t, row);
+                    const fe3 y = ext_op(nd.z, f, u, t, row);
                     f.pe(slot, fe3{gl::sub(x, y.c0), gl::sub(0, y.c1), gl::sub(0, y.c2)});
                 } else if (is_base_kind(nd.z)) {
-                    const fe3 x = ext_op(nd.y, f, u);
-                    f.pe(slot, fe3{gl::sub(x.c0, base_op(nd.z, f, u)), x.c1, x.c2});
+                    const fe3 x = ext_op(nd.y, f, u, t, row);
+                    f.pe(slot, fe3{gl::sub(x.c0, base_op(nd.z, f, u, t, row)), x.c1, x.c2});
                 } else
-                    f.pe(slot, gl::sub3(ext_op(nd.y, f, u), ext_op(nd.z, f, u)));
+                    f.pe(slot, gl::sub3(ext_op(nd.y, f, u, t, row), ext_op(nd.z, f, u, t, row)));
                 break;
             case OP_MUL:
                 if (!rx)
-                    f.pb(slot, gl::mul(base_op(nd.y, f, u), base_op(nd.z, f, u)));
+                    f.pb(slot, gl::mul(base_op(nd.y, f, u, t, row), base_op(nd.z, f, u, t, row)));
                 else if (is_base_kind(nd.y))
-                    f.pe(slot, gl::mulb3(ext_op(nd.z, f, u), base_op(nd.y, f, u)));
+                    f.pe(slot, gl::mulb3(ext_op(nd.z, f, u, t, row), base_op(nd.y, f, u, t, row)));
                 else if (is_base_kind(nd.z))
-                    f.pe(slot, gl::mulb3(ext_op(nd.y, f, u), base_op(nd.z, f, u)));
+                    f.pe(slot, gl::mulb3(ext_op(nd.y, f, u, t, row), base_op(nd.z, f, u, t, row)));
                 else
-                    f.pe(slot, gl::mul3(ext_op(nd.y, f, u), ext_op(nd.z, f, u)));
+                    f.pe(slot, gl::mul3(ext_op(nd.y, f, u, t, row), ext_op(nd.z, f, u, t, row)));
                 break;
             case OP_NEG:
                 if (!rx)
-                    f.pb(slot, gl::neg(base_op(nd.y, f, u)));
+                    f.pb(slot, gl::neg(base_op(nd.y, f, u, t, row)));
                 else {
-                    const fe3 x = ext_op(nd.y, f, u);
+                    const fe3 x = ext_op(nd.y, f, u, t, row);
                     f.pe(slot, fe3{gl::neg(x.c0), gl::neg(x.c1), gl::neg(x.c2)});
                 }
                 break;
-            case OP_EMBED: f.pe(slot, ext_op(nd.y, f, u)); break;
+            case OP_EMBED: f.pe(slot, ext_op(nd.y, f, u, t, row)); break;
             case OP_CONST_BASE: f.pb(slot, __ldg(u.base_consts + nd.y)); break;
-            case OP_CONST_EXT: f.pe(slot, ext_op((OPK_EXT_CONST << OPK_SHIFT) | nd.y, f, u)); break;
-            case OP_RAP_CHALLENGE: f.pe(slot, ext_op((OPK_RAP << OPK_SHIFT) | nd.y, f, u)); break;
-            case OP_ALPHA_POW: f.pe(slot, ext_op((OPK_ALPHA << OPK_SHIFT) | nd.y, f, u)); break;
+            case OP_CONST_EXT: f.pe(slot, ext_op((OPK_EXT_CONST << OPK_SHIFT) | nd.y, f, u, t, row)); break;
+            case OP_RAP_CHALLENGE: f.pe(slot, ext_op((OPK_RAP << OPK_SHIFT) | nd.y, f, u, t, row)); break;
+            case OP_ALPHA_POW: f.pe(slot, ext_op((OPK_ALPHA << OPK_SHIFT) | nd.y, f, u, t, row)); break;
             case OP_TABLE_OFFSET: f.pe(slot, u.offset); break;
             default: break;
+        }
+        if (sk.node_roots) {
+            const uint32_t c = __ldg(sk.node_roots + i);
+            if (c != NO_ROOT) {
+                if (sk.mode == 1) {
+                    const fe3 v = gl::canon3(rx ? f.ge(slot) : fe3{f.gb(slot), 0, 0});
+                    uint64_t* o = sk.out + 3 * ((uint64_t)c * t.rows + row);
+                    o[0] = v.c0;
+                    o[1] = v.c1;
+                    o[2] = v.c2;
+                } else {
+                    const fe3 b{__ldg(sk.beta + 3 * c), __ldg(sk.beta + 3 * c + 1), __ldg(sk.beta + 3 * c + 2)};
+                    *sum = gl::add3(*sum, rx ? gl::mul3(b, f.ge(slot)) : gl::mulb3(b, f.gb(slot)));
+                }
+            }
         }
     }
 }
@@ -199,8 +253,8 @@ struct Comp {
 
 // mode 0: composition H(row); mode 1: per-constraint matrix evals[c*rows + row].
 __global__ void k_constraints(const uint4* nodes, uint32_t num_nodes, const uint32_t* roots, uint32_t num_roots,
-                              uint32_t nbs, uint32_t nes, Uni u, Trace t, Comp cp, int mode, uint64_t* out,
-                              uint64_t* gscratch) {
+                              const uint32_t* node_roots, uint32_t nbs, uint32_t nes, Uni u, Trace t, Comp cp,
+                              int mode, uint64_t* out, uint64_t* gscratch) {
     extern __shared__ uint64_t shs[];
     const uint64_t T = blockDim.x;
     SlotFile f;
@@ -217,7 +271,9 @@ __global__ void k_constraints(const uint4* nodes, uint32_t num_nodes, const uint
     }
     for (uint64_t row = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; row < t.rows;
          row += (uint64_t)gridDim.x * blockDim.x) {
-        walk(nodes, num_nodes, u, f, t, row);
+        fe3 sum{0, 0, 0};
+        walk(nodes, num_nodes, u, f, t, row, Sink{node_roots, cp.beta, mode, out}, &sum);
+        if (node_roots && mode == 1) continue;
         if (mode == 1) {
             for (uint32_t c = 0; c < num_roots; ++c) {
                 const fe3 v = gl::canon3(root_val(roots[c], f));
@@ -228,8 +284,7 @@ __global__ void k_constraints(const uint4* nodes, uint32_t num_nodes, const uint
             }
             continue;
         }
-        fe3 sum{0, 0, 0};
-        for (uint32_t c = 0; c < num_roots; ++c) {
+        for (uint32_t c = 0; node_roots == nullptr && c < num_roots; ++c) {
             const uint32_t enc = roots[c];
             const fe3 b{__ldg(cp.beta + 3 * c), __ldg(cp.beta + 3 * c + 1), __ldg(cp.beta + 3 * c + 2)};
             if (enc & RES_EXT_BIT)
@@ -312,6 +367,9 @@ int sg_eval_constraints(sg_ctx* c, void* stream, const sg_device_program* prog, 
                 case OPK_RAP: return p < n_rap;
                 case OPK_ALPHA: return p < n_alpha;
                 case OPK_OFFSET: return true;
+                case OPK_VAR:
+                    return ((p & VAR_AUX_BIT) ? (p & VAR_COL_MASK) < a : (p & VAR_COL_MASK) < m) &&
+                           (uint64_t)((p >> VAR_OFF_SHIFT) & 0xFFu) * next_step < rows && !(p & ~(VAR_AUX_BIT | (0xFFu << VAR_OFF_SHIFT) | VAR_COL_MASK));
                 default: return false;
             }
         };
@@ -328,9 +386,21 @@ int sg_eval_constraints(sg_ctx* c, void* stream, const sg_device_program* prog, 
         if (op == OP_RAP_CHALLENGE) SG_CHECK_ARG(nd[1] < n_rap, "challenge index");
         if (op == OP_ALPHA_POW) SG_CHECK_ARG(nd[1] < n_alpha, "alpha index");
     }
-    for (uint32_t r = 0; r < nr; ++r) {
-        const uint32_t e = prog->roots[r];
-        SG_CHECK_ARG((e & RES_EXT_BIT) ? (e & RES_SLOT_MASK) < nes : (e & RES_SLOT_MASK) < nbs, "root slot");
+    if (prog->node_roots) {
+        // streaming: every constraint completed by exactly one instruction
+        std::vector<uint8_t> seen(nr, 0);
+        for (uint32_t i = 0; i < nn; ++i) {
+            const uint32_t c = prog->node_roots[i];
+            if (c == NO_ROOT) continue;
+            SG_CHECK_ARG(c < nr && !seen[c], "node_roots: constraint index out of range or repeated");
+            seen[c] = 1;
+        }
+        for (uint32_t c = 0; c < nr; ++c) SG_CHECK_ARG(seen[c], "node_roots: a constraint no instruction completes");
+    } else {
+        for (uint32_t r = 0; r < nr; ++r) {
+            const uint32_t e = prog->roots[r];
+            SG_CHECK_ARG((e & RES_EXT_BIT) ? (e & RES_SLOT_MASK) < nes : (e & RES_SLOT_MASK) < nbs, "root slot");
+        }
     }
     if (comp) {
         SG_CHECK_ARG(comp->z_len >= 1 && comp->d_z_inv && comp->beta_trans, "composition inputs");
@@ -347,6 +417,7 @@ int sg_eval_constraints(sg_ctx* c, void* stream, const sg_device_program* prog, 
     };
     const size_t o_nodes = put(prog->nodes, 16ull * nn);
     const size_t o_roots = put(prog->roots, 4ull * nr);
+    const size_t o_nroots = prog->node_roots ? put(prog->node_roots, 4ull * nn) : 0;
     const size_t o_bc = put(prog->base_consts, 8ull * prog->num_base_consts);
     const size_t o_ec = put(prog->ext_consts, 24ull * prog->num_ext_consts);
     const size_t o_rap = put(rap, 24ull * n_rap);
@@ -393,9 +464,10 @@ int sg_eval_constraints(sg_ctx* c, void* stream, const sg_device_program* prog, 
         }
         const size_t smem = use_smem ? per_thread * T * 8 : 0;
         if (smem > 48 * 1024) cudaFuncSetAttribute(k_constraints, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        const uint32_t* d_nroots = prog->node_roots ? (const uint32_t*)(d_blob + o_nroots) : nullptr;
         k_constraints<<<(unsigned)blocks, T, smem, st>>>((const uint4*)(d_blob + o_nodes), nn,
-                                                         (const uint32_t*)(d_blob + o_roots), nr, nbs, nes, u, t, cp,
-                                                         comp ? 0 : 1, d_out, use_smem ? nullptr : d_scr);
+                                                         (const uint32_t*)(d_blob + o_roots), nr, d_nroots, nbs, nes,
+                                                         u, t, cp, comp ? 0 : 1, d_out, use_smem ? nullptr : d_scr);
         rc = check_launch(ctx, "k_constraints");
         if (rc == SG_OK && cudaStreamSynchronize(st) != cudaSuccess) {
             set_error("constraints: execution failed");

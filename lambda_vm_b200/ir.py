@@ -95,10 +95,30 @@ def _uniform(node):
     return node[0] in ("cb", "ce", "rap", "alpha", "off")
 
 
-def lower(prog):
-    """DeviceProgram::lower (constraint_ir/device.rs:160-330)."""
+OPK_VAR = 7                    # trace operand: payload = aux << 28 | frame offset << 20 | column
+VAR_AUX_BIT, VAR_OFF_SHIFT, VAR_COL_MASK = 1 << 28, 20, (1 << 20) - 1
+NO_ROOT = 0xFFFFFFFF
+
+
+def lower(prog, stream=True):
+    """DeviceProgram::lower (constraint_ir/device.rs:160-330).
+
+    stream=False gives the reference's program shape: every trace read is an
+    OP_VAR node with a slot of its own and every constraint's value stays
+    pinned in its slot until the walk ends, when the roots are combined. That
+    costs a slot for every constraint and every live trace value: a wide AIR
+    (thousands of constraints) needs thousands of slots per row.
+
+    stream=True (the default) lowers for the streaming walker: trace reads
+    become OPK_VAR operands read where they are used, and `node_roots` names
+    the constraint each instruction completes (NO_ROOT otherwise), so the
+    kernel folds the constraint into the composition as soon as it is computed
+    and its slot is free for reuse; a node that several constraints share gets
+    one extra copy instruction per further constraint. Only intermediate
+    values occupy slots, so the slot file stays small whatever the width."""
     nodes, dims, roots = prog["nodes"], prog["dims"], prog["roots"]
     n = len(nodes)
+    base_consts = list(prog["base_consts"])
     used = [False] * n
     last = [0] * n
     for i, nd in enumerate(nodes):
@@ -106,13 +126,24 @@ def lower(prog):
             used[o] = True
             last[o] = i
     is_root = [False] * n
-    for r in roots:
+    root_ids = [[] for _ in range(n)]
+    for c, r in enumerate(roots):
         is_root[r] = True
         used[r] = True
-    emitted = [used[i] and (not _uniform(nodes[i]) or is_root[i]) for i in range(n)]
+        root_ids[r].append(c)
+    leaf = [_uniform(nodes[i]) or (stream and nodes[i][0] == "var") for i in range(n)]
+    emitted = [used[i] and (not leaf[i] or is_root[i]) for i in range(n)]
+    if stream:
+        if 0 not in base_consts:
+            base_consts.append(0)
+        zero_enc = (OPK_BASE_CONST << OPK_SHIFT) | base_consts.index(0)
 
-    def enc_uniform(nd):
+    def enc_leaf(nd):
         k = nd[0]
+        if k == "var":
+            _, is_main, off, col = nd
+            assert off < 256 and col <= VAR_COL_MASK
+            return (OPK_VAR << OPK_SHIFT) | (0 if is_main else VAR_AUX_BIT) | (off << VAR_OFF_SHIFT) | col
         if k == "cb":
             return (OPK_BASE_CONST << OPK_SHIFT) | nd[1]
         if k == "ce":
@@ -126,18 +157,24 @@ def lower(prog):
     slot_of = [None] * n
     free = {BASE: [], EXT: []}
     count = {BASE: 0, EXT: 0}
-    out = []
+    out, node_roots = [], []
+
+    def take(d):
+        s_ = free[d].pop() if free[d] else count[d]
+        if s_ == count[d]:
+            count[d] += 1
+        return s_
+
+    def enc(j):
+        if not emitted[j]:
+            return enc_leaf(nodes[j])
+        kind = OPK_BASE_SLOT if dims[j] == BASE else OPK_EXT_SLOT
+        return (kind << OPK_SHIFT) | slot_of[j]
+
     for i in range(n):
         if not emitted[i]:
             continue
         nd = nodes[i]
-
-        def enc(j):
-            if not emitted[j]:
-                return enc_uniform(nodes[j])
-            kind = OPK_BASE_SLOT if dims[j] == BASE else OPK_EXT_SLOT
-            return (kind << OPK_SHIFT) | slot_of[j]
-
         k = nd[0]
         if k == "cb":
             t = (OP_CONST_BASE, nd[1], 0)
@@ -158,18 +195,43 @@ def lower(prog):
             t = (OP_NEG, enc(nd[1]), 0)
         else:
             t = (OP_EMBED, enc(nd[1]), 0)
+        pinned = (lambda o: is_root[o]) if not stream else (lambda o: False)
         for o in _operands(nd):
-            if emitted[o] and not is_root[o] and last[o] == i and slot_of[o] is not None:
+            if emitted[o] and not pinned(o) and last[o] == i and slot_of[o] is not None:
                 free[dims[o]].append(slot_of[o])
                 slot_of[o] = None
         d = dims[i]
-        s = free[d].pop() if free[d] else count[d]
-        if s == count[d]:
-            count[d] += 1
-        slot_of[i] = s
-        out.append((t[0], t[1], t[2], s | (RES_EXT_BIT if d == EXT else 0)))
-    root_enc = [slot_of[r] | (RES_EXT_BIT if dims[r] == EXT else 0) for r in roots]
-    return {"nodes": np.array(out, np.uint32).reshape(-1, 4), "roots": np.array(root_enc, np.uint32),
-            "base_consts": np.array(prog["base_consts"], np.uint64),
-            "ext_consts": np.array(prog["ext_consts"], np.uint64).reshape(-1, 3),
-            "num_base_slots": count[BASE], "num_ext_slots": count[EXT]}
+        slot_of[i] = take(d)
+        ext = RES_EXT_BIT if d == EXT else 0
+        out.append((t[0], t[1], t[2], slot_of[i] | ext))
+        if stream:
+            ids = root_ids[i]
+            node_roots.append(ids[0] if ids else NO_ROOT)
+            for c in ids[1:]:  # a node several constraints share: one copy per further constraint
+                sc = take(d)
+                out.append((OP_ADD, enc(i), zero_enc, sc | ext))
+                node_roots.append(c)
+                free[d].append(sc)
+            if not last[i] > i:  # no later use: the slot is free again
+                free[d].append(slot_of[i])
+                slot_of[i] = None
+    if stream:
+        root_enc = [0] * len(roots)
+    else:
+        root_enc = [slot_of[r] | (RES_EXT_BIT if dims[r] == EXT else 0) for r in roots]
+    low = {"nodes": np.array(out, np.uint32).reshape(-1, 4), "roots": np.array(root_enc, np.uint32),
+           "base_consts": np.array(base_consts, np.uint64),
+           "ext_consts": np.array(prog["ext_consts"], np.uint64).reshape(-1, 3),
+           "num_base_slots": count[BASE], "num_ext_slots": count[EXT]}
+    if stream:
+        low["node_roots"] = np.array(node_roots, np.uint32)
+    return low
+
+
+def lowered(prog):
+    """lower(prog), computed once per program (kept in the program dict: a
+    table's program does not change, and a wide AIR takes a while to lower)."""
+    low = prog.get("_lowered")
+    if low is None:
+        low = prog["_lowered"] = lower(prog)
+    return low

@@ -464,6 +464,7 @@ def _program_struct(lowered, keep):
     p.num_roots = int(np.asarray(lowered["roots"]).size)
     p.num_base_slots = int(lowered["num_base_slots"])
     p.num_ext_slots = int(lowered["num_ext_slots"])
+    p.node_roots = arr(lowered["node_roots"], np.uint32) if lowered.get("node_roots") is not None else None
     return p
 
 

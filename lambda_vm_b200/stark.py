@@ -32,7 +32,7 @@ from . import field as F
 from . import math_cuda as mc
 from . import native
 from .device import DeviceBuffer, backend as _backend
-from .ir import lower
+from .ir import lowered
 
 P = F.P
 
@@ -721,8 +721,7 @@ def multi_prove(airs, traces, opts=None, bk=None, label=b"lambda_vm_b200/synthet
         forks.append(ti)
     proofs = []
     for i, (air, tm, lde, tree, root) in enumerate(tabs):
-        lowered = lower(air.program)
-        p = prove_table(bk, air, lowered, tm, lde, tree, forks[i], challenges, alpha_pows, opts)
+        p = prove_table(bk, air, lowered(air.program), tm, lde, tree, forks[i], challenges, alpha_pows, opts)
         p["main_root"] = root
         proofs.append(p)
         bk.free(tm, lde, tree)

@@ -22,13 +22,19 @@ def rf(rng, shape):
     return np.where(x >= np.uint64(P), x - np.uint64(P), x)
 
 
+@pytest.mark.parametrize("stream", [True, False])
 @pytest.mark.parametrize("seed,rows,m,a,nodes,roots,next_step", [
     (1, 16, 4, 0, 30, 3, 1), (2, 64, 6, 2, 60, 5, 2), (3, 128, 10, 3, 120, 8, 4), (4, 32, 3, 1, 200, 12, 1),
     (5, 256, 8, 2, 80, 6, 2)])
-def test_constraint_matrix_matches_ir(be, seed, rows, m, a, nodes, roots, next_step):
+def test_constraint_matrix_matches_ir(be, seed, rows, m, a, nodes, roots, next_step, stream):
+    """Both program shapes: streaming (trace operands, constraints folded as
+    completed; the library's lowering) and the reference's pinned roots."""
     rng = np.random.default_rng(seed)
     prog = random_program(rng, m, a, 2, 3, n_nodes=nodes, n_roots=roots)
-    low = lower(prog)
+    if seed == 4:
+        prog["roots"] = prog["roots"] + prog["roots"][:3]  # constraints that share a node
+        prog["roots"].sort(key=lambda r: prog["dims"][r])
+    low = lower(prog, stream)
     main = rf(rng, (rows, m))
     aux = rf(rng, (rows, 3 * a)) if a else np.zeros((rows, 0), np.uint64)
     rap, alpha, off = rf(rng, (2, 3)), rf(rng, (3, 3)), rf(rng, (3,))
@@ -37,12 +43,13 @@ def test_constraint_matrix_matches_ir(be, seed, rows, m, a, nodes, roots, next_s
     assert (got.transpose(1, 0, 2) == want).all()
 
 
+@pytest.mark.parametrize("stream", [True, False])
 @pytest.mark.parametrize("seed,rows,nb", [(7, 64, 0), (8, 128, 3), (9, 256, 2)])
-def test_composition_matches_evaluator(be, seed, rows, nb):
+def test_composition_matches_evaluator(be, seed, rows, nb, stream):
     rng = np.random.default_rng(seed)
     m, a = 6, 2
     prog = random_program(rng, m, a, 2, 3, n_nodes=70, n_roots=6)
-    low = lower(prog)
+    low = lower(prog, stream)
     main = rf(rng, (rows, m))
     aux = rf(rng, (rows, 3 * a))
     rap, alpha, off = rf(rng, (2, 3)), rf(rng, (3, 3)), rf(rng, (3,))
@@ -60,12 +67,28 @@ def test_composition_matches_evaluator(be, seed, rows, nb):
 def test_program_validation_rejects_bad_slots(be):
     rng = np.random.default_rng(11)
     prog = random_program(rng, 4, 0, 1, 1, n_nodes=20, n_roots=2)
-    low = lower(prog)
-    low["num_base_slots"] = 0  # every base slot now out of range
     main = rf(rng, (8, 4))
+    args = (main, np.zeros((8, 0), np.uint64), rf(rng, (1, 3)), rf(rng, (1, 3)), rf(rng, (3,)), 1, None, be)
+    low = lower(prog, False)
+    low["num_base_slots"] = 0  # every base slot now out of range
     with pytest.raises(SgError):
-        mc.eval_constraints_on_device(low, main, np.zeros((8, 0), np.uint64), rf(rng, (1, 3)), rf(rng, (1, 3)),
-                                      rf(rng, (3,)), 1, None, be)
+        mc.eval_constraints_on_device(low, *args)
+    # streaming programs: a trace operand past the last column, a constraint
+    # no instruction completes, a constraint completed twice
+    low = lower(prog)
+    bad = low["nodes"].copy()
+    k, j = next((i, j) for i in range(bad.shape[0]) for j in (1, 2) if bad[i, 0] in (6, 7, 8) and bad[i, j] >> 29 == 7)
+    bad[k, j] = (7 << 29) | 4
+    with pytest.raises(SgError):
+        mc.eval_constraints_on_device(dict(low, nodes=bad), *args)
+    nr = low["node_roots"].copy()
+    nr[nr != 0xFFFFFFFF] = 0xFFFFFFFF
+    with pytest.raises(SgError):
+        mc.eval_constraints_on_device(dict(low, node_roots=nr), *args)
+    nr = low["node_roots"].copy()
+    nr[nr == 1] = 0
+    with pytest.raises(SgError):
+        mc.eval_constraints_on_device(dict(low, node_roots=nr), *args)
 
 
 def test_decompose_d2_matches_formula(be):
