@@ -96,7 +96,14 @@ struct Trace {
     uint64_t A;
     uint64_t rows;
     uint64_t next_step;
+    const uint64_t* cm;   // the main LDE column-major (m x rows), or null
 };
+
+// One main-trace cell of an OPK_VAR operand: column-major when the copy
+// exists (a warp's 32 rows are then one coalesced segment), else row-major.
+__device__ __forceinline__ uint64_t main_cell(const Trace& t, uint64_t r, uint32_t col) {
+    return t.cm ? t.cm[(uint64_t)col * t.rows + r] : t.main[r * t.m + col];
+}
 
 __device__ __forceinline__ bool is_base_kind(uint32_t enc) {
     const uint32_t k = enc >> OPK_SHIFT;
@@ -112,7 +119,7 @@ __device__ __forceinline__ uint64_t base_op(uint32_t enc, const SlotFile& f, con
     const uint32_t p = enc & OPK_PAYLOAD_MASK;
     switch (enc >> OPK_SHIFT) {
         case OPK_BASE_SLOT: return f.gb(p);
-        case OPK_VAR: return t.main[var_row(p, t, row) * t.m + (p & VAR_COL_MASK)];
+        case OPK_VAR: return main_cell(t, var_row(p, t, row), p & VAR_COL_MASK);
         default: return __ldg(u.base_consts + p);
     }
 }
@@ -127,7 +134,7 @@ __device__ __forceinline__ fe3 ext_op(uint32_t enc, const SlotFile& f, const Uni
         case OPK_ALPHA: return fe3{__ldg(u.alpha + 3 * p), __ldg(u.alpha + 3 * p + 1), __ldg(u.alpha + 3 * p + 2)};
         case OPK_VAR: {
             const uint64_t r = var_row(p, t, row);
-            if (!(p & VAR_AUX_BIT)) return fe3{t.main[r * t.m + (p & VAR_COL_MASK)], 0, 0};
+            if (!(p & VAR_AUX_BIT)) return fe3{main_cell(t, r, p & VAR_COL_MASK), 0, 0};
             const uint64_t* q = t.aux + (r * t.A + (p & VAR_COL_MASK)) * 3;
             return fe3{q[0], q[1], q[2]};
         }
@@ -144,92 +151,139 @@ struct Sink {
     uint64_t* out;
 };
 
+// A main-trace operand (OPK_VAR, not aux) is fetched PF nodes ahead of its
+// node into a register ring, so its load latency overlaps the nodes between;
+// every other operand is read where it is used.
+__device__ __forceinline__ bool is_main_var(uint32_t enc) {
+    return (enc >> OPK_SHIFT) == OPK_VAR && !(enc & VAR_AUX_BIT);
+}
+// operand k (1: a, 2: b) of node nd, when it is a main-trace read: only the
+// operands of arithmetic nodes are operands (and validated as such)
+__device__ __forceinline__ uint64_t prefetch(const uint4& nd, int k, const Trace& t, uint64_t row) {
+    const bool arith = nd.x >= OP_ADD && nd.x <= (k == 1 ? OP_EMBED : OP_MUL);
+    const uint32_t enc = k == 1 ? nd.y : nd.z;
+    if (!arith || !is_main_var(enc)) return 0;
+    const uint32_t p = enc & OPK_PAYLOAD_MASK;
+    return main_cell(t, var_row(p, t, row), p & VAR_COL_MASK);
+}
+__device__ __forceinline__ uint64_t bop(uint32_t enc, uint64_t pv, const SlotFile& f, const Uni& u, const Trace& t,
+                                        uint64_t row) {
+    return is_main_var(enc) ? pv : base_op(enc, f, u, t, row);
+}
+__device__ __forceinline__ fe3 eop(uint32_t enc, uint64_t pv, const SlotFile& f, const Uni& u, const Trace& t,
+                                   uint64_t row) {
+    return is_main_var(enc) ? fe3{pv, 0, 0} : ext_op(enc, f, u, t, row);
+}
+
+// Node i of the walk; va, vb: the prefetched main-trace operands.
+__device__ __forceinline__ void exec_node(const uint4 nd, uint32_t i, uint64_t va, uint64_t vb, const Uni& u,
+                                          const SlotFile& f, const Trace& t, uint64_t row, const Sink& sk, fe3* sum) {
+    const uint32_t slot = nd.w & RES_SLOT_MASK;
+    const bool rx = (nd.w & RES_EXT_BIT) != 0;
+    switch (nd.x) {
+        case OP_VAR: {
+            const uint32_t off = (nd.z >> 8) & 0xFFu;
+            uint64_t r = row + (uint64_t)off * t.next_step;
+            if (r >= t.rows) r -= t.rows;
+            const uint32_t col = nd.y & 0xFFFFu;
+            if ((nd.z >> 16) & 1u)
+                f.pb(slot, main_cell(t, r, col));
+            else {
+                const uint64_t* p = t.aux + (r * t.A + col) * 3;
+                f.pe(slot, fe3{p[0], p[1], p[2]});
+            }
+            break;
+        }
+        case OP_ADD:
+            if (!rx)
+                f.pb(slot, gl::add(bop(nd.y, va, f, u, t, row), bop(nd.z, vb, f, u, t, row)));
+            else if (is_base_kind(nd.y)) {
+                const uint64_t x = bop(nd.y, va, f, u, t, row);
+                const fe3 y = eop(nd.z, vb, f, u, t, row);
+                f.pe(slot, fe3{gl::add(x, y.c0), y.c1, y.c2});
+            } else if (is_base_kind(nd.z)) {
+                const fe3 x = eop(nd.y, va, f, u, t, row);
+                f.pe(slot, fe3{gl::add(x.c0, bop(nd.z, vb, f, u, t, row)), x.c1, x.c2});
+            } else
+                f.pe(slot, gl::add3(eop(nd.y, va, f, u, t, row), eop(nd.z, vb, f, u, t, row)));
+            break;
+        case OP_SUB:
+            if (!rx)
+                f.pb(slot, gl::sub(bop(nd.y, va, f, u, t, row), bop(nd.z, vb, f, u, t, row)));
+            else if (is_base_kind(nd.y)) {
+                const uint64_t x = bop(nd.y, va, f, u, t, row);
+                const fe3 y = eop(nd.z, vb, f, u, t, row);
+                f.pe(slot, fe3{gl::sub(x, y.c0), gl::sub(0, y.c1), gl::sub(0, y.c2)});
+            } else if (is_base_kind(nd.z)) {
+                const fe3 x = eop(nd.y, va, f, u, t, row);
+                f.pe(slot, fe3{gl::sub(x.c0, bop(nd.z, vb, f, u, t, row)), x.c1, x.c2});
+            } else
+                f.pe(slot, gl::sub3(eop(nd.y, va, f, u, t, row), eop(nd.z, vb, f, u, t, row)));
+            break;
+        case OP_MUL:
+            if (!rx)
+                f.pb(slot, gl::mul(bop(nd.y, va, f, u, t, row), bop(nd.z, vb, f, u, t, row)));
+            else if (is_base_kind(nd.y))
+                f.pe(slot, gl::mulb3(eop(nd.z, vb, f, u, t, row), bop(nd.y, va, f, u, t, row)));
+            else if (is_base_kind(nd.z))
+                f.pe(slot, gl::mulb3(eop(nd.y, va, f, u, t, row), bop(nd.z, vb, f, u, t, row)));
+            else
+                f.pe(slot, gl::mul3(eop(nd.y, va, f, u, t, row), eop(nd.z, vb, f, u, t, row)));
+            break;
+        case OP_NEG:
+            if (!rx)
+                f.pb(slot, gl::neg(bop(nd.y, va, f, u, t, row)));
+            else {
+                const fe3 x = eop(nd.y, va, f, u, t, row);
+                f.pe(slot, fe3{gl::neg(x.c0), gl::neg(x.c1), gl::neg(x.c2)});
+            }
+            break;
+        case OP_EMBED: f.pe(slot, eop(nd.y, va, f, u, t, row)); break;
+        case OP_CONST_BASE: f.pb(slot, __ldg(u.base_consts + nd.y)); break;
+        case OP_CONST_EXT: f.pe(slot, ext_op((OPK_EXT_CONST << OPK_SHIFT) | nd.y, f, u, t, row)); break;
+        case OP_RAP_CHALLENGE: f.pe(slot, ext_op((OPK_RAP << OPK_SHIFT) | nd.y, f, u, t, row)); break;
+        case OP_ALPHA_POW: f.pe(slot, ext_op((OPK_ALPHA << OPK_SHIFT) | nd.y, f, u, t, row)); break;
+        case OP_TABLE_OFFSET: f.pe(slot, u.offset); break;
+        default: break;
+    }
+    if (sk.node_roots) {
+        const uint32_t c = __ldg(sk.node_roots + i);
+        if (c != NO_ROOT) {
+            if (sk.mode == 1) {
+                const fe3 v = gl::canon3(rx ? f.ge(slot) : fe3{f.gb(slot), 0, 0});
+                uint64_t* o = sk.out + 3 * ((uint64_t)c * t.rows + row);
+                o[0] = v.c0;
+                o[1] = v.c1;
+                o[2] = v.c2;
+            } else {
+                const fe3 b{__ldg(sk.beta + 3 * c), __ldg(sk.beta + 3 * c + 1), __ldg(sk.beta + 3 * c + 2)};
+                *sum = gl::add3(*sum, rx ? gl::mul3(b, f.ge(slot)) : gl::mulb3(b, f.gb(slot)));
+            }
+        }
+    }
+}
+
+constexpr int PF = 4;             // prefetch distance, in nodes
+constexpr uint64_t CM_MIN_COLS = 32;  // narrower main LDEs are walked row-major
+
 __device__ __forceinline__ void walk(const uint4* nodes, uint32_t num_nodes, const Uni& u, const SlotFile& f,
                                      const Trace& t, uint64_t row, const Sink& sk, fe3* sum) {
-    for (uint32_t i = 0; i < num_nodes; ++i) {
-        const uint4 nd = __ldg(nodes + i);
-        const uint32_t slot = nd.w & RES_SLOT_MASK;
-        const bool rx = (nd.w & RES_EXT_BIT) != 0;
-        switch (nd.x) {
-            case OP_VAR: {
-                const uint32_t off = (nd.z >> 8) & 0xFFu;
-                uint64_t r = row + (uint64_t)off * t.next_step;
-                if (r >= t.rows) r -= t.rows;
-                const uint32_t col = nd.y & 0xFFFFu;
-                if ((nd.z >> 16) & 1u)
-                    f.pb(slot, t.main[r * t.m + col]);
-                else {
-                    const uint64_t* p = t.aux + (r * t.A + col) * 3;
-                    f.pe(slot, fe3{p[0], p[1], p[2]});
-                }
-                break;
-            }
-            case OP_ADD:
-                if (!rx)
-                    f.pb(slot, gl::add(base_op(nd.y, f, u, t, row), base_op(nd.z, f, u, t, row)));
-                else if (is_base_kind(nd.y)) {
-                    const uint64_t x = base_op(nd.y, f, u, t, row);
-                    const fe3 y = ext_op(nd.z, f, u, t, row);
-                    f.pe(slot, fe3{gl::add(x, y.c0), y.c1, y.c2});
-                } else if (is_base_kind(nd.z)) {
-                    const fe3 x = ext_op(nd.y, f, u, t, row);
-                    f.pe(slot, fe3{gl::add(x.c0, base_op(nd.z, f, u, t, row)), x.c1, x.c2});
-                } else
-                    f.pe(slot, gl::add3(ext_op(nd.y, f, u, t, row), ext_op(nd.z, f, u, t, row)));
-                break;
-            case OP_SUB:
-                if (!rx)
-                    f.pb(slot, gl::sub(base_op(nd.y, f, u, t, row), base_op(nd.z, f, u, t, row)));
-                else if (is_base_kind(nd.y)) {
-                    const uint64_t x = base_op(nd.y, f, u, t, row);
-                    const fe3 y = ext_op(nd.z, f, u, t, row);
-                    f.pe(slot, fe3{gl::sub(x, y.c0), gl::sub(0, y.c1), gl::sub(0, y.c2)});
-                } else if (is_base_kind(nd.z)) {
-                    const fe3 x = ext_op(nd.y, f, u, t, row);
-                    f.pe(slot, fe3{gl::sub(x.c0, base_op(nd.z, f, u, t, row)), x.c1, x.c2});
-                } else
-                    f.pe(slot, gl::sub3(ext_op(nd.y, f, u, t, row), ext_op(nd.z, f, u, t, row)));
-                break;
-            case OP_MUL:
-                if (!rx)
-                    f.pb(slot, gl::mul(base_op(nd.y, f, u, t, row), base_op(nd.z, f, u, t, row)));
-                else if (is_base_kind(nd.y))
-                    f.pe(slot, gl::mulb3(ext_op(nd.z, f, u, t, row), base_op(nd.y, f, u, t, row)));
-                else if (is_base_kind(nd.z))
-                    f.pe(slot, gl::mulb3(ext_op(nd.y, f, u, t, row), base_op(nd.z, f, u, t, row)));
-                else
-                    f.pe(slot, gl::mul3(ext_op(nd.y, f, u, t, row), ext_op(nd.z, f, u, t, row)));
-                break;
-            case OP_NEG:
-                if (!rx)
-                    f.pb(slot, gl::neg(base_op(nd.y, f, u, t, row)));
-                else {
-                    const fe3 x = ext_op(nd.y, f, u, t, row);
-                    f.pe(slot, fe3{gl::neg(x.c0), gl::neg(x.c1), gl::neg(x.c2)});
-                }
-                break;
-            case OP_EMBED: f.pe(slot, ext_op(nd.y, f, u, t, row)); break;
-            case OP_CONST_BASE: f.pb(slot, __ldg(u.base_consts + nd.y)); break;
-            case OP_CONST_EXT: f.pe(slot, ext_op((OPK_EXT_CONST << OPK_SHIFT) | nd.y, f, u, t, row)); break;
-            case OP_RAP_CHALLENGE: f.pe(slot, ext_op((OPK_RAP << OPK_SHIFT) | nd.y, f, u, t, row)); break;
-            case OP_ALPHA_POW: f.pe(slot, ext_op((OPK_ALPHA << OPK_SHIFT) | nd.y, f, u, t, row)); break;
-            case OP_TABLE_OFFSET: f.pe(slot, u.offset); break;
-            default: break;
-        }
-        if (sk.node_roots) {
-            const uint32_t c = __ldg(sk.node_roots + i);
-            if (c != NO_ROOT) {
-                if (sk.mode == 1) {
-                    const fe3 v = gl::canon3(rx ? f.ge(slot) : fe3{f.gb(slot), 0, 0});
-                    uint64_t* o = sk.out + 3 * ((uint64_t)c * t.rows + row);
-                    o[0] = v.c0;
-                    o[1] = v.c1;
-                    o[2] = v.c2;
-                } else {
-                    const fe3 b{__ldg(sk.beta + 3 * c), __ldg(sk.beta + 3 * c + 1), __ldg(sk.beta + 3 * c + 2)};
-                    *sum = gl::add3(*sum, rx ? gl::mul3(b, f.ge(slot)) : gl::mulb3(b, f.gb(slot)));
-                }
-            }
+    uint4 q[PF];
+    uint64_t pa[PF], pb[PF];
+#pragma unroll
+    for (int j = 0; j < PF; ++j) {
+        q[j] = (uint32_t)j < num_nodes ? __ldg(nodes + j) : make_uint4(0xFFFFFFFFu, 0, 0, 0);
+        pa[j] = prefetch(q[j], 1, t, row);
+        pb[j] = prefetch(q[j], 2, t, row);
+    }
+    for (uint32_t i = 0; i < num_nodes; i += PF) {
+#pragma unroll
+        for (int j = 0; j < PF; ++j) {
+            if (i + j < num_nodes) exec_node(q[j], i + j, pa[j], pb[j], u, f, t, row, sk, sum);
+            const uint32_t nx = i + j + PF;
+            q[j] = nx < num_nodes ? __ldg(nodes + nx) : make_uint4(0xFFFFFFFFu, 0, 0, 0);
+            pa[j] = prefetch(q[j], 1, t, row);
+            pb[j] = prefetch(q[j], 2, t, row);
         }
     }
 }
@@ -311,6 +365,22 @@ __global__ void k_constraints(const uint4* nodes, uint32_t num_nodes, const uint
         out[3 * row] = h.c0;
         out[3 * row + 1] = h.c1;
         out[3 * row + 2] = h.c2;
+    }
+}
+
+// The main LDE column-major for the walk: 32 x 32 tiles through shared memory,
+// rows x m in, m x rows out. Grid: x = row tiles, y = column tiles.
+__global__ void k_to_columns(const uint64_t* __restrict__ in, uint64_t rows, uint64_t m, uint64_t* __restrict__ out) {
+    __shared__ uint64_t tile[32][33];
+    const uint64_t r0 = (uint64_t)blockIdx.x * 32, c0 = (uint64_t)blockIdx.y * 32;
+    for (uint32_t k = threadIdx.y; k < 32; k += blockDim.y) {
+        const uint64_t r = r0 + k, c = c0 + threadIdx.x;
+        if (r < rows && c < m) tile[k][threadIdx.x] = in[r * m + c];
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.y; k < 32; k += blockDim.y) {
+        const uint64_t c = c0 + k, r = r0 + threadIdx.x;
+        if (r < rows && c < m) out[c * rows + r] = tile[threadIdx.x][k];
     }
 }
 
@@ -456,7 +526,22 @@ int sg_eval_constraints(sg_ctx* c, void* stream, const sg_device_program* prog, 
     if (rc == SG_OK) {
         Uni u{d_blob + o_bc, d_blob + o_ec, d_blob + o_rap, d_blob + o_al,
               fe3{table_offset[0], table_offset[1], table_offset[2]}};
-        Trace t{d_main, m, d_aux, a, rows, next_step};
+        // A streaming walk reads the main LDE where each operand is used: a
+        // column-major copy makes those reads coalesced (a warp's 32 rows are
+        // one segment) instead of 32 rows 8m bytes apart. Skipped when the
+        // budget has no room for it.
+        uint64_t* d_cm = nullptr;
+        const uint64_t cm_bytes = rows * m * 8;
+        if (prog->node_roots && m >= CM_MIN_COLS && rows >= 32 && rows / 32 <= 0x7FFFFFFFull && m / 32 < 65535) {
+            if (dev_alloc(ctx, st, cm_bytes, (void**)&d_cm) == SG_OK) {
+                k_to_columns<<<dim3((unsigned)((rows + 31) / 32), (unsigned)((m + 31) / 32)), dim3(32, 8), 0, st>>>(
+                    d_main, rows, m, d_cm);
+                rc = check_launch(ctx, "k_to_columns");
+            } else {
+                d_cm = nullptr;  // no room: the walk reads the row-major LDE
+            }
+        }
+        Trace t{d_main, m, d_aux, a, rows, next_step, d_cm};
         Comp cp{};
         if (comp) {
             cp = Comp{d_blob + o_beta, comp->d_z_inv, comp->z_len, nb, d_blob + o_bcol, d_blob + o_baux,
@@ -465,14 +550,18 @@ int sg_eval_constraints(sg_ctx* c, void* stream, const sg_device_program* prog, 
         const size_t smem = use_smem ? per_thread * T * 8 : 0;
         if (smem > 48 * 1024) cudaFuncSetAttribute(k_constraints, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         const uint32_t* d_nroots = prog->node_roots ? (const uint32_t*)(d_blob + o_nroots) : nullptr;
-        k_constraints<<<(unsigned)blocks, T, smem, st>>>((const uint4*)(d_blob + o_nodes), nn,
-                                                         (const uint32_t*)(d_blob + o_roots), nr, d_nroots, nbs, nes,
-                                                         u, t, cp, comp ? 0 : 1, d_out, use_smem ? nullptr : d_scr);
-        rc = check_launch(ctx, "k_constraints");
+        if (rc == SG_OK) {
+            k_constraints<<<(unsigned)blocks, T, smem, st>>>((const uint4*)(d_blob + o_nodes), nn,
+                                                             (const uint32_t*)(d_blob + o_roots), nr, d_nroots, nbs,
+                                                             nes, u, t, cp, comp ? 0 : 1, d_out,
+                                                             use_smem ? nullptr : d_scr);
+            rc = check_launch(ctx, "k_constraints");
+        }
         if (rc == SG_OK && cudaStreamSynchronize(st) != cudaSuccess) {
             set_error("constraints: execution failed");
             rc = SG_ERR_CUDA;
         }
+        if (d_cm) dev_free(ctx, st, d_cm, cm_bytes);
     }
     if (d_scr) dev_free(ctx, st, d_scr, sb);
     dev_free(ctx, st, d_blob, bb);

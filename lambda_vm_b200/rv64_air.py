@@ -854,9 +854,9 @@ class KeccakAir(BusAir):
                 b.emit(b.sub(CP[x][z], e.xor3(C[x][z], C[(x - 1) % 5][z], C[(x + 1) % 5][(z - 1) % 64])))
                 t = b.sub(e.total([AP[x][y][z] for y in range(5)]), CP[x][z])
                 b.emit(b.mul(b.mul(t, b.sub(t, two)), b.sub(t, four)))
-        for x in range(5):
-            for y in range(5):
-                for l in range(4):
+        for x in range(5):  # the five lanes of a column share C[x][z] * C'[x][z]: y innermost
+            for l in range(4):
+                for y in range(5):
                     bits = [e.xor3(AP[x][y][z], C[x][z], CP[x][z]) for z in range(16 * l, 16 * l + 16)]
                     b.emit(b.sub(M(KA + 4 * _lane(x, y) + l), e.total([e.scaled(1 << i, v) for i, v in enumerate(bits)])))
         # rho and pi: Bm[y][2x + 3y] = rot(A'[x][y], r[x][y])
