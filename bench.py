@@ -816,10 +816,11 @@ def main():
         except Exception as e:  # noqa: BLE001
             line["proof_workload"] = {"error": f"{type(e).__name__}: {e}"}
     if world == 1 and not a.no_proof_summary:
-        try:
-            line["vm_workload"] = measure_vm(a)
-        except Exception as e:  # noqa: BLE001
-            line["vm_workload"] = {"error": f"{type(e).__name__}: {e}"}
+        for key, guest in (("vm_workload", "fib"), ("keccak_workload", "keccak")):
+            try:
+                line[key] = measure_vm(a, guest)
+            except Exception as e:  # noqa: BLE001
+                line[key] = {"error": f"{type(e).__name__}: {e}"}
     if world == 1 and not a.no_serve_summary:
         try:
             line["serving"] = serve_summary(a)

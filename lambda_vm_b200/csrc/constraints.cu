@@ -420,7 +420,12 @@ int sg_eval_constraints(sg_ctx* c, void* stream, const sg_device_program* prog, 
     const uint32_t nn = prog->num_nodes, nr = prog->num_roots;
     const uint32_t nbs = prog->num_base_slots, nes = prog->num_ext_slots;
     // Validate the blob on the host: every slot, table index, column and frame
-    // offset must be in range, so the walk never reads out of bounds.
+    // offset must be in range, so the walk never reads out of bounds. Count
+    // the main-trace operands a row reads, for the layout choice below.
+    uint64_t main_reads = 0;
+    auto is_main_operand = [](uint32_t enc) {
+        return (enc >> OPK_SHIFT) == OPK_VAR && !(enc & VAR_AUX_BIT) ? 1u : 0u;
+    };
     for (uint32_t i = 0; i < nn; ++i) {
         const uint32_t* nd = prog->nodes + 4 * i;
         const uint32_t op = nd[0], slot = nd[3] & RES_SLOT_MASK;
@@ -444,6 +449,8 @@ int sg_eval_constraints(sg_ctx* c, void* stream, const sg_device_program* prog, 
             }
         };
         if (op >= OP_ADD && op <= OP_MUL) SG_CHECK_ARG(ok_operand(nd[1]) && ok_operand(nd[2]), "operand out of range");
+        if (op >= OP_ADD && op <= OP_EMBED) main_reads += is_main_operand(nd[1]);
+        if (op >= OP_ADD && op <= OP_MUL) main_reads += is_main_operand(nd[2]);
         if (op == OP_NEG || op == OP_EMBED) SG_CHECK_ARG(ok_operand(nd[1]), "operand out of range");
         if (op == OP_VAR) {
             const uint32_t col = nd[1] & 0xFFFFu, off = (nd[2] >> 8) & 0xFFu;
@@ -528,11 +535,13 @@ int sg_eval_constraints(sg_ctx* c, void* stream, const sg_device_program* prog, 
               fe3{table_offset[0], table_offset[1], table_offset[2]}};
         // A streaming walk reads the main LDE where each operand is used: a
         // column-major copy makes those reads coalesced (a warp's 32 rows are
-        // one segment) instead of 32 rows 8m bytes apart. Skipped when the
-        // budget has no room for it.
+        // one segment; row-major, each read moves a 32-byte sector for 8
+        // bytes). The copy moves 2m words a row, so it pays once a row reads
+        // at least m operands; skipped when the budget has no room for it.
         uint64_t* d_cm = nullptr;
         const uint64_t cm_bytes = rows * m * 8;
-        if (prog->node_roots && m >= CM_MIN_COLS && rows >= 32 && rows / 32 <= 0x7FFFFFFFull && m / 32 < 65535) {
+        if (prog->node_roots && m >= CM_MIN_COLS && main_reads >= m && rows >= 32 && rows / 32 <= 0x7FFFFFFFull &&
+            m / 32 < 65535) {
             if (dev_alloc(ctx, st, cm_bytes, (void**)&d_cm) == SG_OK) {
                 k_to_columns<<<dim3((unsigned)((rows + 31) / 32), (unsigned)((m + 31) / 32)), dim3(32, 8), 0, st>>>(
                     d_main, rows, m, d_cm);
