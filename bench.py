@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--job-max-log-n", type=int, default=18, help="serve: largest job height (log2 cycles)")
     ap.add_argument("--max-jobs", type=int, default=4, help="serve: concurrent jobs")
     ap.add_argument("--policy", default="backfill", choices=["backfill", "fifo"], help="serve: admission policy")
+    ap.add_argument("--beside-big", type=int, default=1, help="serve: small jobs allowed beside a running large one")
+    ap.add_argument("--big-cells", type=int, default=1 << 23, help="serve: trace cells from which a job is large")
     ap.add_argument("--job-kind", default="mix", choices=["mix", "synth"],
                     help="serve: Fibonacci and Keccak guests alternating, or synthetic chip tables only")
     ap.add_argument("--no-serve-summary", action="store_true",
@@ -426,7 +428,8 @@ def measure_serve(a):
     sweep = []
     for i, rate in enumerate(float(x) for x in a.rates.split(",")):
         def batched():
-            with ProofServer(budget, max_jobs=a.max_jobs, drivers=4, opts=opts, be=be, policy=a.policy) as srv:
+            with ProofServer(budget, max_jobs=a.max_jobs, drivers=4, opts=opts, be=be, policy=a.policy,
+                             beside_big=getattr(a, "beside_big", 1), big_cells=getattr(a, "big_cells", 1 << 23)) as srv:
                 return serve_poisson(srv, specs, rate, seed=int(rate * 1000))[1]
 
         def one_at_a_time():
@@ -466,7 +469,8 @@ def serve_summary(a):
     24 jobs each, admission server against one proof at a time."""
     import types
     b = types.SimpleNamespace(jobs=24, job_max_log_n=a.job_max_log_n, max_jobs=a.max_jobs, rates="5,50",
-                              policy=a.policy, job_kind=getattr(a, "job_kind", "mix"))
+                              policy=a.policy, job_kind=getattr(a, "job_kind", "mix"), beside_big=a.beside_big,
+                              big_cells=a.big_cells)
     line = measure_serve(b)
     return {"workload": line["config"]["workload"], "policy": a.policy,
             "rates": [{"rate_jobs_per_s": s["rate_jobs_per_s"],
