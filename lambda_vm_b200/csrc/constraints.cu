@@ -151,179 +151,139 @@ struct Sink {
     uint64_t* out;
 };
 
-// The walk runs micro-ops, the program re-encoded on the host (micro_ops
-// below) so that each node's operand sources are known from its opcode:
-//   x: micro-op (bits 0-7) | constraint index (bits 8-30) | completes a
-//      constraint (bit 31);
-//   y, z: operand payloads; w: result slot (| RES_EXT_BIT).
-// Base-field nodes (add / sub / mul / neg with base operands) get one opcode
-// per operand-source combination (slot, constant, main-trace cell), whose
-// payload is the slot, the constant index or the cell (column | frame offset
-// << 20); a main-trace cell is fetched PF nodes ahead into a register ring,
-// so its load overlaps the nodes between. Everything else (extension-field
-// nodes: LogUp, challenges) keeps the program's operand encoding and the
-// generic path.
-enum : uint32_t {
-    M_VAR_MAIN = 0,  // y: column | offset << 20
-    M_VAR_AUX = 1,   // y: column | offset << 20
-    M_CONST = 2,     // y: base constant index
-    M_BIN = 3,       // 3 + 9 op + 3 ka + kb; op 0 add, 1 sub, 2 mul; k 0 slot, 1 constant, 2 cell
-    M_NEG = 30,      // 30 + k
-    M_GEN = 40,      // 40 + program op: generic path on the program's operand encoding
-};
-constexpr uint32_t M_ROOT_BIT = 0x80000000u, M_ROOT_SHIFT = 8, M_ROOT_MASK = 0x7FFFFFu;
-__host__ __device__ constexpr bool m_var_a(uint32_t m) {
-    return (m >= M_BIN && m < M_NEG && ((m - M_BIN) / 3) % 3 == 2) || m == M_NEG + 2;
+// A main-trace operand (OPK_VAR, not aux) is fetched PF nodes ahead of its
+// node into a register ring, so its load latency overlaps the nodes between;
+// every other operand is read where it is used.
+__device__ __forceinline__ bool is_main_var(uint32_t enc) {
+    return (enc >> OPK_SHIFT) == OPK_VAR && !(enc & VAR_AUX_BIT);
 }
-__host__ __device__ constexpr bool m_var_b(uint32_t m) { return m >= M_BIN && m < M_NEG && (m - M_BIN) % 3 == 2; }
-
-__device__ __forceinline__ uint64_t cell_at(uint32_t p, const Trace& t, uint64_t row) {
-    uint64_t r = row + (uint64_t)((p >> VAR_OFF_SHIFT) & 0xFFu) * t.next_step;
-    if (r >= t.rows) r -= t.rows;
-    return main_cell(t, r, p & VAR_COL_MASK);
+// operand k (1: a, 2: b) of node nd, when it is a main-trace read: only the
+// operands of arithmetic nodes are operands (and validated as such)
+__device__ __forceinline__ uint64_t prefetch(const uint4& nd, int k, const Trace& t, uint64_t row) {
+    const bool arith = nd.x >= OP_ADD && nd.x <= (k == 1 ? OP_EMBED : OP_MUL);
+    const uint32_t enc = k == 1 ? nd.y : nd.z;
+    if (!arith || !is_main_var(enc)) return 0;
+    const uint32_t p = enc & OPK_PAYLOAD_MASK;
+    return main_cell(t, var_row(p, t, row), p & VAR_COL_MASK);
 }
-template <int K>
-__device__ __forceinline__ uint64_t bsrc(uint32_t p, uint64_t pv, const SlotFile& f, const Uni& u) {
-    if (K == 0) return f.gb(p);
-    if (K == 1) return __ldg(u.base_consts + p);
-    return pv;
+__device__ __forceinline__ uint64_t bop(uint32_t enc, uint64_t pv, const SlotFile& f, const Uni& u, const Trace& t,
+                                        uint64_t row) {
+    return is_main_var(enc) ? pv : base_op(enc, f, u, t, row);
 }
-template <int OP, int KA, int KB>
-__device__ __forceinline__ uint64_t bin(const uint4& nd, uint64_t va, uint64_t vb, const SlotFile& f, const Uni& u) {
-    const uint64_t a = bsrc<KA>(nd.y, va, f, u), b = bsrc<KB>(nd.z, vb, f, u);
-    return OP == 0 ? gl::add(a, b) : OP == 1 ? gl::sub(a, b) : gl::mul(a, b);
+__device__ __forceinline__ fe3 eop(uint32_t enc, uint64_t pv, const SlotFile& f, const Uni& u, const Trace& t,
+                                   uint64_t row) {
+    return is_main_var(enc) ? fe3{pv, 0, 0} : ext_op(enc, f, u, t, row);
 }
 
-// Generic node (extension-field result): the program's operand encoding.
-__device__ __noinline__ fe3 exec_generic(const uint4 nd, uint32_t op, const Uni& u, const SlotFile& f,
-                                         const Trace& t, uint64_t row) {
-    switch (op) {
+// Node i of the walk; va, vb: the prefetched main-trace operands.
+__device__ __forceinline__ void exec_node(const uint4 nd, uint32_t i, uint64_t va, uint64_t vb, const Uni& u,
+                                          const SlotFile& f, const Trace& t, uint64_t row, const Sink& sk, fe3* sum) {
+    const uint32_t slot = nd.w & RES_SLOT_MASK;
+    const bool rx = (nd.w & RES_EXT_BIT) != 0;
+    switch (nd.x) {
+        case OP_VAR: {
+            const uint32_t off = (nd.z >> 8) & 0xFFu;
+            uint64_t r = row + (uint64_t)off * t.next_step;
+            if (r >= t.rows) r -= t.rows;
+            const uint32_t col = nd.y & 0xFFFFu;
+            if ((nd.z >> 16) & 1u)
+                f.pb(slot, main_cell(t, r, col));
+            else {
+                const uint64_t* p = t.aux + (r * t.A + col) * 3;
+                f.pe(slot, fe3{p[0], p[1], p[2]});
+            }
+            break;
+        }
         case OP_ADD:
-            if (is_base_kind(nd.y)) {
-                const uint64_t x = base_op(nd.y, f, u, t, row);
-                const fe3 y = ext_op(nd.z, f, u, t, row);
-                return fe3{gl::add(x, y.c0), y.c1, y.c2};
-            }
-            if (is_base_kind(nd.z)) {
-                const fe3 x = ext_op(nd.y, f, u, t, row);
-                return fe3{gl::add(x.c0, base_op(nd.z, f, u, t, row)), x.c1, x.c2};
-            }
-            return gl::add3(ext_op(nd.y, f, u, t, row), ext_op(nd.z, f, u, t, row));
+            if (!rx)
+                f.pb(slot, gl::add(bop(nd.y, va, f, u, t, row), bop(nd.z, vb, f, u, t, row)));
+            else if (is_base_kind(nd.y)) {
+                const uint64_t x = bop(nd.y, va, f, u, t, row);
+                const fe3 y = eop(nd.z, vb, f, u, t, row);
+                f.pe(slot, fe3{gl::add(x, y.c0), y.c1, y.c2});
+            } else if (is_base_kind(nd.z)) {
+                const fe3 x = eop(nd.y, va, f, u, t, row);
+                f.pe(slot, fe3{gl::add(x.c0, bop(nd.z, vb, f, u, t, row)), x.c1, x.c2});
+            } else
+                f.pe(slot, gl::add3(eop(nd.y, va, f, u, t, row), eop(nd.z, vb, f, u, t, row)));
+            break;
         case OP_SUB:
-            if (is_base_kind(nd.y)) {
-                const uint64_t x = base_op(nd.y, f, u, t, row);
-                const fe3 y = ext_op(nd.z, f, u, t, row);
-                return fe3{gl::sub(x, y.c0), gl::sub(0, y.c1), gl::sub(0, y.c2)};
-            }
-            if (is_base_kind(nd.z)) {
-                const fe3 x = ext_op(nd.y, f, u, t, row);
-                return fe3{gl::sub(x.c0, base_op(nd.z, f, u, t, row)), x.c1, x.c2};
-            }
-            return gl::sub3(ext_op(nd.y, f, u, t, row), ext_op(nd.z, f, u, t, row));
+            if (!rx)
+                f.pb(slot, gl::sub(bop(nd.y, va, f, u, t, row), bop(nd.z, vb, f, u, t, row)));
+            else if (is_base_kind(nd.y)) {
+                const uint64_t x = bop(nd.y, va, f, u, t, row);
+                const fe3 y = eop(nd.z, vb, f, u, t, row);
+                f.pe(slot, fe3{gl::sub(x, y.c0), gl::sub(0, y.c1), gl::sub(0, y.c2)});
+            } else if (is_base_kind(nd.z)) {
+                const fe3 x = eop(nd.y, va, f, u, t, row);
+                f.pe(slot, fe3{gl::sub(x.c0, bop(nd.z, vb, f, u, t, row)), x.c1, x.c2});
+            } else
+                f.pe(slot, gl::sub3(eop(nd.y, va, f, u, t, row), eop(nd.z, vb, f, u, t, row)));
+            break;
         case OP_MUL:
-            if (is_base_kind(nd.y)) return gl::mulb3(ext_op(nd.z, f, u, t, row), base_op(nd.y, f, u, t, row));
-            if (is_base_kind(nd.z)) return gl::mulb3(ext_op(nd.y, f, u, t, row), base_op(nd.z, f, u, t, row));
-            return gl::mul3(ext_op(nd.y, f, u, t, row), ext_op(nd.z, f, u, t, row));
-        case OP_NEG: {
-            const fe3 x = ext_op(nd.y, f, u, t, row);
-            return fe3{gl::neg(x.c0), gl::neg(x.c1), gl::neg(x.c2)};
-        }
-        case OP_EMBED: return ext_op(nd.y, f, u, t, row);
-        case OP_CONST_EXT: return ext_op((OPK_EXT_CONST << OPK_SHIFT) | nd.y, f, u, t, row);
-        case OP_RAP_CHALLENGE: return ext_op((OPK_RAP << OPK_SHIFT) | nd.y, f, u, t, row);
-        case OP_ALPHA_POW: return ext_op((OPK_ALPHA << OPK_SHIFT) | nd.y, f, u, t, row);
-        default: return u.offset;  // OP_TABLE_OFFSET
-    }
-}
-
-#define BIN_CASE(OP, KA, KB) \
-    case M_BIN + 9 * OP + 3 * KA + KB: v = bin<OP, KA, KB>(nd, va, vb, f, u); break;
-#define BIN_OP(OP) BIN_CASE(OP, 0, 0) BIN_CASE(OP, 0, 1) BIN_CASE(OP, 0, 2) BIN_CASE(OP, 1, 0) BIN_CASE(OP, 1, 1) \
-    BIN_CASE(OP, 1, 2) BIN_CASE(OP, 2, 0) BIN_CASE(OP, 2, 1) BIN_CASE(OP, 2, 2)
-
-// One micro-op; va, vb: the prefetched main-trace cells of its operands.
-__device__ __forceinline__ void exec_node(const uint4 nd, uint64_t va, uint64_t vb, const Uni& u, const SlotFile& f,
-                                          const Trace& t, uint64_t row, const Sink& sk, fe3* sum) {
-    const uint32_t m = nd.x & 0xFFu, slot = nd.w & RES_SLOT_MASK;
-    if (m < M_GEN) {
-        uint64_t v;
-        switch (m) {
-            case M_VAR_MAIN: v = cell_at(nd.y, t, row); break;
-            case M_CONST: v = __ldg(u.base_consts + nd.y); break;
-            BIN_OP(0) BIN_OP(1) BIN_OP(2)
-            case M_NEG: v = gl::neg(bsrc<0>(nd.y, va, f, u)); break;
-            case M_NEG + 1: v = gl::neg(bsrc<1>(nd.y, va, f, u)); break;
-            case M_NEG + 2: v = gl::neg(va); break;
-            default: {  // M_VAR_AUX
-                uint64_t r = row + (uint64_t)((nd.y >> VAR_OFF_SHIFT) & 0xFFu) * t.next_step;
-                if (r >= t.rows) r -= t.rows;
-                const uint64_t* q = t.aux + (r * t.A + (nd.y & VAR_COL_MASK)) * 3;
-                const fe3 e{q[0], q[1], q[2]};
-                f.pe(slot, e);
-                if (nd.x & M_ROOT_BIT) {
-                    const uint32_t c = (nd.x >> M_ROOT_SHIFT) & M_ROOT_MASK;
-                    if (sk.mode == 1) {
-                        const fe3 cv = gl::canon3(e);
-                        uint64_t* o = sk.out + 3 * ((uint64_t)c * t.rows + row);
-                        o[0] = cv.c0, o[1] = cv.c1, o[2] = cv.c2;
-                    } else {
-                        const fe3 b{__ldg(sk.beta + 3 * c), __ldg(sk.beta + 3 * c + 1), __ldg(sk.beta + 3 * c + 2)};
-                        *sum = gl::add3(*sum, gl::mul3(b, e));
-                    }
-                }
-                return;
+            if (!rx)
+                f.pb(slot, gl::mul(bop(nd.y, va, f, u, t, row), bop(nd.z, vb, f, u, t, row)));
+            else if (is_base_kind(nd.y))
+                f.pe(slot, gl::mulb3(eop(nd.z, vb, f, u, t, row), bop(nd.y, va, f, u, t, row)));
+            else if (is_base_kind(nd.z))
+                f.pe(slot, gl::mulb3(eop(nd.y, va, f, u, t, row), bop(nd.z, vb, f, u, t, row)));
+            else
+                f.pe(slot, gl::mul3(eop(nd.y, va, f, u, t, row), eop(nd.z, vb, f, u, t, row)));
+            break;
+        case OP_NEG:
+            if (!rx)
+                f.pb(slot, gl::neg(bop(nd.y, va, f, u, t, row)));
+            else {
+                const fe3 x = eop(nd.y, va, f, u, t, row);
+                f.pe(slot, fe3{gl::neg(x.c0), gl::neg(x.c1), gl::neg(x.c2)});
             }
-        }
-        f.pb(slot, v);
-        if (nd.x & M_ROOT_BIT) {
-            const uint32_t c = (nd.x >> M_ROOT_SHIFT) & M_ROOT_MASK;
+            break;
+        case OP_EMBED: f.pe(slot, eop(nd.y, va, f, u, t, row)); break;
+        case OP_CONST_BASE: f.pb(slot, __ldg(u.base_consts + nd.y)); break;
+        case OP_CONST_EXT: f.pe(slot, ext_op((OPK_EXT_CONST << OPK_SHIFT) | nd.y, f, u, t, row)); break;
+        case OP_RAP_CHALLENGE: f.pe(slot, ext_op((OPK_RAP << OPK_SHIFT) | nd.y, f, u, t, row)); break;
+        case OP_ALPHA_POW: f.pe(slot, ext_op((OPK_ALPHA << OPK_SHIFT) | nd.y, f, u, t, row)); break;
+        case OP_TABLE_OFFSET: f.pe(slot, u.offset); break;
+        default: break;
+    }
+    if (sk.node_roots) {
+        const uint32_t c = __ldg(sk.node_roots + i);
+        if (c != NO_ROOT) {
             if (sk.mode == 1) {
+                const fe3 v = gl::canon3(rx ? f.ge(slot) : fe3{f.gb(slot), 0, 0});
                 uint64_t* o = sk.out + 3 * ((uint64_t)c * t.rows + row);
-                o[0] = gl::canon(v), o[1] = 0, o[2] = 0;
+                o[0] = v.c0;
+                o[1] = v.c1;
+                o[2] = v.c2;
             } else {
                 const fe3 b{__ldg(sk.beta + 3 * c), __ldg(sk.beta + 3 * c + 1), __ldg(sk.beta + 3 * c + 2)};
-                *sum = gl::add3(*sum, gl::mulb3(b, v));
+                *sum = gl::add3(*sum, rx ? gl::mul3(b, f.ge(slot)) : gl::mulb3(b, f.gb(slot)));
             }
         }
-        return;
-    }
-    const fe3 e = exec_generic(nd, m - M_GEN, u, f, t, row);
-    f.pe(slot, e);
-    if (nd.x & M_ROOT_BIT) {
-        const uint32_t c = (nd.x >> M_ROOT_SHIFT) & M_ROOT_MASK;
-        if (sk.mode == 1) {
-            const fe3 cv = gl::canon3(e);
-            uint64_t* o = sk.out + 3 * ((uint64_t)c * t.rows + row);
-            o[0] = cv.c0, o[1] = cv.c1, o[2] = cv.c2;
-        } else {
-            const fe3 b{__ldg(sk.beta + 3 * c), __ldg(sk.beta + 3 * c + 1), __ldg(sk.beta + 3 * c + 2)};
-            *sum = gl::add3(*sum, gl::mul3(b, e));
-        }
     }
 }
 
-constexpr int PF = 4;                 // prefetch distance, in nodes
+constexpr int PF = 4;             // prefetch distance, in nodes
 constexpr uint64_t CM_MIN_COLS = 32;  // narrower main LDEs are walked row-major
-
-__device__ __forceinline__ void fetch(const uint4* nodes, uint32_t k, uint32_t n, const Trace& t, uint64_t row,
-                                      uint4* q, uint64_t* pa, uint64_t* pb) {
-    *q = k < n ? __ldg(nodes + k) : make_uint4(M_GEN + 0xFFu, 0, 0, 0);
-    const uint32_t m = q->x & 0xFFu;
-    *pa = m_var_a(m) ? cell_at(q->y, t, row) : 0;
-    *pb = m_var_b(m) ? cell_at(q->z, t, row) : 0;
-}
 
 __device__ __forceinline__ void walk(const uint4* nodes, uint32_t num_nodes, const Uni& u, const SlotFile& f,
                                      const Trace& t, uint64_t row, const Sink& sk, fe3* sum) {
     uint4 q[PF];
     uint64_t pa[PF], pb[PF];
 #pragma unroll
-    for (int j = 0; j < PF; ++j) fetch(nodes, j, num_nodes, t, row, &q[j], &pa[j], &pb[j]);
+    for (int j = 0; j < PF; ++j) {
+        q[j] = (uint32_t)j < num_nodes ? __ldg(nodes + j) : make_uint4(0xFFFFFFFFu, 0, 0, 0);
+        pa[j] = prefetch(q[j], 1, t, row);
+        pb[j] = prefetch(q[j], 2, t, row);
+    }
     for (uint32_t i = 0; i < num_nodes; i += PF) {
 #pragma unroll
         for (int j = 0; j < PF; ++j) {
-            if (i + j < num_nodes) exec_node(q[j], pa[j], pb[j], u, f, t, row, sk, sum);
-            fetch(nodes, i + j + PF, num_nodes, t, row, &q[j], &pa[j], &pb[j]);
+            if (i + j < num_nodes) exec_node(q[j], i + j, pa[j], pb[j], u, f, t, row, sk, sum);
+            const uint32_t nx = i + j + PF;
+            q[j] = nx < num_nodes ? __ldg(nodes + nx) : make_uint4(0xFFFFFFFFu, 0, 0, 0);
+            pa[j] = prefetch(q[j], 1, t, row);
+            pb[j] = prefetch(q[j], 2, t, row);
         }
     }
 }
@@ -470,7 +430,6 @@ int sg_eval_constraints(sg_ctx* c, void* stream, const sg_device_program* prog, 
         const uint32_t k = enc >> OPK_SHIFT;
         return k == OPK_BASE_SLOT || k == OPK_BASE_CONST || is_main_operand(enc);
     };
-    SG_CHECK_ARG(nr <= M_ROOT_MASK, "too many constraints");
     for (uint32_t i = 0; i < nn; ++i) {
         const uint32_t* nd = prog->nodes + 4 * i;
         const uint32_t op = nd[0], slot = nd[3] & RES_SLOT_MASK;
@@ -548,45 +507,7 @@ int sg_eval_constraints(sg_ctx* c, void* stream, const sg_device_program* prog, 
         if (bytes) memcpy(blob.data() + off, p, bytes);
         return off;
     };
-    // The walk's micro-ops (see exec_node): each node re-encoded with its
-    // operand sources in the opcode and its constraint index in the node.
-    std::vector<uint32_t> mops(4ull * nn);
-    auto src_kind = [](uint32_t enc) -> uint32_t {
-        const uint32_t k = enc >> OPK_SHIFT;
-        return k == OPK_BASE_SLOT ? 0 : k == OPK_BASE_CONST ? 1 : 2;
-    };
-    auto src_payload = [](uint32_t enc) -> uint32_t {
-        return (enc >> OPK_SHIFT) == OPK_VAR ? enc & (VAR_COL_MASK | (0xFFu << VAR_OFF_SHIFT)) : enc & OPK_PAYLOAD_MASK;
-    };
-    for (uint32_t i = 0; i < nn; ++i) {
-        const uint32_t* nd = prog->nodes + 4 * i;
-        const uint32_t op = nd[0];
-        const bool rx = (nd[3] & RES_EXT_BIT) != 0;
-        uint32_t m, y = nd[1], z = nd[2];
-        if (op == OP_VAR) {
-            m = ((nd[2] >> 16) & 1u) ? M_VAR_MAIN : M_VAR_AUX;
-            y = (nd[1] & 0xFFFFu) | (((nd[2] >> 8) & 0xFFu) << VAR_OFF_SHIFT);
-            z = 0;
-        } else if (op == OP_CONST_BASE) {
-            m = M_CONST;
-        } else if (!rx && op >= OP_ADD && op <= OP_MUL) {
-            m = M_BIN + 9 * (op - OP_ADD) + 3 * src_kind(nd[1]) + src_kind(nd[2]);
-            y = src_payload(nd[1]);
-            z = src_payload(nd[2]);
-        } else if (!rx && op == OP_NEG) {
-            m = M_NEG + src_kind(nd[1]);
-            y = src_payload(nd[1]);
-            z = 0;
-        } else {
-            m = M_GEN + op;
-        }
-        const uint32_t c = prog->node_roots ? prog->node_roots[i] : NO_ROOT;
-        mops[4 * i] = m | (c != NO_ROOT ? M_ROOT_BIT | (c << M_ROOT_SHIFT) : 0u);
-        mops[4 * i + 1] = y;
-        mops[4 * i + 2] = z;
-        mops[4 * i + 3] = nd[3];
-    }
-    const size_t o_nodes = put(mops.data(), 16ull * nn);
+    const size_t o_nodes = put(prog->nodes, 16ull * nn);
     const size_t o_roots = put(prog->roots, 4ull * nr);
     const size_t o_nroots = prog->node_roots ? put(prog->node_roots, 4ull * nn) : 0;
     const size_t o_bc = put(prog->base_consts, 8ull * prog->num_base_consts);
