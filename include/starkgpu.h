@@ -366,7 +366,12 @@ typedef struct {
     uint32_t num_base_slots;
     uint32_t num_ext_slots;
     const uint32_t* node_roots; /* NULL, or num_nodes entries (streaming program) */
+    uint32_t hand_kernel;       /* 0, or SG_AIR_KECCAK: constraints [0, hand_roots) are the KECCAK chip
+                                   table's, evaluated by the library's own kernel (main width 2605); the
+                                   nodes complete the rest */
+    uint32_t hand_roots;
 } sg_device_program;
+#define SG_AIR_KECCAK 1u
 
 /* Composition accumulation (CompositionAccum, crypto/math-cuda/src/constraint_interp.rs:157). */
 typedef struct {

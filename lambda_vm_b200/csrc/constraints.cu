@@ -30,6 +30,7 @@
 
 #include "common.cuh"
 #include "gl.cuh"
+#include "keccak_air.cuh"
 
 namespace sg {
 
@@ -308,7 +309,7 @@ struct Comp {
 // mode 0: composition H(row); mode 1: per-constraint matrix evals[c*rows + row].
 __global__ void k_constraints(const uint4* nodes, uint32_t num_nodes, const uint32_t* roots, uint32_t num_roots,
                               const uint32_t* node_roots, uint32_t nbs, uint32_t nes, Uni u, Trace t, Comp cp,
-                              int mode, uint64_t* out, uint64_t* gscratch) {
+                              int mode, uint64_t* out, uint64_t* gscratch, const uint64_t* extra) {
     extern __shared__ uint64_t shs[];
     const uint64_t T = blockDim.x;
     SlotFile f;
@@ -325,7 +326,7 @@ __global__ void k_constraints(const uint4* nodes, uint32_t num_nodes, const uint
     }
     for (uint64_t row = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; row < t.rows;
          row += (uint64_t)gridDim.x * blockDim.x) {
-        fe3 sum{0, 0, 0};
+        fe3 sum = extra ? fe3{extra[3 * row], extra[3 * row + 1], extra[3 * row + 2]} : fe3{0, 0, 0};
         walk(nodes, num_nodes, u, f, t, row, Sink{node_roots, cp.beta, mode, out}, &sum);
         if (node_roots && mode == 1) continue;
         if (mode == 1) {
@@ -478,16 +479,22 @@ int sg_eval_constraints(sg_ctx* c, void* stream, const sg_device_program* prog, 
         if (op == OP_RAP_CHALLENGE) SG_CHECK_ARG(nd[1] < n_rap, "challenge index");
         if (op == OP_ALPHA_POW) SG_CHECK_ARG(nd[1] < n_alpha, "alpha index");
     }
+    const uint32_t hand = prog->hand_kernel ? prog->hand_roots : 0;
+    if (prog->hand_kernel) {
+        SG_CHECK_ARG(prog->hand_kernel == SG_AIR_KECCAK && prog->node_roots, "unknown hand kernel");
+        SG_CHECK_ARG(hand == KAIR_CONSTRAINTS && nr >= hand && m == KAIR_WIDTH, "not the KECCAK table's program");
+    }
     if (prog->node_roots) {
         // streaming: every constraint completed by exactly one instruction
+        // (those of a hand kernel by none)
         std::vector<uint8_t> seen(nr, 0);
         for (uint32_t i = 0; i < nn; ++i) {
             const uint32_t c = prog->node_roots[i];
             if (c == NO_ROOT) continue;
-            SG_CHECK_ARG(c < nr && !seen[c], "node_roots: constraint index out of range or repeated");
+            SG_CHECK_ARG(c < nr && c >= hand && !seen[c], "node_roots: constraint index out of range or repeated");
             seen[c] = 1;
         }
-        for (uint32_t c = 0; c < nr; ++c) SG_CHECK_ARG(seen[c], "node_roots: a constraint no instruction completes");
+        for (uint32_t c = hand; c < nr; ++c) SG_CHECK_ARG(seen[c], "node_roots: a constraint no instruction completes");
     } else {
         for (uint32_t r = 0; r < nr; ++r) {
             const uint32_t e = prog->roots[r];
@@ -555,8 +562,8 @@ int sg_eval_constraints(sg_ctx* c, void* stream, const sg_device_program* prog, 
         // at least m operands; skipped when the budget has no room for it.
         uint64_t* d_cm = nullptr;
         const uint64_t cm_bytes = rows * m * 8;
-        if (prog->node_roots && m >= CM_MIN_COLS && main_reads >= m && rows >= 32 && rows / 32 <= 0x7FFFFFFFull &&
-            m / 32 < 65535) {
+        if (prog->node_roots && m >= CM_MIN_COLS && (main_reads >= m || hand) && rows >= 32 &&
+            rows / 32 <= 0x7FFFFFFFull && m / 32 < 65535) {
             if (dev_alloc(ctx, st, cm_bytes, (void**)&d_cm) == SG_OK) {
                 k_to_columns<<<dim3((unsigned)((rows + 31) / 32), (unsigned)((m + 31) / 32)), dim3(32, 8), 0, st>>>(
                     d_main, rows, m, d_cm);
@@ -574,11 +581,25 @@ int sg_eval_constraints(sg_ctx* c, void* stream, const sg_device_program* prog, 
         const size_t smem = use_smem ? per_thread * T * 8 : 0;
         if (smem > 48 * 1024) cudaFuncSetAttribute(k_constraints, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         const uint32_t* d_nroots = prog->node_roots ? (const uint32_t*)(d_blob + o_nroots) : nullptr;
+        // the KECCAK table's own constraints first: per-row sums the walk starts
+        // from (composition), or their values written directly (per constraint)
+        uint64_t* d_extra = nullptr;
+        const uint64_t extra_bytes = rows * 24;
+        if (rc == SG_OK && hand) {
+            if (comp) rc = dev_alloc(ctx, st, extra_bytes, (void**)&d_extra);
+            if (rc == SG_OK) {
+                const uint64_t hb = (rows + 127) / 128, hcap = 148ull * 16;
+                k_keccak_constraints<<<(unsigned)(hb < hcap ? hb : hcap), 128, 0, st>>>(
+                    d_cm, d_main, rows, next_step, keccak_consts(), d_blob + o_beta, comp ? 0 : 1,
+                    comp ? d_extra : d_out);
+                rc = check_launch(ctx, "k_keccak_constraints");
+            }
+        }
         if (rc == SG_OK) {
             k_constraints<<<(unsigned)blocks, T, smem, st>>>((const uint4*)(d_blob + o_nodes), nn,
                                                              (const uint32_t*)(d_blob + o_roots), nr, d_nroots, nbs,
                                                              nes, u, t, cp, comp ? 0 : 1, d_out,
-                                                             use_smem ? nullptr : d_scr);
+                                                             use_smem ? nullptr : d_scr, d_extra);
             rc = check_launch(ctx, "k_constraints");
         }
         if (rc == SG_OK && cudaStreamSynchronize(st) != cudaSuccess) {
@@ -586,6 +607,7 @@ int sg_eval_constraints(sg_ctx* c, void* stream, const sg_device_program* prog, 
             rc = SG_ERR_CUDA;
         }
         if (d_cm) dev_free(ctx, st, d_cm, cm_bytes);
+        if (d_extra) dev_free(ctx, st, d_extra, extra_bytes);
     }
     if (d_scr) dev_free(ctx, st, d_scr, sb);
     dev_free(ctx, st, d_blob, bb);

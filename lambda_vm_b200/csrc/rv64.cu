@@ -23,6 +23,7 @@
 
 #include "common.cuh"
 #include "gl.cuh"
+#include "keccak_air.cuh"
 
 namespace {
 
@@ -91,43 +92,9 @@ bool decode(uint32_t w, Ins* o) {
     return true;
 }
 
-// keccak-f[1600] on the host, its round constants and rotation offsets
-// derived from their definitions in FIPS 202 (the rc(t) LFSR over
-// x^8 + x^6 + x^5 + x^4 + 1, the (x, y) -> (y, 2x + 3y) walk).
-struct KeccakTables {
-    uint64_t rc[24];
-    int rot[25];  // by lane x + 5y
-    KeccakTables() {
-        auto rc_bit = [](int t) {
-            if (t % 255 == 0) return 1u;
-            unsigned r = 1;
-            for (int i = 0; i < t % 255; ++i) {
-                r <<= 1;
-                if (r & 0x100) r ^= 0x171;
-            }
-            return r & 1u;
-        };
-        for (int ir = 0; ir < 24; ++ir) {
-            uint64_t c = 0;
-            for (int j = 0; j < 7; ++j) c |= (uint64_t)rc_bit(j + 7 * ir) << ((1 << j) - 1);
-            rc[ir] = c;
-        }
-        rot[0] = 0;
-        int x = 1, y = 0;
-        for (int t = 0; t < 24; ++t) {
-            rot[x + 5 * y] = ((t + 1) * (t + 2) / 2) % 64;
-            const int nx = y, ny = (2 * x + 3 * y) % 5;
-            x = nx, y = ny;
-        }
-    }
-};
-const KeccakTables& ktab() {
-    static const KeccakTables t;
-    return t;
-}
 uint64_t rotl(uint64_t v, int r) { return r ? (v << r) | (v >> (64 - r)) : v; }
 void keccak_f(uint64_t a[25]) {
-    const KeccakTables& k = ktab();
+    const sg::KeccakTables& k = sg::keccak_tables();
     for (int ir = 0; ir < 24; ++ir) {
         uint64_t c[5], d[5], b[25];
         for (int x = 0; x < 5; ++x) c[x] = a[x] ^ a[x + 5] ^ a[x + 10] ^ a[x + 15] ^ a[x + 20];
@@ -289,11 +256,6 @@ constexpr int KW = 2605;  // KECCAK table columns
 constexpr int K_A = 24, K_C = 124, K_CP = 444, K_AP = 764, K_OUT = 2364, K_B00 = 2464, K_BASE = 2528, K_CLK = 2529,
               K_TOLD = 2530, K_TD = 2555;
 constexpr int K_SLOTS = 86;  // per round: A[25], C[5], C'[5], A'[25], OUT[25], chi lane 0 before iota
-
-struct KeccakConsts {
-    uint64_t rc[24];
-    int rot[25];
-};
 
 // One CTA per ecall: thread 0 runs the 24 rounds into shared memory, then the
 // CTA writes the ecall's 24 rows, consecutive threads on consecutive columns.
@@ -553,9 +515,7 @@ extern "C" int sg_rv64_keccak_table(sg_ctx* c, void* stream, const uint64_t* cal
         return SG_ERR_CUDA;
     }
     if (!count) return SG_OK;
-    KeccakConsts kc;
-    for (int i = 0; i < 24; ++i) kc.rc[i] = ktab().rc[i];
-    for (int i = 0; i < 25; ++i) kc.rot[i] = ktab().rot[i];
+    const KeccakConsts kc = keccak_consts();
     uint64_t* d_ev = nullptr;
     SG_TRY(upload_events(ctx, st, calls, 52 * count, &d_ev));
     const unsigned grid = (unsigned)std::min<uint64_t>(count, 148ull * 16);

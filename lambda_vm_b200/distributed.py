@@ -14,7 +14,7 @@ processing time first), with a table's weight its LDE cells.
 import torch.distributed as dist
 
 from . import field as F
-from .ir import lowered
+from .ir import device_program, lowered
 from .stark import Options, _gen_trace, _u64le, prove_table
 
 
@@ -73,7 +73,7 @@ def multi_prove_distributed(airs, sources, opts=None, bk=None, group=None,
         if len(airs) > 1:
             ti.append_bytes(_u64le(i))
         tm, lde, tree, root = local[i]
-        p = prove_table(bk, airs[i], lowered(airs[i].program), tm, lde, tree, ti, challenges, alpha_pows, opts)
+        p = prove_table(bk, airs[i], lowered(device_program(airs[i])), tm, lde, tree, ti, challenges, alpha_pows, opts)
         p["main_root"] = root
         proofs[i] = p
         bk.free(tm, lde, tree)

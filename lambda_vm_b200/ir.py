@@ -117,6 +117,9 @@ def lower(prog, stream=True):
     one extra copy instruction per further constraint. Only intermediate
     values occupy slots, so the slot file stays small whatever the width."""
     nodes, dims, roots = prog["nodes"], prog["dims"], prog["roots"]
+    # a device program may name its constraints' indices in a larger program
+    # whose first constraints a hand-written kernel evaluates (prog["hand"])
+    index = prog.get("root_index", list(range(len(roots))))
     n = len(nodes)
     base_consts = list(prog["base_consts"])
     used = [False] * n
@@ -130,7 +133,7 @@ def lower(prog, stream=True):
     for c, r in enumerate(roots):
         is_root[r] = True
         used[r] = True
-        root_ids[r].append(c)
+        root_ids[r].append(index[c])
     leaf = [_uniform(nodes[i]) or (stream and nodes[i][0] == "var") for i in range(n)]
     emitted = [used[i] and (not leaf[i] or is_root[i]) for i in range(n)]
     if stream:
@@ -225,6 +228,10 @@ def lower(prog, stream=True):
            "num_base_slots": count[BASE], "num_ext_slots": count[EXT]}
     if stream:
         low["node_roots"] = np.array(node_roots, np.uint32)
+    if "hand" in prog:
+        assert stream, "a hand kernel's program is a streaming program"
+        low["hand_kernel"], low["hand_roots"] = prog["hand"]
+        low["num_roots"] = prog["hand"][1] + len(roots)
     return low
 
 
@@ -235,3 +242,10 @@ def lowered(prog):
     if low is None:
         low = prog["_lowered"] = lower(prog)
     return low
+
+
+def device_program(air):
+    """The program the GPU prover runs for `air`: its device_program when it
+    has one (a program whose first constraints a hand-written kernel
+    evaluates), else its constraint program."""
+    return getattr(air, "device_program", None) or air.program

@@ -461,10 +461,12 @@ def _program_struct(lowered, keep):
     p.ext_consts = arr(lowered["ext_consts"], np.uint64)
     p.num_ext_consts = int(np.asarray(lowered["ext_consts"]).size // 3)
     p.roots = arr(lowered["roots"], np.uint32)
-    p.num_roots = int(np.asarray(lowered["roots"]).size)
+    p.num_roots = int(lowered.get("num_roots", np.asarray(lowered["roots"]).size))
     p.num_base_slots = int(lowered["num_base_slots"])
     p.num_ext_slots = int(lowered["num_ext_slots"])
     p.node_roots = arr(lowered["node_roots"], np.uint32) if lowered.get("node_roots") is not None else None
+    p.hand_kernel = int(lowered.get("hand_kernel", 0))
+    p.hand_roots = int(lowered.get("hand_roots", 0))
     return p
 
 

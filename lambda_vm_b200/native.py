@@ -63,7 +63,8 @@ class DeviceProgram(C.Structure):
     _fields_ = [("nodes", C.c_void_p), ("num_nodes", C.c_uint32), ("base_consts", C.c_void_p),
                 ("num_base_consts", C.c_uint32), ("ext_consts", C.c_void_p), ("num_ext_consts", C.c_uint32),
                 ("roots", C.c_void_p), ("num_roots", C.c_uint32), ("num_base_slots", C.c_uint32),
-                ("num_ext_slots", C.c_uint32), ("node_roots", C.c_void_p)]
+                ("num_ext_slots", C.c_uint32), ("node_roots", C.c_void_p), ("hand_kernel", C.c_uint32),
+                ("hand_roots", C.c_uint32)]
 
 
 class Composition(C.Structure):

@@ -824,6 +824,24 @@ class KeccakAir(BusAir):
             its.append({"bus": BUS_RANGE, "sender": True, "mult": _col(KR), "elems": [_col(KTD + j)]})
         self._logup_setup(its)
         self.program = self._program(("keccak",))
+        self.device_program = self._device_program()
+
+    def _device_program(self):
+        """The GPU prover's program: the library's KECCAK kernel
+        (SG_AIR_KECCAK) evaluates the first 3383 constraints, this program's
+        nodes the LogUp constraints, under their indices in `program`."""
+        key = ("keccak-device",)
+        if key not in _PROGRAMS:
+            nb = self.program["num_base"]
+            assert nb == 3383 and len(self.program["roots"]) == nb + self.num_committed + 1
+            b = Builder()
+            self._emit_logup(b)
+            prog = b.program()
+            assert prog["num_base"] == 0
+            prog["root_index"] = [nb + c for c in range(len(prog["roots"]))]
+            prog["hand"] = (1, nb)
+            _PROGRAMS[key] = prog
+        return _PROGRAMS[key]
 
     def _build_program(self):
         b = Builder()

@@ -23,7 +23,7 @@ import numpy as np
 from . import field as F
 from . import native
 from .device import backend as _backend
-from .ir import lowered
+from .ir import device_program, lowered
 from .stark import GpuBackend, Options, _gen_trace, _u64le, prove_table
 
 
@@ -166,7 +166,7 @@ def multi_prove_scheduled(airs, sources, opts=None, workers=8, budget_bytes=None
             bk = pool.take()
             tm, lde, tree, root, release = r1[i]
             try:
-                p = prove_table(bk, airs[i], lowered(airs[i].program), tm, lde, tree, forks[i], challenges, alpha_pows,
+                p = prove_table(bk, airs[i], lowered(device_program(airs[i])), tm, lde, tree, forks[i], challenges, alpha_pows,
                                 opts)
                 p["main_root"] = root
                 proofs[i] = p

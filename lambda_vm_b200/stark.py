@@ -32,7 +32,7 @@ from . import field as F
 from . import math_cuda as mc
 from . import native
 from .device import DeviceBuffer, backend as _backend
-from .ir import lowered
+from .ir import device_program, lowered
 
 P = F.P
 
@@ -566,11 +566,12 @@ def prove_table(bk, air, lowered, trace_mat, main_lde, main_tree, t, challenges,
     proof["table_contribution"] = Lc
     # ---- R2
     beta = F.f3(t.sample_ext3())
-    ncons = len(lowered["roots"]) + len(air.boundary)
+    nroots = lowered.get("num_roots", len(lowered["roots"]))
+    ncons = nroots + len(air.boundary)
     coefs = [(1, 0, 0)]
     for _ in range(ncons - 1):
         coefs.append(F.f3mul(coefs[-1], beta))
-    beta_t, beta_b = coefs[:len(lowered["roots"])], coefs[len(lowered["roots"]):]
+    beta_t, beta_b = coefs[:nroots], coefs[nroots:]
     offset = F.f3scale(Lc, F.inv_int(n))
     boundary = [(col, is_aux, (0, 0, 0), beta_b[i]) for i, (col, is_aux, _row) in enumerate(air.boundary)]
     H = bk.composition(air.program, lowered, main_lde, aux_lde, [challenges[0], challenges[1]], alpha_pows, offset, B,
@@ -721,7 +722,7 @@ def multi_prove(airs, traces, opts=None, bk=None, label=b"lambda_vm_b200/synthet
         forks.append(ti)
     proofs = []
     for i, (air, tm, lde, tree, root) in enumerate(tabs):
-        p = prove_table(bk, air, lowered(air.program), tm, lde, tree, forks[i], challenges, alpha_pows, opts)
+        p = prove_table(bk, air, lowered(device_program(air)), tm, lde, tree, forks[i], challenges, alpha_pows, opts)
         p["main_root"] = root
         proofs.append(p)
         bk.free(tm, lde, tree)

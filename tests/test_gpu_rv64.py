@@ -112,3 +112,33 @@ def test_device_chip_tables_equal_the_host_tables(be):
     same(ssrc, sair, ssrc.host_trace(sair))
     empty = RA.ShiftSource(np.zeros((0, 3), np.uint64))
     same(empty, RA.ShiftAir(6), empty.host_trace(RA.ShiftAir(6)))
+
+
+@pytest.mark.parametrize("rows,step", [(256, 2), (1024, 4)])
+def test_keccak_table_kernel_equals_the_walk(be, rows, step):
+    """The KECCAK table's hand-written constraint kernel (SG_AIR_KECCAK, the
+    first 3383 constraints) with the walk for the LogUp constraints, against
+    the walk of the table's whole program, on random field elements (not a
+    valid trace: every constraint value is compared): each constraint's value
+    and the composition with boundary terms, exactly."""
+    import numpy as np
+    from lambda_vm_b200 import math_cuda as mc
+    from lambda_vm_b200.ir import lower
+    P_ = 0xFFFFFFFF00000001
+    rng = np.random.default_rng(rows)
+    rf = lambda shape: np.where((x := rng.integers(0, 2**64, size=shape, dtype=np.uint64)) >= np.uint64(P_),
+                                x - np.uint64(P_), x)
+    air = RA.KeccakAir(8)
+    full, dev = lower(air.program), lower(air.device_program)
+    assert dev["hand_kernel"] == 1 and dev["num_roots"] == len(full["roots"]) == 3434
+    main = rf((rows, air.width))
+    aux = rf((rows, 3 * air.aux_width))
+    rap, alpha, off = rf((2, 3)), rf((air.max_alpha, 3)), rf((3,))
+    a = mc.eval_constraints_on_device(full, main, aux, rap, alpha, off, step, None, be)
+    b = mc.eval_constraints_on_device(dev, main, aux, rap, alpha, off, step, None, be)
+    assert a.shape == b.shape and np.array_equal(a, b)
+    comp = {"beta": rf((3434, 3)), "z_inv": rf((rows // 4,)),
+            "boundary": [(air.acc_col, True, rf((3,)), rf((3,)))], "b_z_inv": rf((1, rows))}
+    ha = mc.eval_constraints_on_device(full, main, aux, rap, alpha, off, step, comp, be)
+    hb = mc.eval_constraints_on_device(dev, main, aux, rap, alpha, off, step, comp, be)
+    assert np.array_equal(ha, hb)

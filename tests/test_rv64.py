@@ -257,3 +257,18 @@ def test_statement_binds_the_chip_heights():
     fw = rv64.fib_program(9)
     _, _, fp = RA.build(fw)
     assert fp["label"] == RA.statement_label(fw, fp["counts"], fp["output"])
+
+
+def test_keccak_device_program_covers_the_logup_constraints():
+    """The KECCAK table's device program: the LogUp constraints only, under
+    their indices in the whole program (after its 3383 base constraints, which
+    the library's kernel evaluates), every one completed once."""
+    from lambda_vm_b200.ir import lower
+    air = RA.KeccakAir(6)
+    full = air.program
+    dev = lower(air.device_program)
+    nb = full["num_base"]
+    assert nb == 3383 and dev["hand_kernel"] == 1 and dev["hand_roots"] == nb
+    assert dev["num_roots"] == len(full["roots"])
+    done = sorted(int(c) for c in dev["node_roots"] if c != 0xFFFFFFFF)
+    assert done == list(range(nb, len(full["roots"])))
