@@ -670,24 +670,28 @@ class ShiftAir(BusAir):
         b.emit(b.sub(x.total(s), x.one))
         b.emit(b.sub(x.total(q), x.one))
 
-        def shifted(src, j, k_):
-            """Bit j of src shifted by k_ in the row's direction (None: zero either way)."""
+        def shifted(src, j, k_, size=64):
+            """Element j of src (size elements) shifted by k_ in the row's
+            direction (None: zero either way)."""
             parts = []
             if j - k_ >= 0:
                 parts.append(b.mul(nd, src[j - k_]))
-            if j + k_ < 64:
+            if j + k_ < size:
                 parts.append(b.mul(d, src[j + k_]))
             return x.total(parts) if parts else None
 
         for j in range(64):
             terms = [b.mul(s[k_], e) for k_ in range(8) if (e := shifted(a, j, k_)) is not None]
             b.emit(b.sub(tb[j], x.total(terms)))
+        # the second stage moves whole bytes: with TB's bytes tB[i] = sum_j 2^j
+        # TB_(8i+j), r's byte k is sum_q Q_q tB[k -+ q] (the same polynomial as
+        # the bit-by-bit sum, with 16 products a limb instead of 256)
+        tB = [x.total([x.scaled(1 << j, tb[8 * i + j]) for j in range(8)]) for i in range(8)]
         for limb, col in ((0, self.R_LO), (1, self.R_HI)):
             acc = []
-            for i in range(32 * limb, 32 * limb + 32):
-                terms = [b.mul(q[k_], e) for k_ in range(8) if (e := shifted(tb, i, 8 * k_)) is not None]
-                if terms:
-                    acc.append(x.scaled(1 << (i - 32 * limb), x.total(terms)))
+            for k in range(4 * limb, 4 * limb + 4):
+                terms = [b.mul(q[k_], e) for k_ in range(8) if (e := shifted(tB, k, k_, 8)) is not None]
+                acc.append(x.scaled(1 << (8 * (k - 4 * limb)), x.total(terms)))
             b.emit(b.sub(M(col), x.total(acc)))
         self._emit_logup(b)
         return b.program()
