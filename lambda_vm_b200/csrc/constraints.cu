@@ -264,7 +264,7 @@ __device__ __forceinline__ void exec_node(const uint4 nd, uint32_t i, uint64_t v
     }
 }
 
-constexpr int PF = 4;             // prefetch distance, in nodes
+constexpr int PF = 1;             // prefetch distance, in nodes (1, 2, 4, 8 measured: 1 is fastest)
 constexpr uint64_t CM_MIN_COLS = 32;  // narrower main LDEs are walked row-major
 
 __device__ __forceinline__ void walk(const uint4* nodes, uint32_t num_nodes, const Uni& u, const SlotFile& f,
