@@ -366,12 +366,15 @@ typedef struct {
     uint32_t num_base_slots;
     uint32_t num_ext_slots;
     const uint32_t* node_roots; /* NULL, or num_nodes entries (streaming program) */
-    uint32_t hand_kernel;       /* 0, or SG_AIR_KECCAK: constraints [0, hand_roots) are the KECCAK chip
-                                   table's, evaluated by the library's own kernel (main width 2605); the
-                                   nodes complete the rest */
+    uint32_t hand_kernel;       /* 0; SG_AIR_KECCAK: constraints [0, hand_roots) are the KECCAK chip
+                                   table's (main width 2605); SG_AIR_CPU | chips << 8: the RV64 CPU table's
+                                   with that chip set (width 200 without chips, else 234; chips as
+                                   SG_RV64_CHIP_*). The library's own kernel evaluates those; the nodes
+                                   complete the rest */
     uint32_t hand_roots;
 } sg_device_program;
 #define SG_AIR_KECCAK 1u
+#define SG_AIR_CPU 2u
 
 /* Composition accumulation (CompositionAccum, crypto/math-cuda/src/constraint_interp.rs:157). */
 typedef struct {

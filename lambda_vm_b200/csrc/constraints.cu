@@ -30,6 +30,7 @@
 
 #include "common.cuh"
 #include "gl.cuh"
+#include "cpu_air.cuh"
 #include "keccak_air.cuh"
 
 namespace sg {
@@ -480,9 +481,17 @@ int sg_eval_constraints(sg_ctx* c, void* stream, const sg_device_program* prog, 
         if (op == OP_ALPHA_POW) SG_CHECK_ARG(nd[1] < n_alpha, "alpha index");
     }
     const uint32_t hand = prog->hand_kernel ? prog->hand_roots : 0;
+    const uint32_t hand_id = prog->hand_kernel & 0xFFu, hand_chips = prog->hand_kernel >> 8;
     if (prog->hand_kernel) {
-        SG_CHECK_ARG(prog->hand_kernel == SG_AIR_KECCAK && prog->node_roots, "unknown hand kernel");
-        SG_CHECK_ARG(hand == KAIR_CONSTRAINTS && nr >= hand && m == KAIR_WIDTH, "not the KECCAK table's program");
+        SG_CHECK_ARG(prog->node_roots && nr >= hand, "a hand kernel needs a streaming program");
+        if (hand_id == SG_AIR_KECCAK)
+            SG_CHECK_ARG(hand == KAIR_CONSTRAINTS && m == KAIR_WIDTH && !hand_chips, "not the KECCAK table's program");
+        else if (hand_id == SG_AIR_CPU)
+            SG_CHECK_ARG(hand_chips < 16 && hand == cpu_air_constraints(hand_chips) &&
+                             m == (hand_chips ? CPU_FULL_WIDTH : CPU_CORE_WIDTH),
+                         "not the CPU table's program");
+        else
+            SG_CHECK_ARG(false, "unknown hand kernel");
     }
     if (prog->node_roots) {
         // streaming: every constraint completed by exactly one instruction
@@ -589,10 +598,16 @@ int sg_eval_constraints(sg_ctx* c, void* stream, const sg_device_program* prog, 
             if (comp) rc = dev_alloc(ctx, st, extra_bytes, (void**)&d_extra);
             if (rc == SG_OK) {
                 const uint64_t hb = (rows + 127) / 128, hcap = 148ull * 16;
-                k_keccak_constraints<<<(unsigned)(hb < hcap ? hb : hcap), 128, 0, st>>>(
-                    d_cm, d_main, rows, next_step, keccak_consts(), d_blob + o_beta, comp ? 0 : 1,
-                    comp ? d_extra : d_out);
-                rc = check_launch(ctx, "k_keccak_constraints");
+                const unsigned grid = (unsigned)(hb < hcap ? hb : hcap);
+                if (hand_id == SG_AIR_KECCAK) {
+                    k_keccak_constraints<<<grid, 128, 0, st>>>(d_cm, d_main, rows, next_step, keccak_consts(),
+                                                               d_blob + o_beta, comp ? 0 : 1, comp ? d_extra : d_out);
+                    rc = check_launch(ctx, "k_keccak_constraints");
+                } else {
+                    k_cpu_constraints<<<grid, 128, 0, st>>>(d_cm, d_main, m, rows, next_step, hand_chips,
+                                                            d_blob + o_beta, comp ? 0 : 1, comp ? d_extra : d_out);
+                    rc = check_launch(ctx, "k_cpu_constraints");
+                }
             }
         }
         if (rc == SG_OK) {

@@ -316,6 +316,24 @@ class CpuAir(BusAir):
                         "elems": [_col(CLK), _col(MA)]})
         self._logup_setup(its)
         self.program = self._program(("cpu", self.chips))
+        self.device_program = self._device_program()
+
+    def _device_program(self):
+        """The GPU prover's program: the library's CPU-table kernel (SG_AIR_CPU
+        with this chip set) evaluates the base constraints, this program's
+        nodes the LogUp constraints, under their indices in `program`."""
+        key = ("cpu-device", self.chips)
+        if key not in _PROGRAMS:
+            nb = self.program["num_base"]
+            b = Builder()
+            self._emit_logup(b)
+            prog = b.program()
+            assert prog["num_base"] == 0 and nb + len(prog["roots"]) == len(self.program["roots"])
+            prog["root_index"] = [nb + c for c in range(len(prog["roots"]))]
+            mask = sum(1 << i for i, c in enumerate(CHIPS) if c in self.chips)
+            prog["hand"] = (2 | (mask << 8), nb)
+            _PROGRAMS[key] = prog
+        return _PROGRAMS[key]
 
     def _build_program(self):
         b = Builder()

@@ -142,3 +142,33 @@ def test_keccak_table_kernel_equals_the_walk(be, rows, step):
     ha = mc.eval_constraints_on_device(full, main, aux, rap, alpha, off, step, comp, be)
     hb = mc.eval_constraints_on_device(dev, main, aux, rap, alpha, off, step, comp, be)
     assert np.array_equal(ha, hb)
+
+
+@pytest.mark.parametrize("chips", [(), ("bitwise", "shift", "memory", "keccak"), ("shift",), ("memory",),
+                                   ("bitwise", "memory", "keccak")])
+def test_cpu_table_kernel_equals_the_walk(be, chips):
+    """The CPU table's hand-written constraint kernel (SG_AIR_CPU with the
+    chip set) with the walk for the LogUp constraints, against the walk of
+    the table's whole program, on random field elements: every constraint's
+    value and the composition with its boundary term, exactly."""
+    import numpy as np
+    from lambda_vm_b200 import math_cuda as mc
+    from lambda_vm_b200.ir import lower
+    P_ = 0xFFFFFFFF00000001
+    rng = np.random.default_rng(len(chips) + 7)
+    rf = lambda shape: np.where((x := rng.integers(0, 2**64, size=shape, dtype=np.uint64)) >= np.uint64(P_),
+                                x - np.uint64(P_), x)
+    air = RA.CpuAir(rv64.keccak_program(136), 9, chips)
+    full, dev = lower(air.program), lower(air.device_program)
+    assert dev["hand_kernel"] & 0xFF == 2 and dev["num_roots"] == len(full["roots"])
+    rows, step = 512, 2
+    main = rf((rows, air.width))
+    aux = rf((rows, 3 * air.aux_width))
+    rap, alpha, off = rf((2, 3)), rf((air.max_alpha, 3)), rf((3,))
+    a = mc.eval_constraints_on_device(full, main, aux, rap, alpha, off, step, None, be)
+    b = mc.eval_constraints_on_device(dev, main, aux, rap, alpha, off, step, None, be)
+    assert a.shape == b.shape and np.array_equal(a, b)
+    comp = {"beta": rf((len(full["roots"]), 3)), "z_inv": rf((rows // 4,)),
+            "boundary": [(air.acc_col, True, rf((3,)), rf((3,)))], "b_z_inv": rf((1, rows))}
+    assert np.array_equal(mc.eval_constraints_on_device(full, main, aux, rap, alpha, off, step, comp, be),
+                          mc.eval_constraints_on_device(dev, main, aux, rap, alpha, off, step, comp, be))
