@@ -369,12 +369,13 @@ typedef struct {
     uint32_t hand_kernel;       /* 0; SG_AIR_KECCAK: constraints [0, hand_roots) are the KECCAK chip
                                    table's (main width 2605); SG_AIR_CPU | chips << 8: the RV64 CPU table's
                                    with that chip set (width 200 without chips, else 234; chips as
-                                   SG_RV64_CHIP_*). The library's own kernel evaluates those; the nodes
-                                   complete the rest */
+                                   SG_RV64_CHIP_*); SG_AIR_SHIFT: the SHIFT chip table's (width 148). The
+                                   library's own kernel evaluates those; the nodes complete the rest */
     uint32_t hand_roots;
 } sg_device_program;
 #define SG_AIR_KECCAK 1u
 #define SG_AIR_CPU 2u
+#define SG_AIR_SHIFT 3u
 
 /* Composition accumulation (CompositionAccum, crypto/math-cuda/src/constraint_interp.rs:157). */
 typedef struct {

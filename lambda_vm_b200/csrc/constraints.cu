@@ -486,6 +486,8 @@ int sg_eval_constraints(sg_ctx* c, void* stream, const sg_device_program* prog, 
         SG_CHECK_ARG(prog->node_roots && nr >= hand, "a hand kernel needs a streaming program");
         if (hand_id == SG_AIR_KECCAK)
             SG_CHECK_ARG(hand == KAIR_CONSTRAINTS && m == KAIR_WIDTH && !hand_chips, "not the KECCAK table's program");
+        else if (hand_id == SG_AIR_SHIFT)
+            SG_CHECK_ARG(hand == SH_CONSTRAINTS && m == SH_WIDTH && !hand_chips, "not the SHIFT table's program");
         else if (hand_id == SG_AIR_CPU)
             SG_CHECK_ARG(hand_chips < 16 && hand == cpu_air_constraints(hand_chips) &&
                              m == (hand_chips ? CPU_FULL_WIDTH : CPU_CORE_WIDTH),
@@ -603,6 +605,10 @@ int sg_eval_constraints(sg_ctx* c, void* stream, const sg_device_program* prog, 
                     k_keccak_constraints<<<grid, 128, 0, st>>>(d_cm, d_main, rows, next_step, keccak_consts(),
                                                                d_blob + o_beta, comp ? 0 : 1, comp ? d_extra : d_out);
                     rc = check_launch(ctx, "k_keccak_constraints");
+                } else if (hand_id == SG_AIR_SHIFT) {
+                    k_shift_constraints<<<grid, 128, 0, st>>>(d_cm, d_main, rows, next_step, d_blob + o_beta,
+                                                              comp ? 0 : 1, comp ? d_extra : d_out);
+                    rc = check_launch(ctx, "k_shift_constraints");
                 } else {
                     k_cpu_constraints<<<grid, 128, 0, st>>>(d_cm, d_main, m, rows, next_step, hand_chips,
                                                             d_blob + o_beta, comp ? 0 : 1, comp ? d_extra : d_out);

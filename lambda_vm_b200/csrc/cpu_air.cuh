@@ -1,4 +1,5 @@
-// The RV64 CPU table's layout, and its constraints as a hand-written kernel.
+// The RV64 CPU and SHIFT tables' layouts, and their constraints as
+// hand-written kernels.
 //
 // The CPU table (lambda_vm_b200/rv64_air.py CpuAir) has 200 or 234 columns
 // and ~300 base-field constraints (one-hot selectors, operand reads from the
@@ -196,6 +197,67 @@ static __global__ void k_cpu_constraints(const uint64_t* __restrict__ cm, const 
         for (uint32_t k = 1; k < 32; ++k) {
             s.put(gl::mul(nstep, w.N(cpu_xlo(k))));
             s.put(gl::mul(nstep, w.N(cpu_xlo(k) + 1)));
+        }
+        if (mode == 0) {
+            uint64_t* o = out + 3 * row;
+            o[0] = s.sum.c0, o[1] = s.sum.c1, o[2] = s.sum.c2;
+        }
+    }
+}
+
+// The SHIFT table (rv64_air.py ShiftAir): DIR, the operand's bits, one-hot
+// s = k mod 8 and q = k div 8, the operand shifted by s bits, the result's
+// limbs, the multiplicity. Its 149 base constraints in ShiftAir's order.
+constexpr uint32_t SH_DIR = 0, SH_AB = 1, SH_S = 65, SH_Q = 73, SH_TB = 81, SH_R_LO = 145, SH_R_HI = 146,
+                   SH_WIDTH = 148, SH_CONSTRAINTS = 149;
+
+static __global__ void k_shift_constraints(const uint64_t* __restrict__ cm, const uint64_t* __restrict__ rm,
+                                           uint64_t rows, uint64_t next_step, const uint64_t* __restrict__ beta,
+                                           int mode, uint64_t* __restrict__ out) {
+    for (uint64_t row = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; row < rows;
+         row += (uint64_t)gridDim.x * blockDim.x) {
+        const CRow w{cm, rm, rows, SH_WIDTH, row, row};
+        KSink s{beta, mode, out, rows, row, 0, gl::fe3{0, 0, 0}};
+        const uint64_t d = w.M(SH_DIR), nd = gl::sub(1, d);
+        s.put(kbool(d));
+        for (uint32_t i = 0; i < 64; ++i) s.put(kbool(w.M(SH_AB + i)));
+        for (uint32_t i = 0; i < 8; ++i) s.put(kbool(w.M(SH_S + i)));
+        for (uint32_t i = 0; i < 8; ++i) s.put(kbool(w.M(SH_Q + i)));
+        uint64_t ts = 0, tq = 0;
+        for (uint32_t i = 0; i < 8; ++i) ts = gl::add(ts, w.M(SH_S + i)), tq = gl::add(tq, w.M(SH_Q + i));
+        s.put(gl::sub(ts, 1));
+        s.put(gl::sub(tq, 1));
+        // TB_j = sum_s S_s (nd a[j - s] + d a[j + s]), bits past either end zero
+        for (int j = 0; j < 64; ++j) {
+            uint64_t t = 0;
+            for (int k = 0; k < 8; ++k) {
+                uint64_t e = 0;
+                if (j - k >= 0) e = gl::mul(nd, w.M(SH_AB + j - k));
+                if (j + k < 64) e = gl::add(e, gl::mul(d, w.M(SH_AB + j + k)));
+                t = gl::add(t, gl::mul(w.M(SH_S + k), e));
+            }
+            s.put(gl::sub(w.M(SH_TB + j), t));
+        }
+        // the result moves TB by whole bytes: byte k = sum_q Q_q (nd tB[k - q] + d tB[k + q])
+        uint64_t tB[8];
+        for (int i = 0; i < 8; ++i) {
+            uint64_t t = 0;
+            for (int j = 7; j >= 0; --j) t = gl::add(gl::add(t, t), w.M(SH_TB + 8 * i + j));
+            tB[i] = t;
+        }
+        for (int limb = 0; limb < 2; ++limb) {
+            uint64_t acc = 0;
+            for (int k = 4 * limb + 3; k >= 4 * limb; --k) {
+                uint64_t t = 0;
+                for (int q = 0; q < 8; ++q) {
+                    uint64_t e = 0;
+                    if (k - q >= 0) e = gl::mul(nd, tB[k - q]);
+                    if (k + q < 8) e = gl::add(e, gl::mul(d, tB[k + q]));
+                    t = gl::add(t, gl::mul(w.M(SH_Q + q), e));
+                }
+                acc = gl::add(gl::mul(acc, 256), t);
+            }
+            s.put(gl::sub(w.M(limb ? SH_R_HI : SH_R_LO), acc));
         }
         if (mode == 0) {
             uint64_t* o = out + 3 * row;

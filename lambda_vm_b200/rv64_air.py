@@ -60,6 +60,23 @@ CHIPS = ("bitwise", "shift", "memory", "keccak")
 _PROGRAMS = {}  # constraint programs by (table, parameters): a table's program depends on neither its height nor its trace
 
 
+def _hand_program(air, key, kernel):
+    """The GPU prover's program for a table whose base constraints a
+    hand-written library kernel evaluates (SG_AIR_* `kernel`): the LogUp
+    constraints only, under their indices in the table's whole program,
+    which come after its base constraints."""
+    if key not in _PROGRAMS:
+        nb = air.program["num_base"]
+        b = Builder()
+        air._emit_logup(b)
+        prog = b.program()
+        assert prog["num_base"] == 0 and nb + len(prog["roots"]) == len(air.program["roots"])
+        prog["root_index"] = [nb + c for c in range(len(prog["roots"]))]
+        prog["hand"] = (kernel, nb)
+        _PROGRAMS[key] = prog
+    return _PROGRAMS[key]
+
+
 class BusAir:
     """LogUp plumbing shared by the front-end tables. An interaction is
     {"bus", "elems": [lin], "mult": lin, "sender"} with lin = (const, [(coef,
@@ -316,24 +333,8 @@ class CpuAir(BusAir):
                         "elems": [_col(CLK), _col(MA)]})
         self._logup_setup(its)
         self.program = self._program(("cpu", self.chips))
-        self.device_program = self._device_program()
-
-    def _device_program(self):
-        """The GPU prover's program: the library's CPU-table kernel (SG_AIR_CPU
-        with this chip set) evaluates the base constraints, this program's
-        nodes the LogUp constraints, under their indices in `program`."""
-        key = ("cpu-device", self.chips)
-        if key not in _PROGRAMS:
-            nb = self.program["num_base"]
-            b = Builder()
-            self._emit_logup(b)
-            prog = b.program()
-            assert prog["num_base"] == 0 and nb + len(prog["roots"]) == len(self.program["roots"])
-            prog["root_index"] = [nb + c for c in range(len(prog["roots"]))]
-            mask = sum(1 << i for i, c in enumerate(CHIPS) if c in self.chips)
-            prog["hand"] = (2 | (mask << 8), nb)
-            _PROGRAMS[key] = prog
-        return _PROGRAMS[key]
+        mask = sum(1 << i for i, c in enumerate(CHIPS) if c in self.chips)
+        self.device_program = _hand_program(self, ("cpu-device", self.chips), 2 | (mask << 8))
 
     def _build_program(self):
         b = Builder()
@@ -672,6 +673,7 @@ class ShiftAir(BusAir):
         self._logup_setup([{"bus": BUS_SHIFT, "sender": False, "mult": _col(self.M),
                             "elems": [_col(self.DIR), alo, ahi, k, _col(self.R_LO), _col(self.R_HI)]}])
         self.program = self._program(("shift",))
+        self.device_program = _hand_program(self, ("shift-device",), 3)
 
     def _build_program(self):
         b = Builder()
@@ -846,24 +848,7 @@ class KeccakAir(BusAir):
             its.append({"bus": BUS_RANGE, "sender": True, "mult": _col(KR), "elems": [_col(KTD + j)]})
         self._logup_setup(its)
         self.program = self._program(("keccak",))
-        self.device_program = self._device_program()
-
-    def _device_program(self):
-        """The GPU prover's program: the library's KECCAK kernel
-        (SG_AIR_KECCAK) evaluates the first 3383 constraints, this program's
-        nodes the LogUp constraints, under their indices in `program`."""
-        key = ("keccak-device",)
-        if key not in _PROGRAMS:
-            nb = self.program["num_base"]
-            assert nb == 3383 and len(self.program["roots"]) == nb + self.num_committed + 1
-            b = Builder()
-            self._emit_logup(b)
-            prog = b.program()
-            assert prog["num_base"] == 0
-            prog["root_index"] = [nb + c for c in range(len(prog["roots"]))]
-            prog["hand"] = (1, nb)
-            _PROGRAMS[key] = prog
-        return _PROGRAMS[key]
+        self.device_program = _hand_program(self, ("keccak-device",), 1)
 
     def _build_program(self):
         b = Builder()

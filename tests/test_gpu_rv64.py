@@ -172,3 +172,27 @@ def test_cpu_table_kernel_equals_the_walk(be, chips):
             "boundary": [(air.acc_col, True, rf((3,)), rf((3,)))], "b_z_inv": rf((1, rows))}
     assert np.array_equal(mc.eval_constraints_on_device(full, main, aux, rap, alpha, off, step, comp, be),
                           mc.eval_constraints_on_device(dev, main, aux, rap, alpha, off, step, comp, be))
+
+
+def test_shift_table_kernel_equals_the_walk(be):
+    """The SHIFT table's hand-written constraint kernel (SG_AIR_SHIFT) against
+    the walk of its whole program, on random field elements, exactly."""
+    import numpy as np
+    from lambda_vm_b200 import math_cuda as mc
+    from lambda_vm_b200.ir import lower
+    P_ = 0xFFFFFFFF00000001
+    rng = np.random.default_rng(31)
+    rf = lambda shape: np.where((x := rng.integers(0, 2**64, size=shape, dtype=np.uint64)) >= np.uint64(P_),
+                                x - np.uint64(P_), x)
+    air = RA.ShiftAir(8)
+    full, dev = lower(air.program), lower(air.device_program)
+    assert dev["hand_kernel"] == 3 and dev["num_roots"] == len(full["roots"])
+    rows = 512
+    main, aux = rf((rows, air.width)), rf((rows, 3 * air.aux_width))
+    rap, alpha, off = rf((2, 3)), rf((air.max_alpha, 3)), rf((3,))
+    assert np.array_equal(mc.eval_constraints_on_device(full, main, aux, rap, alpha, off, 2, None, be),
+                          mc.eval_constraints_on_device(dev, main, aux, rap, alpha, off, 2, None, be))
+    comp = {"beta": rf((len(full["roots"]), 3)), "z_inv": rf((rows // 4,)),
+            "boundary": [(air.acc_col, True, rf((3,)), rf((3,)))], "b_z_inv": rf((1, rows))}
+    assert np.array_equal(mc.eval_constraints_on_device(full, main, aux, rap, alpha, off, 2, comp, be),
+                          mc.eval_constraints_on_device(dev, main, aux, rap, alpha, off, 2, comp, be))
