@@ -576,6 +576,15 @@ typedef struct {
 SG_API int sg_rv64_run(const uint32_t* words, uint32_t nwords, uint64_t max_steps, uint64_t n_rows,
                        uint64_t* rows_out, uint64_t* regs_out, uint64_t* counts_out, uint64_t* shifts_out,
                        uint64_t* cells_out, uint64_t* keccak_out, sg_rv64_info* info);
+/* sg_rv64_run, also counting the lookups as the machine runs (both need
+ * rows_out): range_counts (65536) gets how many times the CPU table (every
+ * one of its n_rows rows) and the KECCAK table look each 16-bit value up in
+ * RANGE; bitwise_counts (3 x 65536: XOR, OR, AND) how many times the CPU
+ * table looks each byte pair x << 8 | y up in BITWISE. */
+SG_API int sg_rv64_run_counted(const uint32_t* words, uint32_t nwords, uint64_t max_steps, uint64_t n_rows,
+                               uint64_t* rows_out, uint64_t* regs_out, uint64_t* counts_out, uint64_t* shifts_out,
+                               uint64_t* cells_out, uint64_t* keccak_out, uint64_t* range_counts,
+                               uint64_t* bitwise_counts, sg_rv64_info* info);
 /* The CPU table (n_rows x width u64, row-major, into device memory) written on
  * the device from sg_rv64_run's `count` row records and register snapshots
  * (host arrays): width SG_RV64_CPU_CORE_WIDTH (no chip instruction executed)

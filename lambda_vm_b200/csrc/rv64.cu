@@ -18,6 +18,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <memory>
 #include <unordered_map>
 #include <vector>
 
@@ -109,7 +110,39 @@ void keccak_f(uint64_t a[25]) {
 }
 
 struct Cell {
-    uint64_t value, stamp;
+    uint64_t value, stamp;  // stamp 0: never accessed
+};
+
+// Data memory: 8-byte cells in pages of 4096, allocated on first touch, the
+// last page cached (a guest's accesses stay in a few pages at a time).
+class Memory {
+  public:
+    Cell* at(uint64_t addr) {
+        const uint64_t pg = addr >> 15;
+        if (pg != last_pg_ || !last_) {
+            auto& p = pages_[pg];
+            if (!p) p.reset(new Cell[4096]());
+            last_pg_ = pg, last_ = p.get();
+        }
+        return last_ + ((addr >> 3) & 4095);
+    }
+    // every accessed cell in ascending address order
+    template <class F>
+    void each_touched(F f) const {
+        std::vector<uint64_t> pgs;
+        for (const auto& kv : pages_) pgs.push_back(kv.first);
+        std::sort(pgs.begin(), pgs.end());
+        for (uint64_t pg : pgs) {
+            const Cell* c = pages_.at(pg).get();
+            for (uint64_t i = 0; i < 4096; ++i)
+                if (c[i].stamp) f((pg << 15) | (i << 3), c[i]);
+        }
+    }
+
+  private:
+    std::unordered_map<uint64_t, std::unique_ptr<Cell[]>> pages_;
+    uint64_t last_pg_ = ~0ull;
+    Cell* last_ = nullptr;
 };
 
 }  // namespace
@@ -119,6 +152,14 @@ using namespace sg;
 extern "C" int sg_rv64_run(const uint32_t* words, uint32_t nwords, uint64_t max_steps, uint64_t n_rows,
                            uint64_t* rows_out, uint64_t* regs_out, uint64_t* counts_out, uint64_t* shifts_out,
                            uint64_t* cells_out, uint64_t* keccak_out, sg_rv64_info* info) {
+    return sg_rv64_run_counted(words, nwords, max_steps, n_rows, rows_out, regs_out, counts_out, shifts_out, cells_out,
+                               keccak_out, nullptr, nullptr, info);
+}
+
+extern "C" int sg_rv64_run_counted(const uint32_t* words, uint32_t nwords, uint64_t max_steps, uint64_t n_rows,
+                                   uint64_t* rows_out, uint64_t* regs_out, uint64_t* counts_out, uint64_t* shifts_out,
+                                   uint64_t* cells_out, uint64_t* keccak_out, uint64_t* range_counts,
+                                   uint64_t* bitwise_counts, sg_rv64_info* info) {
     SG_CHECK_ARG(words && nwords && info, "null argument");
     SG_CHECK_ARG(!rows_out || (n_rows >= 2 && (n_rows & (n_rows - 1)) == 0), "n_rows must be a power of two >= 2");
     std::vector<Ins> prog(nwords);
@@ -127,13 +168,17 @@ extern "C" int sg_rv64_run(const uint32_t* words, uint32_t nwords, uint64_t max_
     uint64_t x[32] = {0};
     uint64_t pc = 0, t = 0, nshift = 0, ncall = 0;
     uint32_t chips = 0;
-    std::unordered_map<uint64_t, Cell> mem;
-    mem.reserve(1 << 16);
+    Memory mem;
+    uint64_t ncells = 0;
     auto cell = [&](uint64_t addr, Cell** c) {
         if (addr % 8 || addr >> 32) return false;
-        *c = &mem[addr];  // a new cell starts as (0, timestamp 0)
+        *c = mem.at(addr);  // a new cell is (0, timestamp 0)
+        ncells += (*c)->stamp == 0;
         return true;
     };
+    SG_CHECK_ARG(!range_counts || rows_out, "lookup counts need the n_rows table");
+    if (range_counts) memset(range_counts, 0, 65536 * 8);
+    if (bitwise_counts) memset(bitwise_counts, 0, 3 * 65536 * 8);
     bool halted = false;
     while (!halted) {
         SG_CHECK_ARG(t < max_steps, "the program did not halt within max_steps");
@@ -188,11 +233,35 @@ extern "C" int sg_rv64_run(const uint32_t* words, uint32_t nwords, uint64_t max_
                         k[0] = clk, k[1] = ma;
                         for (int i = 0; i < 25; ++i) k[2 + i] = lanes[i], k[27 + i] = cs[i]->stamp;
                     }
+                    if (range_counts)  // the KECCAK table's reads: the gaps to the cells' last accesses
+                        for (int i = 0; i < 25; ++i) {
+                            const uint64_t gap = clk - cs[i]->stamp - 1;
+                            range_counts[gap & 0xFFFF] += 1;
+                            range_counts[gap >> 16] += 1;
+                        }
                     keccak_f(lanes);
                     for (int i = 0; i < 25; ++i) *cs[i] = Cell{lanes[i], clk};
                     ++ncall;
                 }
                 break;
+        }
+        if (range_counts) {  // the CPU row's RANGE lookups
+            for (int j = 0; j < 4; ++j) range_counts[(r >> (16 * j)) & 0xFFFF] += 1;
+            if (op == LD || op == SD || op == KECCAK_OP) {
+                range_counts[(ma >> 3) & 0xFFFF] += 1;
+                range_counts[8 * (ma >> 19)] += 1;
+            }
+            if (op == LD || op == SD) {
+                const uint64_t gap = clk - mt - 1;
+                range_counts[gap & 0xFFFF] += 1;
+                range_counts[gap >> 16] += 1;
+            }
+        }
+        if (bitwise_counts && op >= XOR && op <= ANDI) {  // its BITWISE lookups: eight byte pairs
+            const uint64_t second = op <= AND ? b : iu;
+            const uint32_t kind = (op == XOR || op == XORI) ? 0 : (op == OR || op == ORI) ? 1 : 2;
+            for (int i = 0; i < 8; ++i)
+                bitwise_counts[kind * 65536 + ((((a >> (8 * i)) & 0xFF) << 8) | ((second >> (8 * i)) & 0xFF))] += 1;
         }
         if (op == SLLI || op == SRLI) {
             if (shifts_out) {
@@ -222,25 +291,24 @@ extern "C" int sg_rv64_run(const uint32_t* words, uint32_t nwords, uint64_t max_
     info->cycles = t;
     info->a0 = x[10];
     info->shifts = nshift;
-    info->cells = mem.size();
+    info->cells = ncells;
     info->keccak_calls = ncall;
     info->chips = chips;
     if (rows_out) {
         // the halting row repeats to fill the table, with the final registers
         if (counts_out) counts_out[pc / 4] += n_rows - t;
+        if (range_counts) range_counts[0] += 4 * (n_rows - t);  // its zero result
         if (regs_out)
             for (uint64_t r = (t + SG_RV64_REG_CHUNK - 1) / SG_RV64_REG_CHUNK * SG_RV64_REG_CHUNK; r < n_rows;
                  r += SG_RV64_REG_CHUNK)
                 memcpy(regs_out + 32 * (r / SG_RV64_REG_CHUNK), x, 256);
     }
     if (cells_out) {
-        std::vector<std::pair<uint64_t, Cell>> cs(mem.begin(), mem.end());
-        std::sort(cs.begin(), cs.end(), [](const auto& u, const auto& v) { return u.first < v.first; });
-        for (size_t i = 0; i < cs.size(); ++i) {
-            cells_out[3 * i] = cs[i].first;
-            cells_out[3 * i + 1] = cs[i].second.value;
-            cells_out[3 * i + 2] = cs[i].second.stamp;
-        }
+        uint64_t i = 0;
+        mem.each_touched([&](uint64_t addr, const Cell& c) {
+            cells_out[3 * i] = addr, cells_out[3 * i + 1] = c.value, cells_out[3 * i + 2] = c.stamp;
+            ++i;
+        });
     }
     return SG_OK;
 }

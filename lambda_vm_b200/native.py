@@ -176,6 +176,7 @@ PROTOTYPES = {
     "sg_synth_trace": (i32, [vp, vp, vp, u64, u64, u64, u32]),
     "sg_ctx_pass_log": (i32, [vp, i32]),
     "sg_rv64_run": (i32, [vp, u32, u64, u64, vp, vp, vp, vp, vp, vp, vp]),
+    "sg_rv64_run_counted": (i32, [vp, u32, u64, u64, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
     "sg_rv64_cpu_table": (i32, [vp, vp, vp, u64, vp, u64, u32, vp]),
     "sg_rv64_keccak_table": (i32, [vp, vp, vp, u64, u64, vp]),
     "sg_rv64_shift_table": (i32, [vp, vp, vp, u64, u64, vp]),

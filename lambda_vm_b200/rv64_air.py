@@ -587,12 +587,13 @@ class RangeAir(BusAir):
         self._emit_logup(b)
         return b.program()
 
-    def trace(self, lookups):
-        """lookups: arrays of the 16-bit values looked up (with repetition)."""
+    def trace(self, lookups, counts=None):
+        """lookups: arrays of the 16-bit values looked up (with repetition),
+        added to counts (per value) if given."""
         t = np.zeros((self.n, 3), np.uint64)
         t[:, self.V] = np.arange(self.n, dtype=np.uint64)
         t[self.n - 1, self.W] = 1
-        m = np.zeros(self.n, np.int64)
+        m = np.zeros(self.n, np.int64) if counts is None else np.asarray(counts, np.uint64).astype(np.int64)
         for v in lookups:
             v = np.asarray(v).reshape(-1).astype(np.int64)
             assert v.size == 0 or (v.min() >= 0 and v.max() < self.n), "a range lookup outside 0..2^16-1"
@@ -633,9 +634,10 @@ class BitwiseAir(BusAir):
         self._emit_logup(b)
         return b.program()
 
-    def trace(self, records):
+    def trace(self, records, counts=None):
         """The table with the multiplicities of the byte triples the CPU's
-        bitwise rows (row records, as CpuAir.trace) look up."""
+        bitwise rows (row records, as CpuAir.trace) look up, or with the
+        executor's counts (3 x 2^16: XOR, OR, AND)."""
         t = np.zeros((self.n, self.width), np.uint64)
         v = np.arange(self.n, dtype=np.uint64)
         xv, yv = v >> np.uint64(8), v & np.uint64(0xFF)
@@ -643,6 +645,10 @@ class BitwiseAir(BusAir):
             t[:, self.XB + i] = (xv >> np.uint64(i)) & np.uint64(1)
             t[:, self.YB + i] = (yv >> np.uint64(i)) & np.uint64(1)
         t[:, self.XOR], t[:, self.OR], t[:, self.AND] = xv ^ yv, xv | yv, xv & yv
+        if counts is not None:
+            cnt = np.asarray(counts, np.uint64).reshape(3, self.n)
+            t[:, self.MX], t[:, self.MO], t[:, self.MAN] = cnt[0], cnt[1], cnt[2]
+            return t
         rec = np.asarray(records, np.uint64).reshape(-1, 8)
         op = ((rec[:, 0] >> np.uint64(32)) & np.uint64(0xFF)).astype(np.int64)
         sh = np.arange(0, 64, 8, dtype=np.uint64)
@@ -1028,9 +1034,14 @@ class Events:
     final timestamps); Keccak ecalls (timestamps, addresses, input lanes,
     previous timestamps)."""
 
-    def __init__(self, records, regs, counts, output, cycles, chips, shifts, cells, keccak):
+    def __init__(self, records, regs, counts, output, cycles, chips, shifts, cells, keccak, range_counts=None,
+                 bitwise_counts=None):
         self.records, self.regs, self.counts, self.output, self.cycles = records, regs, counts, output, cycles
         self.chips, self.shifts, self.cells, self.keccak = chips, shifts, cells, keccak
+        # lookup multiplicities counted by the executor: the CPU and KECCAK
+        # tables' RANGE lookups, the CPU table's BITWISE lookups (None: count
+        # them from the records)
+        self.range_counts, self.bitwise_counts = range_counts, bitwise_counts
 
 
 def _chips_used(ops):
@@ -1171,13 +1182,15 @@ def tables_from_events(words, ev, host_tables=False):
     # the CPU's RANGE lookups: the result's four 16-bit pieces on every row
     # (rows past the halt repeat its zero result), the address and timestamp
     # pieces of memory rows
+    counted = ev.range_counts is not None
     op = ((rec[:, 0] >> np.uint64(32)) & np.uint64(0xFF)).astype(np.int64)
     r = rec[:, 4]
-    look = [(r[:, None] >> np.arange(0, 64, 16, dtype=np.uint64)) & np.uint64(0xFFFF), np.zeros(4 * (n - T), np.uint64)]
+    look = [] if counted else [(r[:, None] >> np.arange(0, 64, 16, dtype=np.uint64)) & np.uint64(0xFFFF),
+                               np.zeros(4 * (n - T), np.uint64)]
     if "bitwise" in chips:
         a = BitwiseAir()
         airs.append(a)
-        traces.append(a.trace(rec))
+        traces.append(a.trace(rec, ev.bitwise_counts))
     if "shift" in chips:
         a = ShiftAir(heights["shift"])
         src = ShiftSource(ev.shifts)
@@ -1188,19 +1201,22 @@ def tables_from_events(words, ev, host_tables=False):
         mt = a.trace(*ev.cells)
         airs.append(a)
         traces.append(mt)
-        mem = np.isin(op, [OP_ID["ld"], OP_ID["sd"]])
-        addr = mem | (op == KECCAK_OP)
-        ma = rec[addr, 5]
-        gap = np.nonzero(mem)[0].astype(np.uint64) - rec[mem, 7]   # (row + 1) - mt - 1
-        look += [(ma >> np.uint64(3)) & np.uint64(0xFFFF), np.uint64(8) * (ma >> np.uint64(19)),
-                 gap & np.uint64(0xFFFF), gap >> np.uint64(16), mt[:, MemoryAir.D0], mt[:, MemoryAir.D1]]
+        if not counted:
+            mem = np.isin(op, [OP_ID["ld"], OP_ID["sd"]])
+            addr = mem | (op == KECCAK_OP)
+            ma = rec[addr, 5]
+            gap = np.nonzero(mem)[0].astype(np.uint64) - rec[mem, 7]   # (row + 1) - mt - 1
+            look += [(ma >> np.uint64(3)) & np.uint64(0xFFFF), np.uint64(8) * (ma >> np.uint64(19)),
+                     gap & np.uint64(0xFFFF), gap >> np.uint64(16)]
+        look += [mt[:, MemoryAir.D0], mt[:, MemoryAir.D1]]
     if "keccak" in chips:
         a = KeccakAir(heights["keccak"])
         src = KeccakSource(*ev.keccak)
         airs.append(a)
         traces.append(src.host_trace(a) if host_tables else src)
-        look += src.range_lookups()
-    traces[1] = airs[1].trace(look)
+        if not counted:
+            look += src.range_lookups()
+    traces[1] = airs[1].trace(look, ev.range_counts)
     pub = {"words": list(words), "counts": ev.counts, "output": ev.output, "cycles": ev.cycles,
            "heights": heights, "label": statement_label(words, ev.counts, ev.output, heights),
            "terms": cpu.public_terms(ev.counts, ev.output)}
@@ -1223,13 +1239,16 @@ def native_events(words, max_steps=1 << 32):
     shifts = np.empty((info.shifts, 3), np.uint64)
     cells = np.empty((info.cells, 3), np.uint64)
     kc = np.empty((info.keccak_calls, 52), np.uint64)
+    rcount = np.empty(1 << 16, np.uint64)
+    bcount = np.empty(3 << 16, np.uint64)
     ptr = lambda a: a.ctypes.data if a.size else None
-    native.check(L.sg_rv64_run(w.ctypes.data, len(w), max_steps, n, rec.ctypes.data, regs.ctypes.data,
-                               counts.ctypes.data, ptr(shifts), ptr(cells), ptr(kc), C.byref(info)))
+    native.check(L.sg_rv64_run_counted(w.ctypes.data, len(w), max_steps, n, rec.ctypes.data, regs.ctypes.data,
+                                       counts.ctypes.data, ptr(shifts), ptr(cells), ptr(kc), rcount.ctypes.data,
+                                       bcount.ctypes.data, C.byref(info)))
     chips = tuple(c for i, c in enumerate(CHIPS) if info.chips >> i & 1)
     return Events(rec, regs, [int(c) for c in counts], info.a0, info.cycles, chips, shifts,
                   (cells[:, 0].copy(), cells[:, 1].copy(), cells[:, 2].copy()),
-                  (kc[:, 0].copy(), kc[:, 1].copy(), kc[:, 2:27].copy(), kc[:, 27:52].copy()))
+                  (kc[:, 0].copy(), kc[:, 1].copy(), kc[:, 2:27].copy(), kc[:, 27:52].copy()), rcount, bcount)
 
 
 def build(words, native_exec=True, host_tables=False):

@@ -116,6 +116,11 @@ def test_native_events_equal_the_python_events(prog):
     for a, b in zip(pe.cells + pe.keccak, ne.cells + ne.keccak):
         assert np.array_equal(a, b)
     airs, traces, pub = RA.tables_from_events(words, ne, host_tables=True)
+    # the executor's lookup counts give the same RANGE and BITWISE tables as
+    # counting the records
+    _, ptraces, ppub = RA.tables_from_events(words, pe, host_tables=True)
+    assert len(traces) == len(ptraces) and all(np.array_equal(x, y) for x, y in zip(traces, ptraces))
+    assert ppub["label"] == pub["label"]
     if prog == "wrap":
         bad, total = _check(airs, traces, pub)
         assert not any(bad.values()) and total == (0, 0, 0)
