@@ -19,6 +19,7 @@
 
 #include <algorithm>
 #include <memory>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -145,6 +146,55 @@ class Memory {
     Cell* last_ = nullptr;
 };
 
+// The CPU table's lookups, counted from the row records after the run, a
+// slice of rows per host thread into thread-local histograms: RANGE (the
+// written value's four 16-bit pieces on every row, the address pieces of
+// memory and keccak rows, the timestamp-gap pieces of memory rows) and
+// BITWISE (the eight byte pairs of a bitwise row, by kind).
+void count_cpu_lookups(const uint64_t* rec, uint64_t T, uint64_t* range_counts, uint64_t* bitwise_counts) {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const unsigned nt = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>({hw ? hw : 1u, 16u, T / 65536 + 1}));
+    std::vector<std::vector<uint32_t>> rh(nt, std::vector<uint32_t>(range_counts ? 65536 : 0)),
+        bh(nt, std::vector<uint32_t>(bitwise_counts ? 3 * 65536 : 0));
+    auto work = [&](unsigned k) {
+        uint32_t* rr = range_counts ? rh[k].data() : nullptr;
+        uint32_t* bb = bitwise_counts ? bh[k].data() : nullptr;
+        for (uint64_t row = T * k / nt; row < T * (k + 1) / nt; ++row) {
+            const uint64_t* q = rec + 8 * row;
+            const uint32_t op = (uint32_t)(q[0] >> 32) & 0xFF;
+            const uint64_t iu = q[1], a = q[2], b = q[3], r = q[4], ma = q[5], mt = q[7];
+            if (rr) {
+                for (int j = 0; j < 4; ++j) rr[(r >> (16 * j)) & 0xFFFF] += 1;
+                if (op == LD || op == SD || op == KECCAK_OP) {
+                    rr[(ma >> 3) & 0xFFFF] += 1;
+                    rr[8 * (ma >> 19)] += 1;
+                }
+                if (op == LD || op == SD) {
+                    const uint64_t gap = row - mt;  // (row + 1) - mt - 1
+                    rr[gap & 0xFFFF] += 1;
+                    rr[gap >> 16] += 1;
+                }
+            }
+            if (bb && op >= XOR && op <= ANDI) {
+                const uint64_t second = op <= AND ? b : iu;
+                const uint32_t kind = (op == XOR || op == XORI) ? 0 : (op == OR || op == ORI) ? 1 : 2;
+                for (int i = 0; i < 8; ++i)
+                    bb[kind * 65536 + ((((a >> (8 * i)) & 0xFF) << 8) | ((second >> (8 * i)) & 0xFF))] += 1;
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (unsigned k = 1; k < nt; ++k) pool.emplace_back(work, k);
+    work(0);
+    for (auto& th : pool) th.join();
+    for (unsigned k = 0; k < nt; ++k) {
+        if (range_counts)
+            for (uint32_t v = 0; v < 65536; ++v) range_counts[v] += rh[k][v];
+        if (bitwise_counts)
+            for (uint32_t v = 0; v < 3 * 65536; ++v) bitwise_counts[v] += bh[k][v];
+    }
+}
+
 }  // namespace
 
 using namespace sg;
@@ -245,24 +295,6 @@ extern "C" int sg_rv64_run_counted(const uint32_t* words, uint32_t nwords, uint6
                 }
                 break;
         }
-        if (range_counts) {  // the CPU row's RANGE lookups
-            for (int j = 0; j < 4; ++j) range_counts[(r >> (16 * j)) & 0xFFFF] += 1;
-            if (op == LD || op == SD || op == KECCAK_OP) {
-                range_counts[(ma >> 3) & 0xFFFF] += 1;
-                range_counts[8 * (ma >> 19)] += 1;
-            }
-            if (op == LD || op == SD) {
-                const uint64_t gap = clk - mt - 1;
-                range_counts[gap & 0xFFFF] += 1;
-                range_counts[gap >> 16] += 1;
-            }
-        }
-        if (bitwise_counts && op >= XOR && op <= ANDI) {  // its BITWISE lookups: eight byte pairs
-            const uint64_t second = op <= AND ? b : iu;
-            const uint32_t kind = (op == XOR || op == XORI) ? 0 : (op == OR || op == ORI) ? 1 : 2;
-            for (int i = 0; i < 8; ++i)
-                bitwise_counts[kind * 65536 + ((((a >> (8 * i)) & 0xFF) << 8) | ((second >> (8 * i)) & 0xFF))] += 1;
-        }
         if (op == SLLI || op == SRLI) {
             if (shifts_out) {
                 uint64_t* sh = shifts_out + 3 * nshift;
@@ -303,6 +335,7 @@ extern "C" int sg_rv64_run_counted(const uint32_t* words, uint32_t nwords, uint6
                  r += SG_RV64_REG_CHUNK)
                 memcpy(regs_out + 32 * (r / SG_RV64_REG_CHUNK), x, 256);
     }
+    if (range_counts || bitwise_counts) count_cpu_lookups(rows_out, t, range_counts, bitwise_counts);
     if (cells_out) {
         uint64_t i = 0;
         mem.each_touched([&](uint64_t addr, const Cell& c) {
