@@ -466,9 +466,10 @@ def measure_serve(a):
 
 def serve_summary(a):
     """A bounded serving run for the default bench line: two arrival rates,
-    24 jobs each, admission server against one proof at a time."""
+    48 jobs each (the p99 of fewer is the slowest one or two jobs), admission
+    server against one proof at a time."""
     import types
-    b = types.SimpleNamespace(jobs=24, job_max_log_n=a.job_max_log_n, max_jobs=a.max_jobs, rates="5,50",
+    b = types.SimpleNamespace(jobs=48, job_max_log_n=a.job_max_log_n, max_jobs=a.max_jobs, rates="5,50",
                               policy=a.policy, job_kind=getattr(a, "job_kind", "mix"), beside_big=a.beside_big,
                               big_cells=a.big_cells)
     line = measure_serve(b)
