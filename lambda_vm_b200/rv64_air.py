@@ -1259,13 +1259,6 @@ def build(words, native_exec=True, host_tables=False):
     return tables_from_events(words, ev, host_tables)
 
 
-def native_trace(words, max_steps=1 << 32):
-    """(CPU table built on the host, counts, a0, cycles) of a run of the native executor."""
-    ev = native_events(words, max_steps)
-    cpu = CpuAir(words, max(1, (ev.cycles - 1).bit_length()), ev.chips)
-    return cpu.trace(ev.records), ev.counts, ev.output, ev.cycles
-
-
 def prove(words, opts, bk):
     """Execute `words` and prove the execution on backend `bk` (stark.multi_prove,
     the plain per-table form): (proof, public statement)."""

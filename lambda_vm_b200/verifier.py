@@ -151,6 +151,9 @@ def _replay(airs, proof, opts, label, public_terms=()):
     query indexes); returns (ok, reason, per-table values for the query phase)."""
     T = mc.Transcript(label)
     tabs = proof["tables"]
+    if len(tabs) != len(airs):
+        # every table of the proof is checked against an AIR of the statement
+        return False, "the proof's table count is not the statement's", None
     for tp in tabs:
         T.append_bytes(tp["main_root"])
     ch = [f3(T.sample_ext3()), f3(T.sample_ext3())]

@@ -126,6 +126,9 @@ def public_sum(terms, z, apows):
 def verify(airs, proof, opts, label=b"lambda_vm_b200/synthetic-multi-table", public_terms=()):
     T = O.Transcript(label)
     tabs = proof["tables"]
+    if len(tabs) != len(airs):
+        # every table of the proof is checked against an AIR of the statement
+        return False, "the proof's table count is not the statement's"
     for tp in tabs:
         T.append_bytes(tp["main_root"])
     ch = [f3(T.sample_ext3()), f3(T.sample_ext3())]

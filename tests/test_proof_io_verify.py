@@ -70,3 +70,18 @@ def test_tampering_is_rejected_by_both_verifiers(proof, where):
     assert verify(airs, q, OPTS)[0] is False
     assert oracle_verify(airs, q, OPTS)[0] is False
     assert verify_bytes(airs, serialize(q), OPTS)[0] is False
+
+
+def test_a_proof_with_more_or_fewer_tables_than_the_statement_is_rejected(proof):
+    """Every table of a proof is checked against an AIR of the statement: a
+    proof carrying an extra table (whose bus contribution would otherwise
+    go unchecked) or missing one is rejected by both verifiers."""
+    airs, p = proof
+    extra = copy.deepcopy(p)
+    extra["tables"].append(copy.deepcopy(p["tables"][0]))
+    short = copy.deepcopy(p)
+    short["tables"].pop()
+    for q in (extra, short):
+        assert verify(airs, q, OPTS)[0] is False
+        assert oracle_verify(airs, q, OPTS)[0] is False
+    assert verify(airs[:2], p, OPTS)[0] is False
