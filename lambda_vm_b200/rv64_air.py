@@ -1273,7 +1273,10 @@ def verify(words, counts, output, proof, opts, device=None, heights=None):
     having executed each instruction counts[i] times, with the chips'
     heights of the statement: (ok, reason)."""
     from . import verifier
-    airs = airs_for(words, counts, heights)
+    try:
+        airs = airs_for(words, counts, heights)
+    except (AssertionError, ValueError, StopIteration) as e:
+        return False, f"malformed statement: {e}"
     cpu = airs[0]
     return verifier.verify(airs, proof, opts, label=statement_label(words, counts, output, heights), device=device,
                            public_terms=cpu.public_terms(counts, output))
