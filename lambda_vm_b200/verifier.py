@@ -132,16 +132,20 @@ def verify(airs, proof, opts, label=b"lambda_vm_b200/synthetic-multi-table", dev
     """Verify a multi-table proof: (ok, reason). With `device` (a context from
     device.backend()) the query phase runs on the GPU (sg_verify_queries).
     `public_terms` are bus terms whose content the statement fixes
-    (public_sum); they join the tables' contributions in the bus balance."""
-    ok, reason, prep = _replay(airs, proof, opts, label, public_terms)
-    if not ok:
-        return ok, reason
-    if device is not None:
-        return verify_queries_gpu([prep], device)[0]
-    for pr in prep:
-        ok, reason = _check_queries_host(pr)
+    (public_sum); they join the tables' contributions in the bus balance. A
+    proof of the wrong shape (missing fields, short vectors) is rejected."""
+    try:
+        ok, reason, prep = _replay(airs, proof, opts, label, public_terms)
         if not ok:
             return ok, reason
+        if device is not None:
+            return verify_queries_gpu([prep], device)[0]
+        for pr in prep:
+            ok, reason = _check_queries_host(pr)
+            if not ok:
+                return ok, reason
+    except (IndexError, KeyError, TypeError, ValueError) as e:
+        return False, f"malformed proof: {type(e).__name__}"
     return True, "ok"
 
 

@@ -85,3 +85,13 @@ def test_a_proof_with_more_or_fewer_tables_than_the_statement_is_rejected(proof)
         assert verify(airs, q, OPTS)[0] is False
         assert oracle_verify(airs, q, OPTS)[0] is False
     assert verify(airs[:2], p, OPTS)[0] is False
+
+
+def test_a_malformed_proof_is_rejected_not_raised(proof):
+    airs, p = proof
+    q = copy.deepcopy(p)
+    q["tables"][0]["trace_ood"] = [[]]
+    assert verify(airs, q, OPTS)[0] is False
+    q = copy.deepcopy(p)
+    del q["tables"][2]["fri_roots"]
+    assert verify(airs, q, OPTS)[0] is False
