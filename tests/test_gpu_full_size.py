@@ -117,3 +117,30 @@ def test_large_table_proof_verifies(be):
     sched = multi_prove_scheduled(airs, seeds, opts, workers=2, be=be)
     assert serialize(plain) == serialize(sched)
     assert verify(airs, plain, opts) == (True, "ok")
+
+
+def test_keccak_guest_1mib_proof_verifies(be):
+    """The Keccak guest at its benchmark size (a 1 048 560-byte buffer, 1.8 M
+    cycles, six tables up to 2^21 x 234 and 2^18 x 2605) proved on the GPU by
+    the plain and the batched prover: the same proof, the guest's own output,
+    accepted by the library verifier (GPU query phase) and by the independent
+    verifier built on the oracle; a wrong output is rejected."""
+    from lambda_vm_b200 import rv64
+    from lambda_vm_b200 import rv64_air as RA
+    from lambda_vm_b200.proof_io import serialize
+    from lambda_vm_b200.scheduler import multi_prove_scheduled
+    from lambda_vm_b200.stark import GpuBackend, Options, multi_prove
+    from oracle.verifier import verify as oracle_verify
+    opts = Options(blowup=2, grinding=20, final_log_degree=5)
+    words = rv64.keccak_program(136 * 7710)
+    airs, traces, pub = RA.build(words)
+    assert pub["cycles"] == 1796454 and pub["output"] == rv64.keccak_reference(136 * 7710)
+    proof = multi_prove(airs, traces, opts, GpuBackend(be), label=pub["label"])
+    batched = multi_prove_scheduled(airs, traces, opts, workers=8, be=be, label=pub["label"])
+    assert serialize(batched) == serialize(proof)
+    counts, out, h = pub["counts"], pub["output"], pub["heights"]
+    assert RA.verify(words, counts, out, proof, opts, device=be, heights=h) == (True, "ok")
+    full = RA.airs_for(words, counts, h)
+    assert oracle_verify(full, proof, opts, label=RA.statement_label(words, counts, out, h),
+                         public_terms=full[0].public_terms(counts, out)) == (True, "ok")
+    assert RA.verify(words, counts, out ^ (1 << 63), proof, opts, heights=h)[0] is False
