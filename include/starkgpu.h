@@ -565,6 +565,7 @@ SG_API int sg_verify_queries(sg_ctx* ctx, void* stream, const sg_verify_table* t
 #define SG_RV64_CPU_CORE_WIDTH 200
 #define SG_RV64_CPU_WIDTH 234
 #define SG_RV64_REG_CHUNK 64
+#define SG_RV64_MEMORY_WIDTH 8
 #define SG_RV64_CHIP_BITWISE 1u
 #define SG_RV64_CHIP_SHIFT 2u
 #define SG_RV64_CHIP_MEMORY 4u
@@ -602,6 +603,15 @@ SG_API int sg_rv64_keccak_table(sg_ctx* ctx, void* stream, const uint64_t* calls
                                 uint64_t* d_out);
 SG_API int sg_rv64_shift_table(sg_ctx* ctx, void* stream, const uint64_t* shifts, uint64_t count, uint64_t n_rows,
                                uint64_t* d_out);
+/* The MEMORY table (n_rows x SG_RV64_MEMORY_WIDTH: address, final value's low
+ * and high 32 bits, final timestamp, active, not-the-wrap-row, the gap to the
+ * next address in two 16-bit pieces) written on the device from sg_rv64_run's
+ * `count` >= 1 cells (address, final value, final timestamp; addresses
+ * ascending multiples of 8 below 2^32, else SG_ERR_INVALID); rows past the
+ * cells continue the addresses in steps of 8. Layout:
+ * lambda_vm_b200/rv64_air.py's MemoryAir. Asynchronous on `stream`. */
+SG_API int sg_rv64_memory_table(sg_ctx* ctx, void* stream, const uint64_t* cells, uint64_t count, uint64_t n_rows,
+                                uint64_t* d_out);
 
 /* ---- DFT pass log: the autotuner's measurements. No counterpart in the
  *      reference (its NTT has one fixed plan). While enabled, every DFT pass

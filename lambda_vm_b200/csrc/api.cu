@@ -441,6 +441,32 @@ static int stage_reserve(Ctx* ctx, uint64_t half_bytes) {
     return SG_OK;
 }
 
+int sg::upload_host(Ctx* ctx, cudaStream_t st, const void* host, uint64_t bytes, void* dst) {
+    if (!bytes) return SG_OK;
+    cudaPointerAttributes pa;
+    const bool pageable = cudaPointerGetAttributes(&pa, host) != cudaSuccess || pa.type == cudaMemoryTypeUnregistered;
+    cudaGetLastError();
+    constexpr uint64_t kDirect = 4ull << 20, kPiece = 32ull << 20;
+    if (!pageable || bytes <= kDirect) {
+        SG_CUDA(cudaMemcpyAsync(dst, host, bytes, cudaMemcpyHostToDevice, st));
+        return SG_OK;
+    }
+    std::lock_guard<std::mutex> lock(ctx->stage_mu);
+    SG_TRY(stage_reserve(ctx, std::min(bytes, kPiece)));
+    const uint64_t piece = std::min(ctx->stage_bytes, kPiece);
+    for (uint64_t off = 0, k = 0; off < bytes; off += piece, ++k) {
+        const uint64_t len = std::min(piece, bytes - off);
+        uint8_t* half = (uint8_t*)ctx->stage + (k & 1) * ctx->stage_bytes;
+        const uint8_t* src = (const uint8_t*)host + off;
+        // the half is free once its previous copy (this call's or an earlier one's) has left it
+        SG_CUDA(cudaEventSynchronize(ctx->stage_free[k & 1]));
+        host_parallel(len, 1ull << 20, [&](uint64_t lo, uint64_t hi) { memcpy(half + lo, src + lo, hi - lo); });
+        SG_CUDA(cudaMemcpyAsync((uint8_t*)dst + off, half, len, cudaMemcpyHostToDevice, st));
+        SG_CUDA(cudaEventRecord(ctx->stage_free[k & 1], st));
+    }
+    return SG_OK;
+}
+
 // When `leaves` is non-null the commit's leaves are one LDE row each over the
 // whole row: they are then absorbed window by window as the LDE columns
 // complete (whole 17-lane sponge blocks), so hashing also runs under the

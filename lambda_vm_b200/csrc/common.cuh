@@ -5,10 +5,12 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <atomic>
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/starkgpu.h"
@@ -122,6 +124,25 @@ void trim_cache(Ctx* ctx);
 // Stream-ordered allocation charged against the context budget.
 int dev_alloc(Ctx* ctx, cudaStream_t st, uint64_t bytes, void** out);
 int dev_free(Ctx* ctx, cudaStream_t st, void* p, uint64_t bytes);
+
+// Copy `bytes` of host memory to device memory `dst` in `st`'s order (api.cu).
+// Page-locked memory goes up directly; pageable memory goes through the
+// context's page-locked staging, host threads copying one chunk into a
+// staging half while the previous chunk's DMA is in flight (the driver's own
+// staging of a pageable copy runs at a few GB/s).
+int upload_host(Ctx* ctx, cudaStream_t st, const void* host, uint64_t bytes, void* dst);
+
+// f(lo, hi) over contiguous slices of [0, n), at least `grain` items a slice,
+// on up to 16 host threads; the calling thread takes the first slice.
+template <class F>
+void host_parallel(uint64_t n, uint64_t grain, F f) {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const uint64_t T = std::max<uint64_t>(1, std::min<uint64_t>({hw ? hw : 1u, 16u, n / (grain ? grain : 1)}));
+    std::vector<std::thread> th;
+    for (uint64_t t = 1; t < T; ++t) th.emplace_back([&f, n, T, t] { f(n * t / T, n * (t + 1) / T); });
+    f(0, n / T);
+    for (auto& x : th) x.join();
+}
 
 // Table of omega_{2^log}^e, e in [0, 2^log), cached per context.
 int roots_table(Ctx* ctx, cudaStream_t st, uint32_t log, const uint64_t** out);

@@ -561,12 +561,35 @@ __global__ void k_cpu_rows(const uint64_t* __restrict__ recs, uint64_t T, const 
     }
 }
 
+// MEMORY table rows (ADDR, V_LO, V_HI, T, ACT, NW, D0, D1; rv64_air.py's
+// MemoryAir) from `count` touched cells (address, final value, final
+// timestamp) in ascending address order; rows past the cells continue the
+// addresses in steps of 8, and every row but the last steps to the next.
+constexpr int MW = 8;
+static_assert(MW == SG_RV64_MEMORY_WIDTH, "MEMORY table width");
+__global__ void k_memory_rows(const uint64_t* __restrict__ cells, uint64_t count, uint64_t n_rows,
+                              uint64_t* __restrict__ out) {
+    const uint64_t last = cells[3 * (count - 1)];
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_rows;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const bool act = i < count;
+        const uint64_t a = act ? cells[3 * i] : last + 8 * (i - count + 1);
+        const uint64_t v = act ? cells[3 * i + 1] : 0, t = act ? cells[3 * i + 2] : 0;
+        uint64_t d = 0;
+        if (i + 1 < n_rows) d = ((i + 1 < count ? cells[3 * (i + 1)] : last + 8 * (i + 2 - count)) - a - 8) >> 3;
+        uint64_t* o = out + MW * i;
+        o[0] = a, o[1] = v & M32, o[2] = v >> 32, o[3] = t;
+        o[4] = act, o[5] = i + 1 < n_rows, o[6] = d & 0xFFFF, o[7] = d >> 16;
+    }
+}
+
 int upload_events(Ctx* ctx, cudaStream_t st, const uint64_t* host, uint64_t words, uint64_t** d) {
     SG_TRY(dev_alloc(ctx, st, 8 * words, (void**)d));
-    if (cudaMemcpyAsync(*d, host, 8 * words, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+    const int rc = upload_host(ctx, st, host, 8 * words, *d);
+    if (rc != SG_OK) {
         dev_free(ctx, st, *d, 8 * words);
-        set_error("rv64: event upload failed");
-        return SG_ERR_CUDA;
+        set_error(std::string("rv64: event upload failed: ") + last_error());
+        return rc;
     }
     return SG_OK;
 }
@@ -580,14 +603,26 @@ extern "C" int sg_rv64_cpu_table(sg_ctx* c, void* stream, const uint64_t* rows, 
     SG_ENTER(ctx);
     SG_CHECK_ARG(count >= 1 && count <= n_rows, "the execution does not fit n_rows");
     SG_CHECK_ARG(width == SG_RV64_CPU_CORE_WIDTH || width == SG_RV64_CPU_WIDTH, "width is the core or the full width");
-    for (uint64_t i = 0; i < count; ++i) {
-        const uint64_t w0 = rows[8 * i];
-        const uint32_t op = (uint32_t)(w0 >> 32) & 0xFF;
-        SG_CHECK_ARG(op >= 1 && op <= KECCAK_OP && ((w0 >> 40) & 0xFF) < 32 && ((w0 >> 48) & 0xFF) < 32 &&
-                         (w0 >> 56) < 32, "bad row record");
-        SG_CHECK_ARG(width == SG_RV64_CPU_WIDTH || op < XOR || op == SLLI || op == SRLI,
-                     "a chip instruction in a table without the chips' columns");
-    }
+    // 0: good; 1: a bad record; 2: a chip instruction in a core-width table
+    std::atomic<int> bad{0};
+    host_parallel(count, 1 << 16, [&](uint64_t lo, uint64_t hi) {
+        int b = 0;
+        for (uint64_t i = lo; i < hi && !b; ++i) {
+            const uint64_t w0 = rows[8 * i];
+            const uint32_t op = (uint32_t)(w0 >> 32) & 0xFF;
+            if (!(op >= 1 && op <= KECCAK_OP && ((w0 >> 40) & 0xFF) < 32 && ((w0 >> 48) & 0xFF) < 32 &&
+                  (w0 >> 56) < 32))
+                b = 1;
+            else if (!(width == SG_RV64_CPU_WIDTH || op < XOR || op == SLLI || op == SRLI))
+                b = 2;
+        }
+        if (b) {
+            int z = 0;
+            bad.compare_exchange_strong(z, b);
+        }
+    });
+    SG_CHECK_ARG(bad.load() != 1, "bad row record");
+    SG_CHECK_ARG(bad.load() != 2, "a chip instruction in a table without the chips' columns");
     cudaStream_t st = (cudaStream_t)stream;
     const uint64_t nchunks = (n_rows + SG_RV64_REG_CHUNK - 1) / SG_RV64_REG_CHUNK;
     uint64_t *d_rows = nullptr, *d_regs = nullptr;
@@ -641,5 +676,32 @@ extern "C" int sg_rv64_shift_table(sg_ctx* c, void* stream, const uint64_t* shif
     k_shift_rows<<<grid, 256, 0, st>>>(d_ev, count, n_rows, d_out);
     const int rc = check_launch(ctx, "k_shift_rows");
     if (d_ev) dev_free(ctx, st, d_ev, 8 * 3 * count);
+    return rc;
+}
+
+extern "C" int sg_rv64_memory_table(sg_ctx* c, void* stream, const uint64_t* cells, uint64_t count, uint64_t n_rows,
+                                    uint64_t* d_out) {
+    Ctx* ctx = reinterpret_cast<Ctx*>(c);
+    SG_CHECK_ARG(ctx && d_out && cells, "null argument");
+    SG_ENTER(ctx);
+    SG_CHECK_ARG(count >= 1 && count <= n_rows && n_rows <= (1ull << 32), "the cells do not fit n_rows");
+    std::atomic<bool> bad{false};
+    host_parallel(count, 1 << 16, [&](uint64_t lo, uint64_t hi) {
+        for (uint64_t i = lo; i < hi; ++i) {
+            const uint64_t a = cells[3 * i];
+            if (a % 8 || a >> 32 || (i && a <= cells[3 * (i - 1)])) {
+                bad = true;
+                return;
+            }
+        }
+    });
+    SG_CHECK_ARG(!bad.load(), "cell addresses must be ascending multiples of 8 below 2^32");
+    cudaStream_t st = (cudaStream_t)stream;
+    uint64_t* d_ev = nullptr;
+    SG_TRY(upload_events(ctx, st, cells, 3 * count, &d_ev));
+    const unsigned grid = (unsigned)std::min<uint64_t>((n_rows + 255) / 256, 148ull * 16);
+    k_memory_rows<<<grid, 256, 0, st>>>(d_ev, count, n_rows, d_out);
+    const int rc = check_launch(ctx, "k_memory_rows");
+    dev_free(ctx, st, d_ev, 8 * 3 * count);
     return rc;
 }

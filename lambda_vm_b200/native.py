@@ -180,6 +180,7 @@ PROTOTYPES = {
     "sg_rv64_cpu_table": (i32, [vp, vp, vp, u64, vp, u64, u32, vp]),
     "sg_rv64_keccak_table": (i32, [vp, vp, vp, u64, u64, vp]),
     "sg_rv64_shift_table": (i32, [vp, vp, vp, u64, u64, vp]),
+    "sg_rv64_memory_table": (i32, [vp, vp, vp, u64, u64, vp]),
     "sg_verify_queries": (i32, [vp, vp, C.POINTER(VerifyTable), u32, vp]),
     "sg_ctx_pass_log_read": (i32, [vp, C.POINTER(PassRecord), u32, C.POINTER(u32)]),
     "sg_mlp_loss_grad": (i32, [vp, vp, vp, vp, u32, vp, vp, vp]),

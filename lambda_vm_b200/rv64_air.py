@@ -634,17 +634,30 @@ class BitwiseAir(BusAir):
         self._emit_logup(b)
         return b.program()
 
+    _fixed_columns = None
+
+    @classmethod
+    def _fixed(cls):
+        """The table with zero multiplicities (the bit and result columns do
+        not depend on the run), built once a process."""
+        if cls._fixed_columns is None:
+            n = 1 << 16
+            t = np.zeros((n, 22), np.uint64)
+            v = np.arange(n, dtype=np.uint64)
+            xv, yv = v >> np.uint64(8), v & np.uint64(0xFF)
+            for i in range(8):
+                t[:, cls.XB + i] = (xv >> np.uint64(i)) & np.uint64(1)
+                t[:, cls.YB + i] = (yv >> np.uint64(i)) & np.uint64(1)
+            t[:, cls.XOR], t[:, cls.OR], t[:, cls.AND] = xv ^ yv, xv | yv, xv & yv
+            t.setflags(write=False)
+            cls._fixed_columns = t
+        return cls._fixed_columns
+
     def trace(self, records, counts=None):
         """The table with the multiplicities of the byte triples the CPU's
         bitwise rows (row records, as CpuAir.trace) look up, or with the
         executor's counts (3 x 2^16: XOR, OR, AND)."""
-        t = np.zeros((self.n, self.width), np.uint64)
-        v = np.arange(self.n, dtype=np.uint64)
-        xv, yv = v >> np.uint64(8), v & np.uint64(0xFF)
-        for i in range(8):
-            t[:, self.XB + i] = (xv >> np.uint64(i)) & np.uint64(1)
-            t[:, self.YB + i] = (yv >> np.uint64(i)) & np.uint64(1)
-        t[:, self.XOR], t[:, self.OR], t[:, self.AND] = xv ^ yv, xv | yv, xv & yv
+        t = self._fixed().copy()
         if counts is not None:
             cnt = np.asarray(counts, np.uint64).reshape(3, self.n)
             t[:, self.MX], t[:, self.MO], t[:, self.MAN] = cnt[0], cnt[1], cnt[2]
@@ -1130,6 +1143,34 @@ class ShiftSource:
         return m
 
 
+class MemorySource:
+    """The MEMORY table of a run's touched cells (address, final value, final
+    timestamp; ascending addresses): written on the device by the GPU backend
+    (sg_rv64_memory_table), built with numpy otherwise."""
+
+    def __init__(self, addrs, values, stamps):
+        self.cells = np.ascontiguousarray(np.stack([np.asarray(addrs, np.uint64), np.asarray(values, np.uint64),
+                                                    np.asarray(stamps, np.uint64)], axis=1).reshape(-1, 3))
+
+    def host_trace(self, air):
+        c = self.cells
+        return air.trace(c[:, 0], c[:, 1], c[:, 2])
+
+    def device_trace(self, bk, air):
+        from . import native
+        m = bk._alloc(air.n, air.width)
+        native.check(bk.L.sg_rv64_memory_table(bk.be.h, bk.st, self.cells.ctypes.data, self.cells.shape[0], air.n,
+                                               m.ptr))
+        return m
+
+    def range_lookups(self, n):
+        """The table's RANGE lookups at n rows: the D0 and D1 pieces of every
+        row's address gap (zero from the last cell on)."""
+        a = self.cells[:, 0]
+        d = (a[1:] - a[:-1] - np.uint64(8)) >> np.uint64(3)
+        return [d & np.uint64(0xFFFF), d >> np.uint64(16), np.zeros(2 * (n - a.size + 1), np.uint64)]
+
+
 class KeccakSource:
     """The KECCAK table of a run's ecalls (timestamp, address, 25 input lanes,
     25 previous timestamps): written on the device by the GPU backend
@@ -1160,9 +1201,9 @@ class KeccakSource:
 
 def tables_from_events(words, ev, host_tables=False):
     """(airs, traces, public) of a run's events: public = {"words", "counts",
-    "output", "cycles", "heights", "label", "terms"}. The CPU, SHIFT and
-    KECCAK entries of traces are table sources the GPU backend writes on the
-    device (stark._gen_trace), or numpy tables with host_tables."""
+    "output", "cycles", "heights", "label", "terms"}. The CPU, SHIFT, MEMORY
+    and KECCAK entries of traces are table sources the GPU backend writes on
+    the device (stark._gen_trace), or numpy tables with host_tables."""
     rec = ev.records
     T = rec.shape[0]
     heights = {"cpu": max(1, (T - 1).bit_length()), "range": 16}
@@ -1183,10 +1224,12 @@ def tables_from_events(words, ev, host_tables=False):
     # (rows past the halt repeat its zero result), the address and timestamp
     # pieces of memory rows
     counted = ev.range_counts is not None
-    op = ((rec[:, 0] >> np.uint64(32)) & np.uint64(0xFF)).astype(np.int64)
-    r = rec[:, 4]
-    look = [] if counted else [(r[:, None] >> np.arange(0, 64, 16, dtype=np.uint64)) & np.uint64(0xFFFF),
-                               np.zeros(4 * (n - T), np.uint64)]
+    if counted:
+        look = []
+    else:
+        op = ((rec[:, 0] >> np.uint64(32)) & np.uint64(0xFF)).astype(np.int64)
+        look = [(rec[:, 4, None] >> np.arange(0, 64, 16, dtype=np.uint64)) & np.uint64(0xFFFF),
+                np.zeros(4 * (n - T), np.uint64)]
     if "bitwise" in chips:
         a = BitwiseAir()
         airs.append(a)
@@ -1198,9 +1241,9 @@ def tables_from_events(words, ev, host_tables=False):
         traces.append(src.host_trace(a) if host_tables else src)
     if "memory" in chips:
         a = MemoryAir(heights["memory"])
-        mt = a.trace(*ev.cells)
+        src = MemorySource(*ev.cells)
         airs.append(a)
-        traces.append(mt)
+        traces.append(src.host_trace(a) if host_tables else src)
         if not counted:
             mem = np.isin(op, [OP_ID["ld"], OP_ID["sd"]])
             addr = mem | (op == KECCAK_OP)
@@ -1208,7 +1251,7 @@ def tables_from_events(words, ev, host_tables=False):
             gap = np.nonzero(mem)[0].astype(np.uint64) - rec[mem, 7]   # (row + 1) - mt - 1
             look += [(ma >> np.uint64(3)) & np.uint64(0xFFFF), np.uint64(8) * (ma >> np.uint64(19)),
                      gap & np.uint64(0xFFFF), gap >> np.uint64(16)]
-        look += [mt[:, MemoryAir.D0], mt[:, MemoryAir.D1]]
+        look += src.range_lookups(a.n)
     if "keccak" in chips:
         a = KeccakAir(heights["keccak"])
         src = KeccakSource(*ev.keccak)

@@ -69,12 +69,13 @@ def test_keccak_guest_scheduled_proof_equals_plain(be):
 
 
 def test_device_chip_tables_equal_the_host_tables(be):
-    """sg_rv64_cpu_table, sg_rv64_keccak_table and sg_rv64_shift_table
-    (tables written on the device from the run's events) against the numpy
-    builders, cell for cell: the Keccak guest (full CPU width), the Fibonacci
-    guest (core width), a branch on low limbs 2^32 - 1 and 0, then random
-    lanes and timestamps and every shift amount in both directions, with
-    padding rows."""
+    """sg_rv64_cpu_table, sg_rv64_keccak_table, sg_rv64_shift_table and
+    sg_rv64_memory_table (tables written on the device from the run's events)
+    against the numpy builders, cell for cell: the Keccak guest (full CPU
+    width), the Fibonacci guest (core width), a branch on low limbs 2^32 - 1
+    and 0, then random lanes and timestamps, every shift amount in both
+    directions, and memory tables of one cell, of as many cells as rows and of
+    address gaps past 2^16 cells, with padding rows."""
     import numpy as np
     bk = GpuBackend(be)
 
@@ -87,7 +88,7 @@ def test_device_chip_tables_equal_the_host_tables(be):
     wrap = rv64.assemble([("li", "t0", -1), ("srli", "t0", "t0", 32), ("li", "t1", 0),
                           ("beq", "t0", "t1", "end"), ("bne", "t0", "t1", "end"), ("li", "t1", 5),
                           "end:", ("li", "a7", 93), ("ecall",)])
-    for words, expect in ((rv64.keccak_program(136 * 11), 3), (rv64.fib_program(3000), 1), (wrap, 2)):
+    for words, expect in ((rv64.keccak_program(136 * 11), 4), (rv64.fib_program(3000), 1), (wrap, 2)):
         ev = RA.native_events(words)
         airs, srcs, _ = RA.tables_from_events(words, ev)
         _, host, _ = RA.tables_from_events(words, ev, host_tables=True)
@@ -112,6 +113,33 @@ def test_device_chip_tables_equal_the_host_tables(be):
     same(ssrc, sair, ssrc.host_trace(sair))
     empty = RA.ShiftSource(np.zeros((0, 3), np.uint64))
     same(empty, RA.ShiftAir(6), empty.host_trace(RA.ShiftAir(6)))
+    for addrs, log_n in (([8], 6), (np.arange(64) * 8 + 4096, 6),
+                         (np.cumsum(rng.integers(1, 2**20, 300)) * 8, 9)):
+        a = np.asarray(addrs, np.uint64)
+        msrc = RA.MemorySource(a, rng.integers(0, 2**64, a.size, dtype=np.uint64),
+                               rng.integers(0, 2**40, a.size, dtype=np.uint64))
+        mair = RA.MemoryAir(log_n)
+        same(msrc, mair, msrc.host_trace(mair))
+
+
+def test_memory_table_rejects_bad_cells(be):
+    """sg_rv64_memory_table refuses, before any launch, cells whose addresses
+    are not ascending multiples of 8 below 2^32, and more cells than rows."""
+    import ctypes as C
+    import numpy as np
+    from lambda_vm_b200 import native
+    bk = GpuBackend(be)
+    m = bk._alloc(64, RA.MemoryAir(6).width)
+    for addrs in ([16, 8], [8, 8], [8, 12], [8, 1 << 32]):
+        cells = np.zeros((len(addrs), 3), np.uint64)
+        cells[:, 0] = addrs
+        rc = bk.L.sg_rv64_memory_table(bk.be.h, bk.st, cells.ctypes.data, len(addrs), 64, m.ptr)
+        assert rc == native.SG_ERR_INVALID, addrs
+    cells = np.zeros((65, 3), np.uint64)
+    cells[:, 0] = np.arange(65) * 8
+    assert bk.L.sg_rv64_memory_table(bk.be.h, bk.st, cells.ctypes.data, 65, 64, m.ptr) == native.SG_ERR_INVALID
+    assert bk.L.sg_rv64_memory_table(bk.be.h, bk.st, cells.ctypes.data, 0, 64, m.ptr) == native.SG_ERR_INVALID
+    bk.free(m)
 
 
 @pytest.mark.parametrize("rows,step", [(256, 2), (1024, 4)])

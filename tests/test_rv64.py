@@ -264,6 +264,20 @@ def test_statement_binds_the_chip_heights():
     assert fp["label"] == RA.statement_label(fw, fp["counts"], fp["output"])
 
 
+def test_memory_source_range_lookups_are_the_table_gaps():
+    """MemorySource.range_lookups (what RANGE counts for the MEMORY table
+    when the table is written on the device) holds the values of the host
+    table's D0 and D1 columns, row for row including padding."""
+    ev = RA.native_events(rv64.keccak_program(136 * 3))
+    src = RA.MemorySource(*ev.cells)
+    for log_n in (RA._log2_rows(len(ev.cells[0])), RA._log2_rows(len(ev.cells[0])) + 2):
+        air = RA.MemoryAir(log_n)
+        t = src.host_trace(air)
+        want = np.bincount(np.concatenate([t[:, air.D0], t[:, air.D1]]).astype(np.int64), minlength=1 << 16)
+        got = np.bincount(np.concatenate(src.range_lookups(air.n)).astype(np.int64), minlength=1 << 16)
+        assert np.array_equal(want, got)
+
+
 def test_keccak_device_program_covers_the_logup_constraints():
     """The KECCAK table's device program: the LogUp constraints only, under
     their indices in the whole program (after its 3383 base constraints, which
