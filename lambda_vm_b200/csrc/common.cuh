@@ -221,6 +221,17 @@ int leaves_row_major(Ctx* ctx, cudaStream_t st, const uint64_t* data, uint64_t n
                      uint64_t col_start, uint64_t col_end, uint32_t rows_per_leaf, int little_endian,
                      uint8_t* out);
 int merkle_inner(Ctx* ctx, cudaStream_t st, uint8_t* nodes, uint64_t num_leaves_pow2);
+
+// FRI commit steps on the device (rounds.cu). fri_state_load_dev puts a host
+// transcript state (an fs::State) into device memory; fri_challenge_dev
+// absorbs d_root (32 bytes, or nothing when null; copied to d_root_out) into
+// the state at d_state and samples the next challenge into d_zeta (3 u64),
+// which fri_fold_dev's fold reads.
+int fri_state_load_dev(Ctx* ctx, cudaStream_t st, const void* host_state, void* d_state);
+int fri_challenge_dev(Ctx* ctx, cudaStream_t st, void* d_state, const uint8_t* d_root, uint8_t* d_root_out,
+                      uint64_t* d_zeta);
+int fri_fold_dev(Ctx* ctx, cudaStream_t st, const uint64_t* d_in, uint64_t h, const uint64_t* d_inv_tw,
+                 const uint64_t* d_zeta, uint64_t* d_out, uint64_t* d_inv_tw_next, uint8_t* d_leaves);
 // One-row leaves absorbed in column windows [c0, c0 + w) with the sponge
 // state (25 x num_rows u64) kept in HBM between windows; see merkle.cu.
 int leaves_window(Ctx* ctx, cudaStream_t st, const uint64_t* data, uint64_t num_rows, uint64_t row_u64, uint64_t c0,

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "fs.cuh"
 
 namespace sg {
 namespace {
@@ -310,7 +311,11 @@ extern "C" int sg_prove_table(sg_ctx* c, void* stream, sg_transcript* t, const s
                                gh.data(), gt.data(), 2, d_inv_h, d_inv_t, 1, d_deep));
     bf.release(d_inv_h);
     bf.release(d_inv_t);
-    // ---- FRI commit phase
+    // ---- FRI commit phase. The transcript steps between layers (absorb a
+    // root, sample the next challenge) run on the device on a copy of the
+    // transcript, so every layer is enqueued without a host round trip; the
+    // advanced transcript, the roots and the final codeword come back in one
+    // copy (laid out state | roots | codeword in one device block).
     struct Layer {
         uint64_t* ev;
         uint64_t len;
@@ -322,20 +327,30 @@ extern "C" int sg_prove_table(sg_ctx* c, void* stream, sg_transcript* t, const s
     uint64_t ev_len = N;
     const uint64_t* tw = j->d_tw0;
     uint64_t* own_tw = nullptr;
+    const uint64_t state_bytes = (sizeof(fs::State) + 63) / 64 * 64, roots_bytes = 32ull * shp.fri_layers;
+    const uint64_t final_len = shp.total_folds > 0 ? N >> shp.total_folds : 0;
+    uint8_t* d_back = nullptr;
+    uint64_t* d_zeta = nullptr;
+    if (shp.total_folds > 0) {
+        d_back = (uint8_t*)bf.alloc(state_bytes + roots_bytes + final_len * 24, &rc);
+        d_zeta = (uint64_t*)bf.alloc(3 * 8, &rc);
+        if (rc) return rc;
+        SG_TRY(fri_state_load_dev(ctx, st, &t->s, d_back));
+    }
+    const uint8_t* prev_root = nullptr;
     for (uint32_t l = 0; l < shp.fri_layers; ++l) {
-        const E3 zeta = sample_e3(t);
         const uint64_t h = ev_len / 2;
         uint64_t* ev2 = (uint64_t*)bf.alloc(h * 3 * 8, &rc);
         uint64_t* tw2 = (uint64_t*)bf.alloc((h / 2 ? h / 2 : 1) * 8, &rc);
         uint8_t* nodes = (uint8_t*)bf.alloc((2 * (h / 2) - 1) * 32, &rc);
         if (rc) return rc;
         const uint64_t nl = h / 2;
-        SG_TRY(sg_fri_fold_layer(c, st, ev, h, tw, zeta.v, ev2, tw2, nodes + (nl - 1) * 32));
+        SG_TRY(fri_challenge_dev(ctx, st, d_back, prev_root, l ? d_back + state_bytes + 32 * (l - 1) : nullptr,
+                                 d_zeta));
+        SG_TRY(fri_fold_dev(ctx, st, ev, h, tw, d_zeta, ev2, tw2, nodes + (nl - 1) * 32));
         SG_TRY(merkle_inner(ctx, st, nodes, nl));
-        SG_CUDA(cudaMemcpyAsync(o->fri_roots + 32 * l, nodes, 32, cudaMemcpyDeviceToHost, st));
-        SG_CUDA(cudaStreamSynchronize(st));
-        sg_transcript_append(t, o->fri_roots + 32 * l, 32);
-        if (own_tw) bf.release(own_tw);
+        prev_root = nodes;
+        if (own_tw) bf.release(own_tw);  // stream-ordered: the fold above has read it
         layers.push_back({ev2, h, nodes, nl});
         ev = ev2;
         ev_len = h;
@@ -343,16 +358,20 @@ extern "C" int sg_prove_table(sg_ctx* c, void* stream, sg_transcript* t, const s
     }
     std::vector<uint64_t> final_cw;
     if (shp.total_folds > 0) {
-        const E3 zeta = sample_e3(t);
         const uint64_t h = ev_len / 2;
-        uint64_t* evf = (uint64_t*)bf.alloc(h * 3 * 8, &rc);
+        uint64_t* evf = (uint64_t*)(d_back + state_bytes + roots_bytes);
         uint64_t* twf = (uint64_t*)bf.alloc((h / 2 ? h / 2 : 1) * 8, &rc);
         if (rc) return rc;
-        SG_TRY(sg_fri_fold_layer(c, st, ev, h, tw, zeta.v, evf, twf, nullptr));
-        final_cw.resize(h * 3);
-        SG_CUDA(cudaMemcpyAsync(final_cw.data(), evf, h * 24, cudaMemcpyDeviceToHost, st));
+        SG_TRY(fri_challenge_dev(ctx, st, d_back, prev_root,
+                                 prev_root ? d_back + state_bytes + roots_bytes - 32 : nullptr, d_zeta));
+        SG_TRY(fri_fold_dev(ctx, st, ev, h, tw, d_zeta, evf, twf, nullptr));
+        std::vector<uint8_t> back(state_bytes + roots_bytes + h * 24);
+        SG_CUDA(cudaMemcpyAsync(back.data(), d_back, back.size(), cudaMemcpyDeviceToHost, st));
         SG_CUDA(cudaStreamSynchronize(st));
-        bf.release(evf);
+        memcpy(&t->s, back.data(), sizeof(fs::State));
+        memcpy(o->fri_roots, back.data() + state_bytes, roots_bytes);
+        final_cw.resize(h * 3);
+        memcpy(final_cw.data(), back.data() + state_bytes + roots_bytes, h * 24);
         bf.release(twf);
     } else {
         final_cw.resize(ev_len * 3);

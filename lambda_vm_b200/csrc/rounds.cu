@@ -16,6 +16,7 @@
 #include "common.cuh"
 #include "gl.cuh"
 #include "keccak.cuh"
+#include "fs.cuh"
 
 namespace sg {
 
@@ -383,11 +384,12 @@ __device__ __forceinline__ fe3 fold_one(const uint64_t* in, uint64_t j, uint64_t
     return gl::add3(gl::add3(lo, hi), gl::mulb3(gl::mul3(zeta, gl::sub3(lo, hi)), tw));
 }
 
+// zeta is (z0, z1, z2), or read from device memory when dz is non-null.
 __global__ void __launch_bounds__(128) k_fri_fold(const uint64_t* in, uint64_t h, const uint64_t* tw, uint64_t z0,
-                                                  uint64_t z1, uint64_t z2, uint64_t* out, uint64_t* tw_next,
-                                                  uint64_t* leaves) {
+                                                  uint64_t z1, uint64_t z2, const uint64_t* dz, uint64_t* out,
+                                                  uint64_t* tw_next, uint64_t* leaves) {
     const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const fe3 zeta{z0, z1, z2};
+    const fe3 zeta = dz ? fe3{dz[0], dz[1], dz[2]} : fe3{z0, z1, z2};
     if (2 * t >= h) return;
     const uint64_t tw0 = tw[2 * t];
     const fe3 a = gl::canon3(fold_one(in, 2 * t, tw0, zeta));
@@ -717,7 +719,7 @@ int sg_fri_fold_layer(sg_ctx* c, void* stream, const uint64_t* d_in, uint64_t h,
     if (h == 0) return SG_OK;
     const uint64_t threads = (h + 1) / 2;
     k_fri_fold<<<(unsigned)((threads + 127) / 128), 128, 0, (cudaStream_t)stream>>>(
-        d_in, h, d_inv_tw, zeta[0], zeta[1], zeta[2], d_out, d_inv_tw_next, (uint64_t*)d_leaves);
+        d_in, h, d_inv_tw, zeta[0], zeta[1], zeta[2], nullptr, d_out, d_inv_tw_next, (uint64_t*)d_leaves);
     return check_launch(CX(c), "k_fri_fold");
 }
 
@@ -1053,3 +1055,54 @@ extern "C" int sg_field_ops(sg_ctx* c, void* stream, uint32_t op, const uint64_t
     k_field_ops<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(op, d_a, d_b, d_out, n);
     return check_launch(CX(c), "k_field_ops");
 }
+
+// ---- FRI commit phase without host round trips (fri/mod.rs:27-151): the
+// transcript steps between layers run on the device on a copy of the
+// transcript, so a table's layers are all enqueued before anything is read
+// back.
+namespace sg {
+
+// Absorb the previous layer's root when there is one (and keep a copy of it
+// at root_out), then sample the next folding challenge into zeta. One thread:
+// a step is one or two permutations.
+__global__ void k_fri_challenge(fs::State* ts, const uint8_t* root, uint8_t* root_out, uint64_t* zeta) {
+    if (threadIdx.x || blockIdx.x) return;
+    fs::State s = *ts;
+    if (root) {
+        fs::append(s, root, 32);
+        for (int i = 0; i < 32; ++i) root_out[i] = root[i];
+    }
+    uint64_t z[3];
+    fs::sample_ext3(s, z);
+    zeta[0] = z[0], zeta[1] = z[1], zeta[2] = z[2];
+    *ts = s;
+}
+
+// The host transcript's state into device memory, as a kernel argument (no
+// copy from pageable memory, which would wait for the stream).
+__global__ void k_fs_load(fs::State s, fs::State* ts) {
+    if (threadIdx.x || blockIdx.x) return;
+    *ts = s;
+}
+
+int fri_state_load_dev(Ctx* ctx, cudaStream_t st, const void* host_state, void* d_state) {
+    k_fs_load<<<1, 32, 0, st>>>(*(const fs::State*)host_state, (fs::State*)d_state);
+    return check_launch(ctx, "k_fs_load");
+}
+
+int fri_challenge_dev(Ctx* ctx, cudaStream_t st, void* d_state, const uint8_t* d_root, uint8_t* d_root_out,
+                      uint64_t* d_zeta) {
+    k_fri_challenge<<<1, 32, 0, st>>>((fs::State*)d_state, d_root, d_root_out, d_zeta);
+    return check_launch(ctx, "k_fri_challenge");
+}
+
+int fri_fold_dev(Ctx* ctx, cudaStream_t st, const uint64_t* d_in, uint64_t h, const uint64_t* d_inv_tw,
+                 const uint64_t* d_zeta, uint64_t* d_out, uint64_t* d_inv_tw_next, uint8_t* d_leaves) {
+    if (h == 0) return SG_OK;
+    const uint64_t threads = (h + 1) / 2;
+    k_fri_fold<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(d_in, h, d_inv_tw, 0, 0, 0, d_zeta, d_out,
+                                                                  d_inv_tw_next, (uint64_t*)d_leaves);
+    return check_launch(ctx, "k_fri_fold");
+}
+
+}  // namespace sg
