@@ -64,7 +64,7 @@ static __global__ void k_cpu_constraints(const uint64_t* __restrict__ cm, const 
     for (uint64_t row = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; row < rows;
          row += (uint64_t)gridDim.x * blockDim.x) {
         const CRow w{cm, rm, rows, width, row, row + next_step >= rows ? row + next_step - rows : row + next_step};
-        KSink s{beta, mode, out, rows, row, 0, gl::fe3{0, 0, 0}};
+        KSink s{beta, mode, out, rows, row, gl::wzero3(), 0};
         const uint64_t step = w.M(CPU_STEP), c0 = w.M(CPU_C0), c1 = w.M(CPU_C1);
         // one-hot selections and booleans
         s.put(kbool(step));
@@ -200,7 +200,8 @@ static __global__ void k_cpu_constraints(const uint64_t* __restrict__ cm, const 
         }
         if (mode == 0) {
             uint64_t* o = out + 3 * row;
-            o[0] = s.sum.c0, o[1] = s.sum.c1, o[2] = s.sum.c2;
+            const gl::fe3 sum = s.total();
+            o[0] = sum.c0, o[1] = sum.c1, o[2] = sum.c2;
         }
     }
 }
@@ -217,7 +218,7 @@ static __global__ void k_shift_constraints(const uint64_t* __restrict__ cm, cons
     for (uint64_t row = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; row < rows;
          row += (uint64_t)gridDim.x * blockDim.x) {
         const CRow w{cm, rm, rows, SH_WIDTH, row, row};
-        KSink s{beta, mode, out, rows, row, 0, gl::fe3{0, 0, 0}};
+        KSink s{beta, mode, out, rows, row, gl::wzero3(), 0};
         const uint64_t d = w.M(SH_DIR), nd = gl::sub(1, d);
         s.put(kbool(d));
         for (uint32_t i = 0; i < 64; ++i) s.put(kbool(w.M(SH_AB + i)));
@@ -261,7 +262,8 @@ static __global__ void k_shift_constraints(const uint64_t* __restrict__ cm, cons
         }
         if (mode == 0) {
             uint64_t* o = out + 3 * row;
-            o[0] = s.sum.c0, o[1] = s.sum.c1, o[2] = s.sum.c2;
+            const gl::fe3 sum = s.total();
+            o[0] = sum.c0, o[1] = sum.c1, o[2] = sum.c2;
         }
     }
 }

@@ -6,8 +6,9 @@
 // three bits, the parity of five, 16-bit limbs of XORed or chi-ed bits). The
 // generic constraint walk spends ~120 instructions a program node on them;
 // this kernel evaluates the same polynomials directly, one thread per LDE
-// row, and folds them into the composition with the same constraint indices
-// (the KeccakAir emission order), so its sum equals the walk's exactly
+// row, and folds them into the composition under the same constraint indices
+// (the KeccakAir emission order; the kernel's own order keeps column reads
+// few), so its sum equals the walk's exactly
 // (field arithmetic is exact: any evaluation of a polynomial gives the same
 // value). The LogUp constraints of the table stay with the walk.
 #pragma once
@@ -90,24 +91,28 @@ __device__ __forceinline__ uint64_t kxor2(uint64_t x, uint64_t y) {
 __device__ __forceinline__ uint64_t kxor3(uint64_t x, uint64_t y, uint64_t z) { return kxor2(x, kxor2(y, z)); }
 __device__ __forceinline__ uint64_t kdbl(uint64_t v) { return gl::add(v, v); }
 
-// Where the kernel puts each constraint: mode 0 folds beta_c C_c into the
-// row's sum; mode 1 writes C_c to out[c * rows + row].
+// Where a kernel puts each constraint: mode 0 folds beta_c C_c into the
+// row's sum (kept unreduced, reduced once per row by total()); mode 1 writes
+// C_c to out[c * rows + row]. c is the constraint's index in the table's
+// program: given, or the next one after the previous put.
 struct KSink {
     const uint64_t* beta;
     int mode;
     uint64_t* out;
     uint64_t rows, row;
-    uint32_t c;
-    gl::fe3 sum;
-    __device__ __forceinline__ void put(uint64_t v) {
+    gl::wacc3 sum;
+    uint32_t next;
+    __device__ __forceinline__ void put(uint64_t v) { put(next, v); }
+    __device__ __forceinline__ gl::fe3 total() const { return gl::wreduce3(sum); }
+    __device__ __forceinline__ void put(uint32_t c, uint64_t v) {
+        next = c + 1;
         if (mode == 1) {
             uint64_t* o = out + 3 * ((uint64_t)c * rows + row);
             o[0] = gl::canon(v), o[1] = 0, o[2] = 0;
         } else {
             const gl::fe3 b{__ldg(beta + 3 * c), __ldg(beta + 3 * c + 1), __ldg(beta + 3 * c + 2)};
-            sum = gl::add3(sum, gl::mulb3(b, v));
+            gl::wmacb3(sum, b, v);
         }
-        ++c;
     }
 };
 
@@ -124,64 +129,83 @@ __device__ __forceinline__ uint64_t kchi(const KRow& w, const KeccakConsts& kc, 
 }
 
 // One thread per LDE row; mode 0 writes the row's sum over the 3383
-// constraints to out (rows ext3), mode 1 every constraint's value.
+// constraints to out (rows ext3), mode 1 every constraint's value. The
+// constraints are evaluated in an order that reads each column few times
+// (the A' bits twice: once per (x, z) with C, C' and the A limbs, once per
+// (Y, z) for chi's five lanes) and folded under their indices in the table's
+// program:
+//   0..23 round flags boolean, 24 their sum boolean;
+//   25 + 7 (64 x + z) + {0: C, 1: C', 2 + y: A'[x + 5y]} booleans;
+//   2265 + z lane-0-before-iota bits boolean;
+//   2329 + 2 (64 x + z) + {0: C' = C ^ C[x-1] ^ C[x+1] rotated, 1: parity};
+//   2969 + 5 (4 x + l) + y: A[x + 5y] limb l from A' ^ C ^ C';
+//   3069 + 4 (5 X + Y - 1) + l: OUT limb l of lane (X, Y) != (0, 0) from chi;
+//   3165 + z: lane 0's chi bit; 3229 + l: lane 0's OUT limb after iota;
+//   3233.. the transitions and the timestamp gaps, in program order.
 static __global__ void k_keccak_constraints(const uint64_t* __restrict__ cm, const uint64_t* __restrict__ rm, uint64_t rows,
                                      uint64_t next_step, KeccakConsts kc, const uint64_t* __restrict__ beta, int mode,
                                      uint64_t* __restrict__ out) {
     for (uint64_t row = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; row < rows;
          row += (uint64_t)gridDim.x * blockDim.x) {
         KRow w{cm, rm, rows, row, row + next_step >= rows ? row + next_step - rows : row + next_step};
-        KSink s{beta, mode, out, rows, row, 0, gl::fe3{0, 0, 0}};
-        // bit checks: the round flags and their sum, C, C', A' per (x, z), lane 0 before iota
+        KSink s{beta, mode, out, rows, row, gl::wzero3(), 0};
         uint64_t act = 0;
         for (int i = 0; i < 24; ++i) {
             const uint64_t r = w.M(KAIR_R + i);
-            s.put(kbool(r));
+            s.put(i, kbool(r));
             act = gl::add(act, r);
         }
-        s.put(kbool(act));
+        s.put(24, kbool(act));
+        // per (x, z): the C, C' and A' bits, theta, and the A limbs (z descending inside a limb)
         for (int x = 0; x < 5; ++x)
-            for (int z = 0; z < 64; ++z) {
-                s.put(kbool(w.M(KAIR_C + 64 * x + z)));
-                s.put(kbool(w.M(KAIR_CP + 64 * x + z)));
-                for (int y = 0; y < 5; ++y) s.put(kbool(w.M(KAIR_AP + 64 * (x + 5 * y) + z)));
-            }
-        for (int z = 0; z < 64; ++z) s.put(kbool(w.M(KAIR_B00 + z)));
-        // theta: C' = C ^ C[x-1] ^ rot(C[x+1], 1); the five A' bits and C' have even parity
-        for (int x = 0; x < 5; ++x)
-            for (int z = 0; z < 64; ++z) {
-                const uint64_t cp = w.M(KAIR_CP + 64 * x + z);
-                s.put(gl::sub(cp, kxor3(w.M(KAIR_C + 64 * x + z), w.M(KAIR_C + 64 * ((x + 4) % 5) + z),
-                                        w.M(KAIR_C + 64 * ((x + 1) % 5) + ((z + 63) & 63)))));
-                uint64_t t = 0;
-                for (int y = 0; y < 5; ++y) t = gl::add(t, w.M(KAIR_AP + 64 * (x + 5 * y) + z));
-                t = gl::sub(t, cp);
-                s.put(gl::mul(gl::mul(t, gl::sub(t, 2)), gl::sub(t, 4)));
-            }
-        // A's limbs are the bits A' ^ C ^ C' (lanes of a column innermost)
-        for (int x = 0; x < 5; ++x)
-            for (int l = 0; l < 4; ++l)
-                for (int y = 0; y < 5; ++y) {
-                    uint64_t acc = 0;
-                    for (int i = 15; i >= 0; --i) {
-                        const int z = 16 * l + i;
-                        acc = gl::add(kdbl(acc), kxor3(w.M(KAIR_AP + 64 * (x + 5 * y) + z), w.M(KAIR_C + 64 * x + z),
-                                                       w.M(KAIR_CP + 64 * x + z)));
-                    }
-                    s.put(gl::sub(w.M(KAIR_A + 4 * (x + 5 * y) + l), acc));
+            for (int l = 0; l < 4; ++l) {
+                uint64_t acc[5] = {0, 0, 0, 0, 0};
+                for (int i = 15; i >= 0; --i) {
+                    const int z = 16 * l + i;
+                    const uint32_t b = 25 + 7 * (64 * x + z), t = 2329 + 2 * (64 * x + z);
+                    const uint64_t c = w.M(KAIR_C + 64 * x + z), cp = w.M(KAIR_CP + 64 * x + z);
+                    uint64_t ap[5];
+#pragma unroll
+                    for (int y = 0; y < 5; ++y) ap[y] = w.M(KAIR_AP + 64 * (x + 5 * y) + z);
+                    s.put(b, kbool(c));
+                    s.put(b + 1, kbool(cp));
+#pragma unroll
+                    for (int y = 0; y < 5; ++y) s.put(b + 2 + y, kbool(ap[y]));
+                    s.put(t, gl::sub(cp, kxor3(c, w.M(KAIR_C + 64 * ((x + 4) % 5) + z),
+                                               w.M(KAIR_C + 64 * ((x + 1) % 5) + ((z + 63) & 63)))));
+                    uint64_t par = 0;
+#pragma unroll
+                    for (int y = 0; y < 5; ++y) par = gl::add(par, ap[y]);
+                    par = gl::sub(par, cp);
+                    s.put(t + 1, gl::mul(gl::mul(par, gl::sub(par, 2)), gl::sub(par, 4)));
+#pragma unroll
+                    for (int y = 0; y < 5; ++y) acc[y] = gl::add(kdbl(acc[y]), kxor3(ap[y], c, cp));
                 }
-        // OUT's limbs (lanes other than 0) are chi of rho-pi of A'
-        for (int x = 0; x < 5; ++x)
-            for (int y = 0; y < 5; ++y) {
-                if (x == 0 && y == 0) continue;
-                for (int l = 0; l < 4; ++l) {
-                    uint64_t acc = 0;
-                    for (int i = 15; i >= 0; --i) acc = gl::add(kdbl(acc), kchi(w, kc, x, y, 16 * l + i));
-                    s.put(gl::sub(w.M(KAIR_OUT + 4 * (x + 5 * y) + l), acc));
-                }
+#pragma unroll
+                for (int y = 0; y < 5; ++y) s.put(2969 + 5 * (4 * x + l) + y, gl::sub(w.M(KAIR_A + 4 * (x + 5 * y) + l), acc[y]));
             }
-        // lane 0 before iota, bit by bit; then iota with the flags' round constant
-        for (int z = 0; z < 64; ++z) s.put(gl::sub(w.M(KAIR_B00 + z), kchi(w, kc, 0, 0, z)));
+        for (int z = 0; z < 64; ++z) s.put(2265 + z, kbool(w.M(KAIR_B00 + z)));
+        // chi per output row Y: the five lanes' rho-pi bits at z, each read once
+        for (int Y = 0; Y < 5; ++Y)
+            for (int l = 0; l < 4; ++l) {
+                uint64_t acc[5] = {0, 0, 0, 0, 0};
+                for (int i = 15; i >= 0; --i) {
+                    const int z = 16 * l + i;
+                    uint64_t bb[5], ch[5];
+#pragma unroll
+                    for (int X = 0; X < 5; ++X) bb[X] = kB(w, kc, X, Y, z);
+#pragma unroll
+                    for (int X = 0; X < 5; ++X) ch[X] = kxor2(bb[X], gl::mul(gl::sub(1, bb[(X + 1) % 5]), bb[(X + 2) % 5]));
+#pragma unroll
+                    for (int X = 0; X < 5; ++X) acc[X] = gl::add(kdbl(acc[X]), ch[X]);
+                    if (Y == 0) s.put(3165 + z, gl::sub(w.M(KAIR_B00 + z), ch[0]));
+                }
+#pragma unroll
+                for (int X = 0; X < 5; ++X)
+                    if (X || Y)
+                        s.put(3069 + 4 * (5 * X + Y - 1) + l, gl::sub(w.M(KAIR_OUT + 4 * (X + 5 * Y) + l), acc[X]));
+            }
+        // lane 0 after iota with the flags' round constant
         for (int l = 0; l < 4; ++l) {
             uint64_t acc = 0;
             for (int i = 15; i >= 0; --i) {
@@ -193,28 +217,30 @@ static __global__ void k_keccak_constraints(const uint64_t* __restrict__ cm, con
                 const uint64_t b = w.M(KAIR_B00 + z);
                 acc = gl::add(kdbl(acc), any ? kxor2(b, rcz) : b);
             }
-            s.put(gl::sub(w.M(KAIR_OUT + l), acc));
+            s.put(3229 + l, gl::sub(w.M(KAIR_OUT + l), acc));
         }
         // transitions inside a permutation
+        uint32_t c = 3233;
         uint64_t g = 0;
         for (int i = 0; i < 23; ++i) {
             const uint64_t r = w.M(KAIR_R + i);
-            s.put(gl::sub(w.N(KAIR_R + i + 1), r));
+            s.put(c++, gl::sub(w.N(KAIR_R + i + 1), r));
             g = gl::add(g, r);
         }
-        for (int c = 0; c < 100; ++c) s.put(gl::mul(g, gl::sub(w.N(KAIR_A + c), w.M(KAIR_OUT + c))));
-        s.put(gl::mul(g, gl::sub(w.N(KAIR_BASE), w.M(KAIR_BASE))));
-        s.put(gl::mul(g, gl::sub(w.N(KAIR_CLK), w.M(KAIR_CLK))));
+        for (int k = 0; k < 100; ++k) s.put(c++, gl::mul(g, gl::sub(w.N(KAIR_A + k), w.M(KAIR_OUT + k))));
+        s.put(c++, gl::mul(g, gl::sub(w.N(KAIR_BASE), w.M(KAIR_BASE))));
+        s.put(c++, gl::mul(g, gl::sub(w.N(KAIR_CLK), w.M(KAIR_CLK))));
         // reads of earlier timestamps
         const uint64_t r0 = w.M(KAIR_R), clk = w.M(KAIR_CLK);
         for (int i = 0; i < 25; ++i) {
             const uint64_t gap = gl::sub(gl::sub(clk, w.M(KAIR_TOLD + i)), 1);
             const uint64_t v = gl::add(w.M(KAIR_TD + 2 * i), gl::mul(1ull << 16, w.M(KAIR_TD + 2 * i + 1)));
-            s.put(gl::mul(r0, gl::sub(gap, v)));
+            s.put(c++, gl::mul(r0, gl::sub(gap, v)));
         }
         if (mode == 0) {
+            const gl::fe3 sum = s.total();
             uint64_t* o = out + 3 * row;
-            o[0] = s.sum.c0, o[1] = s.sum.c1, o[2] = s.sum.c2;
+            o[0] = sum.c0, o[1] = sum.c1, o[2] = sum.c2;
         }
     }
 }
