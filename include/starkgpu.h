@@ -372,6 +372,16 @@ typedef struct {
                                    SG_RV64_CHIP_*); SG_AIR_SHIFT: the SHIFT chip table's (width 148). The
                                    library's own kernel evaluates those; the nodes complete the rest */
     uint32_t hand_roots;
+    const sg_logup_desc* logup; /* NULL, or the table's LogUp descriptor in its standard layout (committed
+                                   columns = interaction pairs (2p, 2p+1), then one accumulated column over
+                                   the one or two interactions left): the library evaluates the table's
+                                   LogUp constraints (lookup.rs:2185-2290: aux_p fa fb - ma fb - mb fa per
+                                   pair, then delta f - m or delta f1 f2 - m1 f2 - m2 f1 with delta =
+                                   aux'_acc - aux_acc - sum_p aux_p + table_offset; fingerprints from
+                                   z = rap[0] and the alpha table) as constraints [logup_root,
+                                   logup_root + num_committed + 1), which no node completes (streaming
+                                   programs only) */
+    uint32_t logup_root;
 } sg_device_program;
 #define SG_AIR_KECCAK 1u
 #define SG_AIR_CPU 2u

@@ -63,6 +63,11 @@ class SynthTableAir:
         self.max_alpha = 3  # alpha^0..alpha^2 used (two values per tuple)
         self.program = self._build_program()
         self.num_transition = len(self.program["roots"])
+        # the GPU prover's program: the checksum walked, the LogUp constraints
+        # evaluated by the library from the descriptor
+        self.device_program = self._build_program(logup=False)
+        self.device_program["logup"] = (1, self.logup_descriptor())
+        self.device_program["num_roots"] = self.num_transition
         self.boundary = [(self.acc_col, True, 0)]  # (column, is_aux, row)
         self.num_parts = 2
 
@@ -78,7 +83,7 @@ class SynthTableAir:
         t = b.mul(b.main(0, self.mult_col), other_fp)
         return t if it["sender"] else b.neg(t)
 
-    def _build_program(self):
+    def _build_program(self, logup=True):
         b = Builder()
         # T0: checksum (base)
         s = None
@@ -86,6 +91,8 @@ class SynthTableAir:
             prod = b.mul(b.main(0, j), b.main(1, j))
             s = prod if s is None else b.add(s, prod)
         b.emit(b.sub(b.main(0, self.sum_col), s))
+        if not logup:
+            return b.program()
         # batched committed terms
         for p in range(self.num_committed):
             ia, ib = self.interactions[2 * p], self.interactions[2 * p + 1]

@@ -404,6 +404,115 @@ __global__ void k_decompose_d2(const uint64_t* h, const uint64_t* inv_2x, uint64
     o[5] = b.c2;
 }
 
+// ---- a table's LogUp constraints from its descriptor (lookup.rs:2185-2290)
+// Interaction k's fingerprint fp_k = z - (bus_k + sum_e alpha^{ea_e}
+// (c_e + sum_t coef_t main[col_t])) and signed multiplicity m_k = mc_k +
+// sum_t mk_t main[ml_t] (the descriptor carries the sign). Committed column p
+// holds the pair (2p, 2p+1): aux_p fa fb - ma fb - mb fa; the accumulated
+// column, with delta = aux'_acc - aux_acc - sum_p aux_p + table_offset, is
+// delta f - m over one remaining interaction or delta f1 f2 - m1 f2 - m2 f1
+// over two.
+struct LogupDev {
+    const uint64_t *bus, *ec, *tc, *mc, *mk;
+    const uint32_t *eo, *ea, *to, *tl, *mo, *ml;
+    uint32_t K, nc;
+};
+
+__device__ __forceinline__ fe3 logup_fp(const LogupDev& d, const Trace& t, uint64_t row, uint32_t k, fe3 z,
+                                        const uint64_t* alpha) {
+    gl::wacc3 acc = gl::wzero3();
+    for (uint32_t e = __ldg(d.eo + k), e1 = __ldg(d.eo + k + 1); e < e1; ++e) {
+        uint64_t v = __ldg(d.ec + e);
+        for (uint32_t q = __ldg(d.to + e), q1 = __ldg(d.to + e + 1); q < q1; ++q)
+            v = gl::add(v, gl::mul(__ldg(d.tc + q), main_cell(t, row, __ldg(d.tl + q))));
+        const uint32_t ai = __ldg(d.ea + e);
+        gl::wmacb3(acc, fe3{__ldg(alpha + 3 * ai), __ldg(alpha + 3 * ai + 1), __ldg(alpha + 3 * ai + 2)}, v);
+    }
+    const fe3 s = gl::wreduce3(acc);
+    return fe3{gl::sub(gl::sub(z.c0, __ldg(d.bus + k)), s.c0), gl::sub(z.c1, s.c1), gl::sub(z.c2, s.c2)};
+}
+
+__device__ __forceinline__ uint64_t logup_mult(const LogupDev& d, const Trace& t, uint64_t row, uint32_t k) {
+    uint64_t m = __ldg(d.mc + k);
+    for (uint32_t q = __ldg(d.mo + k), q1 = __ldg(d.mo + k + 1); q < q1; ++q)
+        m = gl::add(m, gl::mul(__ldg(d.mk + q), main_cell(t, row, __ldg(d.ml + q))));
+    return m;
+}
+
+// mode 0: out[row] (+)= sum_c beta[root0 + c] C_c (add: out already holds the
+// row's other constraints); mode 1: out[(root0 + c) * rows + row] = C_c.
+__global__ void __launch_bounds__(128) k_logup_constraints(Trace t, LogupDev d, fe3 z, const uint64_t* alpha,
+                                                           fe3 off, const uint64_t* beta, uint32_t root0, int mode,
+                                                           int add, uint64_t* out) {
+    for (uint64_t row = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; row < t.rows;
+         row += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t rn = row + t.next_step >= t.rows ? row + t.next_step - t.rows : row + t.next_step;
+        const uint64_t* ar = t.aux + row * t.A * 3;
+        const uint64_t* an = t.aux + (rn * t.A + d.nc) * 3;
+        fe3 sum{0, 0, 0};
+        auto emit = [&](uint32_t c, const fe3& v) {
+            if (mode == 1) {
+                const fe3 w = gl::canon3(v);
+                uint64_t* o = out + 3 * ((uint64_t)(root0 + c) * t.rows + row);
+                o[0] = w.c0, o[1] = w.c1, o[2] = w.c2;
+            } else {
+                const uint64_t* b = beta + 3 * (uint64_t)(root0 + c);
+                sum = gl::add3(sum, gl::mul3(fe3{__ldg(b), __ldg(b + 1), __ldg(b + 2)}, v));
+            }
+        };
+        fe3 delta = gl::sub3(fe3{an[0], an[1], an[2]}, fe3{ar[3 * d.nc], ar[3 * d.nc + 1], ar[3 * d.nc + 2]});
+        for (uint32_t p = 0; p < d.nc; ++p) {
+            const fe3 ap{ar[3 * p], ar[3 * p + 1], ar[3 * p + 2]};
+            delta = gl::sub3(delta, ap);
+            const fe3 fa = logup_fp(d, t, row, 2 * p, z, alpha), fb = logup_fp(d, t, row, 2 * p + 1, z, alpha);
+            const uint64_t ma = logup_mult(d, t, row, 2 * p), mb = logup_mult(d, t, row, 2 * p + 1);
+            emit(p, gl::sub3(gl::sub3(gl::mul3(gl::mul3(ap, fa), fb), gl::mulb3(fb, ma)), gl::mulb3(fa, mb)));
+        }
+        delta = gl::add3(delta, off);
+        const uint32_t k0 = 2 * d.nc;
+        if (d.K == k0 + 1) {
+            const fe3 f = logup_fp(d, t, row, k0, z, alpha);
+            emit(d.nc, gl::sub3(gl::mul3(delta, f), fe3{logup_mult(d, t, row, k0), 0, 0}));
+        } else {
+            const fe3 f1 = logup_fp(d, t, row, k0, z, alpha), f2 = logup_fp(d, t, row, k0 + 1, z, alpha);
+            const uint64_t m1 = logup_mult(d, t, row, k0), m2 = logup_mult(d, t, row, k0 + 1);
+            emit(d.nc, gl::sub3(gl::sub3(gl::mul3(gl::mul3(delta, f1), f2), gl::mulb3(f2, m1)), gl::mulb3(f1, m2)));
+        }
+        if (mode == 0) {
+            if (add) sum = gl::add3(sum, fe3{out[3 * row], out[3 * row + 1], out[3 * row + 2]});
+            out[3 * row] = sum.c0, out[3 * row + 1] = sum.c1, out[3 * row + 2] = sum.c2;
+        }
+    }
+}
+
+// A descriptor the LogUp kernel can evaluate: CSR arrays in range for a main
+// trace of m columns and n_alpha alpha powers, in the standard column layout.
+static int check_logup_desc(const sg_logup_desc* d, uint64_t m, uint32_t n_alpha) {
+    const uint32_t K = d->num_interactions, nc = d->num_committed;
+    SG_CHECK_ARG(K >= 1 && d->bus_ids && d->elem_offsets && d->term_offsets && d->mult_consts && d->mult_term_offsets,
+                 "logup: empty descriptor");
+    SG_CHECK_ARG(K == 2 * nc + 1 || K == 2 * nc + 2, "logup: one or two interactions beyond the committed pairs");
+    SG_CHECK_ARG(d->num_out_cols == nc + 1 && d->out_col_offsets && d->out_col_interactions,
+                 "logup: committed columns plus one accumulated column");
+    for (uint32_t o = 0; o <= nc; ++o)
+        SG_CHECK_ARG(d->out_col_offsets[o] == 2 * o, "logup: committed columns hold interaction pairs");
+    SG_CHECK_ARG(d->out_col_offsets[nc + 1] == K, "logup: the accumulated column holds the rest");
+    for (uint32_t i = 0; i < K; ++i) SG_CHECK_ARG(d->out_col_interactions[i] == i, "logup: interactions in order");
+    for (uint32_t k = 0; k < K; ++k) {
+        SG_CHECK_ARG(d->elem_offsets[k] <= d->elem_offsets[k + 1], "logup: elem offsets");
+        SG_CHECK_ARG(d->mult_term_offsets[k] <= d->mult_term_offsets[k + 1], "logup: mult offsets");
+    }
+    const uint32_t ne = d->elem_offsets[K], nmt = d->mult_term_offsets[K];
+    for (uint32_t e = 0; e < ne; ++e) {
+        SG_CHECK_ARG(d->term_offsets[e] <= d->term_offsets[e + 1], "logup: term offsets");
+        SG_CHECK_ARG(d->elem_alpha_idx[e] < n_alpha, "logup: alpha power index out of range");
+    }
+    const uint32_t nt = ne ? d->term_offsets[ne] : 0;
+    for (uint32_t q = 0; q < nt; ++q) SG_CHECK_ARG(d->term_cols[q] < m, "logup: fingerprint term column out of range");
+    for (uint32_t q = 0; q < nmt; ++q) SG_CHECK_ARG(d->mult_term_cols[q] < m, "logup: multiplicity column out of range");
+    return SG_OK;
+}
+
 }  // namespace sg
 
 using namespace sg;
@@ -495,17 +604,29 @@ int sg_eval_constraints(sg_ctx* c, void* stream, const sg_device_program* prog, 
         else
             SG_CHECK_ARG(false, "unknown hand kernel");
     }
+    // LogUp constraints evaluated from the table's descriptor: [lg_root, lg_root + lg_n)
+    const sg_logup_desc* lg = prog->logup;
+    const uint32_t lg_root = lg ? prog->logup_root : 0, lg_n = lg ? lg->num_committed + 1 : 0;
+    if (lg) {
+        SG_CHECK_ARG(prog->node_roots, "LogUp constraints from a descriptor need a streaming program");
+        SG_TRY(check_logup_desc(lg, m, n_alpha));
+        SG_CHECK_ARG(n_rap >= 1 && rap, "LogUp constraints need z = rap[0]");
+        SG_CHECK_ARG(a >= lg_n && d_aux, "LogUp constraints need the committed and accumulated aux columns");
+        SG_CHECK_ARG(lg_root >= hand && (uint64_t)lg_root + lg_n <= nr, "LogUp constraint indices out of range");
+    }
+    auto by_library = [&](uint32_t c) { return c < hand || (c >= lg_root && c - lg_root < lg_n); };
     if (prog->node_roots) {
         // streaming: every constraint completed by exactly one instruction
-        // (those of a hand kernel by none)
+        // (those of a hand kernel or of the LogUp descriptor by none)
         std::vector<uint8_t> seen(nr, 0);
         for (uint32_t i = 0; i < nn; ++i) {
             const uint32_t c = prog->node_roots[i];
             if (c == NO_ROOT) continue;
-            SG_CHECK_ARG(c < nr && c >= hand && !seen[c], "node_roots: constraint index out of range or repeated");
+            SG_CHECK_ARG(c < nr && !by_library(c) && !seen[c], "node_roots: constraint index out of range or repeated");
             seen[c] = 1;
         }
-        for (uint32_t c = hand; c < nr; ++c) SG_CHECK_ARG(seen[c], "node_roots: a constraint no instruction completes");
+        for (uint32_t c = 0; c < nr; ++c)
+            SG_CHECK_ARG(seen[c] || by_library(c), "node_roots: a constraint no instruction completes");
     } else {
         for (uint32_t r = 0; r < nr; ++r) {
             const uint32_t e = prog->roots[r];
@@ -532,6 +653,22 @@ int sg_eval_constraints(sg_ctx* c, void* stream, const sg_device_program* prog, 
     const size_t o_ec = put(prog->ext_consts, 24ull * prog->num_ext_consts);
     const size_t o_rap = put(rap, 24ull * n_rap);
     const size_t o_al = put(alpha, 24ull * n_alpha);
+    size_t o_lg[11] = {0};
+    if (lg) {
+        const uint32_t K = lg->num_interactions, ne = lg->elem_offsets[K], nt = ne ? lg->term_offsets[ne] : 0,
+                       nmt = lg->mult_term_offsets[K];
+        o_lg[0] = put(lg->bus_ids, 8ull * K);
+        o_lg[1] = put(lg->elem_consts, 8ull * ne);
+        o_lg[2] = put(lg->term_coefs, 8ull * nt);
+        o_lg[3] = put(lg->mult_consts, 8ull * K);
+        o_lg[4] = put(lg->mult_term_coefs, 8ull * nmt);
+        o_lg[5] = put(lg->elem_offsets, 4ull * (K + 1));
+        o_lg[6] = put(lg->elem_alpha_idx, 4ull * ne);
+        o_lg[7] = put(lg->term_offsets, 4ull * (ne + 1));
+        o_lg[8] = put(lg->term_cols, 4ull * nt);
+        o_lg[9] = put(lg->mult_term_offsets, 4ull * (K + 1));
+        o_lg[10] = put(lg->mult_term_cols, 4ull * nmt);
+    }
     size_t o_beta = 0, o_bcol = 0, o_baux = 0, o_bval = 0, o_bbeta = 0;
     const uint32_t nb = comp ? comp->num_boundary : 0;
     if (comp) {
@@ -592,29 +729,40 @@ int sg_eval_constraints(sg_ctx* c, void* stream, const sg_device_program* prog, 
         const size_t smem = use_smem ? per_thread * T * 8 : 0;
         if (smem > 48 * 1024) cudaFuncSetAttribute(k_constraints, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         const uint32_t* d_nroots = prog->node_roots ? (const uint32_t*)(d_blob + o_nroots) : nullptr;
-        // the KECCAK table's own constraints first: per-row sums the walk starts
-        // from (composition), or their values written directly (per constraint)
+        // the library's own constraint kernels first (a hand-written table
+        // kernel, the LogUp descriptor's): per-row sums the walk starts from
+        // (composition), or their values written directly (per constraint)
         uint64_t* d_extra = nullptr;
         const uint64_t extra_bytes = rows * 24;
+        if (rc == SG_OK && comp && (hand || lg)) rc = dev_alloc(ctx, st, extra_bytes, (void**)&d_extra);
         if (rc == SG_OK && hand) {
-            if (comp) rc = dev_alloc(ctx, st, extra_bytes, (void**)&d_extra);
-            if (rc == SG_OK) {
-                const uint64_t hb = (rows + 127) / 128, hcap = 148ull * 16;
-                const unsigned grid = (unsigned)(hb < hcap ? hb : hcap);
-                if (hand_id == SG_AIR_KECCAK) {
-                    k_keccak_constraints<<<grid, 128, 0, st>>>(d_cm, d_main, rows, next_step, keccak_consts(),
-                                                               d_blob + o_beta, comp ? 0 : 1, comp ? d_extra : d_out);
-                    rc = check_launch(ctx, "k_keccak_constraints");
-                } else if (hand_id == SG_AIR_SHIFT) {
-                    k_shift_constraints<<<grid, 128, 0, st>>>(d_cm, d_main, rows, next_step, d_blob + o_beta,
-                                                              comp ? 0 : 1, comp ? d_extra : d_out);
-                    rc = check_launch(ctx, "k_shift_constraints");
-                } else {
-                    k_cpu_constraints<<<grid, 128, 0, st>>>(d_cm, d_main, m, rows, next_step, hand_chips,
-                                                            d_blob + o_beta, comp ? 0 : 1, comp ? d_extra : d_out);
-                    rc = check_launch(ctx, "k_cpu_constraints");
-                }
+            const uint64_t hb = (rows + 127) / 128, hcap = 148ull * 16;
+            const unsigned grid = (unsigned)(hb < hcap ? hb : hcap);
+            if (hand_id == SG_AIR_KECCAK) {
+                k_keccak_constraints<<<grid, 128, 0, st>>>(d_cm, d_main, rows, next_step, keccak_consts(),
+                                                           d_blob + o_beta, comp ? 0 : 1, comp ? d_extra : d_out);
+                rc = check_launch(ctx, "k_keccak_constraints");
+            } else if (hand_id == SG_AIR_SHIFT) {
+                k_shift_constraints<<<grid, 128, 0, st>>>(d_cm, d_main, rows, next_step, d_blob + o_beta,
+                                                          comp ? 0 : 1, comp ? d_extra : d_out);
+                rc = check_launch(ctx, "k_shift_constraints");
+            } else {
+                k_cpu_constraints<<<grid, 128, 0, st>>>(d_cm, d_main, m, rows, next_step, hand_chips,
+                                                        d_blob + o_beta, comp ? 0 : 1, comp ? d_extra : d_out);
+                rc = check_launch(ctx, "k_cpu_constraints");
             }
+        }
+        if (rc == SG_OK && lg) {
+            const uint64_t* b = d_blob;
+            LogupDev dv{b + o_lg[0], b + o_lg[1], b + o_lg[2], b + o_lg[3], b + o_lg[4],
+                        (const uint32_t*)(b + o_lg[5]), (const uint32_t*)(b + o_lg[6]), (const uint32_t*)(b + o_lg[7]),
+                        (const uint32_t*)(b + o_lg[8]), (const uint32_t*)(b + o_lg[9]), (const uint32_t*)(b + o_lg[10]),
+                        lg->num_interactions, lg->num_committed};
+            const uint64_t lb = (rows + 127) / 128, lcap = 148ull * 16;
+            k_logup_constraints<<<(unsigned)(lb < lcap ? lb : lcap), 128, 0, st>>>(
+                t, dv, fe3{rap[0], rap[1], rap[2]}, d_blob + o_al, u.offset, d_blob + o_beta, lg_root, comp ? 0 : 1,
+                hand ? 1 : 0, comp ? d_extra : d_out);
+            rc = check_launch(ctx, "k_logup_constraints");
         }
         if (rc == SG_OK) {
             k_constraints<<<(unsigned)blocks, T, smem, st>>>((const uint4*)(d_blob + o_nodes), nn,

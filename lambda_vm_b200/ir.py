@@ -118,7 +118,10 @@ def lower(prog, stream=True):
     values occupy slots, so the slot file stays small whatever the width."""
     nodes, dims, roots = prog["nodes"], prog["dims"], prog["roots"]
     # a device program may name its constraints' indices in a larger program
-    # whose first constraints a hand-written kernel evaluates (prog["hand"])
+    # (prog["num_roots"] constraints) whose first constraints a hand-written
+    # kernel evaluates (prog["hand"]) and whose LogUp constraints the library
+    # evaluates from the table's descriptor (prog["logup"] = (first index,
+    # descriptor))
     index = prog.get("root_index", list(range(len(roots))))
     n = len(nodes)
     base_consts = list(prog["base_consts"])
@@ -232,7 +235,41 @@ def lower(prog, stream=True):
         assert stream, "a hand kernel's program is a streaming program"
         low["hand_kernel"], low["hand_roots"] = prog["hand"]
         low["num_roots"] = prog["hand"][1] + len(roots)
+    if "logup" in prog:
+        # the table's LogUp constraints, evaluated by the library from its descriptor
+        assert stream, "LogUp constraints from a descriptor need a streaming program"
+        low["logup_root"], low["logup_desc"] = prog["logup"]
+    if "num_roots" in prog:
+        low["num_roots"] = prog["num_roots"]
     return low
+
+
+def restrict(prog, keep):
+    """The program of the nodes the roots `keep` (indices into prog["roots"])
+    depend on, renumbered in their order, with those roots in that order."""
+    nodes, dims = prog["nodes"], prog["dims"]
+    need = [False] * len(nodes)
+    stack = [prog["roots"][c] for c in keep]
+    while stack:
+        i = stack.pop()
+        if not need[i]:
+            need[i] = True
+            stack.extend(_operands(nodes[i]))
+    new_id, out, out_dims = {}, [], []
+    for i, nd in enumerate(nodes):
+        if not need[i]:
+            continue
+        new_id[i] = len(out)
+        if nd[0] in ("add", "sub", "mul"):
+            nd = (nd[0], new_id[nd[1]], new_id[nd[2]])
+        elif nd[0] in ("neg", "embed"):
+            nd = (nd[0], new_id[nd[1]])
+        out.append(nd)
+        out_dims.append(dims[i])
+    roots = [new_id[prog["roots"][c]] for c in keep]
+    return {"nodes": out, "dims": out_dims, "base_consts": list(prog["base_consts"]),
+            "ext_consts": list(prog["ext_consts"]), "roots": roots,
+            "num_base": sum(1 for r in roots if out_dims[r] == BASE)}
 
 
 def lowered(prog):
@@ -246,6 +283,7 @@ def lowered(prog):
 
 def device_program(air):
     """The program the GPU prover runs for `air`: its device_program when it
-    has one (a program whose first constraints a hand-written kernel
-    evaluates), else its constraint program."""
+    has one (a program some of whose constraints the library's own kernels
+    evaluate: a hand-written table kernel, the LogUp constraints from the
+    table's descriptor), else its constraint program."""
     return getattr(air, "device_program", None) or air.program

@@ -467,7 +467,35 @@ def _program_struct(lowered, keep):
     p.node_roots = arr(lowered["node_roots"], np.uint32) if lowered.get("node_roots") is not None else None
     p.hand_kernel = int(lowered.get("hand_kernel", 0))
     p.hand_roots = int(lowered.get("hand_roots", 0))
+    if lowered.get("logup_desc") is not None:
+        d = logup_struct(lowered["logup_desc"], keep)
+        keep.append(d)
+        p.logup = C.addressof(d)
+        p.logup_root = int(lowered["logup_root"])
     return p
+
+
+def logup_struct(desc, keep):
+    """sg_logup_desc of a LogUp descriptor dict (AIR.logup_descriptor()); the
+    arrays it points to are appended to keep."""
+    def arr(name, dt):
+        a = np.ascontiguousarray(desc[name], dt)
+        if a.size == 0:
+            a = np.zeros(1, dt)
+        keep.append(a)
+        return a.ctypes.data
+
+    d = native.LogupDesc()
+    d.num_interactions = desc["num_interactions"]
+    for nm, dt in (("bus_ids", np.uint64), ("elem_offsets", np.uint32), ("elem_alpha_idx", np.uint32),
+                   ("elem_consts", np.uint64), ("term_offsets", np.uint32), ("term_coefs", np.uint64),
+                   ("term_cols", np.uint32), ("out_col_offsets", np.uint32), ("out_col_interactions", np.uint32),
+                   ("mult_consts", np.uint64), ("mult_term_offsets", np.uint32), ("mult_term_coefs", np.uint64),
+                   ("mult_term_cols", np.uint32)):
+        setattr(d, nm, arr(nm, dt))
+    d.num_out_cols = desc["num_out_cols"]
+    d.num_committed = desc["num_committed"]
+    return d
 
 
 def eval_constraints_on_device(lowered, main, aux, rap, alpha, table_offset, next_step, composition=None, be=None):

@@ -64,7 +64,7 @@ class DeviceProgram(C.Structure):
                 ("num_base_consts", C.c_uint32), ("ext_consts", C.c_void_p), ("num_ext_consts", C.c_uint32),
                 ("roots", C.c_void_p), ("num_roots", C.c_uint32), ("num_base_slots", C.c_uint32),
                 ("num_ext_slots", C.c_uint32), ("node_roots", C.c_void_p), ("hand_kernel", C.c_uint32),
-                ("hand_roots", C.c_uint32)]
+                ("hand_roots", C.c_uint32), ("logup", C.c_void_p), ("logup_root", C.c_uint32)]
 
 
 class Composition(C.Structure):

@@ -48,7 +48,7 @@ import numpy as np
 
 from . import field as F
 from .air import split_interactions
-from .ir import Builder
+from .ir import Builder, restrict
 from .rv64 import EXIT, KECCAK, KECCAK_RC, KECCAK_ROT, MASK64, OP_ID, OPS, decode, run
 
 P = F.P
@@ -62,17 +62,32 @@ _PROGRAMS = {}  # constraint programs by (table, parameters): a table's program 
 
 def _hand_program(air, key, kernel):
     """The GPU prover's program for a table whose base constraints a
-    hand-written library kernel evaluates (SG_AIR_* `kernel`): the LogUp
-    constraints only, under their indices in the table's whole program,
-    which come after its base constraints."""
+    hand-written library kernel evaluates (SG_AIR_* `kernel`): no nodes; the
+    library also evaluates the LogUp constraints, which follow the base
+    constraints in the table's whole program, from the table's descriptor."""
     if key not in _PROGRAMS:
         nb = air.program["num_base"]
-        b = Builder()
-        air._emit_logup(b)
-        prog = b.program()
-        assert prog["num_base"] == 0 and nb + len(prog["roots"]) == len(air.program["roots"])
-        prog["root_index"] = [nb + c for c in range(len(prog["roots"]))]
+        prog = Builder().program()
+        assert nb + air.num_committed + 1 == len(air.program["roots"])
+        prog["root_index"] = []
         prog["hand"] = (kernel, nb)
+        prog["logup"] = (nb, air.logup_descriptor())
+        prog["num_roots"] = len(air.program["roots"])
+        _PROGRAMS[key] = prog
+    return _PROGRAMS[key]
+
+
+def _logup_program(air, key):
+    """The GPU prover's program for a table without a hand-written kernel:
+    its base constraints walked, its LogUp constraints (which follow them in
+    the table's whole program) evaluated by the library from its descriptor."""
+    if key not in _PROGRAMS:
+        full = air.program
+        nb = full["num_base"]
+        assert nb + air.num_committed + 1 == len(full["roots"])
+        prog = restrict(full, range(nb))
+        prog["logup"] = (nb, air.logup_descriptor())
+        prog["num_roots"] = len(full["roots"])
         _PROGRAMS[key] = prog
     return _PROGRAMS[key]
 
@@ -576,6 +591,7 @@ class RangeAir(BusAir):
         self.log_n, self.n, self.width = 16, 1 << 16, 3
         self._logup_setup([{"bus": BUS_RANGE, "sender": False, "mult": _col(self.M), "elems": [_col(self.V)]}])
         self.program = self._program(("range",))
+        self.device_program = _logup_program(self, ("range-device",))
 
     def _build_program(self):
         b = Builder()
@@ -616,6 +632,7 @@ class BitwiseAir(BusAir):
         self._logup_setup([{"bus": BUS_BITWISE, "sender": False, "mult": _col(m), "elems": [(k, []), xs, ys, _col(r)]}
                            for k, r, m in ((1, self.XOR, self.MX), (2, self.OR, self.MO), (3, self.AND, self.MAN))])
         self.program = self._program(("bitwise",))
+        self.device_program = _logup_program(self, ("bitwise-device",))
 
     def _build_program(self):
         b = Builder()
@@ -788,6 +805,7 @@ class MemoryAir(BusAir):
             {"bus": BUS_WRAP, "sender": True, "mult": (1, [(NEG_ONE, self.NW)]), "elems": [(1, [])]},
         ])
         self.program = self._program(("memory",))
+        self.device_program = _logup_program(self, ("memory-device",))
 
     def _build_program(self):
         b = Builder()

@@ -224,3 +224,73 @@ def test_shift_table_kernel_equals_the_walk(be):
             "boundary": [(air.acc_col, True, rf((3,)), rf((3,)))], "b_z_inv": rf((1, rows))}
     assert np.array_equal(mc.eval_constraints_on_device(full, main, aux, rap, alpha, off, 2, comp, be),
                           mc.eval_constraints_on_device(dev, main, aux, rap, alpha, off, 2, comp, be))
+
+
+def _tables_with_logup_programs():
+    from lambda_vm_b200.air import SynthTableAir
+    return [("range", RA.RangeAir()), ("bitwise", RA.BitwiseAir()), ("memory", RA.MemoryAir(9)),
+            ("synth2", SynthTableAir(9, 10, num_interactions=2)), ("synth4", SynthTableAir(9, 24, num_interactions=4)),
+            ("synth6", SynthTableAir(9, 40, num_interactions=6))]
+
+
+@pytest.mark.parametrize("name", [n for n, _ in _tables_with_logup_programs()])
+def test_logup_descriptor_constraints_equal_the_walk(be, name):
+    """The tables whose device program walks only the base constraints and
+    leaves the LogUp ones to the library's descriptor kernel
+    (k_logup_constraints): RANGE, BITWISE, MEMORY and synthetic chip tables
+    of one and two committed pairs and a two-interaction tail (the RV64
+    CPU, SHIFT and KECCAK tables, with one- and two-interaction tails, are
+    covered with their hand kernels above), against the walk of the whole
+    program on random field elements: every constraint and the composition,
+    exactly."""
+    import numpy as np
+    from lambda_vm_b200 import math_cuda as mc
+    from lambda_vm_b200.ir import lower
+    P_ = 0xFFFFFFFF00000001
+    air = dict(_tables_with_logup_programs())[name]
+    rng = np.random.default_rng(len(name) * 101 + air.width)
+    rf = lambda shape: np.where((x := rng.integers(0, 2**64, size=shape, dtype=np.uint64)) >= np.uint64(P_),
+                                x - np.uint64(P_), x)
+    full, dev = lower(air.program), lower(air.device_program)
+    assert dev["logup_desc"] is not None and dev["num_roots"] == len(full["roots"])
+    rows = 1 << 9
+    main, aux = rf((rows, air.width)), rf((rows, 3 * air.aux_width))
+    rap, alpha, off = rf((2, 3)), rf((air.max_alpha, 3)), rf((3,))
+    assert np.array_equal(mc.eval_constraints_on_device(full, main, aux, rap, alpha, off, 2, None, be),
+                          mc.eval_constraints_on_device(dev, main, aux, rap, alpha, off, 2, None, be))
+    comp = {"beta": rf((len(full["roots"]), 3)), "z_inv": rf((rows // 4,)),
+            "boundary": [(air.acc_col, True, rf((3,)), rf((3,)))], "b_z_inv": rf((1, rows))}
+    assert np.array_equal(mc.eval_constraints_on_device(full, main, aux, rap, alpha, off, 2, comp, be),
+                          mc.eval_constraints_on_device(dev, main, aux, rap, alpha, off, 2, comp, be))
+
+
+def test_logup_descriptor_is_validated(be):
+    """sg_eval_constraints refuses, before any launch, a LogUp descriptor
+    outside the kernel's layout or reading out of range, and LogUp indices a
+    node also completes or beyond the program."""
+    import copy
+    import numpy as np
+    from lambda_vm_b200 import math_cuda as mc, native
+    from lambda_vm_b200.air import SynthTableAir
+    from lambda_vm_b200.ir import lower
+    air = SynthTableAir(6, 12, num_interactions=4)
+    dev = lower(air.device_program)
+    rows = 64
+    main = np.zeros((rows, air.width), np.uint64)
+    aux = np.zeros((rows, 3 * air.aux_width), np.uint64)
+    rap, alpha, off = np.zeros((2, 3), np.uint64), np.zeros((air.max_alpha, 3), np.uint64), np.zeros(3, np.uint64)
+    mc.eval_constraints_on_device(dev, main, aux, rap, alpha, off, 2, None, be)
+
+    def bad(edit):
+        d = copy.deepcopy({k: v for k, v in dev.items()})
+        edit(d, d["logup_desc"])
+        with pytest.raises(native.SgError, match="INVALID"):
+            mc.eval_constraints_on_device(d, main, aux, rap, alpha, off, 2, None, be)
+
+    bad(lambda d, g: g.__setitem__("term_cols", np.array([air.width] + list(g["term_cols"][1:]), np.uint32)))
+    bad(lambda d, g: g.__setitem__("mult_term_cols", np.array([air.width + 5] * len(g["mult_term_cols"]), np.uint32)))
+    bad(lambda d, g: g.__setitem__("elem_alpha_idx", np.array([air.max_alpha] * len(g["elem_alpha_idx"]), np.uint32)))
+    bad(lambda d, g: g.__setitem__("out_col_interactions", np.array([1, 0, 2, 3], np.uint32)))
+    bad(lambda d, g: g.__setitem__("num_committed", 0))
+    bad(lambda d, g: d.__setitem__("logup_root", 0))
+    bad(lambda d, g: d.__setitem__("logup_root", d["num_roots"] - 1))

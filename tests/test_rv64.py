@@ -279,15 +279,32 @@ def test_memory_source_range_lookups_are_the_table_gaps():
 
 
 def test_keccak_device_program_covers_the_logup_constraints():
-    """The KECCAK table's device program: the LogUp constraints only, under
-    their indices in the whole program (after its 3383 base constraints, which
-    the library's kernel evaluates), every one completed once."""
+    """The KECCAK table's device program: no nodes; the library's kernels
+    evaluate its 3383 base constraints and, from the table's LogUp
+    descriptor, its LogUp constraints, which follow them in the whole
+    program (one per committed pair, then the accumulated column)."""
     from lambda_vm_b200.ir import lower
     air = RA.KeccakAir(6)
     full = air.program
     dev = lower(air.device_program)
     nb = full["num_base"]
     assert nb == 3383 and dev["hand_kernel"] == 1 and dev["hand_roots"] == nb
-    assert dev["num_roots"] == len(full["roots"])
-    done = sorted(int(c) for c in dev["node_roots"] if c != 0xFFFFFFFF)
-    assert done == list(range(nb, len(full["roots"])))
+    assert dev["num_roots"] == len(full["roots"]) and len(dev["nodes"]) == 0
+    assert dev["logup_root"] == nb and nb + air.num_committed + 1 == len(full["roots"])
+    d = dev["logup_desc"]
+    assert d["num_committed"] == air.num_committed and d["num_interactions"] in (2 * air.num_committed + 1,
+                                                                                 2 * air.num_committed + 2)
+    assert list(d["out_col_offsets"]) == [2 * c for c in range(air.num_committed + 1)] + [d["num_interactions"]]
+
+
+def test_synthetic_device_program_leaves_logup_to_the_descriptor():
+    """A synthetic chip table's device program walks its base constraint
+    only; its LogUp constraints (indices 1..) come from its descriptor."""
+    from lambda_vm_b200.air import SynthTableAir
+    from lambda_vm_b200.ir import lower
+    for k in (2, 4, 6):
+        air = SynthTableAir(6, 12, num_interactions=k)
+        dev = lower(air.device_program)
+        assert dev["num_roots"] == len(air.program["roots"]) == 2 + air.num_committed
+        assert sorted(int(c) for c in dev["node_roots"] if c != 0xFFFFFFFF) == [0]
+        assert dev["logup_root"] == 1 and dev["logup_desc"]["num_committed"] == air.num_committed
