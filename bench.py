@@ -44,11 +44,14 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-proof-summary", action="store_true",
                     help="skip the multi-table proof summary the default line carries at N = 1")
-    ap.add_argument("--workload", default="commit", choices=["commit", "proof", "serve", "rounds", "vm"],
+    ap.add_argument("--workload", default="commit",
+                    choices=["commit", "proof", "serve", "rounds", "vm", "constraints"],
                     help="commit: LDE + Merkle commit of one trace (default); proof: multi-table proof, plain vs "
                          "scheduled; serve: Poisson stream of proof jobs, concurrent admission vs one at a time; "
                          "rounds: the round-2..4 kernels of one large table, one by one; vm: an RV64 guest (--guest) "
-                         "executed and its execution proved")
+                         "executed and its execution proved; constraints: the RV64 tables' constraint evaluation")
+    ap.add_argument("--constraint-tables", default="keccak:19,cpu:22,shift:20",
+                    help="constraints: table:log2(LDE rows) list (keccak, cpu, shift)")
     ap.add_argument("--fib-n", type=int, default=30000, help="vm: Fibonacci loop iterations (5 cycles each)")
     ap.add_argument("--guest", default="fib", choices=["fib", "keccak"], help="vm: which guest")
     ap.add_argument("--vm-steps", type=int, default=3, help="vm: timed proofs per form")
@@ -616,6 +619,58 @@ def run_rounds(a):
                       "data": "synthetic (seeded uniform words)", "kernels": out}), flush=True)
 
 
+def run_constraints(a):
+    """Constraint evaluation (composition mode, sg_eval_constraints) of the
+    RV64 tables on random field elements at LDE heights --constraint-tables
+    (default: the 1 MiB Keccak guest's KECCAK 2^19, CPU 2^22 and SHIFT 2^20
+    LDE rows): the column-major copy, the table's hand-written kernel, the
+    LogUp kernel and the walk, one call per step (median of `steps` after
+    `warmup`, the call synchronous)."""
+    import ctypes as C
+    import torch
+    from lambda_vm_b200 import math_cuda as mc, native
+    from lambda_vm_b200 import rv64_air as RA
+    from lambda_vm_b200.device import backend
+    from lambda_vm_b200.ir import device_program, lowered
+    L = native.lib()
+    be = backend(0)
+    make = {"keccak": lambda: RA.KeccakAir(6), "cpu": lambda: RA.CpuAir([0x73], 6, RA.CHIPS),
+            "shift": lambda: RA.ShiftAir(6)}
+    out = {}
+    for spec in a.constraint_tables.split(","):
+        name, log_rows = spec.split(":")
+        air, rows = make[name](), 1 << int(log_rows)
+        keep = []
+        prog = mc._program_struct(lowered(device_program(air)), keep)
+        g = torch.Generator(device="cuda")
+        g.manual_seed(1)
+        R = lambda k: torch.randint(0, 2**62, (k,), dtype=torch.int64, device="cuda", generator=g)
+        main, aux, zinv = R(rows * air.width), R(rows * 3 * air.aux_width), R(rows // 2)
+        res = torch.empty(rows * 3, dtype=torch.int64, device="cuda")
+        rng = np.random.default_rng(2)
+        beta = rng.integers(0, 2**62, size=3 * prog.num_roots, dtype=np.uint64)
+        rap = rng.integers(0, 2**62, size=6, dtype=np.uint64)
+        al = rng.integers(0, 2**62, size=3 * air.max_alpha, dtype=np.uint64)
+        off = np.zeros(3, np.uint64)
+        c = native.Composition()
+        c.beta_trans, c.d_z_inv, c.z_len, c.num_boundary = beta.ctypes.data, zinv.data_ptr(), rows // 2, 0
+        ts = []
+        for it in range(a.warmup + a.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            native.check(L.sg_eval_constraints(be.h, None, C.byref(prog), rap.ctypes.data, 2, al.ctypes.data,
+                                               air.max_alpha, off.ctypes.data, main.data_ptr(), air.width,
+                                               aux.data_ptr(), air.aux_width, rows, 2, C.byref(c), res.data_ptr()))
+            if it >= a.warmup:
+                ts.append(1e3 * (time.perf_counter() - t0))
+        out[f"{name}_2^{log_rows}_rows_ms"] = round(statistics.median(ts), 3) if ts else None
+        del main, aux, zinv, res
+        torch.cuda.empty_cache()
+    print(json.dumps({"metric": "constraint evaluation per table (RV64 tables, composition)", "unit": "ms",
+                      "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "higher_is_better": False,
+                      "data": "synthetic (seeded uniform field elements)", "tables": out}), flush=True)
+
+
 def main():
     a = parse()
     if a.workload == "proof" and a.impl == "ours":
@@ -633,6 +688,9 @@ def main():
         return
     if a.workload == "vm" and a.impl == "ours":
         run_vm(a)
+        return
+    if a.workload == "constraints" and a.impl == "ours":
+        run_constraints(a)
         return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -418,13 +418,19 @@ struct LogupDev {
     uint32_t K, nc;
 };
 
+// coef * x, without the product for the common coefficients 1 and -1 (the
+// descriptor is the same for every thread, so the branch is uniform)
+__device__ __forceinline__ uint64_t logup_scale(uint64_t coef, uint64_t x) {
+    return coef == 1 ? x : coef == 0xFFFFFFFF00000000ULL ? gl::neg(x) : gl::mul(coef, x);
+}
+
 __device__ __forceinline__ fe3 logup_fp(const LogupDev& d, const Trace& t, uint64_t row, uint32_t k, fe3 z,
                                         const uint64_t* alpha) {
     gl::wacc3 acc = gl::wzero3();
     for (uint32_t e = __ldg(d.eo + k), e1 = __ldg(d.eo + k + 1); e < e1; ++e) {
         uint64_t v = __ldg(d.ec + e);
         for (uint32_t q = __ldg(d.to + e), q1 = __ldg(d.to + e + 1); q < q1; ++q)
-            v = gl::add(v, gl::mul(__ldg(d.tc + q), main_cell(t, row, __ldg(d.tl + q))));
+            v = gl::add(v, logup_scale(__ldg(d.tc + q), main_cell(t, row, __ldg(d.tl + q))));
         const uint32_t ai = __ldg(d.ea + e);
         gl::wmacb3(acc, fe3{__ldg(alpha + 3 * ai), __ldg(alpha + 3 * ai + 1), __ldg(alpha + 3 * ai + 2)}, v);
     }
@@ -435,7 +441,7 @@ __device__ __forceinline__ fe3 logup_fp(const LogupDev& d, const Trace& t, uint6
 __device__ __forceinline__ uint64_t logup_mult(const LogupDev& d, const Trace& t, uint64_t row, uint32_t k) {
     uint64_t m = __ldg(d.mc + k);
     for (uint32_t q = __ldg(d.mo + k), q1 = __ldg(d.mo + k + 1); q < q1; ++q)
-        m = gl::add(m, gl::mul(__ldg(d.mk + q), main_cell(t, row, __ldg(d.ml + q))));
+        m = gl::add(m, logup_scale(__ldg(d.mk + q), main_cell(t, row, __ldg(d.ml + q))));
     return m;
 }
 

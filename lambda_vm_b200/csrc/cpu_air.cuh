@@ -8,8 +8,8 @@
 // and folds them into the composition with the CpuAir emission order's
 // constraint indices, so its sum equals the constraint walk's exactly. The
 // chips the proof carries (bitwise, shift, memory, keccak) decide which
-// constraint blocks exist, as in CpuAir. The LogUp constraints stay with the
-// walk.
+// constraint blocks exist, as in CpuAir. The LogUp constraints come from the
+// table's descriptor (k_logup_constraints).
 #pragma once
 
 #include <stdint.h>

@@ -10,7 +10,8 @@
 // (the KeccakAir emission order; the kernel's own order keeps column reads
 // few), so its sum equals the walk's exactly
 // (field arithmetic is exact: any evaluation of a polynomial gives the same
-// value). The LogUp constraints of the table stay with the walk.
+// value). The table's LogUp constraints come from its descriptor
+// (k_logup_constraints).
 #pragma once
 
 #include <stdint.h>
