@@ -596,6 +596,27 @@ SG_API int sg_rv64_run_counted(const uint32_t* words, uint32_t nwords, uint64_t 
                                uint64_t* rows_out, uint64_t* regs_out, uint64_t* counts_out, uint64_t* shifts_out,
                                uint64_t* cells_out, uint64_t* keccak_out, uint64_t* range_counts,
                                uint64_t* bitwise_counts, sg_rv64_info* info);
+/* sg_rv64_run_counted in one run: the library keeps the outputs, in buffers
+ * that grow as the machine runs (the row records in one anonymous mapping
+ * grown with mremap, so nothing is copied), for an n_rows table of the power
+ * of two >= max(2, cycles) rows. sg_rv64_trace_part gives a part's words in
+ * place (SG_RV64_PART_*: rows 8 per instruction, regs 32 per 64-row chunk,
+ * counts nwords, shifts 3 per shift, cells 3 per touched cell, keccak 52 per
+ * ecall, range_counts 65536, bitwise_counts 3 x 65536), valid until
+ * sg_rv64_trace_free. */
+typedef struct sg_rv64_trace sg_rv64_trace;
+#define SG_RV64_PART_ROWS 0u
+#define SG_RV64_PART_REGS 1u
+#define SG_RV64_PART_COUNTS 2u
+#define SG_RV64_PART_SHIFTS 3u
+#define SG_RV64_PART_CELLS 4u
+#define SG_RV64_PART_KECCAK 5u
+#define SG_RV64_PART_RANGE_COUNTS 6u
+#define SG_RV64_PART_BITWISE_COUNTS 7u
+SG_API int sg_rv64_exec(const uint32_t* words, uint32_t nwords, uint64_t max_steps, sg_rv64_trace** out,
+                        sg_rv64_info* info);
+SG_API int sg_rv64_trace_part(const sg_rv64_trace* trace, uint32_t part, const uint64_t** data, uint64_t* words);
+SG_API void sg_rv64_trace_free(sg_rv64_trace* trace);
 /* The CPU table (n_rows x width u64, row-major, into device memory) written on
  * the device from sg_rv64_run's `count` row records and register snapshots
  * (host arrays): width SG_RV64_CPU_CORE_WIDTH (no chip instruction executed)

@@ -16,6 +16,7 @@
 // STEP = 0. Writing the rows as the machine runs keeps the front-end at
 // memory speed on the host.
 #include <string.h>
+#include <sys/mman.h>
 
 #include <algorithm>
 #include <memory>
@@ -195,26 +196,73 @@ void count_cpu_lookups(const uint64_t* rec, uint64_t T, uint64_t* range_counts, 
     }
 }
 
-}  // namespace
+// Where a run's outputs go. FixedOut: the caller's arrays, sized from an
+// earlier run without outputs (sg_rv64_run / sg_rv64_run_counted). GrowOut:
+// buffers that grow as the machine runs (sg_rv64_exec), so one run suffices;
+// the row records live in an anonymous mapping grown with mremap, which moves
+// page tables rather than copying the records.
+struct FixedOut {
+    uint64_t n_rows;
+    uint64_t *rows, *regs, *counts, *shifts, *cells, *keccak;
+    const char* fit(uint64_t t) const { return rows && t >= n_rows ? "the execution does not fit n_rows" : nullptr; }
+    void snapshot(uint64_t t, const uint64_t* x) {
+        if (regs && t % SG_RV64_REG_CHUNK == 0) memcpy(regs + 32 * (t / SG_RV64_REG_CHUNK), x, 256);
+    }
+    uint64_t* row(uint64_t t) { return rows ? rows + 8 * t : nullptr; }
+    void count(uint64_t i) {
+        if (counts) counts[i] += 1;
+    }
+    void shift(uint64_t k, uint64_t dir, uint64_t a, uint64_t amt) {
+        if (shifts) shifts[3 * k] = dir, shifts[3 * k + 1] = a, shifts[3 * k + 2] = amt;
+    }
+    uint64_t* call(uint64_t k) { return keccak ? keccak + 52 * k : nullptr; }
+    uint64_t* cell(uint64_t i) { return cells ? cells + 3 * i : nullptr; }
+};
 
-using namespace sg;
+struct GrowOut {
+    uint64_t* rows = nullptr;
+    uint64_t cap = 0;  // rows the mapping holds
+    std::vector<uint64_t> regs, counts, shifts, cells, keccak, range, bitwise;
+    ~GrowOut() {
+        if (rows) munmap(rows, cap * 64);
+    }
+    const char* fit(uint64_t t) {
+        if (t < cap) return nullptr;
+        const uint64_t ncap = cap ? 2 * cap : 1ull << 16;
+        void* p = rows ? mremap(rows, cap * 64, ncap * 64, MREMAP_MAYMOVE)
+                       : mmap(nullptr, ncap * 64, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
+        if (p == MAP_FAILED) return "out of host memory for the row records";
+        madvise(p, ncap * 64, MADV_HUGEPAGE);  // fewer first-touch faults; advice only
+        rows = (uint64_t*)p;
+        cap = ncap;
+        return nullptr;
+    }
+    void snapshot(uint64_t t, const uint64_t* x) {
+        if (t % SG_RV64_REG_CHUNK == 0) regs.insert(regs.end(), x, x + 32);
+    }
+    uint64_t* row(uint64_t t) { return rows + 8 * t; }
+    void count(uint64_t i) { counts[i] += 1; }
+    void shift(uint64_t, uint64_t dir, uint64_t a, uint64_t amt) {
+        shifts.push_back(dir), shifts.push_back(a), shifts.push_back(amt);
+    }
+    uint64_t* call(uint64_t k) {
+        keccak.resize(52 * (k + 1));
+        return keccak.data() + 52 * k;
+    }
+    uint64_t* cell(uint64_t i) {
+        if (cells.size() < 3 * (i + 1)) cells.resize(3 * (i + 1));
+        return cells.data() + 3 * i;
+    }
+};
 
-extern "C" int sg_rv64_run(const uint32_t* words, uint32_t nwords, uint64_t max_steps, uint64_t n_rows,
-                           uint64_t* rows_out, uint64_t* regs_out, uint64_t* counts_out, uint64_t* shifts_out,
-                           uint64_t* cells_out, uint64_t* keccak_out, sg_rv64_info* info) {
-    return sg_rv64_run_counted(words, nwords, max_steps, n_rows, rows_out, regs_out, counts_out, shifts_out, cells_out,
-                               keccak_out, nullptr, nullptr, info);
-}
-
-extern "C" int sg_rv64_run_counted(const uint32_t* words, uint32_t nwords, uint64_t max_steps, uint64_t n_rows,
-                                   uint64_t* rows_out, uint64_t* regs_out, uint64_t* counts_out, uint64_t* shifts_out,
-                                   uint64_t* cells_out, uint64_t* keccak_out, uint64_t* range_counts,
-                                   uint64_t* bitwise_counts, sg_rv64_info* info) {
-    SG_CHECK_ARG(words && nwords && info, "null argument");
-    SG_CHECK_ARG(!rows_out || (n_rows >= 2 && (n_rows & (n_rows - 1)) == 0), "n_rows must be a power of two >= 2");
+// The machine, writing into `o`. n_rows: the table height the fill past the
+// halt targets (the FixedOut's; for GrowOut 0: the power of two >= the run).
+template <class O>
+int run_machine(const uint32_t* words, uint32_t nwords, uint64_t max_steps, uint64_t n_rows, bool want_rows, O& o,
+                uint64_t* counts, uint64_t* range_counts, uint64_t* bitwise_counts, sg_rv64_info* info) {
     std::vector<Ins> prog(nwords);
     for (uint32_t i = 0; i < nwords; ++i) SG_CHECK_ARG(decode(words[i], &prog[i]), "unsupported instruction word");
-    if (counts_out) memset(counts_out, 0, nwords * sizeof(uint64_t));
+    if (counts) memset(counts, 0, nwords * sizeof(uint64_t));
     uint64_t x[32] = {0};
     uint64_t pc = 0, t = 0, nshift = 0, ncall = 0;
     uint32_t chips = 0;
@@ -226,15 +274,17 @@ extern "C" int sg_rv64_run_counted(const uint32_t* words, uint32_t nwords, uint6
         ncells += (*c)->stamp == 0;
         return true;
     };
-    SG_CHECK_ARG(!range_counts || rows_out, "lookup counts need the n_rows table");
     if (range_counts) memset(range_counts, 0, 65536 * 8);
     if (bitwise_counts) memset(bitwise_counts, 0, 3 * 65536 * 8);
     bool halted = false;
     while (!halted) {
         SG_CHECK_ARG(t < max_steps, "the program did not halt within max_steps");
         SG_CHECK_ARG(pc % 4 == 0 && pc / 4 < nwords, "pc outside the program");
-        SG_CHECK_ARG(!rows_out || t < n_rows, "the execution does not fit n_rows");
-        if (regs_out && t % SG_RV64_REG_CHUNK == 0) memcpy(regs_out + 32 * (t / SG_RV64_REG_CHUNK), x, 256);
+        if (want_rows) {
+            const char* why = o.fit(t);
+            SG_CHECK_ARG(!why, why);
+        }
+        o.snapshot(t, x);
         const Ins& in = prog[pc / 4];
         const uint64_t a = x[in.rs1], b = x[in.rs2], iu = (uint64_t)in.imm, clk = t + 1;
         uint64_t r = 0, npc = pc + 4, ma = 0, mv = 0, mt = 0;
@@ -278,8 +328,7 @@ extern "C" int sg_rv64_run_counted(const uint32_t* words, uint32_t nwords, uint6
                         SG_CHECK_ARG(cell(ma + 8 * (uint64_t)i, &cs[i]), "keccak state unaligned or outside the data space");
                         lanes[i] = cs[i]->value;
                     }
-                    if (keccak_out) {
-                        uint64_t* k = keccak_out + 52 * ncall;
+                    if (uint64_t* k = o.call(ncall)) {
                         k[0] = clk, k[1] = ma;
                         for (int i = 0; i < 25; ++i) k[2 + i] = lanes[i], k[27 + i] = cs[i]->stamp;
                     }
@@ -296,10 +345,7 @@ extern "C" int sg_rv64_run_counted(const uint32_t* words, uint32_t nwords, uint6
                 break;
         }
         if (op == SLLI || op == SRLI) {
-            if (shifts_out) {
-                uint64_t* sh = shifts_out + 3 * nshift;
-                sh[0] = op == SRLI, sh[1] = a, sh[2] = iu;
-            }
+            o.shift(nshift, op == SRLI, a, iu);
             ++nshift;
             chips |= SG_RV64_CHIP_SHIFT;
         } else if (op >= XOR && op <= ANDI) {
@@ -309,12 +355,12 @@ extern "C" int sg_rv64_run_counted(const uint32_t* words, uint32_t nwords, uint6
         } else if (op == KECCAK_OP) {
             chips |= SG_RV64_CHIP_MEMORY | SG_RV64_CHIP_KECCAK;
         }
-        if (rows_out) {
-            uint64_t* q = rows_out + 8 * t;
+        if (want_rows) {
+            uint64_t* q = o.row(t);
             q[0] = pc | ((uint64_t)op << 32) | ((uint64_t)in.rd << 40) | ((uint64_t)in.rs1 << 48) | ((uint64_t)in.rs2 << 56);
             q[1] = iu, q[2] = a, q[3] = b, q[4] = r, q[5] = ma, q[6] = mv, q[7] = mt;
         }
-        if (counts_out) counts_out[pc / 4] += 1;
+        o.count(pc / 4);
         const bool writes = !(in.op == BEQ || in.op == BNE || in.op == ECALL || in.op == SD);
         if (in.rd && writes) x[in.rd] = r;
         pc = npc;
@@ -326,25 +372,93 @@ extern "C" int sg_rv64_run_counted(const uint32_t* words, uint32_t nwords, uint6
     info->cells = ncells;
     info->keccak_calls = ncall;
     info->chips = chips;
-    if (rows_out) {
+    if (want_rows) {
+        if (!n_rows) n_rows = std::max<uint64_t>(2, 1ull << (64 - __builtin_clzll(t - 1 | 1)));
         // the halting row repeats to fill the table, with the final registers
-        if (counts_out) counts_out[pc / 4] += n_rows - t;
+        if (counts) counts[pc / 4] += n_rows - t;
         if (range_counts) range_counts[0] += 4 * (n_rows - t);  // its zero result
-        if (regs_out)
-            for (uint64_t r = (t + SG_RV64_REG_CHUNK - 1) / SG_RV64_REG_CHUNK * SG_RV64_REG_CHUNK; r < n_rows;
-                 r += SG_RV64_REG_CHUNK)
-                memcpy(regs_out + 32 * (r / SG_RV64_REG_CHUNK), x, 256);
+        for (uint64_t r = (t + SG_RV64_REG_CHUNK - 1) / SG_RV64_REG_CHUNK * SG_RV64_REG_CHUNK; r < n_rows;
+             r += SG_RV64_REG_CHUNK)
+            o.snapshot(r, x);
+        if (range_counts || bitwise_counts) count_cpu_lookups(o.row(0), t, range_counts, bitwise_counts);
     }
-    if (range_counts || bitwise_counts) count_cpu_lookups(rows_out, t, range_counts, bitwise_counts);
-    if (cells_out) {
-        uint64_t i = 0;
-        mem.each_touched([&](uint64_t addr, const Cell& c) {
-            cells_out[3 * i] = addr, cells_out[3 * i + 1] = c.value, cells_out[3 * i + 2] = c.stamp;
-            ++i;
-        });
+    uint64_t i = 0;
+    mem.each_touched([&](uint64_t addr, const Cell& c) {
+        if (uint64_t* q = o.cell(i)) q[0] = addr, q[1] = c.value, q[2] = c.stamp;
+        ++i;
+    });
+    return SG_OK;
+}
+
+}  // namespace
+
+using namespace sg;
+
+// One run's outputs, owned by the library (sg_rv64_exec).
+struct sg_rv64_trace {
+    GrowOut out;
+    sg_rv64_info info;
+};
+
+extern "C" int sg_rv64_run(const uint32_t* words, uint32_t nwords, uint64_t max_steps, uint64_t n_rows,
+                           uint64_t* rows_out, uint64_t* regs_out, uint64_t* counts_out, uint64_t* shifts_out,
+                           uint64_t* cells_out, uint64_t* keccak_out, sg_rv64_info* info) {
+    return sg_rv64_run_counted(words, nwords, max_steps, n_rows, rows_out, regs_out, counts_out, shifts_out, cells_out,
+                               keccak_out, nullptr, nullptr, info);
+}
+
+extern "C" int sg_rv64_run_counted(const uint32_t* words, uint32_t nwords, uint64_t max_steps, uint64_t n_rows,
+                                   uint64_t* rows_out, uint64_t* regs_out, uint64_t* counts_out, uint64_t* shifts_out,
+                                   uint64_t* cells_out, uint64_t* keccak_out, uint64_t* range_counts,
+                                   uint64_t* bitwise_counts, sg_rv64_info* info) {
+    SG_CHECK_ARG(words && nwords && info, "null argument");
+    SG_CHECK_ARG(!rows_out || (n_rows >= 2 && (n_rows & (n_rows - 1)) == 0), "n_rows must be a power of two >= 2");
+    SG_CHECK_ARG(!range_counts || rows_out, "lookup counts need the n_rows table");
+    SG_CHECK_ARG(!bitwise_counts || rows_out, "lookup counts need the n_rows table");
+    FixedOut o{n_rows, rows_out, regs_out, counts_out, shifts_out, cells_out, keccak_out};
+    return run_machine(words, nwords, max_steps, n_rows, rows_out != nullptr, o, counts_out, range_counts,
+                       bitwise_counts, info);
+}
+
+extern "C" int sg_rv64_exec(const uint32_t* words, uint32_t nwords, uint64_t max_steps, sg_rv64_trace** out,
+                            sg_rv64_info* info) {
+    SG_CHECK_ARG(words && nwords && out && info, "null argument");
+    *out = nullptr;
+    sg_rv64_trace* tr = new (std::nothrow) sg_rv64_trace();
+    SG_CHECK_ARG(tr, "out of host memory");
+    GrowOut& o = tr->out;
+    o.counts.assign(nwords, 0);
+    o.range.assign(65536, 0);
+    o.bitwise.assign(3 * 65536, 0);
+    const int rc = run_machine(words, nwords, max_steps, 0, true, o, o.counts.data(), o.range.data(),
+                               o.bitwise.data(), info);
+    if (rc != SG_OK) {
+        delete tr;
+        return rc;
+    }
+    tr->info = *info;
+    *out = tr;
+    return SG_OK;
+}
+
+extern "C" int sg_rv64_trace_part(const sg_rv64_trace* tr, uint32_t part, const uint64_t** data, uint64_t* words) {
+    SG_CHECK_ARG(tr && data && words, "null argument");
+    const GrowOut& o = tr->out;
+    switch (part) {
+        case SG_RV64_PART_ROWS: *data = o.rows, *words = 8 * tr->info.cycles; break;
+        case SG_RV64_PART_REGS: *data = o.regs.data(), *words = o.regs.size(); break;
+        case SG_RV64_PART_COUNTS: *data = o.counts.data(), *words = o.counts.size(); break;
+        case SG_RV64_PART_SHIFTS: *data = o.shifts.data(), *words = o.shifts.size(); break;
+        case SG_RV64_PART_CELLS: *data = o.cells.data(), *words = o.cells.size(); break;
+        case SG_RV64_PART_KECCAK: *data = o.keccak.data(), *words = o.keccak.size(); break;
+        case SG_RV64_PART_RANGE_COUNTS: *data = o.range.data(), *words = o.range.size(); break;
+        case SG_RV64_PART_BITWISE_COUNTS: *data = o.bitwise.data(), *words = o.bitwise.size(); break;
+        default: SG_CHECK_ARG(false, "unknown trace part");
     }
     return SG_OK;
 }
+
+extern "C" void sg_rv64_trace_free(sg_rv64_trace* tr) { delete tr; }
 
 // ---------------------------------------------------------------------------
 // Chip tables expanded on the device from the run's compact events, so the

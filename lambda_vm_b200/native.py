@@ -181,6 +181,9 @@ PROTOTYPES = {
     "sg_rv64_keccak_table": (i32, [vp, vp, vp, u64, u64, vp]),
     "sg_rv64_shift_table": (i32, [vp, vp, vp, u64, u64, vp]),
     "sg_rv64_memory_table": (i32, [vp, vp, vp, u64, u64, vp]),
+    "sg_rv64_exec": (i32, [vp, u32, u64, C.POINTER(vp), C.POINTER(Rv64Info)]),
+    "sg_rv64_trace_part": (i32, [vp, u32, C.POINTER(vp), C.POINTER(u64)]),
+    "sg_rv64_trace_free": (None, [vp]),
     "sg_verify_queries": (i32, [vp, vp, C.POINTER(VerifyTable), u32, vp]),
     "sg_ctx_pass_log_read": (i32, [vp, C.POINTER(PassRecord), u32, C.POINTER(u32)]),
     "sg_mlp_loss_grad": (i32, [vp, vp, vp, vp, u32, vp, vp, vp]),

@@ -1284,8 +1284,65 @@ def tables_from_events(words, ev, host_tables=False):
     return airs, traces, pub
 
 
+class _NativeTrace:
+    """A run's outputs held by the library (sg_rv64_exec), freed with the last
+    array that views them."""
+
+    def __init__(self, L, handle):
+        self.L, self.h = L, handle
+
+    def __del__(self):
+        if self.h:
+            self.L.sg_rv64_trace_free(self.h)
+            self.h = None
+
+    def part(self, part, cols):
+        """The part's words in place, as a (-1, cols) uint64 array that keeps this trace alive."""
+        import ctypes as C
+        from . import native
+        p, n = C.c_void_p(), C.c_uint64()
+        native.check(self.L.sg_rv64_trace_part(self.h, part, C.byref(p), C.byref(n)))
+        if not n.value:
+            return np.zeros((0, cols), np.uint64)
+        return np.asarray(_View(self, p.value, (n.value // cols, cols)))
+
+
+class _View:
+    """Library memory as a numpy array's base: the array keeps `owner` alive."""
+
+    def __init__(self, owner, ptr, shape):
+        self.owner = owner
+        self.__array_interface__ = {"shape": shape, "typestr": "<u8", "data": (ptr, False), "version": 3}
+
+
 def native_events(words, max_steps=1 << 32):
-    """Events of a run of the library's C++ executor (sg_rv64_run)."""
+    """Events of a run of the library's C++ executor, in one run (sg_rv64_exec:
+    the outputs grow as the machine runs and are read in place)."""
+    import ctypes as C
+    from . import native
+    L = native.lib()
+    w = np.ascontiguousarray(np.asarray(words, dtype=np.uint32))
+    info = native.Rv64Info()
+    h = C.c_void_p()
+    native.check(L.sg_rv64_exec(w.ctypes.data, len(w), max_steps, C.byref(h), C.byref(info)))
+    tr = _NativeTrace(L, h)
+    rec = tr.part(0, 8)
+    regs = tr.part(1, 32)
+    counts = tr.part(2, 1).reshape(-1)
+    shifts = tr.part(3, 3)
+    cells = tr.part(4, 3)
+    kc = tr.part(5, 52)
+    rcount = tr.part(6, 1).reshape(-1)
+    bcount = tr.part(7, 1).reshape(-1)
+    chips = tuple(c for i, c in enumerate(CHIPS) if info.chips >> i & 1)
+    return Events(rec, regs, [int(c) for c in counts], info.a0, info.cycles, chips, shifts,
+                  (cells[:, 0].copy(), cells[:, 1].copy(), cells[:, 2].copy()),
+                  (kc[:, 0].copy(), kc[:, 1].copy(), kc[:, 2:27].copy(), kc[:, 27:52].copy()), rcount, bcount)
+
+
+def native_events_two_runs(words, max_steps=1 << 32):
+    """The same events from the caller-buffer entry: a run without outputs to
+    size them, then sg_rv64_run_counted into them."""
     import ctypes as C
     from . import native
     L = native.lib()

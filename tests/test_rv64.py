@@ -128,6 +128,39 @@ def test_native_events_equal_the_python_events(prog):
         assert airs[0].width == (RA.CPU_CORE_WIDTH if prog.startswith("fib") else RA.CPU_WIDTH)
 
 
+@pytest.mark.parametrize("prog", ["fib1", "fib2047", "keccak1", "keccak9"])
+def test_single_run_executor_equals_the_two_run_one(prog):
+    """sg_rv64_exec (one run, outputs growing in library buffers read in
+    place) against sg_rv64_run + sg_rv64_run_counted (a run to size the
+    caller's arrays, then one to fill them): every output, word for word."""
+    words = rv64.fib_program(int(prog[3:])) if prog.startswith("fib") else rv64.keccak_program(136 * int(prog[6:]))
+    a, b = RA.native_events(words), RA.native_events_two_runs(words)
+    assert np.array_equal(a.records, b.records) and np.array_equal(a.regs, b.regs)
+    assert (a.counts, a.output, a.cycles, a.chips) == (b.counts, b.output, b.cycles, b.chips)
+    assert np.array_equal(a.shifts, b.shifts)
+    assert all(np.array_equal(x, y) for x, y in zip(a.cells + a.keccak, b.cells + b.keccak))
+    assert np.array_equal(a.range_counts, b.range_counts) and np.array_equal(a.bitwise_counts, b.bitwise_counts)
+
+
+def test_single_run_executor_errors():
+    """sg_rv64_exec refuses what sg_rv64_run refuses, and an unknown part."""
+    import ctypes as C
+    from lambda_vm_b200 import native
+    L = native.lib()
+    bad = np.array(rv64.assemble([("li", "t0", 4), ("ld", "t1", 0, "t0"), ("li", "a7", 93), ("ecall",)]), np.uint32)
+    info, h = native.Rv64Info(), C.c_void_p()
+    assert L.sg_rv64_exec(bad.ctypes.data, len(bad), 1 << 20, C.byref(h), C.byref(info)) == native.SG_ERR_INVALID
+    assert not h.value
+    loop = np.array(rv64.assemble(["top:", ("beq", "zero", "zero", "top")]), np.uint32)
+    assert L.sg_rv64_exec(loop.ctypes.data, len(loop), 1000, C.byref(h), C.byref(info)) == native.SG_ERR_INVALID
+    ok = np.array(rv64.fib_program(3), np.uint32)
+    assert L.sg_rv64_exec(ok.ctypes.data, len(ok), 1 << 20, C.byref(h), C.byref(info)) == native.SG_OK
+    p, n = C.c_void_p(), C.c_uint64()
+    assert L.sg_rv64_trace_part(h, 8, C.byref(p), C.byref(n)) == native.SG_ERR_INVALID
+    assert L.sg_rv64_trace_part(h, 0, C.byref(p), C.byref(n)) == native.SG_OK and n.value == 8 * info.cycles
+    L.sg_rv64_trace_free(h)
+
+
 def _aux_and_apows(airs, z, alpha):
     apows = [(1, 0, 0)]
     for _ in range(max(a.max_alpha for a in airs) - 1):
