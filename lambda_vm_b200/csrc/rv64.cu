@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <memory>
+#include <mutex>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -155,16 +156,20 @@ class Memory {
 void count_cpu_lookups(const uint64_t* rec, uint64_t T, uint64_t* range_counts, uint64_t* bitwise_counts) {
     const unsigned hw = std::thread::hardware_concurrency();
     const unsigned nt = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>({hw ? hw : 1u, 16u, T / 65536 + 1}));
-    std::vector<std::vector<uint32_t>> rh(nt, std::vector<uint32_t>(range_counts ? 65536 : 0)),
-        bh(nt, std::vector<uint32_t>(bitwise_counts ? 3 * 65536 : 0));
-    auto work = [&](unsigned k) {
-        uint32_t* rr = range_counts ? rh[k].data() : nullptr;
-        uint32_t* bb = bitwise_counts ? bh[k].data() : nullptr;
+    const uint32_t RB = range_counts ? 65536 : 0, BB = bitwise_counts ? 3 * 65536 : 0;
+    // one histogram block per thread (RANGE bins then BITWISE bins), each
+    // zeroed by its own thread; then the blocks are summed bin slice by bin
+    // slice, also one slice per thread
+    std::unique_ptr<uint32_t[]> hist(new uint32_t[(uint64_t)nt * (RB + BB)]);
+    auto count = [&](unsigned k) {
+        uint32_t* rr = hist.get() + (uint64_t)k * (RB + BB);
+        uint32_t* bb = rr + RB;
+        memset(rr, 0, 4ull * (RB + BB));
         for (uint64_t row = T * k / nt; row < T * (k + 1) / nt; ++row) {
             const uint64_t* q = rec + 8 * row;
             const uint32_t op = (uint32_t)(q[0] >> 32) & 0xFF;
             const uint64_t iu = q[1], a = q[2], b = q[3], r = q[4], ma = q[5], mt = q[7];
-            if (rr) {
+            if (RB) {
                 for (int j = 0; j < 4; ++j) rr[(r >> (16 * j)) & 0xFFFF] += 1;
                 if (op == LD || op == SD || op == KECCAK_OP) {
                     rr[(ma >> 3) & 0xFFFF] += 1;
@@ -176,7 +181,7 @@ void count_cpu_lookups(const uint64_t* rec, uint64_t T, uint64_t* range_counts, 
                     rr[gap >> 16] += 1;
                 }
             }
-            if (bb && op >= XOR && op <= ANDI) {
+            if (BB && op >= XOR && op <= ANDI) {
                 const uint64_t second = op <= AND ? b : iu;
                 const uint32_t kind = (op == XOR || op == XORI) ? 0 : (op == OR || op == ORI) ? 1 : 2;
                 for (int i = 0; i < 8; ++i)
@@ -184,15 +189,22 @@ void count_cpu_lookups(const uint64_t* rec, uint64_t T, uint64_t* range_counts, 
             }
         }
     };
-    std::vector<std::thread> pool;
-    for (unsigned k = 1; k < nt; ++k) pool.emplace_back(work, k);
-    work(0);
-    for (auto& th : pool) th.join();
-    for (unsigned k = 0; k < nt; ++k) {
-        if (range_counts)
-            for (uint32_t v = 0; v < 65536; ++v) range_counts[v] += rh[k][v];
-        if (bitwise_counts)
-            for (uint32_t v = 0; v < 3 * 65536; ++v) bitwise_counts[v] += bh[k][v];
+    auto merge = [&](unsigned k) {
+        const uint32_t nb = RB + BB, v0 = (uint32_t)((uint64_t)nb * k / nt), v1 = (uint32_t)((uint64_t)nb * (k + 1) / nt);
+        for (uint32_t v = v0; v < v1; ++v) {
+            uint64_t sum = 0;
+            for (unsigned j = 0; j < nt; ++j) sum += hist[(uint64_t)j * nb + v];
+            if (v < RB)
+                range_counts[v] += sum;
+            else
+                bitwise_counts[v - RB] += sum;
+        }
+    };
+    for (auto phase : {0, 1}) {
+        std::vector<std::thread> pool;
+        for (unsigned k = 1; k < nt; ++k) pool.emplace_back([&, k, phase] { phase ? merge(k) : count(k); });
+        phase ? merge(0) : count(0);
+        for (auto& th : pool) th.join();
     }
 }
 
@@ -219,15 +231,42 @@ struct FixedOut {
     uint64_t* cell(uint64_t i) { return cells ? cells + 3 * i : nullptr; }
 };
 
+// One freed record mapping is kept for the next run (up to kKeepBytes): its
+// pages stay mapped, so a later run of a similar size writes its records
+// without first-touch faults (on the 1 MiB Keccak guest the faults cost more
+// than writing the records).
+constexpr uint64_t kKeepBytes = 8ull << 30;
+std::mutex g_keep_mu;
+void* g_keep = nullptr;
+uint64_t g_keep_rows = 0;
+
 struct GrowOut {
     uint64_t* rows = nullptr;
     uint64_t cap = 0;  // rows the mapping holds
     std::vector<uint64_t> regs, counts, shifts, cells, keccak, range, bitwise;
     ~GrowOut() {
-        if (rows) munmap(rows, cap * 64);
+        if (!rows) return;
+        void* drop = rows;
+        uint64_t drop_rows = cap;
+        if (cap * 64 <= kKeepBytes) {
+            std::lock_guard<std::mutex> g(g_keep_mu);
+            if (cap > g_keep_rows) {  // keep the larger of the two
+                std::swap(drop, g_keep);
+                std::swap(drop_rows, g_keep_rows);
+            }
+        }
+        if (drop) munmap(drop, drop_rows * 64);
     }
     const char* fit(uint64_t t) {
         if (t < cap) return nullptr;
+        if (!rows) {
+            std::lock_guard<std::mutex> g(g_keep_mu);
+            if (g_keep) {
+                rows = (uint64_t*)g_keep, cap = g_keep_rows;
+                g_keep = nullptr, g_keep_rows = 0;
+                if (t < cap) return nullptr;
+            }
+        }
         const uint64_t ncap = cap ? 2 * cap : 1ull << 16;
         void* p = rows ? mremap(rows, cap * 64, ncap * 64, MREMAP_MAYMOVE)
                        : mmap(nullptr, ncap * 64, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
