@@ -17,6 +17,9 @@
 // memory speed on the host.
 #include <string.h>
 #include <sys/mman.h>
+#if defined(__x86_64__)
+#include <immintrin.h>
+#endif
 
 #include <algorithm>
 #include <memory>
@@ -208,6 +211,29 @@ void count_cpu_lookups(const uint64_t* rec, uint64_t T, uint64_t* range_counts, 
     }
 }
 
+// A row record is written once and read back only by other threads and the
+// device upload, long after: on x86-64 it goes out with non-temporal stores,
+// which skip reading the line into the cache first (the records are larger
+// than the last-level cache). records_done orders those stores before any
+// later read.
+inline void put_record(uint64_t* q, uint64_t w0, uint64_t w1, uint64_t w2, uint64_t w3, uint64_t w4, uint64_t w5,
+                       uint64_t w6, uint64_t w7) {
+#if defined(__x86_64__)
+    long long* p = (long long*)q;
+    _mm_stream_si64(p, (long long)w0), _mm_stream_si64(p + 1, (long long)w1);
+    _mm_stream_si64(p + 2, (long long)w2), _mm_stream_si64(p + 3, (long long)w3);
+    _mm_stream_si64(p + 4, (long long)w4), _mm_stream_si64(p + 5, (long long)w5);
+    _mm_stream_si64(p + 6, (long long)w6), _mm_stream_si64(p + 7, (long long)w7);
+#else
+    q[0] = w0, q[1] = w1, q[2] = w2, q[3] = w3, q[4] = w4, q[5] = w5, q[6] = w6, q[7] = w7;
+#endif
+}
+inline void records_done() {
+#if defined(__x86_64__)
+    _mm_sfence();
+#endif
+}
+
 // Where a run's outputs go. FixedOut: the caller's arrays, sized from an
 // earlier run without outputs (sg_rv64_run / sg_rv64_run_counted). GrowOut:
 // buffers that grow as the machine runs (sg_rv64_exec), so one run suffices;
@@ -394,17 +420,18 @@ int run_machine(const uint32_t* words, uint32_t nwords, uint64_t max_steps, uint
         } else if (op == KECCAK_OP) {
             chips |= SG_RV64_CHIP_MEMORY | SG_RV64_CHIP_KECCAK;
         }
-        if (want_rows) {
-            uint64_t* q = o.row(t);
-            q[0] = pc | ((uint64_t)op << 32) | ((uint64_t)in.rd << 40) | ((uint64_t)in.rs1 << 48) | ((uint64_t)in.rs2 << 56);
-            q[1] = iu, q[2] = a, q[3] = b, q[4] = r, q[5] = ma, q[6] = mv, q[7] = mt;
-        }
+        if (want_rows)
+            put_record(o.row(t),
+                       pc | ((uint64_t)op << 32) | ((uint64_t)in.rd << 40) | ((uint64_t)in.rs1 << 48) |
+                           ((uint64_t)in.rs2 << 56),
+                       iu, a, b, r, ma, mv, mt);
         o.count(pc / 4);
         const bool writes = !(in.op == BEQ || in.op == BNE || in.op == ECALL || in.op == SD);
         if (in.rd && writes) x[in.rd] = r;
         pc = npc;
         ++t;
     }
+    records_done();
     info->cycles = t;
     info->a0 = x[10];
     info->shifts = nshift;
