@@ -257,42 +257,45 @@ struct FixedOut {
     uint64_t* cell(uint64_t i) { return cells ? cells + 3 * i : nullptr; }
 };
 
-// One freed record mapping is kept for the next run (up to kKeepBytes): its
-// pages stay mapped, so a later run of a similar size writes its records
-// without first-touch faults (on the 1 MiB Keccak guest the faults cost more
-// than writing the records).
+// A freed run's buffers are kept for the next run (one set, its record
+// mapping up to kKeepBytes): their pages stay mapped, so a later run of a
+// similar size writes without first-touch faults or vector growth (on the
+// 1 MiB Keccak guest the faults cost more than writing the records).
 constexpr uint64_t kKeepBytes = 8ull << 30;
-std::mutex g_keep_mu;
-void* g_keep = nullptr;
-uint64_t g_keep_rows = 0;
 
 struct GrowOut {
     uint64_t* rows = nullptr;
     uint64_t cap = 0;  // rows the mapping holds
     std::vector<uint64_t> regs, counts, shifts, cells, keccak, range, bitwise;
+
+    static std::mutex& keep_mu() {
+        static std::mutex m;
+        return m;
+    }
+    static GrowOut& kept() {  // the kept buffers (never destroyed: they only ever move)
+        static GrowOut* k = new GrowOut(false);
+        return *k;
+    }
+    explicit GrowOut(bool take = true) {
+        if (!take) return;
+        std::lock_guard<std::mutex> g(keep_mu());
+        swap_buffers(kept());
+        for (auto* v : {&regs, &counts, &shifts, &cells, &keccak, &range, &bitwise}) v->clear();
+    }
     ~GrowOut() {
-        if (!rows) return;
-        void* drop = rows;
-        uint64_t drop_rows = cap;
-        if (cap * 64 <= kKeepBytes) {
-            std::lock_guard<std::mutex> g(g_keep_mu);
-            if (cap > g_keep_rows) {  // keep the larger of the two
-                std::swap(drop, g_keep);
-                std::swap(drop_rows, g_keep_rows);
-            }
+        if (rows && cap * 64 <= kKeepBytes) {
+            std::lock_guard<std::mutex> g(keep_mu());
+            if (cap >= kept().cap) swap_buffers(kept());  // keep the larger set; free the other below
         }
-        if (drop) munmap(drop, drop_rows * 64);
+        if (rows) munmap(rows, cap * 64);
+    }
+    void swap_buffers(GrowOut& o) {
+        std::swap(rows, o.rows), std::swap(cap, o.cap);
+        regs.swap(o.regs), counts.swap(o.counts), shifts.swap(o.shifts), cells.swap(o.cells);
+        keccak.swap(o.keccak), range.swap(o.range), bitwise.swap(o.bitwise);
     }
     const char* fit(uint64_t t) {
         if (t < cap) return nullptr;
-        if (!rows) {
-            std::lock_guard<std::mutex> g(g_keep_mu);
-            if (g_keep) {
-                rows = (uint64_t*)g_keep, cap = g_keep_rows;
-                g_keep = nullptr, g_keep_rows = 0;
-                if (t < cap) return nullptr;
-            }
-        }
         const uint64_t ncap = cap ? 2 * cap : 1ull << 16;
         void* p = rows ? mremap(rows, cap * 64, ncap * 64, MREMAP_MAYMOVE)
                        : mmap(nullptr, ncap * 64, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
