@@ -441,29 +441,42 @@ static int stage_reserve(Ctx* ctx, uint64_t half_bytes) {
     return SG_OK;
 }
 
-int sg::upload_host(Ctx* ctx, cudaStream_t st, const void* host, uint64_t bytes, void* dst) {
+int sg::upload_host(Ctx* ctx, cudaStream_t st, const void* host, uint64_t bytes, void* dst,
+                    const std::function<bool(uint64_t lo, uint64_t hi)>& check) {
     if (!bytes) return SG_OK;
+    std::atomic<bool> bad{false};
     cudaPointerAttributes pa;
     const bool pageable = cudaPointerGetAttributes(&pa, host) != cudaSuccess || pa.type == cudaMemoryTypeUnregistered;
     cudaGetLastError();
     constexpr uint64_t kDirect = 4ull << 20, kPiece = 32ull << 20;
     if (!pageable || bytes <= kDirect) {
+        if (check) host_parallel(bytes, 1ull << 20, [&](uint64_t lo, uint64_t hi) {
+            if (!check(lo, hi)) bad = true;
+        });
+        SG_CHECK_ARG(!bad.load(), "bad input records");
         SG_CUDA(cudaMemcpyAsync(dst, host, bytes, cudaMemcpyHostToDevice, st));
         return SG_OK;
     }
     std::lock_guard<std::mutex> lock(ctx->stage_mu);
     SG_TRY(stage_reserve(ctx, std::min(bytes, kPiece)));
     const uint64_t piece = std::min(ctx->stage_bytes, kPiece);
-    for (uint64_t off = 0, k = 0; off < bytes; off += piece, ++k) {
-        const uint64_t len = std::min(piece, bytes - off);
+    // the first pieces are small, so the device starts copying soon (the
+    // host fills a piece before its copy can start); then they double
+    uint64_t len = std::min<uint64_t>(piece, kDirect);
+    for (uint64_t off = 0, k = 0; off < bytes; off += len, len = std::min(2 * len, piece), ++k) {
+        len = std::min(len, bytes - off);
         uint8_t* half = (uint8_t*)ctx->stage + (k & 1) * ctx->stage_bytes;
         const uint8_t* src = (const uint8_t*)host + off;
         // the half is free once its previous copy (this call's or an earlier one's) has left it
         SG_CUDA(cudaEventSynchronize(ctx->stage_free[k & 1]));
-        host_parallel(len, 1ull << 20, [&](uint64_t lo, uint64_t hi) { memcpy(half + lo, src + lo, hi - lo); });
+        host_parallel(len, 1ull << 20, [&](uint64_t lo, uint64_t hi) {
+            memcpy(half + lo, src + lo, hi - lo);
+            if (check && !check(off + lo, off + hi)) bad = true;
+        });
         SG_CUDA(cudaMemcpyAsync((uint8_t*)dst + off, half, len, cudaMemcpyHostToDevice, st));
         SG_CUDA(cudaEventRecord(ctx->stage_free[k & 1], st));
     }
+    SG_CHECK_ARG(!bad.load(), "bad input records");
     return SG_OK;
 }
 

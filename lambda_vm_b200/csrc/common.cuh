@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <functional>
 #include <map>
 #include <mutex>
 #include <string>
@@ -130,7 +131,12 @@ int dev_free(Ctx* ctx, cudaStream_t st, void* p, uint64_t bytes);
 // context's page-locked staging, host threads copying one chunk into a
 // staging half while the previous chunk's DMA is in flight (the driver's own
 // staging of a pageable copy runs at a few GB/s).
-int upload_host(Ctx* ctx, cudaStream_t st, const void* host, uint64_t bytes, void* dst);
+// `check`, when given, is called on every byte range [lo, hi) of the upload
+// by the host thread that copies it (while the bytes are in its cache); a
+// false return makes the call fail with SG_ERR_INVALID once the copies are
+// enqueued (the caller frees `dst` in stream order).
+int upload_host(Ctx* ctx, cudaStream_t st, const void* host, uint64_t bytes, void* dst,
+                const std::function<bool(uint64_t lo, uint64_t hi)>& check = nullptr);
 
 // f(lo, hi) over contiguous slices of [0, n), at least `grain` items a slice,
 // on up to 16 host threads; the calling thread takes the first slice.

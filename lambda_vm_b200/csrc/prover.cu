@@ -260,6 +260,30 @@ extern "C" int sg_prove_table(sg_ctx* c, void* stream, sg_transcript* t, const s
     SG_CUDA(cudaStreamSynchronize(st));
     bf.release(d_invd);
     bf.release(d_S);
+    // round 4's denominators depend on z only: they are inverted while the
+    // host absorbs the OOD values and samples gamma below. A point lies in
+    // the LDE coset g * <w_N> iff it is a base-field element c with
+    // (c / g)^N = 1, checked here instead of by the inversion's flag (whose
+    // read would wait for it).
+    auto in_lde_coset = [&](const E3& p) {
+        return p.v[1] % P == 0 && p.v[2] % P == 0 && sg_host_gl_pow(sg_host_gl_mul(p.v[0], sg_host_gl_inv(g)), N) == 1;
+    };
+    if (in_lde_coset(z2)) {
+        set_error("prove_table: z^2 lies in the LDE coset");
+        return SG_ERR_INVALID;
+    }
+    if (in_lde_coset(z) || in_lde_coset(zw)) {
+        set_error("prove_table: z_ood lies in the LDE coset");
+        return SG_ERR_INVALID;
+    }
+    uint64_t* d_inv_h = (uint64_t*)bf.alloc(N * 3 * 8, &rc);
+    uint64_t* d_inv_t = (uint64_t*)bf.alloc(2 * N * 3 * 8, &rc);
+    if (rc) return rc;
+    SG_TRY(sg_inv_denoms_ext3(c, st, j->d_pts_N, N, z2.v, 1, 1, d_inv_h, nullptr));
+    uint64_t zzw[6];
+    memcpy(zzw, z.v, 24);
+    memcpy(zzw + 3, zw.v, 24);
+    SG_TRY(sg_inv_denoms_ext3(c, st, j->d_pts_N, N, zzw, 2, 1, d_inv_t, nullptr));
     const E3 sc[3] = {ood_scale(z, n, g), ood_scale(zw, n, g), ood_scale(z2, n, g)};
     const uint64_t W = m + A;
     for (int k = 0; k < 2; ++k) {
@@ -289,22 +313,6 @@ extern "C" int sg_prove_table(sg_ctx* c, void* stream, sg_transcript* t, const s
     }
     for (uint64_t col = 0; col < W; ++col)
         for (int k = 0; k < 2; ++k) memcpy(&tood[3 * (2 * col + k)], o->trace_ood + 3 * (k * W + col), 24);
-    uint64_t* d_inv_h = (uint64_t*)bf.alloc(N * 3 * 8, &rc);
-    uint64_t* d_inv_t = (uint64_t*)bf.alloc(2 * N * 3 * 8, &rc);
-    if (rc) return rc;
-    SG_TRY(sg_inv_denoms_ext3(c, st, j->d_pts_N, N, z2.v, 1, 1, d_inv_h, &zero));
-    if (zero) {
-        set_error("prove_table: z^2 lies in the LDE coset");
-        return SG_ERR_INVALID;
-    }
-    uint64_t zzw[6];
-    memcpy(zzw, z.v, 24);
-    memcpy(zzw + 3, zw.v, 24);
-    SG_TRY(sg_inv_denoms_ext3(c, st, j->d_pts_N, N, zzw, 2, 1, d_inv_t, &zero));
-    if (zero) {
-        set_error("prove_table: z_ood lies in the LDE coset");
-        return SG_ERR_INVALID;
-    }
     uint64_t* d_deep = (uint64_t*)bf.alloc(N * 3 * 8, &rc);
     if (rc) return rc;
     SG_TRY(sg_deep_composition(c, st, j->d_main_lde, m, d_aux_lde, A, d_parts, 2, N, o->parts_ood, tood.data(),

@@ -766,9 +766,10 @@ __global__ void k_memory_rows(const uint64_t* __restrict__ cells, uint64_t count
     }
 }
 
-int upload_events(Ctx* ctx, cudaStream_t st, const uint64_t* host, uint64_t words, uint64_t** d) {
+int upload_events(Ctx* ctx, cudaStream_t st, const uint64_t* host, uint64_t words, uint64_t** d,
+                  const std::function<bool(uint64_t lo, uint64_t hi)>& check = nullptr) {
     SG_TRY(dev_alloc(ctx, st, 8 * words, (void**)d));
-    const int rc = upload_host(ctx, st, host, 8 * words, *d);
+    const int rc = upload_host(ctx, st, host, 8 * words, *d, check);
     if (rc != SG_OK) {
         dev_free(ctx, st, *d, 8 * words);
         set_error(std::string("rv64: event upload failed: ") + last_error());
@@ -787,10 +788,13 @@ extern "C" int sg_rv64_cpu_table(sg_ctx* c, void* stream, const uint64_t* rows, 
     SG_CHECK_ARG(count >= 1 && count <= n_rows, "the execution does not fit n_rows");
     SG_CHECK_ARG(width == SG_RV64_CPU_CORE_WIDTH || width == SG_RV64_CPU_WIDTH, "width is the core or the full width");
     // 0: good; 1: a bad record; 2: a chip instruction in a core-width table
+    // the records are checked by the threads that stage them for the upload
+    // (each record whose first byte falls in the range it copies): 1 a bad
+    // record, 2 a chip instruction in a core-width table
     std::atomic<int> bad{0};
-    host_parallel(count, 1 << 16, [&](uint64_t lo, uint64_t hi) {
+    auto check = [&](uint64_t lo, uint64_t hi) {
         int b = 0;
-        for (uint64_t i = lo; i < hi && !b; ++i) {
+        for (uint64_t i = (lo + 63) / 64; i < (hi + 63) / 64 && !b; ++i) {
             const uint64_t w0 = rows[8 * i];
             const uint32_t op = (uint32_t)(w0 >> 32) & 0xFF;
             if (!(op >= 1 && op <= KECCAK_OP && ((w0 >> 40) & 0xFF) < 32 && ((w0 >> 48) & 0xFF) < 32 &&
@@ -803,13 +807,17 @@ extern "C" int sg_rv64_cpu_table(sg_ctx* c, void* stream, const uint64_t* rows, 
             int z = 0;
             bad.compare_exchange_strong(z, b);
         }
-    });
-    SG_CHECK_ARG(bad.load() != 1, "bad row record");
-    SG_CHECK_ARG(bad.load() != 2, "a chip instruction in a table without the chips' columns");
+        return b == 0;
+    };
     cudaStream_t st = (cudaStream_t)stream;
     const uint64_t nchunks = (n_rows + SG_RV64_REG_CHUNK - 1) / SG_RV64_REG_CHUNK;
     uint64_t *d_rows = nullptr, *d_regs = nullptr;
-    SG_TRY(upload_events(ctx, st, rows, 8 * count, &d_rows));
+    int rc0 = upload_events(ctx, st, rows, 8 * count, &d_rows, check);
+    if (rc0 != SG_OK) {
+        SG_CHECK_ARG(bad.load() != 1, "bad row record");
+        SG_CHECK_ARG(bad.load() != 2, "a chip instruction in a table without the chips' columns");
+        return rc0;
+    }
     int rc = upload_events(ctx, st, regs, 32 * nchunks, &d_regs);
     if (rc == SG_OK) {
         const uint64_t warps = nchunks < 148ull * 64 ? nchunks : 148ull * 64;
@@ -850,10 +858,20 @@ extern "C" int sg_rv64_shift_table(sg_ctx* c, void* stream, const uint64_t* shif
     SG_CHECK_ARG(ctx && d_out && (shifts || !count), "null argument");
     SG_ENTER(ctx);
     SG_CHECK_ARG(count <= n_rows, "the shifts do not fit n_rows");
-    for (uint64_t i = 0; i < count; ++i) SG_CHECK_ARG(shifts[3 * i] <= 1 && shifts[3 * i + 2] < 64, "bad shift event");
     cudaStream_t st = (cudaStream_t)stream;
     uint64_t* d_ev = nullptr;
-    if (count) SG_TRY(upload_events(ctx, st, shifts, 3 * count, &d_ev));
+    // the events are checked by the threads that stage them (each whose first byte falls in the range)
+    std::atomic<bool> bad{false};
+    auto check = [&](uint64_t lo, uint64_t hi) {
+        for (uint64_t i = (lo + 23) / 24; i < (hi + 23) / 24; ++i)
+            if (shifts[3 * i] > 1 || shifts[3 * i + 2] >= 64) return !(bad = true);
+        return true;
+    };
+    if (count) {
+        const int rc0 = upload_events(ctx, st, shifts, 3 * count, &d_ev, check);
+        SG_CHECK_ARG(!bad.load(), "bad shift event");
+        SG_TRY(rc0);
+    }
     const uint64_t total = n_rows * SW;
     const unsigned grid = (unsigned)std::min<uint64_t>((total + 255) / 256, 148ull * 32);
     k_shift_rows<<<grid, 256, 0, st>>>(d_ev, count, n_rows, d_out);

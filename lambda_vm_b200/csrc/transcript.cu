@@ -23,14 +23,28 @@ extern "C" {
 
 uint64_t sg_host_gl_canon(uint64_t a) { return a >= P ? a - P : a; }
 uint64_t sg_host_gl_add(uint64_t a, uint64_t b) {
-    u128 s = (u128)sg_host_gl_canon(a) + sg_host_gl_canon(b);
-    return (uint64_t)(s % P);
+    const uint64_t x = sg_host_gl_canon(a), y = sg_host_gl_canon(b);
+    uint64_t s = x + y;
+    if (s < x) s += 0xFFFFFFFFull;  // the carry 2^64 = 2^32 - 1 (mod p); no second carry (x + y < 2p)
+    return sg_host_gl_canon(s);
 }
 uint64_t sg_host_gl_sub(uint64_t a, uint64_t b) {
     uint64_t x = sg_host_gl_canon(a), y = sg_host_gl_canon(b);
     return x >= y ? x - y : x + (P - y);
 }
-uint64_t sg_host_gl_mul(uint64_t a, uint64_t b) { return (uint64_t)(((u128)a * b) % P); }
+// A 128-bit product reduced with 2^64 = 2^32 - 1 and 2^96 = -1 (mod p):
+// lo + hl 2^64 + hh 2^96 = lo - hh + hl (2^32 - 1), each step folding its
+// borrow or carry back in once (the sums leave no second one).
+uint64_t sg_host_gl_mul(uint64_t a, uint64_t b) {
+    const u128 x = (u128)a * b;
+    const uint64_t lo = (uint64_t)x, hi = (uint64_t)(x >> 64), hh = hi >> 32, hl = hi & 0xFFFFFFFFull;
+    uint64_t t = lo - hh;
+    if (lo < hh) t -= 0xFFFFFFFFull;
+    const uint64_t u = hl * 0xFFFFFFFFull;
+    uint64_t r = t + u;
+    if (r < u) r += 0xFFFFFFFFull;
+    return sg_host_gl_canon(r);
+}
 uint64_t sg_host_gl_pow(uint64_t a, uint64_t e) {
     uint64_t r = 1, b = sg_host_gl_canon(a);
     while (e) {

@@ -294,3 +294,55 @@ def test_logup_descriptor_is_validated(be):
     bad(lambda d, g: g.__setitem__("num_committed", 0))
     bad(lambda d, g: d.__setitem__("logup_root", 0))
     bad(lambda d, g: d.__setitem__("logup_root", d["num_roots"] - 1))
+
+
+def test_cpu_table_rejects_bad_records(be):
+    """sg_rv64_cpu_table refuses a record with an unknown opcode or a
+    register index past 31, and a chip instruction in a core-width table,
+    whether the records go up directly (small) or through the staged upload
+    that checks them as it copies (large, the bad record in a late piece)."""
+    import numpy as np
+    from lambda_vm_b200 import native
+    bk = GpuBackend(be)
+    for count, log_n in ((1000, 10), (150000, 18)):
+        n = 1 << log_n
+        rec = np.zeros((count, 8), np.uint64)
+        rec[:, 0] = (np.arange(count, dtype=np.uint64) * np.uint64(4)) | (np.uint64(1) << np.uint64(32))  # add x0,x0,x0
+        regs = np.zeros(((n + 63) // 64, 32), np.uint64)
+        m = bk._alloc(n, RA.CPU_WIDTH)
+        call = lambda r, width: bk.L.sg_rv64_cpu_table(bk.be.h, bk.st, r.ctypes.data, count, regs.ctypes.data, n,
+                                                       width, m.ptr)
+        assert call(rec, RA.CPU_WIDTH) == native.SG_OK
+        for word in ((np.uint64(0) << np.uint64(32)),                       # op 0
+                     (np.uint64(1) << np.uint64(32)) | (np.uint64(40) << np.uint64(40))):  # rd 40
+            bad = rec.copy()
+            bad[count - 3, 0] = word
+            assert call(bad, RA.CPU_WIDTH) == native.SG_ERR_INVALID
+        chip = rec.copy()
+        chip[count - 2, 0] = np.uint64(RA.OP_ID["xor"]) << np.uint64(32)
+        assert call(chip, RA.CPU_CORE_WIDTH) == native.SG_ERR_INVALID
+        assert call(chip, RA.CPU_WIDTH) == native.SG_OK
+        bk.to_host(m)  # waits for the accepted calls' kernels
+        bk.free(m)
+
+
+def test_shift_table_rejects_bad_events(be):
+    """sg_rv64_shift_table refuses a direction past 1 or an amount past 63,
+    on the direct and on the staged upload."""
+    import numpy as np
+    from lambda_vm_b200 import native
+    bk = GpuBackend(be)
+    for count, log_n in ((500, 9), (200000, 18)):
+        n = 1 << log_n
+        ev = np.zeros((count, 3), np.uint64)
+        ev[:, 1] = np.arange(count, dtype=np.uint64)
+        ev[:, 2] = np.arange(count, dtype=np.uint64) % np.uint64(64)
+        m = bk._alloc(n, RA.ShiftAir(log_n).width)
+        call = lambda e: bk.L.sg_rv64_shift_table(bk.be.h, bk.st, e.ctypes.data, count, n, m.ptr)
+        assert call(ev) == native.SG_OK
+        for col, v in ((0, 2), (2, 64)):
+            bad = ev.copy()
+            bad[count - 5, col] = v
+            assert call(bad) == native.SG_ERR_INVALID
+        bk.to_host(m)
+        bk.free(m)
