@@ -672,6 +672,8 @@ def run_constraints(a):
 
 
 def main():
+    import faulthandler
+    faulthandler.enable()  # a fatal signal prints every thread's Python stack
     a = parse()
     if a.workload == "proof" and a.impl == "ours":
         if int(os.environ.get("WORLD_SIZE", "1")) > 1:

@@ -653,7 +653,9 @@ int sg_eval_constraints(sg_ctx* c, void* stream, const sg_device_program* prog, 
         return off;
     };
     const size_t o_nodes = put(prog->nodes, 16ull * nn);
-    const size_t o_roots = put(prog->roots, 4ull * nr);
+    // `roots` is read only by the reference shape; a streaming program's
+    // caller may pass fewer entries (or none), so nothing is copied from it
+    const size_t o_roots = prog->node_roots ? put(nullptr, 0) : put(prog->roots, 4ull * nr);
     const size_t o_nroots = prog->node_roots ? put(prog->node_roots, 4ull * nn) : 0;
     const size_t o_bc = put(prog->base_consts, 8ull * prog->num_base_consts);
     const size_t o_ec = put(prog->ext_consts, 24ull * prog->num_ext_consts);

@@ -346,3 +346,36 @@ def test_shift_table_rejects_bad_events(be):
             assert call(bad) == native.SG_ERR_INVALID
         bk.to_host(m)
         bk.free(m)
+
+
+def test_streaming_program_roots_are_not_read(be):
+    """A streaming program's `roots` array is unused (node_roots names the
+    constraints): sg_eval_constraints accepts it as NULL and gives the same
+    composition as with it set (it once copied num_roots entries from it)."""
+    import ctypes as C
+    import numpy as np
+    from lambda_vm_b200 import math_cuda as mc, native
+    from lambda_vm_b200.ir import lower
+    air = RA.KeccakAir(6)
+    dev = lower(air.device_program)
+    rows = 256
+    rng = np.random.default_rng(9)
+    P_ = 0xFFFFFFFF00000001
+    rf = lambda shape: np.where((x := rng.integers(0, 2**64, size=shape, dtype=np.uint64)) >= np.uint64(P_),
+                                x - np.uint64(P_), x)
+    main, aux = rf((rows, air.width)), rf((rows, 3 * air.aux_width))
+    rap, alpha, off = rf((2, 3)), rf((air.max_alpha, 3)), rf((3,))
+    comp = {"beta": rf((dev["num_roots"], 3)), "z_inv": rf((rows // 4,)),
+            "boundary": [(air.acc_col, True, rf((3,)), rf((3,)))], "b_z_inv": rf((1, rows))}
+    want = mc.eval_constraints_on_device(dev, main, aux, rap, alpha, off, 2, comp, be)
+    real = mc._program_struct
+    try:
+        def no_roots(low, keep):
+            p = real(low, keep)
+            p.roots = None
+            return p
+        mc._program_struct = no_roots
+        got = mc.eval_constraints_on_device(dev, main, aux, rap, alpha, off, 2, comp, be)
+    finally:
+        mc._program_struct = real
+    assert np.array_equal(want, got)
