@@ -300,7 +300,12 @@ __global__ void k_bary_combine(const uint64_t* partial, uint64_t chunks, uint64_
 // 16-byte load where it is 16-byte aligned: a warp's load touches 32 rows'
 // sectors either way, so pairs halve the L1 lookups, which bound this kernel.
 #define DEEP_MAX_K 8
-template <int K>
+// POW: the trace coefficients are gam_tr[j K + k] = rho_k gam_tr[j K] (the
+// prover's successive powers of one gamma give rho_k = gamma^k), so each
+// row's K column sums are rho_k times the first: one sum is accumulated
+// (half the products at K = 2) and the others are one product each. rho
+// (K ext3, rho_0 = 1) follows the constants in `consts`.
+template <int K, bool POW>
 __global__ void __launch_bounds__(128) k_deep(const uint64_t* __restrict__ main, uint64_t m,
                                               const uint64_t* __restrict__ aux, uint64_t A,
                                               const uint64_t* __restrict__ parts, uint64_t P, uint64_t rows,
@@ -308,6 +313,7 @@ __global__ void __launch_bounds__(128) k_deep(const uint64_t* __restrict__ main,
                                               const uint64_t* __restrict__ gam_tr, const uint64_t* __restrict__ consts,
                                               const uint64_t* __restrict__ inv_h, const uint64_t* __restrict__ inv_t,
                                               int bitrev_out, uint64_t* __restrict__ out) {
+    constexpr int KS = POW ? 1 : K;  // column sums accumulated
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= rows) return;
     // Column sums are accumulated unreduced (160-bit) and reduced once per row.
@@ -318,7 +324,7 @@ __global__ void __launch_bounds__(128) k_deep(const uint64_t* __restrict__ main,
     auto col = [&](uint64_t j, uint64_t t) {
         const uint64_t* g = gam_tr + 3 * j * K;
 #pragma unroll
-        for (int k = 0; k < K; ++k)
+        for (int k = 0; k < (K < KS ? K : KS); ++k)
             gl::wmacb3(acc[k], fe3{__ldg(g + 3 * k), __ldg(g + 3 * k + 1), __ldg(g + 3 * k + 2)}, t);
     };
     uint64_t j = 0;
@@ -335,7 +341,7 @@ __global__ void __launch_bounds__(128) k_deep(const uint64_t* __restrict__ main,
         const uint64_t t1_2 = gl::add(t.c1, t.c1), t2_2 = gl::add(t.c2, t.c2);
         const uint64_t* g = gam_tr + 3 * (m + j) * K;
 #pragma unroll
-        for (int k = 0; k < K; ++k)
+        for (int k = 0; k < (K < KS ? K : KS); ++k)
             gl::wmac3(acc[k], fe3{__ldg(g + 3 * k), __ldg(g + 3 * k + 1), __ldg(g + 3 * k + 2)}, t, t1_2, t2_2);
     }
     gl::wacc3 acch = gl::wzero3();
@@ -347,7 +353,10 @@ __global__ void __launch_bounds__(128) k_deep(const uint64_t* __restrict__ main,
     }
     fe3 sk[K > 0 ? K : 1];
 #pragma unroll
-    for (int k = 0; k < K; ++k) sk[k] = gl::wreduce3(acc[k]);
+    for (int k = 0; k < K; ++k)
+        sk[k] = !POW ? gl::wreduce3(acc[k])
+              : k == 0 ? gl::wreduce3(acc[0])
+                       : gl::mul3(ld3(consts + 3 * (1 + K + k)), sk[0]);
     const fe3 sh = gl::wreduce3(acch);
     fe3 r = gl::mul3(ld3(inv_h + 3 * i), gl::sub3(sh, ld3(consts)));
 #pragma unroll
@@ -360,19 +369,21 @@ __global__ void __launch_bounds__(128) k_deep(const uint64_t* __restrict__ main,
 typedef void (*deep_fn)(const uint64_t*, uint64_t, const uint64_t*, uint64_t, const uint64_t*, uint64_t, uint64_t,
                         uint32_t, const uint64_t*, const uint64_t*, const uint64_t*, const uint64_t*, const uint64_t*,
                         int, uint64_t*);
-static deep_fn deep_kernel(uint32_t K) {
+template <bool POW>
+static deep_fn deep_kernel_t(uint32_t K) {
     switch (K) {
-        case 0: return k_deep<0>;
-        case 1: return k_deep<1>;
-        case 2: return k_deep<2>;
-        case 3: return k_deep<3>;
-        case 4: return k_deep<4>;
-        case 5: return k_deep<5>;
-        case 6: return k_deep<6>;
-        case 7: return k_deep<7>;
-        default: return k_deep<8>;
+        case 0: return k_deep<0, POW>;
+        case 1: return k_deep<1, POW>;
+        case 2: return k_deep<2, POW>;
+        case 3: return k_deep<3, POW>;
+        case 4: return k_deep<4, POW>;
+        case 5: return k_deep<5, POW>;
+        case 6: return k_deep<6, POW>;
+        case 7: return k_deep<7, POW>;
+        default: return k_deep<8, POW>;
     }
 }
+static deep_fn deep_kernel(uint32_t K, bool pow) { return pow ? deep_kernel_t<true>(K) : deep_kernel_t<false>(K); }
 
 // ---------------------------------------------------------------- FRI
 // Fold one layer (evaluations in bit-reversed order, pairs (2j, 2j+1) are
@@ -685,6 +696,24 @@ int sg_deep_composition(sg_ctx* c, void* stream, const uint64_t* d_main, uint64_
         consts[3 * (1 + kk) + 1] = acc[1];
         consts[3 * (1 + kk) + 2] = acc[2];
     }
+    // When every column's coefficients are rho_kk times its first (the
+    // prover's powers of one gamma), the kernel accumulates one sum a row:
+    // rho_kk = g[kk] / g[0] from column 0, checked on every column.
+    bool pow = k > 1;
+    std::vector<uint64_t> rho(3 * k, 0);
+    if (pow) {
+        uint64_t g0i[3];
+        pow = sg_host_fp3_inv(gammas_tr, g0i) == 0;
+        for (uint32_t kk = 0; pow && kk < k; ++kk) mulc(gammas_tr + 3 * kk, g0i, rho.data() + 3 * kk);
+        for (uint64_t j = 1; pow && j < m + a; ++j)
+            for (uint32_t kk = 1; pow && kk < k; ++kk) {
+                uint64_t t[3];
+                mulc(rho.data() + 3 * kk, gammas_tr + 3 * (j * k), t);
+                const uint64_t* g = gammas_tr + 3 * (j * k + kk);
+                pow = t[0] == sg_host_gl_canon(g[0]) && t[1] == sg_host_gl_canon(g[1]) && t[2] == sg_host_gl_canon(g[2]);
+            }
+    }
+    if (pow) consts.insert(consts.end(), rho.begin(), rho.end());
     uint64_t* d_g = nullptr;
     const uint64_t gbytes = 8 * (ng_h + ng_t + consts.size());
     SG_TRY(dev_alloc(ctx, st, gbytes, (void**)&d_g));
@@ -696,7 +725,7 @@ int sg_deep_composition(sg_ctx* c, void* stream, const uint64_t* d_main, uint64_
         rc = SG_ERR_CUDA;
     }
     if (rc == SG_OK) {
-        deep_kernel(k)<<<(unsigned)((rows + 127) / 128), 128, 0, st>>>(d_main, m, d_aux, a, d_parts, p, rows,
+        deep_kernel(k, pow)<<<(unsigned)((rows + 127) / 128), 128, 0, st>>>(d_main, m, d_aux, a, d_parts, p, rows,
                                                                         lr < 0 ? 0 : (uint32_t)lr, d_g, d_g + ng_h,
                                                                         d_g + ng_h + ng_t, d_inv_h, d_inv_t,
                                                                         bitrev_out, d_out);

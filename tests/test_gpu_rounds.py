@@ -81,6 +81,35 @@ def test_deep_matches_oracle(be, rows, m, a, p, k):
     assert (gotb[br] == want).all()
 
 
+@pytest.mark.parametrize("rows,m,a,k", [(256, 17, 2, 2), (1024, 64, 5, 3), (128, 1, 0, 2)])
+def test_deep_with_power_coefficients_matches_oracle(be, rows, m, a, k):
+    """Trace coefficients that are successive powers of one gamma (the
+    prover's): the kernel then accumulates one column sum a row and scales
+    it by gamma^k; against the oracle's full sums. A single broken power
+    falls back to the general kernel, also against the oracle."""
+    rng = np.random.default_rng(7 * rows + m)
+    main, aux, parts = rf(rng, (rows, m)), rf(rng, (rows, 3 * a)), rf(rng, (rows, 3 * 2))
+    h_ood, gh = rf(rng, (3 * 2,)), rf(rng, (3 * 2,))
+    t_ood = rf(rng, (3 * (m + a) * k,))
+    gamma = np.array([int(v) for v in rf(rng, (3,))], np.uint64)
+    gt = np.zeros(3 * (m + a) * k, np.uint64)
+    pw = np.array([1, 0, 0], np.uint64)
+    for q in range(2 + (m + a) * k):
+        if q >= 2:
+            gt[3 * (q - 2):3 * (q - 1)] = pw
+        pw = O.fp3_mul(pw, gamma)
+    inv_h, inv_t = rf(rng, (3 * rows,)), rf(rng, (3 * k * rows,))
+    for broken in (False, True):
+        g = gt.copy()
+        if broken:
+            g[3 * ((m + a) * k - 1)] ^= np.uint64(1)
+        want = O.canon_array(O.deep(main, aux if a else np.zeros((rows, 0), np.uint64),
+                                    parts, h_ood, t_ood, gh, g, inv_h, inv_t, k)).reshape(rows, 3)
+        got = mc.deep_composition_ext3(main, aux, parts, h_ood, t_ood, gh, g, inv_h, inv_t, k, False,
+                                       be).reshape(rows, 3)
+        assert (got == want).all(), broken
+
+
 @pytest.mark.parametrize("h", [1, 2, 4, 64, 1024, 1 << 15])
 def test_fri_fold_layer_matches_oracle(be, h):
     rng = np.random.default_rng(h)
