@@ -228,15 +228,20 @@ static __global__ void k_shift_constraints(const uint64_t* __restrict__ cm, cons
         for (uint32_t i = 0; i < 8; ++i) ts = gl::add(ts, w.M(SH_S + i)), tq = gl::add(tq, w.M(SH_Q + i));
         s.put(gl::sub(ts, 1));
         s.put(gl::sub(tq, 1));
-        // TB_j = sum_s S_s (nd a[j - s] + d a[j + s]), bits past either end zero
+        // TB_j = sum_s S_s (nd a[j - s] + d a[j + s]), bits past either end
+        // zero, evaluated as nd (sum_s S_s a[j - s]) + d (sum_s S_s a[j + s])
+        // with both sums kept unreduced (the same polynomial)
+        uint64_t sv[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) sv[k] = w.M(SH_S + k);
         for (int j = 0; j < 64; ++j) {
-            uint64_t t = 0;
+            gl::wacc lo = gl::wzero(), hi = gl::wzero();
+#pragma unroll
             for (int k = 0; k < 8; ++k) {
-                uint64_t e = 0;
-                if (j - k >= 0) e = gl::mul(nd, w.M(SH_AB + j - k));
-                if (j + k < 64) e = gl::add(e, gl::mul(d, w.M(SH_AB + j + k)));
-                t = gl::add(t, gl::mul(w.M(SH_S + k), e));
+                if (j - k >= 0) gl::wmac(lo, sv[k], w.M(SH_AB + j - k));
+                if (j + k < 64) gl::wmac(hi, sv[k], w.M(SH_AB + j + k));
             }
+            const uint64_t t = gl::add(gl::mul(nd, gl::wreduce(lo)), gl::mul(d, gl::wreduce(hi)));
             s.put(gl::sub(w.M(SH_TB + j), t));
         }
         // the result moves TB by whole bytes: byte k = sum_q Q_q (nd tB[k - q] + d tB[k + q])
@@ -246,16 +251,19 @@ static __global__ void k_shift_constraints(const uint64_t* __restrict__ cm, cons
             for (int j = 7; j >= 0; --j) t = gl::add(gl::add(t, t), w.M(SH_TB + 8 * i + j));
             tB[i] = t;
         }
+        uint64_t qv[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) qv[q] = w.M(SH_Q + q);
         for (int limb = 0; limb < 2; ++limb) {
             uint64_t acc = 0;
             for (int k = 4 * limb + 3; k >= 4 * limb; --k) {
-                uint64_t t = 0;
+                gl::wacc lo = gl::wzero(), hi = gl::wzero();
+#pragma unroll
                 for (int q = 0; q < 8; ++q) {
-                    uint64_t e = 0;
-                    if (k - q >= 0) e = gl::mul(nd, tB[k - q]);
-                    if (k + q < 8) e = gl::add(e, gl::mul(d, tB[k + q]));
-                    t = gl::add(t, gl::mul(w.M(SH_Q + q), e));
+                    if (k - q >= 0) gl::wmac(lo, qv[q], tB[k - q]);
+                    if (k + q < 8) gl::wmac(hi, qv[q], tB[k + q]);
                 }
+                const uint64_t t = gl::add(gl::mul(nd, gl::wreduce(lo)), gl::mul(d, gl::wreduce(hi)));
                 acc = gl::add(gl::mul(acc, 256), t);
             }
             s.put(gl::sub(w.M(limb ? SH_R_HI : SH_R_LO), acc));
