@@ -93,9 +93,9 @@ static __global__ void k_cpu_constraints(const uint64_t* __restrict__ cm, const 
         for (uint32_t op2 = 0; op2 < 2; ++op2)
             for (uint32_t limb = 0; limb < 2; ++limb) {
                 const uint32_t base = op2 ? CPU_RS20 : CPU_RS10;
-                uint64_t t = 0;
-                for (uint32_t k = 1; k < 32; ++k) t = gl::add(t, gl::mul(w.M(base + k), w.M(cpu_xlo(k) + limb)));
-                s.put(gl::sub(w.M((base == CPU_RS10 ? CPU_A_LO : CPU_B_LO) + limb), t));
+                gl::wacc t = gl::wzero();  // the 31 products summed unreduced
+                for (uint32_t k = 1; k < 32; ++k) gl::wmac(t, w.M(base + k), w.M(cpu_xlo(k) + limb));
+                s.put(gl::sub(w.M((base == CPU_RS10 ? CPU_A_LO : CPU_B_LO) + limb), gl::wreduce(t)));
             }
         const uint64_t rl = w.M(CPU_R_LO), rh = w.M(CPU_R_HI), al = w.M(CPU_A_LO), ah = w.M(CPU_A_HI),
                        bl = w.M(CPU_B_LO), bh = w.M(CPU_B_HI), il = w.M(CPU_IMM_LO), ih = w.M(CPU_IMM_HI);
