@@ -716,13 +716,14 @@ int sg_eval_constraints(sg_ctx* c, void* stream, const sg_device_program* prog, 
         // one segment; row-major, each read moves a 32-byte sector for 8
         // bytes). The copy moves 2m words a row, so it pays once a row reads
         // at least m operands; skipped when the budget has no room for it.
-        // The KECCAK and SHIFT kernels take it too; the CPU table's kernel
-        // reads its row's columns nearly in order, so the rest of each
+        // The KECCAK kernel takes it too; the CPU and SHIFT tables' kernels
+        // read their rows' columns nearly in order, so the rest of each
         // sector is still in L1 when it is needed, and measured faster
-        // without the copy (2^22 rows: 24.2 -> 20.5 ms with the copy's time).
+        // without the copy (with the copy's time: CPU 2^22 rows 24.2 ->
+        // 20.5 ms, SHIFT 2^20 rows 3.53 -> 2.82 ms).
         uint64_t* d_cm = nullptr;
         const uint64_t cm_bytes = rows * m * 8;
-        const bool hand_copy = hand && hand_id != SG_AIR_CPU;
+        const bool hand_copy = hand && hand_id == SG_AIR_KECCAK;
         if (prog->node_roots && m >= CM_MIN_COLS && (main_reads >= m || hand_copy) && rows >= 32 &&
             rows / 32 <= 0x7FFFFFFFull && m / 32 < 65535) {
             if (dev_alloc(ctx, st, cm_bytes, (void**)&d_cm) == SG_OK) {
